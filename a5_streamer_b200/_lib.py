@@ -1,0 +1,100 @@
+"""ctypes binding of the C ABI declared in include/a5g.h.
+
+The library is loaded from the package directory; if it is missing the import
+raises instead of falling back to anything else.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "liba5g.so")
+
+A5G_OK, A5G_EINVAL, A5G_ENOMEM, A5G_ECUDA, A5G_TIMEOUT, A5G_ENONFINITE, A5G_ESTATE = range(7)
+STATUS_NAMES = {0: "A5G_OK", 1: "A5G_EINVAL", 2: "A5G_ENOMEM", 3: "A5G_ECUDA",
+                4: "A5G_TIMEOUT", 5: "A5G_ENONFINITE", 6: "A5G_ESTATE"}
+
+
+class A5GError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Params(ctypes.Structure):
+    _fields_ = [
+        ("box_size", ctypes.c_int), ("coord", ctypes.c_int), ("lvls_max", ctypes.c_int),
+        ("dr_base", ctypes.c_double), ("domain_len_z", ctypes.c_double),
+        ("applied_fld", ctypes.c_double), ("epsilon_diel", ctypes.c_double),
+        ("dt_max", ctypes.c_double), ("use_drt", ctypes.c_int), ("n_cycle_base", ctypes.c_int),
+        ("ref_init_time", ctypes.c_double), ("crv_refine", ctypes.c_double),
+        ("n_seeds", ctypes.c_int),
+        ("seed_r0", (ctypes.c_double * 2) * 8), ("seed_r1", (ctypes.c_double * 2) * 8),
+        ("seed_width", ctypes.c_double * 8),
+    ]
+
+
+# name -> (restype, argtypes); every function returns an a5g_status int
+_P = ctypes.c_void_p
+_D = ctypes.c_double
+_I = ctypes.c_int
+_PD = ctypes.POINTER(ctypes.c_double)
+_PI = ctypes.POINTER(ctypes.c_int)
+SIGNATURES = {
+    "a5g_last_error": (ctypes.c_char_p, []),
+    "a5g_version": (_I, []),
+    "a5g_create": (_I, [ctypes.POINTER(Params), ctypes.POINTER(_P)]),
+    "a5g_destroy": (_I, [_P]),
+    "a5g_set_table": (_I, [_P, _I, _I, _D, _D, _PD]),
+    "a5g_upload_tree": (_I, [_P, _I, _I, _I, _PI, _PD, _PI, _PI]),
+    "a5g_upload_cc": (_I, [_P, _I, _PD]),
+    "a5g_download_cc": (_I, [_P, _I, _PD]),
+    "a5g_upload_fc": (_I, [_P, _I, _I, _PD]),
+    "a5g_download_fc": (_I, [_P, _I, _I, _PD]),
+    "a5g_tree_copy_cc": (_I, [_P, _I, _I]),
+    "a5g_fluxes_koren": (_I, [_P, _D]),
+    "a5g_consistent_fluxes": (_I, [_P]),
+    "a5g_update_solution": (_I, [_P, _D]),
+    "a5g_restrict_tree": (_I, [_P, _I]),
+    "a5g_gc_tree": (_I, [_P, _I, _I]),
+    "a5g_average_dens": (_I, [_P]),
+    "a5g_compute_fld": (_I, [_P, _I]),
+    "a5g_fas_fmg": (_I, [_P, _I, _I]),
+    "a5g_fld_from_pot": (_I, [_P]),
+    "a5g_dt_reductions": (_I, [_P, _PD]),
+    "a5g_get_max_dt": (_I, [_P, _PD]),
+    "a5g_ref_flags": (_I, [_P, _D, _PI]),
+    "a5g_prolong_new": (_I, [_P, _PI, _PI]),
+    "a5g_step": (_I, [_P, _D]),
+    "a5g_step_batch": (_I, [ctypes.POINTER(_P), _I, _PD]),
+    "a5g_sync": (_I, [_P]),
+    "a5g_n_leaf_cells": (_I, [_P, ctypes.POINTER(ctypes.c_longlong)]),
+}
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with "
+                              "`python -m a5_streamer_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(code: int) -> None:
+    if code != A5G_OK:
+        msg = lib().a5g_last_error()
+        raise A5GError(code, msg.decode() if msg else "")
+
+
+def call(name: str, *args) -> None:
+    check(getattr(lib(), name)(*args))

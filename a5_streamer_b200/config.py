@@ -1,0 +1,242 @@
+"""Run configuration for the streamer time step.
+
+Mirrors the reference's configuration surface (``ST_create_cfg`` in
+src/m_streamer.f90:145-228, read by ``ST_read_cfg_files`` / ``ST_load_cfg``,
+src/m_streamer.f90:364-417) plus the keys the 8 mm / cylindrical workloads need
+that the reference driver does not have: a rectangular base grid of several
+boxes, a finest level, and the dielectric-relaxation step limit.
+
+The reference's text format is ``name = v1 v2 # comment``; several files are
+applied in order and later ones override earlier ones
+(fosito/m_config.f90:83-182). :func:`load_cfg_files` reads that format.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+import re
+from dataclasses import dataclass, field
+from typing import Dict, List, Sequence, Tuple
+
+# Column order of the transport table (src/m_streamer.f90:37-41).
+TD_COLUMNS = ("mobility", "diffusion", "alpha", "eta")
+
+# Seed fall-off types (src/m_geom.f90:8-11).
+FALLOFF = {"sigmoid": 1, "gaussian": 2, "smoothstep": 3, "step": 4}
+
+
+@dataclass
+class Seed:
+    r0: Tuple[float, ...]
+    r1: Tuple[float, ...]
+    dens: float
+    width: float
+    falloff: int = 2
+
+
+@dataclass
+class StreamerConfig:
+    dim: int = 2
+    coord: str = "xyz"                  # "xyz" or "cyl"
+    box_size: int = 8
+    n_base: Tuple[int, ...] = (4, 4)    # base boxes per direction
+    domain_len: Tuple[float, ...] = (8e-3, 8e-3)
+    lvls_max: int = 7
+    applied_fld: float = 2.5e6
+    epsilon_diel: float = 1.0
+    bg_dens: float = 1e15
+    seeds: List[Seed] = field(default_factory=list)
+    dt_max: float = 1e-10
+    num_steps_amr: int = 2
+    end_time: float = 2e-9
+    use_drt: bool = True
+    lkptbl_size: int = 200
+    lkptbl_max_fld: float = 3e7
+    # transport input pairs per column: name -> (x list, y list)
+    td: Dict[str, Tuple[List[float], List[float]]] = field(default_factory=dict)
+    photoi_enabled: bool = False
+
+    # --- derived quantities -------------------------------------------------
+    @property
+    def dr_base(self) -> float:
+        return self.domain_len[0] / (self.n_base[0] * self.box_size)
+
+    @property
+    def domain_len_z(self) -> float:
+        return self.domain_len[self.dim - 1]
+
+    @property
+    def is_cyl(self) -> bool:
+        return self.coord == "cyl"
+
+    @property
+    def n_cycle_base(self) -> int:
+        # src/streamer_2d.f90:43 (8) and src/streamer_cyl.f90:46 (4)
+        return 4 if self.is_cyl else 8
+
+    @property
+    def ref_init_time(self) -> float:
+        # src/streamer_2d.f90:200, src/streamer_cyl.f90:212, src/streamer_3d.f90
+        if self.is_cyl:
+            return 5.0e-9
+        return 2.0e-9 if self.dim == 2 else 2.5e-9
+
+    @property
+    def crv_refine(self) -> float:
+        # src/streamer_2d.f90:214 (1), src/streamer_cyl.f90:226 (0), 3D 0.1
+        if self.is_cyl:
+            return 0.0
+        return 1.0 if self.dim == 2 else 0.1
+
+    @property
+    def applied_voltage(self) -> float:
+        # src/m_streamer.f90:411: ST_applied_voltage = -ST_domain_len * fld
+        return -self.domain_len_z * self.applied_fld
+
+    def dr_at(self, lvl: int) -> float:
+        return self.dr_base * 0.5 ** (lvl - 1)
+
+    def validate(self) -> None:
+        if self.dim != 2:
+            raise ValueError("only dim=2 is implemented")
+        if self.coord not in ("xyz", "cyl"):
+            raise ValueError(f"coord must be 'xyz' or 'cyl', got {self.coord!r}")
+        nc = self.box_size
+        if nc < 4 or nc & (nc - 1):
+            raise ValueError("box_size must be a power of two >= 4")
+        if len(self.n_base) != self.dim or len(self.domain_len) != self.dim:
+            raise ValueError("n_base and domain_len need one entry per dimension")
+        dy = self.domain_len[1] / (self.n_base[1] * nc)
+        if abs(dy - self.dr_base) > 1e-12 * self.dr_base:
+            raise ValueError("base cells must be square: domain_len / n_base must agree")
+        if len(self.seeds) > 8:
+            raise ValueError("at most 8 seeds")
+        for name in TD_COLUMNS:
+            if name not in self.td:
+                raise ValueError(f"transport column {name!r} missing")
+            x, y = self.td[name]
+            if len(x) != len(y) or len(x) < 1 or len(x) > 4096:
+                raise ValueError(f"transport column {name!r}: bad length")
+        if not (1 <= self.lvls_max <= 30):
+            raise ValueError("lvls_max must be in 1..30")
+
+
+def table_nodes(n_rows: int, x_max: float, x_min: float = 0.0) -> List[float]:
+    """The x grid of a lookup table: LT_get_xdata (fosito/m_lookup_table.f90:180-189)."""
+    inv_dx = (n_rows - 1) / (x_max - x_min)
+    dx = 1 / inv_dx
+    return [x_min + (ix - 1) * dx for ix in range(1, n_rows + 1)]
+
+
+def synthetic_transport(n_rows: int = 200, x_max: float = 3e7, mobility: float = 0.03,
+                        diffusion: float = 0.1, alpha_a: float = 4.3e5,
+                        alpha_b: float = 1.4e7, eta_a: float = 0.0,
+                        eta_b: float = 4e6) -> Dict[str, Tuple[List[float], List[float]]]:
+    """Synthetic transport pairs placed exactly on the table nodes, so that the
+    table built from them holds the analytic values: mu, D constant,
+    alpha = A exp(-B/|E|) (alpha(0) = 0), eta = a exp(-b/|E|)."""
+    xs = table_nodes(n_rows, x_max)
+    mu = [mobility] * n_rows
+    dif = [diffusion] * n_rows
+    alpha = [alpha_a * math.exp(-alpha_b / x) if x > 0 else 0.0 for x in xs]
+    eta = [eta_a * math.exp(-eta_b / x) if (x > 0 and eta_a != 0.0) else 0.0 for x in xs]
+    return {"mobility": (xs, mu), "diffusion": (xs, dif), "alpha": (xs, alpha),
+            "eta": (xs, eta)}
+
+
+def cartesian_8mm(**overrides) -> StreamerConfig:
+    """2D Cartesian FP64 case: 8 mm x 8 mm, 4x4 base boxes of 8^2 cells,
+    finest dx 3.906 um (level 7), E_bg = 2.5e6 V/m, background 1e15 m^-3,
+    Gaussian seed 1e19 m^-3 with sigma 0.2 mm (GM_gaussian width sqrt(2) sigma)
+    at (4, 7) mm, synthetic transport, no photoionization, t_end = 2 ns."""
+    sigma = 0.2e-3
+    cfg = StreamerConfig(
+        dim=2, coord="xyz", box_size=8, n_base=(4, 4), domain_len=(8e-3, 8e-3),
+        lvls_max=7, applied_fld=2.5e6, epsilon_diel=1.0, bg_dens=1e15,
+        seeds=[Seed(r0=(4e-3, 7e-3), r1=(4e-3, 7e-3), dens=1e19,
+                    width=math.sqrt(2.0) * sigma, falloff=2)],
+        dt_max=1e-10, num_steps_amr=2, end_time=2e-9, use_drt=True,
+        lkptbl_size=200, lkptbl_max_fld=3e7, td=synthetic_transport())
+    return dataclasses.replace(cfg, **overrides)
+
+
+def cylindrical_16mm(**overrides) -> StreamerConfig:
+    """Axisymmetric (r, z) FP64 case: R = 8 mm, Z = 16 mm (two base boxes
+    stacked in z, base dx 1 mm), E_bg = 2e6 V/m, background 1e15 m^-3, seed
+    1e19 m^-3 with sigma 0.1 mm on the axis at z = 15 mm, attachment
+    eta = 1e3 exp(-4e6/|E|). Photoionization is not part of this form."""
+    sigma = 0.1e-3
+    cfg = StreamerConfig(
+        dim=2, coord="cyl", box_size=8, n_base=(1, 2), domain_len=(8e-3, 16e-3),
+        lvls_max=10, applied_fld=2.0e6, epsilon_diel=1.0, bg_dens=1e15,
+        seeds=[Seed(r0=(0.0, 15e-3), r1=(0.0, 15e-3), dens=1e19,
+                    width=math.sqrt(2.0) * sigma, falloff=2)],
+        dt_max=1e-10, num_steps_amr=2, end_time=10e-9, use_drt=True,
+        lkptbl_size=200, lkptbl_max_fld=3e7,
+        td=synthetic_transport(eta_a=1.0e3, eta_b=4e6))
+    return dataclasses.replace(cfg, **overrides)
+
+
+# --- the reference's text configuration format -------------------------------
+_LINE = re.compile(r"^\s*([A-Za-z_][A-Za-z0-9_]*)\s*=\s*(.*?)\s*$")
+
+
+def parse_cfg_text(text: str) -> Dict[str, List[str]]:
+    """Parse ``name = v1 v2 ...  # comment`` lines (fosito/m_config.f90:83-182)."""
+    out: Dict[str, List[str]] = {}
+    for raw in text.splitlines():
+        line = raw.split("#", 1)[0]
+        m = _LINE.match(line)
+        if not m:
+            continue
+        out[m.group(1)] = m.group(2).split()
+    return out
+
+
+def _f(v: Sequence[str]) -> float:
+    return float(v[0].replace("d", "e").replace("D", "E"))
+
+
+def load_cfg_files(paths: Sequence[str], base: StreamerConfig | None = None) -> StreamerConfig:
+    """Apply reference-format config files in order on top of ``base``."""
+    cfg = base if base is not None else cartesian_8mm()
+    kv: Dict[str, List[str]] = {}
+    for p in paths:
+        with open(p) as fh:
+            kv.update(parse_cfg_text(fh.read()))
+    upd: Dict[str, object] = {}
+    if "end_time" in kv: upd["end_time"] = _f(kv["end_time"])
+    if "box_size" in kv: upd["box_size"] = int(kv["box_size"][0])
+    if "applied_fld" in kv: upd["applied_fld"] = _f(kv["applied_fld"])
+    if "epsilon_diel" in kv: upd["epsilon_diel"] = _f(kv["epsilon_diel"])
+    if "bg_dens" in kv: upd["bg_dens"] = _f(kv["bg_dens"])
+    if "dt_max" in kv: upd["dt_max"] = _f(kv["dt_max"])
+    if "num_steps_amr" in kv: upd["num_steps_amr"] = int(kv["num_steps_amr"][0])
+    if "lkptbl_size" in kv: upd["lkptbl_size"] = int(kv["lkptbl_size"][0])
+    if "lkptbl_max_fld" in kv: upd["lkptbl_max_fld"] = _f(kv["lkptbl_max_fld"])
+    if "photoi_enabled" in kv: upd["photoi_enabled"] = kv["photoi_enabled"][0].upper().startswith("T")
+    if "lvls_max" in kv: upd["lvls_max"] = int(kv["lvls_max"][0])
+    if "use_drt" in kv: upd["use_drt"] = kv["use_drt"][0].upper().startswith("T")
+    if "coord" in kv: upd["coord"] = kv["coord"][0]
+    if "n_base" in kv: upd["n_base"] = tuple(int(v) for v in kv["n_base"])
+    if "domain_len" in kv:
+        vals = [_f([v]) for v in kv["domain_len"]]
+        if len(vals) == 1:
+            vals = vals * cfg.dim
+        upd["domain_len"] = tuple(vals)
+    out = dataclasses.replace(cfg, **upd)
+    if "seed_dens" in kv:
+        dl = out.domain_len_z
+        dens = [_f([v]) for v in kv["seed_dens"]]
+        r0 = [_f([v]) for v in kv.get("seed_rel_r0", [])]
+        r1 = [_f([v]) for v in kv.get("seed_rel_r1", [])]
+        wid = [_f([v]) for v in kv.get("seed_width", [])]
+        fo = [int(v) for v in kv.get("seed_falloff", ["1"] * len(dens))]
+        d = out.dim
+        if len(r0) != d * len(dens) or len(r1) != d * len(dens) or len(wid) != len(dens):
+            raise ValueError("seed_... variables have incompatible size")
+        seeds = [Seed(r0=tuple(dl * x for x in r0[d * n:d * n + d]),
+                      r1=tuple(dl * x for x in r1[d * n:d * n + d]),
+                      dens=dens[n], width=wid[n], falloff=fo[n]) for n in range(len(dens))]
+        out = dataclasses.replace(out, seeds=seeds)
+    return out

@@ -1,0 +1,1628 @@
+// a5g — sm_100a device path for a5_streamer's per-timestep work (2D).
+//
+// Execution model. The trees of the streamer workloads are small (a few
+// thousand to a few hundred thousand cells) and every multigrid half-sweep,
+// ghost fill or restriction is a dependency point across the boxes of a
+// level: one step holds about a thousand of them. Launching a kernel (or
+// crossing a grid-wide barrier) per phase would make the step launch-bound.
+// Instead one persistent thread block runs a whole operation -- up to a full
+// time step -- for one run, with __syncthreads() between phases; independent
+// runs are batched as one block each in the same launch. All box data stay
+// resident in device memory (L2-resident for these sizes) between calls.
+//
+// Thread mapping: a block of NTHR threads is split into groups of GT = 64
+// threads; a group owns one box at a time (one thread per interior cell of
+// an 8x8 box, one per ghost cell, or one per face), and the groups stride
+// over the box list of the current phase.
+//
+// Arithmetic is IEEE double with --fmad=false, so every expression rounds as
+// in the reference's Fortran (compiled for x86-64 without FMA) and as in the
+// CPU oracle; each device routine cites the reference routine it follows.
+#include "../../include/a5g.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace {
+
+constexpr int NC = 8;                 // box_size on levels >= 1
+constexpr int SLOT = (NC + 2) * (NC + 2);
+constexpr int FSLOT = (NC + 1) * NC;
+constexpr int GT = 64;                // threads per box group
+constexpr int NTHR = 512;             // threads per block
+constexpr int NGRP = NTHR / GT;
+constexpr int MAXLEV = 40;            // levels min_lvl..max_lvl+1
+
+// Variable indices, src/m_streamer.f90:17-43 (0-based).
+enum { I_ELEC = 0, I_PION, I_ELEC_OLD, I_PION_OLD, I_PHI, I_FLD, I_RHS, I_PHO, I_EPS };
+enum { F_ELEC = 0, F_FLD = 1 };
+enum { C_MOB = 0, C_DIF = 1, C_ALPHA = 2, C_ETA = 3 };
+// Ghost-cell kinds: refinement-boundary / physical-boundary routine pairs.
+enum { GC_LIM = 0, GC_INTERP = 1, GC_PHI = 2 };
+
+// fosito/m_units_constants.f90:201-202
+constexpr double UC_EPS0 = 8.8541878176e-12;
+constexpr double UC_ELEM_CHARGE = 1.6022e-19;
+
+struct BoxMeta {
+  int lvl, nc, ix0, ix1;
+  int parent, ch[4], nb[4], p0, p1, p2;
+  double dr, r0, r1, p3;
+};
+static_assert(sizeof(BoxMeta) == 96, "BoxMeta layout");
+
+struct RunDev {
+  int capacity, min_lvl, max_lvl, lvls_max;
+  int coord, n_cycle_base, nlev, pad0;
+  int lv_off[3][MAXLEV + 1];   // [ids|leaves|parents][level index] -> start in lists
+  int new_off[MAXLEV + 1];     // new-box lists for prolong_new
+  int *lists;
+  int *new_lists;
+  BoxMeta *meta;
+  double *cc, *fx, *fy;
+  const double *tbl;
+  int tbl_rows, pad1;
+  double tbl_xmin, tbl_inv_dx;
+  double applied_voltage, domain_len_z, epsilon_diel;
+  double ref_init_time, crv_refine;
+  int n_seeds, pad2;
+  double seed_r0[8][2], seed_r1[8][2], seed_width[8];
+  double *scal;                // dt reductions out
+  int *flags;                  // refinement flags out
+  int *status;
+};
+
+enum OpCode {
+  OP_COPY = 1, OP_FLUXES, OP_CONSISTENT, OP_UPDATE, OP_RESTRICT, OP_GC, OP_AVERAGE,
+  OP_COMPUTE_FLD, OP_FMG, OP_FLD_FROM_POT, OP_DT_RED, OP_REF_FLAGS, OP_PROLONG_NEW,
+  OP_STEP, OP_SET_RHS
+};
+struct Op {
+  int code, i0, i1, i2;
+  double d0, d1;
+};
+
+__constant__ int c_nb_dix[4][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}};
+__constant__ int c_ch_dix[4][2] = {{0, 0}, {1, 0}, {0, 1}, {1, 1}};
+__constant__ int c_ch_adj_nb[4][2] = {{0, 2}, {1, 3}, {0, 1}, {2, 3}};
+
+// ---------------------------------------------------------------------------
+// Accessors. Box `id` of variable v: slot (v * capacity + id); the box's own
+// (nc+2)^2 values are stored i-fastest with row length nc+2.
+__device__ __forceinline__ double *CC(const RunDev &R, int v, int id) {
+  return R.cc + ((size_t)v * R.capacity + id) * SLOT;
+}
+__device__ __forceinline__ double *FX(const RunDev &R, int f, int id) {
+  return R.fx + ((size_t)f * R.capacity + id) * FSLOT;
+}
+__device__ __forceinline__ double *FY(const RunDev &R, int f, int id) {
+  return R.fy + ((size_t)f * R.capacity + id) * FSLOT;
+}
+// fx(i, j): i in 1..nc+1, j in 1..nc;  fy(i, j): i in 1..nc, j in 1..nc+1
+__device__ __forceinline__ int fxi(int i, int j, int nc) { return (i - 1) + (nc + 1) * (j - 1); }
+__device__ __forceinline__ int fyi(int i, int j, int nc) { return (i - 1) + nc * (j - 1); }
+
+__device__ __forceinline__ int list_n(const RunDev &R, int kind, int lvl) {
+  int li = lvl - R.min_lvl;
+  if (li < 0 || li >= R.nlev) return 0;
+  return R.lv_off[kind][li + 1] - R.lv_off[kind][li];
+}
+__device__ __forceinline__ const int *list_p(const RunDev &R, int kind, int lvl) {
+  return R.lists + R.lv_off[kind][lvl - R.min_lvl];
+}
+// Contiguous list of a kind over levels [lo, hi]
+__device__ __forceinline__ void list_range(const RunDev &R, int kind, int lo, int hi,
+                                           const int *&p, int &n) {
+  lo = max(lo, R.min_lvl);
+  hi = min(hi, R.max_lvl);
+  if (hi < lo) { p = R.lists; n = 0; return; }
+  int a = R.lv_off[kind][lo - R.min_lvl], b = R.lv_off[kind][hi - R.min_lvl + 1];
+  p = R.lists + a;
+  n = b - a;
+}
+
+template <class F>
+__device__ __forceinline__ void box_loop(const int *list, int n, F &&f) {
+  const int g = threadIdx.x / GT, t = threadIdx.x % GT;
+  for (int b = g; b < n; b += NGRP) f(list[b], t);
+}
+
+// afivo/src/m_aX_utils.f90:227-239 (a$D_get_child_offset); nb < 0: absent
+__device__ __forceinline__ void child_offset(const BoxMeta &m, int nb, int &o0, int &o1) {
+  if (m.lvl > 1) {
+    o0 = ((m.ix0 - 1) & 1) * (m.nc >> 1);
+    o1 = ((m.ix1 - 1) & 1) * (m.nc >> 1);
+    if (nb >= 0) { o0 -= c_nb_dix[nb][0] * m.nc; o1 -= c_nb_dix[nb][1] * m.nc; }
+  } else {
+    o0 = 0;
+    o1 = 0;
+    if (nb >= 0) {
+      o0 -= c_nb_dix[nb][0] * (m.nc >> 1);
+      o1 -= c_nb_dix[nb][1] * (m.nc >> 1);
+    }
+  }
+}
+
+// gfortran's inline NORM2 for two elements (scaled sum of squares)
+__device__ __forceinline__ double norm2_2(double x0, double x1) {
+  double scale = 0.0, ssq = 1.0;
+  double xs[2] = {x0, x1};
+#pragma unroll
+  for (int k = 0; k < 2; k++) {
+    if (xs[k] != 0.0) {
+      double ax = fabs(xs[k]);
+      if (scale < ax) {
+        double v = scale / ax;
+        ssq = 1.0 + ssq * v * v;
+        scale = ax;
+      } else {
+        double v = ax / scale;
+        ssq += v * v;
+      }
+    }
+  }
+  return scale * sqrt(ssq);
+}
+
+// fosito/m_lookup_table.f90:107-125 (get_loc) and 154-161 (LT_get_col_at_loc)
+struct Loc { int ix; double fr; };
+__device__ __forceinline__ Loc get_loc(const RunDev &R, double x) {
+  double frac = (x - R.tbl_xmin) * R.tbl_inv_dx;
+  Loc l;
+  if (frac < 2.0e9 && frac > -2.0e9) {
+    l.ix = (int)ceil(frac);
+    l.fr = l.ix - frac;
+  } else {
+    l.ix = frac > 0 ? R.tbl_rows : 0;
+    l.fr = 0;
+  }
+  if (l.ix < 1) { l.ix = 1; l.fr = 1; }
+  else if (l.ix >= R.tbl_rows) { l.ix = R.tbl_rows - 1; l.fr = 0; }
+  return l;
+}
+__device__ __forceinline__ double col_at(const RunDev &R, int c, const Loc &l) {
+  const double *T = R.tbl + (size_t)R.tbl_rows * c;
+  return l.fr * __ldg(T + l.ix - 1) + (1 - l.fr) * __ldg(T + l.ix);
+}
+
+// src/m_streamer.f90:339-362 (koren_mlim)
+__device__ __forceinline__ double koren_mlim(double a, double b) {
+  const double sixth = 1 / 6.0;
+  double aa = a * a, ab = a * b;
+  if (ab <= 0) return 0;
+  if (aa <= 0.25 * ab) return a;
+  if (aa <= 2.5 * ab) return sixth * (b + 2 * a);
+  return b;
+}
+
+// ---------------------------------------------------------------------------
+// Ghost cells (afivo/src/m_aX_gc.f90). Value of side ghost (nb, k), k = 1..nc,
+// of box id for variable iv.
+__device__ double ghost_value(const RunDev &R, const BoxMeta &m, int id, int iv, int nb,
+                              int k, int kind) {
+  const int nc = m.nc, ncg = nc + 2;
+  const double *own = CC(R, iv, id);
+  const int nb_id = m.nb[nb];
+  const int dim = nb >> 1;
+  const bool low = (nb & 1) == 0;
+  if (nb_id > 0) {
+    // sides_from_nb, m_aX_gc.f90:368-402
+    const double *nbc = CC(R, iv, nb_id);
+    if (dim == 0) return nbc[(low ? nc : 1) + ncg * k];
+    return nbc[k + ncg * (low ? nc : 1)];
+  }
+  if (nb_id == 0) {
+    if (kind == GC_PHI) {
+      // mg$D_sides_rb (m_aX_mg.f90:261-301) after a$D_gc_prolong0 (m_aX_gc.f90:71-86)
+      int o0, o1;
+      child_offset(m, -1, o0, o1);
+      const BoxMeta &pm = R.meta[m.parent];
+      const double *par = CC(R, iv, m.parent);
+      const int pncg = pm.nc + 2;
+      const int ix = low ? 1 : nc, di = low ? 1 : -1;
+      const int dk = -1 + 2 * (k & 1);
+      if (dim == 0) {
+        int ig = ix - di;
+        double g = par[(o0 + ((ig + 1) >> 1)) + pncg * (o1 + ((k + 1) >> 1))];
+        return 0.5 * g + own[ix + ncg * k] -
+               0.25 * (own[(ix + di) + ncg * k] + own[ix + ncg * (k + dk)]);
+      } else {
+        int jg = ix - di;
+        double g = par[(o0 + ((k + 1) >> 1)) + pncg * (o1 + ((jg + 1) >> 1))];
+        return 0.5 * g + own[k + ncg * ix] -
+               0.25 * (own[(k + dk) + ncg * ix] + own[k + ncg * (ix + di)]);
+      }
+    }
+    // a$D_gc_interp / a$D_gc_interp_lim, m_aX_gc.f90:90-295
+    const double sixth = 1 / 6.0, third = 1 / 3.0;
+    int o0, o1;
+    child_offset(m, nb, o0, o1);
+    const int pn = R.meta[m.parent].nb[nb];
+    const double *pc = CC(R, iv, pn);
+    const int ix_f = low ? 1 : nc, ix_c = low ? nc : 1;
+    double c1, c2, f;
+    if (dim == 0) {
+      int j_c1 = o1 + ((k + 1) >> 1);
+      int j_c2 = j_c1 + 1 - 2 * (k & 1);
+      c1 = pc[ix_c + ncg * j_c1];
+      c2 = pc[ix_c + ncg * j_c2];
+      f = own[ix_f + ncg * k];
+    } else {
+      int i_c1 = o0 + ((k + 1) >> 1);
+      int i_c2 = i_c1 + 1 - 2 * (k & 1);
+      c1 = pc[i_c1 + ncg * ix_c];
+      c2 = pc[i_c2 + ncg * ix_c];
+      f = own[k + ncg * ix_f];
+    }
+    double v = 0.5 * c1 + sixth * c2 + third * f;
+    if (kind == GC_LIM && v > 2 * c1) v = 2 * c1;
+    return v;
+  }
+  // physical boundary
+  if (kind == GC_PHI) {
+    // sides_bc_pot, src/streamer_2d.f90:620-638 (cyl :395-413)
+    switch (nb) {
+      case 0: return own[1 + ncg * k];
+      case 1: return own[nc + ncg * k];
+      case 2: return -own[k + ncg * 1];
+      default: return 2 * R.applied_voltage - own[k + ncg * nc];
+    }
+  }
+  // a$D_gc_neumann, m_aX_gc.f90:298-330
+  switch (nb) {
+    case 0: return own[1 + ncg * k];
+    case 1: return own[nc + ncg * k];
+    case 2: return own[k + ncg * 1];
+    default: return own[k + ncg * nc];
+  }
+}
+
+__device__ __forceinline__ int ghost_index(int nb, int k, int nc) {
+  const int ncg = nc + 2;
+  switch (nb) {
+    case 0: return 0 + ncg * k;
+    case 1: return (nc + 1) + ncg * k;
+    case 2: return k;
+    default: return k + ncg * (nc + 1);
+  }
+}
+
+// a$D_gc_box for one box, group thread t (4*nc side ghosts).
+__device__ __forceinline__ void gc_box(const RunDev &R, int id, int t, int iv, int kind) {
+  const BoxMeta &m = R.meta[id];
+  const int nc = m.nc;
+  if (t < 4 * nc) {
+    int nb = t / nc, k = t % nc + 1;
+    double v = ghost_value(R, m, id, iv, nb, k, kind);
+    CC(R, iv, id)[ghost_index(nb, k, nc)] = v;
+  }
+}
+
+// a$D_gc_tree for one or two variables, level by level (m_aX_gc.f90:28-46)
+__device__ void gc_tree(const RunDev &R, int iv0, int iv1, int kind) {
+  for (int lvl = R.min_lvl; lvl <= R.max_lvl; lvl++) {
+    int n = list_n(R, 0, lvl);
+    const int *ids = list_p(R, 0, lvl);
+    box_loop(ids, n, [&](int id, int t) {
+      gc_box(R, id, t, iv0, kind);
+      if (iv1 >= 0) gc_box(R, id, t, iv1, kind);
+    });
+    __syncthreads();
+  }
+}
+
+// Second ghost layer, afivo/src/m_aX_gc.f90:407-622 (gc2_box with
+// gc2_prolong1 on refinement boundaries and gc2_neumann on physical ones)
+__device__ double gc2_value(const RunDev &R, const BoxMeta &m, int id, int iv, int nb, int k) {
+  const int nc = m.nc, ncg = nc + 2;
+  const int nb_id = m.nb[nb];
+  const int dim = nb >> 1;
+  if (nb_id > 0) {
+    const double *n = CC(R, iv, nb_id);
+    switch (nb) {
+      case 0: return n[(nc - 1) + ncg * k];
+      case 1: return n[2 + ncg * k];
+      case 2: return n[k + ncg * (nc - 1)];
+      default: return n[k + ncg * 2];
+    }
+  }
+  if (nb_id == 0) {
+    int o0, o1;
+    child_offset(m, nb, o0, o1);
+    const double *P = CC(R, iv, R.meta[m.parent].nb[nb]);
+    const int ix = (nb & 1) * (nc + 3) - 1;  // -1 or nc+2
+    const int hs = (ix + 1) >> 1, par = ix & 1;
+    int i_c1, i_c2, j_c1, j_c2;
+    if (dim == 0) {
+      i_c1 = o0 + hs;
+      i_c2 = i_c1 + 1 - 2 * par;
+      j_c1 = o1 + ((k + 1) >> 1);
+      j_c2 = j_c1 + 1 - 2 * (k & 1);
+    } else {
+      j_c1 = o1 + hs;
+      j_c2 = j_c1 + 1 - 2 * par;
+      i_c1 = o0 + ((k + 1) >> 1);
+      i_c2 = i_c1 + 1 - 2 * (k & 1);
+    }
+    return 0.5 * P[i_c1 + ncg * j_c1] + 0.25 * P[i_c2 + ncg * j_c1] +
+           0.25 * P[i_c1 + ncg * j_c2];
+  }
+  const double *own = CC(R, iv, id);
+  switch (nb) {
+    case 0: return own[2 + ncg * k];
+    case 1: return own[(nc - 1) + ncg * k];
+    case 2: return own[k + ncg * 2];
+    default: return own[k + ncg * (nc - 1)];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Flux and source update.
+
+// fluxes_koren, src/streamer_2d.f90:384-489 (cyl :416-521 is the same)
+__device__ void fluxes_koren(const RunDev &R, double dt) {
+  const int *ids;
+  int n;
+  list_range(R, 1, R.min_lvl, R.max_lvl, ids, n);
+  const double fac = -0.8 * UC_EPS0 / (UC_ELEM_CHARGE * dt);
+  box_loop(ids, n, [&](int id, int t) {
+    const BoxMeta &m = R.meta[id];
+    const int nc = m.nc, ncg = nc + 2;
+    const double inv_dr = 1 / m.dr;
+    const double *e = CC(R, I_ELEC, id), *fl = CC(R, I_FLD, id);
+    double *fxe = FX(R, F_ELEC, id), *fye = FY(R, F_ELEC, id);
+    const double *fxf = FX(R, F_FLD, id), *fyf = FY(R, F_FLD, id);
+    const int nf = (nc + 1) * nc;
+    for (int f = t; f < 2 * nf; f += GT) {
+      const bool xd = f < nf;
+      const int g = xd ? f : f - nf;
+      int i, j;
+      if (xd) { i = g % (nc + 1) + 1; j = g / (nc + 1) + 1; }
+      else { i = g % nc + 1; j = g / nc + 1; }
+      // stride between the two cells adjacent to the face
+      const int s = xd ? 1 : ncg;
+      const int c = i + ncg * j;          // cell (i, j): high side of the face
+      const int pos = xd ? i : j;         // face index along the direction
+      double fld_avg = 0.5 * (fl[c] + fl[c - s]);
+      Loc loc = get_loc(R, fld_avg);
+      double mobility = col_at(R, C_MOB, loc);
+      double diff_coeff = col_at(R, C_DIF, loc);
+      double fld = xd ? fxf[fxi(i, j, nc)] : fyf[fyi(i, j, nc)];
+      double v_drift = -mobility * fld;
+      double gradc = e[c] - e[c - s];
+      double fv;
+      const int k = xd ? j : i;
+      if (v_drift < 0.0) {
+        double tmp = (pos == nc + 1) ? gc2_value(R, m, id, I_ELEC, xd ? 1 : 3, k) : e[c + s];
+        double gradn = tmp - e[c];
+        fv = v_drift * (e[c] - koren_mlim(gradc, gradn));
+        if (fv < fac * fld) fv = fac * fld;
+      } else {
+        double tmp = (pos == 1) ? gc2_value(R, m, id, I_ELEC, xd ? 0 : 2, k) : e[c - 2 * s];
+        double gradp = e[c - s] - tmp;
+        fv = v_drift * (e[c - s] + koren_mlim(gradc, gradp));
+        if (fv > fac * fld) fv = fac * fld;
+      }
+      fv = fv - diff_coeff * gradc * inv_dr;
+      if (xd) fxe[fxi(i, j, nc)] = fv;
+      else fye[fyi(i, j, nc)] = fv;
+    }
+  });
+}
+
+// a$D_consistent_fluxes([f_elec]) with flux_from_children,
+// afivo/src/m_aX_core.f90:818-930. All parent levels in one phase: the faces
+// written (coarse leaves next to refined neighbours) are never read here.
+__device__ void consistent_fluxes(const RunDev &R) {
+  const int *ids;
+  int n;
+  list_range(R, 2, R.min_lvl, R.max_lvl - 1, ids, n);
+  box_loop(ids, n, [&](int id, int t) {
+    const BoxMeta &m = R.meta[id];
+    const int nc = m.nc, nch = nc >> 1;
+    if (t >= 4 * nc) return;
+    const int nb = t / nc, mm0 = t % nc, kk = mm0 / nch, mm = mm0 % nch;
+    const int nb_id = m.nb[nb];
+    if (nb_id <= 0) return;
+    if (R.meta[nb_id].ch[0] != 0) return;
+    const bool low = (nb & 1) == 0;
+    const int i = low ? 1 : nc + 1, i_nb = low ? nc + 1 : 1;
+    const int i_ch = c_ch_adj_nb[nb][kk];
+    const int cid = m.ch[i_ch];
+    if ((nb >> 1) == 0) {
+      const int ioff1 = nch * c_ch_dix[i_ch][1];
+      const double *cf = FX(R, F_ELEC, cid);
+      FX(R, F_ELEC, nb_id)[fxi(i_nb, ioff1 + mm + 1, nc)] =
+          0.5 * (cf[fxi(i, 2 * mm + 1, nc)] + cf[fxi(i, 2 * mm + 2, nc)]);
+    } else {
+      const int ioff0 = nch * c_ch_dix[i_ch][0];
+      const double *cf = FY(R, F_ELEC, cid);
+      FY(R, F_ELEC, nb_id)[fyi(ioff0 + mm + 1, i_nb, nc)] =
+          0.5 * (cf[fyi(2 * mm + 1, i, nc)] + cf[fyi(2 * mm + 2, i, nc)]);
+    }
+  });
+}
+
+// update_solution, src/streamer_2d.f90:499-542 and src/streamer_cyl.f90:531-570
+__device__ void update_solution(const RunDev &R, double dt) {
+  const int *ids;
+  int n;
+  list_range(R, 1, R.min_lvl, R.max_lvl, ids, n);
+  const bool cyl = R.coord == 1;
+  box_loop(ids, n, [&](int id, int t) {
+    const BoxMeta &m = R.meta[id];
+    const int nc = m.nc, ncg = nc + 2;
+    if (t >= nc * nc) return;
+    const int i = t % nc + 1, j = t / nc + 1, c = i + ncg * j;
+    const double inv_dr = 1 / m.dr;
+    double *e = CC(R, I_ELEC, id), *pi = CC(R, I_PION, id);
+    const double *fxe = FX(R, F_ELEC, id), *fye = FY(R, F_ELEC, id);
+    double fld = CC(R, I_FLD, id)[c];
+    Loc loc = get_loc(R, fld);
+    double alpha = col_at(R, C_ALPHA, loc);
+    double eta = col_at(R, C_ETA, loc);
+    double fx0 = fxe[fxi(i, j, nc)], fx1 = fxe[fxi(i + 1, j, nc)];
+    double fy0 = fye[fyi(i, j, nc)], fy1 = fye[fyi(i, j + 1, nc)];
+    double src = 0.5 * norm2_2(fx0 + fx1, fy0 + fy1) * (alpha - eta);
+    double sflux;
+    if (cyl) {
+      int ioff = (m.ix0 - 1) * nc;
+      double den = i + ioff - 0.5;
+      double rf1 = (i + ioff - 1) / den, rf2 = (i + ioff) / den;
+      sflux = (fy0 - fy1 + rf1 * fx0 - rf2 * fx1) * inv_dr;
+    } else {
+      sflux = (fx0 - fx1 + fy0 - fy1) * inv_dr;
+    }
+    double ne = e[c] + (src + sflux) * dt;
+    double ni = pi[c] + src * dt;
+    if (!cyl && CC(R, I_EPS, id)[c] > 1.0) {
+      ni = ni - ne;
+      ne = 0;
+    }
+    e[c] = ne;
+    pi[c] = ni;
+  });
+}
+
+// a$D_restrict_tree for one or two variables, afivo/src/m_aX_restrict.f90:54-142
+// (cylindrical weights :95-113, radius evaluated at the child-local index).
+__device__ void restrict_tree(const RunDev &R, int iv0, int iv1) {
+  const bool cyl = R.coord == 1;
+  for (int lvl = R.max_lvl - 1; lvl >= R.min_lvl; lvl--) {
+    box_loop(list_p(R, 2, lvl), list_n(R, 2, lvl), [&](int id, int t) {
+      const BoxMeta &pm = R.meta[id];
+      const int ncp = pm.nc;
+      if (t >= ncp * ncp) return;
+      const int ic = t % ncp + 1, jc = t / ncp + 1;
+      for (int q = 0; q < 4; q++) {
+        int cid = pm.ch[q];
+        if (cid == 0) continue;
+        const BoxMeta &cm = R.meta[cid];
+        int o0, o1;
+        child_offset(cm, -1, o0, o1);
+        const int hnc = cm.nc >> 1;
+        const int i = ic - o0, j = jc - o1;
+        if (i < 1 || i > hnc || j < 1 || j > hnc) continue;
+        const int cg = cm.nc + 2, i_f = 2 * i - 1, j_f = 2 * j - 1;
+        for (int w = 0; w < 2; w++) {
+          int iv = w == 0 ? iv0 : iv1;
+          if (iv < 0) continue;
+          const double *cc = CC(R, iv, cid);
+          double a = cc[i_f + cg * j_f], b = cc[(i_f + 1) + cg * j_f];
+          double c = cc[i_f + cg * (j_f + 1)], d = cc[(i_f + 1) + cg * (j_f + 1)];
+          double v;
+          if (cyl) {
+            double dr16 = 0.0625 * pm.dr;
+            double r = pm.r0 + (i - 0.5) * pm.dr;
+            double rfac = dr16 / r;
+            v = (0.25 - rfac) * (a + c) + (0.25 + rfac) * (b + d);
+          } else {
+            v = 0.25 * (a + b + c + d);
+          }
+          CC(R, iv, id)[ic + (ncp + 2) * jc] = v;
+        }
+      }
+    });
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Multigrid, afivo/src/m_aX_mg.f90 (normal boxes: Laplacian or cylindrical
+// Laplacian; eps == 1 everywhere). i_phi = 4, i_tmp = 5 (the |E| variable,
+// src/streamer_2d.f90:37-40), i_rhs = 6.
+constexpr int MP = I_PHI, MT = I_FLD, MR = I_RHS;
+
+// box_lpl (m_aX_mg.f90:662-680) / box_clpl (:1027-1049) at interior cell c
+__device__ __forceinline__ double box_op_at(const double *phi, int i, int j, int nc, int ix0,
+                                            double dr, bool cyl) {
+  const int ncg = nc + 2, c = i + ncg * j;
+  double inv_dr_sq = 1 / (dr * dr);
+  if (cyl) {
+    int ioff = (ix0 - 1) * nc;
+    double den = i + ioff - 0.5;
+    double rf1 = (i + ioff - 1) / den, rf2 = (i + ioff) / den;
+    return (rf1 * phi[c - 1] + rf2 * phi[c + 1] + phi[c - ncg] + phi[c + ncg] - 4 * phi[c]) *
+           inv_dr_sq;
+  }
+  return inv_dr_sq * (phi[c - 1] + phi[c + 1] + phi[c - ncg] + phi[c + ncg] - 4 * phi[c]);
+}
+
+// fill_gc_phi over the boxes of one level (m_aX_mg.f90:303-316)
+__device__ __forceinline__ void fill_gc_phi(const RunDev &R, int lvl) {
+  box_loop(list_p(R, 0, lvl), list_n(R, 0, lvl),
+           [&](int id, int t) { gc_box(R, id, t, MP, GC_PHI); });
+  __syncthreads();
+}
+
+// gsrb_boxes (m_aX_mg.f90:343-366) with box_gsrb_lpl (:636-659) / _clpl (:998-1024)
+__device__ void gsrb_level(const RunDev &R, int lvl, int n_cycle) {
+  const bool cyl = R.coord == 1;
+  const int *ids = list_p(R, 0, lvl);
+  const int n = list_n(R, 0, lvl);
+  for (int it = 1; it <= 2 * n_cycle; it++) {
+    box_loop(ids, n, [&](int id, int t) {
+      const BoxMeta &m = R.meta[id];
+      const int nc = m.nc, ncg = nc + 2;
+      if (t >= nc * nc) return;
+      const int i = t % nc + 1, j = t / nc + 1;
+      if (((i + j + it) & 1) != 0) return;
+      double *phi = CC(R, MP, id);
+      const double rhs = CC(R, MR, id)[i + ncg * j];
+      const double dx2 = m.dr * m.dr;
+      const int c = i + ncg * j;
+      if (cyl) {
+        int ioff = (m.ix0 - 1) * nc;
+        double den = i + ioff - 0.5;
+        double rf1 = (i + ioff - 1) / den, rf2 = (i + ioff) / den;
+        phi[c] = 0.25 * (rf1 * phi[c - 1] + rf2 * phi[c + 1] + phi[c + ncg] + phi[c - ncg] -
+                         dx2 * rhs);
+      } else {
+        phi[c] = 0.25 * (phi[c + 1] + phi[c - 1] + phi[c + ncg] + phi[c - ncg] - dx2 * rhs);
+      }
+    });
+    __syncthreads();
+    fill_gc_phi(R, lvl);
+  }
+}
+
+// Residual of box id at fine cell (i, j): rhs - A phi (residual_box, :475-484)
+__device__ __forceinline__ double residual_at(const RunDev &R, const BoxMeta &m, int id, int i,
+                                              int j, bool cyl) {
+  const double *phi = CC(R, MP, id);
+  double a = box_op_at(phi, i, j, m.nc, m.ix0, m.dr, cyl);
+  return CC(R, MR, id)[i + (m.nc + 2) * j] - a;
+}
+
+// For each box of level lvl: residual into the parent's tmp and phi into the
+// parent's phi (box_rstr_lpl, :683-705). store_res: also keep the residual in
+// the box's own tmp (set_coarse_phi_rhs); otherwise the box's tmp is left as
+// it was (update_coarse saves and restores it).
+__device__ void residual_restrict(const RunDev &R, int lvl, bool store_res) {
+  const bool cyl = R.coord == 1;
+  box_loop(list_p(R, 0, lvl), list_n(R, 0, lvl), [&](int id, int t) {
+    const BoxMeta &m = R.meta[id];
+    const int nc = m.nc, ncg = nc + 2, hnc = nc >> 1;
+    if (store_res && t < nc * nc) {
+      int i = t % nc + 1, j = t / nc + 1;
+      CC(R, MT, id)[i + ncg * j] = residual_at(R, m, id, i, j, cyl);
+    }
+    if (t < hnc * hnc) {
+      int ii = t % hnc + 1, jj = t / hnc + 1;
+      int o0, o1;
+      child_offset(m, -1, o0, o1);
+      int i_c = o0 + ii, j_c = o1 + jj, i_f = 2 * ii - 1, j_f = 2 * jj - 1;
+      const BoxMeta &pm = R.meta[m.parent];
+      const int pc = i_c + (pm.nc + 2) * j_c;
+      double r00 = residual_at(R, m, id, i_f, j_f, cyl);
+      double r10 = residual_at(R, m, id, i_f + 1, j_f, cyl);
+      double r01 = residual_at(R, m, id, i_f, j_f + 1, cyl);
+      double r11 = residual_at(R, m, id, i_f + 1, j_f + 1, cyl);
+      CC(R, MT, m.parent)[pc] = 0.25 * (r00 + r10 + r01 + r11);
+      const double *phi = CC(R, MP, id);
+      CC(R, MP, m.parent)[pc] =
+          0.25 * (phi[i_f + ncg * j_f] + phi[(i_f + 1) + ncg * j_f] +
+                  phi[i_f + ncg * (j_f + 1)] + phi[(i_f + 1) + ncg * (j_f + 1)]);
+    }
+  });
+  __syncthreads();
+}
+
+// For parents of level lvl: rhs = A phi (interior); rhs += tmp (whole box);
+// optionally tmp = phi (whole box). update_coarse :395-409 /
+// set_coarse_phi_rhs :439-446.
+__device__ void coarse_rhs(const RunDev &R, int lvl, bool copy_phi_tmp) {
+  const bool cyl = R.coord == 1;
+  box_loop(list_p(R, 2, lvl), list_n(R, 2, lvl), [&](int id, int t) {
+    const BoxMeta &m = R.meta[id];
+    const int nc = m.nc, ncg = nc + 2;
+    const double *phi = CC(R, MP, id);
+    double *rhs = CC(R, MR, id), *tmp = CC(R, MT, id);
+    for (int c = t; c < ncg * ncg; c += GT) {
+      int i = c % ncg, j = c / ncg;
+      double r = rhs[c];
+      if (i >= 1 && i <= nc && j >= 1 && j <= nc) r = box_op_at(phi, i, j, nc, m.ix0, m.dr, cyl);
+      rhs[c] = r + tmp[c];
+      if (copy_phi_tmp) tmp[c] = phi[c];
+    }
+  });
+  __syncthreads();
+}
+
+// update_coarse, m_aX_mg.f90:370-410
+__device__ void update_coarse(const RunDev &R, int lvl) {
+  residual_restrict(R, lvl, false);
+  fill_gc_phi(R, lvl - 1);
+  coarse_rhs(R, lvl - 1, true);
+}
+
+// set_coarse_phi_rhs, m_aX_mg.f90:414-447
+__device__ void set_coarse_phi_rhs(const RunDev &R, int lvl) {
+  if (lvl == R.max_lvl) fill_gc_phi(R, lvl);
+  residual_restrict(R, lvl, true);
+  fill_gc_phi(R, lvl - 1);
+  coarse_rhs(R, lvl - 1, false);
+}
+
+// correct_children for the parents of level lvl-1 (m_aX_mg.f90:319-341) with
+// box_corr_lpl (:605-633): tmp = phi - tmp on the parents (whole box), then
+// phi += prolongation of tmp on their children (all boxes of level lvl).
+__device__ void correct_children(const RunDev &R, int lvl) {
+  box_loop(list_p(R, 2, lvl - 1), list_n(R, 2, lvl - 1), [&](int id, int t) {
+    const int ncg = R.meta[id].nc + 2;
+    const double *phi = CC(R, MP, id);
+    double *tmp = CC(R, MT, id);
+    for (int c = t; c < ncg * ncg; c += GT) tmp[c] = phi[c] - tmp[c];
+  });
+  __syncthreads();
+  box_loop(list_p(R, 0, lvl), list_n(R, 0, lvl), [&](int id, int t) {
+    const BoxMeta &m = R.meta[id];
+    const int nc = m.nc, ncg = nc + 2;
+    if (t >= nc * nc) return;
+    const int i = t % nc + 1, j = t / nc + 1;
+    int o0, o1;
+    child_offset(m, -1, o0, o1);
+    const double *pt = CC(R, MT, m.parent);
+    const int pg = R.meta[m.parent].nc + 2;
+    int j_c1 = o1 + ((j + 1) >> 1), j_c2 = j_c1 + 1 - 2 * (j & 1);
+    int i_c1 = o0 + ((i + 1) >> 1), i_c2 = i_c1 + 1 - 2 * (i & 1);
+    double *phi = CC(R, MP, id);
+    const int c = i + ncg * j;
+    phi[c] = phi[c] + 0.5 * pt[i_c1 + pg * j_c1] +
+             0.25 * (pt[i_c2 + pg * j_c1] + pt[i_c1 + pg * j_c2]);
+  });
+  __syncthreads();
+}
+
+// Whole-box copy of phi to tmp for the boxes of one level (a$D_boxes_copy_cc)
+__device__ void copy_phi_tmp(const RunDev &R, int lvl) {
+  box_loop(list_p(R, 0, lvl), list_n(R, 0, lvl), [&](int id, int t) {
+    const int ncg = R.meta[id].nc + 2;
+    const double *phi = CC(R, MP, id);
+    double *tmp = CC(R, MT, id);
+    for (int c = t; c < ncg * ncg; c += GT) tmp[c] = phi[c];
+  });
+  __syncthreads();
+}
+
+// init_phi_rhs, m_aX_mg.f90:450-473
+__device__ void init_phi_rhs(const RunDev &R) {
+  for (int lvl = R.max_lvl; lvl >= R.min_lvl + 1; lvl--) {
+    box_loop(list_p(R, 0, lvl), list_n(R, 0, lvl), [&](int id, int t) {
+      const BoxMeta &m = R.meta[id];
+      const int nc = m.nc, ncg = nc + 2, hnc = nc >> 1;
+      double *phi = CC(R, MP, id);
+      for (int c = t; c < ncg * ncg; c += GT) phi[c] = 0.0;
+      if (t < hnc * hnc) {
+        int ii = t % hnc + 1, jj = t / hnc + 1;
+        int o0, o1;
+        child_offset(m, -1, o0, o1);
+        int i_f = 2 * ii - 1, j_f = 2 * jj - 1;
+        const double *rhs = CC(R, MR, id);
+        const BoxMeta &pm = R.meta[m.parent];
+        CC(R, MR, m.parent)[(o0 + ii) + (pm.nc + 2) * (o1 + jj)] =
+            0.25 * (rhs[i_f + ncg * j_f] + rhs[(i_f + 1) + ncg * j_f] +
+                    rhs[i_f + ncg * (j_f + 1)] + rhs[(i_f + 1) + ncg * (j_f + 1)]);
+      }
+    });
+    __syncthreads();
+  }
+}
+
+// mg$D_fas_vcycle, m_aX_mg.f90:208-254 (set_residual = false)
+__device__ void fas_vcycle(const RunDev &R, int max_lvl, int n_cycle_base) {
+  const int min_lvl = R.min_lvl;
+  for (int lvl = max_lvl; lvl >= min_lvl + 1; lvl--) {
+    gsrb_level(R, lvl, 2);
+    update_coarse(R, lvl);
+  }
+  gsrb_level(R, min_lvl, n_cycle_base);
+  for (int lvl = min_lvl + 1; lvl <= max_lvl; lvl++) {
+    correct_children(R, lvl);
+    fill_gc_phi(R, lvl);
+    gsrb_level(R, lvl, 2);
+  }
+}
+
+// Residual of every box of levels min..max into tmp (vcycle set_residual)
+__device__ void residual_all(const RunDev &R, int max_lvl) {
+  const bool cyl = R.coord == 1;
+  for (int lvl = R.min_lvl; lvl <= max_lvl; lvl++)
+    box_loop(list_p(R, 0, lvl), list_n(R, 0, lvl), [&](int id, int t) {
+      const BoxMeta &m = R.meta[id];
+      const int nc = m.nc;
+      if (t >= nc * nc) return;
+      int i = t % nc + 1, j = t / nc + 1;
+      CC(R, MT, id)[i + (nc + 2) * j] = residual_at(R, m, id, i, j, cyl);
+    });
+  __syncthreads();
+}
+
+// mg$D_fas_fmg, m_aX_mg.f90:163-202
+__device__ void fas_fmg(const RunDev &R, bool set_residual, bool first_call) {
+  const int min_lvl = R.min_lvl;
+  if (first_call) {
+    init_phi_rhs(R);
+  } else {
+    for (int lvl = R.max_lvl; lvl >= min_lvl + 1; lvl--) set_coarse_phi_rhs(R, lvl);
+  }
+  for (int lvl = min_lvl; lvl <= R.max_lvl; lvl++) {
+    copy_phi_tmp(R, lvl);
+    if (lvl > min_lvl) {
+      correct_children(R, lvl);
+      fill_gc_phi(R, lvl);
+    }
+    fas_vcycle(R, lvl, R.n_cycle_base);
+    if (set_residual && lvl == R.max_lvl) residual_all(R, lvl);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Field.
+
+// space charge on leaves of levels >= 1, whole boxes (src/streamer_2d.f90:317-329)
+__device__ void set_rhs(const RunDev &R) {
+  const int *ids;
+  int n;
+  list_range(R, 1, 1, R.max_lvl, ids, n);
+  const double fac = UC_ELEM_CHARGE / UC_EPS0;
+  box_loop(ids, n, [&](int id, int t) {
+    const int ncg = R.meta[id].nc + 2;
+    const double *e = CC(R, I_ELEC, id), *pi = CC(R, I_PION, id);
+    double *rhs = CC(R, I_RHS, id);
+    for (int c = t; c < ncg * ncg; c += GT) rhs[c] = fac * (e[c] - pi[c]);
+  });
+  __syncthreads();
+}
+
+// fld_from_pot on all boxes (src/streamer_2d.f90:346-381) and the |E| ghost
+// fill a$D_gc_tree(i_fld, a$D_gc_interp, a$D_gc_neumann)
+__device__ void fld_from_pot(const RunDev &R) {
+  const int *ids;
+  int n;
+  list_range(R, 0, R.min_lvl, R.max_lvl, ids, n);
+  box_loop(ids, n, [&](int id, int t) {
+    const BoxMeta &m = R.meta[id];
+    const int nc = m.nc, ncg = nc + 2, nf = (nc + 1) * nc;
+    const double inv_dr = 1 / m.dr;
+    const double *phi = CC(R, I_PHI, id), *eps = CC(R, I_EPS, id);
+    double *fxf = FX(R, F_FLD, id), *fyf = FY(R, F_FLD, id);
+    for (int f = t; f < 2 * nf; f += GT) {
+      const bool xd = f < nf;
+      const int g = xd ? f : f - nf;
+      int i, j;
+      if (xd) { i = g % (nc + 1) + 1; j = g / (nc + 1) + 1; }
+      else { i = g % nc + 1; j = g / nc + 1; }
+      const int s = xd ? 1 : ncg;
+      const int c = i + ncg * j, pos = xd ? i : j;
+      double v;
+      if (pos == 1) {
+        v = 2 * inv_dr * (phi[c - s] - phi[c]) * eps[c - s] / (eps[c] + eps[c - s]);
+      } else if (pos == nc + 1) {
+        v = 2 * inv_dr * (phi[c - s] - phi[c]) * eps[c] / (eps[c] + eps[c - s]);
+      } else {
+        v = inv_dr * (phi[c - s] - phi[c]);
+      }
+      if (xd) fxf[fxi(i, j, nc)] = v;
+      else fyf[fyi(i, j, nc)] = v;
+    }
+  });
+  __syncthreads();
+  box_loop(ids, n, [&](int id, int t) {
+    const BoxMeta &m = R.meta[id];
+    const int nc = m.nc, ncg = nc + 2;
+    if (t >= nc * nc) return;
+    const int i = t % nc + 1, j = t / nc + 1;
+    const double *fxf = FX(R, F_FLD, id), *fyf = FY(R, F_FLD, id);
+    double sx = fxf[fxi(i, j, nc)] + fxf[fxi(i + 1, j, nc)];
+    double sy = fyf[fyi(i, j, nc)] + fyf[fyi(i, j + 1, nc)];
+    CC(R, I_FLD, id)[i + ncg * j] = sqrt(0.25 * (sx * sx) + 0.25 * (sy * sy));
+  });
+  __syncthreads();
+  gc_tree(R, I_FLD, -1, GC_INTERP);
+}
+
+// compute_fld, src/streamer_2d.f90:307-343 (one FMG cycle)
+__device__ void compute_fld(const RunDev &R, bool no_guess) {
+  set_rhs(R);
+  fas_fmg(R, false, no_guess);
+  fld_from_pot(R);
+}
+
+// Whole-array copy / average over every slot (unused slots included; their
+// contents are never read).
+__device__ void copy_var(const RunDev &R, int from, int to) {
+  const size_t n = (size_t)R.capacity * SLOT;
+  const double *a = R.cc + (size_t)from * n;
+  double *b = R.cc + (size_t)to * n;
+  for (size_t k = threadIdx.x; k < n; k += NTHR) b[k] = a[k];
+  __syncthreads();
+}
+// average_dens, src/streamer_2d.f90:492-496
+__device__ void average_dens(const RunDev &R) {
+  const size_t n = (size_t)R.capacity * SLOT;
+  for (int v = 0; v < 2; v++) {
+    double *x = R.cc + (size_t)v * n;
+    const double *o = R.cc + (size_t)(v + 2) * n;
+    for (size_t k = threadIdx.x; k < n; k += NTHR) x[k] = 0.5 * (x[k] + o[k]);
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// Reductions and refinement flags.
+
+__device__ __forceinline__ double dmax(double a, double b) { return a < b ? b : a; }
+__device__ __forceinline__ double dmin(double a, double b) { return b < a ? b : a; }
+
+// a$D_tree_max_cc / _min_cc over leaves (afivo/src/m_aX_utils.f90:559-619)
+__device__ void dt_reductions(const RunDev &R) {
+  __shared__ double red[3][NTHR / 32];
+  const int *ids;
+  int n;
+  list_range(R, 1, R.min_lvl, R.max_lvl, ids, n);
+  double mx = -1.7976931348623157e308, mn = 1.7976931348623157e308,
+         me = -1.7976931348623157e308;
+  box_loop(ids, n, [&](int id, int t) {
+    const BoxMeta &m = R.meta[id];
+    const int nc = m.nc;
+    if (t >= nc * nc) return;
+    const int c = (t % nc + 1) + (nc + 2) * (t / nc + 1);
+    double f = CC(R, I_FLD, id)[c];
+    mx = dmax(mx, f);
+    mn = dmin(mn, f);
+    me = dmax(me, CC(R, I_ELEC, id)[c]);
+  });
+  for (int o = 16; o > 0; o >>= 1) {
+    mx = dmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    mn = dmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    me = dmax(me, __shfl_xor_sync(0xffffffffu, me, o));
+  }
+  const int w = threadIdx.x / 32, l = threadIdx.x % 32;
+  if (l == 0) { red[0][w] = mx; red[1][w] = mn; red[2][w] = me; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < NTHR / 32; k++) {
+      mx = dmax(mx, red[0][k]);
+      mn = dmin(mn, red[1][k]);
+      me = dmax(me, red[2][k]);
+    }
+    mx = dmax(red[0][0], mx);
+    mn = dmin(red[1][0], mn);
+    me = dmax(red[2][0], me);
+    R.scal[0] = mx;
+    R.scal[1] = mn;
+    R.scal[2] = me;
+    if (!isfinite(mx) || !isfinite(mn) || !isfinite(me)) atomicExch(R.status, A5G_ENONFINITE);
+  }
+  __syncthreads();
+}
+
+// GM_dist_line (src/m_geom.f90:29-46), 2D, with gfortran's NORM2
+__device__ double dist_line(double x, double y, const double r0[2], const double r1[2]) {
+  double line_len2 = 0, temp = 0;
+  line_len2 += (r1[0] - r0[0]) * (r1[0] - r0[0]);
+  line_len2 += (r1[1] - r0[1]) * (r1[1] - r0[1]);
+  temp += (x - r0[0]) * (r1[0] - r0[0]);
+  temp += (y - r0[1]) * (r1[1] - r0[1]);
+  double v0, v1;
+  if (temp <= 0.0) { v0 = x - r0[0]; v1 = y - r0[1]; }
+  else if (temp >= line_len2) { v0 = x - r1[0]; v1 = y - r1[1]; }
+  else {
+    double p0 = r0[0] + temp / line_len2 * (r1[0] - r0[0]);
+    double p1 = r0[1] + temp / line_len2 * (r1[1] - r0[1]);
+    v0 = x - p0;
+    v1 = y - p1;
+  }
+  return norm2_2(v0, v1);
+}
+
+// set_ref_flags on every box of levels 1..max_lvl (src/streamer_2d.f90:177-216,
+// cyl :190-227). One warp per box (levels >= 1 have nc = 8: two cells/lane).
+__device__ void ref_flags(const RunDev &R, double time) {
+  for (int id = threadIdx.x; id < R.capacity; id += NTHR) R.flags[id] = INT_MIN + 1;
+  __syncthreads();
+  const int *ids;
+  int n;
+  list_range(R, 0, 1, R.max_lvl, ids, n);
+  const int w = threadIdx.x / 32, l = threadIdx.x % 32;
+  for (int b = w; b < n; b += NTHR / 32) {
+    const int id = ids[b];
+    const BoxMeta &m = R.meta[id];
+    const int nc = m.nc, ncg = nc + 2;
+    double mr = 0.0, mf = -1.7976931348623157e308;
+    for (int c = l; c < nc * nc; c += 32) {
+      int k = (c % nc + 1) + ncg * (c / nc + 1);
+      mr = dmax(mr, fabs(CC(R, I_RHS, id)[k]));
+      mf = dmax(mf, CC(R, I_FLD, id)[k]);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      mr = dmax(mr, __shfl_xor_sync(0xffffffffu, mr, o));
+      mf = dmax(mf, __shfl_xor_sync(0xffffffffu, mf, o));
+    }
+    if (l == 0) {
+      int flag = INT_MIN + 1;
+      double dr2 = m.dr * m.dr;
+      double crv_phi = dr2 * mr;
+      double alpha = col_at(R, C_ALPHA, get_loc(R, mf));
+      double adx = m.dr * alpha;
+      if (adx < 0.1 && m.dr < 2.0e-5) flag = -1;
+      if (adx < 0.1 && crv_phi < 4.0 && m.dr < 5.0e-5) flag = -1;
+      if (time < R.ref_init_time) {
+        double boxlen = m.nc * m.dr;
+        double cx = m.r0 + 0.5 * m.nc * m.dr, cy = m.r1 + 0.5 * m.nc * m.dr;
+        for (int s = 0; s < R.n_seeds; s++) {
+          double dist = dist_line(cx, cy, R.seed_r0[s], R.seed_r1[s]);
+          if (dist - R.seed_width[s] < boxlen && m.dr > 0.2 * R.seed_width[s]) flag = 1;
+        }
+      }
+      if (adx > 1.0 && crv_phi > R.crv_refine) flag = 1;
+      R.flags[id] = flag;
+    }
+  }
+  __syncthreads();
+}
+
+// prolong_to_new_boxes, src/streamer_2d.f90:592-617, with a$D_prolong1_to
+// (afivo/src/m_aX_prolong.f90:99-191) and set_box_eps (:250-266).
+__device__ void prolong_new(const RunDev &R) {
+  const bool cyl = R.coord == 1;
+  for (int li = 0; li < R.nlev; li++) {
+    const int *ids = R.new_lists + R.new_off[li];
+    const int n = R.new_off[li + 1] - R.new_off[li];
+    if (n == 0) continue;
+    box_loop(ids, n, [&](int id, int t) {
+      const BoxMeta &m = R.meta[id];
+      const int nc = m.nc, ncg = nc + 2, hnc = nc >> 1;
+      const BoxMeta &pm = R.meta[m.parent];
+      const int pg = pm.nc + 2;
+      if (t < hnc * hnc) {
+        int ii = t % hnc + 1, jj = t / hnc + 1;
+        int o0, o1;
+        child_offset(m, -1, o0, o1);
+        int i_c = ii + o0, j_c = jj + o1, i_f = 2 * ii - 1, j_f = 2 * jj - 1;
+        const int vars[3] = {I_ELEC, I_PION, I_PHI};
+        for (int v = 0; v < 3; v++) {
+          const double *p = CC(R, vars[v], m.parent);
+          double *b = CC(R, vars[v], id);
+          const int pc = i_c + pg * j_c;
+          double f0 = 0.5 * p[pc];
+          double flx = 0.25 * p[pc - 1], fhx = 0.25 * p[pc + 1];
+          double fly = 0.25 * p[pc - pg], fhy = 0.25 * p[pc + pg];
+          b[i_f + ncg * j_f] = f0 + flx + fly + 0.0;
+          b[(i_f + 1) + ncg * j_f] = f0 + fhx + fly + 0.0;
+          b[i_f + ncg * (j_f + 1)] = f0 + flx + fhy + 0.0;
+          b[(i_f + 1) + ncg * (j_f + 1)] = f0 + fhx + fhy + 0.0;
+        }
+      }
+      double *eps = CC(R, I_EPS, id);
+      for (int c = t; c < ncg * ncg; c += GT) {
+        int i = c % ncg, j = c / ncg;
+        double x = m.r0 + (i - 0.5) * m.dr, y = m.r1 + (j - 0.5) * m.dr;
+        double rel = (cyl ? x : y) / R.domain_len_z;
+        eps[c] = rel < 0.25 ? R.epsilon_diel : 1.0;
+      }
+    });
+    __syncthreads();
+    box_loop(ids, n, [&](int id, int t) {
+      gc_box(R, id, t, I_ELEC, GC_LIM);
+      gc_box(R, id, t, I_PION, GC_LIM);
+      gc_box(R, id, t, I_PHI, GC_PHI);
+    });
+    __syncthreads();
+  }
+}
+
+// One full time step, src/streamer_2d.f90:99-127
+__device__ void step(const RunDev &R, double dt) {
+  copy_var(R, I_ELEC, I_ELEC_OLD);
+  copy_var(R, I_PION, I_PION_OLD);
+  for (int stage = 1; stage <= 2; stage++) {
+    fluxes_koren(R, dt);
+    __syncthreads();
+    consistent_fluxes(R);
+    __syncthreads();
+    update_solution(R, dt);
+    __syncthreads();
+    restrict_tree(R, I_ELEC, I_PION);
+    gc_tree(R, I_ELEC, I_PION, GC_LIM);
+    if (stage == 1) compute_fld(R, false);
+  }
+  average_dens(R);
+  compute_fld(R, false);
+}
+
+__device__ void run_op(const RunDev &R, const Op &op) {
+  switch (op.code) {
+    case OP_COPY: copy_var(R, op.i0, op.i1); break;
+    case OP_FLUXES: fluxes_koren(R, op.d0); __syncthreads(); break;
+    case OP_CONSISTENT: consistent_fluxes(R); __syncthreads(); break;
+    case OP_UPDATE: update_solution(R, op.d0); __syncthreads(); break;
+    case OP_RESTRICT: restrict_tree(R, op.i0, -1); break;
+    case OP_GC: gc_tree(R, op.i0, -1, op.i1); break;
+    case OP_AVERAGE: average_dens(R); break;
+    case OP_COMPUTE_FLD: compute_fld(R, op.i0 != 0); break;
+    case OP_FMG: fas_fmg(R, op.i0 != 0, op.i1 != 0); break;
+    case OP_FLD_FROM_POT: fld_from_pot(R); break;
+    case OP_DT_RED: dt_reductions(R); break;
+    case OP_REF_FLAGS: ref_flags(R, op.d0); break;
+    case OP_PROLONG_NEW: prolong_new(R); break;
+    case OP_STEP: step(R, op.d0); break;
+    case OP_SET_RHS: set_rhs(R); break;
+    default: if (threadIdx.x == 0) atomicExch(R.status, A5G_EINVAL);
+  }
+}
+
+// One block per run. The run descriptor is staged in shared memory.
+__global__ void __launch_bounds__(NTHR, 1)
+a5g_run_kernel(const RunDev *single, Op single_op, const RunDev *const *runs, const Op *ops) {
+  __shared__ RunDev sR;
+  const RunDev *src = runs ? runs[blockIdx.x] : single;
+  {
+    const int *s = reinterpret_cast<const int *>(src);
+    int *d = reinterpret_cast<int *>(&sR);
+    for (int k = threadIdx.x; k < (int)(sizeof(RunDev) / sizeof(int)); k += NTHR) d[k] = s[k];
+  }
+  __syncthreads();
+  Op op = runs ? ops[blockIdx.x] : single_op;
+  run_op(sR, op);
+}
+
+}  // namespace
+
+// ===========================================================================
+// Host side: contexts and the C ABI.
+
+static thread_local std::string g_err;
+
+static int fail(int code, const std::string &msg) {
+  g_err = msg;
+  return code;
+}
+#define CK(call)                                                                    \
+  do {                                                                              \
+    cudaError_t e_ = (call);                                                        \
+    if (e_ != cudaSuccess)                                                          \
+      return fail(e_ == cudaErrorMemoryAllocation ? A5G_ENOMEM : A5G_ECUDA,         \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));              \
+  } while (0)
+
+struct a5g_ctx {
+  a5g_params p{};
+  cudaStream_t stream = nullptr;
+  RunDev h{};
+  RunDev *d_run = nullptr;
+  int capacity = 0;
+  int max_id = 0;
+  bool has_tree = false, has_table = false;
+  double *cc = nullptr, *fx = nullptr, *fy = nullptr;
+  BoxMeta *meta = nullptr;
+  int *lists = nullptr;
+  size_t lists_cap = 0;
+  int *new_lists = nullptr;
+  size_t new_cap = 0;
+  double *tbl = nullptr;
+  double *scal = nullptr;
+  int *flags = nullptr;
+  int *status = nullptr;
+  std::vector<double> h_tbl;
+  int tbl_rows = 0, tbl_cols = 0;
+  double tbl_xmin = 0, tbl_inv_dx = 0;
+  long long n_leaf_cells = 0;
+  int min_lvl = 0, max_lvl = 0;
+};
+
+static int push_run(a5g_ctx *c) {
+  CK(cudaMemcpyAsync(c->d_run, &c->h, sizeof(RunDev), cudaMemcpyHostToDevice, c->stream));
+  return A5G_OK;
+}
+
+static int check_status(a5g_ctx *c) {
+  int st = 0;
+  CK(cudaMemcpyAsync(&st, c->status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (st != 0) {
+    int z = 0;
+    CK(cudaMemcpy(c->status, &z, sizeof(int), cudaMemcpyHostToDevice));
+    return fail(st, "device reported status " + std::to_string(st));
+  }
+  return A5G_OK;
+}
+
+static int launch(a5g_ctx *c, const Op &op) {
+  if (!c) return fail(A5G_EINVAL, "null context");
+  if (!c->has_tree) return fail(A5G_ESTATE, "no tree uploaded");
+  if (!c->has_table) return fail(A5G_ESTATE, "no transport table set");
+  a5g_run_kernel<<<1, NTHR, 0, c->stream>>>(c->d_run, op, nullptr, nullptr);
+  CK(cudaGetLastError());
+  return A5G_OK;
+}
+
+extern "C" {
+
+const char *a5g_last_error(void) { return g_err.c_str(); }
+int a5g_version(void) { return 1; }
+
+int a5g_create(const a5g_params *p, a5g_ctx **out) {
+  if (!p || !out) return fail(A5G_EINVAL, "null argument");
+  *out = nullptr;
+  if (p->box_size != NC) return fail(A5G_EINVAL, "box_size must be 8");
+  if (p->coord != 0 && p->coord != 1) return fail(A5G_EINVAL, "coord must be 0 or 1");
+  if (p->epsilon_diel != 1.0)
+    return fail(A5G_EINVAL, "epsilon_diel != 1 needs the dielectric operators (not built)");
+  if (p->n_seeds < 0 || p->n_seeds > 8) return fail(A5G_EINVAL, "n_seeds must be 0..8");
+  if (p->lvls_max < 1 || p->lvls_max > 30) return fail(A5G_EINVAL, "lvls_max must be 1..30");
+  if (!(p->dr_base > 0)) return fail(A5G_EINVAL, "dr_base must be > 0");
+  a5g_ctx *c = new a5g_ctx();
+  c->p = *p;
+  cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete c;
+    return fail(A5G_ECUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+  }
+  if (cudaMalloc(&c->d_run, sizeof(RunDev)) != cudaSuccess ||
+      cudaMalloc(&c->scal, 16 * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&c->status, sizeof(int)) != cudaSuccess) {
+    a5g_destroy(c);
+    return fail(A5G_ENOMEM, "cudaMalloc failed");
+  }
+  cudaMemset(c->status, 0, sizeof(int));
+  RunDev &h = c->h;
+  std::memset(&h, 0, sizeof(RunDev));
+  h.coord = p->coord;
+  h.n_cycle_base = p->n_cycle_base;
+  h.lvls_max = p->lvls_max;
+  h.applied_voltage = -p->domain_len_z * p->applied_fld;
+  h.domain_len_z = p->domain_len_z;
+  h.epsilon_diel = p->epsilon_diel;
+  h.ref_init_time = p->ref_init_time;
+  h.crv_refine = p->crv_refine;
+  h.n_seeds = p->n_seeds;
+  for (int s = 0; s < p->n_seeds; s++) {
+    for (int d = 0; d < 2; d++) {
+      h.seed_r0[s][d] = p->seed_r0[s][d];
+      h.seed_r1[s][d] = p->seed_r1[s][d];
+    }
+    h.seed_width[s] = p->seed_width[s];
+  }
+  h.scal = c->scal;
+  h.status = c->status;
+  *out = c;
+  return A5G_OK;
+}
+
+int a5g_destroy(a5g_ctx *c) {
+  if (!c) return A5G_OK;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  cudaFree(c->d_run);
+  cudaFree(c->cc);
+  cudaFree(c->fx);
+  cudaFree(c->fy);
+  cudaFree(c->meta);
+  cudaFree(c->lists);
+  cudaFree(c->new_lists);
+  cudaFree(c->tbl);
+  cudaFree(c->scal);
+  cudaFree(c->flags);
+  cudaFree(c->status);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return A5G_OK;
+}
+
+int a5g_set_table(a5g_ctx *c, int n_rows, int n_cols, double x_min, double inv_dx,
+                  const double *rows_cols) {
+  if (!c || !rows_cols) return fail(A5G_EINVAL, "null argument");
+  if (n_rows < 2 || n_cols != 4) return fail(A5G_EINVAL, "table needs >= 2 rows and 4 columns");
+  if (!(inv_dx > 0) || !std::isfinite(x_min)) return fail(A5G_EINVAL, "bad table grid");
+  cudaFree(c->tbl);
+  c->tbl = nullptr;
+  CK(cudaMalloc(&c->tbl, sizeof(double) * n_rows * n_cols));
+  CK(cudaMemcpyAsync(c->tbl, rows_cols, sizeof(double) * n_rows * n_cols,
+                     cudaMemcpyHostToDevice, c->stream));
+  c->h_tbl.assign(rows_cols, rows_cols + (size_t)n_rows * n_cols);
+  c->tbl_rows = n_rows;
+  c->tbl_cols = n_cols;
+  c->tbl_xmin = x_min;
+  c->tbl_inv_dx = inv_dx;
+  c->h.tbl = c->tbl;
+  c->h.tbl_rows = n_rows;
+  c->h.tbl_xmin = x_min;
+  c->h.tbl_inv_dx = inv_dx;
+  c->has_table = true;
+  return push_run(c);
+}
+
+static int grow(a5g_ctx *c, int need) {
+  if (need <= c->capacity) return A5G_OK;
+  int cap = std::max(need, c->capacity + c->capacity / 2);
+  cap = std::max(cap, 64);
+  double *ncc = nullptr, *nfx = nullptr, *nfy = nullptr;
+  BoxMeta *nmeta = nullptr;
+  int *nflags = nullptr;
+  size_t scc = (size_t)cap * SLOT * A5G_N_VAR_CELL, sfc = (size_t)cap * FSLOT * A5G_N_VAR_FACE;
+  if (cudaMalloc(&ncc, scc * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&nfx, sfc * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&nfy, sfc * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&nmeta, (size_t)cap * sizeof(BoxMeta)) != cudaSuccess ||
+      cudaMalloc(&nflags, (size_t)cap * sizeof(int)) != cudaSuccess) {
+    cudaFree(ncc); cudaFree(nfx); cudaFree(nfy); cudaFree(nmeta); cudaFree(nflags);
+    return fail(A5G_ENOMEM, "cannot grow box storage to " + std::to_string(cap) + " boxes");
+  }
+  CK(cudaMemsetAsync(ncc, 0, scc * sizeof(double), c->stream));
+  CK(cudaMemsetAsync(nfx, 0, sfc * sizeof(double), c->stream));
+  CK(cudaMemsetAsync(nfy, 0, sfc * sizeof(double), c->stream));
+  CK(cudaMemsetAsync(nmeta, 0, (size_t)cap * sizeof(BoxMeta), c->stream));
+  if (c->capacity > 0) {
+    for (int v = 0; v < A5G_N_VAR_CELL; v++)
+      CK(cudaMemcpyAsync(ncc + (size_t)v * cap * SLOT, c->cc + (size_t)v * c->capacity * SLOT,
+                         (size_t)c->capacity * SLOT * sizeof(double), cudaMemcpyDeviceToDevice,
+                         c->stream));
+    for (int f = 0; f < A5G_N_VAR_FACE; f++) {
+      CK(cudaMemcpyAsync(nfx + (size_t)f * cap * FSLOT, c->fx + (size_t)f * c->capacity * FSLOT,
+                         (size_t)c->capacity * FSLOT * sizeof(double), cudaMemcpyDeviceToDevice,
+                         c->stream));
+      CK(cudaMemcpyAsync(nfy + (size_t)f * cap * FSLOT, c->fy + (size_t)f * c->capacity * FSLOT,
+                         (size_t)c->capacity * FSLOT * sizeof(double), cudaMemcpyDeviceToDevice,
+                         c->stream));
+    }
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  cudaFree(c->cc); cudaFree(c->fx); cudaFree(c->fy); cudaFree(c->meta); cudaFree(c->flags);
+  c->cc = ncc; c->fx = nfx; c->fy = nfy; c->meta = nmeta; c->flags = nflags;
+  c->capacity = cap;
+  c->h.capacity = cap;
+  c->h.cc = ncc; c->h.fx = nfx; c->h.fy = nfy; c->h.meta = nmeta; c->h.flags = nflags;
+  return A5G_OK;
+}
+
+int a5g_upload_tree(a5g_ctx *c, int max_id, int min_lvl, int max_lvl, const int *meta16,
+                    const double *geom4, const int *lvl_counts, const int *lvl_ids) {
+  if (!c || !meta16 || !geom4 || !lvl_counts || !lvl_ids) return fail(A5G_EINVAL, "null argument");
+  if (max_id < 1) return fail(A5G_EINVAL, "max_id must be >= 1");
+  int nlev = max_lvl - min_lvl + 1;
+  if (nlev < 1 || nlev + 1 > MAXLEV) return fail(A5G_EINVAL, "bad level range");
+  if (max_lvl > c->p.lvls_max) return fail(A5G_EINVAL, "max_lvl above lvls_max");
+  // validate topology
+  std::vector<BoxMeta> hm(max_id + 1);
+  std::memset(hm.data(), 0, hm.size() * sizeof(BoxMeta));
+  for (int id = 1; id <= max_id; id++) {
+    const int *m = meta16 + 16 * id;
+    if (!m[0]) continue;
+    BoxMeta &b = hm[id];
+    b.lvl = m[1];
+    b.ix0 = m[2];
+    b.ix1 = m[3];
+    b.parent = m[5];
+    for (int k = 0; k < 4; k++) b.ch[k] = m[6 + k];
+    for (int k = 0; k < 4; k++) b.nb[k] = m[10 + k];
+    b.nc = m[14];
+    b.dr = geom4[4 * id + 3];
+    b.r0 = geom4[4 * id + 0];
+    b.r1 = geom4[4 * id + 1];
+    int expect = b.lvl >= 1 ? NC : (NC >> (1 - b.lvl));
+    if (b.nc != expect || b.nc < 2) return fail(A5G_EINVAL, "box " + std::to_string(id) + ": bad n_cell");
+    if (b.parent < 0 || b.parent > max_id) return fail(A5G_EINVAL, "bad parent id");
+    for (int k = 0; k < 4; k++)
+      if (b.ch[k] < 0 || b.ch[k] > max_id || b.nb[k] > max_id)
+        return fail(A5G_EINVAL, "bad child/neighbour id at box " + std::to_string(id));
+    if (!(b.dr > 0)) return fail(A5G_EINVAL, "bad dr");
+  }
+  std::vector<int> lists;
+  int off[3][MAXLEV + 1];
+  {
+    // regroup per-level (ids, leaves, parents) into three contiguous blocks
+    std::vector<std::vector<int>> by(3);
+    size_t k = 0;
+    std::vector<int> starts[3];
+    for (int li = 0; li < nlev; li++) {
+      for (int kind = 0; kind < 3; kind++) {
+        int n = lvl_counts[3 * li + kind];
+        if (n < 0) return fail(A5G_EINVAL, "negative level count");
+        off[kind][li] = (int)by[kind].size();
+        for (int q = 0; q < n; q++) {
+          int id = lvl_ids[k++];
+          if (id < 1 || id > max_id || !meta16[16 * id])
+            return fail(A5G_EINVAL, "level list names an unused id");
+          if (hm[id].lvl != min_lvl + li) return fail(A5G_EINVAL, "level list / box level mismatch");
+          by[kind].push_back(id);
+        }
+      }
+    }
+    for (int kind = 0; kind < 3; kind++) off[kind][nlev] = (int)by[kind].size();
+    int base[3] = {0, (int)by[0].size(), (int)(by[0].size() + by[1].size())};
+    for (int kind = 0; kind < 3; kind++) {
+      for (int li = 0; li <= nlev; li++) off[kind][li] += base[kind];
+      lists.insert(lists.end(), by[kind].begin(), by[kind].end());
+    }
+  }
+  // every referenced box must exist and be in use
+  for (int id = 1; id <= max_id; id++) {
+    if (!meta16[16 * id]) continue;
+    const BoxMeta &b = hm[id];
+    if (b.parent > 0 && !meta16[16 * b.parent]) return fail(A5G_EINVAL, "parent not in use");
+    for (int k = 0; k < 4; k++) {
+      if (b.ch[k] > 0 && !meta16[16 * b.ch[k]]) return fail(A5G_EINVAL, "child not in use");
+      if (b.nb[k] > 0 && !meta16[16 * b.nb[k]]) return fail(A5G_EINVAL, "neighbour not in use");
+    }
+    if (b.lvl > min_lvl && b.parent <= 0) return fail(A5G_EINVAL, "box without parent");
+  }
+  int r = grow(c, max_id + 1);
+  if (r) return r;
+  CK(cudaMemcpyAsync(c->meta, hm.data(), hm.size() * sizeof(BoxMeta), cudaMemcpyHostToDevice,
+                     c->stream));
+  if (lists.size() + 1 > c->lists_cap) {
+    cudaFree(c->lists);
+    c->lists = nullptr;
+    c->lists_cap = std::max(lists.size() + 1, 2 * c->lists_cap);
+    CK(cudaMalloc(&c->lists, c->lists_cap * sizeof(int)));
+  }
+  if (!lists.empty())
+    CK(cudaMemcpyAsync(c->lists, lists.data(), lists.size() * sizeof(int), cudaMemcpyHostToDevice,
+                       c->stream));
+  RunDev &h = c->h;
+  h.min_lvl = min_lvl;
+  h.max_lvl = max_lvl;
+  h.nlev = nlev;
+  for (int kind = 0; kind < 3; kind++)
+    for (int li = 0; li <= nlev; li++) h.lv_off[kind][li] = off[kind][li];
+  h.lists = c->lists;
+  c->max_id = max_id;
+  c->min_lvl = min_lvl;
+  c->max_lvl = max_lvl;
+  long long nl = 0;
+  for (int li = 0; li < nlev; li++)
+    for (int q = off[1][li]; q < off[1][li + 1]; q++) nl += (long long)hm[lists[q]].nc * hm[lists[q]].nc;
+  c->n_leaf_cells = nl;
+  c->has_tree = true;
+  CK(cudaStreamSynchronize(c->stream));
+  return push_run(c);
+}
+
+int a5g_upload_cc(a5g_ctx *c, int iv, const double *host) {
+  if (!c || !host) return fail(A5G_EINVAL, "null argument");
+  if (!c->has_tree) return fail(A5G_ESTATE, "no tree uploaded");
+  if (iv < 0 || iv >= A5G_N_VAR_CELL) return fail(A5G_EINVAL, "bad variable index");
+  CK(cudaMemcpyAsync(c->cc + (size_t)iv * c->capacity * SLOT, host,
+                     (size_t)(c->max_id + 1) * SLOT * sizeof(double), cudaMemcpyHostToDevice,
+                     c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return A5G_OK;
+}
+
+int a5g_download_cc(a5g_ctx *c, int iv, double *host) {
+  if (!c || !host) return fail(A5G_EINVAL, "null argument");
+  if (!c->has_tree) return fail(A5G_ESTATE, "no tree uploaded");
+  if (iv < 0 || iv >= A5G_N_VAR_CELL) return fail(A5G_EINVAL, "bad variable index");
+  CK(cudaMemcpyAsync(host, c->cc + (size_t)iv * c->capacity * SLOT,
+                     (size_t)(c->max_id + 1) * SLOT * sizeof(double), cudaMemcpyDeviceToHost,
+                     c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return check_status(c);
+}
+
+int a5g_upload_fc(a5g_ctx *c, int dimf, int f, const double *host) {
+  if (!c || !host) return fail(A5G_EINVAL, "null argument");
+  if (!c->has_tree) return fail(A5G_ESTATE, "no tree uploaded");
+  if (dimf < 0 || dimf > 1 || f < 0 || f >= A5G_N_VAR_FACE) return fail(A5G_EINVAL, "bad face index");
+  double *base = dimf == 0 ? c->fx : c->fy;
+  CK(cudaMemcpyAsync(base + (size_t)f * c->capacity * FSLOT, host,
+                     (size_t)(c->max_id + 1) * FSLOT * sizeof(double), cudaMemcpyHostToDevice,
+                     c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return A5G_OK;
+}
+
+int a5g_download_fc(a5g_ctx *c, int dimf, int f, double *host) {
+  if (!c || !host) return fail(A5G_EINVAL, "null argument");
+  if (!c->has_tree) return fail(A5G_ESTATE, "no tree uploaded");
+  if (dimf < 0 || dimf > 1 || f < 0 || f >= A5G_N_VAR_FACE) return fail(A5G_EINVAL, "bad face index");
+  double *base = dimf == 0 ? c->fx : c->fy;
+  CK(cudaMemcpyAsync(host, base + (size_t)f * c->capacity * FSLOT,
+                     (size_t)(c->max_id + 1) * FSLOT * sizeof(double), cudaMemcpyDeviceToHost,
+                     c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return check_status(c);
+}
+
+static Op mkop(int code, int i0 = 0, int i1 = 0, double d0 = 0) {
+  Op o{};
+  o.code = code;
+  o.i0 = i0;
+  o.i1 = i1;
+  o.d0 = d0;
+  return o;
+}
+
+int a5g_tree_copy_cc(a5g_ctx *c, int a, int b) {
+  if (a < 0 || a >= A5G_N_VAR_CELL || b < 0 || b >= A5G_N_VAR_CELL)
+    return fail(A5G_EINVAL, "bad variable index");
+  return launch(c, mkop(OP_COPY, a, b));
+}
+int a5g_fluxes_koren(a5g_ctx *c, double dt) {
+  if (!(dt > 0)) return fail(A5G_EINVAL, "dt must be > 0");
+  return launch(c, mkop(OP_FLUXES, 0, 0, dt));
+}
+int a5g_consistent_fluxes(a5g_ctx *c) { return launch(c, mkop(OP_CONSISTENT)); }
+int a5g_update_solution(a5g_ctx *c, double dt) { return launch(c, mkop(OP_UPDATE, 0, 0, dt)); }
+int a5g_restrict_tree(a5g_ctx *c, int iv) {
+  if (iv < 0 || iv >= A5G_N_VAR_CELL) return fail(A5G_EINVAL, "bad variable index");
+  return launch(c, mkop(OP_RESTRICT, iv));
+}
+int a5g_gc_tree(a5g_ctx *c, int iv, int rb_kind) {
+  if (iv < 0 || iv >= A5G_N_VAR_CELL) return fail(A5G_EINVAL, "bad variable index");
+  if (rb_kind != 0 && rb_kind != 1) return fail(A5G_EINVAL, "rb_kind must be 0 or 1");
+  return launch(c, mkop(OP_GC, iv, rb_kind == 0 ? GC_LIM : GC_INTERP));
+}
+int a5g_average_dens(a5g_ctx *c) { return launch(c, mkop(OP_AVERAGE)); }
+int a5g_compute_fld(a5g_ctx *c, int no_guess) { return launch(c, mkop(OP_COMPUTE_FLD, no_guess ? 1 : 0)); }
+int a5g_fas_fmg(a5g_ctx *c, int set_residual, int first_call) {
+  return launch(c, mkop(OP_FMG, set_residual ? 1 : 0, first_call ? 1 : 0));
+}
+int a5g_fld_from_pot(a5g_ctx *c) { return launch(c, mkop(OP_FLD_FROM_POT)); }
+
+int a5g_dt_reductions(a5g_ctx *c, double *out3) {
+  if (!out3) return fail(A5G_EINVAL, "null argument");
+  int r = launch(c, mkop(OP_DT_RED));
+  if (r) return r;
+  CK(cudaMemcpyAsync(out3, c->scal, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  return check_status(c);
+}
+
+static double lt_col(const a5g_ctx *c, int col, double x) {
+  double frac = (x - c->tbl_xmin) * c->tbl_inv_dx;
+  int ix;
+  double fr;
+  if (frac < 2.0e9 && frac > -2.0e9) {
+    ix = (int)std::ceil(frac);
+    fr = ix - frac;
+  } else {
+    ix = frac > 0 ? c->tbl_rows : 0;
+    fr = 0;
+  }
+  if (ix < 1) { ix = 1; fr = 1; }
+  else if (ix >= c->tbl_rows) { ix = c->tbl_rows - 1; fr = 0; }
+  const double *T = c->h_tbl.data() + (size_t)c->tbl_rows * col;
+  return fr * T[ix - 1] + (1 - fr) * T[ix];
+}
+
+int a5g_get_max_dt(a5g_ctx *c, double *dt) {
+  if (!dt) return fail(A5G_EINVAL, "null argument");
+  double r3[3];
+  int r = a5g_dt_reductions(c, r3);
+  if (r) return r;
+  // get_max_dt, src/streamer_2d.f90:284-302 (cyl :294-313)
+  const double max_fld = r3[0], min_fld = r3[1], max_dns = r3[2];
+  const double eps_mach = 2.220446049250313e-16;
+  double dr_min = c->p.dr_base * std::pow(0.5, c->max_lvl - 1);
+  double mobility = lt_col(c, 0, max_fld);
+  double max_mobility = lt_col(c, 0, min_fld);
+  double diff_coeff = lt_col(c, 1, max_fld);
+  double alpha = lt_col(c, 2, max_fld);
+  double dt_cfl = dr_min / (mobility * max_fld);
+  double dt_dif = 0.25 * (dr_min * dr_min) / diff_coeff;
+  double dns = c->p.coord == 1 ? std::max(eps_mach, max_dns) : max_dns;
+  double dt_drt = UC_EPS0 / (UC_ELEM_CHARGE * max_mobility * dns);
+  double dt_alpha = 1 / std::max(mobility * max_fld * alpha, eps_mach);
+  double m = std::min(std::min(1 / (1 / dt_cfl + 1 / dt_dif), dt_alpha), c->p.dt_max);
+  if (c->p.use_drt) m = std::min(m, dt_drt);
+  *dt = 0.5 * m;
+  return A5G_OK;
+}
+
+int a5g_ref_flags(a5g_ctx *c, double time, int *flags) {
+  if (!flags) return fail(A5G_EINVAL, "null argument");
+  int r = launch(c, mkop(OP_REF_FLAGS, 0, 0, time));
+  if (r) return r;
+  CK(cudaMemcpyAsync(flags, c->flags, (size_t)(c->max_id + 1) * sizeof(int),
+                     cudaMemcpyDeviceToHost, c->stream));
+  return check_status(c);
+}
+
+int a5g_prolong_new(a5g_ctx *c, const int *n_new, const int *new_ids) {
+  if (!c || !n_new || !new_ids) return fail(A5G_EINVAL, "null argument");
+  if (!c->has_tree) return fail(A5G_ESTATE, "no tree uploaded");
+  int nlev = c->h.nlev;
+  size_t tot = 0;
+  for (int li = 0; li < nlev; li++) {
+    if (n_new[li] < 0) return fail(A5G_EINVAL, "negative count");
+    tot += n_new[li];
+  }
+  for (size_t k = 0; k < tot; k++)
+    if (new_ids[k] < 1 || new_ids[k] > c->max_id) return fail(A5G_EINVAL, "bad new id");
+  if (tot + 1 > c->new_cap) {
+    cudaFree(c->new_lists);
+    c->new_lists = nullptr;
+    c->new_cap = std::max(tot + 1, 2 * c->new_cap);
+    CK(cudaMalloc(&c->new_lists, c->new_cap * sizeof(int)));
+  }
+  if (tot) CK(cudaMemcpyAsync(c->new_lists, new_ids, tot * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  int acc = 0;
+  for (int li = 0; li < nlev; li++) {
+    c->h.new_off[li] = acc;
+    acc += n_new[li];
+  }
+  c->h.new_off[nlev] = acc;
+  c->h.new_lists = c->new_lists;
+  int r = push_run(c);
+  if (r) return r;
+  r = launch(c, mkop(OP_PROLONG_NEW));
+  if (r) return r;
+  CK(cudaStreamSynchronize(c->stream));
+  return A5G_OK;
+}
+
+int a5g_step(a5g_ctx *c, double dt) {
+  if (!(dt > 0)) return fail(A5G_EINVAL, "dt must be > 0");
+  return launch(c, mkop(OP_STEP, 0, 0, dt));
+}
+
+int a5g_step_batch(a5g_ctx **ctxs, int n, const double *dts) {
+  if (!ctxs || !dts || n < 1) return fail(A5G_EINVAL, "bad batch");
+  for (int k = 0; k < n; k++) {
+    if (!ctxs[k] || !ctxs[k]->has_tree || !ctxs[k]->has_table)
+      return fail(A5G_ESTATE, "batch member without tree or table");
+    if (!(dts[k] > 0)) return fail(A5G_EINVAL, "dt must be > 0");
+  }
+  a5g_ctx *c0 = ctxs[0];
+  std::vector<const RunDev *> rp(n);
+  std::vector<Op> ops(n);
+  for (int k = 0; k < n; k++) {
+    rp[k] = ctxs[k]->d_run;
+    ops[k] = mkop(OP_STEP, 0, 0, dts[k]);
+  }
+  // other members' queued work must finish before the batch runs on c0's stream
+  for (int k = 1; k < n; k++) CK(cudaStreamSynchronize(ctxs[k]->stream));
+  const RunDev **d_rp = nullptr;
+  Op *d_ops = nullptr;
+  CK(cudaMallocAsync((void **)&d_rp, n * sizeof(void *), c0->stream));
+  CK(cudaMallocAsync((void **)&d_ops, n * sizeof(Op), c0->stream));
+  CK(cudaMemcpyAsync(d_rp, rp.data(), n * sizeof(void *), cudaMemcpyHostToDevice, c0->stream));
+  CK(cudaMemcpyAsync(d_ops, ops.data(), n * sizeof(Op), cudaMemcpyHostToDevice, c0->stream));
+  a5g_run_kernel<<<n, NTHR, 0, c0->stream>>>(nullptr, Op{}, d_rp, d_ops);
+  CK(cudaGetLastError());
+  CK(cudaFreeAsync(d_rp, c0->stream));
+  CK(cudaFreeAsync(d_ops, c0->stream));
+  return A5G_OK;
+}
+
+int a5g_sync(a5g_ctx *c) {
+  if (!c) return fail(A5G_EINVAL, "null context");
+  CK(cudaStreamSynchronize(c->stream));
+  return check_status(c);
+}
+
+int a5g_n_leaf_cells(a5g_ctx *c, long long *n) {
+  if (!c || !n) return fail(A5G_EINVAL, "null argument");
+  *n = c->n_leaf_cells;
+  return A5G_OK;
+}
+
+}  // extern "C"

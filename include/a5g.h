@@ -1,0 +1,161 @@
+/*
+ * a5g — B200-native (sm_100a) device path for a5_streamer's per-timestep work.
+ *
+ * C ABI: plain pointers and sizes, no C++ or torch types. One context holds
+ * one run (a quadtree of boxes and their cell/face data) resident in device
+ * memory. Every call returns an a5g_status; a5g_last_error() gives the text.
+ *
+ * The reference drives this path from Fortran through Afivo's procedure-
+ * pointer "plugin" API (afivo/src/m_aX_t.f90:207-268 for the box-loop and
+ * ghost-cell callback interfaces, afivo/src/m_aX_mg.f90:20-85 for the
+ * multigrid operator table). Device code cannot call host procedure
+ * pointers, so each callback the streamer drivers plug in becomes a named
+ * entry point below; boundary-condition callbacks become enums.
+ *
+ * Data conventions (same as the reference):
+ *  - box ids are 1-based (0 = no box, negative = physical boundary) and index
+ *    device slots directly; slot 0 is unused;
+ *  - cell variable iv of box id is a slot of (box_size+2)^2 doubles holding
+ *    that box's (nc+2)^2 values i-fastest (nc = box_size on levels >= 1,
+ *    smaller on the coarse subtree levels <= 0);
+ *  - face variables: fx(1:nc+1,1:nc) and fy(1:nc,1:nc+1) in slots of
+ *    (box_size+1)*box_size doubles;
+ *  - cell variables: 0 n_e, 1 n_i, 2 n_e old, 3 n_i old, 4 phi, 5 |E|,
+ *    6 rhs, 7 photoionization, 8 eps (src/m_streamer.f90:17-27);
+ *    face variables: 0 electron flux, 1 field (src/m_streamer.f90:31-33).
+ */
+#ifndef A5G_H
+#define A5G_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum a5g_status {
+  A5G_OK = 0,
+  A5G_EINVAL = 1,      /* bad argument or unsupported configuration */
+  A5G_ENOMEM = 2,      /* device allocation failed */
+  A5G_ECUDA = 3,       /* CUDA runtime error */
+  A5G_TIMEOUT = 4,     /* a bounded device wait gave up */
+  A5G_ENONFINITE = 5,  /* a NaN/Inf was detected where a finite value is required */
+  A5G_ESTATE = 6       /* call out of order (no tree, no table, ...) */
+} a5g_status;
+
+#define A5G_N_VAR_CELL 9
+#define A5G_N_VAR_FACE 2
+
+/* Parameters of one run. Mirrors the reference's configuration variables
+ * that the device path reads (src/m_streamer.f90:145-228, 386-417). */
+typedef struct a5g_params {
+  int box_size;          /* cells per box edge; 8 is supported */
+  int coord;             /* 0 Cartesian (x,y), 1 cylindrical (r,z) */
+  int lvls_max;          /* finest allowed level */
+  double dr_base;        /* cell size at level 1 (a$D_lvl_dr) */
+  double domain_len_z;   /* domain length along the last axis (m) */
+  double applied_fld;    /* background field (V/m); phi(top) = -len_z * fld */
+  double epsilon_diel;   /* must be 1: the dielectric operators are not built */
+  double dt_max;         /* ST_dt_max */
+  int use_drt;           /* 1: dielectric-relaxation limit enters the dt minimum */
+  int n_cycle_base;      /* base-level Gauss-Seidel cycles (8 Cartesian, 4 cyl) */
+  double ref_init_time;  /* refine around the seeds while t < this */
+  double crv_refine;     /* refine if dx*alpha > 1 and crv_phi > this */
+  int n_seeds;           /* seed lines for the refinement criterion (<= 8) */
+  double seed_r0[8][2];
+  double seed_r1[8][2];
+  double seed_width[8];
+} a5g_params;
+
+/* Box metadata for a5g_upload_tree: per id (0..max_id) 16 ints
+ *   [0] in_use, [1] lvl, [2] ix0, [3] ix1, [4] unused, [5] parent,
+ *   [6..9] children, [10..13] neighbors (lx, hx, ly, hy), [14] n_cell, [15] 0
+ * and per id 4 doubles: r_min0, r_min1, unused, dr.
+ * Level lists: for lvl = min_lvl..max_lvl, counts[3*k + {0,1,2}] = number of
+ * ids / leaves / parents, and ids[] holds, level by level, the ids, then the
+ * leaves, then the parents (the lists of lvl_t, afivo/src/m_aX_t.f90:165-169).
+ */
+
+typedef struct a5g_ctx a5g_ctx;
+
+const char *a5g_last_error(void);
+int a5g_version(void);
+
+/* Context life cycle. Replaces a$D_init (afivo/src/m_aX_core.f90:47-116):
+ * the device context owns all box storage. */
+int a5g_create(const a5g_params *p, a5g_ctx **out);
+int a5g_destroy(a5g_ctx *ctx);
+
+/* Transport table: replaces LT_create/LT_set_col
+ * (fosito/m_lookup_table.f90:46-72). rows_cols is n_rows x n_cols,
+ * column-major (rows_cols(n_rows, n_cols)); columns mobility, diffusion,
+ * alpha, eta (src/m_streamer.f90:37-41). */
+int a5g_set_table(a5g_ctx *ctx, int n_rows, int n_cols, double x_min,
+                  double inv_dx, const double *rows_cols);
+
+/* Topology upload after a$D_set_base / a$D_adjust_refinement
+ * (afivo/src/m_aX_core.f90:134-217, 456-520). Cell and face data of ids
+ * that stay in use are preserved on the device; storage grows as needed. */
+int a5g_upload_tree(a5g_ctx *ctx, int max_id, int min_lvl, int max_lvl,
+                    const int *meta16, const double *geom4,
+                    const int *lvl_counts, const int *lvl_ids);
+
+/* Host <-> device copies of one cell / face variable for ids 0..max_id,
+ * slot layout as described above. */
+int a5g_upload_cc(a5g_ctx *ctx, int iv, const double *host);
+int a5g_download_cc(a5g_ctx *ctx, int iv, double *host);
+int a5g_upload_fc(a5g_ctx *ctx, int dimf, int f, const double *host);
+int a5g_download_fc(a5g_ctx *ctx, int dimf, int f, double *host);
+
+/* Box-loop equivalents of the streamer callbacks and Afivo tree routines. */
+/* a$D_tree_copy_cc, afivo/src/m_aX_utils.f90:432-453 */
+int a5g_tree_copy_cc(a5g_ctx *ctx, int iv_from, int iv_to);
+/* a$D_loop_boxes_arg(fluxes_koren), src/streamer_2d.f90:384-489 (with the
+ * second ghost layer of afivo/src/m_aX_gc.f90:407-622) */
+int a5g_fluxes_koren(a5g_ctx *ctx, double dt);
+/* a$D_consistent_fluxes([f_elec]), afivo/src/m_aX_core.f90:818-930 */
+int a5g_consistent_fluxes(a5g_ctx *ctx);
+/* a$D_loop_box_arg(update_solution), src/streamer_2d.f90:499-542,
+ * src/streamer_cyl.f90:531-570 */
+int a5g_update_solution(a5g_ctx *ctx, double dt);
+/* a$D_restrict_tree, afivo/src/m_aX_restrict.f90:54-142 */
+int a5g_restrict_tree(a5g_ctx *ctx, int iv);
+/* a$D_gc_tree(iv, a$D_gc_interp_lim | a$D_gc_interp, a$D_gc_neumann),
+ * afivo/src/m_aX_gc.f90:28-330. rb_kind 0 = interp_lim, 1 = interp. */
+int a5g_gc_tree(a5g_ctx *ctx, int iv, int rb_kind);
+/* a$D_loop_box(average_dens), src/streamer_2d.f90:492-496 */
+int a5g_average_dens(a5g_ctx *ctx);
+/* compute_fld, src/streamer_2d.f90:307-343: space charge, one FAS FMG cycle
+ * (afivo/src/m_aX_mg.f90:163-565), fld_from_pot and the |E| ghost fill. */
+int a5g_compute_fld(a5g_ctx *ctx, int no_guess);
+/* mg$D_fas_fmg(tree, mg, set_residual, first_call) alone */
+int a5g_fas_fmg(a5g_ctx *ctx, int set_residual, int first_call);
+/* fld_from_pot on all boxes + a$D_gc_tree(i_fld, a$D_gc_interp, neumann) */
+int a5g_fld_from_pot(a5g_ctx *ctx);
+/* The reductions of get_max_dt (src/streamer_2d.f90:280-282):
+ * out3 = {max |E|, min |E|, max n_e} over leaf interiors. */
+int a5g_dt_reductions(a5g_ctx *ctx, double *out3);
+/* get_max_dt, src/streamer_2d.f90:271-303 (cyl :281-314) */
+int a5g_get_max_dt(a5g_ctx *ctx, double *dt);
+/* set_ref_flags for every box on levels 1..max_lvl
+ * (src/streamer_2d.f90:177-216, cyl :190-227); flags has max_id+1 ints,
+ * ids not visited hold INT_MIN+1 (the reference's -huge). */
+int a5g_ref_flags(a5g_ctx *ctx, double time, int *flags);
+/* prolong_to_new_boxes, src/streamer_2d.f90:592-617: for each level
+ * min_lvl..max_lvl in turn, n_new[k] ids taken from new_ids in order. */
+int a5g_prolong_new(a5g_ctx *ctx, const int *n_new, const int *new_ids);
+/* One full time step on the current mesh (src/streamer_2d.f90:93-128, one
+ * iteration of the n loop): save old densities, two forward-Euler stages
+ * with a field solve after the first, trapezoidal average, field solve.
+ * Runs as a single device launch. */
+int a5g_step(a5g_ctx *ctx, double dt);
+/* The same step for several independent runs in one launch (one persistent
+ * thread block per run). dts[k] is the step of run k. */
+int a5g_step_batch(a5g_ctx **ctxs, int n, const double *dts);
+/* Wait for all work queued on the context's stream. */
+int a5g_sync(a5g_ctx *ctx);
+/* Leaf cells of the uploaded tree (for throughput accounting). */
+int a5g_n_leaf_cells(a5g_ctx *ctx, long long *n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

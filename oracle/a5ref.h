@@ -1,0 +1,151 @@
+/*
+ * a5ref — CPU oracle for the a5_streamer per-timestep path.
+ *
+ * TEST INFRASTRUCTURE ONLY. This library is a plain C++ restatement of the
+ * reference's Fortran algorithm (Afivo tree, ghost cells, restriction,
+ * prolongation, FAS multigrid, and the 2D/cylindrical streamer callbacks).
+ * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may
+ * load it, and only as the checker or the timed CPU baseline. The product
+ * (a5_streamer_b200) never links or calls it.
+ *
+ * Parity status: the reference is Fortran 2008 and no Fortran compiler exists
+ * in this build environment, and the reference ships no golden vectors. The
+ * restatement is therefore pinned only by the reference's own known-answer
+ * cases (manufactured Poisson solutions, lookup-table convergence), restated
+ * in tests/. In that sense its parity with the reference binary is UNPINNED.
+ *
+ * All arithmetic is IEEE double, compiled with -ffp-contract=off so that no
+ * fused multiply-add changes the rounding of any expression; operation order
+ * follows the Fortran source expression by expression.
+ */
+#ifndef A5REF_H
+#define A5REF_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define A5REF_MAX_SEEDS 8
+#define A5REF_MAX_TD_ROWS 4096
+
+typedef struct a5ref_params {
+  int dim;               /* 2 (3 not yet restated) */
+  int coord;             /* 0 = Cartesian, 1 = cylindrical (r,z) */
+  int box_size;          /* cells per box edge (ST_box_size) */
+  int n_base[3];         /* base boxes per direction (4x4 in the 8 mm case) */
+  double dr_base;        /* cell size at level 1 */
+  int lvls_max;          /* finest allowed level */
+  double domain_len_z;   /* length along the last axis, sets the applied voltage */
+  double applied_fld;    /* ST_applied_fld (V/m); voltage = -len_z * fld */
+  double epsilon_diel;   /* ST_epsilon_diel */
+  double bg_dens;
+  int n_seeds;
+  double seed_r0[A5REF_MAX_SEEDS][3];
+  double seed_r1[A5REF_MAX_SEEDS][3];
+  double seed_dens[A5REF_MAX_SEEDS];
+  double seed_width[A5REF_MAX_SEEDS];
+  int seed_falloff[A5REF_MAX_SEEDS];
+  double dt_max;
+  int num_steps_amr;
+  int use_drt;           /* 1: include dt_drt in the step-size minimum */
+  int n_cycle_base;      /* 8 (Cartesian) / 4 (cylindrical) in the reference */
+  double ref_init_time;  /* refine around the seed while t < this */
+  double crv_refine;     /* refine if adx > 1 and crv_phi > this */
+  /* transport table */
+  int lkptbl_size;
+  double lkptbl_max_fld;
+  int td_n[4];                          /* number of input pairs per column */
+  double td_x[4][A5REF_MAX_TD_ROWS];    /* input x (|E|) per column */
+  double td_y[4][A5REF_MAX_TD_ROWS];    /* input y per column */
+  int n_threads;         /* OpenMP threads; <= 0 keeps the runtime default */
+} a5ref_params;
+
+typedef struct a5ref_sim a5ref_sim;
+
+a5ref_sim *a5ref_create(const a5ref_params *p);
+void a5ref_destroy(a5ref_sim *s);
+
+/* Initial refinement loop: set_init_cond / compute_fld / adjust_refinement
+ * until no box is added (src/streamer_2d.f90:58-63). Returns #iterations. */
+int a5ref_init(a5ref_sim *s);
+/* One pass of set_init_cond over all boxes (no refinement). */
+void a5ref_set_init_cond(a5ref_sim *s);
+
+/* get_max_dt (src/streamer_2d.f90:271-303). */
+double a5ref_get_max_dt(a5ref_sim *s);
+/* The three reductions get_max_dt uses: max |E|, min |E|, max n_e. */
+void a5ref_dt_reductions(a5ref_sim *s, double out3[3]);
+/* One full time step at fixed dt on a frozen mesh
+ * (src/streamer_2d.f90:93-128, one iteration of the n loop). */
+void a5ref_step(a5ref_sim *s, double dt);
+/* Main-loop block: get_max_dt, num_steps_amr steps, adjust_refinement,
+ * prolong_to_new_boxes + compute_fld if the mesh changed. Returns dt used. */
+double a5ref_advance(a5ref_sim *s, int do_regrid);
+/* Run the main loop until time > t_end or max_blocks blocks; returns blocks. */
+int a5ref_run(a5ref_sim *s, double t_end, int max_blocks);
+double a5ref_time(a5ref_sim *s);
+void a5ref_set_time(a5ref_sim *s, double t);
+
+/* Individual operations, for per-phase parity tests. */
+void a5ref_op_copy_cc(a5ref_sim *s, int iv_from, int iv_to);
+void a5ref_op_fluxes_koren(a5ref_sim *s, double dt);
+void a5ref_op_consistent_fluxes(a5ref_sim *s);
+void a5ref_op_update_solution(a5ref_sim *s, double dt);
+void a5ref_op_restrict_tree(a5ref_sim *s, int iv);
+/* rb_kind: 0 = interp_lim, 1 = interp; bc is Neumann */
+void a5ref_op_gc_tree(a5ref_sim *s, int iv, int rb_kind);
+void a5ref_op_average_dens(a5ref_sim *s);
+void a5ref_op_compute_fld(a5ref_sim *s, int no_guess);
+void a5ref_op_set_rhs(a5ref_sim *s);
+void a5ref_op_fmg(a5ref_sim *s, int set_residual, int first_call);
+void a5ref_op_fld_from_pot(a5ref_sim *s);
+/* Per-box refinement flags from set_ref_flags (levels 1..max_lvl; boxes not
+ * visited hold -huge). out has max_id+1 entries, index = box id. */
+void a5ref_op_ref_flags(a5ref_sim *s, int *out);
+/* adjust_refinement + prolong_to_new_boxes; returns n_add + n_rm. */
+int a5ref_op_regrid(a5ref_sim *s, int *n_add, int *n_rm);
+
+/* Tree export. Boxes are numbered 1..max_id as in the reference. */
+int a5ref_max_id(a5ref_sim *s);
+int a5ref_max_lvl(a5ref_sim *s);
+int a5ref_min_lvl(a5ref_sim *s);
+int a5ref_n_leaf_cells(a5ref_sim *s);
+int a5ref_n_cells_all(a5ref_sim *s);
+/* meta: per id (0..max_id) 16 ints: in_use, lvl, ix0, ix1, ix2, parent,
+ * children[4] (2D: first 4 used), neighbors[4], n_cell, pad. */
+void a5ref_export_meta(a5ref_sim *s, int *meta);
+/* per id: r_min[3], dr */
+void a5ref_export_geom(a5ref_sim *s, double *geom);
+/* level lists: for each level min..max writes ids/leaves/parents counts
+ * into counts[3*(nlev)] and the ids concatenated into ids (capacity cap). */
+int a5ref_export_levels(a5ref_sim *s, int *counts, int *ids, int cap);
+/* Cell data for variable iv: per id, (n_cell+2)^2 values laid out i-fastest
+ * in a slot of (box_size+2)^2 doubles; unused ids are zero. */
+void a5ref_export_cc(a5ref_sim *s, int iv, double *out);
+void a5ref_import_cc(a5ref_sim *s, int iv, const double *in);
+/* Face data fx/fy of face variable f: per id a slot of (nc+1)*nc doubles. */
+void a5ref_export_fc(a5ref_sim *s, int dimf, int f, double *out);
+void a5ref_import_fc(a5ref_sim *s, int dimf, int f, const double *in);
+/* The built lookup table rows_cols (n_rows x 4, column-major) and x grid. */
+void a5ref_export_table(a5ref_sim *s, double *rows_cols, double *x_min,
+                        double *inv_dx, int *n_rows);
+double a5ref_applied_voltage(a5ref_sim *s);
+
+/* Known-answer multigrid case restating afivo/examples/multigrid/test_mg2_2d.f90
+ * (two Gaussians, Dirichlet by the exact solution, curvature refinement).
+ * Writes per-FMG-cycle max |residual| and max |error| and returns #cells. */
+int a5ref_kat_mg2_2d(int n_fmg, double *res_out, double *err_out,
+                     int *max_lvl_out);
+/* Cylindrical variant restating afivo/examples/multigrid/test_mg_cyl.f90. */
+int a5ref_kat_mg_cyl(int n_fmg, double *res_out, double *err_out,
+                     int *max_lvl_out);
+/* Lookup-table convergence test restating fosito/test/test_m_lookup_table.f90:
+ * max error of LT_get_col on sin(x) for a table of n_rows over [0, x_max]. */
+double a5ref_kat_lookup(int n_rows, int n_pairs, double x_max, int n_samples);
+/* Koren limiter (src/m_streamer.f90:339-362). */
+double a5ref_koren_mlim(double a, double b);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,308 @@
+"""ctypes wrapper of the CPU oracle (test infrastructure only).
+
+The oracle is a plain C++ restatement of the reference's Fortran algorithm,
+built into oracle/liba5ref.so by oracle/Makefile. Only the tests, the smoke
+check and the CPU-baseline leg of the benchmark use it, as the checker or as
+the timed CPU baseline; the product never imports this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liba5ref.so")
+
+MAX_SEEDS = 8
+MAX_TD = 4096
+TD_COLUMNS = ("mobility", "diffusion", "alpha", "eta")
+
+# variable indices (src/m_streamer.f90:17-43), 0-based
+I_ELEC, I_PION, I_ELEC_OLD, I_PION_OLD, I_PHI, I_FLD, I_RHS, I_PHO, I_EPS = range(9)
+F_ELEC, F_FLD = 0, 1
+
+
+class Params(ctypes.Structure):
+    _fields_ = [
+        ("dim", ctypes.c_int), ("coord", ctypes.c_int), ("box_size", ctypes.c_int),
+        ("n_base", ctypes.c_int * 3), ("dr_base", ctypes.c_double),
+        ("lvls_max", ctypes.c_int), ("domain_len_z", ctypes.c_double),
+        ("applied_fld", ctypes.c_double), ("epsilon_diel", ctypes.c_double),
+        ("bg_dens", ctypes.c_double), ("n_seeds", ctypes.c_int),
+        ("seed_r0", (ctypes.c_double * 3) * MAX_SEEDS),
+        ("seed_r1", (ctypes.c_double * 3) * MAX_SEEDS),
+        ("seed_dens", ctypes.c_double * MAX_SEEDS),
+        ("seed_width", ctypes.c_double * MAX_SEEDS),
+        ("seed_falloff", ctypes.c_int * MAX_SEEDS),
+        ("dt_max", ctypes.c_double), ("num_steps_amr", ctypes.c_int),
+        ("use_drt", ctypes.c_int), ("n_cycle_base", ctypes.c_int),
+        ("ref_init_time", ctypes.c_double), ("crv_refine", ctypes.c_double),
+        ("lkptbl_size", ctypes.c_int), ("lkptbl_max_fld", ctypes.c_double),
+        ("td_n", ctypes.c_int * 4),
+        ("td_x", (ctypes.c_double * MAX_TD) * 4),
+        ("td_y", (ctypes.c_double * MAX_TD) * 4),
+        ("n_threads", ctypes.c_int),
+    ]
+
+
+def build(force: bool = False) -> str:
+    src = os.path.join(HERE, "a5ref.cpp")
+    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
+        subprocess.check_call(["make", "-s", "-C", HERE])
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(LIB_PATH)
+        P, D, I, V = ctypes.c_void_p, ctypes.c_double, ctypes.c_int, None
+        pd, pi = ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)
+        sig = {
+            "a5ref_create": (P, [ctypes.POINTER(Params)]), "a5ref_destroy": (V, [P]),
+            "a5ref_init": (I, [P]), "a5ref_set_init_cond": (V, [P]),
+            "a5ref_get_max_dt": (D, [P]), "a5ref_dt_reductions": (V, [P, pd]),
+            "a5ref_step": (V, [P, D]), "a5ref_advance": (D, [P, I]),
+            "a5ref_run": (I, [P, D, I]), "a5ref_time": (D, [P]), "a5ref_set_time": (V, [P, D]),
+            "a5ref_op_copy_cc": (V, [P, I, I]), "a5ref_op_fluxes_koren": (V, [P, D]),
+            "a5ref_op_consistent_fluxes": (V, [P]), "a5ref_op_update_solution": (V, [P, D]),
+            "a5ref_op_restrict_tree": (V, [P, I]), "a5ref_op_gc_tree": (V, [P, I, I]),
+            "a5ref_op_average_dens": (V, [P]), "a5ref_op_compute_fld": (V, [P, I]),
+            "a5ref_op_set_rhs": (V, [P]), "a5ref_op_fmg": (V, [P, I, I]),
+            "a5ref_op_fld_from_pot": (V, [P]), "a5ref_op_ref_flags": (V, [P, pi]),
+            "a5ref_op_regrid": (I, [P, pi, pi]),
+            "a5ref_max_id": (I, [P]), "a5ref_max_lvl": (I, [P]), "a5ref_min_lvl": (I, [P]),
+            "a5ref_n_leaf_cells": (I, [P]), "a5ref_n_cells_all": (I, [P]),
+            "a5ref_export_meta": (V, [P, pi]), "a5ref_export_geom": (V, [P, pd]),
+            "a5ref_export_levels": (I, [P, pi, pi, I]),
+            "a5ref_export_cc": (V, [P, I, pd]), "a5ref_import_cc": (V, [P, I, pd]),
+            "a5ref_export_fc": (V, [P, I, I, pd]), "a5ref_import_fc": (V, [P, I, I, pd]),
+            "a5ref_export_table": (V, [P, pd, pd, pd, pi]),
+            "a5ref_applied_voltage": (D, [P]),
+            "a5ref_kat_mg2_2d": (I, [I, pd, pd, pi]), "a5ref_kat_mg_cyl": (I, [I, pd, pd, pi]),
+            "a5ref_kat_lookup": (D, [I, I, D, I]), "a5ref_koren_mlim": (D, [D, D]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _ip(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+def make_params(cfg, n_threads: int = 0) -> Params:
+    """Fill the oracle's parameter block from a StreamerConfig-like object."""
+    p = Params()
+    p.dim = cfg.dim
+    p.coord = 1 if cfg.coord == "cyl" else 0
+    p.box_size = cfg.box_size
+    for d in range(cfg.dim):
+        p.n_base[d] = cfg.n_base[d]
+    p.dr_base = cfg.dr_base
+    p.lvls_max = cfg.lvls_max
+    p.domain_len_z = cfg.domain_len_z
+    p.applied_fld = cfg.applied_fld
+    p.epsilon_diel = cfg.epsilon_diel
+    p.bg_dens = cfg.bg_dens
+    p.n_seeds = len(cfg.seeds)
+    for n, s in enumerate(cfg.seeds):
+        for d in range(cfg.dim):
+            p.seed_r0[n][d] = s.r0[d]
+            p.seed_r1[n][d] = s.r1[d]
+        p.seed_dens[n] = s.dens
+        p.seed_width[n] = s.width
+        p.seed_falloff[n] = s.falloff
+    p.dt_max = cfg.dt_max
+    p.num_steps_amr = cfg.num_steps_amr
+    p.use_drt = 1 if cfg.use_drt else 0
+    p.n_cycle_base = cfg.n_cycle_base
+    p.ref_init_time = cfg.ref_init_time
+    p.crv_refine = cfg.crv_refine
+    p.lkptbl_size = cfg.lkptbl_size
+    p.lkptbl_max_fld = cfg.lkptbl_max_fld
+    for c, name in enumerate(TD_COLUMNS):
+        xs, ys = cfg.td[name]
+        p.td_n[c] = len(xs)
+        for k in range(len(xs)):
+            p.td_x[c][k] = xs[k]
+            p.td_y[c][k] = ys[k]
+    p.n_threads = n_threads
+    return p
+
+
+class Sim:
+    """One oracle simulation (tree + fields)."""
+
+    def __init__(self, cfg, n_threads: int = 0):
+        self.cfg = cfg
+        self._p = make_params(cfg, n_threads)
+        self.h = lib().a5ref_create(ctypes.byref(self._p))
+        if not self.h:
+            raise ValueError("oracle rejected the parameters")
+        self.nc = cfg.box_size
+
+    def close(self):
+        if self.h:
+            lib().a5ref_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # driver -----------------------------------------------------------------
+    def init(self) -> int:
+        return lib().a5ref_init(self.h)
+
+    def set_init_cond(self):
+        lib().a5ref_set_init_cond(self.h)
+
+    def get_max_dt(self) -> float:
+        return lib().a5ref_get_max_dt(self.h)
+
+    def dt_reductions(self) -> np.ndarray:
+        out = np.zeros(3)
+        lib().a5ref_dt_reductions(self.h, _dp(out))
+        return out
+
+    def step(self, dt: float):
+        lib().a5ref_step(self.h, dt)
+
+    def advance(self, regrid: bool = True) -> float:
+        return lib().a5ref_advance(self.h, 1 if regrid else 0)
+
+    def run(self, t_end: float, max_blocks: int = 1 << 30) -> int:
+        return lib().a5ref_run(self.h, t_end, max_blocks)
+
+    @property
+    def time(self) -> float:
+        return lib().a5ref_time(self.h)
+
+    @time.setter
+    def time(self, t: float):
+        lib().a5ref_set_time(self.h, t)
+
+    # ops ------------------------------------------------------------------------
+    def op(self, name: str, *args):
+        return getattr(lib(), "a5ref_op_" + name)(self.h, *args)
+
+    def ref_flags(self) -> np.ndarray:
+        out = np.zeros(self.max_id + 1, dtype=np.int32)
+        lib().a5ref_op_ref_flags(self.h, _ip(out))
+        return out
+
+    def regrid(self):
+        a, r = ctypes.c_int(0), ctypes.c_int(0)
+        lib().a5ref_op_regrid(self.h, ctypes.byref(a), ctypes.byref(r))
+        return a.value, r.value
+
+    # tree / data export -------------------------------------------------------
+    @property
+    def max_id(self) -> int:
+        return lib().a5ref_max_id(self.h)
+
+    @property
+    def max_lvl(self) -> int:
+        return lib().a5ref_max_lvl(self.h)
+
+    @property
+    def min_lvl(self) -> int:
+        return lib().a5ref_min_lvl(self.h)
+
+    def n_leaf_cells(self) -> int:
+        return lib().a5ref_n_leaf_cells(self.h)
+
+    def n_cells_all(self) -> int:
+        return lib().a5ref_n_cells_all(self.h)
+
+    def meta(self) -> np.ndarray:
+        m = np.zeros((self.max_id + 1, 16), dtype=np.int32)
+        lib().a5ref_export_meta(self.h, _ip(m))
+        return m
+
+    def geom(self) -> np.ndarray:
+        g = np.zeros((self.max_id + 1, 4))
+        lib().a5ref_export_geom(self.h, _dp(g))
+        return g
+
+    def levels(self):
+        nlev = self.max_lvl - self.min_lvl + 1
+        counts = np.zeros((nlev, 3), dtype=np.int32)
+        cap = 3 * (self.max_id + 1)
+        ids = np.zeros(cap, dtype=np.int32)
+        lib().a5ref_export_levels(self.h, _ip(counts), _ip(ids), cap)
+        out, k = {}, 0
+        for li in range(nlev):
+            lvl = self.min_lvl + li
+            n_ids, n_lv, n_pa = counts[li]
+            a = ids[k:k + n_ids].copy(); k += n_ids
+            b = ids[k:k + n_lv].copy(); k += n_lv
+            c = ids[k:k + n_pa].copy(); k += n_pa
+            out[lvl] = (a, b, c)
+        return out
+
+    def cc(self, iv: int) -> np.ndarray:
+        S = (self.nc + 2) ** 2
+        out = np.zeros((self.max_id + 1, S))
+        lib().a5ref_export_cc(self.h, iv, _dp(out))
+        return out
+
+    def set_cc(self, iv: int, data: np.ndarray):
+        data = np.ascontiguousarray(data, dtype=np.float64)
+        lib().a5ref_import_cc(self.h, iv, _dp(data))
+
+    def fc(self, dimf: int, f: int) -> np.ndarray:
+        S = (self.nc + 1) * self.nc
+        out = np.zeros((self.max_id + 1, S))
+        lib().a5ref_export_fc(self.h, dimf, f, _dp(out))
+        return out
+
+    def set_fc(self, dimf: int, f: int, data: np.ndarray):
+        data = np.ascontiguousarray(data, dtype=np.float64)
+        lib().a5ref_import_fc(self.h, dimf, f, _dp(data))
+
+    def table(self):
+        n = ctypes.c_int(0)
+        xm, inv = ctypes.c_double(0), ctypes.c_double(0)
+        lib().a5ref_export_table(self.h, None, ctypes.byref(xm), ctypes.byref(inv), ctypes.byref(n))
+        rc = np.zeros(n.value * 4)
+        lib().a5ref_export_table(self.h, _dp(rc), None, None, None)
+        return rc.reshape(4, n.value).T.copy(), xm.value, inv.value
+
+    @property
+    def applied_voltage(self) -> float:
+        return lib().a5ref_applied_voltage(self.h)
+
+
+def kat_mg(cyl: bool, n_fmg: int):
+    res, err = np.zeros(n_fmg), np.zeros(n_fmg)
+    ml = ctypes.c_int(0)
+    fn = lib().a5ref_kat_mg_cyl if cyl else lib().a5ref_kat_mg2_2d
+    cells = fn(n_fmg, _dp(res), _dp(err), ctypes.byref(ml))
+    return res, err, ml.value, cells
+
+
+def kat_lookup(n_rows: int, n_pairs: int = 100000, x_max: float = 10.0,
+               n_samples: int = 10000) -> float:
+    return lib().a5ref_kat_lookup(n_rows, n_pairs, x_max, n_samples)
+
+
+def koren_mlim(a: float, b: float) -> float:
+    return lib().a5ref_koren_mlim(a, b)
