@@ -70,7 +70,39 @@ SIGNATURES = {
     "a5g_step_batch": (_I, [ctypes.POINTER(_P), _I, _PD]),
     "a5g_sync": (_I, [_P]),
     "a5g_n_leaf_cells": (_I, [_P, ctypes.POINTER(ctypes.c_longlong)]),
+    "a5g_get_stream": (_I, [_P, ctypes.POINTER(_P)]),
+    # host tree (include/a5t.h)
+    "a5t_create": (_I, [_I, _I, _D, _PD, _I, ctypes.POINTER(_P)]),
+    "a5t_destroy": (_I, [_P]),
+    "a5t_set_base": (_I, [_P, _I, _PI, _PI]),
+    "a5t_adjust_refinement": (_I, [_P, _PI, _PI, _PI]),
+    "a5t_max_id": (_I, [_P]),
+    "a5t_min_lvl": (_I, [_P]),
+    "a5t_max_lvl": (_I, [_P]),
+    "a5t_export": (_I, [_P, _PI, _PD, _PI, _PI]),
+    "a5t_n_level_ids": (_I, [_P]),
+    "a5t_new_boxes": (_I, [_P, _PI, _PI]),
+    # streamer driver
+    "a5s_create": (_I, [ctypes.c_void_p, ctypes.POINTER(_P)]),
+    "a5s_destroy": (_I, [_P]),
+    "a5s_init": (_I, [_P, _PI]),
+    "a5s_advance": (_I, [_P, _I, _PD]),
+    "a5s_run": (_I, [_P, _D, _I, _PI]),
+    "a5s_time": (_I, [_P, _PD]),
+    "a5s_ctx": (_I, [_P, ctypes.POINTER(_P)]),
+    "a5s_tree": (_I, [_P, ctypes.POINTER(_P)]),
+    "a5s_table": (_I, [_P, _PD, _PD, _PD, _PI]),
 }
+
+
+class SimConfig(ctypes.Structure):
+    _fields_ = [
+        ("dev", Params), ("n_base", ctypes.c_int * 2), ("bg_dens", ctypes.c_double),
+        ("n_seeds", ctypes.c_int), ("seed_dens", ctypes.c_double * 8),
+        ("seed_falloff", ctypes.c_int * 8), ("num_steps_amr", ctypes.c_int),
+        ("lkptbl_size", ctypes.c_int), ("lkptbl_max_fld", ctypes.c_double),
+        ("td_n", ctypes.c_int * 4), ("td_x", _PD * 4), ("td_y", _PD * 4),
+    ]
 
 _lib = None
 

@@ -1167,6 +1167,7 @@ static int launch(a5g_ctx *c, const Op &op) {
 
 extern "C" {
 
+int a5g_internal_fail(int code, const char *msg) { return fail(code, msg ? msg : ""); }
 const char *a5g_last_error(void) { return g_err.c_str(); }
 int a5g_version(void) { return 1; }
 
@@ -1617,6 +1618,12 @@ int a5g_sync(a5g_ctx *c) {
   if (!c) return fail(A5G_EINVAL, "null context");
   CK(cudaStreamSynchronize(c->stream));
   return check_status(c);
+}
+
+int a5g_get_stream(a5g_ctx *c, void **stream) {
+  if (!c || !stream) return fail(A5G_EINVAL, "null argument");
+  *stream = (void *)c->stream;
+  return A5G_OK;
 }
 
 int a5g_n_leaf_cells(a5g_ctx *c, long long *n) {

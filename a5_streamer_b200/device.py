@@ -181,6 +181,11 @@ class DeviceRun:
     def sync(self):
         call("a5g_sync", self.h)
 
+    def stream_ptr(self) -> int:
+        s = ctypes.c_void_p()
+        call("a5g_get_stream", self.h, ctypes.byref(s))
+        return s.value or 0
+
     def n_leaf_cells(self) -> int:
         n = ctypes.c_longlong(0)
         call("a5g_n_leaf_cells", self.h, ctypes.byref(n))

@@ -1,0 +1,81 @@
+"""Throughput accounting: tree census and the algorithmic-bytes model of one
+full time step.
+
+The model counts compulsory traffic: every phase of the step reads each
+distinct input field once and writes each output once over the interior
+cells, plus ghost traffic of g = 4D/nc words per variable per ghost fill.
+Per full step (two forward-Euler stages, two field solves, the trapezoidal
+average; src/streamer_2d.f90:93-128), in 8-byte words:
+
+  T1 save old densities        4 N_all
+  T2 fluxes + update (x2)      2 (3D + 7 + 2D/nc) N_leaf
+  T3 restriction (x2)          2 * 2 (1 + 2^-D) N_{l>=2}
+  T4 ghost fill n_e, n_i (x2)  2 * 2 g N_all
+  T5 average                   6 N_all
+  T6 space charge (x2)         2 * 3 N_leaf
+  T7 FAS FMG (x2)              2 [ sum_l N_l ((L-l+1) V + F) + 5 sum_l P_l (L-l+1) ]
+                               V = 2(n_down+n_up) 2.5 + 2(n_down+n_up) g + 3 + 2(1+2^-D) + 2 + 2 + g
+                               F = 12 + 2g
+  T8 field from potential (x2) 2 (D + 2 + g) N_all
+  T9 step-size reductions      3 N_leaf
+
+with N_l the cells of all boxes on level l, P_l the cells of parent boxes on
+level l, L the finest level, N_all = sum over levels >= 1, N_leaf the leaf
+cells. For a uniform 2D tree this is about 253 words (2 kB) per leaf cell.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+from typing import Dict, Tuple
+
+import numpy as np
+
+
+@dataclass
+class Census:
+    dim: int
+    nc: int
+    min_lvl: int
+    max_lvl: int
+    cells: Dict[int, int]         # all boxes per level
+    leaf_cells: Dict[int, int]
+    parent_cells: Dict[int, int]
+
+    @property
+    def n_leaf(self) -> int:
+        return sum(self.leaf_cells.values())
+
+    @property
+    def n_all(self) -> int:
+        return sum(v for l, v in self.cells.items() if l >= 1)
+
+
+def census(meta: np.ndarray, levels: Dict[int, Tuple[np.ndarray, np.ndarray, np.ndarray]],
+           nc: int, dim: int = 2) -> Census:
+    cells, leaf, par = {}, {}, {}
+    for lvl, (ids, lv, pa) in levels.items():
+        cnt = lambda xs: int(sum(int(meta[i, 14]) ** dim for i in xs))
+        cells[lvl], leaf[lvl], par[lvl] = cnt(ids), cnt(lv), cnt(pa)
+    return Census(dim, nc, min(levels), max(levels), cells, leaf, par)
+
+
+def bytes_per_step(c: Census, n_down: int = 2, n_up: int = 2, word: int = 8) -> float:
+    D, nc = c.dim, c.nc
+    g = 4.0 * D / nc
+    N_all, N_leaf = c.n_all, c.n_leaf
+    N_ge2 = sum(v for l, v in c.cells.items() if l >= 2)
+    t1 = 4 * N_all
+    t2 = 2 * (3 * D + 7 + 2.0 * D / nc) * N_leaf
+    t3 = 2 * 2 * (1 + 2.0 ** -D) * N_ge2
+    t4 = 2 * 2 * g * N_all
+    t5 = 6 * N_all
+    t6 = 2 * 3 * N_leaf
+    V = 2 * (n_down + n_up) * 2.5 + 2 * (n_down + n_up) * g + 3 + 2 * (1 + 2.0 ** -D) + 2 + 2 + g
+    F = 12 + 2 * g
+    L = c.max_lvl
+    fmg = sum(n * ((L - l + 1) * V + F) for l, n in c.cells.items())
+    fmg += 5 * sum(n * (L - l + 1) for l, n in c.parent_cells.items())
+    t7 = 2 * fmg
+    t8 = 2 * (D + 2 + g) * N_all
+    t9 = 3 * N_leaf
+    return word * (t1 + t2 + t3 + t4 + t5 + t6 + t7 + t8 + t9)

@@ -1,0 +1,355 @@
+#!/usr/bin/env python
+"""Benchmark: leaf-cell updates per second per full streamer time step.
+
+One "step" is one full time step of the streamer model on the current mesh
+(save old densities, two forward-Euler stages with a field solve after the
+first, trapezoidal average, second field solve), i.e. one iteration of the
+inner loop of src/streamer_2d.f90:93-128. The workload is the 8 mm Cartesian
+FP64 case evolved from its initial conditions to its end time t = 2 ns with
+the full regrid cycle; the mesh is then frozen and K steps are timed at the
+step size get_max_dt gives.
+
+Arms:
+  --impl b200       (default) the sm_100a device path through its C ABI
+  --impl reference  the CPU implementation of the same path (the oracle port
+                    of the reference's Fortran) on all host cores
+
+Multi-GPU (torchrun): one independent replica of the run per rank ("weak"
+scaling, no data-path collective); the device time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("cell-updates/s per full step, mixed vs FP64 on 1 B200 at stated error; %HBM roof")
+UNIT = "cell-updates/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--workload", choices=["cartesian_8mm", "cylindrical_16mm"], default="cartesian_8mm")
+    ap.add_argument("--batch", type=int, default=148, help="replicas in the batched extra (0: skip)")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0, help="budget of the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload_cfg(name):
+    from a5_streamer_b200 import config
+    if name == "cartesian_8mm":
+        return config.cartesian_8mm(), "cartesian_8mm_fp64_t2ns"
+    return config.cylindrical_16mm(), "cylindrical_16mm_fp64_t10ns_no_photoionization"
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """Samples SM clocks and clock-event reasons through NVML while running."""
+
+    REASONS = {
+        "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+        "sw_power_cap": 0x4,
+    }
+
+    def __init__(self, index: int, period: float = 0.01):
+        self.index, self.period = index, period
+        self.samples, self.reasons = [], set()
+        self._stop = threading.Event()
+        self.max_mhz = None
+        self.ok = False
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception:
+            self.ok = False
+
+    def _run(self):
+        nv = self.nv
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                try:
+                    r = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                except Exception:
+                    r = nv.nvmlDeviceGetCurrentClocksThrottleReasons(self.h)
+                for name, bit in self.REASONS.items():
+                    if r & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(self.period)
+
+    def __enter__(self):
+        if self.ok:
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        if self.ok:
+            self._stop.set()
+            self.t.join()
+
+    def summary(self):
+        if not self.ok or not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                    "samples": len(self.samples)}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_per_launch(workload):
+    """DRAM bytes per step launch from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", f"a5g_step_{workload}.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["dram_bytes_per_launch"])
+    except Exception:
+        return None
+
+
+# ---------------------------------------------------------------------------
+def cpu_baseline(cfg, seconds, threads):
+    """The oracle port of the reference's algorithm on the host cores: the same
+    run to the end time, then as many full steps as fit in the budget."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import a5ref
+    sim = a5ref.Sim(cfg, n_threads=threads)
+    sim.init()
+    sim.run(cfg.end_time)
+    n_leaf = sim.n_leaf_cells()
+    dt = sim.get_max_dt()
+    sim.step(dt)  # warm
+    steps, t0 = 0, time.perf_counter()
+    while True:
+        sim.step(dt)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el > seconds or steps >= 100000:
+            break
+    return n_leaf * steps / el, steps, el, n_leaf
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    cfg, wname = workload_cfg(args.workload)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import a5ref
+    threads = os.cpu_count() or 1
+    sim = a5ref.Sim(cfg, n_threads=threads)
+    sim.init()
+    sim.run(cfg.end_time)
+    n_leaf = sim.n_leaf_cells()
+    dt = sim.get_max_dt()
+    for _ in range(args.warmup):
+        sim.step(dt)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        sim.step(dt)
+    el = time.perf_counter() - t0
+    value = n_leaf * args.steps / el
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": wname, "leaf_cells": n_leaf, "max_lvl": sim.max_lvl},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} full steps of the {wname} mesh at t_end, "
+                                   f"OpenMP over the boxes of each level"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+def run_b200(args):
+    import numpy as np
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    from a5_streamer_b200 import build, metrics, streamer
+    from a5_streamer_b200 import device as dv
+    build.build()  # no-op when the in-tree library is current
+
+    cfg, wname = workload_cfg(args.workload)
+    sim = streamer.Simulation(cfg)
+    sim.init()
+    sim.run(cfg.end_time)
+    run = sim.device
+    n_leaf = run.n_leaf_cells()
+    meta, geom, levels = sim.tree.export()
+    cen = metrics.census(meta, levels, cfg.box_size)
+    bytes_step = metrics.bytes_per_step(cen)
+    dt = run.get_max_dt()
+
+    ext = torch.cuda.ExternalStream(run.stream_ptr())
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+    for _ in range(args.warmup):
+        run.step(dt)
+    run.sync()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+
+    K = args.steps
+    e0 = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    e1 = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    with ClockSampler(local) as clk:
+        with torch.cuda.stream(ext):
+            for k in range(K):
+                flush.fill_(k & 0xFF)
+                e0[k].record(ext)
+                run.step(dt)
+                e1[k].record(ext)
+        run.sync()
+        torch.cuda.synchronize()
+    step_ms = [a.elapsed_time(b) for a, b in zip(e0, e1)]
+    total_s = sum(step_ms) / 1e3
+    if dist:
+        t = torch.tensor([total_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_s = float(t.item())
+    value = n_leaf * K * world / total_s
+    ms_per_step = 1e3 * total_s / K
+
+    # end to end through the public API: dt computed from device reductions
+    # read back to the host each step, the step launched with the host dt
+    run.sync()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(K):
+        d = run.get_max_dt()
+        run.step(d)
+    run.sync()
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": n_leaf * K * world / e2e_s, "unit": UNIT,
+           "h2d_bytes_per_step": 8, "d2h_bytes_per_step": 24}
+
+    # batched extra: B replicas of the same mesh and state, one block each
+    batched = None
+    if args.batch > 0:
+        cc = [run.cc(iv) for iv in range(9)]
+        fc = [[run.fc(d, f) for f in range(2)] for d in range(2)]
+        rc, xm, inv = sim.table()
+        reps = []
+        for _ in range(args.batch):
+            r = dv.DeviceRun(cfg)
+            r.set_table(rc, xm, inv)
+            r.upload_tree(meta, geom, sim.tree.min_lvl, sim.tree.max_lvl, levels)
+            for iv in range(9):
+                r.set_cc(iv, cc[iv])
+            for d in range(2):
+                for f in range(2):
+                    r.set_fc(d, f, fc[d][f])
+            reps.append(r)
+        bstream = torch.cuda.ExternalStream(reps[0].stream_ptr())
+        dts = [dt] * len(reps)
+        for _ in range(2):
+            dv.step_batch(reps, dts)
+        reps[0].sync()
+        nb = max(3, K // 10)
+        b0 = [torch.cuda.Event(enable_timing=True) for _ in range(nb)]
+        b1 = [torch.cuda.Event(enable_timing=True) for _ in range(nb)]
+        with torch.cuda.stream(bstream):
+            for k in range(nb):
+                flush.fill_(k & 0xFF)
+                b0[k].record(bstream)
+                dv.step_batch(reps, dts)
+                b1[k].record(bstream)
+        reps[0].sync()
+        torch.cuda.synchronize()
+        bt = sum(a.elapsed_time(b) for a, b in zip(b0, b1)) / 1e3
+        batched = {"replicas": len(reps), "steps": nb, "value": n_leaf * len(reps) * nb / bt,
+                   "unit": UNIT, "ms_per_step": 1e3 * bt / nb,
+                   "achieved_gbs": bytes_step * len(reps) * nb / bt / 1e9}
+        for r in reps:
+            r.close()
+
+    peak, peak_kind = measured_peak()
+    achieved = bytes_step / (ms_per_step / 1e3) / 1e9
+    traffic = traffic_per_launch(wname)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic,
+                "peak_kind": peak_kind, "algorithmic_bytes_per_launch": bytes_step}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        v, steps, el, nl = cpu_baseline(cfg, args.cpu_seconds, threads)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{steps} full steps ({el:.1f} s) of the same mesh at t_end, "
+                         f"oracle port, OpenMP over the boxes of each level"}
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": wname, "leaf_cells": n_leaf, "boxes_in_use": int(meta[:, 0].sum()),
+                       "min_lvl": sim.tree.min_lvl, "max_lvl": sim.tree.max_lvl,
+                       "precision": "fp64", "parallelism": f"replicas{world}",
+                       "l2": "flushed before every timed step (256 MiB write)"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": K,
+            "clocks": clk.summary(), "batched": batched,
+        }
+        print(json.dumps(out), flush=True)
+    sim.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

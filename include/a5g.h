@@ -152,6 +152,9 @@ int a5g_step(a5g_ctx *ctx, double dt);
 int a5g_step_batch(a5g_ctx **ctxs, int n, const double *dts);
 /* Wait for all work queued on the context's stream. */
 int a5g_sync(a5g_ctx *ctx);
+/* The cudaStream_t (as void*) all work of this context is queued on, so a
+ * caller can order its own work or timing events with it. */
+int a5g_get_stream(a5g_ctx *ctx, void **stream);
 /* Leaf cells of the uploaded tree (for throughput accounting). */
 int a5g_n_leaf_cells(a5g_ctx *ctx, long long *n);
 
