@@ -68,6 +68,7 @@ SIGNATURES = {
     "a5g_prolong_new": (_I, [_P, _PI, _PI]),
     "a5g_step": (_I, [_P, _D]),
     "a5g_step_batch": (_I, [ctypes.POINTER(_P), _I, _PD]),
+    "a5g_step_batch_static": (_I, [ctypes.POINTER(_P), _I, _PD]),
     "a5g_sync": (_I, [_P]),
     "a5g_n_leaf_cells": (_I, [_P, ctypes.POINTER(ctypes.c_longlong)]),
     "a5g_get_stream": (_I, [_P, ctypes.POINTER(_P)]),

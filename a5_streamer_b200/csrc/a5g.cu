@@ -27,6 +27,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1095,7 +1096,34 @@ a5g_run_kernel(const RunDev *single, Op single_op, const RunDev *const *runs, co
   run_op(sR, op);
 }
 
+// Descriptor of one member of a launch of a5g_step_batch_static.
+struct BatchSlot {
+  const RunDev *run;
+  Op op;
+};
+
+// Same work as a5g_run_kernel, with each block's run and operation read from
+// a descriptor table (the fixed array below).
+__global__ void __launch_bounds__(NTHR, 1) a5g_run_kernel_slots(const BatchSlot *slots) {
+  __shared__ RunDev sR;
+  const RunDev *src = slots[blockIdx.x].run;
+  {
+    const int *s = reinterpret_cast<const int *>(src);
+    int *d = reinterpret_cast<int *>(&sR);
+    for (int k = threadIdx.x; k < (int)(sizeof(RunDev) / sizeof(int)); k += NTHR) d[k] = s[k];
+  }
+  __syncthreads();
+  Op op = slots[blockIdx.x].op;
+  run_op(sR, op);
+}
+
 }  // namespace
+
+// Descriptor table of a5g_step_batch_static: a fixed device array, so that
+// entry point needs no allocation. Host code must not pass this name to a
+// kernel (on the host it only stands in for the symbol); its device address
+// comes from cudaGetSymbolAddress.
+static __device__ __align__(256) BatchSlot g_batch_scratch[A5G_STATIC_BATCH_MAX];
 
 // ===========================================================================
 // Host side: contexts and the C ABI.
@@ -1611,6 +1639,53 @@ int a5g_step_batch(a5g_ctx **ctxs, int n, const double *dts) {
   CK(cudaGetLastError());
   CK(cudaFreeAsync(d_rp, c0->stream));
   CK(cudaFreeAsync(d_ops, c0->stream));
+  return A5G_OK;
+}
+
+// Per-device address of g_batch_scratch, looked up on first use with the
+// device current; host staging of the descriptors in a fixed host array.
+static std::mutex g_static_mu;
+static BatchSlot *g_static_dev[256] = {};
+static BatchSlot g_static_host[A5G_STATIC_BATCH_MAX];
+
+int a5g_step_batch_static(a5g_ctx **ctxs, int n, const double *dts) {
+  if (!ctxs || !dts || n < 1) return fail(A5G_EINVAL, "bad batch");
+  if (n > A5G_STATIC_BATCH_MAX)
+    return fail(A5G_EINVAL, "a5g_step_batch_static: n = " + std::to_string(n) +
+                                " exceeds A5G_STATIC_BATCH_MAX (" +
+                                std::to_string(A5G_STATIC_BATCH_MAX) + ")");
+  int dev = -1;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 256) return fail(A5G_EINVAL, "device ordinal out of range");
+  for (int k = 0; k < n; k++) {
+    if (!ctxs[k] || !ctxs[k]->has_tree || !ctxs[k]->has_table)
+      return fail(A5G_ESTATE, "batch member without tree or table");
+    if (!(dts[k] > 0)) return fail(A5G_EINVAL, "dt must be > 0");
+    cudaPointerAttributes at{};
+    CK(cudaPointerGetAttributes(&at, ctxs[k]->d_run));
+    if (at.device != dev)
+      return fail(A5G_EINVAL, "a5g_step_batch_static: context on another device than the current one");
+  }
+  std::lock_guard<std::mutex> lock(g_static_mu);
+  if (!g_static_dev[dev]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_batch_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(A5G_ECUDA, std::string("cudaGetSymbolAddress(g_batch_scratch): ") +
+                                 cudaGetErrorString(e));
+    g_static_dev[dev] = static_cast<BatchSlot *>(p);
+  }
+  a5g_ctx *c0 = ctxs[0];
+  for (int k = 1; k < n; k++) CK(cudaStreamSynchronize(ctxs[k]->stream));
+  for (int k = 0; k < n; k++) {
+    g_static_host[k].run = ctxs[k]->d_run;
+    g_static_host[k].op = mkop(OP_STEP, 0, 0, dts[k]);
+  }
+  // pageable source: the copy is staged before the call returns
+  CK(cudaMemcpyAsync(g_static_dev[dev], g_static_host, (size_t)n * sizeof(BatchSlot),
+                     cudaMemcpyHostToDevice, c0->stream));
+  a5g_run_kernel_slots<<<n, NTHR, 0, c0->stream>>>(g_static_dev[dev]);
+  CK(cudaGetLastError());
   return A5G_OK;
 }
 

@@ -150,6 +150,27 @@ int a5g_step(a5g_ctx *ctx, double dt);
 /* The same step for several independent runs in one launch (one persistent
  * thread block per run). dts[k] is the step of run k. */
 int a5g_step_batch(a5g_ctx **ctxs, int n, const double *dts);
+/* Batched step that allocates no device memory. Same result as
+ * a5g_step_batch; no counterpart in the reference (its Fortran host has no
+ * device at all).
+ *
+ * Some callers cannot allocate device memory while they step: a host that
+ * fixed its device-memory budget before the time loop, or one whose stepping
+ * path must not block on the allocator (cudaMallocAsync may wait on the
+ * memory pool). This entry point keeps the per-run descriptor table of the
+ * launch in a fixed file-scope device array of A5G_STATIC_BATCH_MAX entries
+ * (40 KiB), held by every GPU that loads the library until the process
+ * exits, and calls no allocating routine. The caller still creates the
+ * contexts (which own the inputs and outputs) beforehand.
+ *  - n above A5G_STATIC_BATCH_MAX is rejected with A5G_EINVAL;
+ *  - all contexts must belong to the current device;
+ *  - the first call on a device looks up the array's device address
+ *    (cudaGetSymbolAddress) with that device current; make that first call
+ *    before any stream capture;
+ *  - every call shares the one array: calls that overlap on the GPU (on
+ *    different streams) race; calls queued on one stream are ordered. */
+#define A5G_STATIC_BATCH_MAX 1024
+int a5g_step_batch_static(a5g_ctx **ctxs, int n, const double *dts);
 /* Wait for all work queued on the context's stream. */
 int a5g_sync(a5g_ctx *ctx);
 /* The cudaStream_t (as void*) all work of this context is queued on, so a
