@@ -206,7 +206,7 @@ def run_b200(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
 
-    from a5_streamer_b200 import build, metrics, streamer
+    from a5_streamer_b200 import build, metrics, replicas, streamer
     from a5_streamer_b200 import device as dv
     build.build()  # no-op when the in-tree library is current
 
@@ -243,12 +243,8 @@ def run_b200(args):
         run.sync()
         torch.cuda.synchronize()
     step_ms = [a.elapsed_time(b) for a, b in zip(e0, e1)]
-    total_s = sum(step_ms) / 1e3
-    if dist:
-        t = torch.tensor([total_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_s = float(t.item())
-    value = n_leaf * K * world / total_s
+    total_s = replicas.max_over_ranks(sum(step_ms) / 1e3, device="cuda")
+    value = replicas.replica_throughput(n_leaf * K * world, total_s)
     ms_per_step = 1e3 * total_s / K
 
     # end to end through the public API: dt computed from device reductions
@@ -261,12 +257,8 @@ def run_b200(args):
         d = run.get_max_dt()
         run.step(d)
     run.sync()
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = {"value": n_leaf * K * world / e2e_s, "unit": UNIT,
+    e2e_s = replicas.max_over_ranks(time.perf_counter() - t0, device="cuda")
+    e2e = {"value": replicas.replica_throughput(n_leaf * K * world, e2e_s), "unit": UNIT,
            "h2d_bytes_per_step": 8, "d2h_bytes_per_step": 24}
 
     # batched extra: B replicas of the same mesh and state, one block each

@@ -1,0 +1,63 @@
+"""The reference's text configuration format (fosito/m_config.f90) and the
+two workload presets."""
+import math
+
+import pytest
+
+from a5_streamer_b200 import config
+
+SAMPLE = """
+ # The desired endtime in seconds of the simulation:
+ end_time = 0.1500E-07
+ box_size = 8
+ domain_len = 0.3200E-01
+ applied_fld = 0.2500E+07   # trailing comment
+ bg_dens = 0.1000E+14
+ seed_dens = 0.2000E+20
+ seed_rel_r0 = 0.5000E+00 0.6000E+00
+ seed_rel_r1 = 0.5000E+00 0.5000E+00
+ seed_width = 0.2000E-03
+ seed_falloff = 3
+ dt_max = 0.1000E-09
+ num_steps_amr = 2
+ photoi_enabled = F
+ lkptbl_size = 1000
+"""
+
+
+def test_parse_and_apply(tmp_path):
+    p = tmp_path / "a.txt"
+    p.write_text(SAMPLE)
+    q = tmp_path / "b.txt"
+    q.write_text("applied_fld = 3.0e6\nn_base = 1 1\n")
+    cfg = config.load_cfg_files([str(p), str(q)], base=config.cartesian_8mm())
+    assert cfg.end_time == 1.5e-8 and cfg.applied_fld == 3.0e6  # later file wins
+    assert cfg.domain_len == (0.032, 0.032) and cfg.n_base == (1, 1)
+    assert cfg.dr_base == 0.032 / 8
+    assert len(cfg.seeds) == 1
+    s = cfg.seeds[0]
+    assert s.r0 == (0.016, 0.032 * 0.6) and s.r1 == (0.016, 0.016) and s.falloff == 3
+    assert cfg.lkptbl_size == 1000 and not cfg.photoi_enabled
+    cfg.validate()
+
+
+def test_presets():
+    c = config.cartesian_8mm()
+    c.validate()
+    assert c.dr_base == 2.5e-4 and c.dr_at(7) == 2.5e-4 / 64
+    assert c.applied_voltage == -0.008 * 2.5e6
+    assert c.n_cycle_base == 8 and c.crv_refine == 1.0
+    assert math.isclose(c.seeds[0].width, math.sqrt(2) * 0.2e-3)
+    y = config.cylindrical_16mm()
+    y.validate()
+    assert y.is_cyl and y.n_cycle_base == 4 and y.crv_refine == 0.0
+    assert y.dr_base == 1e-3 and y.dr_at(10) < 2e-6
+    xs = config.table_nodes(200, 3e7)
+    assert xs[0] == 0.0 and xs[-1] == (199) * (1 / (199 / 3e7))
+
+
+def test_validate_rejects():
+    with pytest.raises(ValueError):
+        config.cartesian_8mm(box_size=6).validate()
+    with pytest.raises(ValueError):
+        config.cartesian_8mm(domain_len=(8e-3, 9e-3)).validate()
