@@ -59,6 +59,27 @@ struct BoxMeta {
 };
 static_assert(sizeof(BoxMeta) == 96, "BoxMeta layout");
 
+// Plan records, built on the host once per topology (build_plans).
+// CellRec: one interior cell: global index g (slot * SLOT + local), the four
+// neighbour codes (lx, hx, ly, hy; see NBK_*), the three parent cells of the
+// multigrid correction, the global i index (cylindrical weights), flags and
+// the level index.
+struct __align__(16) CellRec { int g, nb[4], pc[3], gi, flags, li, pad; };
+// GhostRec: one side-ghost cell: destination, kind (GK_*), sources.
+struct GhostRec { int dst, kind, s[4]; };
+// RstRec: one parent cell of a restriction: destination, first fine source,
+// cylindrical weight.
+struct RstRec { int dst, src; double rfac; };
+// FrRec: one parent cell of the multigrid residual restriction: destination
+// and the four fine cells (indices into the cell table).
+struct __align__(16) FrRec { int dst, c[4], pad[3]; };
+enum { NBK_DIRECT = 0, NBK_NEG = 1, NBK_APPLIED = 2, NBK_RECIPE = 3 };
+enum { GK_COPY = 0, GK_NEG = 1, GK_APPLIED = 2, GK_RB = 3, GK_INTERP = 4 };
+constexpr int GK_PARENT = 0x100;  // ghost of a box that has children
+constexpr int CF_LEAF = 1;
+constexpr int NB_MASK = 0x0FFFFFFF;
+static_assert(sizeof(CellRec) == 48 && sizeof(FrRec) == 32, "plan layout");
+
 struct RunDev {
   int capacity, min_lvl, max_lvl, lvls_max;
   int coord, n_cycle_base, nlev, pad0;
@@ -75,6 +96,17 @@ struct RunDev {
   double ref_init_time, crv_refine;
   int n_seeds, pad2;
   double seed_r0[8][2], seed_r1[8][2], seed_width[8];
+  // plans, per level index
+  int cell_off[MAXLEV + 1], cell_split[MAXLEV];
+  int gphi_off[MAXLEV + 1], gden_off[MAXLEV + 1];
+  int rst_off[MAXLEV + 1], fr_off[MAXLEV + 1], pcell_off[MAXLEV + 1];
+  int lv_nc[MAXLEV], pad3;
+  double lv_dr[MAXLEV];
+  const CellRec *cells;
+  const GhostRec *gphi, *gden;
+  const RstRec *rst;
+  const FrRec *fr;
+  const int *pcells;
   double *scal;                // dt reductions out
   int *flags;                  // refinement flags out
   int *status;
@@ -306,19 +338,6 @@ __device__ __forceinline__ void gc_box(const RunDev &R, int id, int t, int iv, i
   }
 }
 
-// a$D_gc_tree for one or two variables, level by level (m_aX_gc.f90:28-46)
-__device__ void gc_tree(const RunDev &R, int iv0, int iv1, int kind) {
-  for (int lvl = R.min_lvl; lvl <= R.max_lvl; lvl++) {
-    int n = list_n(R, 0, lvl);
-    const int *ids = list_p(R, 0, lvl);
-    box_loop(ids, n, [&](int id, int t) {
-      gc_box(R, id, t, iv0, kind);
-      if (iv1 >= 0) gc_box(R, id, t, iv1, kind);
-    });
-    __syncthreads();
-  }
-}
-
 // Second ghost layer, afivo/src/m_aX_gc.f90:407-622 (gc2_box with
 // gc2_prolong1 on refinement boundaries and gc2_neumann on physical ones)
 __device__ double gc2_value(const RunDev &R, const BoxMeta &m, int id, int iv, int nb, int k) {
@@ -492,369 +511,398 @@ __device__ void update_solution(const RunDev &R, double dt) {
   });
 }
 
-// a$D_restrict_tree for one or two variables, afivo/src/m_aX_restrict.f90:54-142
-// (cylindrical weights :95-113, radius evaluated at the child-local index).
-__device__ void restrict_tree(const RunDev &R, int iv0, int iv1) {
-  const bool cyl = R.coord == 1;
-  for (int lvl = R.max_lvl - 1; lvl >= R.min_lvl; lvl--) {
-    box_loop(list_p(R, 2, lvl), list_n(R, 2, lvl), [&](int id, int t) {
-      const BoxMeta &pm = R.meta[id];
-      const int ncp = pm.nc;
-      if (t >= ncp * ncp) return;
-      const int ic = t % ncp + 1, jc = t / ncp + 1;
-      for (int q = 0; q < 4; q++) {
-        int cid = pm.ch[q];
-        if (cid == 0) continue;
-        const BoxMeta &cm = R.meta[cid];
-        int o0, o1;
-        child_offset(cm, -1, o0, o1);
-        const int hnc = cm.nc >> 1;
-        const int i = ic - o0, j = jc - o1;
-        if (i < 1 || i > hnc || j < 1 || j > hnc) continue;
-        const int cg = cm.nc + 2, i_f = 2 * i - 1, j_f = 2 * j - 1;
-        for (int w = 0; w < 2; w++) {
-          int iv = w == 0 ? iv0 : iv1;
-          if (iv < 0) continue;
-          const double *cc = CC(R, iv, cid);
-          double a = cc[i_f + cg * j_f], b = cc[(i_f + 1) + cg * j_f];
-          double c = cc[i_f + cg * (j_f + 1)], d = cc[(i_f + 1) + cg * (j_f + 1)];
-          double v;
-          if (cyl) {
-            double dr16 = 0.0625 * pm.dr;
-            double r = pm.r0 + (i - 0.5) * pm.dr;
-            double rfac = dr16 / r;
-            v = (0.25 - rfac) * (a + c) + (0.25 + rfac) * (b + d);
-          } else {
-            v = 0.25 * (a + b + c + d);
-          }
-          CC(R, iv, id)[ic + (ncp + 2) * jc] = v;
-        }
-      }
-    });
-    __syncthreads();
-  }
-}
-
-// ---------------------------------------------------------------------------
-// Multigrid, afivo/src/m_aX_mg.f90 (normal boxes: Laplacian or cylindrical
-// Laplacian; eps == 1 everywhere). i_phi = 4, i_tmp = 5 (the |E| variable,
-// src/streamer_2d.f90:37-40), i_rhs = 6.
 constexpr int MP = I_PHI, MT = I_FLD, MR = I_RHS;
 
-// box_lpl (m_aX_mg.f90:662-680) / box_clpl (:1027-1049) at interior cell c
-__device__ __forceinline__ double box_op_at(const double *phi, int i, int j, int nc, int ix0,
-                                            double dr, bool cyl) {
-  const int ncg = nc + 2, c = i + ncg * j;
-  double inv_dr_sq = 1 / (dr * dr);
-  if (cyl) {
-    int ioff = (ix0 - 1) * nc;
-    double den = i + ioff - 0.5;
-    double rf1 = (i + ioff - 1) / den, rf2 = (i + ioff) / den;
-    return (rf1 * phi[c - 1] + rf2 * phi[c + 1] + phi[c - ncg] + phi[c + ncg] - 4 * phi[c]) *
-           inv_dr_sq;
-  }
-  return inv_dr_sq * (phi[c - 1] + phi[c + 1] + phi[c - ncg] + phi[c + ncg] - 4 * phi[c]);
+// ---------------------------------------------------------------------------
+// Plan-based operations. The host resolves, once per topology, every index
+// the per-level phases need (see build_plans): a table of interior cells per
+// level ordered by red/black colour, with the four neighbours of each cell
+// encoded as a direct index, a negated index (grounded wall), an
+// applied-voltage index, or a ghost recipe; ghost recipes per level for the
+// potential (copy / mg$D_sides_rb / sides_bc_pot) and for the densities and
+// |E| (copy / a$D_gc_interp(_lim) / Neumann); restriction records; and
+// residual-restriction records. A phase is then a flat loop of all threads
+// over one of these lists.
+
+__device__ __forceinline__ double *VAR(const RunDev &R, int v) {
+  return R.cc + (size_t)v * R.capacity * SLOT;
 }
 
-// fill_gc_phi over the boxes of one level (m_aX_mg.f90:303-316)
-__device__ __forceinline__ void fill_gc_phi(const RunDev &R, int lvl) {
-  box_loop(list_p(R, 0, lvl), list_n(R, 0, lvl),
-           [&](int id, int t) { gc_box(R, id, t, MP, GC_PHI); });
+// Ghost of the potential from its recipe
+__device__ __forceinline__ double recipe_phi(const RunDev &R, const double *phi,
+                                             const GhostRec &r) {
+  switch (r.kind & 0xff) {
+    case GK_COPY: return phi[r.s[0]];
+    case GK_NEG: return -phi[r.s[0]];
+    case GK_APPLIED: return 2 * R.applied_voltage - phi[r.s[0]];
+    default:  // mg$D_sides_rb, m_aX_mg.f90:283-298
+      return 0.5 * phi[r.s[0]] + phi[r.s[1]] - 0.25 * (phi[r.s[2]] + phi[r.s[3]]);
+  }
+}
+
+// Neighbour value of the potential from a cell's neighbour code
+__device__ __forceinline__ double nbv(const RunDev &R, const double *phi, int code,
+                                      const GhostRec *gl) {
+  const int idx = code & NB_MASK;
+  switch ((unsigned)code >> 28) {
+    case NBK_DIRECT: return phi[idx];
+    case NBK_NEG: return -phi[idx];
+    case NBK_APPLIED: return 2 * R.applied_voltage - phi[idx];
+    default: return recipe_phi(R, phi, gl[idx]);
+  }
+}
+
+// box_lpl (m_aX_mg.f90:662-680) / box_clpl (:1027-1049) at one cell
+__device__ __forceinline__ double lap_at(const RunDev &R, const double *phi, const CellRec &c,
+                                         const GhostRec *gl, double inv_dr_sq) {
+  const double lx = nbv(R, phi, c.nb[0], gl), hx = nbv(R, phi, c.nb[1], gl);
+  const double ly = nbv(R, phi, c.nb[2], gl), hy = nbv(R, phi, c.nb[3], gl);
+  const double v = phi[c.g];
+  if (R.coord == 1) {
+    const double den = c.gi - 0.5;
+    const double rf1 = (c.gi - 1) / den, rf2 = c.gi / den;
+    return (rf1 * lx + rf2 * hx + ly + hy - 4 * v) * inv_dr_sq;
+  }
+  return inv_dr_sq * (lx + hx + ly + hy - 4 * v);
+}
+
+// Red-black Gauss-Seidel half-sweep `it` on level lvl (box_gsrb_lpl,
+// m_aX_mg.f90:636-659; box_gsrb_clpl :998-1024). Ghost neighbours are taken
+// from their recipes, which equals the ghost fill the reference performs
+// after every half-sweep (gsrb_boxes, :343-366): the recipes read only cells
+// of the colour not updated in this half-sweep, the updated cell itself
+// (read before it is written), or coarser-level cells. mem: read ghosts from
+// memory instead (the first half-sweep of a first FMG call, where the
+// reference's ghosts are not yet consistent with the interior).
+__device__ void p_sweep(const RunDev &R, int lvl, int it, bool mem) {
+  const int li = lvl - R.min_lvl;
+  const bool odd = it & 1;
+  const int a = odd ? R.cell_split[li] : R.cell_off[li];
+  const int b = odd ? R.cell_off[li + 1] : R.cell_split[li];
+  double *phi = VAR(R, MP);
+  const double *rhs = VAR(R, MR);
+  const GhostRec *gl = R.gphi + R.gphi_off[li];
+  const double dr = R.lv_dr[li], dx2 = dr * dr;
+  const int ncg = R.lv_nc[li] + 2;
+  const bool cyl = R.coord == 1;
+  for (int k = a + threadIdx.x; k < b; k += NTHR) {
+    const CellRec c = R.cells[k];
+    double lx, hx, ly, hy;
+    if (mem) {
+      lx = phi[c.g - 1]; hx = phi[c.g + 1]; ly = phi[c.g - ncg]; hy = phi[c.g + ncg];
+    } else {
+      lx = nbv(R, phi, c.nb[0], gl); hx = nbv(R, phi, c.nb[1], gl);
+      ly = nbv(R, phi, c.nb[2], gl); hy = nbv(R, phi, c.nb[3], gl);
+    }
+    const double r = rhs[c.g];
+    if (cyl) {
+      const double den = c.gi - 0.5;
+      const double rf1 = (c.gi - 1) / den, rf2 = c.gi / den;
+      phi[c.g] = 0.25 * (rf1 * lx + rf2 * hx + hy + ly - dx2 * r);
+    } else {
+      phi[c.g] = 0.25 * (hx + lx + hy + ly - dx2 * r);
+    }
+  }
   __syncthreads();
 }
 
-// gsrb_boxes (m_aX_mg.f90:343-366) with box_gsrb_lpl (:636-659) / _clpl (:998-1024)
-__device__ void gsrb_level(const RunDev &R, int lvl, int n_cycle) {
-  const bool cyl = R.coord == 1;
-  const int *ids = list_p(R, 0, lvl);
-  const int n = list_n(R, 0, lvl);
-  for (int it = 1; it <= 2 * n_cycle; it++) {
-    box_loop(ids, n, [&](int id, int t) {
-      const BoxMeta &m = R.meta[id];
-      const int nc = m.nc, ncg = nc + 2;
-      if (t >= nc * nc) return;
-      const int i = t % nc + 1, j = t / nc + 1;
-      if (((i + j + it) & 1) != 0) return;
-      double *phi = CC(R, MP, id);
-      const double rhs = CC(R, MR, id)[i + ncg * j];
-      const double dx2 = m.dr * m.dr;
-      const int c = i + ncg * j;
-      if (cyl) {
-        int ioff = (m.ix0 - 1) * nc;
-        double den = i + ioff - 0.5;
-        double rf1 = (i + ioff - 1) / den, rf2 = (i + ioff) / den;
-        phi[c] = 0.25 * (rf1 * phi[c - 1] + rf2 * phi[c + 1] + phi[c + ncg] + phi[c - ncg] -
-                         dx2 * rhs);
+// Ghost fill of the potential on level index li (fill_gc_phi, :303-316), no
+// barrier. copy_tmp: also tmp = phi on the ghosts of parent boxes (the
+// whole-box copy of update_coarse, :407).
+__device__ __forceinline__ void fill_phi_loop(const RunDev &R, int li, bool copy_tmp) {
+  const GhostRec *gl = R.gphi + R.gphi_off[li];
+  const int n = R.gphi_off[li + 1] - R.gphi_off[li];
+  double *phi = VAR(R, MP), *tmp = VAR(R, MT);
+  for (int k = threadIdx.x; k < n; k += NTHR) {
+    const GhostRec r = gl[k];
+    const double v = recipe_phi(R, phi, r);
+    phi[r.dst] = v;
+    if (copy_tmp && (r.kind & GK_PARENT)) tmp[r.dst] = v;
+  }
+}
+__device__ void p_fill(const RunDev &R, int lvl) {
+  fill_phi_loop(R, lvl - R.min_lvl, false);
+  __syncthreads();
+}
+
+// For every box of level lvl: the residual rhs - A phi (residual_box,
+// :475-484) restricted into the parent's tmp and phi restricted into the
+// parent's phi (box_rstr_lpl, :683-705); the ghosts of level lvl are filled in
+// the same phase (the residual takes ghost neighbours from the recipes).
+// leaf_rhs: first set the space charge e/eps0 (n_e - n_i) on leaf cells
+// (src/streamer_2d.f90:317-329). store_res: keep the residual in the box's
+// own tmp (set_coarse_phi_rhs); otherwise tmp is left as it was
+// (update_coarse saves and restores it).
+__device__ void p_fr(const RunDev &R, int lvl, bool fill, bool leaf_rhs, bool store_res) {
+  const int li = lvl - R.min_lvl;
+  const FrRec *fr = R.fr + R.fr_off[li];
+  const int n = R.fr_off[li + 1] - R.fr_off[li];
+  double *phi = VAR(R, MP), *tmp = VAR(R, MT), *rhs = VAR(R, MR);
+  const double *e = VAR(R, I_ELEC), *pi = VAR(R, I_PION);
+  const GhostRec *gl = R.gphi + R.gphi_off[li];
+  const double dr = R.lv_dr[li], inv_dr_sq = 1 / (dr * dr);
+  const double fac = UC_ELEM_CHARGE / UC_EPS0;
+  for (int k = threadIdx.x; k < n; k += NTHR) {
+    const FrRec rec = fr[k];
+    double rs[4], ps[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const CellRec c = R.cells[rec.c[q]];
+      double rh;
+      if (leaf_rhs && (c.flags & CF_LEAF)) {
+        rh = fac * (e[c.g] - pi[c.g]);
+        rhs[c.g] = rh;
       } else {
-        phi[c] = 0.25 * (phi[c + 1] + phi[c - 1] + phi[c + ncg] + phi[c - ncg] - dx2 * rhs);
+        rh = rhs[c.g];
       }
-    });
-    __syncthreads();
-    fill_gc_phi(R, lvl);
+      const double res = rh - lap_at(R, phi, c, gl, inv_dr_sq);
+      if (store_res) tmp[c.g] = res;
+      rs[q] = res;
+      ps[q] = phi[c.g];
+    }
+    tmp[rec.dst] = 0.25 * (rs[0] + rs[1] + rs[2] + rs[3]);
+    phi[rec.dst] = 0.25 * (ps[0] + ps[1] + ps[2] + ps[3]);
   }
+  if (fill) fill_phi_loop(R, li, false);
+  __syncthreads();
 }
 
-// Residual of box id at fine cell (i, j): rhs - A phi (residual_box, :475-484)
-__device__ __forceinline__ double residual_at(const RunDev &R, const BoxMeta &m, int id, int i,
-                                              int j, bool cyl) {
-  const double *phi = CC(R, MP, id);
-  double a = box_op_at(phi, i, j, m.nc, m.ix0, m.dr, cyl);
-  return CC(R, MR, id)[i + (m.nc + 2) * j] - a;
+// Ghost fill of level lvl and the coarse right-hand side of its parent
+// boxes: rhs = A phi + tmp (box_op then a$D_box_add_cc, :399-402 / :441-444);
+// copy_tmp: then tmp = phi (a$D_box_copy_cc, :403).
+__device__ void p_fc(const RunDev &R, int lvl, bool copy_tmp) {
+  const int li = lvl - R.min_lvl;
+  const int *pc = R.pcells + R.pcell_off[li];
+  const int n = R.pcell_off[li + 1] - R.pcell_off[li];
+  double *phi = VAR(R, MP), *tmp = VAR(R, MT), *rhs = VAR(R, MR);
+  const GhostRec *gl = R.gphi + R.gphi_off[li];
+  const double dr = R.lv_dr[li], inv_dr_sq = 1 / (dr * dr);
+  for (int k = threadIdx.x; k < n; k += NTHR) {
+    const CellRec c = R.cells[pc[k]];
+    const double a = lap_at(R, phi, c, gl, inv_dr_sq);
+    rhs[c.g] = a + tmp[c.g];
+    if (copy_tmp) tmp[c.g] = phi[c.g];
+  }
+  fill_phi_loop(R, li, copy_tmp);
+  __syncthreads();
 }
 
-// For each box of level lvl: residual into the parent's tmp and phi into the
-// parent's phi (box_rstr_lpl, :683-705). store_res: also keep the residual in
-// the box's own tmp (set_coarse_phi_rhs); otherwise the box's tmp is left as
-// it was (update_coarse saves and restores it).
-__device__ void residual_restrict(const RunDev &R, int lvl, bool store_res) {
-  const bool cyl = R.coord == 1;
-  box_loop(list_p(R, 0, lvl), list_n(R, 0, lvl), [&](int id, int t) {
-    const BoxMeta &m = R.meta[id];
-    const int nc = m.nc, ncg = nc + 2, hnc = nc >> 1;
-    if (store_res && t < nc * nc) {
-      int i = t % nc + 1, j = t / nc + 1;
-      CC(R, MT, id)[i + ncg * j] = residual_at(R, m, id, i, j, cyl);
+// Boxes of level lvl: copy: tmp = phi (a$D_boxes_copy_cc in mg$D_fas_fmg,
+// :187-188); correct: phi += prolongation of the parent's correction
+// (correct_children :319-341 with box_corr_lpl :605-633). The correction
+// phi_p - tmp_p is formed where it is used instead of being stored back into
+// the parent's tmp; that stored value is never read again by the reference.
+__device__ void p_correct(const RunDev &R, int lvl, bool copy, bool correct) {
+  const int li = lvl - R.min_lvl;
+  const int a = R.cell_off[li], b = R.cell_off[li + 1];
+  double *phi = VAR(R, MP), *tmp = VAR(R, MT);
+  for (int k = a + threadIdx.x; k < b; k += NTHR) {
+    const CellRec c = R.cells[k];
+    const double v = phi[c.g];
+    if (copy) tmp[c.g] = v;
+    if (correct) {
+      const double c1 = phi[c.pc[0]] - tmp[c.pc[0]];
+      const double c2x = phi[c.pc[1]] - tmp[c.pc[1]];
+      const double c2y = phi[c.pc[2]] - tmp[c.pc[2]];
+      phi[c.g] = v + 0.5 * c1 + 0.25 * (c2x + c2y);
     }
-    if (t < hnc * hnc) {
-      int ii = t % hnc + 1, jj = t / hnc + 1;
-      int o0, o1;
-      child_offset(m, -1, o0, o1);
-      int i_c = o0 + ii, j_c = o1 + jj, i_f = 2 * ii - 1, j_f = 2 * jj - 1;
-      const BoxMeta &pm = R.meta[m.parent];
-      const int pc = i_c + (pm.nc + 2) * j_c;
-      double r00 = residual_at(R, m, id, i_f, j_f, cyl);
-      double r10 = residual_at(R, m, id, i_f + 1, j_f, cyl);
-      double r01 = residual_at(R, m, id, i_f, j_f + 1, cyl);
-      double r11 = residual_at(R, m, id, i_f + 1, j_f + 1, cyl);
-      CC(R, MT, m.parent)[pc] = 0.25 * (r00 + r10 + r01 + r11);
-      const double *phi = CC(R, MP, id);
-      CC(R, MP, m.parent)[pc] =
-          0.25 * (phi[i_f + ncg * j_f] + phi[(i_f + 1) + ncg * j_f] +
-                  phi[i_f + ncg * (j_f + 1)] + phi[(i_f + 1) + ncg * (j_f + 1)]);
+  }
+  if (copy) {
+    const GhostRec *gl = R.gphi + R.gphi_off[li];
+    const int n = R.gphi_off[li + 1] - R.gphi_off[li];
+    for (int k = threadIdx.x; k < n; k += NTHR) {
+      const int d = gl[k].dst;
+      tmp[d] = phi[d];
     }
-  });
+  }
   __syncthreads();
 }
 
-// For parents of level lvl: rhs = A phi (interior); rhs += tmp (whole box);
-// optionally tmp = phi (whole box). update_coarse :395-409 /
-// set_coarse_phi_rhs :439-446.
-__device__ void coarse_rhs(const RunDev &R, int lvl, bool copy_phi_tmp) {
-  const bool cyl = R.coord == 1;
-  box_loop(list_p(R, 2, lvl), list_n(R, 2, lvl), [&](int id, int t) {
-    const BoxMeta &m = R.meta[id];
-    const int nc = m.nc, ncg = nc + 2;
-    const double *phi = CC(R, MP, id);
-    double *rhs = CC(R, MR, id), *tmp = CC(R, MT, id);
-    for (int c = t; c < ncg * ncg; c += GT) {
-      int i = c % ncg, j = c / ncg;
-      double r = rhs[c];
-      if (i >= 1 && i <= nc && j >= 1 && j <= nc) r = box_op_at(phi, i, j, nc, m.ix0, m.dr, cyl);
-      rhs[c] = r + tmp[c];
-      if (copy_phi_tmp) tmp[c] = phi[c];
-    }
-  });
-  __syncthreads();
-}
-
-// update_coarse, m_aX_mg.f90:370-410
-__device__ void update_coarse(const RunDev &R, int lvl) {
-  residual_restrict(R, lvl, false);
-  fill_gc_phi(R, lvl - 1);
-  coarse_rhs(R, lvl - 1, true);
-}
-
-// set_coarse_phi_rhs, m_aX_mg.f90:414-447
-__device__ void set_coarse_phi_rhs(const RunDev &R, int lvl) {
-  if (lvl == R.max_lvl) fill_gc_phi(R, lvl);
-  residual_restrict(R, lvl, true);
-  fill_gc_phi(R, lvl - 1);
-  coarse_rhs(R, lvl - 1, false);
-}
-
-// correct_children for the parents of level lvl-1 (m_aX_mg.f90:319-341) with
-// box_corr_lpl (:605-633): tmp = phi - tmp on the parents (whole box), then
-// phi += prolongation of tmp on their children (all boxes of level lvl).
-__device__ void correct_children(const RunDev &R, int lvl) {
-  box_loop(list_p(R, 2, lvl - 1), list_n(R, 2, lvl - 1), [&](int id, int t) {
-    const int ncg = R.meta[id].nc + 2;
-    const double *phi = CC(R, MP, id);
-    double *tmp = CC(R, MT, id);
-    for (int c = t; c < ncg * ncg; c += GT) tmp[c] = phi[c] - tmp[c];
-  });
-  __syncthreads();
-  box_loop(list_p(R, 0, lvl), list_n(R, 0, lvl), [&](int id, int t) {
-    const BoxMeta &m = R.meta[id];
-    const int nc = m.nc, ncg = nc + 2;
-    if (t >= nc * nc) return;
-    const int i = t % nc + 1, j = t / nc + 1;
-    int o0, o1;
-    child_offset(m, -1, o0, o1);
-    const double *pt = CC(R, MT, m.parent);
-    const int pg = R.meta[m.parent].nc + 2;
-    int j_c1 = o1 + ((j + 1) >> 1), j_c2 = j_c1 + 1 - 2 * (j & 1);
-    int i_c1 = o0 + ((i + 1) >> 1), i_c2 = i_c1 + 1 - 2 * (i & 1);
-    double *phi = CC(R, MP, id);
-    const int c = i + ncg * j;
-    phi[c] = phi[c] + 0.5 * pt[i_c1 + pg * j_c1] +
-             0.25 * (pt[i_c2 + pg * j_c1] + pt[i_c1 + pg * j_c2]);
-  });
-  __syncthreads();
-}
-
-// Whole-box copy of phi to tmp for the boxes of one level (a$D_boxes_copy_cc)
-__device__ void copy_phi_tmp(const RunDev &R, int lvl) {
-  box_loop(list_p(R, 0, lvl), list_n(R, 0, lvl), [&](int id, int t) {
-    const int ncg = R.meta[id].nc + 2;
-    const double *phi = CC(R, MP, id);
-    double *tmp = CC(R, MT, id);
-    for (int c = t; c < ncg * ncg; c += GT) tmp[c] = phi[c];
-  });
-  __syncthreads();
-}
-
-// init_phi_rhs, m_aX_mg.f90:450-473
-__device__ void init_phi_rhs(const RunDev &R) {
-  for (int lvl = R.max_lvl; lvl >= R.min_lvl + 1; lvl--) {
-    box_loop(list_p(R, 0, lvl), list_n(R, 0, lvl), [&](int id, int t) {
-      const BoxMeta &m = R.meta[id];
-      const int nc = m.nc, ncg = nc + 2, hnc = nc >> 1;
-      double *phi = CC(R, MP, id);
-      for (int c = t; c < ncg * ncg; c += GT) phi[c] = 0.0;
-      if (t < hnc * hnc) {
-        int ii = t % hnc + 1, jj = t / hnc + 1;
-        int o0, o1;
-        child_offset(m, -1, o0, o1);
-        int i_f = 2 * ii - 1, j_f = 2 * jj - 1;
-        const double *rhs = CC(R, MR, id);
-        const BoxMeta &pm = R.meta[m.parent];
-        CC(R, MR, m.parent)[(o0 + ii) + (pm.nc + 2) * (o1 + jj)] =
-            0.25 * (rhs[i_f + ncg * j_f] + rhs[(i_f + 1) + ncg * j_f] +
-                    rhs[i_f + ncg * (j_f + 1)] + rhs[(i_f + 1) + ncg * (j_f + 1)]);
+// init_phi_rhs for one level (m_aX_mg.f90:450-473): phi = 0 on the boxes of
+// level lvl and their rhs restricted to the parents.
+__device__ void p_init_level(const RunDev &R, int lvl, bool leaf_rhs) {
+  const int li = lvl - R.min_lvl;
+  const FrRec *fr = R.fr + R.fr_off[li];
+  const int n = R.fr_off[li + 1] - R.fr_off[li];
+  double *rhs = VAR(R, MR), *phi = VAR(R, MP);
+  const double *e = VAR(R, I_ELEC), *pi = VAR(R, I_PION);
+  const double fac = UC_ELEM_CHARGE / UC_EPS0;
+  for (int k = threadIdx.x; k < n; k += NTHR) {
+    const FrRec rec = fr[k];
+    double rs[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const CellRec c = R.cells[rec.c[q]];
+      if (leaf_rhs && (c.flags & CF_LEAF)) {
+        rs[q] = fac * (e[c.g] - pi[c.g]);
+        rhs[c.g] = rs[q];
+      } else {
+        rs[q] = rhs[c.g];
       }
-    });
-    __syncthreads();
+    }
+    rhs[rec.dst] = 0.25 * (rs[0] + rs[1] + rs[2] + rs[3]);
   }
+  const int nb = list_n(R, 0, lvl);
+  const int *ids = list_p(R, 0, lvl);
+  const int cg = R.lv_nc[li] + 2, per = cg * cg;
+  for (int k = threadIdx.x; k < nb * per; k += NTHR) phi[(size_t)ids[k / per] * SLOT + k % per] = 0.0;
+  __syncthreads();
 }
 
-// mg$D_fas_vcycle, m_aX_mg.f90:208-254 (set_residual = false)
-__device__ void fas_vcycle(const RunDev &R, int max_lvl, int n_cycle_base) {
+// Residual rhs - A phi on every cell of levels min..max (set_residual of
+// mg$D_fas_vcycle, :243-253)
+__device__ void p_residual_all(const RunDev &R, int max_lvl) {
+  double *phi = VAR(R, MP), *tmp = VAR(R, MT);
+  const double *rhs = VAR(R, MR);
+  for (int lvl = R.min_lvl; lvl <= max_lvl; lvl++) {
+    const int li = lvl - R.min_lvl;
+    const GhostRec *gl = R.gphi + R.gphi_off[li];
+    const double dr = R.lv_dr[li], inv_dr_sq = 1 / (dr * dr);
+    for (int k = R.cell_off[li] + threadIdx.x; k < R.cell_off[li + 1]; k += NTHR) {
+      const CellRec c = R.cells[k];
+      tmp[c.g] = rhs[c.g] - lap_at(R, phi, c, gl, inv_dr_sq);
+    }
+  }
+  __syncthreads();
+}
+
+// mg$D_fas_vcycle (m_aX_mg.f90:208-254), set_residual handled by the caller.
+// Phases per level: down: 4 half-sweeps, residual/restriction (+ ghost fill),
+// coarse ghost fill + rhs; base: 2 n_cycle_base half-sweeps + ghost fill;
+// up: correction, 4 half-sweeps, ghost fill.
+__device__ void p_vcycle(const RunDev &R, int max_lvl, bool stale_base) {
   const int min_lvl = R.min_lvl;
   for (int lvl = max_lvl; lvl >= min_lvl + 1; lvl--) {
-    gsrb_level(R, lvl, 2);
-    update_coarse(R, lvl);
+    for (int it = 1; it <= 4; it++) p_sweep(R, lvl, it, false);
+    p_fr(R, lvl, true, false, false);
+    p_fc(R, lvl - 1, true);
   }
-  gsrb_level(R, min_lvl, n_cycle_base);
+  for (int it = 1; it <= 2 * R.n_cycle_base; it++) p_sweep(R, min_lvl, it, stale_base && it == 1);
+  p_fill(R, min_lvl);
   for (int lvl = min_lvl + 1; lvl <= max_lvl; lvl++) {
-    correct_children(R, lvl);
-    fill_gc_phi(R, lvl);
-    gsrb_level(R, lvl, 2);
+    p_correct(R, lvl, false, true);
+    for (int it = 1; it <= 4; it++) p_sweep(R, lvl, it, false);
+    p_fill(R, lvl);
   }
 }
 
-// Residual of every box of levels min..max into tmp (vcycle set_residual)
-__device__ void residual_all(const RunDev &R, int max_lvl) {
-  const bool cyl = R.coord == 1;
-  for (int lvl = R.min_lvl; lvl <= max_lvl; lvl++)
-    box_loop(list_p(R, 0, lvl), list_n(R, 0, lvl), [&](int id, int t) {
-      const BoxMeta &m = R.meta[id];
-      const int nc = m.nc;
-      if (t >= nc * nc) return;
-      int i = t % nc + 1, j = t / nc + 1;
-      CC(R, MT, id)[i + (nc + 2) * j] = residual_at(R, m, id, i, j, cyl);
-    });
-  __syncthreads();
-}
-
-// mg$D_fas_fmg, m_aX_mg.f90:163-202
-__device__ void fas_fmg(const RunDev &R, bool set_residual, bool first_call) {
-  const int min_lvl = R.min_lvl;
+// mg$D_fas_fmg, m_aX_mg.f90:163-202. leaf_rhs: compute the space charge of
+// the leaves where it is first needed (compute_fld).
+__device__ void p_fmg(const RunDev &R, bool set_residual, bool first_call, bool leaf_rhs) {
+  const int min_lvl = R.min_lvl, max_lvl = R.max_lvl;
   if (first_call) {
-    init_phi_rhs(R);
+    for (int lvl = max_lvl; lvl >= min_lvl + 1; lvl--) p_init_level(R, lvl, leaf_rhs);
   } else {
-    for (int lvl = R.max_lvl; lvl >= min_lvl + 1; lvl--) set_coarse_phi_rhs(R, lvl);
-  }
-  for (int lvl = min_lvl; lvl <= R.max_lvl; lvl++) {
-    copy_phi_tmp(R, lvl);
-    if (lvl > min_lvl) {
-      correct_children(R, lvl);
-      fill_gc_phi(R, lvl);
+    // set_coarse_phi_rhs for lvl = max..min+1 (:414-447)
+    for (int lvl = max_lvl; lvl >= min_lvl + 1; lvl--) {
+      p_fr(R, lvl, lvl == max_lvl, leaf_rhs, true);
+      p_fc(R, lvl - 1, false);
     }
-    fas_vcycle(R, lvl, R.n_cycle_base);
-    if (set_residual && lvl == R.max_lvl) residual_all(R, lvl);
+  }
+  for (int lvl = min_lvl; lvl <= max_lvl; lvl++) {
+    p_correct(R, lvl, true, lvl > min_lvl);
+    p_vcycle(R, lvl, first_call && lvl == min_lvl);
+    if (set_residual && lvl == max_lvl) p_residual_all(R, lvl);
   }
 }
 
-// ---------------------------------------------------------------------------
-// Field.
-
-// space charge on leaves of levels >= 1, whole boxes (src/streamer_2d.f90:317-329)
-__device__ void set_rhs(const RunDev &R) {
-  const int *ids;
-  int n;
-  list_range(R, 1, 1, R.max_lvl, ids, n);
-  const double fac = UC_ELEM_CHARGE / UC_EPS0;
-  box_loop(ids, n, [&](int id, int t) {
-    const int ncg = R.meta[id].nc + 2;
-    const double *e = CC(R, I_ELEC, id), *pi = CC(R, I_PION, id);
-    double *rhs = CC(R, I_RHS, id);
-    for (int c = t; c < ncg * ncg; c += GT) rhs[c] = fac * (e[c] - pi[c]);
-  });
-  __syncthreads();
-}
-
-// fld_from_pot on all boxes (src/streamer_2d.f90:346-381) and the |E| ghost
-// fill a$D_gc_tree(i_fld, a$D_gc_interp, a$D_gc_neumann)
-__device__ void fld_from_pot(const RunDev &R) {
-  const int *ids;
-  int n;
-  list_range(R, 0, R.min_lvl, R.max_lvl, ids, n);
-  box_loop(ids, n, [&](int id, int t) {
-    const BoxMeta &m = R.meta[id];
-    const int nc = m.nc, ncg = nc + 2, nf = (nc + 1) * nc;
-    const double inv_dr = 1 / m.dr;
-    const double *phi = CC(R, I_PHI, id), *eps = CC(R, I_EPS, id);
-    double *fxf = FX(R, F_FLD, id), *fyf = FY(R, F_FLD, id);
-    for (int f = t; f < 2 * nf; f += GT) {
-      const bool xd = f < nf;
-      const int g = xd ? f : f - nf;
-      int i, j;
-      if (xd) { i = g % (nc + 1) + 1; j = g / (nc + 1) + 1; }
-      else { i = g % nc + 1; j = g / nc + 1; }
-      const int s = xd ? 1 : ncg;
-      const int c = i + ncg * j, pos = xd ? i : j;
-      double v;
-      if (pos == 1) {
-        v = 2 * inv_dr * (phi[c - s] - phi[c]) * eps[c - s] / (eps[c] + eps[c - s]);
-      } else if (pos == nc + 1) {
-        v = 2 * inv_dr * (phi[c - s] - phi[c]) * eps[c] / (eps[c] + eps[c - s]);
-      } else {
-        v = inv_dr * (phi[c - s] - phi[c]);
+// a$D_gc_tree(iv, a$D_gc_interp[_lim], a$D_gc_neumann) for one or two
+// variables, levels ascending (m_aX_gc.f90:28-46, 90-330)
+__device__ void p_gc_den(const RunDev &R, int iv0, int iv1, bool lim) {
+  const double sixth = 1 / 6.0, third = 1 / 3.0;
+  for (int lvl = R.min_lvl; lvl <= R.max_lvl; lvl++) {
+    const int li = lvl - R.min_lvl;
+    const GhostRec *gl = R.gden + R.gden_off[li];
+    const int n = R.gden_off[li + 1] - R.gden_off[li];
+    for (int k = threadIdx.x; k < n; k += NTHR) {
+      const GhostRec r = gl[k];
+      for (int w = 0; w < 2; w++) {
+        const int iv = w == 0 ? iv0 : iv1;
+        if (iv < 0) continue;
+        double *x = VAR(R, iv);
+        double v;
+        if ((r.kind & 0xff) == GK_INTERP) {
+          const double c1 = x[r.s[0]], c2 = x[r.s[1]];
+          v = 0.5 * c1 + sixth * c2 + third * x[r.s[2]];
+          if (lim && v > 2 * c1) v = 2 * c1;
+        } else {
+          v = x[r.s[0]];
+        }
+        x[r.dst] = v;
       }
-      if (xd) fxf[fxi(i, j, nc)] = v;
-      else fyf[fyi(i, j, nc)] = v;
     }
-  });
+    __syncthreads();
+  }
+}
+
+// a$D_restrict_tree for one or two variables, levels descending
+// (afivo/src/m_aX_restrict.f90:54-142; cylindrical weights :95-113)
+__device__ void p_restrict(const RunDev &R, int iv0, int iv1) {
+  const bool cyl = R.coord == 1;
+  for (int lvl = R.max_lvl - 1; lvl >= R.min_lvl; lvl--) {
+    const int li = lvl - R.min_lvl;
+    const RstRec *rr = R.rst + R.rst_off[li];
+    const int n = R.rst_off[li + 1] - R.rst_off[li];
+    const int cg = R.lv_nc[li + 1] + 2;
+    for (int k = threadIdx.x; k < n; k += NTHR) {
+      const RstRec r = rr[k];
+      for (int w = 0; w < 2; w++) {
+        const int iv = w == 0 ? iv0 : iv1;
+        if (iv < 0) continue;
+        double *x = VAR(R, iv);
+        const double a = x[r.src], b = x[r.src + 1], c = x[r.src + cg], d = x[r.src + cg + 1];
+        x[r.dst] = cyl ? (0.25 - r.rfac) * (a + c) + (0.25 + r.rfac) * (b + d)
+                       : 0.25 * (a + b + c + d);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Field of one face from the potential (fld_from_pot, src/streamer_2d.f90:
+// 346-381): g is the cell on the high side, s the stride to the low side,
+// pos the face index along its direction (1..nc+1).
+__device__ __forceinline__ double face_fld(const double *phi, const double *eps, int g, int s,
+                                           int pos, int nc, double inv_dr) {
+  if (pos == 1) return 2 * inv_dr * (phi[g - s] - phi[g]) * eps[g - s] / (eps[g] + eps[g - s]);
+  if (pos == nc + 1) return 2 * inv_dr * (phi[g - s] - phi[g]) * eps[g] / (eps[g] + eps[g - s]);
+  return inv_dr * (phi[g - s] - phi[g]);
+}
+
+// fld_from_pot on every box in one phase (each cell writes its low faces and,
+// on the high box edges, the high faces; |E| from its four faces), then the
+// |E| ghost fill a$D_gc_tree(i_fld, a$D_gc_interp, a$D_gc_neumann).
+__device__ void p_fld_from_pot(const RunDev &R) {
+  const double *phi = VAR(R, I_PHI), *eps = VAR(R, I_EPS);
+  double *fld = VAR(R, I_FLD);
+  const int a = R.cell_off[0], b = R.cell_off[R.nlev];
+  for (int k = a + threadIdx.x; k < b; k += NTHR) {
+    const CellRec c = R.cells[k];
+    const int li = c.li;
+    const int nc = R.lv_nc[li], ncg = nc + 2;
+    const double inv_dr = 1 / R.lv_dr[li];
+    const int id = c.g / SLOT, loc = c.g - id * SLOT;
+    const int i = loc % ncg, j = loc / ncg;
+    const double fxl = face_fld(phi, eps, c.g, 1, i, nc, inv_dr);
+    const double fxh = face_fld(phi, eps, c.g + 1, 1, i + 1, nc, inv_dr);
+    const double fyl = face_fld(phi, eps, c.g, ncg, j, nc, inv_dr);
+    const double fyh = face_fld(phi, eps, c.g + ncg, ncg, j + 1, nc, inv_dr);
+    double *fxf = FX(R, F_FLD, id), *fyf = FY(R, F_FLD, id);
+    fxf[fxi(i, j, nc)] = fxl;
+    if (i == nc) fxf[fxi(nc + 1, j, nc)] = fxh;
+    fyf[fyi(i, j, nc)] = fyl;
+    if (j == nc) fyf[fyi(i, nc + 1, nc)] = fyh;
+    const double sx = fxl + fxh, sy = fyl + fyh;
+    fld[c.g] = sqrt(0.25 * (sx * sx) + 0.25 * (sy * sy));
+  }
   __syncthreads();
-  box_loop(ids, n, [&](int id, int t) {
-    const BoxMeta &m = R.meta[id];
-    const int nc = m.nc, ncg = nc + 2;
-    if (t >= nc * nc) return;
-    const int i = t % nc + 1, j = t / nc + 1;
-    const double *fxf = FX(R, F_FLD, id), *fyf = FY(R, F_FLD, id);
-    double sx = fxf[fxi(i, j, nc)] + fxf[fxi(i + 1, j, nc)];
-    double sy = fyf[fyi(i, j, nc)] + fyf[fyi(i, j + 1, nc)];
-    CC(R, I_FLD, id)[i + ncg * j] = sqrt(0.25 * (sx * sx) + 0.25 * (sy * sy));
-  });
-  __syncthreads();
-  gc_tree(R, I_FLD, -1, GC_INTERP);
+  p_gc_den(R, I_FLD, -1, false);
 }
 
 // compute_fld, src/streamer_2d.f90:307-343 (one FMG cycle)
-__device__ void compute_fld(const RunDev &R, bool no_guess) {
-  set_rhs(R);
-  fas_fmg(R, false, no_guess);
-  fld_from_pot(R);
+__device__ void p_compute_fld(const RunDev &R, bool no_guess) {
+  p_fmg(R, false, no_guess, true);
+  p_fld_from_pot(R);
 }
 
 // Whole-array copy / average over every slot (unused slots included; their
@@ -1043,8 +1091,16 @@ __device__ void prolong_new(const RunDev &R) {
 
 // One full time step, src/streamer_2d.f90:99-127
 __device__ void step(const RunDev &R, double dt) {
-  copy_var(R, I_ELEC, I_ELEC_OLD);
-  copy_var(R, I_PION, I_PION_OLD);
+  {
+    const size_t n = (size_t)R.capacity * SLOT;
+    const double *e = VAR(R, I_ELEC), *pi = VAR(R, I_PION);
+    double *eo = VAR(R, I_ELEC_OLD), *po = VAR(R, I_PION_OLD);
+    for (size_t k = threadIdx.x; k < n; k += NTHR) {
+      eo[k] = e[k];
+      po[k] = pi[k];
+    }
+    __syncthreads();
+  }
   for (int stage = 1; stage <= 2; stage++) {
     fluxes_koren(R, dt);
     __syncthreads();
@@ -1052,12 +1108,12 @@ __device__ void step(const RunDev &R, double dt) {
     __syncthreads();
     update_solution(R, dt);
     __syncthreads();
-    restrict_tree(R, I_ELEC, I_PION);
-    gc_tree(R, I_ELEC, I_PION, GC_LIM);
-    if (stage == 1) compute_fld(R, false);
+    p_restrict(R, I_ELEC, I_PION);
+    p_gc_den(R, I_ELEC, I_PION, true);
+    if (stage == 1) p_compute_fld(R, false);
   }
   average_dens(R);
-  compute_fld(R, false);
+  p_compute_fld(R, false);
 }
 
 __device__ void run_op(const RunDev &R, const Op &op) {
@@ -1066,17 +1122,16 @@ __device__ void run_op(const RunDev &R, const Op &op) {
     case OP_FLUXES: fluxes_koren(R, op.d0); __syncthreads(); break;
     case OP_CONSISTENT: consistent_fluxes(R); __syncthreads(); break;
     case OP_UPDATE: update_solution(R, op.d0); __syncthreads(); break;
-    case OP_RESTRICT: restrict_tree(R, op.i0, -1); break;
-    case OP_GC: gc_tree(R, op.i0, -1, op.i1); break;
+    case OP_RESTRICT: p_restrict(R, op.i0, -1); break;
+    case OP_GC: p_gc_den(R, op.i0, -1, op.i1 == GC_LIM); break;
     case OP_AVERAGE: average_dens(R); break;
-    case OP_COMPUTE_FLD: compute_fld(R, op.i0 != 0); break;
-    case OP_FMG: fas_fmg(R, op.i0 != 0, op.i1 != 0); break;
-    case OP_FLD_FROM_POT: fld_from_pot(R); break;
+    case OP_COMPUTE_FLD: p_compute_fld(R, op.i0 != 0); break;
+    case OP_FMG: p_fmg(R, op.i0 != 0, op.i1 != 0, false); break;
+    case OP_FLD_FROM_POT: p_fld_from_pot(R); break;
     case OP_DT_RED: dt_reductions(R); break;
     case OP_REF_FLAGS: ref_flags(R, op.d0); break;
     case OP_PROLONG_NEW: prolong_new(R); break;
     case OP_STEP: step(R, op.d0); break;
-    case OP_SET_RHS: set_rhs(R); break;
     default: if (threadIdx.x == 0) atomicExch(R.status, A5G_EINVAL);
   }
 }
@@ -1178,7 +1233,330 @@ struct a5g_ctx {
   double tbl_xmin = 0, tbl_inv_dx = 0;
   long long n_leaf_cells = 0;
   int min_lvl = 0, max_lvl = 0;
+  // plan storage
+  CellRec *p_cells = nullptr;
+  GhostRec *p_gphi = nullptr, *p_gden = nullptr;
+  RstRec *p_rst = nullptr;
+  FrRec *p_fr = nullptr;
+  int *p_pcells = nullptr;
+  size_t cap_cells = 0, cap_gphi = 0, cap_gden = 0, cap_rst = 0, cap_fr = 0, cap_pcells = 0;
 };
+
+// ---------------------------------------------------------------------------
+// Plan builder: resolves, per level, every index the plan-based phases use
+// (see the device section "Plan-based operations").
+struct HostPlans {
+  std::vector<CellRec> cells;
+  std::vector<GhostRec> gphi, gden;
+  std::vector<RstRec> rst;
+  std::vector<FrRec> fr;
+  std::vector<int> pcells;
+  int cell_off[MAXLEV + 1], cell_split[MAXLEV], gphi_off[MAXLEV + 1], gden_off[MAXLEV + 1];
+  int rst_off[MAXLEV + 1], fr_off[MAXLEV + 1], pcell_off[MAXLEV + 1];
+  int lv_nc[MAXLEV];
+  double lv_dr[MAXLEV];
+};
+
+static void host_child_offset(const BoxMeta &m, int nb, int &o0, int &o1) {
+  static const int dix[4][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}};
+  if (m.lvl > 1) {
+    o0 = ((m.ix0 - 1) & 1) * (m.nc >> 1);
+    o1 = ((m.ix1 - 1) & 1) * (m.nc >> 1);
+    if (nb >= 0) { o0 -= dix[nb][0] * m.nc; o1 -= dix[nb][1] * m.nc; }
+  } else {
+    o0 = o1 = 0;
+    if (nb >= 0) { o0 -= dix[nb][0] * (m.nc >> 1); o1 -= dix[nb][1] * (m.nc >> 1); }
+  }
+}
+
+// Leaf / parent status is list membership, as in every box loop of the
+// reference (lvl_t%leaves / %parents), not "has children": the two differ on
+// level lvls_max, whose lists a$D_adjust_refinement never rebuilds
+// (afivo/src/m_aX_core.f90:478-515 calls set_leaves_parents for levels below
+// lvls_max and for max_lvl+1 only).
+static void build_plans(const std::vector<BoxMeta> &hm, const std::vector<std::vector<int>> &ids,
+                        const std::vector<std::vector<int>> &leaves,
+                        const std::vector<std::vector<int>> &parents, int min_lvl, int nlev,
+                        double dr_base, int coord, HostPlans &P) {
+  std::vector<char> is_leaf(hm.size(), 0), is_parent(hm.size(), 0);
+  for (const auto &v : leaves)
+    for (int id : v) is_leaf[id] = 1;
+  for (const auto &v : parents)
+    for (int id : v) is_parent[id] = 1;
+  static const int ch_dix[4][2] = {{0, 0}, {1, 0}, {0, 1}, {1, 1}};
+  P.cells.clear(); P.gphi.clear(); P.gden.clear(); P.rst.clear(); P.fr.clear(); P.pcells.clear();
+  auto G = [&](int id, int i, int j) { return id * SLOT + i + (hm[id].nc + 2) * j; };
+  for (int li = 0; li < nlev; li++) {
+    const int lvl = min_lvl + li;
+    const int nc = lvl >= 1 ? NC : (NC >> (1 - lvl));
+    P.lv_nc[li] = nc;
+    P.lv_dr[li] = ids[li].empty() ? dr_base * std::pow(0.5, lvl - 1) : hm[ids[li][0]].dr;
+    P.cell_off[li] = (int)P.cells.size();
+    P.gphi_off[li] = (int)P.gphi.size();
+    P.gden_off[li] = (int)P.gden.size();
+    P.rst_off[li] = (int)P.rst.size();
+    P.fr_off[li] = (int)P.fr.size();
+    P.pcell_off[li] = (int)P.pcells.size();
+    const std::vector<int> &L = ids[li];
+    const int nbx = (int)L.size();
+    // ghost recipes, index (b, nb, k-1) -> b * 4 nc + nb nc + k-1
+    for (int b = 0; b < nbx; b++) {
+      const int id = L[b];
+      const BoxMeta &m = hm[id];
+      const bool parent = is_parent[id] != 0;
+      for (int nb = 0; nb < 4; nb++) {
+        const int dim = nb >> 1;
+        const bool low = (nb & 1) == 0;
+        const int nid = m.nb[nb];
+        for (int k = 1; k <= nc; k++) {
+          GhostRec gp{}, gd{};
+          int gi, gj;  // ghost cell
+          if (dim == 0) { gi = low ? 0 : nc + 1; gj = k; }
+          else { gi = k; gj = low ? 0 : nc + 1; }
+          gp.dst = gd.dst = G(id, gi, gj);
+          if (nid > 0) {
+            // sides_from_nb (m_aX_gc.f90:368-402)
+            int si = dim == 0 ? (low ? nc : 1) : k, sj = dim == 0 ? k : (low ? nc : 1);
+            gp.kind = gd.kind = GK_COPY;
+            gp.s[0] = gd.s[0] = G(nid, si, sj);
+          } else if (nid == 0) {
+            // mg$D_sides_rb after a$D_gc_prolong0 (m_aX_mg.f90:261-301)
+            int o0, o1;
+            host_child_offset(m, -1, o0, o1);
+            const int ix = low ? 1 : nc, di = low ? 1 : -1, dk = -1 + 2 * (k & 1);
+            const int ig = ix - di;
+            gp.kind = GK_RB;
+            if (dim == 0) {
+              gp.s[0] = G(m.parent, o0 + ((ig + 1) >> 1), o1 + ((k + 1) >> 1));
+              gp.s[1] = G(id, ix, k);
+              gp.s[2] = G(id, ix + di, k);
+              gp.s[3] = G(id, ix, k + dk);
+            } else {
+              gp.s[0] = G(m.parent, o0 + ((k + 1) >> 1), o1 + ((ig + 1) >> 1));
+              gp.s[1] = G(id, k, ix);
+              gp.s[2] = G(id, k + dk, ix);
+              gp.s[3] = G(id, k, ix + di);
+            }
+            // a$D_gc_interp(_lim) from the parent's neighbour (m_aX_gc.f90:90-295)
+            int q0, q1;
+            host_child_offset(m, nb, q0, q1);
+            const int pn = hm[m.parent].nb[nb];
+            const int ix_f = low ? 1 : nc, ix_c = low ? nc : 1;
+            gd.kind = GK_INTERP;
+            if (dim == 0) {
+              const int j_c1 = q1 + ((k + 1) >> 1), j_c2 = j_c1 + 1 - 2 * (k & 1);
+              gd.s[0] = G(pn, ix_c, j_c1);
+              gd.s[1] = G(pn, ix_c, j_c2);
+              gd.s[2] = G(id, ix_f, k);
+            } else {
+              const int i_c1 = q0 + ((k + 1) >> 1), i_c2 = i_c1 + 1 - 2 * (k & 1);
+              gd.s[0] = G(pn, i_c1, ix_c);
+              gd.s[1] = G(pn, i_c2, ix_c);
+              gd.s[2] = G(id, k, ix_f);
+            }
+          } else {
+            // physical boundary: sides_bc_pot (src/streamer_2d.f90:620-638)
+            // for the potential, a$D_gc_neumann for the densities and |E|
+            int si = dim == 0 ? (low ? 1 : nc) : k, sj = dim == 0 ? k : (low ? 1 : nc);
+            gp.s[0] = gd.s[0] = G(id, si, sj);
+            gd.kind = GK_COPY;
+            gp.kind = nb == 2 ? GK_NEG : (nb == 3 ? GK_APPLIED : GK_COPY);
+          }
+          if (parent) gp.kind |= GK_PARENT;
+          P.gphi.push_back(gp);
+          P.gden.push_back(gd);
+        }
+      }
+    }
+    // cells, then ordered by colour (i + j) & 1
+    std::vector<CellRec> col[2];
+    std::vector<int> pos_box[2];  // box index, for the position map
+    for (int b = 0; b < nbx; b++) {
+      const int id = L[b];
+      const BoxMeta &m = hm[id];
+      const int gbase = P.gphi_off[li] + b * 4 * nc;
+      auto ghost_code = [&](int nb, int k) {
+        const GhostRec &r = P.gphi[gbase + nb * nc + (k - 1)];
+        switch (r.kind & 0xff) {
+          case GK_COPY: return r.s[0];
+          case GK_NEG: return (NBK_NEG << 28) | r.s[0];
+          case GK_APPLIED: return (NBK_APPLIED << 28) | r.s[0];
+          default: return (NBK_RECIPE << 28) | (gbase - P.gphi_off[li] + nb * nc + (k - 1));
+        }
+      };
+      int o0 = 0, o1 = 0, pg = 0;
+      if (lvl > min_lvl) {
+        host_child_offset(m, -1, o0, o1);
+        pg = hm[m.parent].nc + 2;
+      }
+      for (int j = 1; j <= nc; j++)
+        for (int i = 1; i <= nc; i++) {
+          CellRec c{};
+          c.g = G(id, i, j);
+          const int ncg = nc + 2;
+          c.nb[0] = i > 1 ? c.g - 1 : ghost_code(0, j);
+          c.nb[1] = i < nc ? c.g + 1 : ghost_code(1, j);
+          c.nb[2] = j > 1 ? c.g - ncg : ghost_code(2, i);
+          c.nb[3] = j < nc ? c.g + ncg : ghost_code(3, i);
+          if (lvl > min_lvl) {
+            const int i_c1 = o0 + ((i + 1) >> 1), i_c2 = i_c1 + 1 - 2 * (i & 1);
+            const int j_c1 = o1 + ((j + 1) >> 1), j_c2 = j_c1 + 1 - 2 * (j & 1);
+            const int pb = m.parent * SLOT;
+            c.pc[0] = pb + i_c1 + pg * j_c1;
+            c.pc[1] = pb + i_c2 + pg * j_c1;
+            c.pc[2] = pb + i_c1 + pg * j_c2;
+          }
+          c.gi = (m.ix0 - 1) * nc + i;
+          c.flags = is_leaf[id] ? CF_LEAF : 0;
+          c.li = li;
+          col[(i + j) & 1].push_back(c);
+          pos_box[(i + j) & 1].push_back(b);
+        }
+    }
+    // position map (b, i, j) -> absolute cell index
+    std::vector<int> pos((size_t)nbx * nc * nc);
+    {
+      int at = P.cell_off[li];
+      for (int p = 0; p < 2; p++) {
+        if (p == 1) P.cell_split[li] = at;
+        for (size_t q = 0; q < col[p].size(); q++, at++) {
+          const CellRec &c = col[p][q];
+          const int b = pos_box[p][q];
+          const int loc = c.g - L[b] * SLOT;
+          const int i = loc % (nc + 2), j = loc / (nc + 2);
+          pos[(size_t)b * nc * nc + (i - 1) + nc * (j - 1)] = at;
+          P.cells.push_back(c);
+        }
+      }
+    }
+    for (int b = 0; b < nbx; b++)
+      if (is_parent[L[b]])
+        for (int q = 0; q < nc * nc; q++) P.pcells.push_back(pos[(size_t)b * nc * nc + q]);
+    // residual-restriction records for the boxes of this level
+    if (lvl > min_lvl) {
+      for (int b = 0; b < nbx; b++) {
+        const BoxMeta &m = hm[L[b]];
+        int o0, o1;
+        host_child_offset(m, -1, o0, o1);
+        const int hnc = nc >> 1, pg = hm[m.parent].nc + 2;
+        for (int jj = 1; jj <= hnc; jj++)
+          for (int ii = 1; ii <= hnc; ii++) {
+            FrRec r{};
+            r.dst = m.parent * SLOT + (o0 + ii) + pg * (o1 + jj);
+            const int i_f = 2 * ii - 1, j_f = 2 * jj - 1;
+            const size_t base = (size_t)b * nc * nc;
+            r.c[0] = pos[base + (i_f - 1) + nc * (j_f - 1)];
+            r.c[1] = pos[base + (i_f) + nc * (j_f - 1)];
+            r.c[2] = pos[base + (i_f - 1) + nc * (j_f)];
+            r.c[3] = pos[base + (i_f) + nc * (j_f)];
+            P.fr.push_back(r);
+          }
+      }
+    }
+    // restriction records for the parents of this level
+    for (int pid : parents[li]) {
+      const BoxMeta &pm = hm[pid];
+      for (int jc = 1; jc <= nc; jc++)
+        for (int ic = 1; ic <= nc; ic++) {
+          for (int q = 0; q < 4; q++) {
+            const int cid = pm.ch[q];
+            if (cid == 0) continue;
+            const BoxMeta &cm = hm[cid];
+            int o0, o1;
+            host_child_offset(cm, -1, o0, o1);
+            const int hnc = cm.nc >> 1, i = ic - o0, j = jc - o1;
+            if (i < 1 || i > hnc || j < 1 || j > hnc) continue;
+            RstRec r{};
+            r.dst = G(pid, ic, jc);
+            r.src = G(cid, 2 * i - 1, 2 * j - 1);
+            if (coord == 1) {
+              // m_aX_restrict.f90:95-113; radius at the child-local index [i, j]
+              const double dr16 = 0.0625 * pm.dr;
+              const double rr = pm.r0 + (i - 0.5) * pm.dr;
+              r.rfac = dr16 / rr;
+            }
+            P.rst.push_back(r);
+            (void)ch_dix;
+          }
+        }
+    }
+  }
+  P.cell_off[nlev] = (int)P.cells.size();
+  P.gphi_off[nlev] = (int)P.gphi.size();
+  P.gden_off[nlev] = (int)P.gden.size();
+  P.rst_off[nlev] = (int)P.rst.size();
+  P.fr_off[nlev] = (int)P.fr.size();
+  P.pcell_off[nlev] = (int)P.pcells.size();
+}
+
+template <class T>
+static int upload_vec(a5g_ctx *c, T *&dev, size_t &cap, const std::vector<T> &v) {
+  if (v.size() + 1 > cap) {
+    cudaFree(dev);
+    dev = nullptr;
+    cap = std::max(v.size() + 1, 2 * cap);
+    CK(cudaMalloc(&dev, cap * sizeof(T)));
+  }
+  if (!v.empty())
+    CK(cudaMemcpyAsync(dev, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+  return A5G_OK;
+}
+
+// Host-only export of the plans of a topology (tests and diagnostics; no
+// device needed). Level lists in the a5g_upload_tree format. Output arrays
+// may be NULL; sizes[6] = cells, ghosts, ghosts, rst, fr, pcells.
+extern "C" int a5g_debug_plans(int max_id, int min_lvl, int max_lvl, const int *meta16,
+                               const double *geom4, const int *lvl_counts, const int *lvl_ids,
+                               double dr_base, int coord, int *sizes, int *offs, int *cells,
+                               int *gphi, int *gden, int *rst_i, double *rst_rfac, int *fr,
+                               int *pcells, double *lv_dr, int *lv_nc) {
+  const int nlev = max_lvl - min_lvl + 1;
+  if (nlev < 1 || nlev + 1 > MAXLEV || max_id < 1) return fail(A5G_EINVAL, "bad tree");
+  std::vector<BoxMeta> hm(max_id + 1);
+  std::memset(hm.data(), 0, hm.size() * sizeof(BoxMeta));
+  for (int id = 1; id <= max_id; id++) {
+    const int *m = meta16 + 16 * id;
+    if (!m[0]) continue;
+    BoxMeta &b = hm[id];
+    b.lvl = m[1]; b.ix0 = m[2]; b.ix1 = m[3]; b.parent = m[5];
+    for (int k = 0; k < 4; k++) { b.ch[k] = m[6 + k]; b.nb[k] = m[10 + k]; }
+    b.nc = m[14];
+    b.dr = geom4[4 * id + 3]; b.r0 = geom4[4 * id]; b.r1 = geom4[4 * id + 1];
+  }
+  std::vector<std::vector<int>> lv_ids(nlev), lv_leaves(nlev), lv_parents(nlev);
+  size_t k = 0;
+  for (int li = 0; li < nlev; li++)
+    for (int kind = 0; kind < 3; kind++)
+      for (int q = 0; q < lvl_counts[3 * li + kind]; q++) {
+        int id = lvl_ids[k++];
+        if (kind == 0) lv_ids[li].push_back(id);
+        if (kind == 1) lv_leaves[li].push_back(id);
+        if (kind == 2) lv_parents[li].push_back(id);
+      }
+  HostPlans P;
+  build_plans(hm, lv_ids, lv_leaves, lv_parents, min_lvl, nlev, dr_base, coord, P);
+  if (sizes) {
+    sizes[0] = (int)P.cells.size(); sizes[1] = (int)P.gphi.size(); sizes[2] = (int)P.gden.size();
+    sizes[3] = (int)P.rst.size(); sizes[4] = (int)P.fr.size(); sizes[5] = (int)P.pcells.size();
+  }
+  if (offs) {
+    const int *src[7] = {P.cell_off, P.cell_split, P.gphi_off, P.gden_off, P.rst_off, P.fr_off, P.pcell_off};
+    for (int a = 0; a < 7; a++)
+      for (int li = 0; li <= nlev; li++) offs[a * (MAXLEV + 1) + li] = (a == 1 && li == nlev) ? 0 : src[a][li];
+  }
+  if (cells) std::memcpy(cells, P.cells.data(), P.cells.size() * sizeof(CellRec));
+  if (gphi) std::memcpy(gphi, P.gphi.data(), P.gphi.size() * sizeof(GhostRec));
+  if (gden) std::memcpy(gden, P.gden.data(), P.gden.size() * sizeof(GhostRec));
+  for (size_t q = 0; q < P.rst.size(); q++) {
+    if (rst_i) { rst_i[2 * q] = P.rst[q].dst; rst_i[2 * q + 1] = P.rst[q].src; }
+    if (rst_rfac) rst_rfac[q] = P.rst[q].rfac;
+  }
+  if (fr) std::memcpy(fr, P.fr.data(), P.fr.size() * sizeof(FrRec));
+  if (pcells) std::memcpy(pcells, P.pcells.data(), P.pcells.size() * sizeof(int));
+  if (lv_dr) std::memcpy(lv_dr, P.lv_dr, nlev * sizeof(double));
+  if (lv_nc) std::memcpy(lv_nc, P.lv_nc, nlev * sizeof(int));
+  return A5G_OK;
+}
 
 static int push_run(a5g_ctx *c) {
   CK(cudaMemcpyAsync(c->d_run, &c->h, sizeof(RunDev), cudaMemcpyHostToDevice, c->stream));
@@ -1274,6 +1652,12 @@ int a5g_destroy(a5g_ctx *c) {
   cudaFree(c->scal);
   cudaFree(c->flags);
   cudaFree(c->status);
+  cudaFree(c->p_cells);
+  cudaFree(c->p_gphi);
+  cudaFree(c->p_gden);
+  cudaFree(c->p_rst);
+  cudaFree(c->p_fr);
+  cudaFree(c->p_pcells);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return A5G_OK;
@@ -1379,6 +1763,7 @@ int a5g_upload_tree(a5g_ctx *c, int max_id, int min_lvl, int max_lvl, const int 
   }
   std::vector<int> lists;
   int off[3][MAXLEV + 1];
+  std::vector<std::vector<int>> lv_ids(nlev), lv_leaves(nlev), lv_parents(nlev);
   {
     // regroup per-level (ids, leaves, parents) into three contiguous blocks
     std::vector<std::vector<int>> by(3);
@@ -1395,6 +1780,9 @@ int a5g_upload_tree(a5g_ctx *c, int max_id, int min_lvl, int max_lvl, const int 
             return fail(A5G_EINVAL, "level list names an unused id");
           if (hm[id].lvl != min_lvl + li) return fail(A5G_EINVAL, "level list / box level mismatch");
           by[kind].push_back(id);
+          if (kind == 0) lv_ids[li].push_back(id);
+          if (kind == 1) lv_leaves[li].push_back(id);
+          if (kind == 2) lv_parents[li].push_back(id);
         }
       }
     }
@@ -1429,7 +1817,31 @@ int a5g_upload_tree(a5g_ctx *c, int max_id, int min_lvl, int max_lvl, const int 
   if (!lists.empty())
     CK(cudaMemcpyAsync(c->lists, lists.data(), lists.size() * sizeof(int), cudaMemcpyHostToDevice,
                        c->stream));
+  HostPlans P;
+  build_plans(hm, lv_ids, lv_leaves, lv_parents, min_lvl, nlev, c->p.dr_base, c->p.coord, P);
+  if ((r = upload_vec(c, c->p_cells, c->cap_cells, P.cells)) ||
+      (r = upload_vec(c, c->p_gphi, c->cap_gphi, P.gphi)) ||
+      (r = upload_vec(c, c->p_gden, c->cap_gden, P.gden)) ||
+      (r = upload_vec(c, c->p_rst, c->cap_rst, P.rst)) ||
+      (r = upload_vec(c, c->p_fr, c->cap_fr, P.fr)) ||
+      (r = upload_vec(c, c->p_pcells, c->cap_pcells, P.pcells)))
+    return r;
   RunDev &h = c->h;
+  std::memcpy(h.cell_off, P.cell_off, sizeof(P.cell_off));
+  std::memcpy(h.cell_split, P.cell_split, sizeof(P.cell_split));
+  std::memcpy(h.gphi_off, P.gphi_off, sizeof(P.gphi_off));
+  std::memcpy(h.gden_off, P.gden_off, sizeof(P.gden_off));
+  std::memcpy(h.rst_off, P.rst_off, sizeof(P.rst_off));
+  std::memcpy(h.fr_off, P.fr_off, sizeof(P.fr_off));
+  std::memcpy(h.pcell_off, P.pcell_off, sizeof(P.pcell_off));
+  std::memcpy(h.lv_nc, P.lv_nc, sizeof(P.lv_nc));
+  std::memcpy(h.lv_dr, P.lv_dr, sizeof(P.lv_dr));
+  h.cells = c->p_cells;
+  h.gphi = c->p_gphi;
+  h.gden = c->p_gden;
+  h.rst = c->p_rst;
+  h.fr = c->p_fr;
+  h.pcells = c->p_pcells;
   h.min_lvl = min_lvl;
   h.max_lvl = max_lvl;
   h.nlev = nlev;

@@ -303,7 +303,7 @@ def run_b200(args):
 
     peak, peak_kind = measured_peak()
     achieved = bytes_step / (ms_per_step / 1e3) / 1e9
-    traffic = traffic_per_launch(wname)
+    traffic = traffic_per_launch(args.workload)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic,
                 "peak_kind": peak_kind, "algorithmic_bytes_per_launch": bytes_step}

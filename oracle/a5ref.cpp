@@ -1686,6 +1686,31 @@ int a5ref_op_regrid(a5ref_sim *h, int *n_add, int *n_rm) {
   return ri.n_add + ri.n_rm;
 }
 
+// Multigrid stages, for stepping the solver in lockstep with other
+// implementations in the tests (afivo/src/m_aX_mg.f90:163-447).
+void a5ref_dbg_set_rhs_voltage(a5ref_sim *h) {
+  set_rhs(h->s);
+  h->s.applied_voltage = -h->s.p.domain_len_z * h->s.p.applied_fld;
+}
+void a5ref_dbg_set_coarse(a5ref_sim *h, int lvl) { set_coarse_phi_rhs(h->s.tree, lvl, h->s.mg); }
+void a5ref_dbg_fmg_pre(a5ref_sim *h, int lvl) {
+  Tree &t = h->s.tree;
+  for (int id : t.L(lvl).ids) copy_full(t.boxes[id], h->s.mg.i_phi, h->s.mg.i_tmp);
+  if (lvl > t.min_lvl) {
+    correct_children(t, t.L(lvl - 1).parents, h->s.mg);
+    fill_gc_phi(t, t.L(lvl).ids, h->s.mg);
+  }
+}
+void a5ref_dbg_gsrb(a5ref_sim *h, int lvl, int n_cycle) {
+  gsrb_boxes(h->s.tree, h->s.tree.L(lvl).ids, h->s.mg, n_cycle);
+}
+void a5ref_dbg_update_coarse(a5ref_sim *h, int lvl) { update_coarse(h->s.tree, lvl, h->s.mg); }
+void a5ref_dbg_correct_fill(a5ref_sim *h, int lvl) {
+  Tree &t = h->s.tree;
+  correct_children(t, t.L(lvl - 1).parents, h->s.mg);
+  fill_gc_phi(t, t.L(lvl).ids, h->s.mg);
+}
+
 int a5ref_max_id(a5ref_sim *h) { return h->s.tree.max_id; }
 int a5ref_max_lvl(a5ref_sim *h) { return h->s.tree.max_lvl; }
 int a5ref_min_lvl(a5ref_sim *h) { return h->s.tree.min_lvl; }

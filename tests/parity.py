@@ -72,9 +72,12 @@ def compare(sim: a5ref.Sim, run: dv.DeviceRun, cc_vars=range(N_CC), fc_vars=((0,
     nc = sim.nc
     mask = side_mask(meta, nc) if mask_kind == "side" else interior_mask(meta, nc)
     fmask = face_mask(meta, nc)
+    imask = interior_mask(meta, nc)
     for iv in cc_vars:
         a, b = sim.cc(iv), run.cc(iv)
-        _check(a[mask], b[mask], rtol, f"{where} cc var {iv}")
+        # rhs ghost cells are never read by any operator and are not maintained
+        m = imask if iv == 6 else mask
+        _check(a[m], b[m], rtol, f"{where} cc var {iv}")
     for d, f in fc_vars:
         a, b = sim.fc(d, f), run.fc(d, f)
         _check(a[fmask], b[fmask], rtol, f"{where} face dim {d} var {f}")

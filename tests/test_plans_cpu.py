@@ -1,0 +1,64 @@
+"""The device path's plans and phase schedule, checked on the CPU.
+
+The plans (cell tables with neighbour codes, ghost recipes, restriction and
+residual-restriction records) come from the library's host-only builder; the
+multigrid phases are replayed by tests/plan_emulator.py exactly as the device
+runs them (all outputs of a phase from the state before it, same arithmetic
+order). The result must equal the oracle's FAS FMG bit for bit, on trees that
+include refinement boundaries, physical corners, removed boxes and a full
+finest level (lvls_max reached)."""
+import numpy as np
+import pytest
+
+import a5ref
+from a5_streamer_b200 import config
+from parity import interior_mask, side_mask
+from plan_emulator import Emulator, Plans
+
+CASES = {
+    "cart": (config.cartesian_8mm(), 2),
+    "cyl": (config.cylindrical_16mm(), 2),
+    "cart_active_1": (config.cartesian_8mm(applied_fld=7e6, lvls_max=6), 1),
+    "cart_active_2": (config.cartesian_8mm(applied_fld=7e6, lvls_max=6), 2),
+    "cart_active_6": (config.cartesian_8mm(applied_fld=7e6, lvls_max=6), 6),
+}
+
+
+def _setup(name):
+    cfg, blocks = CASES[name]
+    sim = a5ref.Sim(cfg, n_threads=4)
+    sim.init()
+    for _ in range(blocks):
+        sim.advance(True)
+    meta, geom, levels = sim.meta(), sim.geom(), sim.levels()
+    coord = 1 if cfg.coord == "cyl" else 0
+    P = Plans(meta, geom, levels, sim.min_lvl, sim.max_lvl, cfg.dr_base, coord)
+    em = Emulator(P, [sim.cc(i) for i in range(9)], [sim.fc(0, f) for f in range(2)],
+                  [sim.fc(1, f) for f in range(2)], coord, cfg.applied_voltage, cfg.n_cycle_base)
+    return cfg, sim, meta, em
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+@pytest.mark.parametrize("first_call", [False, True])
+def test_emulated_fmg_matches_oracle(name, first_call):
+    cfg, sim, meta, em = _setup(name)
+    sim.op("set_rhs")
+    sim.op("fmg", 0, 1 if first_call else 0)
+    em.fmg(first_call, True)
+    m = side_mask(meta, cfg.box_size).reshape(-1)
+    mi = interior_mask(meta, cfg.box_size).reshape(-1)
+    assert np.array_equal(sim.cc(4).reshape(-1)[m], em.cc[4][m])
+    assert np.array_equal(sim.cc(6).reshape(-1)[mi], em.cc[6][mi])
+
+
+def test_plan_sizes():
+    cfg, sim, meta, em = _setup("cart")
+    P = em.P
+    n_cells = sum(int(meta[i, 14]) ** 2 for i in range(1, meta.shape[0]) if meta[i, 0])
+    assert P.cell_off[P.nlev] == n_cells
+    # every interior cell appears once in the cell table
+    g = P.cells[:n_cells, 0]
+    assert len(np.unique(g)) == n_cells
+    # 4 nc ghosts per box
+    n_gh = sum(4 * int(meta[i, 14]) for i in range(1, meta.shape[0]) if meta[i, 0])
+    assert P.gphi_off[P.nlev] == n_gh and P.gden_off[P.nlev] == n_gh
