@@ -6,6 +6,14 @@ extern "C" {
 #endif
 /* Record an error message for a5g_last_error() and return code. */
 int a5g_internal_fail(int code, const char *msg);
+/* Diagnostics: shared-memory doubles per multigrid variable, dynamic shared
+ * memory per launch, capacity, levels, device limit, boxes. */
+struct a5g_ctx;
+int a5g_debug_info(struct a5g_ctx *ctx, long long *out8);
+/* Diagnostics: timing probes (0: n barriers, 1: n half-sweeps of level lvl,
+ * 2: n ghost fills of level lvl, 3: empty launch). */
+int a5g_debug_op(struct a5g_ctx *ctx, int code, int n, int lvl, int in_smem);
+int a5g_debug_scal(struct a5g_ctx *ctx, double *out16);
 #ifdef __cplusplus
 }
 #endif

@@ -59,26 +59,26 @@ struct BoxMeta {
 };
 static_assert(sizeof(BoxMeta) == 96, "BoxMeta layout");
 
-// Plan records, built on the host once per topology (build_plans).
-// CellRec: one interior cell: global index g (slot * SLOT + local), the four
-// neighbour codes (lx, hx, ly, hy; see NBK_*), the three parent cells of the
-// multigrid correction, the global i index (cylindrical weights), flags and
-// the level index.
-struct __align__(16) CellRec { int g, nb[4], pc[3], gi, flags, li, pad; };
-// GhostRec: one side-ghost cell: destination, kind (GK_*), sources.
-struct GhostRec { int dst, kind, s[4]; };
-// RstRec: one parent cell of a restriction: destination, first fine source,
-// cylindrical weight.
-struct RstRec { int dst, src; double rfac; };
-// FrRec: one parent cell of the multigrid residual restriction: destination
-// and the four fine cells (indices into the cell table).
-struct __align__(16) FrRec { int dst, c[4], pad[3]; };
-enum { NBK_DIRECT = 0, NBK_NEG = 1, NBK_APPLIED = 2, NBK_RECIPE = 3 };
-enum { GK_COPY = 0, GK_NEG = 1, GK_APPLIED = 2, GK_RB = 3, GK_INTERP = 4 };
-constexpr int GK_PARENT = 0x100;  // ghost of a box that has children
-constexpr int CF_LEAF = 1;
-constexpr int NB_MASK = 0x0FFFFFFF;
-static_assert(sizeof(CellRec) == 48 && sizeof(FrRec) == 32, "plan layout");
+// Plan record of one box, built on the host once per topology (build_plans):
+// slot bases (id * SLOT) of the box, its parent (-1: none), its neighbours per
+// side (NBR_RB at a refinement boundary, NBR_PHYS at a physical one), the
+// parent's neighbours where the box is at a refinement boundary, and its
+// children (0: none); its offset in the parent (cells), its first global i
+// index, list membership flags, r_min(1) and dr. A second set of records
+// addresses the compact shared-memory copy of the multigrid variables
+// (bases into that copy; gbase keeps the device-memory slot base).
+struct __align__(16) BoxRec {
+  int base, pbase;
+  int nb[4];
+  int pnb[4];
+  int ch[4];
+  int o0, o1, gi0, flags;
+  double r0, dr;
+  int gbase, pad;  // slot base in device memory (= base for the device-memory records)
+};
+static_assert(sizeof(BoxRec) == 96, "plan layout");
+constexpr int NBR_RB = -1, NBR_PHYS = -2;
+constexpr int CF_LEAF = 1, CF_PARENT = 2;
 
 struct RunDev {
   int capacity, min_lvl, max_lvl, lvls_max;
@@ -97,16 +97,14 @@ struct RunDev {
   int n_seeds, pad2;
   double seed_r0[8][2], seed_r1[8][2], seed_width[8];
   // plans, per level index
-  int cell_off[MAXLEV + 1], cell_split[MAXLEV];
-  int gphi_off[MAXLEV + 1], gden_off[MAXLEV + 1];
-  int rst_off[MAXLEV + 1], fr_off[MAXLEV + 1], pcell_off[MAXLEV + 1];
+  int bx_off[MAXLEV + 1], pb_off[MAXLEV + 1];
   int lv_nc[MAXLEV], pad3;
   double lv_dr[MAXLEV];
-  const CellRec *cells;
-  const GhostRec *gphi, *gden;
-  const RstRec *rst;
-  const FrRec *fr;
-  const int *pcells;
+  const BoxRec *boxes;
+  const BoxRec *sboxes;        // records addressing the shared-memory copy
+  const int *pbx;
+  int smem_doubles;            // per multigrid variable; 0: tree does not fit
+  int pad4;
   double *scal;                // dt reductions out
   int *flags;                  // refinement flags out
   int *status;
@@ -115,7 +113,7 @@ struct RunDev {
 enum OpCode {
   OP_COPY = 1, OP_FLUXES, OP_CONSISTENT, OP_UPDATE, OP_RESTRICT, OP_GC, OP_AVERAGE,
   OP_COMPUTE_FLD, OP_FMG, OP_FLD_FROM_POT, OP_DT_RED, OP_REF_FLAGS, OP_PROLONG_NEW,
-  OP_STEP, OP_SET_RHS
+  OP_STEP, OP_SET_RHS, OP_DBG_BARRIERS, OP_DBG_SWEEPS, OP_DBG_FILLS, OP_DBG_EMPTY
 };
 struct Op {
   int code, i0, i1, i2;
@@ -514,176 +512,264 @@ __device__ void update_solution(const RunDev &R, double dt) {
 constexpr int MP = I_PHI, MT = I_FLD, MR = I_RHS;
 
 // ---------------------------------------------------------------------------
-// Plan-based operations. The host resolves, once per topology, every index
-// the per-level phases need (see build_plans): a table of interior cells per
-// level ordered by red/black colour, with the four neighbours of each cell
-// encoded as a direct index, a negated index (grounded wall), an
-// applied-voltage index, or a ghost recipe; ghost recipes per level for the
-// potential (copy / mg$D_sides_rb / sides_bc_pot) and for the densities and
-// |E| (copy / a$D_gc_interp(_lim) / Neumann); restriction records; and
-// residual-restriction records. A phase is then a flat loop of all threads
-// over one of these lists.
+// Plan-based operations. The host writes, once per topology, one BoxRec per
+// box (level by level, in list order; build_plans) holding the slot bases of
+// the box, its parent, its same-level neighbours, its parent's neighbours and
+// its children, its offset in the parent and its list membership. Every
+// index a phase needs -- neighbour cells, ghost-cell sources, restriction and
+// correction stencils -- is derived from that record, and a phase is a flat
+// loop of all threads over the (box, cell) items of one level.
 
 __device__ __forceinline__ double *VAR(const RunDev &R, int v) {
   return R.cc + (size_t)v * R.capacity * SLOT;
 }
 
-// Ghost of the potential from its recipe
-__device__ __forceinline__ double recipe_phi(const RunDev &R, const double *phi,
-                                             const GhostRec &r) {
-  switch (r.kind & 0xff) {
-    case GK_COPY: return phi[r.s[0]];
-    case GK_NEG: return -phi[r.s[0]];
-    case GK_APPLIED: return 2 * R.applied_voltage - phi[r.s[0]];
-    default:  // mg$D_sides_rb, m_aX_mg.f90:283-298
-      return 0.5 * phi[r.s[0]] + phi[r.s[1]] - 0.25 * (phi[r.s[2]] + phi[r.s[3]]);
+// Where the multigrid variables live during a solve: device memory, or a
+// compact copy in shared memory when the tree fits (then every read in a
+// phase that follows a write by another thread hits shared memory instead
+// of L2). boxes: the BoxRecs addressing those arrays.
+struct MGV {
+  double *phi, *rhs, *tmp;
+  const BoxRec *boxes;
+  const int *pbx;
+};
+
+// Side ghost (side, k) of the potential: sides_from_nb, mg$D_sides_rb after
+// a$D_gc_prolong0 (m_aX_mg.f90:261-301), or sides_bc_pot
+// (src/streamer_2d.f90:620-638). Reads only interior cells of the box and its
+// neighbours and ghost cells of the parent.
+__device__ __forceinline__ double phi_ghost(const RunDev &R, const double *phi, const BoxRec &B,
+                                            int nc, int ncg, int side, int k) {
+  const int dim = side >> 1;
+  const bool low = (side & 1) == 0;
+  const int nbb = B.nb[side];
+  if (nbb > 0) return phi[nbb + (dim == 0 ? (low ? nc : 1) + ncg * k : k + ncg * (low ? nc : 1))];
+  const int ix = low ? 1 : nc;
+  const int own = B.base + (dim == 0 ? ix + ncg * k : k + ncg * ix);
+  if (nbb == NBR_RB) {
+    const int di = low ? 1 : -1, dk = -1 + 2 * (k & 1), ig = ix - di;
+    int pc, a, b;
+    if (dim == 0) {
+      pc = B.pbase + (B.o0 + ((ig + 1) >> 1)) + ncg * (B.o1 + ((k + 1) >> 1));
+      a = own + di;
+      b = own + ncg * dk;
+    } else {
+      pc = B.pbase + (B.o0 + ((k + 1) >> 1)) + ncg * (B.o1 + ((ig + 1) >> 1));
+      a = own + dk;
+      b = own + ncg * di;
+    }
+    return 0.5 * phi[pc] + phi[own] - 0.25 * (phi[a] + phi[b]);
   }
+  if (side == 2) return -phi[own];
+  if (side == 3) return 2 * R.applied_voltage - phi[own];
+  return phi[own];
 }
 
-// Neighbour value of the potential from a cell's neighbour code
-__device__ __forceinline__ double nbv(const RunDev &R, const double *phi, int code,
-                                      const GhostRec *gl) {
-  const int idx = code & NB_MASK;
-  switch ((unsigned)code >> 28) {
-    case NBK_DIRECT: return phi[idx];
-    case NBK_NEG: return -phi[idx];
-    case NBK_APPLIED: return 2 * R.applied_voltage - phi[idx];
-    default: return recipe_phi(R, phi, gl[idx]);
+// Side ghost (side, k) of a density or |E|: sides_from_nb, a$D_gc_interp
+// (lim: a$D_gc_interp_lim) from the parent's neighbour (m_aX_gc.f90:90-295),
+// or a$D_gc_neumann.
+__device__ __forceinline__ double den_ghost(const double *x, const BoxRec &B, int nc, int ncg,
+                                            int side, int k, bool lim) {
+  const int dim = side >> 1;
+  const bool low = (side & 1) == 0;
+  const int nbb = B.nb[side];
+  if (nbb > 0) return x[nbb + (dim == 0 ? (low ? nc : 1) + ncg * k : k + ncg * (low ? nc : 1))];
+  const int ix = low ? 1 : nc;
+  const int own = B.base + (dim == 0 ? ix + ncg * k : k + ncg * ix);
+  if (nbb == NBR_RB) {
+    const double sixth = 1 / 6.0, third = 1 / 3.0;
+    const int pn = B.pnb[side], ix_c = low ? nc : 1;
+    int s1, s2;
+    if (dim == 0) {
+      const int j_c1 = B.o1 + ((k + 1) >> 1), j_c2 = j_c1 + 1 - 2 * (k & 1);
+      s1 = pn + ix_c + ncg * j_c1;
+      s2 = pn + ix_c + ncg * j_c2;
+    } else {
+      const int i_c1 = B.o0 + ((k + 1) >> 1), i_c2 = i_c1 + 1 - 2 * (k & 1);
+      s1 = pn + i_c1 + ncg * ix_c;
+      s2 = pn + i_c2 + ncg * ix_c;
+    }
+    const double c1 = x[s1], c2 = x[s2];
+    double v = 0.5 * c1 + sixth * c2 + third * x[own];
+    if (lim && v > 2 * c1) v = 2 * c1;
+    return v;
   }
+  return x[own];
+}
+
+// Neighbours (lx, hx, ly, hy) of interior cell (i, j), ghost values from
+// their sources
+__device__ __forceinline__ void phi_nbrs(const RunDev &R, const double *phi, const BoxRec &B,
+                                         int nc, int ncg, int i, int j, int g, double &lx,
+                                         double &hx, double &ly, double &hy) {
+  lx = i > 1 ? phi[g - 1] : phi_ghost(R, phi, B, nc, ncg, 0, j);
+  hx = i < nc ? phi[g + 1] : phi_ghost(R, phi, B, nc, ncg, 1, j);
+  ly = j > 1 ? phi[g - ncg] : phi_ghost(R, phi, B, nc, ncg, 2, i);
+  hy = j < nc ? phi[g + ncg] : phi_ghost(R, phi, B, nc, ncg, 3, i);
 }
 
 // box_lpl (m_aX_mg.f90:662-680) / box_clpl (:1027-1049) at one cell
-__device__ __forceinline__ double lap_at(const RunDev &R, const double *phi, const CellRec &c,
-                                         const GhostRec *gl, double inv_dr_sq) {
-  const double lx = nbv(R, phi, c.nb[0], gl), hx = nbv(R, phi, c.nb[1], gl);
-  const double ly = nbv(R, phi, c.nb[2], gl), hy = nbv(R, phi, c.nb[3], gl);
-  const double v = phi[c.g];
+__device__ __forceinline__ double lap_at(const RunDev &R, const double *phi, const BoxRec &B,
+                                         int nc, int ncg, int i, int j, double inv_dr_sq) {
+  const int g = B.base + i + ncg * j;
+  double lx, hx, ly, hy;
+  phi_nbrs(R, phi, B, nc, ncg, i, j, g, lx, hx, ly, hy);
+  const double v = phi[g];
   if (R.coord == 1) {
-    const double den = c.gi - 0.5;
-    const double rf1 = (c.gi - 1) / den, rf2 = c.gi / den;
+    const int gi = B.gi0 + i;
+    const double den = gi - 0.5;
+    const double rf1 = (gi - 1) / den, rf2 = gi / den;
     return (rf1 * lx + rf2 * hx + ly + hy - 4 * v) * inv_dr_sq;
   }
   return inv_dr_sq * (lx + hx + ly + hy - 4 * v);
 }
 
-// Red-black Gauss-Seidel half-sweep `it` on level lvl (box_gsrb_lpl,
-// m_aX_mg.f90:636-659; box_gsrb_clpl :998-1024). Ghost neighbours are taken
-// from their recipes, which equals the ghost fill the reference performs
-// after every half-sweep (gsrb_boxes, :343-366): the recipes read only cells
-// of the colour not updated in this half-sweep, the updated cell itself
-// (read before it is written), or coarser-level cells. mem: read ghosts from
-// memory instead (the first half-sweep of a first FMG call, where the
-// reference's ghosts are not yet consistent with the interior).
-__device__ void p_sweep(const RunDev &R, int lvl, int it, bool mem) {
+struct LvlInfo {
+  int nc, ncg, sh, b0, nb;
+  double dr;
+};
+__device__ __forceinline__ LvlInfo lvl_info(const RunDev &R, int lvl) {
   const int li = lvl - R.min_lvl;
-  const bool odd = it & 1;
-  const int a = odd ? R.cell_split[li] : R.cell_off[li];
-  const int b = odd ? R.cell_off[li + 1] : R.cell_split[li];
-  double *phi = VAR(R, MP);
-  const double *rhs = VAR(R, MR);
-  const GhostRec *gl = R.gphi + R.gphi_off[li];
-  const double dr = R.lv_dr[li], dx2 = dr * dr;
-  const int ncg = R.lv_nc[li] + 2;
+  LvlInfo L;
+  L.nc = R.lv_nc[li];
+  L.ncg = L.nc + 2;
+  L.sh = 31 - __clz(L.nc);  // log2(nc)
+  L.b0 = R.bx_off[li];
+  L.nb = R.bx_off[li + 1] - L.b0;
+  L.dr = R.lv_dr[li];
+  return L;
+}
+
+// Red-black Gauss-Seidel half-sweep `it` on level lvl (box_gsrb_lpl,
+// m_aX_mg.f90:636-659; box_gsrb_clpl :998-1024). Ghost neighbours are
+// evaluated from their sources, which equals the ghost fill the reference
+// performs after every half-sweep (gsrb_boxes, :343-366): those sources are
+// cells of the colour not updated here, the updated cell itself (read before
+// it is written), or coarser-level cells. mem: read ghosts from memory
+// instead (first half-sweep of a first FMG call, where the reference's
+// ghosts are not consistent with the interior).
+__device__ void p_sweep(const RunDev &R, const MGV &M, int lvl, int it, bool mem) {
+  const LvlInfo L = lvl_info(R, lvl);
+  double *phi = M.phi;
+  const double *rhs = M.rhs;
+  const double dx2 = L.dr * L.dr;
+  const int half = (L.nc * L.nc) >> 1, hsh = 2 * L.sh - 1, hn = L.nc >> 1;
+  const int p = it & 1;  // parity (i + j) & 1 of the updated cells
   const bool cyl = R.coord == 1;
-  for (int k = a + threadIdx.x; k < b; k += NTHR) {
-    const CellRec c = R.cells[k];
+  const int n = L.nb * half;
+  for (int k = threadIdx.x; k < n; k += NTHR) {
+    const BoxRec &B = M.boxes[L.b0 + (k >> hsh)];
+    const int t = k & (half - 1);
+    const int j = t / hn + 1, m = t % hn;
+    const int i = 2 * m + 2 - ((p + j) & 1);
+    const int g = B.base + i + L.ncg * j;
     double lx, hx, ly, hy;
     if (mem) {
-      lx = phi[c.g - 1]; hx = phi[c.g + 1]; ly = phi[c.g - ncg]; hy = phi[c.g + ncg];
+      lx = phi[g - 1]; hx = phi[g + 1]; ly = phi[g - L.ncg]; hy = phi[g + L.ncg];
     } else {
-      lx = nbv(R, phi, c.nb[0], gl); hx = nbv(R, phi, c.nb[1], gl);
-      ly = nbv(R, phi, c.nb[2], gl); hy = nbv(R, phi, c.nb[3], gl);
+      phi_nbrs(R, phi, B, L.nc, L.ncg, i, j, g, lx, hx, ly, hy);
     }
-    const double r = rhs[c.g];
+    const double r = rhs[g];
     if (cyl) {
-      const double den = c.gi - 0.5;
-      const double rf1 = (c.gi - 1) / den, rf2 = c.gi / den;
-      phi[c.g] = 0.25 * (rf1 * lx + rf2 * hx + hy + ly - dx2 * r);
+      const int gi = B.gi0 + i;
+      const double den = gi - 0.5;
+      const double rf1 = (gi - 1) / den, rf2 = gi / den;
+      phi[g] = 0.25 * (rf1 * lx + rf2 * hx + hy + ly - dx2 * r);
     } else {
-      phi[c.g] = 0.25 * (hx + lx + hy + ly - dx2 * r);
+      phi[g] = 0.25 * (hx + lx + hy + ly - dx2 * r);
     }
   }
   __syncthreads();
 }
 
-// Ghost fill of the potential on level index li (fill_gc_phi, :303-316), no
+// Ghost fill of the potential on level lvl (fill_gc_phi, :303-316), no
 // barrier. copy_tmp: also tmp = phi on the ghosts of parent boxes (the
 // whole-box copy of update_coarse, :407).
-__device__ __forceinline__ void fill_phi_loop(const RunDev &R, int li, bool copy_tmp) {
-  const GhostRec *gl = R.gphi + R.gphi_off[li];
-  const int n = R.gphi_off[li + 1] - R.gphi_off[li];
-  double *phi = VAR(R, MP), *tmp = VAR(R, MT);
+__device__ __forceinline__ void fill_phi_loop(const RunDev &R, const MGV &M, const LvlInfo &L, bool copy_tmp) {
+  double *phi = M.phi, *tmp = M.tmp;
+  const int per = 4 * L.nc, n = L.nb * per;
   for (int k = threadIdx.x; k < n; k += NTHR) {
-    const GhostRec r = gl[k];
-    const double v = recipe_phi(R, phi, r);
-    phi[r.dst] = v;
-    if (copy_tmp && (r.kind & GK_PARENT)) tmp[r.dst] = v;
+    const BoxRec &B = M.boxes[L.b0 + k / per];
+    const int r = k % per, side = r >> L.sh, kk = (r & (L.nc - 1)) + 1;
+    const double v = phi_ghost(R, phi, B, L.nc, L.ncg, side, kk);
+    const int dim = side >> 1, gx = (side & 1) ? L.nc + 1 : 0;
+    const int d = B.base + (dim == 0 ? gx + L.ncg * kk : kk + L.ncg * gx);
+    phi[d] = v;
+    if (copy_tmp && (B.flags & CF_PARENT)) tmp[d] = v;
   }
 }
-__device__ void p_fill(const RunDev &R, int lvl) {
-  fill_phi_loop(R, lvl - R.min_lvl, false);
+__device__ void p_fill(const RunDev &R, const MGV &M, int lvl) {
+  fill_phi_loop(R, M, lvl_info(R, lvl), false);
   __syncthreads();
 }
 
 // For every box of level lvl: the residual rhs - A phi (residual_box,
 // :475-484) restricted into the parent's tmp and phi restricted into the
-// parent's phi (box_rstr_lpl, :683-705); the ghosts of level lvl are filled in
-// the same phase (the residual takes ghost neighbours from the recipes).
-// leaf_rhs: first set the space charge e/eps0 (n_e - n_i) on leaf cells
-// (src/streamer_2d.f90:317-329). store_res: keep the residual in the box's
-// own tmp (set_coarse_phi_rhs); otherwise tmp is left as it was
+// parent's phi (box_rstr_lpl, :683-705); fill: the ghosts of level lvl are
+// filled in the same phase (the residual evaluates ghost neighbours from
+// their sources). leaf_rhs: first set the space charge e/eps0 (n_e - n_i) on
+// leaf cells (src/streamer_2d.f90:317-329). store_res: keep the residual in
+// the box's own tmp (set_coarse_phi_rhs); otherwise tmp is left as it was
 // (update_coarse saves and restores it).
-__device__ void p_fr(const RunDev &R, int lvl, bool fill, bool leaf_rhs, bool store_res) {
-  const int li = lvl - R.min_lvl;
-  const FrRec *fr = R.fr + R.fr_off[li];
-  const int n = R.fr_off[li + 1] - R.fr_off[li];
-  double *phi = VAR(R, MP), *tmp = VAR(R, MT), *rhs = VAR(R, MR);
+__device__ void p_fr(const RunDev &R, const MGV &M, int lvl, bool fill, bool leaf_rhs, bool store_res) {
+  const LvlInfo L = lvl_info(R, lvl);
+  const int pncg = R.lv_nc[lvl - 1 - R.min_lvl] + 2;
+  double *phi = M.phi, *tmp = M.tmp, *rhs = M.rhs;
   const double *e = VAR(R, I_ELEC), *pi = VAR(R, I_PION);
-  const GhostRec *gl = R.gphi + R.gphi_off[li];
-  const double dr = R.lv_dr[li], inv_dr_sq = 1 / (dr * dr);
+  const double inv_dr_sq = 1 / (L.dr * L.dr);
   const double fac = UC_ELEM_CHARGE / UC_EPS0;
+  const int hn = L.nc >> 1, per = hn * hn, n = L.nb * per;
   for (int k = threadIdx.x; k < n; k += NTHR) {
-    const FrRec rec = fr[k];
+    const BoxRec &B = M.boxes[L.b0 + k / per];
+    const int t = k % per, ii = t % hn + 1, jj = t / hn + 1;
+    const bool leaf = leaf_rhs && (B.flags & CF_LEAF);
     double rs[4], ps[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) {
-      const CellRec c = R.cells[rec.c[q]];
+      const int i = 2 * ii - 1 + (q & 1), j = 2 * jj - 1 + (q >> 1);
+      const int g = B.base + i + L.ncg * j;
       double rh;
-      if (leaf_rhs && (c.flags & CF_LEAF)) {
-        rh = fac * (e[c.g] - pi[c.g]);
-        rhs[c.g] = rh;
+      if (leaf) {
+        const int gg = B.gbase + i + L.ncg * j;
+        rh = fac * (e[gg] - pi[gg]);
+        rhs[g] = rh;
       } else {
-        rh = rhs[c.g];
+        rh = rhs[g];
       }
-      const double res = rh - lap_at(R, phi, c, gl, inv_dr_sq);
-      if (store_res) tmp[c.g] = res;
+      const double res = rh - lap_at(R, phi, B, L.nc, L.ncg, i, j, inv_dr_sq);
+      if (store_res) tmp[g] = res;
       rs[q] = res;
-      ps[q] = phi[c.g];
+      ps[q] = phi[g];
     }
-    tmp[rec.dst] = 0.25 * (rs[0] + rs[1] + rs[2] + rs[3]);
-    phi[rec.dst] = 0.25 * (ps[0] + ps[1] + ps[2] + ps[3]);
+    const int d = B.pbase + (B.o0 + ii) + pncg * (B.o1 + jj);
+    tmp[d] = 0.25 * (rs[0] + rs[1] + rs[2] + rs[3]);
+    phi[d] = 0.25 * (ps[0] + ps[1] + ps[2] + ps[3]);
   }
-  if (fill) fill_phi_loop(R, li, false);
+  if (fill) fill_phi_loop(R, M, L, false);
   __syncthreads();
 }
 
 // Ghost fill of level lvl and the coarse right-hand side of its parent
 // boxes: rhs = A phi + tmp (box_op then a$D_box_add_cc, :399-402 / :441-444);
 // copy_tmp: then tmp = phi (a$D_box_copy_cc, :403).
-__device__ void p_fc(const RunDev &R, int lvl, bool copy_tmp) {
+__device__ void p_fc(const RunDev &R, const MGV &M, int lvl, bool copy_tmp) {
+  const LvlInfo L = lvl_info(R, lvl);
   const int li = lvl - R.min_lvl;
-  const int *pc = R.pcells + R.pcell_off[li];
-  const int n = R.pcell_off[li + 1] - R.pcell_off[li];
-  double *phi = VAR(R, MP), *tmp = VAR(R, MT), *rhs = VAR(R, MR);
-  const GhostRec *gl = R.gphi + R.gphi_off[li];
-  const double dr = R.lv_dr[li], inv_dr_sq = 1 / (dr * dr);
+  const int *pb = M.pbx + R.pb_off[li];
+  const int npb = R.pb_off[li + 1] - R.pb_off[li];
+  double *phi = M.phi, *tmp = M.tmp, *rhs = M.rhs;
+  const double inv_dr_sq = 1 / (L.dr * L.dr);
+  const int per = L.nc * L.nc, n = npb * per;
   for (int k = threadIdx.x; k < n; k += NTHR) {
-    const CellRec c = R.cells[pc[k]];
-    const double a = lap_at(R, phi, c, gl, inv_dr_sq);
-    rhs[c.g] = a + tmp[c.g];
-    if (copy_tmp) tmp[c.g] = phi[c.g];
+    const BoxRec &B = M.boxes[pb[k >> (2 * L.sh)]];
+    const int t = k & (per - 1), i = (t & (L.nc - 1)) + 1, j = (t >> L.sh) + 1;
+    const int g = B.base + i + L.ncg * j;
+    const double a = lap_at(R, phi, B, L.nc, L.ncg, i, j, inv_dr_sq);
+    const double pv = phi[g];
+    rhs[g] = a + tmp[g];
+    if (copy_tmp) tmp[g] = pv;
   }
-  fill_phi_loop(R, li, copy_tmp);
+  fill_phi_loop(R, M, L, copy_tmp);
   __syncthreads();
 }
 
@@ -692,26 +778,34 @@ __device__ void p_fc(const RunDev &R, int lvl, bool copy_tmp) {
 // (correct_children :319-341 with box_corr_lpl :605-633). The correction
 // phi_p - tmp_p is formed where it is used instead of being stored back into
 // the parent's tmp; that stored value is never read again by the reference.
-__device__ void p_correct(const RunDev &R, int lvl, bool copy, bool correct) {
-  const int li = lvl - R.min_lvl;
-  const int a = R.cell_off[li], b = R.cell_off[li + 1];
-  double *phi = VAR(R, MP), *tmp = VAR(R, MT);
-  for (int k = a + threadIdx.x; k < b; k += NTHR) {
-    const CellRec c = R.cells[k];
-    const double v = phi[c.g];
-    if (copy) tmp[c.g] = v;
+__device__ void p_correct(const RunDev &R, const MGV &M, int lvl, bool copy, bool correct) {
+  const LvlInfo L = lvl_info(R, lvl);
+  const int pncg = correct ? R.lv_nc[lvl - 1 - R.min_lvl] + 2 : 0;
+  double *phi = M.phi, *tmp = M.tmp;
+  const int per = L.nc * L.nc, n = L.nb * per;
+  for (int k = threadIdx.x; k < n; k += NTHR) {
+    const BoxRec &B = M.boxes[L.b0 + (k >> (2 * L.sh))];
+    const int t = k & (per - 1), i = (t & (L.nc - 1)) + 1, j = (t >> L.sh) + 1;
+    const int g = B.base + i + L.ncg * j;
+    const double v = phi[g];
+    if (copy) tmp[g] = v;
     if (correct) {
-      const double c1 = phi[c.pc[0]] - tmp[c.pc[0]];
-      const double c2x = phi[c.pc[1]] - tmp[c.pc[1]];
-      const double c2y = phi[c.pc[2]] - tmp[c.pc[2]];
-      phi[c.g] = v + 0.5 * c1 + 0.25 * (c2x + c2y);
+      const int i_c1 = B.o0 + ((i + 1) >> 1), i_c2 = i_c1 + 1 - 2 * (i & 1);
+      const int j_c1 = B.o1 + ((j + 1) >> 1), j_c2 = j_c1 + 1 - 2 * (j & 1);
+      const int p1 = B.pbase + i_c1 + pncg * j_c1;
+      const int p2 = B.pbase + i_c2 + pncg * j_c1;
+      const int p3 = B.pbase + i_c1 + pncg * j_c2;
+      const double c1 = phi[p1] - tmp[p1], c2x = phi[p2] - tmp[p2], c2y = phi[p3] - tmp[p3];
+      phi[g] = v + 0.5 * c1 + 0.25 * (c2x + c2y);
     }
   }
   if (copy) {
-    const GhostRec *gl = R.gphi + R.gphi_off[li];
-    const int n = R.gphi_off[li + 1] - R.gphi_off[li];
-    for (int k = threadIdx.x; k < n; k += NTHR) {
-      const int d = gl[k].dst;
+    const int pg = 4 * L.nc, ng = L.nb * pg;
+    for (int k = threadIdx.x; k < ng; k += NTHR) {
+      const BoxRec &B = M.boxes[L.b0 + k / pg];
+      const int r = k % pg, side = r >> L.sh, kk = (r & (L.nc - 1)) + 1;
+      const int dim = side >> 1, gx = (side & 1) ? L.nc + 1 : 0;
+      const int d = B.base + (dim == 0 ? gx + L.ncg * kk : kk + L.ncg * gx);
       tmp[d] = phi[d];
     }
   }
@@ -720,47 +814,50 @@ __device__ void p_correct(const RunDev &R, int lvl, bool copy, bool correct) {
 
 // init_phi_rhs for one level (m_aX_mg.f90:450-473): phi = 0 on the boxes of
 // level lvl and their rhs restricted to the parents.
-__device__ void p_init_level(const RunDev &R, int lvl, bool leaf_rhs) {
-  const int li = lvl - R.min_lvl;
-  const FrRec *fr = R.fr + R.fr_off[li];
-  const int n = R.fr_off[li + 1] - R.fr_off[li];
-  double *rhs = VAR(R, MR), *phi = VAR(R, MP);
+__device__ void p_init_level(const RunDev &R, const MGV &M, int lvl, bool leaf_rhs) {
+  const LvlInfo L = lvl_info(R, lvl);
+  const int pncg = R.lv_nc[lvl - 1 - R.min_lvl] + 2;
+  double *rhs = M.rhs, *phi = M.phi;
   const double *e = VAR(R, I_ELEC), *pi = VAR(R, I_PION);
   const double fac = UC_ELEM_CHARGE / UC_EPS0;
+  const int hn = L.nc >> 1, per = hn * hn, n = L.nb * per;
   for (int k = threadIdx.x; k < n; k += NTHR) {
-    const FrRec rec = fr[k];
+    const BoxRec &B = M.boxes[L.b0 + k / per];
+    const int t = k % per, ii = t % hn + 1, jj = t / hn + 1;
+    const bool leaf = leaf_rhs && (B.flags & CF_LEAF);
     double rs[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) {
-      const CellRec c = R.cells[rec.c[q]];
-      if (leaf_rhs && (c.flags & CF_LEAF)) {
-        rs[q] = fac * (e[c.g] - pi[c.g]);
-        rhs[c.g] = rs[q];
+      const int loc = (2 * ii - 1 + (q & 1)) + L.ncg * (2 * jj - 1 + (q >> 1));
+      const int g = B.base + loc;
+      if (leaf) {
+        rs[q] = fac * (e[B.gbase + loc] - pi[B.gbase + loc]);
+        rhs[g] = rs[q];
       } else {
-        rs[q] = rhs[c.g];
+        rs[q] = rhs[g];
       }
     }
-    rhs[rec.dst] = 0.25 * (rs[0] + rs[1] + rs[2] + rs[3]);
+    rhs[B.pbase + (B.o0 + ii) + pncg * (B.o1 + jj)] = 0.25 * (rs[0] + rs[1] + rs[2] + rs[3]);
   }
-  const int nb = list_n(R, 0, lvl);
-  const int *ids = list_p(R, 0, lvl);
-  const int cg = R.lv_nc[li] + 2, per = cg * cg;
-  for (int k = threadIdx.x; k < nb * per; k += NTHR) phi[(size_t)ids[k / per] * SLOT + k % per] = 0.0;
+  const int pc = L.ncg * L.ncg, nz = L.nb * pc;
+  for (int k = threadIdx.x; k < nz; k += NTHR) phi[M.boxes[L.b0 + k / pc].base + k % pc] = 0.0;
   __syncthreads();
 }
 
 // Residual rhs - A phi on every cell of levels min..max (set_residual of
 // mg$D_fas_vcycle, :243-253)
-__device__ void p_residual_all(const RunDev &R, int max_lvl) {
-  double *phi = VAR(R, MP), *tmp = VAR(R, MT);
-  const double *rhs = VAR(R, MR);
+__device__ void p_residual_all(const RunDev &R, const MGV &M, int max_lvl) {
+  double *phi = M.phi, *tmp = M.tmp;
+  const double *rhs = M.rhs;
   for (int lvl = R.min_lvl; lvl <= max_lvl; lvl++) {
-    const int li = lvl - R.min_lvl;
-    const GhostRec *gl = R.gphi + R.gphi_off[li];
-    const double dr = R.lv_dr[li], inv_dr_sq = 1 / (dr * dr);
-    for (int k = R.cell_off[li] + threadIdx.x; k < R.cell_off[li + 1]; k += NTHR) {
-      const CellRec c = R.cells[k];
-      tmp[c.g] = rhs[c.g] - lap_at(R, phi, c, gl, inv_dr_sq);
+    const LvlInfo L = lvl_info(R, lvl);
+    const double inv_dr_sq = 1 / (L.dr * L.dr);
+    const int per = L.nc * L.nc, n = L.nb * per;
+    for (int k = threadIdx.x; k < n; k += NTHR) {
+      const BoxRec &B = M.boxes[L.b0 + (k >> (2 * L.sh))];
+      const int t = k & (per - 1), i = (t & (L.nc - 1)) + 1, j = (t >> L.sh) + 1;
+      const int g = B.base + i + L.ncg * j;
+      tmp[g] = rhs[g] - lap_at(R, phi, B, L.nc, L.ncg, i, j, inv_dr_sq);
     }
   }
   __syncthreads();
@@ -770,65 +867,107 @@ __device__ void p_residual_all(const RunDev &R, int max_lvl) {
 // Phases per level: down: 4 half-sweeps, residual/restriction (+ ghost fill),
 // coarse ghost fill + rhs; base: 2 n_cycle_base half-sweeps + ghost fill;
 // up: correction, 4 half-sweeps, ghost fill.
-__device__ void p_vcycle(const RunDev &R, int max_lvl, bool stale_base) {
+__device__ void p_vcycle(const RunDev &R, const MGV &M, int max_lvl, bool stale_base) {
   const int min_lvl = R.min_lvl;
   for (int lvl = max_lvl; lvl >= min_lvl + 1; lvl--) {
-    for (int it = 1; it <= 4; it++) p_sweep(R, lvl, it, false);
-    p_fr(R, lvl, true, false, false);
-    p_fc(R, lvl - 1, true);
+    for (int it = 1; it <= 4; it++) p_sweep(R, M, lvl, it, false);
+    p_fr(R, M, lvl, true, false, false);
+    p_fc(R, M, lvl - 1, true);
   }
-  for (int it = 1; it <= 2 * R.n_cycle_base; it++) p_sweep(R, min_lvl, it, stale_base && it == 1);
-  p_fill(R, min_lvl);
+  for (int it = 1; it <= 2 * R.n_cycle_base; it++) p_sweep(R, M, min_lvl, it, stale_base && it == 1);
+  p_fill(R, M, min_lvl);
   for (int lvl = min_lvl + 1; lvl <= max_lvl; lvl++) {
-    p_correct(R, lvl, false, true);
-    for (int it = 1; it <= 4; it++) p_sweep(R, lvl, it, false);
-    p_fill(R, lvl);
+    p_correct(R, M, lvl, false, true);
+    for (int it = 1; it <= 4; it++) p_sweep(R, M, lvl, it, false);
+    p_fill(R, M, lvl);
   }
 }
 
 // mg$D_fas_fmg, m_aX_mg.f90:163-202. leaf_rhs: compute the space charge of
 // the leaves where it is first needed (compute_fld).
-__device__ void p_fmg(const RunDev &R, bool set_residual, bool first_call, bool leaf_rhs) {
+__device__ void p_fmg_in(const RunDev &R, const MGV &M, bool set_residual, bool first_call,
+                         bool leaf_rhs) {
   const int min_lvl = R.min_lvl, max_lvl = R.max_lvl;
   if (first_call) {
-    for (int lvl = max_lvl; lvl >= min_lvl + 1; lvl--) p_init_level(R, lvl, leaf_rhs);
+    for (int lvl = max_lvl; lvl >= min_lvl + 1; lvl--) p_init_level(R, M, lvl, leaf_rhs);
   } else {
     // set_coarse_phi_rhs for lvl = max..min+1 (:414-447)
     for (int lvl = max_lvl; lvl >= min_lvl + 1; lvl--) {
-      p_fr(R, lvl, lvl == max_lvl, leaf_rhs, true);
-      p_fc(R, lvl - 1, false);
+      p_fr(R, M, lvl, lvl == max_lvl, leaf_rhs, true);
+      p_fc(R, M, lvl - 1, false);
     }
   }
   for (int lvl = min_lvl; lvl <= max_lvl; lvl++) {
-    p_correct(R, lvl, true, lvl > min_lvl);
-    p_vcycle(R, lvl, first_call && lvl == min_lvl);
-    if (set_residual && lvl == max_lvl) p_residual_all(R, lvl);
+    p_correct(R, M, lvl, true, lvl > min_lvl);
+    p_vcycle(R, M, lvl, first_call && lvl == min_lvl);
+    if (set_residual && lvl == max_lvl) p_residual_all(R, M, lvl);
+  }
+}
+
+// Copy the multigrid variables of every box between device memory and the
+// compact shared-memory arrays (in: to shared memory).
+__device__ void stage_mg(const RunDev &R, const MGV &M, bool in) {
+  double *g[3] = {VAR(R, MP), VAR(R, MR), VAR(R, MT)};
+  double *s[3] = {M.phi, M.rhs, M.tmp};
+  for (int lvl = R.min_lvl; lvl <= R.max_lvl; lvl++) {
+    const int li = lvl - R.min_lvl;
+    const int ncg = R.lv_nc[li] + 2, per = ncg * ncg;
+    const int b0 = R.bx_off[li], n = (R.bx_off[li + 1] - b0) * per;
+    for (int k = threadIdx.x; k < n; k += NTHR) {
+      const BoxRec &B = M.boxes[b0 + k / per];
+      const int c = k % per;
+      for (int v = 0; v < 3; v++) {
+        if (in) s[v][B.base + c] = g[v][B.gbase + c];
+        else g[v][B.gbase + c] = s[v][B.base + c];
+      }
+    }
+  }
+  __syncthreads();
+}
+
+extern __shared__ double g_dsmem[];
+
+// mg$D_fas_fmg in shared memory when the tree fits (the three variables,
+// the box records and the parent-box list), else in device memory
+__device__ void p_fmg(const RunDev &R, bool set_residual, bool first_call, bool leaf_rhs) {
+  if (R.smem_doubles > 0) {
+    const int S = R.smem_doubles, nbx = R.bx_off[R.nlev], npb = R.pb_off[R.nlev];
+    BoxRec *sb = reinterpret_cast<BoxRec *>(g_dsmem + 3 * S);
+    int *spb = reinterpret_cast<int *>(sb + nbx);
+    {
+      const int4 *src = reinterpret_cast<const int4 *>(R.sboxes);
+      int4 *dst = reinterpret_cast<int4 *>(sb);
+      const int n4 = nbx * (int)(sizeof(BoxRec) / sizeof(int4));
+      for (int k = threadIdx.x; k < n4; k += NTHR) dst[k] = src[k];
+      for (int k = threadIdx.x; k < npb; k += NTHR) spb[k] = R.pbx[k];
+    }
+    __syncthreads();
+    MGV M{g_dsmem, g_dsmem + S, g_dsmem + 2 * S, sb, spb};
+    stage_mg(R, M, true);
+    p_fmg_in(R, M, set_residual, first_call, leaf_rhs);
+    stage_mg(R, M, false);
+  } else {
+    MGV M{VAR(R, MP), VAR(R, MR), VAR(R, MT), R.boxes, R.pbx};
+    p_fmg_in(R, M, set_residual, first_call, leaf_rhs);
   }
 }
 
 // a$D_gc_tree(iv, a$D_gc_interp[_lim], a$D_gc_neumann) for one or two
 // variables, levels ascending (m_aX_gc.f90:28-46, 90-330)
 __device__ void p_gc_den(const RunDev &R, int iv0, int iv1, bool lim) {
-  const double sixth = 1 / 6.0, third = 1 / 3.0;
   for (int lvl = R.min_lvl; lvl <= R.max_lvl; lvl++) {
-    const int li = lvl - R.min_lvl;
-    const GhostRec *gl = R.gden + R.gden_off[li];
-    const int n = R.gden_off[li + 1] - R.gden_off[li];
+    const LvlInfo L = lvl_info(R, lvl);
+    const int per = 4 * L.nc, n = L.nb * per;
     for (int k = threadIdx.x; k < n; k += NTHR) {
-      const GhostRec r = gl[k];
+      const BoxRec &B = R.boxes[L.b0 + k / per];
+      const int r = k % per, side = r >> L.sh, kk = (r & (L.nc - 1)) + 1;
+      const int dim = side >> 1, gx = (side & 1) ? L.nc + 1 : 0;
+      const int d = B.base + (dim == 0 ? gx + L.ncg * kk : kk + L.ncg * gx);
       for (int w = 0; w < 2; w++) {
         const int iv = w == 0 ? iv0 : iv1;
         if (iv < 0) continue;
         double *x = VAR(R, iv);
-        double v;
-        if ((r.kind & 0xff) == GK_INTERP) {
-          const double c1 = x[r.s[0]], c2 = x[r.s[1]];
-          v = 0.5 * c1 + sixth * c2 + third * x[r.s[2]];
-          if (lim && v > 2 * c1) v = 2 * c1;
-        } else {
-          v = x[r.s[0]];
-        }
-        x[r.dst] = v;
+        x[d] = den_ghost(x, B, L.nc, L.ncg, side, kk, lim);
       }
     }
     __syncthreads();
@@ -836,23 +975,43 @@ __device__ void p_gc_den(const RunDev &R, int iv0, int iv1, bool lim) {
 }
 
 // a$D_restrict_tree for one or two variables, levels descending
-// (afivo/src/m_aX_restrict.f90:54-142; cylindrical weights :95-113)
+// (afivo/src/m_aX_restrict.f90:54-142; cylindrical weights :95-113 with the
+// radius evaluated at the child-local index [i, j] as in :104)
 __device__ void p_restrict(const RunDev &R, int iv0, int iv1) {
   const bool cyl = R.coord == 1;
   for (int lvl = R.max_lvl - 1; lvl >= R.min_lvl; lvl--) {
+    const LvlInfo L = lvl_info(R, lvl);
     const int li = lvl - R.min_lvl;
-    const RstRec *rr = R.rst + R.rst_off[li];
-    const int n = R.rst_off[li + 1] - R.rst_off[li];
+    const int *pb = R.pbx + R.pb_off[li];
+    const int npb = R.pb_off[li + 1] - R.pb_off[li];
     const int cg = R.lv_nc[li + 1] + 2;
+    const int per = L.nc * L.nc, n = npb * per;
     for (int k = threadIdx.x; k < n; k += NTHR) {
-      const RstRec r = rr[k];
+      const BoxRec &P = R.boxes[pb[k >> (2 * L.sh)]];
+      const int t = k & (per - 1), ic = (t & (L.nc - 1)) + 1, jc = (t >> L.sh) + 1;
+      int q = 0, i = ic, j = jc;
+      if (P.ch[1] != 0) {  // four children, each covering a quadrant
+        const int h = L.nc >> 1;
+        const int qx = ic > h, qy = jc > h;
+        q = qx + 2 * qy;
+        i = ic - qx * h;
+        j = jc - qy * h;
+      }
+      const int src = P.ch[q] + (2 * i - 1) + cg * (2 * j - 1);
+      const int d = P.base + ic + L.ncg * jc;
       for (int w = 0; w < 2; w++) {
         const int iv = w == 0 ? iv0 : iv1;
         if (iv < 0) continue;
         double *x = VAR(R, iv);
-        const double a = x[r.src], b = x[r.src + 1], c = x[r.src + cg], d = x[r.src + cg + 1];
-        x[r.dst] = cyl ? (0.25 - r.rfac) * (a + c) + (0.25 + r.rfac) * (b + d)
-                       : 0.25 * (a + b + c + d);
+        const double a = x[src], b = x[src + 1], c = x[src + cg], dd = x[src + cg + 1];
+        if (cyl) {
+          const double dr16 = 0.0625 * P.dr;
+          const double r = P.r0 + (i - 0.5) * P.dr;
+          const double rfac = dr16 / r;
+          x[d] = (0.25 - rfac) * (a + c) + (0.25 + rfac) * (b + dd);
+        } else {
+          x[d] = 0.25 * (a + b + c + dd);
+        }
       }
     }
     __syncthreads();
@@ -875,25 +1034,28 @@ __device__ __forceinline__ double face_fld(const double *phi, const double *eps,
 __device__ void p_fld_from_pot(const RunDev &R) {
   const double *phi = VAR(R, I_PHI), *eps = VAR(R, I_EPS);
   double *fld = VAR(R, I_FLD);
-  const int a = R.cell_off[0], b = R.cell_off[R.nlev];
-  for (int k = a + threadIdx.x; k < b; k += NTHR) {
-    const CellRec c = R.cells[k];
-    const int li = c.li;
-    const int nc = R.lv_nc[li], ncg = nc + 2;
-    const double inv_dr = 1 / R.lv_dr[li];
-    const int id = c.g / SLOT, loc = c.g - id * SLOT;
-    const int i = loc % ncg, j = loc / ncg;
-    const double fxl = face_fld(phi, eps, c.g, 1, i, nc, inv_dr);
-    const double fxh = face_fld(phi, eps, c.g + 1, 1, i + 1, nc, inv_dr);
-    const double fyl = face_fld(phi, eps, c.g, ncg, j, nc, inv_dr);
-    const double fyh = face_fld(phi, eps, c.g + ncg, ncg, j + 1, nc, inv_dr);
-    double *fxf = FX(R, F_FLD, id), *fyf = FY(R, F_FLD, id);
-    fxf[fxi(i, j, nc)] = fxl;
-    if (i == nc) fxf[fxi(nc + 1, j, nc)] = fxh;
-    fyf[fyi(i, j, nc)] = fyl;
-    if (j == nc) fyf[fyi(i, nc + 1, nc)] = fyh;
-    const double sx = fxl + fxh, sy = fyl + fyh;
-    fld[c.g] = sqrt(0.25 * (sx * sx) + 0.25 * (sy * sy));
+  for (int lvl = R.min_lvl; lvl <= R.max_lvl; lvl++) {
+    const LvlInfo L = lvl_info(R, lvl);
+    const double inv_dr = 1 / L.dr;
+    const int per = L.nc * L.nc, n = L.nb * per;
+    for (int k = threadIdx.x; k < n; k += NTHR) {
+      const BoxRec &B = R.boxes[L.b0 + (k >> (2 * L.sh))];
+      const int t = k & (per - 1), i = (t & (L.nc - 1)) + 1, j = (t >> L.sh) + 1;
+      const int g = B.base + i + L.ncg * j;
+      const int nc = L.nc, ncg = L.ncg;
+      const double fxl = face_fld(phi, eps, g, 1, i, nc, inv_dr);
+      const double fxh = face_fld(phi, eps, g + 1, 1, i + 1, nc, inv_dr);
+      const double fyl = face_fld(phi, eps, g, ncg, j, nc, inv_dr);
+      const double fyh = face_fld(phi, eps, g + ncg, ncg, j + 1, nc, inv_dr);
+      const int id = B.base / SLOT;
+      double *fxf = FX(R, F_FLD, id), *fyf = FY(R, F_FLD, id);
+      fxf[fxi(i, j, nc)] = fxl;
+      if (i == nc) fxf[fxi(nc + 1, j, nc)] = fxh;
+      fyf[fyi(i, j, nc)] = fyl;
+      if (j == nc) fyf[fyi(i, nc + 1, nc)] = fyh;
+      const double sx = fxl + fxh, sy = fyl + fyh;
+      fld[g] = sqrt(0.25 * (sx * sx) + 0.25 * (sy * sy));
+    }
   }
   __syncthreads();
   p_gc_den(R, I_FLD, -1, false);
@@ -1132,6 +1294,77 @@ __device__ void run_op(const RunDev &R, const Op &op) {
     case OP_REF_FLAGS: ref_flags(R, op.d0); break;
     case OP_PROLONG_NEW: prolong_new(R); break;
     case OP_STEP: step(R, op.d0); break;
+    case OP_DBG_BARRIERS:
+      for (int k = 0; k < op.i0; k++) __syncthreads();
+      break;
+    case OP_DBG_SWEEPS:
+    case OP_DBG_FILLS: {
+      MGV M{VAR(R, MP), VAR(R, MR), VAR(R, MT), R.boxes, R.pbx};
+      if (R.smem_doubles > 0 && op.i2) {
+        const int S = R.smem_doubles, nbx = R.bx_off[R.nlev], npb = R.pb_off[R.nlev];
+        BoxRec *sb = reinterpret_cast<BoxRec *>(g_dsmem + 3 * S);
+        int *spb = reinterpret_cast<int *>(sb + nbx);
+        const int4 *src = reinterpret_cast<const int4 *>(R.sboxes);
+        int4 *dst = reinterpret_cast<int4 *>(sb);
+        for (int k = threadIdx.x; k < nbx * 6; k += NTHR) dst[k] = src[k];
+        for (int k = threadIdx.x; k < npb; k += NTHR) spb[k] = R.pbx[k];
+        __syncthreads();
+        M = MGV{g_dsmem, g_dsmem + S, g_dsmem + 2 * S, sb, spb};
+        stage_mg(R, M, true);
+      }
+      for (int k = 0; k < op.i0; k++) {
+        if (op.code == OP_DBG_SWEEPS) p_sweep(R, M, op.i1, k + 1, false);
+        else p_fill(R, M, op.i1);
+      }
+      break;
+    }
+    case OP_DBG_EMPTY: {
+      // timestamps along one sweep item of level op.i1 (thread 0)
+      const LvlInfo L = lvl_info(R, op.i1);
+      MGV M{VAR(R, MP), VAR(R, MR), VAR(R, MT), R.boxes, R.pbx};
+      if (R.smem_doubles > 0 && op.i2) {
+        const int S = R.smem_doubles, nbx = R.bx_off[R.nlev], npb = R.pb_off[R.nlev];
+        BoxRec *sb = reinterpret_cast<BoxRec *>(g_dsmem + 3 * S);
+        int *spb = reinterpret_cast<int *>(sb + nbx);
+        const int4 *src = reinterpret_cast<const int4 *>(R.sboxes);
+        int4 *dst = reinterpret_cast<int4 *>(sb);
+        for (int k = threadIdx.x; k < nbx * 6; k += NTHR) dst[k] = src[k];
+        for (int k = threadIdx.x; k < npb; k += NTHR) spb[k] = R.pbx[k];
+        __syncthreads();
+        M = MGV{g_dsmem, g_dsmem + S, g_dsmem + 2 * S, sb, spb};
+        stage_mg(R, M, true);
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        long long t[8];
+        double *phi = M.phi;
+        t[0] = clock64();
+        const LvlInfo L2 = lvl_info(R, op.i1);
+        t[1] = clock64();
+        const BoxRec &B = M.boxes[L2.b0];
+        const int base = B.base;
+        t[2] = clock64();
+        const int g = base + 1 + L.ncg * 1;
+        double lx, hx, ly, hy;
+        phi_nbrs(R, phi, B, L.nc, L.ncg, 1, 1, g, lx, hx, ly, hy);
+        t[3] = clock64();
+        const double r = M.rhs[g];
+        phi[g] = 0.25 * (hx + lx + hy + ly - L.dr * L.dr * r);
+        t[4] = clock64();
+        double v = phi[g];
+        t[5] = clock64();
+        v = v * 1.0000001 + 0.5;
+        v = v * 1.0000001 + 0.5;
+        v = v * 1.0000001 + 0.5;
+        v = v * 1.0000001 + 0.5;
+        t[6] = clock64();
+        R.scal[8] = v;
+        t[7] = clock64();
+        for (int q = 0; q < 7; q++) R.scal[9 + q] = (double)(t[q + 1] - t[q]);
+      }
+      __syncthreads();
+      break;
+    }
     default: if (threadIdx.x == 0) atomicExch(R.status, A5G_EINVAL);
   }
 }
@@ -1234,259 +1467,103 @@ struct a5g_ctx {
   long long n_leaf_cells = 0;
   int min_lvl = 0, max_lvl = 0;
   // plan storage
-  CellRec *p_cells = nullptr;
-  GhostRec *p_gphi = nullptr, *p_gden = nullptr;
-  RstRec *p_rst = nullptr;
-  FrRec *p_fr = nullptr;
-  int *p_pcells = nullptr;
-  size_t cap_cells = 0, cap_gphi = 0, cap_gden = 0, cap_rst = 0, cap_fr = 0, cap_pcells = 0;
+  BoxRec *p_sboxes = nullptr;
+  size_t cap_sboxes = 0;
+  size_t dyn_smem = 0;  // dynamic shared memory per launch (bytes)
+  BoxRec *p_boxes = nullptr;
+  int *p_pbx = nullptr;
+  size_t cap_boxes = 0, cap_pbx = 0;
 };
 
 // ---------------------------------------------------------------------------
-// Plan builder: resolves, per level, every index the plan-based phases use
-// (see the device section "Plan-based operations").
-struct HostPlans {
-  std::vector<CellRec> cells;
-  std::vector<GhostRec> gphi, gden;
-  std::vector<RstRec> rst;
-  std::vector<FrRec> fr;
-  std::vector<int> pcells;
-  int cell_off[MAXLEV + 1], cell_split[MAXLEV], gphi_off[MAXLEV + 1], gden_off[MAXLEV + 1];
-  int rst_off[MAXLEV + 1], fr_off[MAXLEV + 1], pcell_off[MAXLEV + 1];
-  int lv_nc[MAXLEV];
-  double lv_dr[MAXLEV];
-};
-
-static void host_child_offset(const BoxMeta &m, int nb, int &o0, int &o1) {
-  static const int dix[4][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}};
-  if (m.lvl > 1) {
-    o0 = ((m.ix0 - 1) & 1) * (m.nc >> 1);
-    o1 = ((m.ix1 - 1) & 1) * (m.nc >> 1);
-    if (nb >= 0) { o0 -= dix[nb][0] * m.nc; o1 -= dix[nb][1] * m.nc; }
-  } else {
-    o0 = o1 = 0;
-    if (nb >= 0) { o0 -= dix[nb][0] * (m.nc >> 1); o1 -= dix[nb][1] * (m.nc >> 1); }
-  }
-}
-
+// Plan builder: one BoxRec per box, level by level in list order, and the
+// indices of the parent boxes per level (see "Plan-based operations").
 // Leaf / parent status is list membership, as in every box loop of the
 // reference (lvl_t%leaves / %parents), not "has children": the two differ on
 // level lvls_max, whose lists a$D_adjust_refinement never rebuilds
 // (afivo/src/m_aX_core.f90:478-515 calls set_leaves_parents for levels below
 // lvls_max and for max_lvl+1 only).
+struct HostPlans {
+  std::vector<BoxRec> boxes, sboxes;
+  int smem_doubles = 0;  // doubles per variable of the compact shared-memory copy
+  std::vector<int> pbx;
+  int bx_off[MAXLEV + 1], pb_off[MAXLEV + 1];
+  int lv_nc[MAXLEV];
+  double lv_dr[MAXLEV];
+};
+
+static void host_child_offset(const BoxMeta &m, int &o0, int &o1) {
+  if (m.lvl > 1) {
+    o0 = ((m.ix0 - 1) & 1) * (m.nc >> 1);
+    o1 = ((m.ix1 - 1) & 1) * (m.nc >> 1);
+  } else {
+    o0 = o1 = 0;
+  }
+}
+
 static void build_plans(const std::vector<BoxMeta> &hm, const std::vector<std::vector<int>> &ids,
                         const std::vector<std::vector<int>> &leaves,
                         const std::vector<std::vector<int>> &parents, int min_lvl, int nlev,
-                        double dr_base, int coord, HostPlans &P) {
+                        double dr_base, HostPlans &P) {
   std::vector<char> is_leaf(hm.size(), 0), is_parent(hm.size(), 0);
   for (const auto &v : leaves)
     for (int id : v) is_leaf[id] = 1;
   for (const auto &v : parents)
     for (int id : v) is_parent[id] = 1;
-  static const int ch_dix[4][2] = {{0, 0}, {1, 0}, {0, 1}, {1, 1}};
-  P.cells.clear(); P.gphi.clear(); P.gden.clear(); P.rst.clear(); P.fr.clear(); P.pcells.clear();
-  auto G = [&](int id, int i, int j) { return id * SLOT + i + (hm[id].nc + 2) * j; };
+  P.boxes.clear();
+  P.pbx.clear();
   for (int li = 0; li < nlev; li++) {
     const int lvl = min_lvl + li;
     const int nc = lvl >= 1 ? NC : (NC >> (1 - lvl));
     P.lv_nc[li] = nc;
     P.lv_dr[li] = ids[li].empty() ? dr_base * std::pow(0.5, lvl - 1) : hm[ids[li][0]].dr;
-    P.cell_off[li] = (int)P.cells.size();
-    P.gphi_off[li] = (int)P.gphi.size();
-    P.gden_off[li] = (int)P.gden.size();
-    P.rst_off[li] = (int)P.rst.size();
-    P.fr_off[li] = (int)P.fr.size();
-    P.pcell_off[li] = (int)P.pcells.size();
-    const std::vector<int> &L = ids[li];
-    const int nbx = (int)L.size();
-    // ghost recipes, index (b, nb, k-1) -> b * 4 nc + nb nc + k-1
-    for (int b = 0; b < nbx; b++) {
-      const int id = L[b];
+    P.bx_off[li] = (int)P.boxes.size();
+    P.pb_off[li] = (int)P.pbx.size();
+    for (int id : ids[li]) {
       const BoxMeta &m = hm[id];
-      const bool parent = is_parent[id] != 0;
-      for (int nb = 0; nb < 4; nb++) {
-        const int dim = nb >> 1;
-        const bool low = (nb & 1) == 0;
-        const int nid = m.nb[nb];
-        for (int k = 1; k <= nc; k++) {
-          GhostRec gp{}, gd{};
-          int gi, gj;  // ghost cell
-          if (dim == 0) { gi = low ? 0 : nc + 1; gj = k; }
-          else { gi = k; gj = low ? 0 : nc + 1; }
-          gp.dst = gd.dst = G(id, gi, gj);
-          if (nid > 0) {
-            // sides_from_nb (m_aX_gc.f90:368-402)
-            int si = dim == 0 ? (low ? nc : 1) : k, sj = dim == 0 ? k : (low ? nc : 1);
-            gp.kind = gd.kind = GK_COPY;
-            gp.s[0] = gd.s[0] = G(nid, si, sj);
-          } else if (nid == 0) {
-            // mg$D_sides_rb after a$D_gc_prolong0 (m_aX_mg.f90:261-301)
-            int o0, o1;
-            host_child_offset(m, -1, o0, o1);
-            const int ix = low ? 1 : nc, di = low ? 1 : -1, dk = -1 + 2 * (k & 1);
-            const int ig = ix - di;
-            gp.kind = GK_RB;
-            if (dim == 0) {
-              gp.s[0] = G(m.parent, o0 + ((ig + 1) >> 1), o1 + ((k + 1) >> 1));
-              gp.s[1] = G(id, ix, k);
-              gp.s[2] = G(id, ix + di, k);
-              gp.s[3] = G(id, ix, k + dk);
-            } else {
-              gp.s[0] = G(m.parent, o0 + ((k + 1) >> 1), o1 + ((ig + 1) >> 1));
-              gp.s[1] = G(id, k, ix);
-              gp.s[2] = G(id, k + dk, ix);
-              gp.s[3] = G(id, k, ix + di);
-            }
-            // a$D_gc_interp(_lim) from the parent's neighbour (m_aX_gc.f90:90-295)
-            int q0, q1;
-            host_child_offset(m, nb, q0, q1);
-            const int pn = hm[m.parent].nb[nb];
-            const int ix_f = low ? 1 : nc, ix_c = low ? nc : 1;
-            gd.kind = GK_INTERP;
-            if (dim == 0) {
-              const int j_c1 = q1 + ((k + 1) >> 1), j_c2 = j_c1 + 1 - 2 * (k & 1);
-              gd.s[0] = G(pn, ix_c, j_c1);
-              gd.s[1] = G(pn, ix_c, j_c2);
-              gd.s[2] = G(id, ix_f, k);
-            } else {
-              const int i_c1 = q0 + ((k + 1) >> 1), i_c2 = i_c1 + 1 - 2 * (k & 1);
-              gd.s[0] = G(pn, i_c1, ix_c);
-              gd.s[1] = G(pn, i_c2, ix_c);
-              gd.s[2] = G(id, k, ix_f);
-            }
-          } else {
-            // physical boundary: sides_bc_pot (src/streamer_2d.f90:620-638)
-            // for the potential, a$D_gc_neumann for the densities and |E|
-            int si = dim == 0 ? (low ? 1 : nc) : k, sj = dim == 0 ? k : (low ? 1 : nc);
-            gp.s[0] = gd.s[0] = G(id, si, sj);
-            gd.kind = GK_COPY;
-            gp.kind = nb == 2 ? GK_NEG : (nb == 3 ? GK_APPLIED : GK_COPY);
-          }
-          if (parent) gp.kind |= GK_PARENT;
-          P.gphi.push_back(gp);
-          P.gden.push_back(gd);
-        }
+      BoxRec b{};
+      b.base = id * SLOT;
+      b.pbase = m.parent > 0 ? m.parent * SLOT : -1;
+      for (int s = 0; s < 4; s++) {
+        const int nid = m.nb[s];
+        b.nb[s] = nid > 0 ? nid * SLOT : (nid == 0 ? NBR_RB : NBR_PHYS);
+        const int pn = (nid == 0 && m.parent > 0) ? hm[m.parent].nb[s] : 0;
+        b.pnb[s] = pn > 0 ? pn * SLOT : 0;
       }
-    }
-    // cells, then ordered by colour (i + j) & 1
-    std::vector<CellRec> col[2];
-    std::vector<int> pos_box[2];  // box index, for the position map
-    for (int b = 0; b < nbx; b++) {
-      const int id = L[b];
-      const BoxMeta &m = hm[id];
-      const int gbase = P.gphi_off[li] + b * 4 * nc;
-      auto ghost_code = [&](int nb, int k) {
-        const GhostRec &r = P.gphi[gbase + nb * nc + (k - 1)];
-        switch (r.kind & 0xff) {
-          case GK_COPY: return r.s[0];
-          case GK_NEG: return (NBK_NEG << 28) | r.s[0];
-          case GK_APPLIED: return (NBK_APPLIED << 28) | r.s[0];
-          default: return (NBK_RECIPE << 28) | (gbase - P.gphi_off[li] + nb * nc + (k - 1));
-        }
-      };
-      int o0 = 0, o1 = 0, pg = 0;
-      if (lvl > min_lvl) {
-        host_child_offset(m, -1, o0, o1);
-        pg = hm[m.parent].nc + 2;
-      }
-      for (int j = 1; j <= nc; j++)
-        for (int i = 1; i <= nc; i++) {
-          CellRec c{};
-          c.g = G(id, i, j);
-          const int ncg = nc + 2;
-          c.nb[0] = i > 1 ? c.g - 1 : ghost_code(0, j);
-          c.nb[1] = i < nc ? c.g + 1 : ghost_code(1, j);
-          c.nb[2] = j > 1 ? c.g - ncg : ghost_code(2, i);
-          c.nb[3] = j < nc ? c.g + ncg : ghost_code(3, i);
-          if (lvl > min_lvl) {
-            const int i_c1 = o0 + ((i + 1) >> 1), i_c2 = i_c1 + 1 - 2 * (i & 1);
-            const int j_c1 = o1 + ((j + 1) >> 1), j_c2 = j_c1 + 1 - 2 * (j & 1);
-            const int pb = m.parent * SLOT;
-            c.pc[0] = pb + i_c1 + pg * j_c1;
-            c.pc[1] = pb + i_c2 + pg * j_c1;
-            c.pc[2] = pb + i_c1 + pg * j_c2;
-          }
-          c.gi = (m.ix0 - 1) * nc + i;
-          c.flags = is_leaf[id] ? CF_LEAF : 0;
-          c.li = li;
-          col[(i + j) & 1].push_back(c);
-          pos_box[(i + j) & 1].push_back(b);
-        }
-    }
-    // position map (b, i, j) -> absolute cell index
-    std::vector<int> pos((size_t)nbx * nc * nc);
-    {
-      int at = P.cell_off[li];
-      for (int p = 0; p < 2; p++) {
-        if (p == 1) P.cell_split[li] = at;
-        for (size_t q = 0; q < col[p].size(); q++, at++) {
-          const CellRec &c = col[p][q];
-          const int b = pos_box[p][q];
-          const int loc = c.g - L[b] * SLOT;
-          const int i = loc % (nc + 2), j = loc / (nc + 2);
-          pos[(size_t)b * nc * nc + (i - 1) + nc * (j - 1)] = at;
-          P.cells.push_back(c);
-        }
-      }
-    }
-    for (int b = 0; b < nbx; b++)
-      if (is_parent[L[b]])
-        for (int q = 0; q < nc * nc; q++) P.pcells.push_back(pos[(size_t)b * nc * nc + q]);
-    // residual-restriction records for the boxes of this level
-    if (lvl > min_lvl) {
-      for (int b = 0; b < nbx; b++) {
-        const BoxMeta &m = hm[L[b]];
-        int o0, o1;
-        host_child_offset(m, -1, o0, o1);
-        const int hnc = nc >> 1, pg = hm[m.parent].nc + 2;
-        for (int jj = 1; jj <= hnc; jj++)
-          for (int ii = 1; ii <= hnc; ii++) {
-            FrRec r{};
-            r.dst = m.parent * SLOT + (o0 + ii) + pg * (o1 + jj);
-            const int i_f = 2 * ii - 1, j_f = 2 * jj - 1;
-            const size_t base = (size_t)b * nc * nc;
-            r.c[0] = pos[base + (i_f - 1) + nc * (j_f - 1)];
-            r.c[1] = pos[base + (i_f) + nc * (j_f - 1)];
-            r.c[2] = pos[base + (i_f - 1) + nc * (j_f)];
-            r.c[3] = pos[base + (i_f) + nc * (j_f)];
-            P.fr.push_back(r);
-          }
-      }
-    }
-    // restriction records for the parents of this level
-    for (int pid : parents[li]) {
-      const BoxMeta &pm = hm[pid];
-      for (int jc = 1; jc <= nc; jc++)
-        for (int ic = 1; ic <= nc; ic++) {
-          for (int q = 0; q < 4; q++) {
-            const int cid = pm.ch[q];
-            if (cid == 0) continue;
-            const BoxMeta &cm = hm[cid];
-            int o0, o1;
-            host_child_offset(cm, -1, o0, o1);
-            const int hnc = cm.nc >> 1, i = ic - o0, j = jc - o1;
-            if (i < 1 || i > hnc || j < 1 || j > hnc) continue;
-            RstRec r{};
-            r.dst = G(pid, ic, jc);
-            r.src = G(cid, 2 * i - 1, 2 * j - 1);
-            if (coord == 1) {
-              // m_aX_restrict.f90:95-113; radius at the child-local index [i, j]
-              const double dr16 = 0.0625 * pm.dr;
-              const double rr = pm.r0 + (i - 0.5) * pm.dr;
-              r.rfac = dr16 / rr;
-            }
-            P.rst.push_back(r);
-            (void)ch_dix;
-          }
-        }
+      for (int q = 0; q < 4; q++) b.ch[q] = m.ch[q] > 0 ? m.ch[q] * SLOT : 0;
+      host_child_offset(m, b.o0, b.o1);
+      b.gi0 = (m.ix0 - 1) * nc;
+      b.flags = (is_leaf[id] ? CF_LEAF : 0) | (is_parent[id] ? CF_PARENT : 0);
+      b.r0 = m.r0;
+      b.dr = m.dr;
+      b.gbase = b.base;
+      if (is_parent[id]) P.pbx.push_back((int)P.boxes.size());
+      P.boxes.push_back(b);
     }
   }
-  P.cell_off[nlev] = (int)P.cells.size();
-  P.gphi_off[nlev] = (int)P.gphi.size();
-  P.gden_off[nlev] = (int)P.gden.size();
-  P.rst_off[nlev] = (int)P.rst.size();
-  P.fr_off[nlev] = (int)P.fr.size();
-  P.pcell_off[nlev] = (int)P.pcells.size();
+  P.bx_off[nlev] = (int)P.boxes.size();
+  P.pb_off[nlev] = (int)P.pbx.size();
+  // compact shared-memory layout: boxes one after another, (nc+2)^2 values
+  // each, starting at offset 2 so that no base is 0 (nb[] > 0 means a box)
+  std::vector<int> sbase(hm.size(), 0);
+  int off = 2;
+  for (const BoxRec &b : P.boxes) {
+    const int id = b.base / SLOT, ncg = hm[id].nc + 2;
+    sbase[id] = off;
+    off += ncg * ncg;
+  }
+  P.smem_doubles = (off + 1) & ~1;
+  P.sboxes = P.boxes;
+  auto sb = [&](int gb) { return gb > 0 ? sbase[gb / SLOT] : gb; };
+  for (BoxRec &b : P.sboxes) {
+    b.base = sbase[b.gbase / SLOT];
+    b.pbase = b.pbase > 0 ? sbase[b.pbase / SLOT] : b.pbase;
+    for (int q = 0; q < 4; q++) {
+      b.nb[q] = sb(b.nb[q]);
+      b.pnb[q] = sb(b.pnb[q]);
+      b.ch[q] = sb(b.ch[q]);
+    }
+  }
 }
 
 template <class T>
@@ -1504,12 +1581,12 @@ static int upload_vec(a5g_ctx *c, T *&dev, size_t &cap, const std::vector<T> &v)
 
 // Host-only export of the plans of a topology (tests and diagnostics; no
 // device needed). Level lists in the a5g_upload_tree format. Output arrays
-// may be NULL; sizes[6] = cells, ghosts, ghosts, rst, fr, pcells.
+// may be NULL. sizes[2] = boxes, parent boxes; boxes are written as raw
+// 96-byte records; offs = bx_off[MAXLEV+1] then pb_off[MAXLEV+1].
 extern "C" int a5g_debug_plans(int max_id, int min_lvl, int max_lvl, const int *meta16,
                                const double *geom4, const int *lvl_counts, const int *lvl_ids,
-                               double dr_base, int coord, int *sizes, int *offs, int *cells,
-                               int *gphi, int *gden, int *rst_i, double *rst_rfac, int *fr,
-                               int *pcells, double *lv_dr, int *lv_nc) {
+                               double dr_base, int *sizes, int *offs, void *boxes, int *pbx,
+                               double *lv_dr, int *lv_nc) {
   const int nlev = max_lvl - min_lvl + 1;
   if (nlev < 1 || nlev + 1 > MAXLEV || max_id < 1) return fail(A5G_EINVAL, "bad tree");
   std::vector<BoxMeta> hm(max_id + 1);
@@ -1534,28 +1611,52 @@ extern "C" int a5g_debug_plans(int max_id, int min_lvl, int max_lvl, const int *
         if (kind == 2) lv_parents[li].push_back(id);
       }
   HostPlans P;
-  build_plans(hm, lv_ids, lv_leaves, lv_parents, min_lvl, nlev, dr_base, coord, P);
+  build_plans(hm, lv_ids, lv_leaves, lv_parents, min_lvl, nlev, dr_base, P);
   if (sizes) {
-    sizes[0] = (int)P.cells.size(); sizes[1] = (int)P.gphi.size(); sizes[2] = (int)P.gden.size();
-    sizes[3] = (int)P.rst.size(); sizes[4] = (int)P.fr.size(); sizes[5] = (int)P.pcells.size();
+    sizes[0] = (int)P.boxes.size();
+    sizes[1] = (int)P.pbx.size();
   }
-  if (offs) {
-    const int *src[7] = {P.cell_off, P.cell_split, P.gphi_off, P.gden_off, P.rst_off, P.fr_off, P.pcell_off};
-    for (int a = 0; a < 7; a++)
-      for (int li = 0; li <= nlev; li++) offs[a * (MAXLEV + 1) + li] = (a == 1 && li == nlev) ? 0 : src[a][li];
-  }
-  if (cells) std::memcpy(cells, P.cells.data(), P.cells.size() * sizeof(CellRec));
-  if (gphi) std::memcpy(gphi, P.gphi.data(), P.gphi.size() * sizeof(GhostRec));
-  if (gden) std::memcpy(gden, P.gden.data(), P.gden.size() * sizeof(GhostRec));
-  for (size_t q = 0; q < P.rst.size(); q++) {
-    if (rst_i) { rst_i[2 * q] = P.rst[q].dst; rst_i[2 * q + 1] = P.rst[q].src; }
-    if (rst_rfac) rst_rfac[q] = P.rst[q].rfac;
-  }
-  if (fr) std::memcpy(fr, P.fr.data(), P.fr.size() * sizeof(FrRec));
-  if (pcells) std::memcpy(pcells, P.pcells.data(), P.pcells.size() * sizeof(int));
+  if (offs)
+    for (int li = 0; li <= nlev; li++) {
+      offs[li] = P.bx_off[li];
+      offs[MAXLEV + 1 + li] = P.pb_off[li];
+    }
+  if (boxes) std::memcpy(boxes, P.boxes.data(), P.boxes.size() * sizeof(BoxRec));
+  if (pbx) std::memcpy(pbx, P.pbx.data(), P.pbx.size() * sizeof(int));
   if (lv_dr) std::memcpy(lv_dr, P.lv_dr, nlev * sizeof(double));
   if (lv_nc) std::memcpy(lv_nc, P.lv_nc, nlev * sizeof(int));
   return A5G_OK;
+}
+
+// Largest dynamic shared memory a launch of the run kernels may use on the
+// current device; raises the kernels' limit to it on first use.
+static size_t dyn_smem_limit() {
+  static std::mutex mu;
+  static size_t lim[256] = {};
+  static bool done[256] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return 0;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!done[dev]) {
+    done[dev] = true;
+    int optin = 0;
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    size_t stat = 0;
+    cudaFuncAttributes fa[3];
+    const void *fns[3] = {(const void *)a5g_run_kernel, (const void *)a5g_step_kernel,
+                          (const void *)a5g_run_kernel_slots};
+    for (int k = 0; k < 3; k++)
+      if (cudaFuncGetAttributes(&fa[k], fns[k]) == cudaSuccess)
+        stat = std::max(stat, fa[k].sharedSizeBytes);
+    size_t avail = optin > (int)stat ? (size_t)optin - stat : 0;
+    bool ok = true;
+    for (int k = 0; k < 3; k++)
+      ok = ok && cudaFuncSetAttribute(fns[k], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)avail) == cudaSuccess;
+    lim[dev] = ok ? avail : 0;
+    cudaGetLastError();
+  }
+  return lim[dev];
 }
 
 static int push_run(a5g_ctx *c) {
@@ -1579,7 +1680,7 @@ static int launch(a5g_ctx *c, const Op &op) {
   if (!c) return fail(A5G_EINVAL, "null context");
   if (!c->has_tree) return fail(A5G_ESTATE, "no tree uploaded");
   if (!c->has_table) return fail(A5G_ESTATE, "no transport table set");
-  a5g_run_kernel<<<1, NTHR, 0, c->stream>>>(c->d_run, op, nullptr, nullptr);
+  a5g_run_kernel<<<1, NTHR, c->dyn_smem, c->stream>>>(c->d_run, op, nullptr, nullptr);
   CK(cudaGetLastError());
   return A5G_OK;
 }
@@ -1652,12 +1753,9 @@ int a5g_destroy(a5g_ctx *c) {
   cudaFree(c->scal);
   cudaFree(c->flags);
   cudaFree(c->status);
-  cudaFree(c->p_cells);
-  cudaFree(c->p_gphi);
-  cudaFree(c->p_gden);
-  cudaFree(c->p_rst);
-  cudaFree(c->p_fr);
-  cudaFree(c->p_pcells);
+  cudaFree(c->p_boxes);
+  cudaFree(c->p_sboxes);
+  cudaFree(c->p_pbx);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return A5G_OK;
@@ -1818,30 +1916,27 @@ int a5g_upload_tree(a5g_ctx *c, int max_id, int min_lvl, int max_lvl, const int 
     CK(cudaMemcpyAsync(c->lists, lists.data(), lists.size() * sizeof(int), cudaMemcpyHostToDevice,
                        c->stream));
   HostPlans P;
-  build_plans(hm, lv_ids, lv_leaves, lv_parents, min_lvl, nlev, c->p.dr_base, c->p.coord, P);
-  if ((r = upload_vec(c, c->p_cells, c->cap_cells, P.cells)) ||
-      (r = upload_vec(c, c->p_gphi, c->cap_gphi, P.gphi)) ||
-      (r = upload_vec(c, c->p_gden, c->cap_gden, P.gden)) ||
-      (r = upload_vec(c, c->p_rst, c->cap_rst, P.rst)) ||
-      (r = upload_vec(c, c->p_fr, c->cap_fr, P.fr)) ||
-      (r = upload_vec(c, c->p_pcells, c->cap_pcells, P.pcells)))
+  build_plans(hm, lv_ids, lv_leaves, lv_parents, min_lvl, nlev, c->p.dr_base, P);
+  if ((r = upload_vec(c, c->p_boxes, c->cap_boxes, P.boxes)) ||
+      (r = upload_vec(c, c->p_sboxes, c->cap_sboxes, P.sboxes)) ||
+      (r = upload_vec(c, c->p_pbx, c->cap_pbx, P.pbx)))
     return r;
   RunDev &h = c->h;
-  std::memcpy(h.cell_off, P.cell_off, sizeof(P.cell_off));
-  std::memcpy(h.cell_split, P.cell_split, sizeof(P.cell_split));
-  std::memcpy(h.gphi_off, P.gphi_off, sizeof(P.gphi_off));
-  std::memcpy(h.gden_off, P.gden_off, sizeof(P.gden_off));
-  std::memcpy(h.rst_off, P.rst_off, sizeof(P.rst_off));
-  std::memcpy(h.fr_off, P.fr_off, sizeof(P.fr_off));
-  std::memcpy(h.pcell_off, P.pcell_off, sizeof(P.pcell_off));
+  {
+    // keep the multigrid variables in shared memory when the tree fits
+    const size_t need = 3 * (size_t)P.smem_doubles * sizeof(double) +
+                        P.boxes.size() * sizeof(BoxRec) + P.pbx.size() * sizeof(int);
+    const size_t limit = dyn_smem_limit();
+    h.smem_doubles = need <= limit ? P.smem_doubles : 0;
+    c->dyn_smem = h.smem_doubles ? need : 0;
+  }
+  h.sboxes = c->p_sboxes;
+  std::memcpy(h.bx_off, P.bx_off, sizeof(P.bx_off));
+  std::memcpy(h.pb_off, P.pb_off, sizeof(P.pb_off));
   std::memcpy(h.lv_nc, P.lv_nc, sizeof(P.lv_nc));
   std::memcpy(h.lv_dr, P.lv_dr, sizeof(P.lv_dr));
-  h.cells = c->p_cells;
-  h.gphi = c->p_gphi;
-  h.gden = c->p_gden;
-  h.rst = c->p_rst;
-  h.fr = c->p_fr;
-  h.pcells = c->p_pcells;
+  h.boxes = c->p_boxes;
+  h.pbx = c->p_pbx;
   h.min_lvl = min_lvl;
   h.max_lvl = max_lvl;
   h.nlev = nlev;
@@ -2038,7 +2133,7 @@ int a5g_step(a5g_ctx *c, double dt) {
   if (!(dt > 0)) return fail(A5G_EINVAL, "dt must be > 0");
   if (!c->has_tree) return fail(A5G_ESTATE, "no tree uploaded");
   if (!c->has_table) return fail(A5G_ESTATE, "no transport table set");
-  a5g_step_kernel<<<1, NTHR, 0, c->stream>>>(c->d_run, dt);
+  a5g_step_kernel<<<1, NTHR, c->dyn_smem, c->stream>>>(c->d_run, dt);
   CK(cudaGetLastError());
   return A5G_OK;
 }
@@ -2065,7 +2160,9 @@ int a5g_step_batch(a5g_ctx **ctxs, int n, const double *dts) {
   CK(cudaMallocAsync((void **)&d_ops, n * sizeof(Op), c0->stream));
   CK(cudaMemcpyAsync(d_rp, rp.data(), n * sizeof(void *), cudaMemcpyHostToDevice, c0->stream));
   CK(cudaMemcpyAsync(d_ops, ops.data(), n * sizeof(Op), cudaMemcpyHostToDevice, c0->stream));
-  a5g_run_kernel<<<n, NTHR, 0, c0->stream>>>(nullptr, Op{}, d_rp, d_ops);
+  size_t dyn = 0;
+  for (int k = 0; k < n; k++) dyn = std::max(dyn, ctxs[k]->dyn_smem);
+  a5g_run_kernel<<<n, NTHR, dyn, c0->stream>>>(nullptr, Op{}, d_rp, d_ops);
   CK(cudaGetLastError());
   CK(cudaFreeAsync(d_rp, c0->stream));
   CK(cudaFreeAsync(d_ops, c0->stream));
@@ -2114,7 +2211,9 @@ int a5g_step_batch_static(a5g_ctx **ctxs, int n, const double *dts) {
   // pageable source: the copy is staged before the call returns
   CK(cudaMemcpyAsync(g_static_dev[dev], g_static_host, (size_t)n * sizeof(BatchSlot),
                      cudaMemcpyHostToDevice, c0->stream));
-  a5g_run_kernel_slots<<<n, NTHR, 0, c0->stream>>>(g_static_dev[dev]);
+  size_t dyn = 0;
+  for (int k = 0; k < n; k++) dyn = std::max(dyn, ctxs[k]->dyn_smem);
+  a5g_run_kernel_slots<<<n, NTHR, dyn, c0->stream>>>(g_static_dev[dev]);
   CK(cudaGetLastError());
   return A5G_OK;
 }
@@ -2123,6 +2222,43 @@ int a5g_sync(a5g_ctx *c) {
   if (!c) return fail(A5G_EINVAL, "null context");
   CK(cudaStreamSynchronize(c->stream));
   return check_status(c);
+}
+
+// Internal diagnostics: run a timing probe (code 0: n barriers, 1: n
+// half-sweeps of level lvl, 2: n ghost fills of level lvl, 3: empty launch;
+// in_smem: stage the multigrid variables into shared memory first).
+int a5g_debug_op(a5g_ctx *c, int code, int n, int lvl, int in_smem) {
+  if (!c || n < 0) return fail(A5G_EINVAL, "bad argument");
+  if (code != 0 && code != 3 && (lvl < c->min_lvl || lvl > c->max_lvl)) return fail(A5G_EINVAL, "bad level");
+  Op o{};
+  o.code = code == 0 ? OP_DBG_BARRIERS : code == 1 ? OP_DBG_SWEEPS : code == 2 ? OP_DBG_FILLS : OP_DBG_EMPTY;
+  o.i0 = n;
+  o.i1 = lvl;
+  o.i2 = in_smem;
+  return launch(c, o);
+}
+
+// Internal diagnostics: copy of the 16-double scalar buffer.
+int a5g_debug_scal(a5g_ctx *c, double *out16) {
+  if (!c || !out16) return fail(A5G_EINVAL, "null argument");
+  CK(cudaMemcpyAsync(out16, c->scal, 16 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return A5G_OK;
+}
+
+// Internal diagnostics (not part of the ABI headers): shared-memory use and
+// sizes of the uploaded tree.
+int a5g_debug_info(a5g_ctx *c, long long *out8) {
+  if (!c || !out8) return fail(A5G_EINVAL, "null argument");
+  out8[0] = c->h.smem_doubles;
+  out8[1] = (long long)c->dyn_smem;
+  out8[2] = c->capacity;
+  out8[3] = c->h.nlev;
+  out8[4] = (long long)dyn_smem_limit();
+  out8[5] = c->h.bx_off[c->h.nlev];
+  out8[6] = 0;
+  out8[7] = 0;
+  return A5G_OK;
 }
 
 int a5g_get_stream(a5g_ctx *c, void **stream) {
