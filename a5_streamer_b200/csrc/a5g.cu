@@ -597,15 +597,48 @@ __device__ __forceinline__ double den_ghost(const double *x, const BoxRec &B, in
   return x[own];
 }
 
-// Neighbours (lx, hx, ly, hy) of interior cell (i, j), ghost values from
-// their sources
+// phi_ghost in straight-line form: the addresses of all candidate sources
+// are formed first, the values loaded together and the result selected by
+// the kind of the side (neighbour copy, refinement boundary, physical wall),
+// so that a cell's loads are in flight together instead of behind branches.
+// Same values and the same arithmetic as phi_ghost.
+__device__ __forceinline__ double phi_ghost_sl(const RunDev &R, const double *phi, const BoxRec &B,
+                                               int nc, int ncg, int side, int k) {
+  const int dim = side >> 1;
+  const bool low = (side & 1) == 0;
+  const int nbb = B.nb[side];
+  const int ix = low ? 1 : nc;
+  const int own = B.base + (dim == 0 ? ix + ncg * k : k + ncg * ix);
+  const int di = low ? 1 : -1, dk = -1 + 2 * (k & 1), ig = ix - di;
+  const int h1 = (ig + 1) >> 1, h2 = (k + 1) >> 1;
+  const int pc = B.pbase + (dim == 0 ? (B.o0 + h1) + ncg * (B.o1 + h2)
+                                     : (B.o0 + h2) + ncg * (B.o1 + h1));
+  const int a = own + (dim == 0 ? di : dk);
+  const int b = own + ncg * (dim == 0 ? dk : di);
+  const int cp = nbb + (dim == 0 ? (low ? nc : 1) + ncg * k : k + ncg * (low ? nc : 1));
+  const bool isnb = nbb > 0, isrb = nbb == NBR_RB;
+  const int s0 = isnb ? cp : (isrb ? pc : own);
+  const int s1 = isrb ? own : s0, s2 = isrb ? a : s0, s3 = isrb ? b : s0;
+  const double v0 = phi[s0], v1 = phi[s1], v2 = phi[s2], v3 = phi[s3];
+  const double vrb = 0.5 * v0 + v1 - 0.25 * (v2 + v3);
+  const double vbc = side == 2 ? -v0 : (side == 3 ? 2 * R.applied_voltage - v0 : v0);
+  return isnb ? v0 : (isrb ? vrb : vbc);
+}
+
+// Neighbours (lx, hx, ly, hy) of interior cell (i, j). A cell has at most
+// one ghost neighbour in x and one in y; both are evaluated unconditionally
+// (straight-line) and selected where needed.
 __device__ __forceinline__ void phi_nbrs(const RunDev &R, const double *phi, const BoxRec &B,
                                          int nc, int ncg, int i, int j, int g, double &lx,
                                          double &hx, double &ly, double &hy) {
-  lx = i > 1 ? phi[g - 1] : phi_ghost(R, phi, B, nc, ncg, 0, j);
-  hx = i < nc ? phi[g + 1] : phi_ghost(R, phi, B, nc, ncg, 1, j);
-  ly = j > 1 ? phi[g - ncg] : phi_ghost(R, phi, B, nc, ncg, 2, i);
-  hy = j < nc ? phi[g + ncg] : phi_ghost(R, phi, B, nc, ncg, 3, i);
+  const double gx = phi_ghost_sl(R, phi, B, nc, ncg, i == 1 ? 0 : 1, j);
+  const double gy = phi_ghost_sl(R, phi, B, nc, ncg, j == 1 ? 2 : 3, i);
+  const double dlx = phi[g - (i > 1 ? 1 : 0)], dhx = phi[g + (i < nc ? 1 : 0)];
+  const double dly = phi[g - (j > 1 ? ncg : 0)], dhy = phi[g + (j < nc ? ncg : 0)];
+  lx = i > 1 ? dlx : gx;
+  hx = i < nc ? dhx : gx;
+  ly = j > 1 ? dly : gy;
+  hy = j < nc ? dhy : gy;
 }
 
 // box_lpl (m_aX_mg.f90:662-680) / box_clpl (:1027-1049) at one cell
