@@ -32,6 +32,10 @@ class Params(ctypes.Structure):
         ("n_seeds", ctypes.c_int),
         ("seed_r0", (ctypes.c_double * 2) * 8), ("seed_r1", (ctypes.c_double * 2) * 8),
         ("seed_width", ctypes.c_double * 8),
+        ("photoi_enabled", ctypes.c_int), ("photoi_num_photons", ctypes.c_int),
+        ("photoi_team", ctypes.c_int), ("photoi_pad", ctypes.c_int),
+        ("photoi_coeff", ctypes.c_double), ("photoi_fac_dx", ctypes.c_double),
+        ("rng_seed", ctypes.c_int * 4),
     ]
 
 
@@ -67,6 +71,10 @@ SIGNATURES = {
     "a5g_ref_flags": (_I, [_P, _D, _PI]),
     "a5g_prolong_new": (_I, [_P, _PI, _PI]),
     "a5g_step": (_I, [_P, _D]),
+    "a5g_set_photon_table": (_I, [_P, _I, _D, _D, _PD, _D]),
+    "a5g_get_rng": (_I, [_P, _PI]),
+    "a5g_set_rng": (_I, [_P, _PI]),
+    "a5g_photoionization": (_I, [_P, _D, _I]),
     "a5g_step_batch": (_I, [ctypes.POINTER(_P), _I, _PD]),
     "a5g_step_batch_static": (_I, [ctypes.POINTER(_P), _I, _PD]),
     "a5g_sync": (_I, [_P]),
@@ -84,6 +92,7 @@ SIGNATURES = {
     "a5t_export": (_I, [_P, _PI, _PD, _PI, _PI]),
     "a5t_n_level_ids": (_I, [_P]),
     "a5t_new_boxes": (_I, [_P, _PI, _PI]),
+    "a5t_photon_table": (_I, [_I, _D, _D, _D, _PD, _PD, _PI]),
     # streamer driver
     "a5s_create": (_I, [ctypes.c_void_p, ctypes.POINTER(_P)]),
     "a5s_destroy": (_I, [_P]),
@@ -104,6 +113,8 @@ class SimConfig(ctypes.Structure):
         ("seed_falloff", ctypes.c_int * 8), ("num_steps_amr", ctypes.c_int),
         ("lkptbl_size", ctypes.c_int), ("lkptbl_max_fld", ctypes.c_double),
         ("td_n", ctypes.c_int * 4), ("td_x", _PD * 4), ("td_y", _PD * 4),
+        ("photoi_tbl_kind", ctypes.c_int), ("photoi_tbl_a", ctypes.c_double),
+        ("photoi_tbl_b", ctypes.c_double), ("photoi_max_dist", ctypes.c_double),
     ]
 
 _lib = None

@@ -25,6 +25,17 @@ TD_COLUMNS = ("mobility", "diffusion", "alpha", "eta")
 FALLOFF = {"sigmoid": 1, "gaussian": 2, "smoothstep": 3, "step": 4}
 
 
+def photoi_coeff_air(eta: float = 0.05, gas_pressure: float = 1.0) -> float:
+    """Photons per ionization as the cylindrical driver sets it:
+    photoi_eta * p_quench / (gas_pressure + p_quench) with p_quench = 30 Torr
+    (src/streamer_cyl.f90:572-588; one Torr in bar as in
+    fosito/m_units_constants.f90:44, a single-precision literal times 1e-5)."""
+    import struct
+    torr = struct.unpack("f", struct.pack("f", 133.322368))[0] * 1.0e-5
+    p_quench = 30.0 * torr
+    return eta * (p_quench / (gas_pressure + p_quench))
+
+
 @dataclass
 class Seed:
     r0: Tuple[float, ...]
@@ -54,7 +65,22 @@ class StreamerConfig:
     lkptbl_max_fld: float = 3e7
     # transport input pairs per column: name -> (x list, y list)
     td: Dict[str, Tuple[List[float], List[float]]] = field(default_factory=dict)
+    # photoionization (src/m_streamer.f90:196-203, src/streamer_cyl.f90:572-617)
     photoi_enabled: bool = False
+    photoi_num_photons: int = 50 * 1000
+    # photons per ionization; the reference uses photoi_eta * quench factor
+    # (photoi_coeff_air below)
+    photoi_coeff: float = photoi_coeff_air(0.05, 1.0)
+    # ("air", O2 partial pressure in bar, 0) for PH_get_tbl_air, or
+    # ("logu", shortest, longest absorption length in m)
+    photoi_table: Tuple[str, float, float] = ("air", 0.2, 0.0)
+    photoi_fac_dx: float = 0.25e-3
+    # size of the OpenMP team whose execution of the photon loops is
+    # reproduced: each thread draws from its own generator seeded from the
+    # master (fosito/m_random.f90:44-55), loops split by the static schedule
+    photoi_team: int = 148 * 256
+    # master generator state ST_rng (fosito/m_random.f90:12-13 default)
+    rng_seed: Tuple[int, int, int, int] = (521288629, 362436069, 16163801, 1131199299)
 
     # --- derived quantities -------------------------------------------------
     @property
@@ -93,6 +119,11 @@ class StreamerConfig:
         # src/m_streamer.f90:411: ST_applied_voltage = -ST_domain_len * fld
         return -self.domain_len_z * self.applied_fld
 
+    @property
+    def photoi_max_dist(self) -> float:
+        # src/m_streamer.f90:329-330: table range 2 * ST_domain_len
+        return 2 * self.domain_len_z
+
     def dr_at(self, lvl: int) -> float:
         return self.dr_base * 0.5 ** (lvl - 1)
 
@@ -119,6 +150,17 @@ class StreamerConfig:
                 raise ValueError(f"transport column {name!r}: bad length")
         if not (1 <= self.lvls_max <= 30):
             raise ValueError("lvls_max must be in 1..30")
+        if self.photoi_enabled:
+            if not self.is_cyl:
+                raise ValueError("photoionization is built for the cylindrical form only "
+                                 "(PH_set_src_2d with a constant absorption level)")
+            kind = self.photoi_table[0]
+            if kind not in ("air", "logu"):
+                raise ValueError("photoi_table kind must be 'air' or 'logu'")
+            if kind == "logu" and not (0 < self.photoi_table[1] < self.photoi_table[2]):
+                raise ValueError("log-uniform absorption lengths need 0 < shortest < longest")
+            if self.photoi_team < 1 or self.photoi_num_photons < 0:
+                raise ValueError("photoi_team must be >= 1 and photoi_num_photons >= 0")
 
 
 def table_nodes(n_rows: int, x_max: float, x_min: float = 0.0) -> List[float]:
@@ -160,11 +202,13 @@ def cartesian_8mm(**overrides) -> StreamerConfig:
     return dataclasses.replace(cfg, **overrides)
 
 
-def cylindrical_16mm(**overrides) -> StreamerConfig:
+def cylindrical_16mm(photoi: bool = False, **overrides) -> StreamerConfig:
     """Axisymmetric (r, z) FP64 case: R = 8 mm, Z = 16 mm (two base boxes
     stacked in z, base dx 1 mm), E_bg = 2e6 V/m, background 1e15 m^-3, seed
     1e19 m^-3 with sigma 0.1 mm on the axis at z = 15 mm, attachment
-    eta = 1e3 exp(-4e6/|E|). Photoionization is not part of this form."""
+    eta = 1e3 exp(-4e6/|E|). With ``photoi=True``: Monte Carlo photoionization
+    with 1e5 photons per step, absorption length log-uniform between 0.2 and
+    2 mm, 0.06 photons per ionization."""
     sigma = 0.1e-3
     cfg = StreamerConfig(
         dim=2, coord="cyl", box_size=8, n_base=(1, 2), domain_len=(8e-3, 16e-3),
@@ -173,7 +217,9 @@ def cylindrical_16mm(**overrides) -> StreamerConfig:
                     width=math.sqrt(2.0) * sigma, falloff=2)],
         dt_max=1e-10, num_steps_amr=2, end_time=10e-9, use_drt=True,
         lkptbl_size=200, lkptbl_max_fld=3e7,
-        td=synthetic_transport(eta_a=1.0e3, eta_b=4e6))
+        td=synthetic_transport(eta_a=1.0e3, eta_b=4e6),
+        photoi_enabled=photoi, photoi_num_photons=100 * 1000, photoi_coeff=0.06,
+        photoi_table=("logu", 0.2e-3, 2.0e-3))
     return dataclasses.replace(cfg, **overrides)
 
 
@@ -215,6 +261,14 @@ def load_cfg_files(paths: Sequence[str], base: StreamerConfig | None = None) -> 
     if "lkptbl_size" in kv: upd["lkptbl_size"] = int(kv["lkptbl_size"][0])
     if "lkptbl_max_fld" in kv: upd["lkptbl_max_fld"] = _f(kv["lkptbl_max_fld"])
     if "photoi_enabled" in kv: upd["photoi_enabled"] = kv["photoi_enabled"][0].upper().startswith("T")
+    if "photoi_num_photons" in kv: upd["photoi_num_photons"] = int(kv["photoi_num_photons"][0])
+    if any(k in kv for k in ("photoi_eta", "photoi_frac_O2", "gas_pressure")):
+        # src/m_streamer.f90:327-330 and src/streamer_cyl.f90:584-588
+        eta = _f(kv.get("photoi_eta", ["0.05"]))
+        pressure = _f(kv.get("gas_pressure", ["1.0"]))
+        frac_o2 = _f(kv.get("photoi_frac_O2", ["0.2"]))
+        upd["photoi_coeff"] = photoi_coeff_air(eta, pressure)
+        upd["photoi_table"] = ("air", frac_o2 * pressure, 0.0)
     if "lvls_max" in kv: upd["lvls_max"] = int(kv["lvls_max"][0])
     if "use_drt" in kv: upd["use_drt"] = kv["use_drt"][0].upper().startswith("T")
     if "coord" in kv: upd["coord"] = kv["coord"][0]

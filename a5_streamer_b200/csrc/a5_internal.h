@@ -10,10 +10,6 @@ int a5g_internal_fail(int code, const char *msg);
  * memory per launch, capacity, levels, device limit, boxes. */
 struct a5g_ctx;
 int a5g_debug_info(struct a5g_ctx *ctx, long long *out8);
-/* Diagnostics: timing probes (0: n barriers, 1: n half-sweeps of level lvl,
- * 2: n ghost fills of level lvl, 3: empty launch). */
-int a5g_debug_op(struct a5g_ctx *ctx, int code, int n, int lvl, int in_smem);
-int a5g_debug_scal(struct a5g_ctx *ctx, double *out16);
 #ifdef __cplusplus
 }
 #endif

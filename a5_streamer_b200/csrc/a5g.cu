@@ -108,12 +108,47 @@ struct RunDev {
   double *scal;                // dt reductions out
   int *flags;                  // refinement flags out
   int *status;
+  // photoionization (see "Photoionization" below)
+  int n_ids;                   // max_id + 1
+  int ph_enabled, ph_team, ph_lvl, ph_rows, ph_cap;
+  double ph_coeff, ph_num_photons, ph_xmin, ph_inv_dx, ph_frac;
+  const double *ph_tbl;        // absorption distance per table row
+  int *ph_rng;                 // master generator state (4 int32)
+  int *ph_ncr;                 // photons created per cell (capacity * SLOT)
+  int *ph_cnt;                 // photons absorbed per cell (capacity * SLOT)
+  int *ph_src;                 // source cell (id * SLOT + cell) per photon
+  int *ph_ipart;               // per-thread photon counts, then bases
+  double *ph_part;             // per-thread partial sums of the production
+  struct PhScal *ph_scal;
+  const struct MzJump *ph_jump;
+  const struct PhBox *ph_boxes;
 };
+
+// Scalars of one photoionization call: photons created, the factor fac
+// of PH_set_src_2d and the master generator state at the start of the call.
+struct PhScal {
+  long long n_used;
+  double fac;
+  int st0[4];
+};
+// Jump of 2^b draws of the master generator (see mz_advance).
+struct MzJump {
+  unsigned int m[9];
+  unsigned int a, c;
+};
+constexpr int MZ_NJUMP = 40;
+// Per box geometry for the absorption-location descent (a$D_get_loc).
+struct PhBox {
+  double r0, r1, dr;
+  int ch[4];
+  int lvl, nc;
+};
+static_assert(sizeof(PhBox) == 48, "PhBox layout");
 
 enum OpCode {
   OP_COPY = 1, OP_FLUXES, OP_CONSISTENT, OP_UPDATE, OP_RESTRICT, OP_GC, OP_AVERAGE,
   OP_COMPUTE_FLD, OP_FMG, OP_FLD_FROM_POT, OP_DT_RED, OP_REF_FLAGS, OP_PROLONG_NEW,
-  OP_STEP, OP_SET_RHS, OP_DBG_BARRIERS, OP_DBG_SWEEPS, OP_DBG_FILLS, OP_DBG_EMPTY
+  OP_STEP, OP_NOP, OP_PH_SOURCE, OP_PH_DEPOSIT
 };
 struct Op {
   int code, i0, i1, i2;
@@ -489,6 +524,7 @@ __device__ void update_solution(const RunDev &R, double dt) {
     double fx0 = fxe[fxi(i, j, nc)], fx1 = fxe[fxi(i + 1, j, nc)];
     double fy0 = fye[fyi(i, j, nc)], fy1 = fye[fyi(i, j + 1, nc)];
     double src = 0.5 * norm2_2(fx0 + fx1, fy0 + fy1) * (alpha - eta);
+    if (R.ph_enabled) src = src + CC(R, I_PHO, id)[c];
     double sflux;
     if (cyl) {
       int ioff = (m.ix0 - 1) * nc;
@@ -1284,8 +1320,358 @@ __device__ void prolong_new(const RunDev &R) {
   }
 }
 
-// One full time step, src/streamer_2d.f90:99-127
-__device__ void step(const RunDev &R, double dt) {
+// ---------------------------------------------------------------------------
+// Photoionization: set_photoionization (src/streamer_cyl.f90:572-617) and
+// PH_set_src_2d with use_cyl and a constant absorption level
+// (src/m_photons.f90:207-436).
+//
+// The reference runs the photon loops in OpenMP regions whose outcome
+// depends on the team (every thread draws from its own generator, seeded
+// from the master by PRNG_t%init, fosito/m_random.f90:44-55; loops use the
+// static schedule; photon numbers are taken in a critical section). Here
+// the team has R.ph_team threads, photons are numbered thread by thread and
+// the per-thread partial sums of a$D_tree_sum_cc are added in thread order:
+// one of the executions the reference takes with that many threads.
+//
+// Three launches: ph_source (one block: production rate, sum, photon
+// creation, numbering), a5g_photon_kernel (many blocks: absorption of each
+// thread's chunk of photons and the count per absorbing cell), ph_deposit
+// (one block, at the start of the step: the source term per cell, ghost
+// cells and prolongation). The deposit of the reference adds the same value
+// frac_in_tbl / (fac 2 pi dr^2 r) once per photon to a cleared cell, in
+// photon order; with every addend equal, that sum depends only on the
+// count, so the device counts photons with integer atomics and forms the
+// same sequential sum per cell.
+
+// mzran (fosito/m_random.f90:58-66). Default integers wrap on overflow, as
+// in the reference's gfortran x86-64 build.
+constexpr unsigned int MZ_M = 2147483579u;
+__device__ __forceinline__ int mz_int4(int st[4]) {
+  int rr = (int)((unsigned)st[0] - (unsigned)st[2]);
+  if (rr < 0) rr = (int)((unsigned)rr + MZ_M);
+  st[0] = st[1];
+  st[1] = st[2];
+  st[2] = rr;
+  st[3] = (int)(69069u * (unsigned)st[3] + 1013904243u);
+  return (int)((unsigned)rr + (unsigned)st[3]);
+}
+// uni_01 (fosito/m_random.f90:75-80)
+__device__ __forceinline__ double mz_uni01(int st[4]) { return 0.5 + 0x1p-32 * (double)mz_int4(st); }
+
+// Advance the master generator by k draws. While s1, s2, s3 all lie in
+// [0, m) a draw maps (s1, s2, s3) to (s2, s3, s1 - s3 mod m), a linear map
+// mod m, and s4 to 69069 s4 + 1013904243 mod 2^32; J[b] holds both maps for
+// 2^b draws. Outside that range (a seed set by the caller) the draws are
+// stepped one by one until the state enters it; it then stays there.
+__device__ void mz_advance(int st[4], unsigned long long k, const MzJump *J) {
+  auto clean = [&]() {
+    return st[0] >= 0 && st[0] < (int)MZ_M && st[1] >= 0 && st[1] < (int)MZ_M && st[2] >= 0 &&
+           st[2] < (int)MZ_M;
+  };
+  while (k > 0 && !clean()) {
+    mz_int4(st);
+    k--;
+  }
+  for (int b = 0; k != 0 && b < MZ_NJUMP; b++, k >>= 1) {
+    if (!(k & 1)) continue;
+    const MzJump &j = J[b];
+    const unsigned long long v0 = (unsigned)st[0], v1 = (unsigned)st[1], v2 = (unsigned)st[2];
+    unsigned int n[3];
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+      n[r] = (unsigned)(((unsigned long long)j.m[3 * r] * v0 + (unsigned long long)j.m[3 * r + 1] * v1 +
+                         (unsigned long long)j.m[3 * r + 2] * v2) % MZ_M);
+    st[0] = (int)n[0];
+    st[1] = (int)n[1];
+    st[2] = (int)n[2];
+    st[3] = (int)(j.a * (unsigned)st[3] + j.c);
+  }
+}
+
+// libgomp's static schedule without a chunk size: thread c of W gets the
+// iterations [lo, lo + len) of n.
+__device__ __forceinline__ void static_chunk(long long n, long long W, long long c, long long &lo,
+                                             long long &len) {
+  long long q = n / W, t = n % W;
+  if (c < t) {
+    q++;
+    t = 0;
+  }
+  lo = q * c + t;
+  len = q;
+}
+
+constexpr double PI_DP = 3.141592653589793;   // acos(-1.0_dp)
+constexpr double TWOPI_DP = 6.283185307179586; // 2 * acos(-1.0_dp)
+
+// ph_source: everything up to the photon numbers.
+__device__ void ph_source(const RunDev &R, double dt, bool has_dt) {
+  __shared__ double s_fac;
+  const bool cyl = R.coord == 1;
+  // set_photoi_rate on all leaves (src/streamer_cyl.f90:595-617)
+  {
+    const int *ids;
+    int n;
+    list_range(R, 1, R.min_lvl, R.max_lvl, ids, n);
+    box_loop(ids, n, [&](int id, int t) {
+      const int nc = R.meta[id].nc, ncg = nc + 2;
+      if (t >= nc * nc) return;
+      const int c = (t % nc + 1) + ncg * (t / nc + 1);
+      const double fld = CC(R, I_FLD, id)[c];
+      const Loc loc = get_loc(R, fld);
+      const double alpha = col_at(R, C_ALPHA, loc);
+      const double mobility = col_at(R, C_MOB, loc);
+      double tmp = fld * mobility * alpha * CC(R, I_ELEC, id)[c] * R.ph_coeff;
+      if (tmp < 0) tmp = 0;
+      CC(R, I_PHO, id)[c] = tmp;
+    });
+  }
+  __syncthreads();
+  const long long W = R.ph_team;
+  int max_l = 0, max_l1 = 0;
+  for (int lvl = R.min_lvl; lvl <= R.max_lvl; lvl++) {
+    const int L = list_n(R, 1, lvl);
+    max_l = max(max_l, L);
+    if (lvl >= 1) max_l1 = max(max_l1, L);
+  }
+  const int n_sum = (int)min((long long)max_l, W), n_cr = (int)min((long long)max_l1, W);
+  // a$D_tree_sum_cc (afivo/src/m_aX_utils.f90:623-680) per team thread
+  for (int c = threadIdx.x; c < n_sum; c += NTHR) {
+    double my = 0;
+    for (int lvl = R.min_lvl; lvl <= R.max_lvl; lvl++) {
+      const int L = list_n(R, 1, lvl);
+      long long lo, len;
+      static_chunk(L, W, c, lo, len);
+      if (len == 0) continue;
+      const double dr = R.lv_dr[lvl - R.min_lvl], fac = dr * dr;
+      const int *lv = list_p(R, 1, lvl);
+      for (long long k = lo; k < lo + len; k++) {
+        const int id = lv[k];
+        const BoxMeta &m = R.meta[id];
+        const int nc = m.nc, ncg = nc + 2;
+        const double *x = CC(R, I_PHO, id);
+        double tmp = 0;
+        if (cyl) {
+          for (int j = 1; j <= nc; j++)
+            for (int i = 1; i <= nc; i++) tmp = tmp + x[i + ncg * j] * (m.r0 + (i - 0.5) * m.dr);
+          tmp = tmp * TWOPI_DP;
+        } else {
+          for (int j = 1; j <= nc; j++)
+            for (int i = 1; i <= nc; i++) tmp = tmp + x[i + ncg * j];
+        }
+        my = my + fac * tmp;
+      }
+    }
+    R.ph_part[c] = my;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double total = 0;
+    for (int c = 0; c < n_sum; c++) total = total + R.ph_part[c];
+    double fac = R.ph_num_photons / (total + 2.220446049250313e-16);
+    if (has_dt) fac = dt < fac ? dt : fac;
+    s_fac = fac;
+  }
+  __syncthreads();
+  const double fac = s_fac;
+  int st0[4];
+#pragma unroll
+  for (int q = 0; q < 4; q++) st0[q] = R.ph_rng[q];
+  // photon creation (src/m_photons.f90:263-306): thread c's generator is the
+  // master's draws 4c+1..4c+4
+  for (int c = threadIdx.x; c < n_cr; c += NTHR) {
+    int st[4] = {st0[0], st0[1], st0[2], st0[3]};
+    mz_advance(st, 4ull * (unsigned long long)c, R.ph_jump);
+    int rs[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) rs[q] = mz_int4(st);
+    long long total = 0;
+    for (int lvl = 1; lvl <= R.max_lvl; lvl++) {
+      const int L = list_n(R, 1, lvl);
+      long long lo, len;
+      static_chunk(L, W, c, lo, len);
+      if (len == 0) continue;
+      const double dr = R.lv_dr[lvl - R.min_lvl], dr2 = dr * dr;
+      const int *lv = list_p(R, 1, lvl);
+      for (long long k = lo; k < lo + len; k++) {
+        const int id = lv[k];
+        const BoxMeta &m = R.meta[id];
+        const int nc = m.nc, ncg = nc + 2;
+        const double *x = CC(R, I_PHO, id);
+        int *ncr = R.ph_ncr + (size_t)id * SLOT;
+        for (int j = 1; j <= nc; j++)
+          for (int i = 1; i <= nc; i++) {
+            const int cell = i + ncg * j;
+            double tmp;
+            if (cyl) tmp = fac * 2 * PI_DP * (m.r0 + (i - 0.5) * m.dr) * x[cell] * dr2;
+            else tmp = fac * x[cell] * dr2;
+            const double fl = floor(tmp);
+            int n_create = 0;
+            if (fl >= 0 && fl < 1.0e9) n_create = (int)fl;
+            else atomicExch(R.status, A5G_ENONFINITE);
+            if (mz_uni01(rs) < tmp - n_create) n_create = n_create + 1;
+            ncr[cell] = n_create;
+            total += n_create;
+          }
+      }
+    }
+    R.ph_ipart[c] = (int)min(total, (long long)INT_MAX);
+  }
+  __syncthreads();
+  // photon numbers: threads in order
+  if (threadIdx.x == 0) {
+    long long acc = 0;
+    for (int c = 0; c < n_cr; c++) {
+      const int v = R.ph_ipart[c];
+      R.ph_ipart[c] = (int)min(acc, (long long)INT_MAX);
+      acc += v;
+    }
+    if (acc > R.ph_cap) {
+      atomicExch(R.status, A5G_ENOMEM);
+      acc = 0;
+    }
+    R.ph_scal->n_used = acc;
+    R.ph_scal->fac = fac;
+    for (int q = 0; q < 4; q++) R.ph_scal->st0[q] = st0[q];
+    // the master has given 4W draws to the creation team and gives 4W to
+    // the absorption team
+    int st[4] = {st0[0], st0[1], st0[2], st0[3]};
+    mz_advance(st, 8ull * (unsigned long long)W, R.ph_jump);
+    for (int q = 0; q < 4; q++) R.ph_rng[q] = st[q];
+  }
+  __syncthreads();
+  const bool ok = R.ph_scal->n_used > 0;
+  // per-cell first photon number, in each thread's loop order
+  if (ok) {
+    for (int c = threadIdx.x; c < n_cr; c += NTHR) {
+      long long off = R.ph_ipart[c];
+      for (int lvl = 1; lvl <= R.max_lvl; lvl++) {
+        const int L = list_n(R, 1, lvl);
+        long long lo, len;
+        static_chunk(L, W, c, lo, len);
+        const int *lv = list_p(R, 1, lvl);
+        for (long long k = lo; k < lo + len; k++) {
+          const int id = lv[k];
+          const int nc = R.meta[id].nc, ncg = nc + 2;
+          for (int j = 1; j <= nc; j++)
+            for (int i = 1; i <= nc; i++) {
+              const size_t cell = (size_t)id * SLOT + i + ncg * j;
+              R.ph_cnt[cell] = (int)off;
+              off += R.ph_ncr[cell];
+            }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  // source cell of every photon
+  if (ok) {
+    const int *ids;
+    int n;
+    list_range(R, 1, 1, R.max_lvl, ids, n);
+    box_loop(ids, n, [&](int id, int t) {
+      const int nc = R.meta[id].nc, ncg = nc + 2;
+      if (t >= nc * nc) return;
+      const int cell = (t % nc + 1) + ncg * (t / nc + 1);
+      const size_t k = (size_t)id * SLOT + cell;
+      const int first = R.ph_cnt[k], cnt = R.ph_ncr[k];
+      const int code = id * SLOT + cell;
+      for (int q = 0; q < cnt; q++) R.ph_src[first + q] = code;
+    });
+  }
+  __syncthreads();
+  for (size_t k = threadIdx.x; k < (size_t)R.capacity * SLOT; k += NTHR) R.ph_cnt[k] = 0;
+  __syncthreads();
+}
+
+// LT_get_col on the photon table (fosito/m_lookup_table.f90:107-161)
+__device__ __forceinline__ double ph_dist(const RunDev &R, double x) {
+  double frac = (x - R.ph_xmin) * R.ph_inv_dx;
+  int ix;
+  double fr;
+  if (frac < 2.0e9 && frac > -2.0e9) {
+    ix = (int)ceil(frac);
+    fr = ix - frac;
+  } else {
+    ix = frac > 0 ? R.ph_rows : 0;
+    fr = 0;
+  }
+  if (ix < 1) {
+    ix = 1;
+    fr = 1;
+  } else if (ix >= R.ph_rows) {
+    ix = R.ph_rows - 1;
+    fr = 0;
+  }
+  return fr * R.ph_tbl[ix - 1] + (1 - fr) * R.ph_tbl[ix];
+}
+
+// ph_deposit: clear i_pho on levels 1..max_lvl, the source term from the
+// photon counts, then ghost cells and prolongation from the absorption
+// level (src/m_photons.f90:358-427).
+__device__ void ph_deposit(const RunDev &R) {
+  const double fac = R.ph_scal->fac;
+  const double tmp = fac * 2 * PI_DP;
+  {
+    const int *ids;
+    int n;
+    list_range(R, 0, 1, R.max_lvl, ids, n);
+    box_loop(ids, n, [&](int id, int t) {
+      const BoxMeta &m = R.meta[id];
+      const int ncg = m.nc + 2;
+      double *x = CC(R, I_PHO, id);
+      const int *cnt = R.ph_cnt + (size_t)id * SLOT;
+      for (int c = t; c < ncg * ncg; c += GT) {
+        const int k = cnt[c];
+        double v = 0;
+        if (k > 0) {
+          const double r0 = m.r0 + (c % ncg - 0.5) * m.dr;
+          const double add = R.ph_frac / (tmp * (m.dr * m.dr) * r0);
+          for (int q = 0; q < k; q++) v = v + add;
+        }
+        x[c] = v;
+      }
+    });
+  }
+  __syncthreads();
+  for (int lvl = max(R.ph_lvl, R.min_lvl); lvl <= R.max_lvl - 1; lvl++) {
+    const int *par = list_p(R, 2, lvl);
+    const int np = list_n(R, 2, lvl);
+    box_loop(par, np, [&](int id, int t) { gc_box(R, id, t, I_PHO, GC_INTERP); });
+    __syncthreads();
+    // a$D_prolong1_from(boxes, id, i_pho, add=.true.), m_aX_prolong.f90:81-191
+    box_loop(par, np, [&](int id, int t) {
+      const BoxMeta &pm = R.meta[id];
+      const int q = t >> 4, cc = t & 15;
+      const int cid = pm.ch[q];
+      if (cid <= 0) return;
+      const BoxMeta &m = R.meta[cid];
+      const int nc = m.nc, ncg = nc + 2, hnc = nc >> 1;
+      if (cc >= hnc * hnc) return;
+      int o0, o1;
+      child_offset(m, -1, o0, o1);
+      const int ii = cc % hnc + 1, jj = cc / hnc + 1;
+      const int i_c = ii + o0, j_c = jj + o1, i_f = 2 * ii - 1, j_f = 2 * jj - 1;
+      const int pg = pm.nc + 2;
+      const double *p = CC(R, I_PHO, id);
+      double *b = CC(R, I_PHO, cid);
+      const int pc = i_c + pg * j_c;
+      const double f0 = 0.5 * p[pc];
+      const double flx = 0.25 * p[pc - 1], fhx = 0.25 * p[pc + 1];
+      const double fly = 0.25 * p[pc - pg], fhy = 0.25 * p[pc + pg];
+      b[i_f + ncg * j_f] = f0 + flx + fly + b[i_f + ncg * j_f];
+      b[(i_f + 1) + ncg * j_f] = f0 + fhx + fly + b[(i_f + 1) + ncg * j_f];
+      b[i_f + ncg * (j_f + 1)] = f0 + flx + fhy + b[i_f + ncg * (j_f + 1)];
+      b[(i_f + 1) + ncg * (j_f + 1)] = f0 + fhx + fhy + b[(i_f + 1) + ncg * (j_f + 1)];
+    });
+    __syncthreads();
+  }
+}
+
+// One full time step, src/streamer_2d.f90:99-127; with deposit, the photon
+// source term of this step's photoionization first (src/streamer_cyl.f90:95-97)
+__device__ void step(const RunDev &R, double dt, bool deposit) {
+  if (deposit) ph_deposit(R);
   {
     const size_t n = (size_t)R.capacity * SLOT;
     const double *e = VAR(R, I_ELEC), *pi = VAR(R, I_PION);
@@ -1326,78 +1712,10 @@ __device__ void run_op(const RunDev &R, const Op &op) {
     case OP_DT_RED: dt_reductions(R); break;
     case OP_REF_FLAGS: ref_flags(R, op.d0); break;
     case OP_PROLONG_NEW: prolong_new(R); break;
-    case OP_STEP: step(R, op.d0); break;
-    case OP_DBG_BARRIERS:
-      for (int k = 0; k < op.i0; k++) __syncthreads();
-      break;
-    case OP_DBG_SWEEPS:
-    case OP_DBG_FILLS: {
-      MGV M{VAR(R, MP), VAR(R, MR), VAR(R, MT), R.boxes, R.pbx};
-      if (R.smem_doubles > 0 && op.i2) {
-        const int S = R.smem_doubles, nbx = R.bx_off[R.nlev], npb = R.pb_off[R.nlev];
-        BoxRec *sb = reinterpret_cast<BoxRec *>(g_dsmem + 3 * S);
-        int *spb = reinterpret_cast<int *>(sb + nbx);
-        const int4 *src = reinterpret_cast<const int4 *>(R.sboxes);
-        int4 *dst = reinterpret_cast<int4 *>(sb);
-        for (int k = threadIdx.x; k < nbx * 6; k += NTHR) dst[k] = src[k];
-        for (int k = threadIdx.x; k < npb; k += NTHR) spb[k] = R.pbx[k];
-        __syncthreads();
-        M = MGV{g_dsmem, g_dsmem + S, g_dsmem + 2 * S, sb, spb};
-        stage_mg(R, M, true);
-      }
-      for (int k = 0; k < op.i0; k++) {
-        if (op.code == OP_DBG_SWEEPS) p_sweep(R, M, op.i1, k + 1, false);
-        else p_fill(R, M, op.i1);
-      }
-      break;
-    }
-    case OP_DBG_EMPTY: {
-      // timestamps along one sweep item of level op.i1 (thread 0)
-      const LvlInfo L = lvl_info(R, op.i1);
-      MGV M{VAR(R, MP), VAR(R, MR), VAR(R, MT), R.boxes, R.pbx};
-      if (R.smem_doubles > 0 && op.i2) {
-        const int S = R.smem_doubles, nbx = R.bx_off[R.nlev], npb = R.pb_off[R.nlev];
-        BoxRec *sb = reinterpret_cast<BoxRec *>(g_dsmem + 3 * S);
-        int *spb = reinterpret_cast<int *>(sb + nbx);
-        const int4 *src = reinterpret_cast<const int4 *>(R.sboxes);
-        int4 *dst = reinterpret_cast<int4 *>(sb);
-        for (int k = threadIdx.x; k < nbx * 6; k += NTHR) dst[k] = src[k];
-        for (int k = threadIdx.x; k < npb; k += NTHR) spb[k] = R.pbx[k];
-        __syncthreads();
-        M = MGV{g_dsmem, g_dsmem + S, g_dsmem + 2 * S, sb, spb};
-        stage_mg(R, M, true);
-      }
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        long long t[8];
-        double *phi = M.phi;
-        t[0] = clock64();
-        const LvlInfo L2 = lvl_info(R, op.i1);
-        t[1] = clock64();
-        const BoxRec &B = M.boxes[L2.b0];
-        const int base = B.base;
-        t[2] = clock64();
-        const int g = base + 1 + L.ncg * 1;
-        double lx, hx, ly, hy;
-        phi_nbrs(R, phi, B, L.nc, L.ncg, 1, 1, g, lx, hx, ly, hy);
-        t[3] = clock64();
-        const double r = M.rhs[g];
-        phi[g] = 0.25 * (hx + lx + hy + ly - L.dr * L.dr * r);
-        t[4] = clock64();
-        double v = phi[g];
-        t[5] = clock64();
-        v = v * 1.0000001 + 0.5;
-        v = v * 1.0000001 + 0.5;
-        v = v * 1.0000001 + 0.5;
-        v = v * 1.0000001 + 0.5;
-        t[6] = clock64();
-        R.scal[8] = v;
-        t[7] = clock64();
-        for (int q = 0; q < 7; q++) R.scal[9 + q] = (double)(t[q + 1] - t[q]);
-      }
-      __syncthreads();
-      break;
-    }
+    case OP_STEP: step(R, op.d0, op.i0 != 0); break;
+    case OP_PH_SOURCE: ph_source(R, op.d0, op.i0 != 0); break;
+    case OP_PH_DEPOSIT: ph_deposit(R); break;
+    case OP_NOP: break;
     default: if (threadIdx.x == 0) atomicExch(R.status, A5G_EINVAL);
   }
 }
@@ -1419,7 +1737,7 @@ a5g_run_kernel(const RunDev *single, Op single_op, const RunDev *const *runs, co
 
 // One full time step of one run (a5g_step); a kernel of its own so that
 // profilers can select the hot launch by name.
-__global__ void __launch_bounds__(NTHR, 1) a5g_step_kernel(const RunDev *run, double dt) {
+__global__ void __launch_bounds__(NTHR, 1) a5g_step_kernel(const RunDev *run, double dt, int deposit) {
   __shared__ RunDev sR;
   {
     const int *s = reinterpret_cast<const int *>(run);
@@ -1427,7 +1745,7 @@ __global__ void __launch_bounds__(NTHR, 1) a5g_step_kernel(const RunDev *run, do
     for (int k = threadIdx.x; k < (int)(sizeof(RunDev) / sizeof(int)); k += NTHR) d[k] = s[k];
   }
   __syncthreads();
-  step(sR, dt);
+  step(sR, dt, deposit != 0);
 }
 
 // Descriptor of one member of a launch of a5g_step_batch_static.
@@ -1449,6 +1767,98 @@ __global__ void __launch_bounds__(NTHR, 1) a5g_run_kernel_slots(const BatchSlot 
   __syncthreads();
   Op op = slots[blockIdx.x].op;
   run_op(sR, op);
+}
+
+// Absorption of the photons of one photoionization call (PH_do_absorp,
+// src/m_photons.f90:161-205, then the radius, :318-329, and a$D_get_loc at
+// the absorption level, :331-344). Thread w of the team absorbs its static
+// chunk of the photons in order with its own generator (the master's draws
+// 4W + 4w + 1..4 of the call) and counts each photon in its absorbing cell.
+// blockIdx.y selects the run of a batch. The per-box geometry is staged in
+// shared memory when it fits (ph_smem: bytes available).
+constexpr int PH_THREADS = 256;
+__global__ void __launch_bounds__(PH_THREADS) a5g_photon_kernel(const RunDev *single,
+                                                               const RunDev *const *runs,
+                                                               const BatchSlot *slots,
+                                                               int ph_smem) {
+  const RunDev *rp = runs ? runs[blockIdx.y] : slots ? slots[blockIdx.y].run : single;
+  const RunDev &R = *rp;
+  if (!R.ph_enabled) return;
+  const long long W = R.ph_team;
+  const long long w0 = (long long)blockIdx.x * PH_THREADS;
+  if (w0 >= W) return;
+  const long long n_used = R.ph_scal->n_used;
+  if (n_used == 0) return;
+  const PhBox *tb = R.ph_boxes;
+  if ((size_t)R.n_ids * sizeof(PhBox) <= (size_t)ph_smem) {
+    PhBox *sb = reinterpret_cast<PhBox *>(g_dsmem);
+    for (int k = threadIdx.x; k < R.n_ids; k += PH_THREADS) sb[k] = R.ph_boxes[k];
+    __syncthreads();
+    tb = sb;
+  }
+  const long long w = w0 + threadIdx.x;
+  if (w >= W) return;
+  long long lo, len;
+  static_chunk(n_used, W, w, lo, len);
+  if (len == 0) return;
+  int st[4] = {R.ph_scal->st0[0], R.ph_scal->st0[1], R.ph_scal->st0[2], R.ph_scal->st0[3]};
+  mz_advance(st, 4ull * (unsigned long long)W + 4ull * (unsigned long long)w, R.ph_jump);
+  int rs[4];
+#pragma unroll
+  for (int q = 0; q < 4; q++) rs[q] = mz_int4(st);
+  const int *l1 = list_p(R, 0, 1);
+  const int n1 = list_n(R, 0, 1);
+  const int lvl_max = R.ph_lvl;
+  for (long long p = lo; p < lo + len; p++) {
+    const int code = R.ph_src[p];
+    const int sid = code / SLOT, cell = code - sid * SLOT;
+    const int si = cell % (NC + 2), sj = cell / (NC + 2);
+    const PhBox &S = tb[sid];
+    const double x0 = S.r0 + (si - 0.5) * S.dr, y0 = S.r1 + (sj - 0.5) * S.dr;
+    const double dist = ph_dist(R, mz_uni01(rs));
+    // RNG_t%sphere, fosito/m_random.f90:135-151
+    double a, b, ss;
+    int tries = 0;
+    while (true) {
+      a = -1.0 + mz_uni01(rs) * (1.0 - -1.0);
+      b = -1.0 + mz_uni01(rs) * (1.0 - -1.0);
+      ss = a * a + b * b;
+      if (ss <= 1) break;
+      if (++tries > 100000) {
+        atomicExch(R.status, A5G_ENONFINITE);
+        break;
+      }
+    }
+    const double t = sqrt(1 - ss);
+    const double sx = 2 * a * t * dist, sy = 2 * b * t * dist, sz = (1 - 2 * ss) * dist;
+    const double xo = x0 + sx, yo = y0 + sy, zo = 0.0 + sz;
+    const double x = sqrt(xo * xo + zo * zo), y = yo;
+    // a$D_get_loc (afivo/src/m_aX_utils.f90:244-299)
+    int id = -1;
+    for (int k = 0; k < n1; k++) {
+      const PhBox &B = tb[l1[k]];
+      const double xm = B.r0 + B.dr * B.nc, ym = B.r1 + B.dr * B.nc;
+      if (x >= B.r0 && y >= B.r1 && x <= xm && y <= ym) {
+        id = l1[k];
+        break;
+      }
+    }
+    if (id < 0) continue;
+    for (int guard = 0; guard < 64; guard++) {
+      const PhBox &B = tb[id];
+      if (!(B.lvl < lvl_max && B.ch[0] != 0)) break;
+      const double hc = (double)(B.nc >> 1);
+      const int i_ch = (x > B.r0 + B.dr * hc ? 1 : 0) + (y > B.r1 + B.dr * hc ? 2 : 0);
+      id = B.ch[i_ch];
+    }
+    const PhBox &B = tb[id];
+    const int ix = (int)ceil((x - B.r0) / B.dr), iy = (int)ceil((y - B.r1) / B.dr);
+    if (ix < 0 || iy < 0 || ix > B.nc + 1 || iy > B.nc + 1) {
+      atomicExch(R.status, A5G_EINVAL);
+      continue;
+    }
+    atomicAdd(R.ph_cnt + (size_t)id * SLOT + ix + (B.nc + 2) * iy, 1);
+  }
 }
 
 }  // namespace
@@ -1506,6 +1916,18 @@ struct a5g_ctx {
   BoxRec *p_boxes = nullptr;
   int *p_pbx = nullptr;
   size_t cap_boxes = 0, cap_pbx = 0;
+  // photoionization storage
+  bool has_ph_table = false;
+  double *ph_tbl = nullptr;
+  std::vector<double> h_ph_tbl;
+  int *ph_rng = nullptr, *ph_ncr = nullptr, *ph_cnt = nullptr, *ph_src = nullptr,
+      *ph_ipart = nullptr;
+  double *ph_part = nullptr;
+  PhScal *ph_scal = nullptr;
+  MzJump *ph_jump = nullptr;
+  PhBox *ph_boxes = nullptr;
+  int ph_capacity = 0;   // capacity the per-box photon buffers are sized for
+  size_t ph_src_cap = 0, ph_boxes_cap = 0;
 };
 
 // ---------------------------------------------------------------------------
@@ -1675,15 +2097,15 @@ static size_t dyn_smem_limit() {
     int optin = 0;
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     size_t stat = 0;
-    cudaFuncAttributes fa[3];
-    const void *fns[3] = {(const void *)a5g_run_kernel, (const void *)a5g_step_kernel,
-                          (const void *)a5g_run_kernel_slots};
-    for (int k = 0; k < 3; k++)
+    cudaFuncAttributes fa[4];
+    const void *fns[4] = {(const void *)a5g_run_kernel, (const void *)a5g_step_kernel,
+                          (const void *)a5g_run_kernel_slots, (const void *)a5g_photon_kernel};
+    for (int k = 0; k < 4; k++)
       if (cudaFuncGetAttributes(&fa[k], fns[k]) == cudaSuccess)
         stat = std::max(stat, fa[k].sharedSizeBytes);
     size_t avail = optin > (int)stat ? (size_t)optin - stat : 0;
     bool ok = true;
-    for (int k = 0; k < 3; k++)
+    for (int k = 0; k < 4; k++)
       ok = ok && cudaFuncSetAttribute(fns[k], cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)avail) == cudaSuccess;
     lim[dev] = ok ? avail : 0;
@@ -1709,11 +2131,103 @@ static int check_status(a5g_ctx *c) {
   return A5G_OK;
 }
 
+static Op mkop(int code, int i0 = 0, int i1 = 0, double d0 = 0) {
+  Op o{};
+  o.code = code;
+  o.i0 = i0;
+  o.i1 = i1;
+  o.d0 = d0;
+  return o;
+}
+
 static int launch(a5g_ctx *c, const Op &op) {
   if (!c) return fail(A5G_EINVAL, "null context");
   if (!c->has_tree) return fail(A5G_ESTATE, "no tree uploaded");
   if (!c->has_table) return fail(A5G_ESTATE, "no transport table set");
   a5g_run_kernel<<<1, NTHR, c->dyn_smem, c->stream>>>(c->d_run, op, nullptr, nullptr);
+  CK(cudaGetLastError());
+  return A5G_OK;
+}
+
+// Jumps of 2^b draws of the master generator (see mz_advance): the 3x3
+// matrix of (s1, s2, s3) -> (s2, s3, s1 - s3) mod m and the affine map
+// s4 -> 69069 s4 + 1013904243 mod 2^32, squared b times.
+static void mz_jump_table(MzJump *J) {
+  const unsigned long long m = MZ_M;
+  unsigned long long M[9] = {0, 1, 0, 0, 0, 1, 1, 0, m - 1};
+  unsigned int a = 69069u, cc = 1013904243u;
+  for (int b = 0; b < MZ_NJUMP; b++) {
+    for (int k = 0; k < 9; k++) J[b].m[k] = (unsigned int)M[k];
+    J[b].a = a;
+    J[b].c = cc;
+    unsigned long long N[9];
+    for (int r = 0; r < 3; r++)
+      for (int q = 0; q < 3; q++)
+        N[3 * r + q] = (M[3 * r] * M[q] % m + M[3 * r + 1] * M[3 + q] % m +
+                        M[3 * r + 2] * M[6 + q] % m) % m;
+    std::memcpy(M, N, sizeof(M));
+    cc = a * cc + cc;
+    a = a * a;
+  }
+}
+
+// Photon buffers sized for the current box capacity: counts per cell, one
+// source per photon (at most num_photons + one per leaf cell are created:
+// the expected total is at most num_photons and stochastic rounding adds at
+// most one per cell), and per-thread scratch.
+static int ph_resize(a5g_ctx *c) {
+  if (!c->p.photoi_enabled || c->capacity == c->ph_capacity) return A5G_OK;
+  const size_t cells = (size_t)c->capacity * SLOT;
+  const size_t src = (size_t)c->p.photoi_num_photons + (size_t)c->capacity * NC * NC + 1024;
+  if (src > (size_t)INT_MAX) return fail(A5G_EINVAL, "photon buffer above 2^31 entries");
+  CK(cudaStreamSynchronize(c->stream));
+  cudaFree(c->ph_ncr);
+  cudaFree(c->ph_cnt);
+  cudaFree(c->ph_src);
+  cudaFree(c->ph_ipart);
+  cudaFree(c->ph_part);
+  c->ph_ncr = c->ph_cnt = c->ph_src = c->ph_ipart = nullptr;
+  c->ph_part = nullptr;
+  if (cudaMalloc(&c->ph_ncr, cells * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&c->ph_cnt, cells * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&c->ph_src, src * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&c->ph_ipart, (size_t)c->capacity * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&c->ph_part, (size_t)c->capacity * sizeof(double)) != cudaSuccess)
+    return fail(A5G_ENOMEM, "cannot allocate photon buffers");
+  CK(cudaMemsetAsync(c->ph_ncr, 0, cells * sizeof(int), c->stream));
+  CK(cudaMemsetAsync(c->ph_cnt, 0, cells * sizeof(int), c->stream));
+  c->ph_capacity = c->capacity;
+  c->ph_src_cap = src;
+  RunDev &h = c->h;
+  h.ph_ncr = c->ph_ncr;
+  h.ph_cnt = c->ph_cnt;
+  h.ph_src = c->ph_src;
+  h.ph_ipart = c->ph_ipart;
+  h.ph_part = c->ph_part;
+  h.ph_cap = (int)src;
+  return A5G_OK;
+}
+
+static int ph_ready(a5g_ctx *c) {
+  if (!c->has_ph_table) return fail(A5G_ESTATE, "photoionization enabled but no photon table set");
+  return A5G_OK;
+}
+
+// Dynamic shared memory of a5g_photon_kernel for a run: its box geometry
+// table when that fits, else 0.
+static size_t ph_smem_bytes(const a5g_ctx *c) {
+  const size_t need = (size_t)(c->max_id + 1) * sizeof(PhBox);
+  return need <= dyn_smem_limit() ? need : 0;
+}
+
+// Photon sources and absorption of one call (the deposit follows, either as
+// its own launch or at the start of the step kernel).
+static int ph_launch_source_absorb(a5g_ctx *c, double dt, int has_dt) {
+  int r = launch(c, mkop(OP_PH_SOURCE, has_dt ? 1 : 0, 0, dt));
+  if (r) return r;
+  const size_t smem = ph_smem_bytes(c);
+  dim3 grid((unsigned)((c->p.photoi_team + PH_THREADS - 1) / PH_THREADS), 1);
+  a5g_photon_kernel<<<grid, PH_THREADS, smem, c->stream>>>(c->d_run, nullptr, nullptr, (int)smem);
   CK(cudaGetLastError());
   return A5G_OK;
 }
@@ -1734,6 +2248,12 @@ int a5g_create(const a5g_params *p, a5g_ctx **out) {
   if (p->n_seeds < 0 || p->n_seeds > 8) return fail(A5G_EINVAL, "n_seeds must be 0..8");
   if (p->lvls_max < 1 || p->lvls_max > 30) return fail(A5G_EINVAL, "lvls_max must be 1..30");
   if (!(p->dr_base > 0)) return fail(A5G_EINVAL, "dr_base must be > 0");
+  if (p->photoi_enabled) {
+    if (p->coord != 1)
+      return fail(A5G_EINVAL, "photoionization is built for the cylindrical form only");
+    if (p->photoi_team < 1 || p->photoi_num_photons < 0)
+      return fail(A5G_EINVAL, "photoi_team must be >= 1 and photoi_num_photons >= 0");
+  }
   a5g_ctx *c = new a5g_ctx();
   c->p = *p;
   cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
@@ -1768,6 +2288,26 @@ int a5g_create(const a5g_params *p, a5g_ctx **out) {
   }
   h.scal = c->scal;
   h.status = c->status;
+  if (p->photoi_enabled) {
+    MzJump J[MZ_NJUMP];
+    mz_jump_table(J);
+    if (cudaMalloc(&c->ph_rng, 4 * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&c->ph_scal, sizeof(PhScal)) != cudaSuccess ||
+        cudaMalloc(&c->ph_jump, sizeof(J)) != cudaSuccess) {
+      a5g_destroy(c);
+      return fail(A5G_ENOMEM, "cudaMalloc failed");
+    }
+    cudaMemcpy(c->ph_rng, p->rng_seed, 4 * sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemcpy(c->ph_jump, J, sizeof(J), cudaMemcpyHostToDevice);
+    cudaMemset(c->ph_scal, 0, sizeof(PhScal));
+    h.ph_enabled = 1;
+    h.ph_team = p->photoi_team;
+    h.ph_coeff = p->photoi_coeff;
+    h.ph_num_photons = (double)p->photoi_num_photons;
+    h.ph_rng = c->ph_rng;
+    h.ph_scal = c->ph_scal;
+    h.ph_jump = c->ph_jump;
+  }
   *out = c;
   return A5G_OK;
 }
@@ -1789,6 +2329,16 @@ int a5g_destroy(a5g_ctx *c) {
   cudaFree(c->p_boxes);
   cudaFree(c->p_sboxes);
   cudaFree(c->p_pbx);
+  cudaFree(c->ph_tbl);
+  cudaFree(c->ph_rng);
+  cudaFree(c->ph_ncr);
+  cudaFree(c->ph_cnt);
+  cudaFree(c->ph_src);
+  cudaFree(c->ph_ipart);
+  cudaFree(c->ph_part);
+  cudaFree(c->ph_scal);
+  cudaFree(c->ph_jump);
+  cudaFree(c->ph_boxes);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return A5G_OK;
@@ -1815,6 +2365,60 @@ int a5g_set_table(a5g_ctx *c, int n_rows, int n_cols, double x_min, double inv_d
   c->h.tbl_inv_dx = inv_dx;
   c->has_table = true;
   return push_run(c);
+}
+
+int a5g_set_photon_table(a5g_ctx *c, int n_rows, double x_min, double inv_dx, const double *dist,
+                         double frac_in_tbl) {
+  if (!c || !dist) return fail(A5G_EINVAL, "null argument");
+  if (!c->p.photoi_enabled) return fail(A5G_ESTATE, "photoionization is not enabled");
+  if (n_rows < 2 || !(inv_dx > 0) || !std::isfinite(x_min) || !(frac_in_tbl > 0))
+    return fail(A5G_EINVAL, "bad photon table");
+  cudaFree(c->ph_tbl);
+  c->ph_tbl = nullptr;
+  CK(cudaMalloc(&c->ph_tbl, sizeof(double) * n_rows));
+  CK(cudaMemcpy(c->ph_tbl, dist, sizeof(double) * n_rows, cudaMemcpyHostToDevice));
+  c->h_ph_tbl.assign(dist, dist + n_rows);
+  // pi_lengthscale = LT_get_col(tbl, 1, fac_dx) and get_lvl_length
+  // (src/m_photons.f90:142-155, 331-336)
+  double frac = (c->p.photoi_fac_dx - x_min) * inv_dx;
+  int ix = (int)std::ceil(frac);
+  double w = ix - frac;
+  if (ix < 1) {
+    ix = 1;
+    w = 1;
+  } else if (ix >= n_rows) {
+    ix = n_rows - 1;
+    w = 0;
+  }
+  const double length = w * dist[ix - 1] + (1 - w) * dist[ix];
+  const double invlog2 = 1 / std::log(2.0);
+  const double ratio = c->p.dr_base / length;
+  const int lvl = ratio <= 1 ? 1 : 1 + (int)std::ceil(std::log(ratio) * invlog2);
+  RunDev &h = c->h;
+  h.ph_tbl = c->ph_tbl;
+  h.ph_rows = n_rows;
+  h.ph_xmin = x_min;
+  h.ph_inv_dx = inv_dx;
+  h.ph_frac = frac_in_tbl;
+  h.ph_lvl = lvl;
+  c->has_ph_table = true;
+  return push_run(c);
+}
+
+int a5g_get_rng(a5g_ctx *c, int *st) {
+  if (!c || !st) return fail(A5G_EINVAL, "null argument");
+  if (!c->p.photoi_enabled) return fail(A5G_ESTATE, "photoionization is not enabled");
+  CK(cudaMemcpyAsync(st, c->ph_rng, 4 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return check_status(c);
+}
+
+int a5g_set_rng(a5g_ctx *c, const int *st) {
+  if (!c || !st) return fail(A5G_EINVAL, "null argument");
+  if (!c->p.photoi_enabled) return fail(A5G_ESTATE, "photoionization is not enabled");
+  CK(cudaMemcpyAsync(c->ph_rng, st, 4 * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return A5G_OK;
 }
 
 static int grow(a5g_ctx *c, int need) {
@@ -1857,7 +2461,7 @@ static int grow(a5g_ctx *c, int need) {
   c->capacity = cap;
   c->h.capacity = cap;
   c->h.cc = ncc; c->h.fx = nfx; c->h.fy = nfy; c->h.meta = nmeta; c->h.flags = nflags;
-  return A5G_OK;
+  return ph_resize(c);
 }
 
 int a5g_upload_tree(a5g_ctx *c, int max_id, int min_lvl, int max_lvl, const int *meta16,
@@ -1983,6 +2587,23 @@ int a5g_upload_tree(a5g_ctx *c, int max_id, int min_lvl, int max_lvl, const int 
   for (int li = 0; li < nlev; li++)
     for (int q = off[1][li]; q < off[1][li + 1]; q++) nl += (long long)hm[lists[q]].nc * hm[lists[q]].nc;
   c->n_leaf_cells = nl;
+  h.n_ids = max_id + 1;
+  if (c->p.photoi_enabled) {
+    std::vector<PhBox> pb(max_id + 1);
+    std::memset(pb.data(), 0, pb.size() * sizeof(PhBox));
+    for (int id = 1; id <= max_id; id++) {
+      if (!meta16[16 * id]) continue;
+      const BoxMeta &m = hm[id];
+      pb[id].r0 = m.r0;
+      pb[id].r1 = m.r1;
+      pb[id].dr = m.dr;
+      for (int q = 0; q < 4; q++) pb[id].ch[q] = m.ch[q];
+      pb[id].lvl = m.lvl;
+      pb[id].nc = m.nc;
+    }
+    if ((r = upload_vec(c, c->ph_boxes, c->ph_boxes_cap, pb))) return r;
+    h.ph_boxes = c->ph_boxes;
+  }
   c->has_tree = true;
   CK(cudaStreamSynchronize(c->stream));
   return push_run(c);
@@ -2032,15 +2653,6 @@ int a5g_download_fc(a5g_ctx *c, int dimf, int f, double *host) {
                      c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return check_status(c);
-}
-
-static Op mkop(int code, int i0 = 0, int i1 = 0, double d0 = 0) {
-  Op o{};
-  o.code = code;
-  o.i0 = i0;
-  o.i1 = i1;
-  o.d0 = d0;
-  return o;
 }
 
 int a5g_tree_copy_cc(a5g_ctx *c, int a, int b) {
@@ -2161,12 +2773,29 @@ int a5g_prolong_new(a5g_ctx *c, const int *n_new, const int *new_ids) {
   return A5G_OK;
 }
 
+int a5g_photoionization(a5g_ctx *c, double dt, int has_dt) {
+  if (!c) return fail(A5G_EINVAL, "null context");
+  if (!c->p.photoi_enabled) return fail(A5G_ESTATE, "photoionization is not enabled");
+  if (has_dt && !(dt > 0)) return fail(A5G_EINVAL, "dt must be > 0");
+  int r = ph_ready(c);
+  if (r) return r;
+  if ((r = ph_launch_source_absorb(c, dt, has_dt))) return r;
+  return launch(c, mkop(OP_PH_DEPOSIT));
+}
+
 int a5g_step(a5g_ctx *c, double dt) {
   if (!c) return fail(A5G_EINVAL, "null context");
   if (!(dt > 0)) return fail(A5G_EINVAL, "dt must be > 0");
   if (!c->has_tree) return fail(A5G_ESTATE, "no tree uploaded");
   if (!c->has_table) return fail(A5G_ESTATE, "no transport table set");
-  a5g_step_kernel<<<1, NTHR, c->dyn_smem, c->stream>>>(c->d_run, dt);
+  int deposit = 0;
+  if (c->p.photoi_enabled) {
+    int r = ph_ready(c);
+    if (r) return r;
+    if ((r = ph_launch_source_absorb(c, dt, 1))) return r;
+    deposit = 1;
+  }
+  a5g_step_kernel<<<1, NTHR, c->dyn_smem, c->stream>>>(c->d_run, dt, deposit);
   CK(cudaGetLastError());
   return A5G_OK;
 }
@@ -2180,21 +2809,42 @@ int a5g_step_batch(a5g_ctx **ctxs, int n, const double *dts) {
   }
   a5g_ctx *c0 = ctxs[0];
   std::vector<const RunDev *> rp(n);
-  std::vector<Op> ops(n);
+  std::vector<Op> ops(2 * n);
+  bool any_ph = false;
+  int max_team = 0;
+  size_t ph_smem = 0;
   for (int k = 0; k < n; k++) {
     rp[k] = ctxs[k]->d_run;
-    ops[k] = mkop(OP_STEP, 0, 0, dts[k]);
+    const bool ph = ctxs[k]->p.photoi_enabled != 0;
+    if (ph) {
+      int r = ph_ready(ctxs[k]);
+      if (r) return r;
+      any_ph = true;
+      max_team = std::max(max_team, ctxs[k]->p.photoi_team);
+      ph_smem = std::max(ph_smem, ph_smem_bytes(ctxs[k]));
+    }
+    ops[k] = mkop(OP_STEP, ph ? 1 : 0, 0, dts[k]);
+    ops[n + k] = ph ? mkop(OP_PH_SOURCE, 1, 0, dts[k]) : mkop(OP_NOP);
   }
   // other members' queued work must finish before the batch runs on c0's stream
   for (int k = 1; k < n; k++) CK(cudaStreamSynchronize(ctxs[k]->stream));
   const RunDev **d_rp = nullptr;
   Op *d_ops = nullptr;
   CK(cudaMallocAsync((void **)&d_rp, n * sizeof(void *), c0->stream));
-  CK(cudaMallocAsync((void **)&d_ops, n * sizeof(Op), c0->stream));
+  CK(cudaMallocAsync((void **)&d_ops, 2 * n * sizeof(Op), c0->stream));
   CK(cudaMemcpyAsync(d_rp, rp.data(), n * sizeof(void *), cudaMemcpyHostToDevice, c0->stream));
-  CK(cudaMemcpyAsync(d_ops, ops.data(), n * sizeof(Op), cudaMemcpyHostToDevice, c0->stream));
+  CK(cudaMemcpyAsync(d_ops, ops.data(), 2 * n * sizeof(Op), cudaMemcpyHostToDevice, c0->stream));
   size_t dyn = 0;
   for (int k = 0; k < n; k++) dyn = std::max(dyn, ctxs[k]->dyn_smem);
+  if (any_ph) {
+    // photon sources of every member with photoionization (the others run
+    // an operation that does nothing here), then the absorption
+    a5g_run_kernel<<<n, NTHR, dyn, c0->stream>>>(nullptr, Op{}, d_rp, d_ops + n);
+    CK(cudaGetLastError());
+    dim3 grid((unsigned)((max_team + PH_THREADS - 1) / PH_THREADS), (unsigned)n);
+    a5g_photon_kernel<<<grid, PH_THREADS, ph_smem, c0->stream>>>(nullptr, d_rp, nullptr, (int)ph_smem);
+    CK(cudaGetLastError());
+  }
   a5g_run_kernel<<<n, NTHR, dyn, c0->stream>>>(nullptr, Op{}, d_rp, d_ops);
   CK(cudaGetLastError());
   CK(cudaFreeAsync(d_rp, c0->stream));
@@ -2237,15 +2887,42 @@ int a5g_step_batch_static(a5g_ctx **ctxs, int n, const double *dts) {
   }
   a5g_ctx *c0 = ctxs[0];
   for (int k = 1; k < n; k++) CK(cudaStreamSynchronize(ctxs[k]->stream));
+  size_t dyn = 0, ph_smem = 0;
+  bool any_ph = false;
+  int max_team = 0;
+  for (int k = 0; k < n; k++) {
+    dyn = std::max(dyn, ctxs[k]->dyn_smem);
+    if (ctxs[k]->p.photoi_enabled) {
+      int r = ph_ready(ctxs[k]);
+      if (r) return r;
+      any_ph = true;
+      max_team = std::max(max_team, ctxs[k]->p.photoi_team);
+      ph_smem = std::max(ph_smem, ph_smem_bytes(ctxs[k]));
+    }
+  }
+  if (any_ph) {
+    // photon sources and absorption first; the table is then rewritten with
+    // the step descriptors (copies and launches are ordered on the stream)
+    for (int k = 0; k < n; k++) {
+      g_static_host[k].run = ctxs[k]->d_run;
+      g_static_host[k].op = ctxs[k]->p.photoi_enabled ? mkop(OP_PH_SOURCE, 1, 0, dts[k]) : mkop(OP_NOP);
+    }
+    CK(cudaMemcpyAsync(g_static_dev[dev], g_static_host, (size_t)n * sizeof(BatchSlot),
+                       cudaMemcpyHostToDevice, c0->stream));
+    a5g_run_kernel_slots<<<n, NTHR, dyn, c0->stream>>>(g_static_dev[dev]);
+    CK(cudaGetLastError());
+    dim3 grid((unsigned)((max_team + PH_THREADS - 1) / PH_THREADS), (unsigned)n);
+    a5g_photon_kernel<<<grid, PH_THREADS, ph_smem, c0->stream>>>(nullptr, nullptr, g_static_dev[dev],
+                                                                 (int)ph_smem);
+    CK(cudaGetLastError());
+  }
   for (int k = 0; k < n; k++) {
     g_static_host[k].run = ctxs[k]->d_run;
-    g_static_host[k].op = mkop(OP_STEP, 0, 0, dts[k]);
+    g_static_host[k].op = mkop(OP_STEP, ctxs[k]->p.photoi_enabled ? 1 : 0, 0, dts[k]);
   }
   // pageable source: the copy is staged before the call returns
   CK(cudaMemcpyAsync(g_static_dev[dev], g_static_host, (size_t)n * sizeof(BatchSlot),
                      cudaMemcpyHostToDevice, c0->stream));
-  size_t dyn = 0;
-  for (int k = 0; k < n; k++) dyn = std::max(dyn, ctxs[k]->dyn_smem);
   a5g_run_kernel_slots<<<n, NTHR, dyn, c0->stream>>>(g_static_dev[dev]);
   CK(cudaGetLastError());
   return A5G_OK;
@@ -2255,28 +2932,6 @@ int a5g_sync(a5g_ctx *c) {
   if (!c) return fail(A5G_EINVAL, "null context");
   CK(cudaStreamSynchronize(c->stream));
   return check_status(c);
-}
-
-// Internal diagnostics: run a timing probe (code 0: n barriers, 1: n
-// half-sweeps of level lvl, 2: n ghost fills of level lvl, 3: empty launch;
-// in_smem: stage the multigrid variables into shared memory first).
-int a5g_debug_op(a5g_ctx *c, int code, int n, int lvl, int in_smem) {
-  if (!c || n < 0) return fail(A5G_EINVAL, "bad argument");
-  if (code != 0 && code != 3 && (lvl < c->min_lvl || lvl > c->max_lvl)) return fail(A5G_EINVAL, "bad level");
-  Op o{};
-  o.code = code == 0 ? OP_DBG_BARRIERS : code == 1 ? OP_DBG_SWEEPS : code == 2 ? OP_DBG_FILLS : OP_DBG_EMPTY;
-  o.i0 = n;
-  o.i1 = lvl;
-  o.i2 = in_smem;
-  return launch(c, o);
-}
-
-// Internal diagnostics: copy of the 16-double scalar buffer.
-int a5g_debug_scal(a5g_ctx *c, double *out16) {
-  if (!c || !out16) return fail(A5G_EINVAL, "null argument");
-  CK(cudaMemcpyAsync(out16, c->scal, 16 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
-  return A5G_OK;
 }
 
 // Internal diagnostics (not part of the ABI headers): shared-memory use and

@@ -427,7 +427,89 @@ double interp_pairs(const double *xl, const double *yl, int n, double x) {
   return (1 - w) * yl[lo - 2] + w * yl[lo - 1];
 }
 
+// Photon absorption table, src/m_photons.f90:25-140. The absorption
+// function is the distance density of PH_absfunc_air (:122-140) with
+// coefficients c0 < c1 (per unit pressure) at pressure p.
+struct PhAbs {
+  double c0, c1, p;
+  double f(double dist) const {
+    const double eps = 2.220446049250313e-16;
+    const double r = p * dist;
+    if (r * (c0 + c1) < eps) return (c1 - c0 + 0.5 * (c0 * c0 - c1 * c1) * r) * p / std::log(c1 / c0);
+    if (r * c0 > -std::log(eps)) return eps;
+    return (std::exp(-c0 * r) - std::exp(-c1 * r)) / (dist * std::log(c1 / c0));
+  }
+  // rk4_drdF, :95-117
+  double drdF(double r, double dF) const {
+    const double one_sixth = 1 / 6.0;
+    double d = 1 / f(r);
+    double sum = d;
+    d = 1 / f(r + 0.5 * dF * d);
+    sum = sum + 2 * d;
+    d = 1 / f(r + 0.5 * dF * d);
+    sum = sum + 2 * d;
+    d = 1 / f(r + dF * d);
+    sum = sum + d;
+    return one_sixth * sum;
+  }
+};
+
 }  // namespace
+
+extern "C" int a5t_photon_table(int kind, double a, double b, double max_dist, double *dist_out,
+                                double *frac_out, int *n_rows) {
+  if (!dist_out || !frac_out || !n_rows) return err(A5G_EINVAL, "null argument");
+  if (!(max_dist > 0)) return err(A5G_EINVAL, "max_dist must be > 0");
+  // fosito/m_units_constants.f90:44, a single-precision literal times 1.0D-5
+  const double torr_to_bar = (double)133.322368f * 1.0e-5;
+  PhAbs fn;
+  if (kind == 0) {
+    if (!(a > 0)) return err(A5G_EINVAL, "O2 partial pressure must be > 0");
+    fn = PhAbs{3.5 / torr_to_bar, 200 / torr_to_bar, a};
+  } else if (kind == 1) {
+    if (!(a > 0 && a < b)) return err(A5G_EINVAL, "need 0 < shortest < longest absorption length");
+    fn = PhAbs{1 / b, 1 / a, 1.0};
+  } else {
+    return err(A5G_EINVAL, "photon table kind must be 0 or 1");
+  }
+  const int tbl_size = 500;
+  double frac_guess = 1.0;
+  for (int it = 0; it < 5; it++) {
+    const double dF = frac_guess / (tbl_size - 1);
+    double r = 0, F = 0;
+    for (long guard = 0;; guard++) {
+      r = r + dF * fn.drdF(r, dF);
+      F = F + dF;
+      if (r > max_dist) break;
+      if (guard > 100000000L) return err(A5G_EINVAL, "photon table integration does not reach max_dist");
+    }
+    frac_guess = F;
+  }
+  std::vector<double> fsum(2 * tbl_size), dist(2 * tbl_size);
+  const double dF = frac_guess / (tbl_size - 1);
+  fsum[0] = dist[0] = 0;
+  int used = 2 * tbl_size;  // entries 0..used-1 are the table's input pairs
+  for (int k = 1; k < 2 * tbl_size; k++) {
+    const double d = fn.drdF(dist[k - 1], dF);
+    fsum[k] = fsum[k - 1] + dF;
+    dist[k] = dist[k - 1] + dF * d;
+    if (dist[k] > max_dist) {
+      used = k;
+      break;
+    }
+  }
+  if (used + 1 > tbl_size + 10) return err(A5G_EINVAL, "photon table: integration accuracy fail");
+  const double norm = fsum[used - 1];
+  for (int k = 0; k < used; k++) fsum[k] = fsum[k] / norm;
+  // LT_create(0, 1, tbl_size, 1) + LT_set_col (fosito/m_lookup_table.f90:46-72)
+  const double inv_dx = (tbl_size - 1) / (1.0 - 0.0);
+  const double dx = 1 / inv_dx;
+  for (int ix = 1; ix <= tbl_size; ix++)
+    dist_out[ix - 1] = interp_pairs(fsum.data(), dist.data(), used, 0.0 + (ix - 1) * dx);
+  *frac_out = norm;
+  *n_rows = tbl_size;
+  return A5G_OK;
+}
 
 struct a5s_sim {
   a5s_config cfg{};
@@ -551,6 +633,17 @@ int a5s_create(const a5s_config *cfg, a5s_sim **out) {
     a5s_destroy(s);
     return r;
   }
+  if (cfg->dev.photoi_enabled) {
+    // src/m_streamer.f90:327-330
+    double dist[500], frac = 0;
+    int rows = 0;
+    if ((r = a5t_photon_table(cfg->photoi_tbl_kind, cfg->photoi_tbl_a, cfg->photoi_tbl_b,
+                              cfg->photoi_max_dist, dist, &frac, &rows)) ||
+        (r = a5g_set_photon_table(s->ctx, rows, 0.0, (rows - 1) / 1.0, dist, frac))) {
+      a5s_destroy(s);
+      return r;
+    }
+  }
   *out = s;
   return A5G_OK;
 }
@@ -576,6 +669,8 @@ int a5s_init(a5s_sim *s, int *n_iter) {
     if (na == 0 || it > 100) break;
   }
   if (n_iter) *n_iter = it;
+  // src/streamer_cyl.f90:68-69
+  if (s->cfg.dev.photoi_enabled && (r = a5g_photoionization(s->ctx, 0.0, 0))) return r;
   return a5g_sync(s->ctx);
 }
 

@@ -52,7 +52,26 @@ def make_params(cfg) -> _lib.Params:
             p.seed_r0[n][d] = s.r0[d]
             p.seed_r1[n][d] = s.r1[d]
         p.seed_width[n] = s.width
+    p.photoi_enabled = 1 if cfg.photoi_enabled else 0
+    p.photoi_num_photons = cfg.photoi_num_photons
+    p.photoi_team = cfg.photoi_team
+    p.photoi_coeff = cfg.photoi_coeff
+    p.photoi_fac_dx = cfg.photoi_fac_dx
+    for i in range(4):
+        p.rng_seed[i] = cfg.rng_seed[i]
     return p
+
+
+def photon_table(cfg) -> Tuple[np.ndarray, float]:
+    """PH_get_tbl_air-style absorption table of a configuration
+    (src/m_photons.f90:25-93) built by the library's host code: 500
+    distances at cumulative fractions (i-1)/499, and frac_in_tbl."""
+    kind, a, b = cfg.photoi_table
+    dist = np.zeros(500)
+    frac, n = ctypes.c_double(0), ctypes.c_int(0)
+    call("a5t_photon_table", 0 if kind == "air" else 1, a, b, cfg.photoi_max_dist, _dp(dist),
+         ctypes.byref(frac), ctypes.byref(n))
+    return dist[:n.value], frac.value
 
 
 class DeviceRun:
@@ -177,6 +196,27 @@ class DeviceRun:
 
     def step(self, dt: float):
         call("a5g_step", self.h, dt)
+
+    def set_photon_table(self, dist: np.ndarray, frac_in_tbl: float, x_min: float = 0.0,
+                         inv_dx: float | None = None):
+        d = np.ascontiguousarray(dist, dtype=np.float64)
+        if inv_dx is None:
+            inv_dx = (len(d) - 1) / 1.0
+        call("a5g_set_photon_table", self.h, len(d), x_min, inv_dx, _dp(d), frac_in_tbl)
+
+    def photoionization(self, dt: float | None):
+        """set_photoionization (src/streamer_cyl.f90:572-593); dt None is the
+        call before the time loop."""
+        call("a5g_photoionization", self.h, 0.0 if dt is None else dt, 0 if dt is None else 1)
+
+    def rng_state(self) -> np.ndarray:
+        st = np.zeros(4, dtype=np.int32)
+        call("a5g_get_rng", self.h, _ip(st))
+        return st
+
+    def set_rng_state(self, st) -> None:
+        st = np.ascontiguousarray(st, dtype=np.int32)
+        call("a5g_set_rng", self.h, _ip(st))
 
     def sync(self):
         call("a5g_sync", self.h)

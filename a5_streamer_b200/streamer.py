@@ -137,6 +137,10 @@ class Simulation:
         sc.num_steps_amr = cfg.num_steps_amr
         sc.lkptbl_size = cfg.lkptbl_size
         sc.lkptbl_max_fld = cfg.lkptbl_max_fld
+        kind, a, b = cfg.photoi_table
+        sc.photoi_tbl_kind = 0 if kind == "air" else 1
+        sc.photoi_tbl_a, sc.photoi_tbl_b = a, b
+        sc.photoi_max_dist = cfg.photoi_max_dist
         self._keep = []
         for c, name in enumerate(TD_COLUMNS):
             xs = np.ascontiguousarray(cfg.td[name][0], dtype=np.float64)

@@ -63,6 +63,17 @@ typedef struct a5g_params {
   double seed_r0[8][2];
   double seed_r1[8][2];
   double seed_width[8];
+  /* Monte Carlo photoionization, cylindrical form only: set_photoionization
+   * (src/streamer_cyl.f90:572-617) and PH_set_src_2d with a constant
+   * absorption level (src/m_photons.f90:207-436). */
+  int photoi_enabled;
+  int photoi_num_photons; /* ST_photoi_num_photons */
+  int photoi_team;        /* OpenMP team whose execution of the photon loops
+                             is reproduced; see a5g_photoionization */
+  int photoi_pad;
+  double photoi_coeff;    /* photons per ionization (photoi_eta * quench factor) */
+  double photoi_fac_dx;   /* table fraction that sets the absorption level (0.25e-3) */
+  int rng_seed[4];        /* state of the master generator ST_rng */
 } a5g_params;
 
 /* Box metadata for a5g_upload_tree: per id (0..max_id) 16 ints
@@ -90,6 +101,18 @@ int a5g_destroy(a5g_ctx *ctx);
  * alpha, eta (src/m_streamer.f90:37-41). */
 int a5g_set_table(a5g_ctx *ctx, int n_rows, int n_cols, double x_min,
                   double inv_dx, const double *rows_cols);
+
+/* Photon absorption table: replaces PH_tbl_t (src/m_photons.f90:9-12).
+ * dist[i] is the absorption distance at cumulative fraction
+ * x_min + i / inv_dx (i = 0..n_rows-1), frac_in_tbl the fraction of photons
+ * inside the table's range. Also fixes the absorption level
+ * get_lvl_length(dr_base, LT_get_col(tbl, photoi_fac_dx))
+ * (src/m_photons.f90:142-155, 331-336). */
+int a5g_set_photon_table(a5g_ctx *ctx, int n_rows, double x_min, double inv_dx,
+                         const double *dist, double frac_in_tbl);
+/* State of the master generator (4 int32, fosito/m_random.f90 RNG_t). */
+int a5g_get_rng(a5g_ctx *ctx, int *state4);
+int a5g_set_rng(a5g_ctx *ctx, const int *state4);
 
 /* Topology upload after a$D_set_base / a$D_adjust_refinement
  * (afivo/src/m_aX_core.f90:134-217, 456-520). Cell and face data of ids
@@ -142,10 +165,26 @@ int a5g_ref_flags(a5g_ctx *ctx, double time, int *flags);
 /* prolong_to_new_boxes, src/streamer_2d.f90:592-617: for each level
  * min_lvl..max_lvl in turn, n_new[k] ids taken from new_ids in order. */
 int a5g_prolong_new(a5g_ctx *ctx, const int *n_new, const int *new_ids);
+/* set_photoionization(tree, eta, num_photons[, dt])
+ * (src/streamer_cyl.f90:572-593): photon production per leaf cell, then
+ * PH_set_src_2d (src/m_photons.f90:207-436): photons created by stochastic
+ * rounding, absorbed at a sampled distance in a random direction, counted
+ * per cell at the absorption level, then ghost cells and prolongation.
+ * has_dt = 0 is the call before the time loop (no dt argument).
+ * The reference runs these loops in OpenMP regions whose outcome depends on
+ * the team: every thread draws from its own generator seeded from the master
+ * (PRNG_t), loops are split by the static schedule, and photons are
+ * numbered in the order threads pass a critical section. This call
+ * reproduces the execution with photoi_team threads that pass that section
+ * in thread order and add the partial sums of a$D_tree_sum_cc in thread
+ * order, an execution the reference takes with OMP_NUM_THREADS equal to
+ * photoi_team. The master generator advances by 8 * photoi_team draws. */
+int a5g_photoionization(a5g_ctx *ctx, double dt, int has_dt);
 /* One full time step on the current mesh (src/streamer_2d.f90:93-128, one
- * iteration of the n loop): save old densities, two forward-Euler stages
- * with a field solve after the first, trapezoidal average, field solve.
- * Runs as a single device launch. */
+ * iteration of the n loop): set_photoionization when enabled, save old
+ * densities, two forward-Euler stages with a field solve after the first,
+ * trapezoidal average, field solve. Without photoionization it is a single
+ * device launch; with it, three (photon sources, absorption, step). */
 int a5g_step(a5g_ctx *ctx, double dt);
 /* The same step for several independent runs in one launch (one persistent
  * thread block per run). dts[k] is the step of run k. */

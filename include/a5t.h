@@ -47,6 +47,16 @@ int a5t_n_level_ids(a5t_tree *t);
  * (ref_info%lvls(lvl)%add). Returns the total. */
 int a5t_new_boxes(a5t_tree *t, int *counts, int *ids);
 
+/* Photon absorption table: PH_get_tbl_air (src/m_photons.f90:25-140),
+ * 500 absorption distances at cumulative fractions (i-1)/499 over
+ * [0, max_dist], and the fraction of photons inside that range.
+ * kind 0: air, a = O2 partial pressure (bar), the absorption function
+ * PH_absfunc_air; kind 1: absorption length log-uniform in [a, b] (m), the
+ * same function with coefficients 1/b and 1/a. dist needs 500 entries;
+ * n_rows receives the number of rows (500). */
+int a5t_photon_table(int kind, double a, double b, double max_dist, double *dist,
+                     double *frac_in_tbl, int *n_rows);
+
 typedef struct a5s_config {
   a5g_params dev;
   int n_base[2];            /* base boxes per direction */
@@ -60,6 +70,11 @@ typedef struct a5s_config {
   int td_n[4];              /* transport input pairs per column */
   const double *td_x[4];
   const double *td_y[4];
+  /* photon table when dev.photoi_enabled (see a5t_photon_table); the
+   * reference's range is 2 * domain length (src/m_streamer.f90:327-330) */
+  int photoi_tbl_kind;
+  double photoi_tbl_a, photoi_tbl_b;
+  double photoi_max_dist;
 } a5s_config;
 
 typedef struct a5s_sim a5s_sim;

@@ -16,6 +16,7 @@
 #include <array>
 #include <climits>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <functional>
 #include <vector>
@@ -1065,6 +1066,159 @@ static inline double lt_get_col(const LT &t, int col, double x) {
 }
 
 // ---------------------------------------------------------------------------
+// Random numbers, fosito/m_random.f90. RNG_t holds four default integers and
+// draws with Marsaglia's mzran. The reference's integer arithmetic wraps on
+// overflow (two's complement, as its gfortran x86-64 build computes it);
+// restated here with unsigned arithmetic.
+struct Rng {
+  int32_t st[4] = {521288629, 362436069, 16163801, 1131199299};  // :12-13
+  // int4, :58-66
+  int32_t int4() {
+    int32_t rr = (int32_t)((uint32_t)st[0] - (uint32_t)st[2]);
+    if (rr < 0) rr = (int32_t)((uint32_t)rr + 2147483579u);
+    st[0] = st[1];
+    st[1] = st[2];
+    st[2] = rr;
+    st[3] = (int32_t)(69069u * (uint32_t)st[3] + 1013904243u);
+    return (int32_t)((uint32_t)rr + (uint32_t)st[3]);
+  }
+  // uni_01, :75-80: 0.5 + 2^-32 * int4, exact in double
+  double uni_01() { return 0.5 + 0x1p-32 * (double)int4(); }
+  // uni_ab, :83-88
+  double uni_ab(double a, double b) { return a + uni_01() * (b - a); }
+  // sphere, :135-151 (Marsaglia's method)
+  void sphere(double radius, double xyz[3]) {
+    double r0, r1, ss;
+    while (true) {
+      r0 = uni_ab(-1.0, 1.0);
+      r1 = uni_ab(-1.0, 1.0);
+      ss = r0 * r0 + r1 * r1;
+      if (ss <= 1) break;
+    }
+    double t = std::sqrt(1 - ss);
+    xyz[0] = 2 * r0 * t;
+    xyz[1] = 2 * r1 * t;
+    xyz[2] = 1 - 2 * ss;
+    for (int d = 0; d < 3; d++) xyz[d] = xyz[d] * radius;
+  }
+};
+
+// PRNG_t%init, fosito/m_random.f90:44-55: stream n takes the master's draws
+// 4n+1..4n+4 (0-based n).
+static std::vector<Rng> prng_init(Rng &master, int n_proc) {
+  std::vector<Rng> r(n_proc);
+  for (int n = 0; n < n_proc; n++)
+    for (int i = 0; i < 4; i++) r[n].st[i] = master.int4();
+  return r;
+}
+
+// libgomp's static schedule without a chunk size: iterations [lo, lo+len) of
+// thread c out of n_threads for n iterations.
+static inline void static_chunk(long n, long n_threads, long c, long &lo, long &len) {
+  long q = n / n_threads, t = n % n_threads;
+  if (c < t) {
+    q++;
+    t = 0;
+  }
+  lo = q * c + t;
+  len = q;
+}
+
+// ---------------------------------------------------------------------------
+// Photon absorption table, src/m_photons.f90:25-140. The absorption function
+// is PH_absfunc_air (:122-140) with its two absorption coefficients c0 < c1
+// (1/(m bar)) at O2 pressure p: (exp(-c0 p d) - exp(-c1 p d)) / (d log(c1/c0)),
+// the distance density of an exponential absorption whose coefficient is
+// log-uniform on [c0 p, c1 p]. A log-uniform absorption length [l_lo, l_hi]
+// is the same function with c0 = 1/l_hi, c1 = 1/l_lo and p = 1.
+struct AbsFn {
+  double c0, c1, p;
+};
+// fosito/m_units_constants.f90:44: one Torr in bar, written with a default
+// (single precision) real literal times 1.0D-5.
+static const double UC_TORR_TO_BAR = (double)133.322368f * 1.0e-5;
+
+static AbsFn absfn_air(double p_O2) {
+  return AbsFn{3.5 / UC_TORR_TO_BAR, 200 / UC_TORR_TO_BAR, p_O2};
+}
+static AbsFn absfn_logu(double len_lo, double len_hi) {
+  return AbsFn{1 / len_hi, 1 / len_lo, 1.0};
+}
+
+// src/m_photons.f90:122-140 (PH_absfunc_air)
+static double absfunc(const AbsFn &a, double dist) {
+  const double eps = 2.220446049250313e-16;
+  double r = a.p * dist;
+  if (r * (a.c0 + a.c1) < eps)
+    return (a.c1 - a.c0 + 0.5 * (a.c0 * a.c0 - a.c1 * a.c1) * r) * a.p / std::log(a.c1 / a.c0);
+  if (r * a.c0 > -std::log(eps)) return eps;
+  return (std::exp(-a.c0 * r) - std::exp(-a.c1 * r)) / (dist * std::log(a.c1 / a.c0));
+}
+
+// src/m_photons.f90:95-117 (rk4_drdF)
+static double rk4_drdF(const AbsFn &a, double r, double dF) {
+  const double one_sixth = 1 / 6.0;
+  double drdF = 1 / absfunc(a, r);
+  double sum = drdF;
+  drdF = 1 / absfunc(a, r + 0.5 * dF * drdF);
+  sum = sum + 2 * drdF;
+  drdF = 1 / absfunc(a, r + 0.5 * dF * drdF);
+  sum = sum + 2 * drdF;
+  drdF = 1 / absfunc(a, r + dF * drdF);
+  sum = sum + drdF;
+  return one_sixth * sum;
+}
+
+struct PhTbl {
+  LT tbl;
+  double frac_in_tbl = 0;
+};
+
+// src/m_photons.f90:25-93 (PH_get_tbl_air) for a given absorption function
+static bool ph_get_tbl(const AbsFn &a, double max_dist, PhTbl &out) {
+  const int tbl_size = 500;
+  double frac_guess = 1.0;
+  for (int n = 1; n <= 5; n++) {
+    double dF = frac_guess / (tbl_size - 1), r = 0, F = 0;
+    while (true) {
+      double drdF = rk4_drdF(a, r, dF);
+      r = r + dF * drdF;
+      F = F + dF;
+      if (r > max_dist) {
+        frac_guess = F;
+        break;
+      }
+    }
+  }
+  std::vector<double> fsum(2 * tbl_size), dist(2 * tbl_size);
+  double dF = frac_guess / (tbl_size - 1);
+  dist[0] = 0;
+  fsum[0] = 0;
+  int n;  // 1-based index at exit, as the Fortran loop variable
+  for (n = 2; n <= 2 * tbl_size; n++) {
+    double drdF = rk4_drdF(a, dist[n - 2], dF);
+    fsum[n - 1] = fsum[n - 2] + dF;
+    dist[n - 1] = dist[n - 2] + dF * drdF;
+    if (dist[n - 1] > max_dist) break;
+  }
+  if (n > tbl_size + 10) return false;  // "integration accuracy fail"
+  out.frac_in_tbl = fsum[n - 2];
+  const double norm = fsum[n - 2];
+  for (int k = 0; k < n - 1; k++) fsum[k] = fsum[k] / norm;
+  out.tbl = lt_create(0.0, 1.0, tbl_size, 1);
+  lt_set_col(out.tbl, 0, fsum.data(), dist.data(), n - 1);
+  return true;
+}
+
+// src/m_photons.f90:142-155 (get_lvl_length)
+static int get_lvl_length(double dr_base, double length) {
+  const double invlog2 = 1 / std::log(2.0);
+  double ratio = dr_base / length;
+  if (ratio <= 1) return 1;
+  return 1 + (int)std::ceil(std::log(ratio) * invlog2);
+}
+
+// ---------------------------------------------------------------------------
 // Streamer model, src/streamer_2d.f90 and src/streamer_cyl.f90
 struct Sim {
   a5ref_params p;
@@ -1073,6 +1227,9 @@ struct Sim {
   MG mg;
   double time = 0;
   double applied_voltage = 0;
+  Rng rng;       // ST_rng (src/m_streamer.f90:69)
+  PhTbl ph;      // ST_photoi_tbl
+  int pho_lvl = 1;
 };
 
 // src/m_streamer.f90:339-362 (koren_mlim)
@@ -1406,6 +1563,7 @@ static void update_solution(Sim &s, Box &b, double dt) {
       double dflux[2] = {b.Fx(i, j, F_ELEC) + b.Fx(i + 1, j, F_ELEC),
                          b.Fy(i, j, F_ELEC) + b.Fy(i, j + 1, F_ELEC)};
       double src = 0.5 * norm2(dflux, 2) * (alpha - eta);
+      if (s.p.photoi_enabled) src = src + b.c(i, j, I_PHO);
       double sflux;
       if (cyl) {
         double den = i + ioff - 0.5;
@@ -1469,9 +1627,220 @@ static double get_max_dt(Sim &s) {
   return 0.5 * m;
 }
 
-// src/streamer_2d.f90:99-127, one iteration of the n loop at fixed dt
+// afivo/src/m_aX_utils.f90:244-299 (a$D_get_loc with child_that_contains)
+static void get_loc(Tree &t, const double rr[2], int max_lvl, int &id_out, int ix[2]) {
+  const Level &L1 = t.L(1);
+  int id = 0;
+  size_t i;
+  for (i = 0; i < L1.ids.size(); i++) {
+    id = L1.ids[i];
+    const Box &b = t.boxes[id];
+    bool inside = true;
+    for (int d = 0; d < 2; d++) {
+      double r_max = b.r_min[d] + b.dr * b.n_cell;
+      if (!(rr[d] >= b.r_min[d] && rr[d] <= r_max)) inside = false;
+    }
+    if (inside) break;
+  }
+  if (i == L1.ids.size()) {
+    id_out = -1;
+    ix[0] = ix[1] = -1;
+    return;
+  }
+  while (t.boxes[id].lvl < max_lvl && has_children(t.boxes[id])) {
+    const Box &b = t.boxes[id];
+    int i_ch = 0;
+    for (int d = 0; d < 2; d++) {
+      double cntr = b.r_min[d] + b.dr * (b.n_cell >> 1);
+      if (rr[d] > cntr) i_ch += 1 << d;
+    }
+    id = b.children[i_ch];
+  }
+  const Box &b = t.boxes[id];
+  id_out = id;
+  for (int d = 0; d < 2; d++) ix[d] = (int)std::ceil((rr[d] - b.r_min[d]) / b.dr);
+}
+
+// afivo/src/m_aX_prolong.f90:99-191 (a$D_prolong1_to) with add = .true.
+static void prolong1_add(Tree &t, int id, int iv) {
+  Box &b = t.boxes[id];
+  const Box &p = t.boxes[b.parent];
+  int nc = b.n_cell, hnc = nc >> 1, off[2];
+  child_offset(b, -1, off);
+  for (int j = 1; j <= hnc; j++) {
+    int j_c = j + off[1], j_f = 2 * j - 1;
+    for (int i = 1; i <= hnc; i++) {
+      int i_c = i + off[0], i_f = 2 * i - 1;
+      double f0 = 0.5 * p.c(i_c, j_c, iv);
+      double flx = 0.25 * p.c(i_c - 1, j_c, iv), fhx = 0.25 * p.c(i_c + 1, j_c, iv);
+      double fly = 0.25 * p.c(i_c, j_c - 1, iv), fhy = 0.25 * p.c(i_c, j_c + 1, iv);
+      b.c(i_f, j_f, iv) = f0 + flx + fly + b.c(i_f, j_f, iv);
+      b.c(i_f + 1, j_f, iv) = f0 + fhx + fly + b.c(i_f + 1, j_f, iv);
+      b.c(i_f, j_f + 1, iv) = f0 + flx + fhy + b.c(i_f, j_f + 1, iv);
+      b.c(i_f + 1, j_f + 1, iv) = f0 + fhx + fhy + b.c(i_f + 1, j_f + 1, iv);
+    }
+  }
+}
+
+// afivo/src/m_aX_utils.f90:623-656 (a$D_tree_sum_cc) run by a team of W
+// threads: thread c sums fac * (box sum) over its static chunk of each
+// level's leaves in level order; the partial sums are then added in thread
+// order to the initial 0. Threads without boxes hold +0 and change nothing.
+static double tree_sum_team(Tree &t, int iv, long W) {
+  const double twopi = 2 * std::acos(-1.0);
+  long n_busy = 0;
+  for (int lvl = t.min_lvl; lvl <= t.max_lvl; lvl++)
+    n_busy = std::max(n_busy, (long)t.L(lvl).leaves.size());
+  n_busy = std::min(n_busy, W);
+  double total = 0;
+  for (long c = 0; c < n_busy; c++) {
+    double my = 0;
+    for (int lvl = t.min_lvl; lvl <= t.max_lvl; lvl++) {
+      const double dr = t.dr_base * std::pow(0.5, lvl - 1);
+      const double fac = dr * dr;
+      const Level &L = t.L(lvl);
+      long lo, len;
+      static_chunk((long)L.leaves.size(), W, c, lo, len);
+      for (long k = lo; k < lo + len; k++) {
+        const Box &b = t.boxes[L.leaves[k]];
+        const int nc = b.n_cell;
+        double tmp = 0;
+        if (t.coord == CYL) {
+          // sum_2pr_box, :661-678
+          for (int j = 1; j <= nc; j++)
+            for (int i = 1; i <= nc; i++) tmp = tmp + b.c(i, j, iv) * (b.r_min[0] + (i - 0.5) * b.dr);
+          tmp = tmp * twopi;
+        } else {
+          for (int j = 1; j <= nc; j++)
+            for (int i = 1; i <= nc; i++) tmp = tmp + b.c(i, j, iv);
+        }
+        my = my + fac * tmp;
+      }
+    }
+    total = total + my;
+  }
+  return total;
+}
+
+// src/streamer_cyl.f90:595-617 (set_photoi_rate) on one leaf box
+static void set_photoi_rate(Sim &s, Box &b, double coeff) {
+  const int nc = b.n_cell;
+  for (int j = 1; j <= nc; j++)
+    for (int i = 1; i <= nc; i++) {
+      double fld = b.c(i, j, I_FLD);
+      Loc loc = lt_get_loc(s.td, fld);
+      double alpha = lt_col_at(s.td, I_ALPHA, loc);
+      double mobility = lt_col_at(s.td, I_MOBILITY, loc);
+      double tmp = fld * mobility * alpha * b.c(i, j, I_ELEC) * coeff;
+      if (tmp < 0) tmp = 0;
+      b.c(i, j, I_PHO) = tmp;
+    }
+}
+
+// src/streamer_cyl.f90:572-593 (set_photoionization) and
+// src/m_photons.f90:207-436 (PH_set_src_2d with i_src = i_pho, fac_dx,
+// const_dx = .true., use_cyl = .true.), as run by a team of W threads (see
+// a5ref.h): creation in thread order, absorption in static chunks.
+static void set_photoionization(Sim &s, double dt, bool has_dt) {
+  Tree &t = s.tree;
+  const a5ref_params &p = s.p;
+  const long W = p.photoi_team;
+  const int nc = t.n_cell;
+  const double pi = std::acos(-1.0);
+  loop_leaves(t, [&](Box &b, int) { set_photoi_rate(s, b, p.photoi_coeff); });
+  double sum_production = tree_sum_team(t, I_PHO, W);
+  const double eps = 2.220446049250313e-16;
+  double fac = p.photoi_num_photons / (sum_production + eps);
+  if (has_dt) fac = dt < fac ? dt : fac;
+  // photon creation, :263-306
+  std::vector<Rng> rngs = prng_init(s.rng, (int)W);
+  struct Src {
+    int id, i, j;
+  };
+  std::vector<Src> src;
+  for (long c = 0; c < W; c++) {
+    for (int lvl = 1; lvl <= t.max_lvl; lvl++) {
+      const double dr = t.dr_base * std::pow(0.5, lvl - 1);
+      const Level &L = t.L(lvl);
+      long lo, len;
+      static_chunk((long)L.leaves.size(), W, c, lo, len);
+      for (long k = lo; k < lo + len; k++) {
+        const int id = L.leaves[k];
+        const Box &b = t.boxes[id];
+        for (int j = 1; j <= nc; j++)
+          for (int i = 1; i <= nc; i++) {
+            double tmp;
+            if (b.coord == CYL) {
+              double rc = b.r_min[0] + (i - 0.5) * b.dr;
+              tmp = fac * 2 * pi * rc * b.c(i, j, I_PHO) * (dr * dr);
+            } else {
+              tmp = fac * b.c(i, j, I_PHO) * (dr * dr);
+            }
+            int n_create = (int)std::floor(tmp);
+            if (rngs[c].uni_01() < tmp - n_create) n_create = n_create + 1;
+            for (int q = 0; q < n_create; q++) src.push_back(Src{id, i, j});
+          }
+      }
+    }
+  }
+  const long n_used = (long)src.size();
+  // absorption, PH_do_absorp (:161-205) in 3D, then the radius, :318-329
+  std::vector<Rng> arngs = prng_init(s.rng, (int)W);
+  std::vector<double> dst(2 * (size_t)n_used);
+  for (long w = 0; w < W; w++) {
+    long lo, len;
+    static_chunk(n_used, W, w, lo, len);
+    for (long n = lo; n < lo + len; n++) {
+      const Box &b = t.boxes[src[n].id];
+      double xin[3] = {b.r_min[0] + (src[n].i - 0.5) * b.dr, b.r_min[1] + (src[n].j - 0.5) * b.dr, 0};
+      double rr = arngs[w].uni_01();
+      double dist = lt_get_col(s.ph.tbl, 0, rr);
+      double sph[3];
+      arngs[w].sphere(dist, sph);
+      double xo[3] = {xin[0] + sph[0], xin[1] + sph[1], xin[2] + sph[2]};
+      dst[2 * n] = std::sqrt(xo[0] * xo[0] + xo[2] * xo[2]);
+      dst[2 * n + 1] = xo[1];
+    }
+  }
+  // absorption locations at level pho_lvl, :331-344
+  std::vector<int> loc_id(n_used), loc_ix(2 * (size_t)n_used);
+  for (long n = 0; n < n_used; n++) get_loc(t, &dst[2 * n], s.pho_lvl, loc_id[n], &loc_ix[2 * n]);
+  // clear i_pho, :360-370
+  for (int lvl = 1; lvl <= t.max_lvl; lvl++)
+    for (int id : t.L(lvl).ids) {
+      Box &b = t.boxes[id];
+      for (int j = 0; j <= nc + 1; j++)
+        for (int i = 0; i <= nc + 1; i++) b.c(i, j, I_PHO) = 0;
+    }
+  // sequential deposit, :372-386
+  const double tmp = fac * 2 * pi;
+  for (long n = 0; n < n_used; n++) {
+    int id = loc_id[n];
+    if (id > NO_BOX) {
+      int i = loc_ix[2 * n], j = loc_ix[2 * n + 1];
+      Box &b = t.boxes[id];
+      double dr = b.dr;
+      double r0 = b.r_min[0] + (i - 0.5) * b.dr;
+      b.c(i, j, I_PHO) = b.c(i, j, I_PHO) + s.ph.frac_in_tbl / (tmp * (dr * dr) * r0);
+    }
+  }
+  // ghost cells and prolongation from the absorption level, :402-427
+  for (int lvl = s.pho_lvl; lvl <= t.max_lvl - 1; lvl++) {
+    for (int id : t.L(lvl).parents) gc_box(t, id, I_PHO, gc_interp, gc_neumann);
+    for (int id : t.L(lvl).parents)
+      for (int q = 0; q < NCH; q++) {
+        int c_id = t.boxes[id].children[q];
+        if (c_id == NO_BOX) continue;
+        prolong1_add(t, c_id, I_PHO);
+      }
+  }
+}
+
+// src/streamer_2d.f90:99-127 (cyl :95-130), one iteration of the n loop at
+// fixed dt, with set_photoionization first when it is enabled
 static void step(Sim &s, double dt) {
   Tree &t = s.tree;
+  if (s.p.photoi_enabled) set_photoionization(s, dt, true);
   s.time += dt;
   tree_copy_cc(t, I_ELEC, I_ELEC_OLD);
   tree_copy_cc(t, I_PION, I_PION_OLD);
@@ -1520,7 +1889,7 @@ static void regrid(Sim &s, RefInfo &ri) {
                     ri);
 }
 
-static void setup(Sim &s) {
+static bool setup(Sim &s) {
   const a5ref_params &p = s.p;
   double r0[2] = {0, 0};
   tree_init(s.tree, p.box_size, N_VAR_CELL, N_VAR_FACE, p.dr_base, r0, p.lvls_max, 2,
@@ -1553,6 +1922,16 @@ static void setup(Sim &s) {
   s.mg.sides_bc = [sp](Tree &t, int id, int nb, int iv) { sides_bc_pot(*sp, t, id, nb, iv); };
   s.time = 0;
   s.applied_voltage = -p.domain_len_z * p.applied_fld;
+  for (int i = 0; i < 4; i++) s.rng.st[i] = p.rng_seed[i];
+  if (p.photoi_enabled) {
+    // src/m_streamer.f90:327-330 builds the table; src/m_photons.f90:331-336
+    // picks the absorption level from the length at fraction fac_dx
+    AbsFn a = p.photoi_tbl_kind == 0 ? absfn_air(p.photoi_p_O2)
+                                     : absfn_logu(p.photoi_len_lo, p.photoi_len_hi);
+    if (!ph_get_tbl(a, p.photoi_max_dist, s.ph)) return false;
+    s.pho_lvl = get_lvl_length(s.tree.dr_base, lt_get_col(s.ph.tbl, 0, p.photoi_fac_dx));
+  }
+  return true;
 }
 
 }  // namespace a5ref
@@ -1579,8 +1958,15 @@ a5ref_sim *a5ref_create(const a5ref_params *p) {
   if (!p || p->dim != 2 || p->box_size < 4 || (p->box_size & 1)) return nullptr;
   a5ref_sim *h = new a5ref_sim();
   h->s.p = *p;
+  if (p->photoi_enabled && (p->coord != CYL || p->photoi_team < 1 || p->photoi_num_photons < 0)) {
+    delete h;
+    return nullptr;
+  }
   apply_threads(*p);
-  setup(h->s);
+  if (!setup(h->s)) {
+    delete h;
+    return nullptr;
+  }
   return h;
 }
 
@@ -1603,6 +1989,8 @@ int a5ref_init(a5ref_sim *h) {
     if (ri.n_add == 0) break;
     if (it > 100) break;
   }
+  // src/streamer_cyl.f90:68-69
+  if (s.p.photoi_enabled) set_photoionization(s, 0.0, false);
   return it;
 }
 
@@ -1840,6 +2228,60 @@ void a5ref_export_table(a5ref_sim *h, double *rows_cols, double *x_min, double *
 double a5ref_applied_voltage(a5ref_sim *h) { return h->s.applied_voltage; }
 
 double a5ref_koren_mlim(double a, double b) { return koren_mlim(a, b); }
+
+void a5ref_op_photoionization(a5ref_sim *h, double dt, int has_dt) {
+  if (!h->s.p.photoi_enabled) return;
+  set_photoionization(h->s, dt, has_dt != 0);
+}
+void a5ref_rng_get(a5ref_sim *h, int *st) {
+  for (int i = 0; i < 4; i++) st[i] = h->s.rng.st[i];
+}
+void a5ref_rng_set(a5ref_sim *h, const int *st) {
+  for (int i = 0; i < 4; i++) h->s.rng.st[i] = st[i];
+}
+int a5ref_photon_table(a5ref_sim *h, double *dist, int cap, double *frac, int *pho_lvl) {
+  const PhTbl &ph = h->s.ph;
+  if (dist)
+    for (int i = 0; i < ph.tbl.n_rows && i < cap; i++) dist[i] = ph.tbl.rc(i + 1, 0);
+  if (frac) *frac = ph.frac_in_tbl;
+  if (pho_lvl) *pho_lvl = h->s.pho_lvl;
+  return ph.tbl.n_rows;
+}
+int a5ref_kat_photon_table(int kind, double p_O2, double len_lo, double len_hi, double max_dist,
+                           double *dist, double *frac) {
+  PhTbl ph;
+  AbsFn a = kind == 0 ? absfn_air(p_O2) : absfn_logu(len_lo, len_hi);
+  if (!ph_get_tbl(a, max_dist, ph)) return -1;
+  for (int i = 0; i < ph.tbl.n_rows; i++) dist[i] = ph.tbl.rc(i + 1, 0);
+  *frac = ph.frac_in_tbl;
+  return ph.tbl.n_rows;
+}
+double a5ref_kat_photon_dist(double p_O2, double max_dist, int n_photons, int n_team) {
+  // src/test_m_photons.f90: PH_get_tbl_air(phtbl, 0.2, 10e-3), photons from
+  // the origin, PH_do_absorp in 3D, mean of |xyz_out - xyz_in|
+  PhTbl ph;
+  if (!ph_get_tbl(absfn_air(p_O2), max_dist, ph)) return -1;
+  Rng master;
+  std::vector<Rng> r = prng_init(master, n_team);
+  double sum = 0;
+  for (long w = 0; w < n_team; w++) {
+    long lo, len;
+    static_chunk(n_photons, n_team, w, lo, len);
+    for (long n = lo; n < lo + len; n++) {
+      double rr = r[w].uni_01();
+      double dist = lt_get_col(ph.tbl, 0, rr);
+      double x[3];
+      r[w].sphere(dist, x);
+      sum += norm2(x, 3);
+    }
+  }
+  return sum / n_photons;
+}
+void a5ref_kat_rng(const int *st, int n, int *out) {
+  Rng r;
+  for (int i = 0; i < 4; i++) r.st[i] = st[i];
+  for (int k = 0; k < n; k++) out[k] = r.int4();
+}
 
 // ---------------------------------------------------------------------------
 // Known-answer cases.

@@ -58,7 +58,31 @@ typedef struct a5ref_params {
   double td_x[4][A5REF_MAX_TD_ROWS];    /* input x (|E|) per column */
   double td_y[4][A5REF_MAX_TD_ROWS];    /* input y per column */
   int n_threads;         /* OpenMP threads; <= 0 keeps the runtime default */
+  /* Photoionization, src/m_photons.f90 and src/streamer_cyl.f90:572-617
+   * (cylindrical form: constant absorption level, PH_set_src_2d with
+   * const_dx and use_cyl). */
+  int photoi_enabled;
+  int photoi_num_photons;  /* ST_photoi_num_photons */
+  int photoi_team;         /* size of the OpenMP team whose execution of the
+                              photon loops is reproduced (see below) */
+  int photoi_tbl_kind;     /* 0: PH_get_tbl_air; 1: log-uniform absorption length */
+  double photoi_coeff;     /* photons per ionization: eta * quench factor */
+  double photoi_p_O2;      /* kind 0: O2 partial pressure (bar) */
+  double photoi_len_lo;    /* kind 1: shortest absorption length (m) */
+  double photoi_len_hi;    /* kind 1: longest absorption length (m) */
+  double photoi_max_dist;  /* table range; the reference uses 2 * domain length */
+  double photoi_fac_dx;    /* 0.25e-3 in the cylindrical driver */
+  int rng_seed[4];         /* state of the master generator ST_rng */
 } a5ref_params;
+
+/* The photon loops of PH_set_src_2d run in OpenMP regions whose outcome
+ * depends on the team: each thread draws from its own generator seeded from
+ * the master, loops are split by the static schedule, and photons are
+ * numbered in the order threads pass a critical section. The oracle
+ * reproduces the execution in which a team of photoi_team threads passes
+ * that section thread by thread (thread 0 first), and combines the
+ * reduction of a$D_tree_sum_cc in thread order. Both are executions the
+ * reference can take with OMP_NUM_THREADS = photoi_team. */
 
 typedef struct a5ref_sim a5ref_sim;
 
@@ -142,6 +166,27 @@ int a5ref_kat_mg_cyl(int n_fmg, double *res_out, double *err_out,
 /* Lookup-table convergence test restating fosito/test/test_m_lookup_table.f90:
  * max error of LT_get_col on sin(x) for a table of n_rows over [0, x_max]. */
 double a5ref_kat_lookup(int n_rows, int n_pairs, double x_max, int n_samples);
+/* set_photoionization (src/streamer_cyl.f90:572-593): photon production
+ * rate per leaf cell, then PH_set_src_2d. has_dt = 0 is the call without dt
+ * before the time loop (:68-69). Needs photoi_enabled and coord = 1. */
+void a5ref_op_photoionization(a5ref_sim *s, double dt, int has_dt);
+/* State of the master generator (4 int32). */
+void a5ref_rng_get(a5ref_sim *s, int *state4);
+void a5ref_rng_set(a5ref_sim *s, const int *state4);
+/* The photon absorption table: n_rows distances at the cumulative
+ * fractions x = (i-1)/(n_rows-1); frac_in_tbl; the absorption level. */
+int a5ref_photon_table(a5ref_sim *s, double *dist, int cap, double *frac_in_tbl,
+                       int *pho_lvl);
+/* Stand-alone photon table (kind 0: air with p_O2; kind 1: log-uniform
+ * lengths [len_lo, len_hi]) over [0, max_dist]: returns n_rows (500). */
+int a5ref_kat_photon_table(int kind, double p_O2, double len_lo, double len_hi,
+                           double max_dist, double *dist, double *frac_in_tbl);
+/* Known-answer case restating src/test_m_photons.f90: n photons absorbed
+ * from the origin in 3D with a team of n_team generators seeded from a
+ * default master; returns the mean absorption distance. */
+double a5ref_kat_photon_dist(double p_O2, double max_dist, int n_photons, int n_team);
+/* The first n outputs of RNG_t%int4 from the given state (mzran). */
+void a5ref_kat_rng(const int *state4, int n, int *out);
 /* Koren limiter (src/m_streamer.f90:339-362). */
 double a5ref_koren_mlim(double a, double b);
 

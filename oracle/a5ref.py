@@ -45,6 +45,12 @@ class Params(ctypes.Structure):
         ("td_x", (ctypes.c_double * MAX_TD) * 4),
         ("td_y", (ctypes.c_double * MAX_TD) * 4),
         ("n_threads", ctypes.c_int),
+        ("photoi_enabled", ctypes.c_int), ("photoi_num_photons", ctypes.c_int),
+        ("photoi_team", ctypes.c_int), ("photoi_tbl_kind", ctypes.c_int),
+        ("photoi_coeff", ctypes.c_double), ("photoi_p_O2", ctypes.c_double),
+        ("photoi_len_lo", ctypes.c_double), ("photoi_len_hi", ctypes.c_double),
+        ("photoi_max_dist", ctypes.c_double), ("photoi_fac_dx", ctypes.c_double),
+        ("rng_seed", ctypes.c_int * 4),
     ]
 
 
@@ -88,6 +94,12 @@ def lib() -> ctypes.CDLL:
             "a5ref_applied_voltage": (D, [P]),
             "a5ref_kat_mg2_2d": (I, [I, pd, pd, pi]), "a5ref_kat_mg_cyl": (I, [I, pd, pd, pi]),
             "a5ref_kat_lookup": (D, [I, I, D, I]), "a5ref_koren_mlim": (D, [D, D]),
+            "a5ref_op_photoionization": (V, [P, D, I]),
+            "a5ref_rng_get": (V, [P, pi]), "a5ref_rng_set": (V, [P, pi]),
+            "a5ref_photon_table": (I, [P, pd, I, pd, pi]),
+            "a5ref_kat_photon_table": (I, [I, D, D, D, D, pd, pd]),
+            "a5ref_kat_photon_dist": (D, [D, D, I, I]),
+            "a5ref_kat_rng": (V, [pi, I, pi]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -142,6 +154,20 @@ def make_params(cfg, n_threads: int = 0) -> Params:
             p.td_x[c][k] = xs[k]
             p.td_y[c][k] = ys[k]
     p.n_threads = n_threads
+    p.photoi_enabled = 1 if cfg.photoi_enabled else 0
+    p.photoi_num_photons = cfg.photoi_num_photons
+    p.photoi_team = cfg.photoi_team
+    kind, a, b = cfg.photoi_table
+    p.photoi_tbl_kind = 0 if kind == "air" else 1
+    if kind == "air":
+        p.photoi_p_O2 = a
+    else:
+        p.photoi_len_lo, p.photoi_len_hi = a, b
+    p.photoi_coeff = cfg.photoi_coeff
+    p.photoi_max_dist = cfg.photoi_max_dist
+    p.photoi_fac_dx = cfg.photoi_fac_dx
+    for i in range(4):
+        p.rng_seed[i] = cfg.rng_seed[i]
     return p
 
 
@@ -290,6 +316,26 @@ class Sim:
     def applied_voltage(self) -> float:
         return lib().a5ref_applied_voltage(self.h)
 
+    def photoionization(self, dt: float | None):
+        lib().a5ref_op_photoionization(self.h, 0.0 if dt is None else dt, 0 if dt is None else 1)
+
+    def rng_state(self) -> np.ndarray:
+        st = np.zeros(4, dtype=np.int32)
+        lib().a5ref_rng_get(self.h, _ip(st))
+        return st
+
+    def set_rng_state(self, st) -> None:
+        st = np.ascontiguousarray(st, dtype=np.int32)
+        lib().a5ref_rng_set(self.h, _ip(st))
+
+    def photon_table(self):
+        """(distances at the table's cumulative fractions, frac_in_tbl, absorption level)"""
+        frac, lvl = ctypes.c_double(0), ctypes.c_int(0)
+        n = lib().a5ref_photon_table(self.h, None, 0, ctypes.byref(frac), ctypes.byref(lvl))
+        d = np.zeros(max(n, 1))
+        lib().a5ref_photon_table(self.h, _dp(d), n, None, None)
+        return d[:n], frac.value, lvl.value
+
 
 def kat_mg(cyl: bool, n_fmg: int):
     res, err = np.zeros(n_fmg), np.zeros(n_fmg)
@@ -306,3 +352,25 @@ def kat_lookup(n_rows: int, n_pairs: int = 100000, x_max: float = 10.0,
 
 def koren_mlim(a: float, b: float) -> float:
     return lib().a5ref_koren_mlim(a, b)
+
+
+def kat_photon_table(kind: str, a: float, b: float, max_dist: float):
+    d = np.zeros(500)
+    frac = ctypes.c_double(0)
+    n = lib().a5ref_kat_photon_table(0 if kind == "air" else 1, a if kind == "air" else 0.0,
+                                     a if kind != "air" else 0.0, b if kind != "air" else 0.0,
+                                     max_dist, _dp(d), ctypes.byref(frac))
+    if n < 0:
+        raise ValueError("photon table integration failed")
+    return d[:n], frac.value
+
+
+def kat_photon_dist(p_O2: float, max_dist: float, n_photons: int, n_team: int) -> float:
+    return lib().a5ref_kat_photon_dist(p_O2, max_dist, n_photons, n_team)
+
+
+def kat_rng(state4, n: int) -> np.ndarray:
+    st = np.ascontiguousarray(state4, dtype=np.int32)
+    out = np.zeros(n, dtype=np.int32)
+    lib().a5ref_kat_rng(_ip(st), n, _ip(out))
+    return out
