@@ -75,6 +75,7 @@ SIGNATURES = {
     "a5g_get_rng": (_I, [_P, _PI]),
     "a5g_set_rng": (_I, [_P, _PI]),
     "a5g_photoionization": (_I, [_P, _D, _I]),
+    "a5g_photon_stats": (_I, [_P, ctypes.POINTER(ctypes.c_longlong), _PD]),
     "a5g_step_batch": (_I, [ctypes.POINTER(_P), _I, _PD]),
     "a5g_step_batch_static": (_I, [ctypes.POINTER(_P), _I, _PD]),
     "a5g_sync": (_I, [_P]),

@@ -116,9 +116,9 @@ struct RunDev {
   int *ph_rng;                 // master generator state (4 int32)
   int *ph_ncr;                 // photons created per cell (capacity * SLOT)
   int *ph_cnt;                 // photons absorbed per cell (capacity * SLOT)
-  int *ph_src;                 // source cell (id * SLOT + cell) per photon
-  int *ph_ipart;               // per-thread photon counts, then bases
-  double *ph_part;             // per-thread partial sums of the production
+  int *ph_ipart;               // photon counts, then first numbers (boxes | team)
+  double *ph_part;             // sums of the production (boxes | team)
+  double *ph_u;                // uniform number drawn per leaf cell
   struct PhScal *ph_scal;
   const struct MzJump *ph_jump;
   const struct PhBox *ph_boxes;
@@ -130,6 +130,8 @@ struct PhScal {
   long long n_used;
   double fac;
   int st0[4];
+  int n_boxes;   // leaf boxes on levels >= 1, ranked in photon-number order
+  int pad;
 };
 // Jump of 2^b draws of the master generator (see mz_advance).
 struct MzJump {
@@ -1389,25 +1391,78 @@ __device__ void mz_advance(int st[4], unsigned long long k, const MzJump *J) {
 }
 
 // libgomp's static schedule without a chunk size: thread c of W gets the
-// iterations [lo, lo + len) of n.
+// iterations [lo, lo + len) of n (n and W below 2^31).
 __device__ __forceinline__ void static_chunk(long long n, long long W, long long c, long long &lo,
                                              long long &len) {
-  long long q = n / W, t = n % W;
-  if (c < t) {
+  const unsigned un = (unsigned)n, uw = (unsigned)W;
+  unsigned q = un / uw, t = un - q * uw;
+  if ((unsigned long long)c < t) {
     q++;
     t = 0;
   }
-  lo = q * c + t;
+  lo = (long long)q * c + t;
   len = q;
 }
 
 constexpr double PI_DP = 3.141592653589793;   // acos(-1.0_dp)
 constexpr double TWOPI_DP = 6.283185307179586; // 2 * acos(-1.0_dp)
 
-// ph_source: everything up to the photon numbers.
+// Position of leaf k of level lvl in the leaf lists of all levels.
+__device__ __forceinline__ int leaf_pos(const RunDev &R, int lvl, long long k) {
+  return R.lv_off[1][lvl - R.min_lvl] - R.lv_off[1][0] + (int)k;
+}
+
+// Exclusive prefix sum of two values per lane over a warp, lane order, the
+// lane's first value before its second: returns the sums before each and the
+// warp total.
+__device__ __forceinline__ void warp_scan2(int a, int b, int &ea, int &eb, int &total) {
+  const int lane = threadIdx.x & 31;
+  int x = a;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  const int tot_a = __shfl_sync(0xffffffffu, x, 31);
+  ea = x - a;
+  int z = b;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, z, o);
+    if (lane >= o) z += y;
+  }
+  eb = tot_a + z - b;
+  total = tot_a + __shfl_sync(0xffffffffu, z, 31);
+}
+
+// ph_source: everything up to the photon numbers. Only the generators'
+// draws are sequential per team thread; sums and counts run in parallel
+// over boxes and cells and are combined in the team's order. Photons are
+// numbered team thread by team thread, each thread's boxes in its loop order
+// (levels up, then its chunk of the level's leaves), cells in (j, i) order.
+// Work arrays (cap = box capacity):
+//   ph_part[0, cap)      sum of leaf box k's production, reference order
+//   ph_part[cap, 2cap)   team thread c's partial sum
+//   ph_ipart[0, cap)     photons of leaf box k, then its first photon number
+//   ph_ipart[cap, 2cap)  photons of team thread c, then its first number
+//   ph_ipart[2cap, 3cap) boxes of team thread c, then its first box rank
+//   ph_ipart[3cap, 4cap) first photon number of the box of rank r
+//   ph_ipart[4cap, 5cap) id of the box of rank r
+//   ph_u                 the draw of each leaf cell (int4 output)
+//   ph_ncr               first photon number of each leaf cell
+//   ph_cnt               absorbed photons per cell, zeroed here
 __device__ void ph_source(const RunDev &R, double dt, bool has_dt) {
   __shared__ double s_fac;
+  __shared__ double s_prod[NTHR / 32][64];
   const bool cyl = R.coord == 1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long long W = R.ph_team;
+  const int cap = R.capacity;
+  double *box_sum = R.ph_part, *team_sum = R.ph_part + cap;
+  int *box_cnt = R.ph_ipart, *team_cnt = R.ph_ipart + cap, *team_nbx = R.ph_ipart + 2 * cap;
+  int *rank_first = R.ph_ipart + 3 * cap, *rank_id = R.ph_ipart + 4 * cap;
+  int *draw = reinterpret_cast<int *>(R.ph_u);
+  for (size_t k = threadIdx.x; k < (size_t)cap * SLOT; k += NTHR) R.ph_cnt[k] = 0;
   // set_photoi_rate on all leaves (src/streamer_cyl.f90:595-617)
   {
     const int *ids;
@@ -1427,7 +1482,6 @@ __device__ void ph_source(const RunDev &R, double dt, bool has_dt) {
     });
   }
   __syncthreads();
-  const long long W = R.ph_team;
   int max_l = 0, max_l1 = 0;
   for (int lvl = R.min_lvl; lvl <= R.max_lvl; lvl++) {
     const int L = list_n(R, 1, lvl);
@@ -1435,102 +1489,152 @@ __device__ void ph_source(const RunDev &R, double dt, bool has_dt) {
     if (lvl >= 1) max_l1 = max(max_l1, L);
   }
   const int n_sum = (int)min((long long)max_l, W), n_cr = (int)min((long long)max_l1, W);
-  // a$D_tree_sum_cc (afivo/src/m_aX_utils.f90:623-680) per team thread
-  for (int c = threadIdx.x; c < n_sum; c += NTHR) {
-    double my = 0;
-    for (int lvl = R.min_lvl; lvl <= R.max_lvl; lvl++) {
-      const int L = list_n(R, 1, lvl);
-      long long lo, len;
-      static_chunk(L, W, c, lo, len);
-      if (len == 0) continue;
-      const double dr = R.lv_dr[lvl - R.min_lvl], fac = dr * dr;
-      const int *lv = list_p(R, 1, lvl);
-      for (long long k = lo; k < lo + len; k++) {
-        const int id = lv[k];
-        const BoxMeta &m = R.meta[id];
-        const int nc = m.nc, ncg = nc + 2;
-        const double *x = CC(R, I_PHO, id);
-        double tmp = 0;
-        if (cyl) {
-          for (int j = 1; j <= nc; j++)
-            for (int i = 1; i <= nc; i++) tmp = tmp + x[i + ncg * j] * (m.r0 + (i - 0.5) * m.dr);
-          tmp = tmp * TWOPI_DP;
-        } else {
-          for (int j = 1; j <= nc; j++)
-            for (int i = 1; i <= nc; i++) tmp = tmp + x[i + ncg * j];
-        }
-        my = my + fac * tmp;
-      }
-    }
-    R.ph_part[c] = my;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double total = 0;
-    for (int c = 0; c < n_sum; c++) total = total + R.ph_part[c];
-    double fac = R.ph_num_photons / (total + 2.220446049250313e-16);
-    if (has_dt) fac = dt < fac ? dt : fac;
-    s_fac = fac;
-  }
-  __syncthreads();
-  const double fac = s_fac;
   int st0[4];
 #pragma unroll
   for (int q = 0; q < 4; q++) st0[q] = R.ph_rng[q];
-  // photon creation (src/m_photons.f90:263-306): thread c's generator is the
-  // master's draws 4c+1..4c+4
+  // a$D_tree_sum_cc (afivo/src/m_aX_utils.f90:623-680): per leaf box the sum
+  // over its cells in the reference's order (sum_2pr_box for cyl), one warp
+  // per box; the products are formed in parallel, the additions in order.
+  // Meanwhile the threads of the first n_cr team threads draw their
+  // generators' uniforms for photon creation (src/m_photons.f90:263-306):
+  // team thread c draws once per cell of its boxes, in its loop order, from
+  // the generator seeded with the master's draws 4c+1..4c+4.
+  {
+    const int *ids;
+    int n;
+    list_range(R, 1, R.min_lvl, R.max_lvl, ids, n);
+    for (int k = warp; k < n; k += NTHR / 32) {
+      const int id = ids[k];
+      const BoxMeta &m = R.meta[id];
+      const int nc = m.nc, ncg = nc + 2, nn = nc * nc;
+      const double *x = CC(R, I_PHO, id);
+      for (int t = lane; t < nn; t += 32) {
+        const int i = t % nc + 1, j = t / nc + 1;
+        const double v = x[i + ncg * j];
+        s_prod[warp][t] = cyl ? v * (m.r0 + (i - 0.5) * m.dr) : v;
+      }
+      __syncwarp();
+      if (lane == 0) {
+        double res = 0;
+#pragma unroll 8
+        for (int t = 0; t < nn; t++) res = res + s_prod[warp][t];
+        box_sum[k] = cyl ? res * TWOPI_DP : res;
+      }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
   for (int c = threadIdx.x; c < n_cr; c += NTHR) {
     int st[4] = {st0[0], st0[1], st0[2], st0[3]};
     mz_advance(st, 4ull * (unsigned long long)c, R.ph_jump);
     int rs[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) rs[q] = mz_int4(st);
-    long long total = 0;
     for (int lvl = 1; lvl <= R.max_lvl; lvl++) {
-      const int L = list_n(R, 1, lvl);
       long long lo, len;
-      static_chunk(L, W, c, lo, len);
-      if (len == 0) continue;
-      const double dr = R.lv_dr[lvl - R.min_lvl], dr2 = dr * dr;
+      static_chunk(list_n(R, 1, lvl), W, c, lo, len);
       const int *lv = list_p(R, 1, lvl);
       for (long long k = lo; k < lo + len; k++) {
-        const int id = lv[k];
-        const BoxMeta &m = R.meta[id];
-        const int nc = m.nc, ncg = nc + 2;
-        const double *x = CC(R, I_PHO, id);
-        int *ncr = R.ph_ncr + (size_t)id * SLOT;
-        for (int j = 1; j <= nc; j++)
-          for (int i = 1; i <= nc; i++) {
-            const int cell = i + ncg * j;
-            double tmp;
-            if (cyl) tmp = fac * 2 * PI_DP * (m.r0 + (i - 0.5) * m.dr) * x[cell] * dr2;
-            else tmp = fac * x[cell] * dr2;
-            const double fl = floor(tmp);
-            int n_create = 0;
-            if (fl >= 0 && fl < 1.0e9) n_create = (int)fl;
-            else atomicExch(R.status, A5G_ENONFINITE);
-            if (mz_uni01(rs) < tmp - n_create) n_create = n_create + 1;
-            ncr[cell] = n_create;
-            total += n_create;
-          }
+        int *u = draw + (size_t)lv[k] * SLOT;
+        // leaf boxes on levels >= 1 have NC x NC cells; cell t is (i, j) =
+        // (t % NC + 1, t / NC + 1), the reference's loop order
+#pragma unroll 8
+        for (int t = 0; t < NC * NC; t++) u[t] = mz_int4(rs);
       }
     }
-    R.ph_ipart[c] = (int)min(total, (long long)INT_MAX);
+  }
+  // team thread c: fac_l * box sum over its static chunk of each level
+  for (int c = threadIdx.x; c < n_sum; c += NTHR) {
+    double my = 0;
+    for (int lvl = R.min_lvl; lvl <= R.max_lvl; lvl++) {
+      long long lo, len;
+      static_chunk(list_n(R, 1, lvl), W, c, lo, len);
+      const double dr = R.lv_dr[lvl - R.min_lvl], fac = dr * dr;
+      for (long long k = lo; k < lo + len; k++) my = my + fac * box_sum[leaf_pos(R, lvl, k)];
+    }
+    team_sum[c] = my;
   }
   __syncthreads();
-  // photon numbers: threads in order
+  if (threadIdx.x == 0) {
+    double total = 0;
+#pragma unroll 8
+    for (int c = 0; c < n_sum; c++) total = total + team_sum[c];
+    double fac = R.ph_num_photons / (total + 2.220446049250313e-16);
+    if (has_dt) fac = dt < fac ? dt : fac;
+    s_fac = fac;
+  }
+  __syncthreads();
+  const double fac = s_fac;
+  // photons per cell and their numbers within each box, one warp per box
+  {
+    const int *ids;
+    int n;
+    list_range(R, 1, 1, R.max_lvl, ids, n);
+    const int pos0 = n > 0 ? leaf_pos(R, 1, 0) : 0;
+    for (int k = warp; k < n; k += NTHR / 32) {
+      const int id = ids[k];
+      const BoxMeta &m = R.meta[id];
+      const double dr2 = m.dr * m.dr;
+      const double *x = CC(R, I_PHO, id);
+      const int *u = draw + (size_t)id * SLOT;
+      int cnt[2], cell[2];
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int t = lane + 32 * h;
+        const int i = t % NC + 1, j = t / NC + 1;
+        cell[h] = i + (NC + 2) * j;
+        double tmp;
+        if (cyl) tmp = fac * 2 * PI_DP * (m.r0 + (i - 0.5) * m.dr) * x[cell[h]] * dr2;
+        else tmp = fac * x[cell[h]] * dr2;
+        const double fl = floor(tmp);
+        int n_create = 0;
+        if (fl >= 0 && fl < 1.0e9) n_create = (int)fl;
+        else atomicExch(R.status, A5G_ENONFINITE);
+        // uni_01 (fosito/m_random.f90:75-80)
+        if (0.5 + 0x1p-32 * (double)u[t] < tmp - n_create) n_create = n_create + 1;
+        cnt[h] = n_create;
+      }
+      int e0, e1, tot;
+      warp_scan2(cnt[0], cnt[1], e0, e1, tot);
+      int *first = R.ph_ncr + (size_t)id * SLOT;
+      first[cell[0]] = e0;
+      first[cell[1]] = e1;
+      if (lane == 0) box_cnt[pos0 + k] = tot;
+    }
+  }
+  __syncthreads();
+  // photons and boxes per team thread
+  for (int c = threadIdx.x; c < n_cr; c += NTHR) {
+    long long tot = 0;
+    int nb = 0;
+    for (int lvl = 1; lvl <= R.max_lvl; lvl++) {
+      long long lo, len;
+      static_chunk(list_n(R, 1, lvl), W, c, lo, len);
+      for (long long k = lo; k < lo + len; k++) tot += box_cnt[leaf_pos(R, lvl, k)];
+      nb += (int)len;
+    }
+    team_cnt[c] = (int)min(tot, (long long)INT_MAX);
+    team_nbx[c] = nb;
+  }
+  __syncthreads();
+  // photon numbers and box ranks: threads in order
   if (threadIdx.x == 0) {
     long long acc = 0;
+    int nbx = 0;
+#pragma unroll 8
     for (int c = 0; c < n_cr; c++) {
-      const int v = R.ph_ipart[c];
-      R.ph_ipart[c] = (int)min(acc, (long long)INT_MAX);
+      const int v = team_cnt[c], b = team_nbx[c];
+      team_cnt[c] = (int)min(acc, (long long)INT_MAX);
+      team_nbx[c] = nbx;
       acc += v;
+      nbx += b;
     }
     if (acc > R.ph_cap) {
       atomicExch(R.status, A5G_ENOMEM);
       acc = 0;
     }
     R.ph_scal->n_used = acc;
+    R.ph_scal->n_boxes = nbx;
     R.ph_scal->fac = fac;
     for (int q = 0; q < 4; q++) R.ph_scal->st0[q] = st0[q];
     // the master has given 4W draws to the creation team and gives 4W to
@@ -1540,47 +1644,38 @@ __device__ void ph_source(const RunDev &R, double dt, bool has_dt) {
     for (int q = 0; q < 4; q++) R.ph_rng[q] = st[q];
   }
   __syncthreads();
-  const bool ok = R.ph_scal->n_used > 0;
-  // per-cell first photon number, in each thread's loop order
-  if (ok) {
-    for (int c = threadIdx.x; c < n_cr; c += NTHR) {
-      long long off = R.ph_ipart[c];
-      for (int lvl = 1; lvl <= R.max_lvl; lvl++) {
-        const int L = list_n(R, 1, lvl);
-        long long lo, len;
-        static_chunk(L, W, c, lo, len);
-        const int *lv = list_p(R, 1, lvl);
-        for (long long k = lo; k < lo + len; k++) {
-          const int id = lv[k];
-          const int nc = R.meta[id].nc, ncg = nc + 2;
-          for (int j = 1; j <= nc; j++)
-            for (int i = 1; i <= nc; i++) {
-              const size_t cell = (size_t)id * SLOT + i + ncg * j;
-              R.ph_cnt[cell] = (int)off;
-              off += R.ph_ncr[cell];
-            }
-        }
+  // first photon number and rank of each box, in its team thread's order
+  for (int c = threadIdx.x; c < n_cr; c += NTHR) {
+    long long off = team_cnt[c];
+    int rank = team_nbx[c];
+    for (int lvl = 1; lvl <= R.max_lvl; lvl++) {
+      long long lo, len;
+      static_chunk(list_n(R, 1, lvl), W, c, lo, len);
+      const int *lv = list_p(R, 1, lvl);
+      for (long long k = lo; k < lo + len; k++) {
+        const int p = leaf_pos(R, lvl, k);
+        const int v = box_cnt[p];
+        box_cnt[p] = (int)off;
+        rank_first[rank] = (int)off;
+        rank_id[rank] = lv[k];
+        rank++;
+        off += v;
       }
     }
   }
   __syncthreads();
-  // source cell of every photon
-  if (ok) {
+  // first photon number of each cell
+  {
     const int *ids;
     int n;
     list_range(R, 1, 1, R.max_lvl, ids, n);
-    box_loop(ids, n, [&](int id, int t) {
-      const int nc = R.meta[id].nc, ncg = nc + 2;
-      if (t >= nc * nc) return;
-      const int cell = (t % nc + 1) + ncg * (t / nc + 1);
-      const size_t k = (size_t)id * SLOT + cell;
-      const int first = R.ph_cnt[k], cnt = R.ph_ncr[k];
-      const int code = id * SLOT + cell;
-      for (int q = 0; q < cnt; q++) R.ph_src[first + q] = code;
-    });
+    const int pos0 = n > 0 ? leaf_pos(R, 1, 0) : 0;
+    const int g = threadIdx.x / GT, t = threadIdx.x % GT;
+    for (int b = g; b < n; b += NGRP) {
+      const int cell = (t % NC + 1) + (NC + 2) * (t / NC + 1);
+      R.ph_ncr[(size_t)ids[b] * SLOT + cell] += box_cnt[pos0 + b];
+    }
   }
-  __syncthreads();
-  for (size_t k = threadIdx.x; k < (size_t)R.capacity * SLOT; k += NTHR) R.ph_cnt[k] = 0;
   __syncthreads();
 }
 
@@ -1774,9 +1869,14 @@ __global__ void __launch_bounds__(NTHR, 1) a5g_run_kernel_slots(const BatchSlot 
 // the absorption level, :331-344). Thread w of the team absorbs its static
 // chunk of the photons in order with its own generator (the master's draws
 // 4W + 4w + 1..4 of the call) and counts each photon in its absorbing cell.
-// blockIdx.y selects the run of a batch. The per-box geometry is staged in
-// shared memory when it fits (ph_smem: bytes available).
+// A photon's source cell follows from its number: the last ranked box whose
+// first number is not above it, then the last cell of that box whose first
+// number is not above it. blockIdx.y selects the run of a batch. The per-box
+// geometry and the box ranks are staged in shared memory when they fit
+// (ph_smem: bytes available).
 constexpr int PH_THREADS = 256;
+__device__ __forceinline__ int ph_cell_index(int t) { return (t % NC + 1) + (NC + 2) * (t / NC + 1); }
+
 __global__ void __launch_bounds__(PH_THREADS) a5g_photon_kernel(const RunDev *single,
                                                                const RunDev *const *runs,
                                                                const BatchSlot *slots,
@@ -1789,12 +1889,22 @@ __global__ void __launch_bounds__(PH_THREADS) a5g_photon_kernel(const RunDev *si
   if (w0 >= W) return;
   const long long n_used = R.ph_scal->n_used;
   if (n_used == 0) return;
+  const int nbx = R.ph_scal->n_boxes, cap = R.capacity;
   const PhBox *tb = R.ph_boxes;
-  if ((size_t)R.n_ids * sizeof(PhBox) <= (size_t)ph_smem) {
+  const int *rank_first = R.ph_ipart + 3 * cap, *rank_id = R.ph_ipart + 4 * cap;
+  const size_t need = (size_t)R.n_ids * sizeof(PhBox) + 2 * (size_t)nbx * sizeof(int);
+  if (need <= (size_t)ph_smem) {
     PhBox *sb = reinterpret_cast<PhBox *>(g_dsmem);
+    int *sf = reinterpret_cast<int *>(sb + R.n_ids), *si = sf + nbx;
     for (int k = threadIdx.x; k < R.n_ids; k += PH_THREADS) sb[k] = R.ph_boxes[k];
+    for (int k = threadIdx.x; k < nbx; k += PH_THREADS) {
+      sf[k] = rank_first[k];
+      si[k] = rank_id[k];
+    }
     __syncthreads();
     tb = sb;
+    rank_first = sf;
+    rank_id = si;
   }
   const long long w = w0 + threadIdx.x;
   if (w >= W) return;
@@ -1809,10 +1919,30 @@ __global__ void __launch_bounds__(PH_THREADS) a5g_photon_kernel(const RunDev *si
   const int *l1 = list_p(R, 0, 1);
   const int n1 = list_n(R, 0, 1);
   const int lvl_max = R.ph_lvl;
+  int sid = 0, scell = 0;
+  long long cell_end = -1;  // photons [.., cell_end) come from (sid, scell)
   for (long long p = lo; p < lo + len; p++) {
-    const int code = R.ph_src[p];
-    const int sid = code / SLOT, cell = code - sid * SLOT;
-    const int si = cell % (NC + 2), sj = cell / (NC + 2);
+    if (p >= cell_end) {
+      // box: last rank with first <= p
+      int a = 0, b = nbx - 1;
+      while (a < b) {
+        const int mid = (a + b + 1) >> 1;
+        if (rank_first[mid] <= p) a = mid;
+        else b = mid - 1;
+      }
+      sid = rank_id[a];
+      const long long box_end = a + 1 < nbx ? rank_first[a + 1] : n_used;
+      const int *first = R.ph_ncr + (size_t)sid * SLOT;
+      int ta = 0, tbb = NC * NC - 1;
+      while (ta < tbb) {
+        const int mid = (ta + tbb + 1) >> 1;
+        if (first[ph_cell_index(mid)] <= p) ta = mid;
+        else tbb = mid - 1;
+      }
+      scell = ph_cell_index(ta);
+      cell_end = ta + 1 < NC * NC ? first[ph_cell_index(ta + 1)] : box_end;
+    }
+    const int si = scell % (NC + 2), sj = scell / (NC + 2);
     const PhBox &S = tb[sid];
     const double x0 = S.r0 + (si - 0.5) * S.dr, y0 = S.r1 + (sj - 0.5) * S.dr;
     const double dist = ph_dist(R, mz_uni01(rs));
@@ -1920,14 +2050,13 @@ struct a5g_ctx {
   bool has_ph_table = false;
   double *ph_tbl = nullptr;
   std::vector<double> h_ph_tbl;
-  int *ph_rng = nullptr, *ph_ncr = nullptr, *ph_cnt = nullptr, *ph_src = nullptr,
-      *ph_ipart = nullptr;
-  double *ph_part = nullptr;
+  int *ph_rng = nullptr, *ph_ncr = nullptr, *ph_cnt = nullptr, *ph_ipart = nullptr;
+  double *ph_part = nullptr, *ph_u = nullptr;
   PhScal *ph_scal = nullptr;
   MzJump *ph_jump = nullptr;
   PhBox *ph_boxes = nullptr;
   int ph_capacity = 0;   // capacity the per-box photon buffers are sized for
-  size_t ph_src_cap = 0, ph_boxes_cap = 0;
+  size_t ph_boxes_cap = 0;
 };
 
 // ---------------------------------------------------------------------------
@@ -2171,39 +2300,39 @@ static void mz_jump_table(MzJump *J) {
   }
 }
 
-// Photon buffers sized for the current box capacity: counts per cell, one
-// source per photon (at most num_photons + one per leaf cell are created:
-// the expected total is at most num_photons and stochastic rounding adds at
-// most one per cell), and per-thread scratch.
+// Photon buffers sized for the current box capacity: per cell a draw, a
+// first photon number and an absorption count; per box and per team thread
+// scratch. At most num_photons + one per leaf cell are created (the expected
+// total is at most num_photons and stochastic rounding adds at most one per
+// cell); photon numbers must stay below 2^31.
 static int ph_resize(a5g_ctx *c) {
   if (!c->p.photoi_enabled || c->capacity == c->ph_capacity) return A5G_OK;
   const size_t cells = (size_t)c->capacity * SLOT;
   const size_t src = (size_t)c->p.photoi_num_photons + (size_t)c->capacity * NC * NC + 1024;
-  if (src > (size_t)INT_MAX) return fail(A5G_EINVAL, "photon buffer above 2^31 entries");
+  if (src > (size_t)INT_MAX) return fail(A5G_EINVAL, "photon numbers above 2^31");
   CK(cudaStreamSynchronize(c->stream));
   cudaFree(c->ph_ncr);
   cudaFree(c->ph_cnt);
-  cudaFree(c->ph_src);
   cudaFree(c->ph_ipart);
   cudaFree(c->ph_part);
-  c->ph_ncr = c->ph_cnt = c->ph_src = c->ph_ipart = nullptr;
-  c->ph_part = nullptr;
+  cudaFree(c->ph_u);
+  c->ph_ncr = c->ph_cnt = c->ph_ipart = nullptr;
+  c->ph_part = c->ph_u = nullptr;
   if (cudaMalloc(&c->ph_ncr, cells * sizeof(int)) != cudaSuccess ||
       cudaMalloc(&c->ph_cnt, cells * sizeof(int)) != cudaSuccess ||
-      cudaMalloc(&c->ph_src, src * sizeof(int)) != cudaSuccess ||
-      cudaMalloc(&c->ph_ipart, (size_t)c->capacity * sizeof(int)) != cudaSuccess ||
-      cudaMalloc(&c->ph_part, (size_t)c->capacity * sizeof(double)) != cudaSuccess)
+      cudaMalloc(&c->ph_ipart, 5 * (size_t)c->capacity * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&c->ph_part, 2 * (size_t)c->capacity * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&c->ph_u, cells * sizeof(double)) != cudaSuccess)
     return fail(A5G_ENOMEM, "cannot allocate photon buffers");
   CK(cudaMemsetAsync(c->ph_ncr, 0, cells * sizeof(int), c->stream));
   CK(cudaMemsetAsync(c->ph_cnt, 0, cells * sizeof(int), c->stream));
   c->ph_capacity = c->capacity;
-  c->ph_src_cap = src;
   RunDev &h = c->h;
   h.ph_ncr = c->ph_ncr;
   h.ph_cnt = c->ph_cnt;
-  h.ph_src = c->ph_src;
   h.ph_ipart = c->ph_ipart;
   h.ph_part = c->ph_part;
+  h.ph_u = c->ph_u;
   h.ph_cap = (int)src;
   return A5G_OK;
 }
@@ -2216,7 +2345,8 @@ static int ph_ready(a5g_ctx *c) {
 // Dynamic shared memory of a5g_photon_kernel for a run: its box geometry
 // table when that fits, else 0.
 static size_t ph_smem_bytes(const a5g_ctx *c) {
-  const size_t need = (size_t)(c->max_id + 1) * sizeof(PhBox);
+  // box geometry and, per leaf box, its rank's first photon number and id
+  const size_t need = (size_t)(c->max_id + 1) * (sizeof(PhBox) + 2 * sizeof(int));
   return need <= dyn_smem_limit() ? need : 0;
 }
 
@@ -2333,9 +2463,9 @@ int a5g_destroy(a5g_ctx *c) {
   cudaFree(c->ph_rng);
   cudaFree(c->ph_ncr);
   cudaFree(c->ph_cnt);
-  cudaFree(c->ph_src);
   cudaFree(c->ph_ipart);
   cudaFree(c->ph_part);
+  cudaFree(c->ph_u);
   cudaFree(c->ph_scal);
   cudaFree(c->ph_jump);
   cudaFree(c->ph_boxes);
@@ -2403,6 +2533,17 @@ int a5g_set_photon_table(a5g_ctx *c, int n_rows, double x_min, double inv_dx, co
   h.ph_lvl = lvl;
   c->has_ph_table = true;
   return push_run(c);
+}
+
+int a5g_photon_stats(a5g_ctx *c, long long *n_created, double *fac) {
+  if (!c || !n_created || !fac) return fail(A5G_EINVAL, "null argument");
+  if (!c->p.photoi_enabled) return fail(A5G_ESTATE, "photoionization is not enabled");
+  PhScal h{};
+  CK(cudaMemcpyAsync(&h, c->ph_scal, sizeof(PhScal), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *n_created = h.n_used;
+  *fac = h.fac;
+  return check_status(c);
 }
 
 int a5g_get_rng(a5g_ctx *c, int *st) {

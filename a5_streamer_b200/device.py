@@ -209,6 +209,12 @@ class DeviceRun:
         call before the time loop."""
         call("a5g_photoionization", self.h, 0.0 if dt is None else dt, 0 if dt is None else 1)
 
+    def photon_stats(self) -> Tuple[int, float]:
+        """(photons created by the last photoionization call, its fac)"""
+        n, fac = ctypes.c_longlong(0), ctypes.c_double(0)
+        call("a5g_photon_stats", self.h, ctypes.byref(n), ctypes.byref(fac))
+        return n.value, fac.value
+
     def rng_state(self) -> np.ndarray:
         st = np.zeros(4, dtype=np.int32)
         call("a5g_get_rng", self.h, _ip(st))

@@ -22,6 +22,15 @@ average; src/streamer_2d.f90:93-128), in 8-byte words:
 with N_l the cells of all boxes on level l, P_l the cells of parent boxes on
 level l, L the finest level, N_all = sum over levels >= 1, N_leaf the leaf
 cells. For a uniform 2D tree this is about 253 words (2 kB) per leaf cell.
+
+With photoionization (src/streamer_cyl.f90:572-617, once per step) add
+
+  T10 photon sources           8 N_leaf words + 16 bytes per photon
+
+(production rate: read |E| and n_e, write the rate; the sum and the
+creation pass read the rate; the photon count per cell is written and read;
+the source term is written; per photon a 4-byte source cell written and
+read and a 4-byte counter read and written).
 """
 from __future__ import annotations
 
@@ -59,7 +68,10 @@ def census(meta: np.ndarray, levels: Dict[int, Tuple[np.ndarray, np.ndarray, np.
     return Census(dim, nc, min(levels), max(levels), cells, leaf, par)
 
 
-def bytes_per_step(c: Census, n_down: int = 2, n_up: int = 2, word: int = 8) -> float:
+def bytes_per_step(c: Census, n_down: int = 2, n_up: int = 2, word: int = 8,
+                   photons: float = 0.0) -> float:
+    """Algorithmic bytes of one full step; photons > 0 adds the photon
+    sources of a step with photoionization and that many photons."""
     D, nc = c.dim, c.nc
     g = 4.0 * D / nc
     N_all, N_leaf = c.n_all, c.n_leaf
@@ -78,4 +90,7 @@ def bytes_per_step(c: Census, n_down: int = 2, n_up: int = 2, word: int = 8) -> 
     t7 = 2 * fmg
     t8 = 2 * (D + 2 + g) * N_all
     t9 = 3 * N_leaf
-    return word * (t1 + t2 + t3 + t4 + t5 + t6 + t7 + t8 + t9)
+    total = word * (t1 + t2 + t3 + t4 + t5 + t6 + t7 + t8 + t9)
+    if photons > 0:
+        total += word * 8 * N_leaf + 16.0 * photons
+    return total

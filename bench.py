@@ -4,10 +4,13 @@
 One "step" is one full time step of the streamer model on the current mesh
 (save old densities, two forward-Euler stages with a field solve after the
 first, trapezoidal average, second field solve), i.e. one iteration of the
-inner loop of src/streamer_2d.f90:93-128. The workload is the 8 mm Cartesian
-FP64 case evolved from its initial conditions to its end time t = 2 ns with
-the full regrid cycle; the mesh is then frozen and K steps are timed at the
-step size get_max_dt gives.
+inner loop of src/streamer_cyl.f90:95-130 (src/streamer_2d.f90:93-128),
+including the Monte Carlo photoionization of the step where the workload has
+it. The default workload is the axisymmetric 16 mm FP64 case with
+photoionization (1e5 photons per step) evolved from its initial conditions
+to its end time t = 10 ns with the full regrid cycle; the mesh is then
+frozen and K steps are timed at the step size get_max_dt gives. The 8 mm
+Cartesian case (t = 2 ns, no photoionization) is --workload cartesian_8mm.
 
 Arms:
   --impl b200       (default) the sm_100a device path through its C ABI
@@ -41,7 +44,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--workload", choices=["cartesian_8mm", "cylindrical_16mm"], default="cartesian_8mm")
+    ap.add_argument("--workload", choices=["cylindrical_16mm_photoi", "cylindrical_16mm", "cartesian_8mm"],
+                    default="cylindrical_16mm_photoi")
     ap.add_argument("--batch", type=int, default=148, help="replicas in the batched extra (0: skip)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="budget of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -52,7 +56,9 @@ def workload_cfg(name):
     from a5_streamer_b200 import config
     if name == "cartesian_8mm":
         return config.cartesian_8mm(), "cartesian_8mm_fp64_t2ns"
-    return config.cylindrical_16mm(), "cylindrical_16mm_fp64_t10ns_no_photoionization"
+    if name == "cylindrical_16mm":
+        return config.cylindrical_16mm(), "cylindrical_16mm_fp64_t10ns_no_photoionization"
+    return config.cylindrical_16mm(photoi=True), "cylindrical_16mm_photoi_fp64_t10ns"
 
 
 # ---------------------------------------------------------------------------
@@ -218,7 +224,6 @@ def run_b200(args):
     n_leaf = run.n_leaf_cells()
     meta, geom, levels = sim.tree.export()
     cen = metrics.census(meta, levels, cfg.box_size)
-    bytes_step = metrics.bytes_per_step(cen)
     dt = run.get_max_dt()
 
     ext = torch.cuda.ExternalStream(run.stream_ptr())
@@ -227,6 +232,9 @@ def run_b200(args):
         run.step(dt)
     run.sync()
     torch.cuda.synchronize()
+    photons = run.photon_stats()[0] if cfg.photoi_enabled else 0
+    bytes_step = metrics.bytes_per_step(cen, photons=photons)
+    launches_per_step = 3 if cfg.photoi_enabled else 1
     if dist:
         dist.barrier()
 
@@ -268,9 +276,15 @@ def run_b200(args):
         fc = [[run.fc(d, f) for f in range(2)] for d in range(2)]
         rc, xm, inv = sim.table()
         reps = []
+        if cfg.photoi_enabled:
+            ph_dist, ph_frac = dv.photon_table(cfg)
+            rng = run.rng_state()
         for _ in range(args.batch):
             r = dv.DeviceRun(cfg)
             r.set_table(rc, xm, inv)
+            if cfg.photoi_enabled:
+                r.set_photon_table(ph_dist, ph_frac)
+                r.set_rng_state(rng)
             r.upload_tree(meta, geom, sim.tree.min_lvl, sim.tree.max_lvl, levels)
             for iv in range(9):
                 r.set_cc(iv, cc[iv])
@@ -306,7 +320,9 @@ def run_b200(args):
     traffic = traffic_per_launch(args.workload)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic,
-                "peak_kind": peak_kind, "algorithmic_bytes_per_launch": bytes_step}
+                "peak_kind": peak_kind, "algorithmic_bytes_per_launch": bytes_step,
+                "timed_unit": "one full step" + (" (photon sources, absorption, step kernel)"
+                                                 if cfg.photoi_enabled else " (step kernel)")}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -324,8 +340,10 @@ def run_b200(args):
             "config": {"workload": wname, "leaf_cells": n_leaf, "boxes_in_use": int(meta[:, 0].sum()),
                        "min_lvl": sim.tree.min_lvl, "max_lvl": sim.tree.max_lvl,
                        "precision": "fp64", "parallelism": f"replicas{world}",
+                       "photons_per_step": photons,
                        "l2": "flushed before every timed step (256 MiB write)"},
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": K,
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": K * launches_per_step,
             "clocks": clk.summary(), "batched": batched,
         }
         print(json.dumps(out), flush=True)

@@ -180,6 +180,9 @@ int a5g_prolong_new(a5g_ctx *ctx, const int *n_new, const int *new_ids);
  * order, an execution the reference takes with OMP_NUM_THREADS equal to
  * photoi_team. The master generator advances by 8 * photoi_team draws. */
 int a5g_photoionization(a5g_ctx *ctx, double dt, int has_dt);
+/* Photons created by the last photoionization call and its factor fac
+ * (photons per unit production, src/m_photons.f90:250-256). Synchronises. */
+int a5g_photon_stats(a5g_ctx *ctx, long long *n_created, double *fac);
 /* One full time step on the current mesh (src/streamer_2d.f90:93-128, one
  * iteration of the n loop): set_photoionization when enabled, save old
  * densities, two forward-Euler stages with a field solve after the first,
