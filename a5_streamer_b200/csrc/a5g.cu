@@ -570,6 +570,7 @@ struct MGV {
   double *phi, *rhs, *tmp;
   const BoxRec *boxes;
   const int *pbx;
+  bool plans;  // the cell plans of "Cell plans" are available (shared-memory solve)
 };
 
 // Side ghost (side, k) of the potential: sides_from_nb, mg$D_sides_rb after
@@ -719,7 +720,7 @@ __device__ __forceinline__ LvlInfo lvl_info(const RunDev &R, int lvl) {
 // it is written), or coarser-level cells. mem: read ghosts from memory
 // instead (first half-sweep of a first FMG call, where the reference's
 // ghosts are not consistent with the interior).
-__device__ void p_sweep(const RunDev &R, const MGV &M, int lvl, int it, bool mem) {
+__device__ __noinline__ void p_sweep(const RunDev &R, const MGV &M, int lvl, int it, bool mem) {
   const LvlInfo L = lvl_info(R, lvl);
   double *phi = M.phi;
   const double *rhs = M.rhs;
@@ -782,7 +783,7 @@ __device__ void p_fill(const RunDev &R, const MGV &M, int lvl) {
 // leaf cells (src/streamer_2d.f90:317-329). store_res: keep the residual in
 // the box's own tmp (set_coarse_phi_rhs); otherwise tmp is left as it was
 // (update_coarse saves and restores it).
-__device__ void p_fr(const RunDev &R, const MGV &M, int lvl, bool fill, bool leaf_rhs, bool store_res) {
+__device__ __noinline__ void p_fr(const RunDev &R, const MGV &M, int lvl, bool fill, bool leaf_rhs, bool store_res) {
   const LvlInfo L = lvl_info(R, lvl);
   const int pncg = R.lv_nc[lvl - 1 - R.min_lvl] + 2;
   double *phi = M.phi, *tmp = M.tmp, *rhs = M.rhs;
@@ -885,7 +886,7 @@ __device__ void p_correct(const RunDev &R, const MGV &M, int lvl, bool copy, boo
 
 // init_phi_rhs for one level (m_aX_mg.f90:450-473): phi = 0 on the boxes of
 // level lvl and their rhs restricted to the parents.
-__device__ void p_init_level(const RunDev &R, const MGV &M, int lvl, bool leaf_rhs) {
+__device__ __noinline__ void p_init_level(const RunDev &R, const MGV &M, int lvl, bool leaf_rhs) {
   const LvlInfo L = lvl_info(R, lvl);
   const int pncg = R.lv_nc[lvl - 1 - R.min_lvl] + 2;
   double *rhs = M.rhs, *phi = M.phi;
@@ -917,7 +918,7 @@ __device__ void p_init_level(const RunDev &R, const MGV &M, int lvl, bool leaf_r
 
 // Residual rhs - A phi on every cell of levels min..max (set_residual of
 // mg$D_fas_vcycle, :243-253)
-__device__ void p_residual_all(const RunDev &R, const MGV &M, int max_lvl) {
+__device__ __noinline__ void p_residual_all(const RunDev &R, const MGV &M, int max_lvl) {
   double *phi = M.phi, *tmp = M.tmp;
   const double *rhs = M.rhs;
   for (int lvl = R.min_lvl; lvl <= max_lvl; lvl++) {
@@ -934,6 +935,212 @@ __device__ void p_residual_all(const RunDev &R, const MGV &M, int max_lvl) {
   __syncthreads();
 }
 
+// ---------------------------------------------------------------------------
+// Cell plans of a level visit. When the multigrid variables are in shared
+// memory and every colour of a level has at most one cell per thread, each
+// thread forms once per visit, for its red and its black cell, the cell
+// address and the first source and kind of each ghost neighbour, and keeps
+// them in its two shared-memory plan slots through the half-sweeps (and the
+// residual/restriction) of that visit. The values computed are those of
+// p_sweep / p_fr; only the address work moves out of the phases.
+
+// Kinds of a ghost neighbour: copy of s0 (same-level neighbour or Neumann
+// wall), refinement boundary (mg$D_sides_rb after a$D_gc_prolong0:
+// 0.5 s0 + own - 0.25 (a + b), s0 the parent cell), grounded wall (-own),
+// applied potential (2 V - own); sides_bc_pot (src/streamer_2d.f90:620-638).
+enum { GK_COPY = 0, GK_RB = 1, GK_NEG = 2, GK_TOP = 3 };
+
+// A cell plan as an int4: x = cell address (-1: none), y / z = first source
+// of the x / y ghost neighbour, w = i | j << 8 | x kind << 16 | y kind << 18.
+
+// First source and kind of side ghost (side, k) of box B (as phi_ghost).
+__device__ __forceinline__ void ghost_src(const BoxRec &B, int nc, int ncg, int side, int k, int &s0,
+                                          int &kind) {
+  const int dim = side >> 1;
+  const bool low = (side & 1) == 0;
+  const int nbb = B.nb[side];
+  const int ix = low ? 1 : nc;
+  if (nbb > 0) {
+    s0 = nbb + (dim == 0 ? (low ? nc : 1) + ncg * k : k + ncg * (low ? nc : 1));
+    kind = GK_COPY;
+  } else if (nbb == NBR_RB) {
+    const int ig = ix - (low ? 1 : -1);
+    const int h1 = (ig + 1) >> 1, h2 = (k + 1) >> 1;
+    s0 = B.pbase + (dim == 0 ? (B.o0 + h1) + ncg * (B.o1 + h2) : (B.o0 + h2) + ncg * (B.o1 + h1));
+    kind = GK_RB;
+  } else {
+    s0 = B.base + (dim == 0 ? ix + ncg * k : k + ncg * ix);
+    kind = side == 2 ? GK_NEG : (side == 3 ? GK_TOP : GK_COPY);
+  }
+}
+
+__device__ __forceinline__ int4 make_plan(const BoxRec &B, int nc, int ncg, int i, int j) {
+  int4 c;
+  c.x = B.base + i + ncg * j;
+  int xk, yk;
+  ghost_src(B, nc, ncg, i == 1 ? 0 : 1, j, c.y, xk);
+  ghost_src(B, nc, ncg, j == 1 ? 2 : 3, i, c.z, yk);
+  c.w = i | (j << 8) | (xk << 16) | (yk << 18);
+  return c;
+}
+
+// Value of a ghost neighbour from its first source v0 and the cell's own
+// value vo, its neighbour across the box va and along the side vb.
+__device__ __forceinline__ double ghost_eval(double v0, int kind, double vo, double va, double vb,
+                                             double V) {
+  const double vrb = 0.5 * v0 + vo - 0.25 * (va + vb);
+  const double vw = kind == GK_NEG ? -vo : 2 * V - vo;
+  return kind == GK_COPY ? v0 : (kind == GK_RB ? vrb : vw);
+}
+
+// The four neighbours of the plan's cell (as phi_nbrs; mem: read the ghost
+// cells stored in memory instead). The across and along neighbours a ghost
+// recipe reads are among the cell's direct neighbours.
+__device__ __forceinline__ void plan_nbrs(const RunDev &R, const double *phi, const int4 &c, int nc,
+                                          int ncg, bool mem, double &lx, double &hx, double &ly,
+                                          double &hy) {
+  const int g = c.x, i = c.w & 255, j = (c.w >> 8) & 255;
+  const double dlx = phi[g - 1], dhx = phi[g + 1], dly = phi[g - ncg], dhy = phi[g + ncg];
+  if (mem) {
+    lx = dlx;
+    hx = dhx;
+    ly = dly;
+    hy = dhy;
+    return;
+  }
+  const double vo = phi[g], x0 = phi[c.y], y0 = phi[c.z];
+  const double gx = ghost_eval(x0, (c.w >> 16) & 3, vo, i == 1 ? dhx : dlx, (j & 1) ? dhy : dly,
+                               R.applied_voltage);
+  const double gy = ghost_eval(y0, (c.w >> 18) & 3, vo, j == 1 ? dhy : dly, (i & 1) ? dhx : dlx,
+                               R.applied_voltage);
+  lx = i > 1 ? dlx : gx;
+  hx = i < nc ? dhx : gx;
+  ly = j > 1 ? dly : gy;
+  hy = j < nc ? dhy : gy;
+}
+
+// box_gsrb_clpl weights (i+ioff-1)/(i+ioff-1/2) and (i+ioff)/(i+ioff-1/2)
+__device__ __forceinline__ void cyl_weights(int gi, double &rf1, double &rf2) {
+  const double den = gi - 0.5;
+  rf1 = (gi - 1) / den;
+  rf2 = gi / den;
+}
+
+extern __shared__ double g_dsmem[];
+
+// The plan slots lead the dynamic shared memory of a shared-memory solve:
+// 2 NTHR int4 cell plans, then (cylindrical runs) 2 NTHR double2 weights.
+constexpr int PLAN_DOUBLES = 2 * NTHR * 2;     // doubles taken by the cell plans
+constexpr int WTS_DOUBLES = 2 * NTHR * 2;      // doubles taken by the weights
+__device__ __forceinline__ int4 *plan_slots() { return reinterpret_cast<int4 *>(g_dsmem); }
+__device__ __forceinline__ double2 *wts_slots() { return reinterpret_cast<double2 *>(g_dsmem + PLAN_DOUBLES); }
+
+struct LevelPlan {
+  int bx;    // index of the box record of the thread's cells (-1: none)
+  int item;  // cell index within each colour of the box (row-major, nc/2 per row)
+};
+
+__device__ __forceinline__ bool plan_fits(const MGV &M, const LvlInfo &L) {
+  return M.plans && L.nb * ((L.nc * L.nc) >> 1) <= NTHR;
+}
+
+// Forms the thread's two cell plans (colour p = (i + j) & 1). Each thread
+// reads only its own slots afterwards, so no barrier is needed.
+__device__ __forceinline__ LevelPlan make_level_plan(const MGV &M, const LvlInfo &L, bool cyl) {
+  LevelPlan P;
+  const int half = (L.nc * L.nc) >> 1, hsh = 2 * L.sh - 1, hn = L.nc >> 1;
+  const int k = threadIdx.x;
+  P.bx = -1;
+  P.item = k & (half - 1);
+  int4 c[2];
+  c[0].x = c[1].x = -1;
+  if (k < L.nb * half) {
+    P.bx = L.b0 + (k >> hsh);
+    const BoxRec &B = M.boxes[P.bx];
+    const int j = (P.item >> (L.sh - 1)) + 1, m = P.item & (hn - 1);
+#pragma unroll
+    for (int p = 0; p < 2; p++) c[p] = make_plan(B, L.nc, L.ncg, 2 * m + 2 - ((p + j) & 1), j);
+  }
+  plan_slots()[2 * threadIdx.x] = c[0];
+  plan_slots()[2 * threadIdx.x + 1] = c[1];
+  if (cyl && P.bx >= 0) {
+    const int gi0 = M.boxes[P.bx].gi0;
+#pragma unroll
+    for (int p = 0; p < 2; p++) {
+      double2 w;
+      cyl_weights(gi0 + (c[p].w & 255), w.x, w.y);
+      wts_slots()[2 * threadIdx.x + p] = w;
+    }
+  }
+  return P;
+}
+
+// One red-black half-sweep `it` from the cell plans (p_sweep).
+__device__ __forceinline__ void plan_sweep(const RunDev &R, const MGV &M, const LvlInfo &L,
+                                           const LevelPlan &P, int it, bool mem) {
+  const int4 c = plan_slots()[2 * threadIdx.x + (it & 1)];
+  if (c.x >= 0) {
+    double *phi = M.phi;
+    double lx, hx, ly, hy;
+    plan_nbrs(R, phi, c, L.nc, L.ncg, mem, lx, hx, ly, hy);
+    const double r = M.rhs[c.x], dx2 = L.dr * L.dr;
+    if (R.coord == 1) {
+      const double2 w = wts_slots()[2 * threadIdx.x + (it & 1)];
+      phi[c.x] = 0.25 * (w.x * lx + w.y * hx + hy + ly - dx2 * r);
+    } else {
+      phi[c.x] = 0.25 * (hx + lx + hy + ly - dx2 * r);
+    }
+  }
+  __syncthreads();
+}
+
+// Residual of both cells of the plan, restricted with phi into the parent
+// (p_fr with fill, without leaf_rhs and store_res). The 2x2 block of cells
+// (2ii-1..2ii, 2jj-1..2jj) belongs to the threads of items (2jj-2) hn + ii-1
+// (cells (2ii-1, 2jj-1) and (2ii, 2jj-1)) and that item + hn (cells
+// (2ii, 2jj) and (2ii-1, 2jj)), which are in the same warp; the first adds
+// the four in the order of box_rstr_lpl.
+__device__ __forceinline__ void plan_fr(const RunDev &R, const MGV &M, const LvlInfo &L,
+                                        const LevelPlan &P, int lvl) {
+  double *phi = M.phi, *tmp = M.tmp;
+  const double inv_dr_sq = 1 / (L.dr * L.dr);
+  double res[2] = {0, 0}, ph[2] = {0, 0};
+#pragma unroll
+  for (int p = 0; p < 2; p++) {
+    const int4 c = plan_slots()[2 * threadIdx.x + p];
+    if (c.x < 0) continue;
+    double lx, hx, ly, hy;
+    plan_nbrs(R, phi, c, L.nc, L.ncg, false, lx, hx, ly, hy);
+    const double v = phi[c.x];
+    double lap;
+    if (R.coord == 1) {
+      const double2 w = wts_slots()[2 * threadIdx.x + p];
+      lap = (w.x * lx + w.y * hx + ly + hy - 4 * v) * inv_dr_sq;
+    } else {
+      lap = inv_dr_sq * (lx + hx + ly + hy - 4 * v);
+    }
+    res[p] = M.rhs[c.x] - lap;
+    ph[p] = v;
+  }
+  const int hn = L.nc >> 1;
+  // from the item one row up: its even cell (2ii, 2jj) and odd cell (2ii-1, 2jj)
+  const double r11 = __shfl_down_sync(0xffffffffu, res[0], hn);
+  const double r01 = __shfl_down_sync(0xffffffffu, res[1], hn);
+  const double p11 = __shfl_down_sync(0xffffffffu, ph[0], hn);
+  const double p01 = __shfl_down_sync(0xffffffffu, ph[1], hn);
+  const int row = P.item >> (L.sh - 1);  // j - 1
+  if (P.bx >= 0 && (row & 1) == 0) {
+    const BoxRec &B = M.boxes[P.bx];
+    const int ii = (P.item & (hn - 1)) + 1, jj = (row >> 1) + 1;
+    const int pncg = R.lv_nc[lvl - 1 - R.min_lvl] + 2;
+    const int d = B.pbase + (B.o0 + ii) + pncg * (B.o1 + jj);
+    tmp[d] = 0.25 * (res[0] + res[1] + r01 + r11);
+    phi[d] = 0.25 * (ph[0] + ph[1] + p01 + p11);
+  }
+  fill_phi_loop(R, M, L, false);
+  __syncthreads();
+}
+
 // mg$D_fas_vcycle (m_aX_mg.f90:208-254), set_residual handled by the caller.
 // Phases per level: down: 4 half-sweeps, residual/restriction (+ ghost fill),
 // coarse ghost fill + rhs; base: 2 n_cycle_base half-sweeps + ghost fill;
@@ -941,15 +1148,40 @@ __device__ void p_residual_all(const RunDev &R, const MGV &M, int max_lvl) {
 __device__ void p_vcycle(const RunDev &R, const MGV &M, int max_lvl, bool stale_base) {
   const int min_lvl = R.min_lvl;
   for (int lvl = max_lvl; lvl >= min_lvl + 1; lvl--) {
-    for (int it = 1; it <= 4; it++) p_sweep(R, M, lvl, it, false);
-    p_fr(R, M, lvl, true, false, false);
+    const LvlInfo L = lvl_info(R, lvl);
+    if (plan_fits(M, L)) {
+      const LevelPlan P = make_level_plan(M, L, R.coord == 1);
+      #pragma unroll 1
+      for (int it = 1; it <= 4; it++) plan_sweep(R, M, L, P, it, false);
+      plan_fr(R, M, L, P, lvl);
+    } else {
+      for (int it = 1; it <= 4; it++) p_sweep(R, M, lvl, it, false);
+      p_fr(R, M, lvl, true, false, false);
+    }
     p_fc(R, M, lvl - 1, true);
   }
-  for (int it = 1; it <= 2 * R.n_cycle_base; it++) p_sweep(R, M, min_lvl, it, stale_base && it == 1);
+  {
+    const LvlInfo L = lvl_info(R, min_lvl);
+    if (plan_fits(M, L)) {
+      const LevelPlan P = make_level_plan(M, L, R.coord == 1);
+      #pragma unroll 1
+      for (int it = 1; it <= 2 * R.n_cycle_base; it++) plan_sweep(R, M, L, P, it, stale_base && it == 1);
+    } else {
+      for (int it = 1; it <= 2 * R.n_cycle_base; it++) p_sweep(R, M, min_lvl, it, stale_base && it == 1);
+    }
+  }
   p_fill(R, M, min_lvl);
   for (int lvl = min_lvl + 1; lvl <= max_lvl; lvl++) {
-    p_correct(R, M, lvl, false, true);
-    for (int it = 1; it <= 4; it++) p_sweep(R, M, lvl, it, false);
+    const LvlInfo L = lvl_info(R, lvl);
+    if (plan_fits(M, L)) {
+      const LevelPlan P = make_level_plan(M, L, R.coord == 1);
+      p_correct(R, M, lvl, false, true);
+      #pragma unroll 1
+      for (int it = 1; it <= 4; it++) plan_sweep(R, M, L, P, it, false);
+    } else {
+      p_correct(R, M, lvl, false, true);
+      for (int it = 1; it <= 4; it++) p_sweep(R, M, lvl, it, false);
+    }
     p_fill(R, M, lvl);
   }
 }
@@ -996,14 +1228,14 @@ __device__ void stage_mg(const RunDev &R, const MGV &M, bool in) {
   __syncthreads();
 }
 
-extern __shared__ double g_dsmem[];
 
 // mg$D_fas_fmg in shared memory when the tree fits (the three variables,
 // the box records and the parent-box list), else in device memory
 __device__ void p_fmg(const RunDev &R, bool set_residual, bool first_call, bool leaf_rhs) {
   if (R.smem_doubles > 0) {
     const int S = R.smem_doubles, nbx = R.bx_off[R.nlev], npb = R.pb_off[R.nlev];
-    BoxRec *sb = reinterpret_cast<BoxRec *>(g_dsmem + 3 * S);
+    double *base = g_dsmem + PLAN_DOUBLES + (R.coord == 1 ? WTS_DOUBLES : 0);
+    BoxRec *sb = reinterpret_cast<BoxRec *>(base + 3 * S);
     int *spb = reinterpret_cast<int *>(sb + nbx);
     {
       const int4 *src = reinterpret_cast<const int4 *>(R.sboxes);
@@ -1013,12 +1245,12 @@ __device__ void p_fmg(const RunDev &R, bool set_residual, bool first_call, bool 
       for (int k = threadIdx.x; k < npb; k += NTHR) spb[k] = R.pbx[k];
     }
     __syncthreads();
-    MGV M{g_dsmem, g_dsmem + S, g_dsmem + 2 * S, sb, spb};
+    MGV M{base, base + S, base + 2 * S, sb, spb, true};
     stage_mg(R, M, true);
     p_fmg_in(R, M, set_residual, first_call, leaf_rhs);
     stage_mg(R, M, false);
   } else {
-    MGV M{VAR(R, MP), VAR(R, MR), VAR(R, MT), R.boxes, R.pbx};
+    MGV M{VAR(R, MP), VAR(R, MR), VAR(R, MT), R.boxes, R.pbx, false};
     p_fmg_in(R, M, set_residual, first_call, leaf_rhs);
   }
 }
@@ -2702,7 +2934,8 @@ int a5g_upload_tree(a5g_ctx *c, int max_id, int min_lvl, int max_lvl, const int 
   RunDev &h = c->h;
   {
     // keep the multigrid variables in shared memory when the tree fits
-    const size_t need = 3 * (size_t)P.smem_doubles * sizeof(double) +
+    const size_t need = (PLAN_DOUBLES + (c->p.coord == 1 ? WTS_DOUBLES : 0)) * sizeof(double) +
+                        3 * (size_t)P.smem_doubles * sizeof(double) +
                         P.boxes.size() * sizeof(BoxRec) + P.pbx.size() * sizeof(int);
     const size_t limit = dyn_smem_limit();
     h.smem_doubles = need <= limit ? P.smem_doubles : 0;
