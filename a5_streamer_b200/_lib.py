@@ -39,6 +39,16 @@ class Params(ctypes.Structure):
     ]
 
 
+A5G_FP64, A5G_MIXED = 0, 1
+
+
+class MGSchedule(ctypes.Structure):
+    """a5g_mg_schedule: multigrid schedule of the FP32 correction solve."""
+    _fields_ = [("fmg", ctypes.c_int), ("n_cycle_down", ctypes.c_int),
+                ("n_cycle_up", ctypes.c_int), ("n_cycle_base", ctypes.c_int),
+                ("n_corr", ctypes.c_int)]
+
+
 # name -> (restype, argtypes); every function returns an a5g_status int
 _P = ctypes.c_void_p
 _D = ctypes.c_double
@@ -71,6 +81,8 @@ SIGNATURES = {
     "a5g_ref_flags": (_I, [_P, _D, _PI]),
     "a5g_prolong_new": (_I, [_P, _PI, _PI]),
     "a5g_step": (_I, [_P, _D]),
+    "a5g_set_precision": (_I, [_P, _I, ctypes.POINTER(MGSchedule)]),
+    "a5g_get_precision": (_I, [_P, _PI, ctypes.POINTER(MGSchedule)]),
     "a5g_set_photon_table": (_I, [_P, _I, _D, _D, _PD, _D]),
     "a5g_get_rng": (_I, [_P, _PI]),
     "a5g_set_rng": (_I, [_P, _PI]),
@@ -81,6 +93,7 @@ SIGNATURES = {
     "a5g_sync": (_I, [_P]),
     "a5g_n_leaf_cells": (_I, [_P, ctypes.POINTER(ctypes.c_longlong)]),
     "a5g_get_stream": (_I, [_P, ctypes.POINTER(_P)]),
+    "a5g_debug_set_staging": (_I, [_P, _I]),
     "a5g_debug_plans": (_I, [_I, _I, _I, _PI, _PD, _PI, _PI, _D, _PI, _PI, _P, _PI, _PD, _PI]),
     # host tree (include/a5t.h)
     "a5t_create": (_I, [_I, _I, _D, _PD, _I, ctypes.POINTER(_P)]),

@@ -29,6 +29,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 namespace {
@@ -122,6 +123,14 @@ struct RunDev {
   struct PhScal *ph_scal;
   const struct MzJump *ph_jump;
   const struct PhBox *ph_boxes;
+  // mixed precision (a5g_set_precision): schedule of the FP32 correction
+  // solve, FP32 storage when the tree does not fit in shared memory, FP32
+  // copy of the transport table
+  int mx_enabled, mx_fmg, mx_sw_down, mx_sw_up, mx_sw_base, mx_n_corr;
+  int mx_smem;                 // floats per variable of the shared-memory copy; 0: cc32
+  int mx_pad;
+  float *cc32;
+  const float *tbl32;
 };
 
 // Scalars of one photoionization call: photons created, the factor fac
@@ -150,7 +159,7 @@ static_assert(sizeof(PhBox) == 48, "PhBox layout");
 enum OpCode {
   OP_COPY = 1, OP_FLUXES, OP_CONSISTENT, OP_UPDATE, OP_RESTRICT, OP_GC, OP_AVERAGE,
   OP_COMPUTE_FLD, OP_FMG, OP_FLD_FROM_POT, OP_DT_RED, OP_REF_FLAGS, OP_PROLONG_NEW,
-  OP_STEP, OP_NOP, OP_PH_SOURCE, OP_PH_DEPOSIT
+  OP_STEP, OP_NOP, OP_PH_SOURCE, OP_PH_DEPOSIT, OP_STEP_MIXED, OP_COMPUTE_FLD_MIXED
 };
 struct Op {
   int code, i0, i1, i2;
@@ -218,20 +227,22 @@ __device__ __forceinline__ void child_offset(const BoxMeta &m, int nb, int &o0, 
   }
 }
 
-// gfortran's inline NORM2 for two elements (scaled sum of squares)
-__device__ __forceinline__ double norm2_2(double x0, double x1) {
-  double scale = 0.0, ssq = 1.0;
-  double xs[2] = {x0, x1};
+// gfortran's inline NORM2 for two elements (scaled sum of squares). T is
+// double on the plain path and float for the FP32 transport of the mixed form.
+template <class T>
+__device__ __forceinline__ T norm2_2(T x0, T x1) {
+  T scale = T(0), ssq = T(1);
+  T xs[2] = {x0, x1};
 #pragma unroll
   for (int k = 0; k < 2; k++) {
-    if (xs[k] != 0.0) {
-      double ax = fabs(xs[k]);
+    if (xs[k] != T(0)) {
+      T ax = fabs(xs[k]);
       if (scale < ax) {
-        double v = scale / ax;
-        ssq = 1.0 + ssq * v * v;
+        T v = scale / ax;
+        ssq = T(1) + ssq * v * v;
         scale = ax;
       } else {
-        double v = ax / scale;
+        T v = ax / scale;
         ssq += v * v;
       }
     }
@@ -240,35 +251,49 @@ __device__ __forceinline__ double norm2_2(double x0, double x1) {
 }
 
 // fosito/m_lookup_table.f90:107-125 (get_loc) and 154-161 (LT_get_col_at_loc)
-struct Loc { int ix; double fr; };
-__device__ __forceinline__ Loc get_loc(const RunDev &R, double x) {
-  double frac = (x - R.tbl_xmin) * R.tbl_inv_dx;
-  Loc l;
-  if (frac < 2.0e9 && frac > -2.0e9) {
+// (T = float: the same lookup on the FP32 copy of the table.)
+template <class T> struct Loc { int ix; T fr; };
+template <class T>
+__device__ __forceinline__ Loc<T> get_loc(const RunDev &R, T x) {
+  T frac = (x - T(R.tbl_xmin)) * T(R.tbl_inv_dx);
+  Loc<T> l;
+  if (frac < T(2.0e9) && frac > T(-2.0e9)) {
     l.ix = (int)ceil(frac);
-    l.fr = l.ix - frac;
+    l.fr = T(l.ix) - frac;
   } else {
-    l.ix = frac > 0 ? R.tbl_rows : 0;
-    l.fr = 0;
+    l.ix = frac > T(0) ? R.tbl_rows : 0;
+    l.fr = T(0);
   }
-  if (l.ix < 1) { l.ix = 1; l.fr = 1; }
-  else if (l.ix >= R.tbl_rows) { l.ix = R.tbl_rows - 1; l.fr = 0; }
+  if (l.ix < 1) { l.ix = 1; l.fr = T(1); }
+  else if (l.ix >= R.tbl_rows) { l.ix = R.tbl_rows - 1; l.fr = T(0); }
   return l;
 }
-__device__ __forceinline__ double col_at(const RunDev &R, int c, const Loc &l) {
-  const double *T = R.tbl + (size_t)R.tbl_rows * c;
-  return l.fr * __ldg(T + l.ix - 1) + (1 - l.fr) * __ldg(T + l.ix);
+template <class T> __device__ __forceinline__ const T *table_of(const RunDev &R);
+template <> __device__ __forceinline__ const double *table_of<double>(const RunDev &R) { return R.tbl; }
+template <> __device__ __forceinline__ const float *table_of<float>(const RunDev &R) { return R.tbl32; }
+template <class T>
+__device__ __forceinline__ T col_at(const RunDev &R, int c, const Loc<T> &l) {
+  const T *tb = table_of<T>(R) + (size_t)R.tbl_rows * c;
+  return l.fr * __ldg(tb + l.ix - 1) + (T(1) - l.fr) * __ldg(tb + l.ix);
 }
 
 // src/m_streamer.f90:339-362 (koren_mlim)
-__device__ __forceinline__ double koren_mlim(double a, double b) {
-  const double sixth = 1 / 6.0;
-  double aa = a * a, ab = a * b;
-  if (ab <= 0) return 0;
-  if (aa <= 0.25 * ab) return a;
-  if (aa <= 2.5 * ab) return sixth * (b + 2 * a);
+template <class T>
+__device__ __forceinline__ T koren_mlim(T a, T b) {
+  const T sixth = T(1 / 6.0);
+  T aa = a * a, ab = a * b;
+  if (ab <= T(0)) return T(0);
+  if (aa <= T(0.25) * ab) return a;
+  if (aa <= T(2.5) * ab) return sixth * (b + T(2) * a);
   return b;
 }
+
+// Scale of the densities inside the FP32 fluxes: an exact power of two that
+// keeps squares of density differences (up to ~1e21 m^-3) inside the float
+// range. The fluxes are homogeneous of degree one in the density, so the
+// scaled flux times 1/scale is the flux. 1 on the FP64 path.
+template <class T> __device__ __forceinline__ T dens_scale() { return T(1); }
+template <> __device__ __forceinline__ float dens_scale<float>() { return 0x1p-40f; }
 
 // ---------------------------------------------------------------------------
 // Ghost cells (afivo/src/m_aX_gc.f90). Value of side ghost (nb, k), k = 1..nc,
@@ -421,16 +446,20 @@ __device__ double gc2_value(const RunDev &R, const BoxMeta &m, int id, int iv, i
 // ---------------------------------------------------------------------------
 // Flux and source update.
 
-// fluxes_koren, src/streamer_2d.f90:384-489 (cyl :416-521 is the same)
+// fluxes_koren, src/streamer_2d.f90:384-489 (cyl :416-521 is the same).
+// T: arithmetic type of the flux (double; float in the mixed form, where the
+// densities enter scaled by dens_scale and the flux leaves unscaled).
+template <class T>
 __device__ void fluxes_koren(const RunDev &R, double dt) {
   const int *ids;
   int n;
   list_range(R, 1, R.min_lvl, R.max_lvl, ids, n);
-  const double fac = -0.8 * UC_EPS0 / (UC_ELEM_CHARGE * dt);
+  const T ds = dens_scale<T>();
+  const T fac = T(-0.8 * UC_EPS0 / (UC_ELEM_CHARGE * dt)) * ds;
   box_loop(ids, n, [&](int id, int t) {
     const BoxMeta &m = R.meta[id];
     const int nc = m.nc, ncg = nc + 2;
-    const double inv_dr = 1 / m.dr;
+    const T inv_dr = T(1 / m.dr);
     const double *e = CC(R, I_ELEC, id), *fl = CC(R, I_FLD, id);
     double *fxe = FX(R, F_ELEC, id), *fye = FY(R, F_ELEC, id);
     const double *fxf = FX(R, F_FLD, id), *fyf = FY(R, F_FLD, id);
@@ -445,29 +474,31 @@ __device__ void fluxes_koren(const RunDev &R, double dt) {
       const int s = xd ? 1 : ncg;
       const int c = i + ncg * j;          // cell (i, j): high side of the face
       const int pos = xd ? i : j;         // face index along the direction
-      double fld_avg = 0.5 * (fl[c] + fl[c - s]);
-      Loc loc = get_loc(R, fld_avg);
-      double mobility = col_at(R, C_MOB, loc);
-      double diff_coeff = col_at(R, C_DIF, loc);
-      double fld = xd ? fxf[fxi(i, j, nc)] : fyf[fyi(i, j, nc)];
-      double v_drift = -mobility * fld;
-      double gradc = e[c] - e[c - s];
-      double fv;
+      T fld_avg = T(0.5) * (T(fl[c]) + T(fl[c - s]));
+      Loc<T> loc = get_loc<T>(R, fld_avg);
+      T mobility = col_at<T>(R, C_MOB, loc);
+      T diff_coeff = col_at<T>(R, C_DIF, loc);
+      T fld = T(xd ? fxf[fxi(i, j, nc)] : fyf[fyi(i, j, nc)]);
+      T v_drift = -mobility * fld;
+      const T ec = T(e[c]) * ds, em = T(e[c - s]) * ds;
+      T gradc = ec - em;
+      T fv;
       const int k = xd ? j : i;
-      if (v_drift < 0.0) {
-        double tmp = (pos == nc + 1) ? gc2_value(R, m, id, I_ELEC, xd ? 1 : 3, k) : e[c + s];
-        double gradn = tmp - e[c];
-        fv = v_drift * (e[c] - koren_mlim(gradc, gradn));
+      if (v_drift < T(0)) {
+        T tmp = T((pos == nc + 1) ? gc2_value(R, m, id, I_ELEC, xd ? 1 : 3, k) : e[c + s]) * ds;
+        T gradn = tmp - ec;
+        fv = v_drift * (ec - koren_mlim(gradc, gradn));
         if (fv < fac * fld) fv = fac * fld;
       } else {
-        double tmp = (pos == 1) ? gc2_value(R, m, id, I_ELEC, xd ? 0 : 2, k) : e[c - 2 * s];
-        double gradp = e[c - s] - tmp;
-        fv = v_drift * (e[c - s] + koren_mlim(gradc, gradp));
+        T tmp = T((pos == 1) ? gc2_value(R, m, id, I_ELEC, xd ? 0 : 2, k) : e[c - 2 * s]) * ds;
+        T gradp = em - tmp;
+        fv = v_drift * (em + koren_mlim(gradc, gradp));
         if (fv > fac * fld) fv = fac * fld;
       }
       fv = fv - diff_coeff * gradc * inv_dr;
-      if (xd) fxe[fxi(i, j, nc)] = fv;
-      else fye[fyi(i, j, nc)] = fv;
+      const double out = (double)fv / (double)ds;
+      if (xd) fxe[fxi(i, j, nc)] = out;
+      else fye[fyi(i, j, nc)] = out;
     }
   });
 }
@@ -505,7 +536,10 @@ __device__ void consistent_fluxes(const RunDev &R) {
   });
 }
 
-// update_solution, src/streamer_2d.f90:499-542 and src/streamer_cyl.f90:531-570
+// update_solution, src/streamer_2d.f90:499-542 and src/streamer_cyl.f90:531-570.
+// T: arithmetic type of the source and flux divergence (float in the mixed
+// form); the densities are accumulated in double.
+template <class T>
 __device__ void update_solution(const RunDev &R, double dt) {
   const int *ids;
   int n;
@@ -516,28 +550,29 @@ __device__ void update_solution(const RunDev &R, double dt) {
     const int nc = m.nc, ncg = nc + 2;
     if (t >= nc * nc) return;
     const int i = t % nc + 1, j = t / nc + 1, c = i + ncg * j;
-    const double inv_dr = 1 / m.dr;
+    const T inv_dr = T(1 / m.dr);
     double *e = CC(R, I_ELEC, id), *pi = CC(R, I_PION, id);
     const double *fxe = FX(R, F_ELEC, id), *fye = FY(R, F_ELEC, id);
-    double fld = CC(R, I_FLD, id)[c];
-    Loc loc = get_loc(R, fld);
-    double alpha = col_at(R, C_ALPHA, loc);
-    double eta = col_at(R, C_ETA, loc);
-    double fx0 = fxe[fxi(i, j, nc)], fx1 = fxe[fxi(i + 1, j, nc)];
-    double fy0 = fye[fyi(i, j, nc)], fy1 = fye[fyi(i, j + 1, nc)];
-    double src = 0.5 * norm2_2(fx0 + fx1, fy0 + fy1) * (alpha - eta);
-    if (R.ph_enabled) src = src + CC(R, I_PHO, id)[c];
-    double sflux;
+    T fld = T(CC(R, I_FLD, id)[c]);
+    Loc<T> loc = get_loc<T>(R, fld);
+    T alpha = col_at<T>(R, C_ALPHA, loc);
+    T eta = col_at<T>(R, C_ETA, loc);
+    T fx0 = T(fxe[fxi(i, j, nc)]), fx1 = T(fxe[fxi(i + 1, j, nc)]);
+    T fy0 = T(fye[fyi(i, j, nc)]), fy1 = T(fye[fyi(i, j + 1, nc)]);
+    T src = T(0.5) * norm2_2<T>(fx0 + fx1, fy0 + fy1) * (alpha - eta);
+    if (R.ph_enabled) src = src + T(CC(R, I_PHO, id)[c]);
+    T sflux;
     if (cyl) {
       int ioff = (m.ix0 - 1) * nc;
-      double den = i + ioff - 0.5;
-      double rf1 = (i + ioff - 1) / den, rf2 = (i + ioff) / den;
+      T den = T(i + ioff) - T(0.5);
+      T rf1 = T(i + ioff - 1) / den, rf2 = T(i + ioff) / den;
       sflux = (fy0 - fy1 + rf1 * fx0 - rf2 * fx1) * inv_dr;
     } else {
       sflux = (fx0 - fx1 + fy0 - fy1) * inv_dr;
     }
-    double ne = e[c] + (src + sflux) * dt;
-    double ni = pi[c] + src * dt;
+    const T tdt = T(dt);
+    double ne = e[c] + (double)((src + sflux) * tdt);
+    double ni = pi[c] + (double)(src * tdt);
     if (!cyl && CC(R, I_EPS, id)[c] > 1.0) {
       ni = ni - ne;
       ne = 0;
@@ -566,19 +601,28 @@ __device__ __forceinline__ double *VAR(const RunDev &R, int v) {
 // compact copy in shared memory when the tree fits (then every read in a
 // phase that follows a write by another thread hits shared memory instead
 // of L2). boxes: the BoxRecs addressing those arrays.
+// T is the storage and arithmetic type of the solve: double for the plain
+// FP64 path, float for the inner correction solve of the mixed form. V is the
+// potential of the applied-voltage wall (0 for the homogeneous correction
+// equation); sw_*: half-sweeps per level visit (reference: 4 down, 4 up,
+// 2 n_cycle_base on the coarsest level).
+template <class T>
 struct MGV {
-  double *phi, *rhs, *tmp;
+  T *phi, *rhs, *tmp;
   const BoxRec *boxes;
   const int *pbx;
   bool plans;  // the cell plans of "Cell plans" are available (shared-memory solve)
+  double V;
+  int sw_down, sw_up, sw_base;
 };
 
 // Side ghost (side, k) of the potential: sides_from_nb, mg$D_sides_rb after
 // a$D_gc_prolong0 (m_aX_mg.f90:261-301), or sides_bc_pot
 // (src/streamer_2d.f90:620-638). Reads only interior cells of the box and its
 // neighbours and ghost cells of the parent.
-__device__ __forceinline__ double phi_ghost(const RunDev &R, const double *phi, const BoxRec &B,
-                                            int nc, int ncg, int side, int k) {
+template <class T>
+__device__ __forceinline__ T phi_ghost(double V, const T *phi, const BoxRec &B, int nc, int ncg,
+                                       int side, int k) {
   const int dim = side >> 1;
   const bool low = (side & 1) == 0;
   const int nbb = B.nb[side];
@@ -597,10 +641,10 @@ __device__ __forceinline__ double phi_ghost(const RunDev &R, const double *phi, 
       a = own + dk;
       b = own + ncg * di;
     }
-    return 0.5 * phi[pc] + phi[own] - 0.25 * (phi[a] + phi[b]);
+    return T(0.5) * phi[pc] + phi[own] - T(0.25) * (phi[a] + phi[b]);
   }
   if (side == 2) return -phi[own];
-  if (side == 3) return 2 * R.applied_voltage - phi[own];
+  if (side == 3) return T(2 * V) - phi[own];
   return phi[own];
 }
 
@@ -641,8 +685,9 @@ __device__ __forceinline__ double den_ghost(const double *x, const BoxRec &B, in
 // the kind of the side (neighbour copy, refinement boundary, physical wall),
 // so that a cell's loads are in flight together instead of behind branches.
 // Same values and the same arithmetic as phi_ghost.
-__device__ __forceinline__ double phi_ghost_sl(const RunDev &R, const double *phi, const BoxRec &B,
-                                               int nc, int ncg, int side, int k) {
+template <class T>
+__device__ __forceinline__ T phi_ghost_sl(double V, const T *phi, const BoxRec &B, int nc, int ncg,
+                                          int side, int k) {
   const int dim = side >> 1;
   const bool low = (side & 1) == 0;
   const int nbb = B.nb[side];
@@ -658,22 +703,22 @@ __device__ __forceinline__ double phi_ghost_sl(const RunDev &R, const double *ph
   const bool isnb = nbb > 0, isrb = nbb == NBR_RB;
   const int s0 = isnb ? cp : (isrb ? pc : own);
   const int s1 = isrb ? own : s0, s2 = isrb ? a : s0, s3 = isrb ? b : s0;
-  const double v0 = phi[s0], v1 = phi[s1], v2 = phi[s2], v3 = phi[s3];
-  const double vrb = 0.5 * v0 + v1 - 0.25 * (v2 + v3);
-  const double vbc = side == 2 ? -v0 : (side == 3 ? 2 * R.applied_voltage - v0 : v0);
+  const T v0 = phi[s0], v1 = phi[s1], v2 = phi[s2], v3 = phi[s3];
+  const T vrb = T(0.5) * v0 + v1 - T(0.25) * (v2 + v3);
+  const T vbc = side == 2 ? -v0 : (side == 3 ? T(2 * V) - v0 : v0);
   return isnb ? v0 : (isrb ? vrb : vbc);
 }
 
 // Neighbours (lx, hx, ly, hy) of interior cell (i, j). A cell has at most
 // one ghost neighbour in x and one in y; both are evaluated unconditionally
 // (straight-line) and selected where needed.
-__device__ __forceinline__ void phi_nbrs(const RunDev &R, const double *phi, const BoxRec &B,
-                                         int nc, int ncg, int i, int j, int g, double &lx,
-                                         double &hx, double &ly, double &hy) {
-  const double gx = phi_ghost_sl(R, phi, B, nc, ncg, i == 1 ? 0 : 1, j);
-  const double gy = phi_ghost_sl(R, phi, B, nc, ncg, j == 1 ? 2 : 3, i);
-  const double dlx = phi[g - (i > 1 ? 1 : 0)], dhx = phi[g + (i < nc ? 1 : 0)];
-  const double dly = phi[g - (j > 1 ? ncg : 0)], dhy = phi[g + (j < nc ? ncg : 0)];
+template <class T>
+__device__ __forceinline__ void phi_nbrs(double V, const T *phi, const BoxRec &B, int nc, int ncg,
+                                         int i, int j, int g, T &lx, T &hx, T &ly, T &hy) {
+  const T gx = phi_ghost_sl(V, phi, B, nc, ncg, i == 1 ? 0 : 1, j);
+  const T gy = phi_ghost_sl(V, phi, B, nc, ncg, j == 1 ? 2 : 3, i);
+  const T dlx = phi[g - (i > 1 ? 1 : 0)], dhx = phi[g + (i < nc ? 1 : 0)];
+  const T dly = phi[g - (j > 1 ? ncg : 0)], dhy = phi[g + (j < nc ? ncg : 0)];
   lx = i > 1 ? dlx : gx;
   hx = i < nc ? dhx : gx;
   ly = j > 1 ? dly : gy;
@@ -681,19 +726,20 @@ __device__ __forceinline__ void phi_nbrs(const RunDev &R, const double *phi, con
 }
 
 // box_lpl (m_aX_mg.f90:662-680) / box_clpl (:1027-1049) at one cell
-__device__ __forceinline__ double lap_at(const RunDev &R, const double *phi, const BoxRec &B,
-                                         int nc, int ncg, int i, int j, double inv_dr_sq) {
+template <class T>
+__device__ __forceinline__ T lap_at(const RunDev &R, double V, const T *phi, const BoxRec &B, int nc,
+                                    int ncg, int i, int j, T inv_dr_sq) {
   const int g = B.base + i + ncg * j;
-  double lx, hx, ly, hy;
-  phi_nbrs(R, phi, B, nc, ncg, i, j, g, lx, hx, ly, hy);
-  const double v = phi[g];
+  T lx, hx, ly, hy;
+  phi_nbrs(V, phi, B, nc, ncg, i, j, g, lx, hx, ly, hy);
+  const T v = phi[g];
   if (R.coord == 1) {
     const int gi = B.gi0 + i;
-    const double den = gi - 0.5;
-    const double rf1 = (gi - 1) / den, rf2 = gi / den;
-    return (rf1 * lx + rf2 * hx + ly + hy - 4 * v) * inv_dr_sq;
+    const T den = T(gi) - T(0.5);
+    const T rf1 = T(gi - 1) / den, rf2 = T(gi) / den;
+    return (rf1 * lx + rf2 * hx + ly + hy - T(4) * v) * inv_dr_sq;
   }
-  return inv_dr_sq * (lx + hx + ly + hy - 4 * v);
+  return inv_dr_sq * (lx + hx + ly + hy - T(4) * v);
 }
 
 struct LvlInfo {
@@ -720,11 +766,12 @@ __device__ __forceinline__ LvlInfo lvl_info(const RunDev &R, int lvl) {
 // it is written), or coarser-level cells. mem: read ghosts from memory
 // instead (first half-sweep of a first FMG call, where the reference's
 // ghosts are not consistent with the interior).
-__device__ __noinline__ void p_sweep(const RunDev &R, const MGV &M, int lvl, int it, bool mem) {
+template <class T>
+__device__ __noinline__ void p_sweep(const RunDev &R, const MGV<T> &M, int lvl, int it, bool mem) {
   const LvlInfo L = lvl_info(R, lvl);
-  double *phi = M.phi;
-  const double *rhs = M.rhs;
-  const double dx2 = L.dr * L.dr;
+  T *phi = M.phi;
+  const T *rhs = M.rhs;
+  const T dx2 = T(L.dr * L.dr);
   const int half = (L.nc * L.nc) >> 1, hsh = 2 * L.sh - 1, hn = L.nc >> 1;
   const int p = it & 1;  // parity (i + j) & 1 of the updated cells
   const bool cyl = R.coord == 1;
@@ -735,20 +782,20 @@ __device__ __noinline__ void p_sweep(const RunDev &R, const MGV &M, int lvl, int
     const int j = t / hn + 1, m = t % hn;
     const int i = 2 * m + 2 - ((p + j) & 1);
     const int g = B.base + i + L.ncg * j;
-    double lx, hx, ly, hy;
+    T lx, hx, ly, hy;
     if (mem) {
       lx = phi[g - 1]; hx = phi[g + 1]; ly = phi[g - L.ncg]; hy = phi[g + L.ncg];
     } else {
-      phi_nbrs(R, phi, B, L.nc, L.ncg, i, j, g, lx, hx, ly, hy);
+      phi_nbrs(M.V, phi, B, L.nc, L.ncg, i, j, g, lx, hx, ly, hy);
     }
-    const double r = rhs[g];
+    const T r = rhs[g];
     if (cyl) {
       const int gi = B.gi0 + i;
-      const double den = gi - 0.5;
-      const double rf1 = (gi - 1) / den, rf2 = gi / den;
-      phi[g] = 0.25 * (rf1 * lx + rf2 * hx + hy + ly - dx2 * r);
+      const T den = T(gi) - T(0.5);
+      const T rf1 = T(gi - 1) / den, rf2 = T(gi) / den;
+      phi[g] = T(0.25) * (rf1 * lx + rf2 * hx + hy + ly - dx2 * r);
     } else {
-      phi[g] = 0.25 * (hx + lx + hy + ly - dx2 * r);
+      phi[g] = T(0.25) * (hx + lx + hy + ly - dx2 * r);
     }
   }
   __syncthreads();
@@ -757,20 +804,22 @@ __device__ __noinline__ void p_sweep(const RunDev &R, const MGV &M, int lvl, int
 // Ghost fill of the potential on level lvl (fill_gc_phi, :303-316), no
 // barrier. copy_tmp: also tmp = phi on the ghosts of parent boxes (the
 // whole-box copy of update_coarse, :407).
-__device__ __forceinline__ void fill_phi_loop(const RunDev &R, const MGV &M, const LvlInfo &L, bool copy_tmp) {
-  double *phi = M.phi, *tmp = M.tmp;
+template <class T>
+__device__ __forceinline__ void fill_phi_loop(const RunDev &R, const MGV<T> &M, const LvlInfo &L, bool copy_tmp) {
+  T *phi = M.phi, *tmp = M.tmp;
   const int per = 4 * L.nc, n = L.nb * per;
   for (int k = threadIdx.x; k < n; k += NTHR) {
     const BoxRec &B = M.boxes[L.b0 + k / per];
     const int r = k % per, side = r >> L.sh, kk = (r & (L.nc - 1)) + 1;
-    const double v = phi_ghost(R, phi, B, L.nc, L.ncg, side, kk);
+    const T v = phi_ghost(M.V, phi, B, L.nc, L.ncg, side, kk);
     const int dim = side >> 1, gx = (side & 1) ? L.nc + 1 : 0;
     const int d = B.base + (dim == 0 ? gx + L.ncg * kk : kk + L.ncg * gx);
     phi[d] = v;
     if (copy_tmp && (B.flags & CF_PARENT)) tmp[d] = v;
   }
 }
-__device__ void p_fill(const RunDev &R, const MGV &M, int lvl) {
+template <class T>
+__device__ void p_fill(const RunDev &R, const MGV<T> &M, int lvl) {
   fill_phi_loop(R, M, lvl_info(R, lvl), false);
   __syncthreads();
 }
@@ -783,39 +832,40 @@ __device__ void p_fill(const RunDev &R, const MGV &M, int lvl) {
 // leaf cells (src/streamer_2d.f90:317-329). store_res: keep the residual in
 // the box's own tmp (set_coarse_phi_rhs); otherwise tmp is left as it was
 // (update_coarse saves and restores it).
-__device__ __noinline__ void p_fr(const RunDev &R, const MGV &M, int lvl, bool fill, bool leaf_rhs, bool store_res) {
+template <class T>
+__device__ __noinline__ void p_fr(const RunDev &R, const MGV<T> &M, int lvl, bool fill, bool leaf_rhs, bool store_res) {
   const LvlInfo L = lvl_info(R, lvl);
   const int pncg = R.lv_nc[lvl - 1 - R.min_lvl] + 2;
-  double *phi = M.phi, *tmp = M.tmp, *rhs = M.rhs;
+  T *phi = M.phi, *tmp = M.tmp, *rhs = M.rhs;
   const double *e = VAR(R, I_ELEC), *pi = VAR(R, I_PION);
-  const double inv_dr_sq = 1 / (L.dr * L.dr);
+  const T inv_dr_sq = T(1 / (L.dr * L.dr));
   const double fac = UC_ELEM_CHARGE / UC_EPS0;
   const int hn = L.nc >> 1, per = hn * hn, n = L.nb * per;
   for (int k = threadIdx.x; k < n; k += NTHR) {
     const BoxRec &B = M.boxes[L.b0 + k / per];
     const int t = k % per, ii = t % hn + 1, jj = t / hn + 1;
     const bool leaf = leaf_rhs && (B.flags & CF_LEAF);
-    double rs[4], ps[4];
+    T rs[4], ps[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       const int i = 2 * ii - 1 + (q & 1), j = 2 * jj - 1 + (q >> 1);
       const int g = B.base + i + L.ncg * j;
-      double rh;
+      T rh;
       if (leaf) {
         const int gg = B.gbase + i + L.ncg * j;
-        rh = fac * (e[gg] - pi[gg]);
+        rh = T(fac * (e[gg] - pi[gg]));
         rhs[g] = rh;
       } else {
         rh = rhs[g];
       }
-      const double res = rh - lap_at(R, phi, B, L.nc, L.ncg, i, j, inv_dr_sq);
+      const T res = rh - lap_at(R, M.V, phi, B, L.nc, L.ncg, i, j, inv_dr_sq);
       if (store_res) tmp[g] = res;
       rs[q] = res;
       ps[q] = phi[g];
     }
     const int d = B.pbase + (B.o0 + ii) + pncg * (B.o1 + jj);
-    tmp[d] = 0.25 * (rs[0] + rs[1] + rs[2] + rs[3]);
-    phi[d] = 0.25 * (ps[0] + ps[1] + ps[2] + ps[3]);
+    tmp[d] = T(0.25) * (rs[0] + rs[1] + rs[2] + rs[3]);
+    phi[d] = T(0.25) * (ps[0] + ps[1] + ps[2] + ps[3]);
   }
   if (fill) fill_phi_loop(R, M, L, false);
   __syncthreads();
@@ -824,20 +874,21 @@ __device__ __noinline__ void p_fr(const RunDev &R, const MGV &M, int lvl, bool f
 // Ghost fill of level lvl and the coarse right-hand side of its parent
 // boxes: rhs = A phi + tmp (box_op then a$D_box_add_cc, :399-402 / :441-444);
 // copy_tmp: then tmp = phi (a$D_box_copy_cc, :403).
-__device__ void p_fc(const RunDev &R, const MGV &M, int lvl, bool copy_tmp) {
+template <class T>
+__device__ void p_fc(const RunDev &R, const MGV<T> &M, int lvl, bool copy_tmp) {
   const LvlInfo L = lvl_info(R, lvl);
   const int li = lvl - R.min_lvl;
   const int *pb = M.pbx + R.pb_off[li];
   const int npb = R.pb_off[li + 1] - R.pb_off[li];
-  double *phi = M.phi, *tmp = M.tmp, *rhs = M.rhs;
-  const double inv_dr_sq = 1 / (L.dr * L.dr);
+  T *phi = M.phi, *tmp = M.tmp, *rhs = M.rhs;
+  const T inv_dr_sq = T(1 / (L.dr * L.dr));
   const int per = L.nc * L.nc, n = npb * per;
   for (int k = threadIdx.x; k < n; k += NTHR) {
     const BoxRec &B = M.boxes[pb[k >> (2 * L.sh)]];
     const int t = k & (per - 1), i = (t & (L.nc - 1)) + 1, j = (t >> L.sh) + 1;
     const int g = B.base + i + L.ncg * j;
-    const double a = lap_at(R, phi, B, L.nc, L.ncg, i, j, inv_dr_sq);
-    const double pv = phi[g];
+    const T a = lap_at(R, M.V, phi, B, L.nc, L.ncg, i, j, inv_dr_sq);
+    const T pv = phi[g];
     rhs[g] = a + tmp[g];
     if (copy_tmp) tmp[g] = pv;
   }
@@ -850,16 +901,17 @@ __device__ void p_fc(const RunDev &R, const MGV &M, int lvl, bool copy_tmp) {
 // (correct_children :319-341 with box_corr_lpl :605-633). The correction
 // phi_p - tmp_p is formed where it is used instead of being stored back into
 // the parent's tmp; that stored value is never read again by the reference.
-__device__ void p_correct(const RunDev &R, const MGV &M, int lvl, bool copy, bool correct) {
+template <class T>
+__device__ void p_correct(const RunDev &R, const MGV<T> &M, int lvl, bool copy, bool correct) {
   const LvlInfo L = lvl_info(R, lvl);
   const int pncg = correct ? R.lv_nc[lvl - 1 - R.min_lvl] + 2 : 0;
-  double *phi = M.phi, *tmp = M.tmp;
+  T *phi = M.phi, *tmp = M.tmp;
   const int per = L.nc * L.nc, n = L.nb * per;
   for (int k = threadIdx.x; k < n; k += NTHR) {
     const BoxRec &B = M.boxes[L.b0 + (k >> (2 * L.sh))];
     const int t = k & (per - 1), i = (t & (L.nc - 1)) + 1, j = (t >> L.sh) + 1;
     const int g = B.base + i + L.ncg * j;
-    const double v = phi[g];
+    const T v = phi[g];
     if (copy) tmp[g] = v;
     if (correct) {
       const int i_c1 = B.o0 + ((i + 1) >> 1), i_c2 = i_c1 + 1 - 2 * (i & 1);
@@ -867,8 +919,8 @@ __device__ void p_correct(const RunDev &R, const MGV &M, int lvl, bool copy, boo
       const int p1 = B.pbase + i_c1 + pncg * j_c1;
       const int p2 = B.pbase + i_c2 + pncg * j_c1;
       const int p3 = B.pbase + i_c1 + pncg * j_c2;
-      const double c1 = phi[p1] - tmp[p1], c2x = phi[p2] - tmp[p2], c2y = phi[p3] - tmp[p3];
-      phi[g] = v + 0.5 * c1 + 0.25 * (c2x + c2y);
+      const T c1 = phi[p1] - tmp[p1], c2x = phi[p2] - tmp[p2], c2y = phi[p3] - tmp[p3];
+      phi[g] = v + T(0.5) * c1 + T(0.25) * (c2x + c2y);
     }
   }
   if (copy) {
@@ -886,10 +938,11 @@ __device__ void p_correct(const RunDev &R, const MGV &M, int lvl, bool copy, boo
 
 // init_phi_rhs for one level (m_aX_mg.f90:450-473): phi = 0 on the boxes of
 // level lvl and their rhs restricted to the parents.
-__device__ __noinline__ void p_init_level(const RunDev &R, const MGV &M, int lvl, bool leaf_rhs) {
+template <class T>
+__device__ __noinline__ void p_init_level(const RunDev &R, const MGV<T> &M, int lvl, bool leaf_rhs) {
   const LvlInfo L = lvl_info(R, lvl);
   const int pncg = R.lv_nc[lvl - 1 - R.min_lvl] + 2;
-  double *rhs = M.rhs, *phi = M.phi;
+  T *rhs = M.rhs, *phi = M.phi;
   const double *e = VAR(R, I_ELEC), *pi = VAR(R, I_PION);
   const double fac = UC_ELEM_CHARGE / UC_EPS0;
   const int hn = L.nc >> 1, per = hn * hn, n = L.nb * per;
@@ -897,39 +950,40 @@ __device__ __noinline__ void p_init_level(const RunDev &R, const MGV &M, int lvl
     const BoxRec &B = M.boxes[L.b0 + k / per];
     const int t = k % per, ii = t % hn + 1, jj = t / hn + 1;
     const bool leaf = leaf_rhs && (B.flags & CF_LEAF);
-    double rs[4];
+    T rs[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       const int loc = (2 * ii - 1 + (q & 1)) + L.ncg * (2 * jj - 1 + (q >> 1));
       const int g = B.base + loc;
       if (leaf) {
-        rs[q] = fac * (e[B.gbase + loc] - pi[B.gbase + loc]);
+        rs[q] = T(fac * (e[B.gbase + loc] - pi[B.gbase + loc]));
         rhs[g] = rs[q];
       } else {
         rs[q] = rhs[g];
       }
     }
-    rhs[B.pbase + (B.o0 + ii) + pncg * (B.o1 + jj)] = 0.25 * (rs[0] + rs[1] + rs[2] + rs[3]);
+    rhs[B.pbase + (B.o0 + ii) + pncg * (B.o1 + jj)] = T(0.25) * (rs[0] + rs[1] + rs[2] + rs[3]);
   }
   const int pc = L.ncg * L.ncg, nz = L.nb * pc;
-  for (int k = threadIdx.x; k < nz; k += NTHR) phi[M.boxes[L.b0 + k / pc].base + k % pc] = 0.0;
+  for (int k = threadIdx.x; k < nz; k += NTHR) phi[M.boxes[L.b0 + k / pc].base + k % pc] = T(0);
   __syncthreads();
 }
 
 // Residual rhs - A phi on every cell of levels min..max (set_residual of
 // mg$D_fas_vcycle, :243-253)
-__device__ __noinline__ void p_residual_all(const RunDev &R, const MGV &M, int max_lvl) {
-  double *phi = M.phi, *tmp = M.tmp;
-  const double *rhs = M.rhs;
+template <class T>
+__device__ __noinline__ void p_residual_all(const RunDev &R, const MGV<T> &M, int max_lvl) {
+  T *phi = M.phi, *tmp = M.tmp;
+  const T *rhs = M.rhs;
   for (int lvl = R.min_lvl; lvl <= max_lvl; lvl++) {
     const LvlInfo L = lvl_info(R, lvl);
-    const double inv_dr_sq = 1 / (L.dr * L.dr);
+    const T inv_dr_sq = T(1 / (L.dr * L.dr));
     const int per = L.nc * L.nc, n = L.nb * per;
     for (int k = threadIdx.x; k < n; k += NTHR) {
       const BoxRec &B = M.boxes[L.b0 + (k >> (2 * L.sh))];
       const int t = k & (per - 1), i = (t & (L.nc - 1)) + 1, j = (t >> L.sh) + 1;
       const int g = B.base + i + L.ncg * j;
-      tmp[g] = rhs[g] - lap_at(R, phi, B, L.nc, L.ncg, i, j, inv_dr_sq);
+      tmp[g] = rhs[g] - lap_at(R, M.V, phi, B, L.nc, L.ncg, i, j, inv_dr_sq);
     }
   }
   __syncthreads();
@@ -986,21 +1040,21 @@ __device__ __forceinline__ int4 make_plan(const BoxRec &B, int nc, int ncg, int 
 
 // Value of a ghost neighbour from its first source v0 and the cell's own
 // value vo, its neighbour across the box va and along the side vb.
-__device__ __forceinline__ double ghost_eval(double v0, int kind, double vo, double va, double vb,
-                                             double V) {
-  const double vrb = 0.5 * v0 + vo - 0.25 * (va + vb);
-  const double vw = kind == GK_NEG ? -vo : 2 * V - vo;
+template <class T>
+__device__ __forceinline__ T ghost_eval(T v0, int kind, T vo, T va, T vb, double V) {
+  const T vrb = T(0.5) * v0 + vo - T(0.25) * (va + vb);
+  const T vw = kind == GK_NEG ? -vo : T(2 * V) - vo;
   return kind == GK_COPY ? v0 : (kind == GK_RB ? vrb : vw);
 }
 
 // The four neighbours of the plan's cell (as phi_nbrs; mem: read the ghost
 // cells stored in memory instead). The across and along neighbours a ghost
 // recipe reads are among the cell's direct neighbours.
-__device__ __forceinline__ void plan_nbrs(const RunDev &R, const double *phi, const int4 &c, int nc,
-                                          int ncg, bool mem, double &lx, double &hx, double &ly,
-                                          double &hy) {
+template <class T>
+__device__ __forceinline__ void plan_nbrs(double V, const T *phi, const int4 &c, int nc, int ncg,
+                                          bool mem, T &lx, T &hx, T &ly, T &hy) {
   const int g = c.x, i = c.w & 255, j = (c.w >> 8) & 255;
-  const double dlx = phi[g - 1], dhx = phi[g + 1], dly = phi[g - ncg], dhy = phi[g + ncg];
+  const T dlx = phi[g - 1], dhx = phi[g + 1], dly = phi[g - ncg], dhy = phi[g + ncg];
   if (mem) {
     lx = dlx;
     hx = dhx;
@@ -1008,11 +1062,9 @@ __device__ __forceinline__ void plan_nbrs(const RunDev &R, const double *phi, co
     hy = dhy;
     return;
   }
-  const double vo = phi[g], x0 = phi[c.y], y0 = phi[c.z];
-  const double gx = ghost_eval(x0, (c.w >> 16) & 3, vo, i == 1 ? dhx : dlx, (j & 1) ? dhy : dly,
-                               R.applied_voltage);
-  const double gy = ghost_eval(y0, (c.w >> 18) & 3, vo, j == 1 ? dhy : dly, (i & 1) ? dhx : dlx,
-                               R.applied_voltage);
+  const T vo = phi[g], x0 = phi[c.y], y0 = phi[c.z];
+  const T gx = ghost_eval(x0, (c.w >> 16) & 3, vo, i == 1 ? dhx : dlx, (j & 1) ? dhy : dly, V);
+  const T gy = ghost_eval(y0, (c.w >> 18) & 3, vo, j == 1 ? dhy : dly, (i & 1) ? dhx : dlx, V);
   lx = i > 1 ? dlx : gx;
   hx = i < nc ? dhx : gx;
   ly = j > 1 ? dly : gy;
@@ -1040,13 +1092,15 @@ struct LevelPlan {
   int item;  // cell index within each colour of the box (row-major, nc/2 per row)
 };
 
-__device__ __forceinline__ bool plan_fits(const MGV &M, const LvlInfo &L) {
+template <class T>
+__device__ __forceinline__ bool plan_fits(const MGV<T> &M, const LvlInfo &L) {
   return M.plans && L.nb * ((L.nc * L.nc) >> 1) <= NTHR;
 }
 
 // Forms the thread's two cell plans (colour p = (i + j) & 1). Each thread
 // reads only its own slots afterwards, so no barrier is needed.
-__device__ __forceinline__ LevelPlan make_level_plan(const MGV &M, const LvlInfo &L, bool cyl) {
+template <class T>
+__device__ __forceinline__ LevelPlan make_level_plan(const MGV<T> &M, const LvlInfo &L, bool cyl) {
   LevelPlan P;
   const int half = (L.nc * L.nc) >> 1, hsh = 2 * L.sh - 1, hn = L.nc >> 1;
   const int k = threadIdx.x;
@@ -1076,19 +1130,20 @@ __device__ __forceinline__ LevelPlan make_level_plan(const MGV &M, const LvlInfo
 }
 
 // One red-black half-sweep `it` from the cell plans (p_sweep).
-__device__ __forceinline__ void plan_sweep(const RunDev &R, const MGV &M, const LvlInfo &L,
+template <class T>
+__device__ __forceinline__ void plan_sweep(const RunDev &R, const MGV<T> &M, const LvlInfo &L,
                                            const LevelPlan &P, int it, bool mem) {
   const int4 c = plan_slots()[2 * threadIdx.x + (it & 1)];
   if (c.x >= 0) {
-    double *phi = M.phi;
-    double lx, hx, ly, hy;
-    plan_nbrs(R, phi, c, L.nc, L.ncg, mem, lx, hx, ly, hy);
-    const double r = M.rhs[c.x], dx2 = L.dr * L.dr;
+    T *phi = M.phi;
+    T lx, hx, ly, hy;
+    plan_nbrs(M.V, phi, c, L.nc, L.ncg, mem, lx, hx, ly, hy);
+    const T r = M.rhs[c.x], dx2 = T(L.dr * L.dr);
     if (R.coord == 1) {
       const double2 w = wts_slots()[2 * threadIdx.x + (it & 1)];
-      phi[c.x] = 0.25 * (w.x * lx + w.y * hx + hy + ly - dx2 * r);
+      phi[c.x] = T(0.25) * (T(w.x) * lx + T(w.y) * hx + hy + ly - dx2 * r);
     } else {
-      phi[c.x] = 0.25 * (hx + lx + hy + ly - dx2 * r);
+      phi[c.x] = T(0.25) * (hx + lx + hy + ly - dx2 * r);
     }
   }
   __syncthreads();
@@ -1100,42 +1155,43 @@ __device__ __forceinline__ void plan_sweep(const RunDev &R, const MGV &M, const 
 // (cells (2ii-1, 2jj-1) and (2ii, 2jj-1)) and that item + hn (cells
 // (2ii, 2jj) and (2ii-1, 2jj)), which are in the same warp; the first adds
 // the four in the order of box_rstr_lpl.
-__device__ __forceinline__ void plan_fr(const RunDev &R, const MGV &M, const LvlInfo &L,
+template <class T>
+__device__ __forceinline__ void plan_fr(const RunDev &R, const MGV<T> &M, const LvlInfo &L,
                                         const LevelPlan &P, int lvl) {
-  double *phi = M.phi, *tmp = M.tmp;
-  const double inv_dr_sq = 1 / (L.dr * L.dr);
-  double res[2] = {0, 0}, ph[2] = {0, 0};
+  T *phi = M.phi, *tmp = M.tmp;
+  const T inv_dr_sq = T(1 / (L.dr * L.dr));
+  T res[2] = {0, 0}, ph[2] = {0, 0};
 #pragma unroll
   for (int p = 0; p < 2; p++) {
     const int4 c = plan_slots()[2 * threadIdx.x + p];
     if (c.x < 0) continue;
-    double lx, hx, ly, hy;
-    plan_nbrs(R, phi, c, L.nc, L.ncg, false, lx, hx, ly, hy);
-    const double v = phi[c.x];
-    double lap;
+    T lx, hx, ly, hy;
+    plan_nbrs(M.V, phi, c, L.nc, L.ncg, false, lx, hx, ly, hy);
+    const T v = phi[c.x];
+    T lap;
     if (R.coord == 1) {
       const double2 w = wts_slots()[2 * threadIdx.x + p];
-      lap = (w.x * lx + w.y * hx + ly + hy - 4 * v) * inv_dr_sq;
+      lap = (T(w.x) * lx + T(w.y) * hx + ly + hy - T(4) * v) * inv_dr_sq;
     } else {
-      lap = inv_dr_sq * (lx + hx + ly + hy - 4 * v);
+      lap = inv_dr_sq * (lx + hx + ly + hy - T(4) * v);
     }
     res[p] = M.rhs[c.x] - lap;
     ph[p] = v;
   }
   const int hn = L.nc >> 1;
   // from the item one row up: its even cell (2ii, 2jj) and odd cell (2ii-1, 2jj)
-  const double r11 = __shfl_down_sync(0xffffffffu, res[0], hn);
-  const double r01 = __shfl_down_sync(0xffffffffu, res[1], hn);
-  const double p11 = __shfl_down_sync(0xffffffffu, ph[0], hn);
-  const double p01 = __shfl_down_sync(0xffffffffu, ph[1], hn);
+  const T r11 = __shfl_down_sync(0xffffffffu, res[0], hn);
+  const T r01 = __shfl_down_sync(0xffffffffu, res[1], hn);
+  const T p11 = __shfl_down_sync(0xffffffffu, ph[0], hn);
+  const T p01 = __shfl_down_sync(0xffffffffu, ph[1], hn);
   const int row = P.item >> (L.sh - 1);  // j - 1
   if (P.bx >= 0 && (row & 1) == 0) {
     const BoxRec &B = M.boxes[P.bx];
     const int ii = (P.item & (hn - 1)) + 1, jj = (row >> 1) + 1;
     const int pncg = R.lv_nc[lvl - 1 - R.min_lvl] + 2;
     const int d = B.pbase + (B.o0 + ii) + pncg * (B.o1 + jj);
-    tmp[d] = 0.25 * (res[0] + res[1] + r01 + r11);
-    phi[d] = 0.25 * (ph[0] + ph[1] + p01 + p11);
+    tmp[d] = T(0.25) * (res[0] + res[1] + r01 + r11);
+    phi[d] = T(0.25) * (ph[0] + ph[1] + p01 + p11);
   }
   fill_phi_loop(R, M, L, false);
   __syncthreads();
@@ -1145,17 +1201,18 @@ __device__ __forceinline__ void plan_fr(const RunDev &R, const MGV &M, const Lvl
 // Phases per level: down: 4 half-sweeps, residual/restriction (+ ghost fill),
 // coarse ghost fill + rhs; base: 2 n_cycle_base half-sweeps + ghost fill;
 // up: correction, 4 half-sweeps, ghost fill.
-__device__ void p_vcycle(const RunDev &R, const MGV &M, int max_lvl, bool stale_base) {
+template <class T>
+__device__ void p_vcycle(const RunDev &R, const MGV<T> &M, int max_lvl, bool stale_base) {
   const int min_lvl = R.min_lvl;
   for (int lvl = max_lvl; lvl >= min_lvl + 1; lvl--) {
     const LvlInfo L = lvl_info(R, lvl);
     if (plan_fits(M, L)) {
       const LevelPlan P = make_level_plan(M, L, R.coord == 1);
       #pragma unroll 1
-      for (int it = 1; it <= 4; it++) plan_sweep(R, M, L, P, it, false);
+      for (int it = 1; it <= M.sw_down; it++) plan_sweep(R, M, L, P, it, false);
       plan_fr(R, M, L, P, lvl);
     } else {
-      for (int it = 1; it <= 4; it++) p_sweep(R, M, lvl, it, false);
+      for (int it = 1; it <= M.sw_down; it++) p_sweep(R, M, lvl, it, false);
       p_fr(R, M, lvl, true, false, false);
     }
     p_fc(R, M, lvl - 1, true);
@@ -1165,9 +1222,9 @@ __device__ void p_vcycle(const RunDev &R, const MGV &M, int max_lvl, bool stale_
     if (plan_fits(M, L)) {
       const LevelPlan P = make_level_plan(M, L, R.coord == 1);
       #pragma unroll 1
-      for (int it = 1; it <= 2 * R.n_cycle_base; it++) plan_sweep(R, M, L, P, it, stale_base && it == 1);
+      for (int it = 1; it <= M.sw_base; it++) plan_sweep(R, M, L, P, it, stale_base && it == 1);
     } else {
-      for (int it = 1; it <= 2 * R.n_cycle_base; it++) p_sweep(R, M, min_lvl, it, stale_base && it == 1);
+      for (int it = 1; it <= M.sw_base; it++) p_sweep(R, M, min_lvl, it, stale_base && it == 1);
     }
   }
   p_fill(R, M, min_lvl);
@@ -1177,10 +1234,10 @@ __device__ void p_vcycle(const RunDev &R, const MGV &M, int max_lvl, bool stale_
       const LevelPlan P = make_level_plan(M, L, R.coord == 1);
       p_correct(R, M, lvl, false, true);
       #pragma unroll 1
-      for (int it = 1; it <= 4; it++) plan_sweep(R, M, L, P, it, false);
+      for (int it = 1; it <= M.sw_up; it++) plan_sweep(R, M, L, P, it, false);
     } else {
       p_correct(R, M, lvl, false, true);
-      for (int it = 1; it <= 4; it++) p_sweep(R, M, lvl, it, false);
+      for (int it = 1; it <= M.sw_up; it++) p_sweep(R, M, lvl, it, false);
     }
     p_fill(R, M, lvl);
   }
@@ -1188,7 +1245,8 @@ __device__ void p_vcycle(const RunDev &R, const MGV &M, int max_lvl, bool stale_
 
 // mg$D_fas_fmg, m_aX_mg.f90:163-202. leaf_rhs: compute the space charge of
 // the leaves where it is first needed (compute_fld).
-__device__ void p_fmg_in(const RunDev &R, const MGV &M, bool set_residual, bool first_call,
+template <class T>
+__device__ void p_fmg_in(const RunDev &R, const MGV<T> &M, bool set_residual, bool first_call,
                          bool leaf_rhs) {
   const int min_lvl = R.min_lvl, max_lvl = R.max_lvl;
   if (first_call) {
@@ -1209,9 +1267,10 @@ __device__ void p_fmg_in(const RunDev &R, const MGV &M, bool set_residual, bool 
 
 // Copy the multigrid variables of every box between device memory and the
 // compact shared-memory arrays (in: to shared memory).
-__device__ void stage_mg(const RunDev &R, const MGV &M, bool in) {
-  double *g[3] = {VAR(R, MP), VAR(R, MR), VAR(R, MT)};
-  double *s[3] = {M.phi, M.rhs, M.tmp};
+template <class T>
+__device__ void stage_mg(const RunDev &R, const MGV<T> &M, T *g0, T *g1, T *g2, bool in) {
+  T *g[3] = {g0, g1, g2};
+  T *s[3] = {M.phi, M.rhs, M.tmp};
   for (int lvl = R.min_lvl; lvl <= R.max_lvl; lvl++) {
     const int li = lvl - R.min_lvl;
     const int ncg = R.lv_nc[li] + 2, per = ncg * ncg;
@@ -1245,16 +1304,148 @@ __device__ void p_fmg(const RunDev &R, bool set_residual, bool first_call, bool 
       for (int k = threadIdx.x; k < npb; k += NTHR) spb[k] = R.pbx[k];
     }
     __syncthreads();
-    MGV M{base, base + S, base + 2 * S, sb, spb, true};
-    stage_mg(R, M, true);
+    MGV<double> M{base, base + S, base + 2 * S, sb, spb, true, R.applied_voltage,
+                  4, 4, 2 * R.n_cycle_base};
+    stage_mg(R, M, VAR(R, MP), VAR(R, MR), VAR(R, MT), true);
     p_fmg_in(R, M, set_residual, first_call, leaf_rhs);
-    stage_mg(R, M, false);
+    stage_mg(R, M, VAR(R, MP), VAR(R, MR), VAR(R, MT), false);
   } else {
-    MGV M{VAR(R, MP), VAR(R, MR), VAR(R, MT), R.boxes, R.pbx, false};
+    MGV<double> M{VAR(R, MP), VAR(R, MR), VAR(R, MT), R.boxes, R.pbx, false, R.applied_voltage,
+                  4, 4, 2 * R.n_cycle_base};
     p_fmg_in(R, M, set_residual, first_call, leaf_rhs);
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// Mixed-precision field solve: defect correction around an FP32 multigrid.
+// One pass is
+//  1. FP64, levels max..min (p_mx_residual): on leaf cells the space charge
+//     rhs = e/eps0 (n_e - n_i) and the residual r = rhs - A phi of the FP64
+//     potential, ghost neighbours evaluated from their recipes (as p_fr); on
+//     parent cells the restriction of the children's r. phi and rhs are
+//     restricted into the parents as update_coarse does (box_rstr_lpl,
+//     afivo/src/m_aX_mg.f90:683-705). The correction c starts at 0.
+//  2. FP32: multigrid on A c = r with homogeneous wall values (V = 0), either
+//     the reference's FMG schedule (mg$D_fas_fmg, :163-202) or a single
+//     V-cycle over all levels (mg$D_fas_vcycle, :208-254), with the half-sweep
+//     counts of the run's schedule.
+//  3. FP64 (p_mx_accumulate): phi += c on every cell of every level, then the
+//     ghost cells of phi level by level (fill_gc_phi, :303-316).
+// The correction equation is linear and the ghost recipes are affine in the
+// potential, so this is one FAS cycle on phi whose smoothing runs in FP32,
+// while the residual (which cancels) and the accumulation stay in FP64.
+
+__device__ __noinline__ void p_mx_residual(const RunDev &R, const MGV<float> &M, int lvl) {
+  const LvlInfo L = lvl_info(R, lvl);
+  const bool down = lvl > R.min_lvl;
+  const int pncg = down ? R.lv_nc[lvl - 1 - R.min_lvl] + 2 : 0;
+  double *phi = VAR(R, I_PHI), *rhs = VAR(R, I_RHS);
+  const double *e = VAR(R, I_ELEC), *pi = VAR(R, I_PION);
+  float *ce = M.phi, *cr = M.rhs, *ct = M.tmp;
+  const double inv_dr_sq = 1 / (L.dr * L.dr);
+  const double fac = UC_ELEM_CHARGE / UC_EPS0;
+  const int hn = L.nc >> 1, per = hn * hn, n = L.nb * per;
+  for (int k = threadIdx.x; k < n; k += NTHR) {
+    const int b = L.b0 + k / per;
+    const BoxRec &B = R.boxes[b];  // device-memory slots (phi, rhs, densities)
+    const BoxRec &S = M.boxes[b];  // slots of the FP32 arrays
+    const int t = k % per, ii = t % hn + 1, jj = t / hn + 1;
+    const bool leaf = (B.flags & CF_LEAF) != 0;
+    double rs[4], ps[4], hs[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int i = 2 * ii - 1 + (q & 1), j = 2 * jj - 1 + (q >> 1);
+      const int loc = i + L.ncg * j, g = B.base + loc, sc = S.base + loc;
+      double rh, res;
+      if (leaf) {
+        rh = fac * (e[g] - pi[g]);
+        rhs[g] = rh;
+        res = rh - lap_at(R, R.applied_voltage, (const double *)phi, B, L.nc, L.ncg, i, j, inv_dr_sq);
+        cr[sc] = (float)res;
+      } else {
+        rh = rhs[g];
+        res = (double)cr[sc];
+      }
+      ce[sc] = 0.0f;
+      ct[sc] = 0.0f;
+      rs[q] = res;
+      ps[q] = phi[g];
+      hs[q] = rh;
+    }
+    if (down) {
+      const int o = (B.o0 + ii) + pncg * (B.o1 + jj);
+      cr[S.pbase + o] = (float)(0.25 * (rs[0] + rs[1] + rs[2] + rs[3]));
+      phi[B.pbase + o] = 0.25 * (ps[0] + ps[1] + ps[2] + ps[3]);
+      rhs[B.pbase + o] = 0.25 * (hs[0] + hs[1] + hs[2] + hs[3]);
+    }
+  }
+  // side ghosts of c and of its tmp start at zero (consistent with c = 0 and V = 0)
+  const int pg = 4 * L.nc, ng = L.nb * pg;
+  for (int k = threadIdx.x; k < ng; k += NTHR) {
+    const BoxRec &S = M.boxes[L.b0 + k / pg];
+    const int r = k % pg, side = r >> L.sh, kk = (r & (L.nc - 1)) + 1;
+    const int dim = side >> 1, gx = (side & 1) ? L.nc + 1 : 0;
+    const int d = S.base + (dim == 0 ? gx + L.ncg * kk : kk + L.ncg * gx);
+    ce[d] = 0.0f;
+    ct[d] = 0.0f;
+  }
+  __syncthreads();
+}
+
+__device__ void p_mx_accumulate(const RunDev &R, const MGV<float> &M) {
+  double *phi = VAR(R, I_PHI);
+  for (int lvl = R.min_lvl; lvl <= R.max_lvl; lvl++) {
+    const LvlInfo L = lvl_info(R, lvl);
+    const int per = L.nc * L.nc, n = L.nb * per;
+    for (int k = threadIdx.x; k < n; k += NTHR) {
+      const int b = L.b0 + (k >> (2 * L.sh));
+      const int t = k & (per - 1), i = (t & (L.nc - 1)) + 1, j = (t >> L.sh) + 1;
+      const int loc = i + L.ncg * j;
+      phi[R.boxes[b].base + loc] += (double)M.phi[M.boxes[b].base + loc];
+    }
+  }
+  __syncthreads();
+  const MGV<double> G{phi, VAR(R, MR), VAR(R, MT), R.boxes, R.pbx, false, R.applied_voltage, 0, 0, 0};
+  for (int lvl = R.min_lvl; lvl <= R.max_lvl; lvl++) p_fill(R, G, lvl);
+}
+
+// The mixed-precision solve of compute_fld (see above): the FP32 arrays are
+// in shared memory when the tree fits (mx_smem floats per variable), else in
+// the run's FP32 storage cc32.
+__device__ void p_solve_mixed(const RunDev &R) {
+  MGV<float> M;
+  if (R.mx_smem > 0) {
+    const int S = R.mx_smem, nbx = R.bx_off[R.nlev], npb = R.pb_off[R.nlev];
+    float *base = reinterpret_cast<float *>(g_dsmem + PLAN_DOUBLES + (R.coord == 1 ? WTS_DOUBLES : 0));
+    BoxRec *sb = reinterpret_cast<BoxRec *>(base + 3 * S);
+    int *spb = reinterpret_cast<int *>(sb + nbx);
+    const int4 *src = reinterpret_cast<const int4 *>(R.sboxes);
+    int4 *dst = reinterpret_cast<int4 *>(sb);
+    const int n4 = nbx * (int)(sizeof(BoxRec) / sizeof(int4));
+    for (int k = threadIdx.x; k < n4; k += NTHR) dst[k] = src[k];
+    for (int k = threadIdx.x; k < npb; k += NTHR) spb[k] = R.pbx[k];
+    __syncthreads();
+    M = MGV<float>{base, base + S, base + 2 * S, sb, spb, true, 0.0, R.mx_sw_down, R.mx_sw_up,
+                   R.mx_sw_base};
+  } else {
+    const size_t n = (size_t)R.capacity * SLOT;
+    M = MGV<float>{R.cc32, R.cc32 + n, R.cc32 + 2 * n, R.boxes, R.pbx, false, 0.0, R.mx_sw_down,
+                   R.mx_sw_up, R.mx_sw_base};
+  }
+  for (int pass = 0; pass < R.mx_n_corr; pass++) {
+    for (int lvl = R.max_lvl; lvl >= R.min_lvl; lvl--) p_mx_residual(R, M, lvl);
+    if (R.mx_fmg) {
+      for (int lvl = R.min_lvl; lvl <= R.max_lvl; lvl++) {
+        p_correct(R, M, lvl, true, lvl > R.min_lvl);
+        p_vcycle(R, M, lvl, false);
+      }
+    } else {
+      p_vcycle(R, M, R.max_lvl, false);
+    }
+    p_mx_accumulate(R, M);
+  }
+}
 // a$D_gc_tree(iv, a$D_gc_interp[_lim], a$D_gc_neumann) for one or two
 // variables, levels ascending (m_aX_gc.f90:28-46, 90-330)
 __device__ void p_gc_den(const RunDev &R, int iv0, int iv1, bool lim) {
@@ -1367,6 +1558,11 @@ __device__ void p_fld_from_pot(const RunDev &R) {
 // compute_fld, src/streamer_2d.f90:307-343 (one FMG cycle)
 __device__ void p_compute_fld(const RunDev &R, bool no_guess) {
   p_fmg(R, false, no_guess, true);
+  p_fld_from_pot(R);
+}
+// compute_fld of the mixed form: defect-correction solve, FP64 field
+__device__ void p_compute_fld_mixed(const RunDev &R) {
+  p_solve_mixed(R);
   p_fld_from_pot(R);
 }
 
@@ -1705,7 +1901,7 @@ __device__ void ph_source(const RunDev &R, double dt, bool has_dt) {
       if (t >= nc * nc) return;
       const int c = (t % nc + 1) + ncg * (t / nc + 1);
       const double fld = CC(R, I_FLD, id)[c];
-      const Loc loc = get_loc(R, fld);
+      const Loc<double> loc = get_loc(R, fld);
       const double alpha = col_at(R, C_ALPHA, loc);
       const double mobility = col_at(R, C_MOB, loc);
       double tmp = fld * mobility * alpha * CC(R, I_ELEC, id)[c] * R.ph_coeff;
@@ -1996,7 +2192,12 @@ __device__ void ph_deposit(const RunDev &R) {
 }
 
 // One full time step, src/streamer_2d.f90:99-127; with deposit, the photon
-// source term of this step's photoionization first (src/streamer_cyl.f90:95-97)
+// source term of this step's photoionization first (src/streamer_cyl.f90:95-97).
+// MIXED: the mixed-precision form -- FP32 fluxes, source update and lookups,
+// field solves by defect correction around an FP32 multigrid (p_solve_mixed);
+// densities, the space charge, the potential, the field and the step size
+// stay in FP64.
+template <bool MIXED>
 __device__ void step(const RunDev &R, double dt, bool deposit) {
   if (deposit) ph_deposit(R);
   {
@@ -2009,27 +2210,32 @@ __device__ void step(const RunDev &R, double dt, bool deposit) {
     }
     __syncthreads();
   }
+  using T = typename std::conditional<MIXED, float, double>::type;
   for (int stage = 1; stage <= 2; stage++) {
-    fluxes_koren(R, dt);
+    fluxes_koren<T>(R, dt);
     __syncthreads();
     consistent_fluxes(R);
     __syncthreads();
-    update_solution(R, dt);
+    update_solution<T>(R, dt);
     __syncthreads();
     p_restrict(R, I_ELEC, I_PION);
     p_gc_den(R, I_ELEC, I_PION, true);
-    if (stage == 1) p_compute_fld(R, false);
+    if (stage == 1) {
+      if (MIXED) p_compute_fld_mixed(R);
+      else p_compute_fld(R, false);
+    }
   }
   average_dens(R);
-  p_compute_fld(R, false);
+  if (MIXED) p_compute_fld_mixed(R);
+  else p_compute_fld(R, false);
 }
 
 __device__ void run_op(const RunDev &R, const Op &op) {
   switch (op.code) {
     case OP_COPY: copy_var(R, op.i0, op.i1); break;
-    case OP_FLUXES: fluxes_koren(R, op.d0); __syncthreads(); break;
+    case OP_FLUXES: fluxes_koren<double>(R, op.d0); __syncthreads(); break;
     case OP_CONSISTENT: consistent_fluxes(R); __syncthreads(); break;
-    case OP_UPDATE: update_solution(R, op.d0); __syncthreads(); break;
+    case OP_UPDATE: update_solution<double>(R, op.d0); __syncthreads(); break;
     case OP_RESTRICT: p_restrict(R, op.i0, -1); break;
     case OP_GC: p_gc_den(R, op.i0, -1, op.i1 == GC_LIM); break;
     case OP_AVERAGE: average_dens(R); break;
@@ -2039,7 +2245,9 @@ __device__ void run_op(const RunDev &R, const Op &op) {
     case OP_DT_RED: dt_reductions(R); break;
     case OP_REF_FLAGS: ref_flags(R, op.d0); break;
     case OP_PROLONG_NEW: prolong_new(R); break;
-    case OP_STEP: step(R, op.d0, op.i0 != 0); break;
+    case OP_STEP: step<false>(R, op.d0, op.i0 != 0); break;
+    case OP_STEP_MIXED: step<true>(R, op.d0, op.i0 != 0); break;
+    case OP_COMPUTE_FLD_MIXED: p_compute_fld_mixed(R); break;
     case OP_PH_SOURCE: ph_source(R, op.d0, op.i0 != 0); break;
     case OP_PH_DEPOSIT: ph_deposit(R); break;
     case OP_NOP: break;
@@ -2072,7 +2280,20 @@ __global__ void __launch_bounds__(NTHR, 1) a5g_step_kernel(const RunDev *run, do
     for (int k = threadIdx.x; k < (int)(sizeof(RunDev) / sizeof(int)); k += NTHR) d[k] = s[k];
   }
   __syncthreads();
-  step(sR, dt, deposit != 0);
+  step<false>(sR, dt, deposit != 0);
+}
+
+// One full time step of one run in the mixed-precision form.
+__global__ void __launch_bounds__(NTHR, 1) a5g_step_mixed_kernel(const RunDev *run, double dt,
+                                                                 int deposit) {
+  __shared__ RunDev sR;
+  {
+    const int *s = reinterpret_cast<const int *>(run);
+    int *d = reinterpret_cast<int *>(&sR);
+    for (int k = threadIdx.x; k < (int)(sizeof(RunDev) / sizeof(int)); k += NTHR) d[k] = s[k];
+  }
+  __syncthreads();
+  step<true>(sR, dt, deposit != 0);
 }
 
 // Descriptor of one member of a launch of a5g_step_batch_static.
@@ -2289,7 +2510,32 @@ struct a5g_ctx {
   PhBox *ph_boxes = nullptr;
   int ph_capacity = 0;   // capacity the per-box photon buffers are sized for
   size_t ph_boxes_cap = 0;
+  // mixed precision
+  int precision = 0;     // A5G_FP64 or A5G_MIXED
+  a5g_mg_schedule sched{};
+  float *tbl32 = nullptr;
+  float *cc32 = nullptr;
+  int cc32_cap = 0;      // box capacity cc32 is sized for
+  int mx_smem_fit = 0;   // floats per variable of the shared-memory copy (0: does not fit)
+  size_t dyn_smem32 = 0; // dynamic shared memory of a mixed-precision launch
+  // shared-memory staging of the multigrid (a5g_debug_set_staging can turn it off)
+  bool allow_smem = true;
+  int fit64 = 0, fit32 = 0;       // per-variable sizes when the tree fits, else 0
+  size_t need64 = 0, need32 = 0;  // dynamic shared memory the staged solves take
 };
+
+// Shared-memory staging of the multigrid variables as allowed and as fits.
+static void apply_staging(a5g_ctx *c) {
+  const bool on = c->allow_smem;
+  c->h.smem_doubles = on ? c->fit64 : 0;
+  c->dyn_smem = on && c->fit64 ? c->need64 : 0;
+  c->mx_smem_fit = on ? c->fit32 : 0;
+  c->dyn_smem32 = on && c->fit32 ? c->need32 : 0;
+  c->h.mx_smem = c->mx_smem_fit;
+}
+
+// Dynamic shared memory a step of this context's precision needs.
+static size_t step_smem(const a5g_ctx *c) { return c->precision == A5G_MIXED ? c->dyn_smem32 : c->dyn_smem; }
 
 // ---------------------------------------------------------------------------
 // Plan builder: one BoxRec per box, level by level in list order, and the
@@ -2458,15 +2704,17 @@ static size_t dyn_smem_limit() {
     int optin = 0;
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     size_t stat = 0;
-    cudaFuncAttributes fa[4];
-    const void *fns[4] = {(const void *)a5g_run_kernel, (const void *)a5g_step_kernel,
-                          (const void *)a5g_run_kernel_slots, (const void *)a5g_photon_kernel};
-    for (int k = 0; k < 4; k++)
+    constexpr int NF = 5;
+    cudaFuncAttributes fa[NF];
+    const void *fns[NF] = {(const void *)a5g_run_kernel, (const void *)a5g_step_kernel,
+                           (const void *)a5g_run_kernel_slots, (const void *)a5g_photon_kernel,
+                           (const void *)a5g_step_mixed_kernel};
+    for (int k = 0; k < NF; k++)
       if (cudaFuncGetAttributes(&fa[k], fns[k]) == cudaSuccess)
         stat = std::max(stat, fa[k].sharedSizeBytes);
     size_t avail = optin > (int)stat ? (size_t)optin - stat : 0;
     bool ok = true;
-    for (int k = 0; k < 4; k++)
+    for (int k = 0; k < NF; k++)
       ok = ok && cudaFuncSetAttribute(fns[k], cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)avail) == cudaSuccess;
     lim[dev] = ok ? avail : 0;
@@ -2501,14 +2749,15 @@ static Op mkop(int code, int i0 = 0, int i1 = 0, double d0 = 0) {
   return o;
 }
 
-static int launch(a5g_ctx *c, const Op &op) {
+static int launch_smem(a5g_ctx *c, const Op &op, size_t smem) {
   if (!c) return fail(A5G_EINVAL, "null context");
   if (!c->has_tree) return fail(A5G_ESTATE, "no tree uploaded");
   if (!c->has_table) return fail(A5G_ESTATE, "no transport table set");
-  a5g_run_kernel<<<1, NTHR, c->dyn_smem, c->stream>>>(c->d_run, op, nullptr, nullptr);
+  a5g_run_kernel<<<1, NTHR, smem, c->stream>>>(c->d_run, op, nullptr, nullptr);
   CK(cudaGetLastError());
   return A5G_OK;
 }
+static int launch(a5g_ctx *c, const Op &op) { return launch_smem(c, op, c ? c->dyn_smem : 0); }
 
 // Jumps of 2^b draws of the master generator (see mz_advance): the 3x3
 // matrix of (s1, s2, s3) -> (s2, s3, s1 - s3) mod m and the affine map
@@ -2650,6 +2899,10 @@ int a5g_create(const a5g_params *p, a5g_ctx **out) {
   }
   h.scal = c->scal;
   h.status = c->status;
+  h.mx_fmg = 1;
+  h.mx_sw_down = h.mx_sw_up = 4;
+  h.mx_sw_base = 2 * p->n_cycle_base;
+  h.mx_n_corr = 1;
   if (p->photoi_enabled) {
     MzJump J[MZ_NJUMP];
     mz_jump_table(J);
@@ -2701,6 +2954,8 @@ int a5g_destroy(a5g_ctx *c) {
   cudaFree(c->ph_scal);
   cudaFree(c->ph_jump);
   cudaFree(c->ph_boxes);
+  cudaFree(c->tbl32);
+  cudaFree(c->cc32);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return A5G_OK;
@@ -2721,12 +2976,68 @@ int a5g_set_table(a5g_ctx *c, int n_rows, int n_cols, double x_min, double inv_d
   c->tbl_cols = n_cols;
   c->tbl_xmin = x_min;
   c->tbl_inv_dx = inv_dx;
+  {
+    // FP32 copy for the lookups of the mixed form
+    std::vector<float> t32((size_t)n_rows * n_cols);
+    for (size_t k = 0; k < t32.size(); k++) t32[k] = (float)rows_cols[k];
+    cudaFree(c->tbl32);
+    c->tbl32 = nullptr;
+    CK(cudaMalloc(&c->tbl32, sizeof(float) * t32.size()));
+    CK(cudaMemcpyAsync(c->tbl32, t32.data(), sizeof(float) * t32.size(), cudaMemcpyHostToDevice,
+                       c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  }
   c->h.tbl = c->tbl;
+  c->h.tbl32 = c->tbl32;
   c->h.tbl_rows = n_rows;
   c->h.tbl_xmin = x_min;
   c->h.tbl_inv_dx = inv_dx;
   c->has_table = true;
   return push_run(c);
+}
+
+// FP32 storage of the correction solve when the tree does not fit in shared
+// memory (sized to the box capacity; its contents are scratch).
+static int mx_ready(a5g_ctx *c) {
+  if (c->precision != A5G_MIXED || c->mx_smem_fit > 0 || c->cc32_cap >= c->capacity) return A5G_OK;
+  cudaFree(c->cc32);
+  c->cc32 = nullptr;
+  c->cc32_cap = 0;
+  CK(cudaMalloc(&c->cc32, (size_t)3 * c->capacity * SLOT * sizeof(float)));
+  c->cc32_cap = c->capacity;
+  c->h.cc32 = c->cc32;
+  return push_run(c);
+}
+
+int a5g_set_precision(a5g_ctx *c, int precision, const a5g_mg_schedule *sched) {
+  if (!c) return fail(A5G_EINVAL, "null context");
+  if (precision != A5G_FP64 && precision != A5G_MIXED)
+    return fail(A5G_EINVAL, "precision must be A5G_FP64 or A5G_MIXED");
+  a5g_mg_schedule s{1, 2, 2, c->p.n_cycle_base, 1};
+  if (sched) s = *sched;
+  if (s.fmg != 0 && s.fmg != 1) return fail(A5G_EINVAL, "schedule: fmg must be 0 or 1");
+  if (s.n_cycle_down < 1 || s.n_cycle_down > 8 || s.n_cycle_up < 1 || s.n_cycle_up > 8 ||
+      s.n_cycle_base < 1 || s.n_cycle_base > 64 || s.n_corr < 1 || s.n_corr > 8)
+    return fail(A5G_EINVAL, "schedule: cycles down/up 1..8, base 1..64, corrections 1..8");
+  c->precision = precision;
+  c->sched = s;
+  RunDev &h = c->h;
+  h.mx_enabled = precision == A5G_MIXED;
+  h.mx_fmg = s.fmg;
+  h.mx_sw_down = 2 * s.n_cycle_down;
+  h.mx_sw_up = 2 * s.n_cycle_up;
+  h.mx_sw_base = 2 * s.n_cycle_base;
+  h.mx_n_corr = s.n_corr;
+  int r = push_run(c);
+  if (r) return r;
+  return mx_ready(c);
+}
+
+int a5g_get_precision(a5g_ctx *c, int *precision, a5g_mg_schedule *sched) {
+  if (!c) return fail(A5G_EINVAL, "null context");
+  if (precision) *precision = c->precision;
+  if (sched) *sched = c->precision == A5G_MIXED ? c->sched : a5g_mg_schedule{1, 2, 2, c->p.n_cycle_base, 1};
+  return A5G_OK;
 }
 
 int a5g_set_photon_table(a5g_ctx *c, int n_rows, double x_min, double inv_dx, const double *dist,
@@ -2834,6 +3145,12 @@ static int grow(a5g_ctx *c, int need) {
   c->capacity = cap;
   c->h.capacity = cap;
   c->h.cc = ncc; c->h.fx = nfx; c->h.fy = nfy; c->h.meta = nmeta; c->h.flags = nflags;
+  if (c->cc32) {  // scratch of the mixed form: reallocated at the next mixed launch
+    cudaFree(c->cc32);
+    c->cc32 = nullptr;
+    c->cc32_cap = 0;
+    c->h.cc32 = nullptr;
+  }
   return ph_resize(c);
 }
 
@@ -2938,8 +3255,16 @@ int a5g_upload_tree(a5g_ctx *c, int max_id, int min_lvl, int max_lvl, const int 
                         3 * (size_t)P.smem_doubles * sizeof(double) +
                         P.boxes.size() * sizeof(BoxRec) + P.pbx.size() * sizeof(int);
     const size_t limit = dyn_smem_limit();
-    h.smem_doubles = need <= limit ? P.smem_doubles : 0;
-    c->dyn_smem = h.smem_doubles ? need : 0;
+    c->fit64 = need <= limit ? P.smem_doubles : 0;
+    c->need64 = need;
+    // the FP32 correction solve of the mixed form: three float arrays
+    const int s32 = (P.smem_doubles + 3) & ~3;
+    const size_t need32 = (PLAN_DOUBLES + (c->p.coord == 1 ? WTS_DOUBLES : 0)) * sizeof(double) +
+                          3 * (size_t)s32 * sizeof(float) + P.boxes.size() * sizeof(BoxRec) +
+                          P.pbx.size() * sizeof(int);
+    c->fit32 = need32 <= limit ? s32 : 0;
+    c->need32 = need32;
+    apply_staging(c);
   }
   h.sboxes = c->p_sboxes;
   std::memcpy(h.bx_off, P.bx_off, sizeof(P.bx_off));
@@ -3050,7 +3375,14 @@ int a5g_gc_tree(a5g_ctx *c, int iv, int rb_kind) {
   return launch(c, mkop(OP_GC, iv, rb_kind == 0 ? GC_LIM : GC_INTERP));
 }
 int a5g_average_dens(a5g_ctx *c) { return launch(c, mkop(OP_AVERAGE)); }
-int a5g_compute_fld(a5g_ctx *c, int no_guess) { return launch(c, mkop(OP_COMPUTE_FLD, no_guess ? 1 : 0)); }
+int a5g_compute_fld(a5g_ctx *c, int no_guess) {
+  if (c && c->precision == A5G_MIXED && !no_guess) {
+    int r = mx_ready(c);
+    if (r) return r;
+    return launch_smem(c, mkop(OP_COMPUTE_FLD_MIXED), c->dyn_smem32);
+  }
+  return launch(c, mkop(OP_COMPUTE_FLD, no_guess ? 1 : 0));
+}
 int a5g_fas_fmg(a5g_ctx *c, int set_residual, int first_call) {
   return launch(c, mkop(OP_FMG, set_residual ? 1 : 0, first_call ? 1 : 0));
 }
@@ -3169,7 +3501,13 @@ int a5g_step(a5g_ctx *c, double dt) {
     if ((r = ph_launch_source_absorb(c, dt, 1))) return r;
     deposit = 1;
   }
-  a5g_step_kernel<<<1, NTHR, c->dyn_smem, c->stream>>>(c->d_run, dt, deposit);
+  if (c->precision == A5G_MIXED) {
+    int r = mx_ready(c);
+    if (r) return r;
+    a5g_step_mixed_kernel<<<1, NTHR, c->dyn_smem32, c->stream>>>(c->d_run, dt, deposit);
+  } else {
+    a5g_step_kernel<<<1, NTHR, c->dyn_smem, c->stream>>>(c->d_run, dt, deposit);
+  }
   CK(cudaGetLastError());
   return A5G_OK;
 }
@@ -3197,7 +3535,11 @@ int a5g_step_batch(a5g_ctx **ctxs, int n, const double *dts) {
       max_team = std::max(max_team, ctxs[k]->p.photoi_team);
       ph_smem = std::max(ph_smem, ph_smem_bytes(ctxs[k]));
     }
-    ops[k] = mkop(OP_STEP, ph ? 1 : 0, 0, dts[k]);
+    if (ctxs[k]->precision == A5G_MIXED) {
+      int r = mx_ready(ctxs[k]);
+      if (r) return r;
+    }
+    ops[k] = mkop(ctxs[k]->precision == A5G_MIXED ? OP_STEP_MIXED : OP_STEP, ph ? 1 : 0, 0, dts[k]);
     ops[n + k] = ph ? mkop(OP_PH_SOURCE, 1, 0, dts[k]) : mkop(OP_NOP);
   }
   // other members' queued work must finish before the batch runs on c0's stream
@@ -3209,7 +3551,7 @@ int a5g_step_batch(a5g_ctx **ctxs, int n, const double *dts) {
   CK(cudaMemcpyAsync(d_rp, rp.data(), n * sizeof(void *), cudaMemcpyHostToDevice, c0->stream));
   CK(cudaMemcpyAsync(d_ops, ops.data(), 2 * n * sizeof(Op), cudaMemcpyHostToDevice, c0->stream));
   size_t dyn = 0;
-  for (int k = 0; k < n; k++) dyn = std::max(dyn, ctxs[k]->dyn_smem);
+  for (int k = 0; k < n; k++) dyn = std::max(dyn, std::max(ctxs[k]->dyn_smem, step_smem(ctxs[k])));
   if (any_ph) {
     // photon sources of every member with photoionization (the others run
     // an operation that does nothing here), then the absorption
@@ -3265,7 +3607,11 @@ int a5g_step_batch_static(a5g_ctx **ctxs, int n, const double *dts) {
   bool any_ph = false;
   int max_team = 0;
   for (int k = 0; k < n; k++) {
-    dyn = std::max(dyn, ctxs[k]->dyn_smem);
+    dyn = std::max(dyn, std::max(ctxs[k]->dyn_smem, step_smem(ctxs[k])));
+    if (ctxs[k]->precision == A5G_MIXED) {
+      int r = mx_ready(ctxs[k]);
+      if (r) return r;
+    }
     if (ctxs[k]->p.photoi_enabled) {
       int r = ph_ready(ctxs[k]);
       if (r) return r;
@@ -3292,7 +3638,8 @@ int a5g_step_batch_static(a5g_ctx **ctxs, int n, const double *dts) {
   }
   for (int k = 0; k < n; k++) {
     g_static_host[k].run = ctxs[k]->d_run;
-    g_static_host[k].op = mkop(OP_STEP, ctxs[k]->p.photoi_enabled ? 1 : 0, 0, dts[k]);
+    g_static_host[k].op = mkop(ctxs[k]->precision == A5G_MIXED ? OP_STEP_MIXED : OP_STEP,
+                               ctxs[k]->p.photoi_enabled ? 1 : 0, 0, dts[k]);
   }
   // pageable source: the copy is staged before the call returns
   CK(cudaMemcpyAsync(g_static_dev[dev], g_static_host, (size_t)n * sizeof(BatchSlot),
@@ -3300,6 +3647,19 @@ int a5g_step_batch_static(a5g_ctx **ctxs, int n, const double *dts) {
   a5g_run_kernel_slots<<<n, NTHR, dyn, c0->stream>>>(g_static_dev[dev]);
   CK(cudaGetLastError());
   return A5G_OK;
+}
+
+// Diagnostics: allow (1) or forbid (0) the shared-memory staging of the
+// multigrid, so that tests can run the device-memory path of the solves on
+// trees that fit. Not part of the public interface.
+extern "C" int a5g_debug_set_staging(a5g_ctx *c, int allow_smem) {
+  if (!c) return fail(A5G_EINVAL, "null context");
+  CK(cudaStreamSynchronize(c->stream));
+  c->allow_smem = allow_smem != 0;
+  apply_staging(c);
+  int r = push_run(c);
+  if (r) return r;
+  return mx_ready(c);
 }
 
 int a5g_sync(a5g_ctx *c) {

@@ -197,6 +197,23 @@ class DeviceRun:
     def step(self, dt: float):
         call("a5g_step", self.h, dt)
 
+    def set_precision(self, mixed: bool, schedule=None):
+        """Plain FP64 (the reference's arithmetic) or the mixed form: FP32
+        fluxes, lookups and multigrid smoothing inside an FP64 defect
+        correction. schedule: (fmg, n_cycle_down, n_cycle_up, n_cycle_base,
+        n_corr) of the FP32 solve; None keeps the reference's schedule."""
+        sp = None
+        if schedule is not None:
+            sp = ctypes.byref(_lib.MGSchedule(*[int(v) for v in schedule]))
+        call("a5g_set_precision", self.h, _lib.A5G_MIXED if mixed else _lib.A5G_FP64, sp)
+
+    def precision(self):
+        """(mixed?, schedule tuple)"""
+        p, s = ctypes.c_int(0), _lib.MGSchedule()
+        call("a5g_get_precision", self.h, ctypes.byref(p), ctypes.byref(s))
+        return p.value == _lib.A5G_MIXED, (s.fmg, s.n_cycle_down, s.n_cycle_up, s.n_cycle_base,
+                                            s.n_corr)
+
     def set_photon_table(self, dist: np.ndarray, frac_in_tbl: float, x_min: float = 0.0,
                          inv_dx: float | None = None):
         d = np.ascontiguousarray(dist, dtype=np.float64)
@@ -243,3 +260,29 @@ def step_batch(runs: Sequence[DeviceRun], dts: Sequence[float]):
     arr = (ctypes.c_void_p * n)(*[r.h.value for r in runs])
     d = np.ascontiguousarray(dts, dtype=np.float64)
     call("a5g_step_batch", arr, n, _dp(d))
+
+
+def clone_state(sim, mixed: bool = False, schedule=None, cfg=None) -> DeviceRun:
+    """A new device run holding a copy of ``sim``'s current tree, cell and face
+    data, transport table, photon table and generator state (the state a
+    reference run holds between two steps), in the given precision. cfg: a
+    variant of the run's configuration (e.g. photoionization off)."""
+    cfg = sim.cfg if cfg is None else cfg
+    src = sim.device
+    meta, geom, levels = sim.tree.export()
+    rc, xm, inv = sim.table()
+    r = DeviceRun(cfg)
+    r.set_table(rc, xm, inv)
+    if cfg.photoi_enabled:
+        ph_dist, ph_frac = photon_table(cfg)
+        r.set_photon_table(ph_dist, ph_frac)
+        r.set_rng_state(src.rng_state())
+    r.upload_tree(meta, geom, sim.tree.min_lvl, sim.tree.max_lvl, levels)
+    for iv in range(N_VAR_CELL):
+        r.set_cc(iv, src.cc(iv))
+    for d in range(2):
+        for f in range(N_VAR_FACE):
+            r.set_fc(d, f, src.fc(d, f))
+    if mixed:
+        r.set_precision(True, schedule)
+    return r

@@ -94,3 +94,46 @@ def bytes_per_step(c: Census, n_down: int = 2, n_up: int = 2, word: int = 8,
     if photons > 0:
         total += word * 8 * N_leaf + 16.0 * photons
     return total
+
+
+# ---------------------------------------------------------------------------
+# Observables of the streamer head, used to state the error of the mixed
+# form against the FP64 path.
+
+def line_cells(meta: np.ndarray, geom: np.ndarray, levels, cfg):
+    """Leaf cells along the symmetry line: the axis r = 0 of the cylindrical
+    form (the first cell column of the boxes that touch it), or the line
+    x = L/2 of the Cartesian form (the two cell columns beside it). Returns
+    (box ids, cell indices into the (nc+2)^2 slot, z of the cell centres)."""
+    ids, cells, zs = [], [], []
+    x_line = 0.0 if cfg.coord == "cyl" else 0.5 * cfg.domain_len[0]
+    for lvl, (_, leaves, _) in levels.items():
+        for bid in leaves:
+            n = int(meta[bid, 14])
+            dr = geom[bid, 3]
+            r0, r1 = geom[bid, 0], geom[bid, 1]
+            for i in range(1, n + 1):
+                xc = r0 + (i - 0.5) * dr
+                if abs(xc - x_line) >= dr:
+                    continue
+                for j in range(1, n + 1):
+                    ids.append(bid)
+                    cells.append(i + (n + 2) * j)
+                    zs.append(r1 + (j - 0.5) * dr)
+    return np.asarray(ids), np.asarray(cells), np.asarray(zs)
+
+
+def head_observables(fld: np.ndarray, meta, geom, levels, cfg):
+    """(z of the maximum of |E| on the symmetry line, that maximum, the
+    maximum of |E| over all leaf cells). fld: the |E| cell variable as
+    downloaded, one (nc+2)^2 slot per box id."""
+    ids, cells, zs = line_cells(meta, geom, levels, cfg)
+    vals = fld[ids, cells]
+    k = int(np.argmax(vals))
+    emax = 0.0
+    for lvl, (_, leaves, _) in levels.items():
+        for bid in leaves:
+            n = int(meta[bid, 14])
+            blk = fld[bid, :(n + 2) ** 2].reshape(n + 2, n + 2)[1:n + 1, 1:n + 1]
+            emax = max(emax, float(blk.max()))
+    return float(zs[k]), float(vals[k]), emax

@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--batch", type=int, default=148, help="replicas in the batched extra (0: skip)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="budget of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision form")
     return ap.parse_args()
 
 
@@ -223,6 +224,7 @@ def run_b200(args):
     run = sim.device
     n_leaf = run.n_leaf_cells()
     meta, geom, levels = sim.tree.export()
+    head_fp64 = metrics.head_observables(run.cc(dv.I_FLD), meta, geom, levels, cfg)
     cen = metrics.census(meta, levels, cfg.box_size)
     dt = run.get_max_dt()
 
@@ -273,29 +275,10 @@ def run_b200(args):
     e2e = {"value": replicas.replica_throughput(n_leaf * K * world, e2e_s), "unit": UNIT,
            "h2d_bytes_per_step": 8, "d2h_bytes_per_step": 24}
 
-    # batched extra: B replicas of the same mesh and state, one block each
-    batched = None
-    if args.batch > 0:
-        cc = [run.cc(iv) for iv in range(9)]
-        fc = [[run.fc(d, f) for f in range(2)] for d in range(2)]
-        rc, xm, inv = sim.table()
-        reps = []
-        if cfg.photoi_enabled:
-            ph_dist, ph_frac = dv.photon_table(cfg)
-            rng = run.rng_state()
-        for _ in range(args.batch):
-            r = dv.DeviceRun(cfg)
-            r.set_table(rc, xm, inv)
-            if cfg.photoi_enabled:
-                r.set_photon_table(ph_dist, ph_frac)
-                r.set_rng_state(rng)
-            r.upload_tree(meta, geom, sim.tree.min_lvl, sim.tree.max_lvl, levels)
-            for iv in range(9):
-                r.set_cc(iv, cc[iv])
-            for d in range(2):
-                for f in range(2):
-                    r.set_fc(d, f, fc[d][f])
-            reps.append(r)
+    def time_batch(mixed, schedule=None):
+        """B replicas of the same mesh and state, one block each, one launch
+        per kernel per step; L2 flushed before every timed step."""
+        reps = [dv.clone_state(sim, mixed=mixed, schedule=schedule) for _ in range(args.batch)]
         bstream = torch.cuda.ExternalStream(reps[0].stream_ptr())
         dts = [dt] * len(reps)
         for _ in range(2):
@@ -313,11 +296,76 @@ def run_b200(args):
         reps[0].sync()
         torch.cuda.synchronize()
         bt = sum(a.elapsed_time(b) for a, b in zip(b0, b1)) / 1e3
-        batched = {"replicas": len(reps), "steps": nb, "value": n_leaf * len(reps) * nb / bt,
-                   "unit": UNIT, "ms_per_step": 1e3 * bt / nb,
-                   "achieved_gbs": bytes_step * len(reps) * nb / bt / 1e9}
         for r in reps:
             r.close()
+        return {"replicas": len(reps), "steps": nb, "value": n_leaf * len(reps) * nb / bt,
+                "unit": UNIT, "ms_per_step": 1e3 * bt / nb,
+                "achieved_gbs": bytes_step * len(reps) * nb / bt / 1e9}
+
+    def time_single(r):
+        """K steps of one run, L2 flushed before each, CUDA events on its stream."""
+        st = torch.cuda.ExternalStream(r.stream_ptr())
+        for _ in range(args.warmup):
+            r.step(dt)
+        r.sync()
+        a0 = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+        a1 = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+        with torch.cuda.stream(st):
+            for k in range(K):
+                flush.fill_(k & 0xFF)
+                a0[k].record(st)
+                r.step(dt)
+                a1[k].record(st)
+        r.sync()
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(b) for a, b in zip(a0, a1)) / K
+
+    batched = time_batch(False) if args.batch > 0 else None
+
+    # mixed-precision form: schedule picked by the autotuner on this tree,
+    # errors against the FP64 path (bit-identical to the reference's
+    # arithmetic) over K steps from the same state and over a whole run
+    mixed = None
+    if not args.no_mixed:
+        from a5_streamer_b200 import autotune
+        import dataclasses
+        tuned = autotune.tune_schedule(sim, ref_head=head_fp64)
+        sched = tuned["schedule"]
+        mrun = dv.clone_state(sim, mixed=True, schedule=sched)
+        m_ms = time_single(mrun)
+        mrun.close()
+        # K steps on the frozen mesh, photoionization off in both copies (the
+        # photon counts are stochastic and would diverge between the two)
+        cfg_np = dataclasses.replace(cfg, photoi_enabled=False)
+        a = dv.clone_state(sim, cfg=cfg_np)
+        b = dv.clone_state(sim, mixed=True, schedule=sched, cfg=cfg_np)
+        for _ in range(K):
+            a.step(dt)
+            b.step(dt)
+        a.sync()
+        b.sync()
+        err_k = autotune.errors_against(a, b, meta, geom, levels, cfg)
+        a.close()
+        b.close()
+        head_m = autotune.whole_run_observables(cfg, sched)
+        mixed = {
+            "value": n_leaf / (m_ms / 1e3), "unit": UNIT, "ms_per_step": m_ms,
+            "speedup_vs_fp64": ms_per_step / m_ms, "dtype": "f32 fluxes/lookups/smoothing, f64 residual/potential/densities/dt",
+            "schedule": {"fmg": sched[0], "n_cycle_down": sched[1], "n_cycle_up": sched[2],
+                         "n_cycle_base": sched[3], "n_corr": sched[4]},
+            "errors_after_steps": {"steps": K, "photoionization": False,
+                                   **{k: err_k[k] for k in ("max_E_rel", "head_z_rel", "phi_rel", "n_e_rel")}},
+            "errors_whole_run": {"t_end": cfg.end_time,
+                                 "head_z_rel": abs(head_m[0] - head_fp64[0]) / abs(head_fp64[0]),
+                                 "max_E_rel": abs(head_m[2] - head_fp64[2]) / head_fp64[2],
+                                 "head_z_m": [head_fp64[0], head_m[0]], "max_E": [head_fp64[2], head_m[2]],
+                                 "photoionization": bool(cfg.photoi_enabled),
+                                 "note": ("photon counts are stochastic: the two runs draw different photons "
+                                          "once a cell's rounded count differs") if cfg.photoi_enabled else ""},
+            "bounds": {"max_E_rel": 1e-4, "head_z_rel": 5e-3},
+            "tuner": {"candidates": len(tuned["table"]), "n_steps": tuned["n_steps"]},
+            "batched": time_batch(True, sched) if args.batch > 0 else None,
+        }
 
     peak, peak_kind = measured_peak()
     achieved = bytes_step / (ms_per_step / 1e3) / 1e9
@@ -348,7 +396,7 @@ def run_b200(args):
                        "l2": "flushed before every timed step (256 MiB write)"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": K * launches_per_step,
-            "clocks": clk.summary(), "batched": batched,
+            "clocks": clk.summary(), "batched": batched, "mixed": mixed,
         }
         print(json.dumps(out), flush=True)
     sim.close()

@@ -183,6 +183,34 @@ int a5g_photoionization(a5g_ctx *ctx, double dt, int has_dt);
 /* Photons created by the last photoionization call and its factor fac
  * (photons per unit production, src/m_photons.f90:250-256). Synchronises. */
 int a5g_photon_stats(a5g_ctx *ctx, long long *n_created, double *fac);
+/* Precision of the run's time steps. The reference computes in FP64
+ * throughout (dp = kind(0d0)); A5G_MIXED is an addition of this library with
+ * no counterpart there:
+ *  - fluxes_koren, update_solution and their table lookups run in FP32;
+ *  - every field solve is a defect correction: the residual of the space
+ *    charge (n_i - n_e, which cancels) against the FP64 potential is formed
+ *    in FP64, the correction equation is solved by an FP32 multigrid with
+ *    the schedule below, and the correction is added to the FP64 potential;
+ *  - densities, the potential, the field and the step-size reductions are
+ *    stored and reduced in FP64.
+ * With A5G_MIXED, a5g_step, the batched steps and a5g_compute_fld (except
+ * with no_guess, which keeps the FP64 FMG from a zero potential) take the
+ * mixed form. */
+#define A5G_FP64 0
+#define A5G_MIXED 1
+/* Multigrid schedule of the FP32 correction solve (the FP64 path always
+ * uses the reference's: FMG, 2 down, 2 up and n_cycle_base base cycles,
+ * afivo/src/m_aX_mg.f90:163-254). */
+typedef struct a5g_mg_schedule {
+  int fmg;          /* 1: mg$D_fas_fmg; 0: one V-cycle over all levels */
+  int n_cycle_down; /* red-black cycles per level on the way down, 1..8 */
+  int n_cycle_up;   /* red-black cycles per level on the way up, 1..8 */
+  int n_cycle_base; /* red-black cycles on the coarsest level, 1..64 */
+  int n_corr;       /* defect-correction passes per field solve, 1..8 */
+} a5g_mg_schedule;
+/* sched NULL: the reference's schedule (1, 2, 2, n_cycle_base, 1). */
+int a5g_set_precision(a5g_ctx *ctx, int precision, const a5g_mg_schedule *sched);
+int a5g_get_precision(a5g_ctx *ctx, int *precision, a5g_mg_schedule *sched);
 /* One full time step on the current mesh (src/streamer_2d.f90:93-128, one
  * iteration of the n loop): set_photoionization when enabled, save old
  * densities, two forward-Euler stages with a field solve after the first,

@@ -1,0 +1,177 @@
+"""Mixed-precision form (FP32 fluxes, lookups and multigrid smoothing inside
+an FP64 defect correction) against the FP64 oracle, and the device-memory
+path of the multigrid (trees too large for shared memory), which must stay
+bit-exact in FP64.
+
+Bounds, stated against the FP64 oracle on identical inputs:
+  - max |E| within 1e-4 relative;
+  - streamer-head position (z of the maximum of |E| on the symmetry line)
+    within 0.5 %;
+  - with the reference's own multigrid schedule, the mixed solve tracks the
+    FP64 solve to 1e-6 relative in phi and |E|.
+"""
+import numpy as np
+import pytest
+
+import a5ref
+from a5_streamer_b200 import autotune, config, metrics, streamer
+from a5_streamer_b200 import device as dv
+from a5_streamer_b200._lib import call
+from parity import compare, device_from_oracle
+
+pytestmark = pytest.mark.gpu
+
+TOL_MAX_E = 1e-4
+TOL_HEAD_Z = 5e-3
+DT = 2.5e-11
+
+
+def _oracle(cfg, blocks=2):
+    sim = a5ref.Sim(cfg, n_threads=4)
+    sim.init()
+    for _ in range(blocks):
+        sim.advance(True)
+    return sim
+
+
+def _leaf_rel(a, b, meta, levels):
+    leaves = autotune.leaf_ids(levels)
+    d = autotune.leaf_max_abs_diff(a, b, meta, leaves)
+    m = autotune.leaf_max_abs_diff(a, np.zeros_like(a), meta, leaves)
+    return d / m
+
+
+def _levels(sim):
+    return sim.levels()
+
+
+@pytest.mark.parametrize("name", ["cart", "cyl"])
+def test_mixed_reference_schedule_tracks_oracle(name):
+    """Reference schedule (FMG, 2/2/base cycles): only the arithmetic of the
+    fluxes and of the smoothing changes; 10 steps stay within 1e-6."""
+    cfg = config.cartesian_8mm() if name == "cart" else config.cylindrical_16mm()
+    sim = _oracle(cfg)
+    run = device_from_oracle(sim, cfg)
+    run.set_precision(True)
+    assert run.precision() == (True, (1, 2, 2, cfg.n_cycle_base, 1))
+    for _ in range(10):
+        sim.step(DT)
+        run.step(DT)
+    meta, geom, levels = sim.meta(), sim.geom(), _levels(sim)
+    for iv in (dv.I_PHI, dv.I_FLD, dv.I_ELEC, dv.I_PION):
+        assert _leaf_rel(sim.cc(iv), run.cc(iv), meta, levels) < 1e-6, iv
+
+
+@pytest.mark.parametrize("name,sched", [("cyl", (0, 2, 2, 4, 1)), ("cart", (0, 2, 2, 8, 2)),
+                                        ("cart", (1, 1, 1, 8, 1))])
+def test_mixed_schedules_within_bounds(name, sched):
+    cfg = config.cartesian_8mm() if name == "cart" else config.cylindrical_16mm()
+    sim = _oracle(cfg)
+    run = device_from_oracle(sim, cfg)
+    run.set_precision(True, sched)
+    for _ in range(20):
+        sim.step(DT)
+        run.step(DT)
+    meta, geom, levels = sim.meta(), sim.geom(), _levels(sim)
+    za, _, ma = metrics.head_observables(sim.cc(dv.I_FLD), meta, geom, levels, cfg)
+    zb, _, mb = metrics.head_observables(run.cc(dv.I_FLD), meta, geom, levels, cfg)
+    assert abs(ma - mb) / ma < TOL_MAX_E
+    assert abs(za - zb) / za < TOL_HEAD_Z
+    assert np.isfinite(run.cc(dv.I_PHI)).all()
+
+
+def test_mixed_batch_equals_single():
+    """The batched launch runs the same mixed step per block: bit-identical."""
+    cfg = config.cylindrical_16mm()
+    sim = _oracle(cfg)
+    a = device_from_oracle(sim, cfg)
+    b = device_from_oracle(sim, cfg)
+    c = device_from_oracle(sim, cfg)
+    for r in (a, b):
+        r.set_precision(True, (0, 2, 2, 4, 1))
+    for _ in range(3):
+        a.step(DT)
+        dv.step_batch([b, c], [DT, DT])  # c stays FP64 in the same launch
+        sim.step(DT)
+    for iv in range(9):
+        assert np.array_equal(a.cc(iv), b.cc(iv)), iv
+    compare(sim, c, where="fp64 member of a mixed batch")
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_device_memory_path(mixed):
+    """Multigrid without shared-memory staging (the path of trees larger than
+    shared memory): FP64 stays bit-exact; mixed equals its staged form."""
+    cfg = config.cylindrical_16mm()
+    sim = _oracle(cfg)
+    run = device_from_oracle(sim, cfg)
+    call("a5g_debug_set_staging", run.h, 0)
+    if mixed:
+        staged = device_from_oracle(sim, cfg)
+        for r in (run, staged):
+            r.set_precision(True, (0, 2, 2, 4, 1))
+        for _ in range(3):
+            run.step(DT)
+            staged.step(DT)
+        for iv in (dv.I_PHI, dv.I_FLD, dv.I_ELEC):
+            assert np.array_equal(run.cc(iv), staged.cc(iv)), iv
+    else:
+        for _ in range(3):
+            run.step(DT)
+            sim.step(DT)
+        compare(sim, run, where="device-memory multigrid")
+        sim.op("compute_fld", 0)
+        run.compute_fld(False)
+        compare(sim, run, where="device-memory compute_fld")
+        sim.op("fmg", 0, 1)
+        run.fas_fmg(False, True)
+        compare(sim, run, cc_vars=[0, 1, 2, 3, 4, 6, 7, 8], where="device-memory first FMG")
+
+
+def test_autotuner_choice_within_bounds():
+    cfg = config.cartesian_8mm()
+    sim = streamer.Simulation(cfg)
+    sim.init()
+    sim.advance(True)
+    res = autotune.tune_schedule(sim, n_steps=10,
+                                 candidates=[(0, 1, 1, 2, 1), (0, 2, 2, 16, 2), (1, 1, 1, 8, 1)])
+    assert len(res["table"]) == 3
+    for k, tol in (("max_E_rel", TOL_MAX_E), ("head_z_rel", TOL_HEAD_Z),
+                   ("run_max_E_rel", TOL_MAX_E), ("run_head_z_rel", TOL_HEAD_Z)):
+        assert res["errors"][k] <= tol, k
+    # the cheapest candidate misses the whole-run bound on this tree
+    assert res["schedule"] != (0, 1, 1, 2, 1)
+    chosen = [r for r in res["table"] if tuple(r["schedule"]) == res["schedule"]][0]
+    assert chosen["ok"]
+    assert all(r["ms"] >= chosen["ms"] for r in res["table"] if r["ok"])
+
+
+@pytest.mark.parametrize("name", ["cart", "cyl"])
+def test_mixed_whole_run_against_oracle(name):
+    """The driver in the mixed form (regrids included) to the end time against
+    the oracle's FP64 run: streamer head and max |E| within the bounds."""
+    cfg = config.cartesian_8mm() if name == "cart" else config.cylindrical_16mm()
+    sched = (1, 1, 1, 8, 1) if name == "cart" else (0, 2, 2, 4, 1)
+    sim = streamer.Simulation(cfg)
+    sim.device.set_precision(True, sched)
+    sim.init()
+    sim.run(cfg.end_time)
+    ref = a5ref.Sim(cfg, n_threads=8)
+    ref.init()
+    ref.run(cfg.end_time)
+    meta, geom, levels = sim.tree.export()
+    zb, _, mb = metrics.head_observables(sim.device.cc(dv.I_FLD), meta, geom, levels, cfg)
+    za, _, ma = metrics.head_observables(ref.cc(dv.I_FLD), ref.meta(), ref.geom(), ref.levels(), cfg)
+    assert abs(ma - mb) / ma < TOL_MAX_E, (ma, mb)
+    assert abs(za - zb) / za < TOL_HEAD_Z, (za, zb)
+
+
+def test_precision_argument_checks():
+    cfg = config.cartesian_8mm()
+    run = dv.DeviceRun(cfg)
+    with pytest.raises(Exception):
+        run.set_precision(True, (2, 2, 2, 8, 1))
+    with pytest.raises(Exception):
+        run.set_precision(True, (0, 0, 2, 8, 1))
+    run.set_precision(False)
+    assert run.precision()[0] is False
