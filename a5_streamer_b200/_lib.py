@@ -91,6 +91,10 @@ SIGNATURES = {
     "a5g_step_batch": (_I, [ctypes.POINTER(_P), _I, _PD]),
     "a5g_step_batch_static": (_I, [ctypes.POINTER(_P), _I, _PD]),
     "a5g_sync": (_I, [_P]),
+    "a5g_batch_create": (_I, [ctypes.POINTER(_P), _I, ctypes.POINTER(_P)]),
+    "a5g_batch_destroy": (_I, [_P]),
+    "a5g_batch_begin": (_I, [_P, _PD, _PD]),
+    "a5g_batch_block": (_I, [_P, _I, _I, _PD, _PD, _PI, ctypes.POINTER(ctypes.c_float)]),
     "a5g_n_leaf_cells": (_I, [_P, ctypes.POINTER(ctypes.c_longlong)]),
     "a5g_get_stream": (_I, [_P, ctypes.POINTER(_P)]),
     "a5g_debug_set_staging": (_I, [_P, _I]),
@@ -114,6 +118,7 @@ SIGNATURES = {
     "a5s_advance": (_I, [_P, _I, _PD]),
     "a5s_run": (_I, [_P, _D, _I, _PI]),
     "a5s_time": (_I, [_P, _PD]),
+    "a5s_batch_run": (_I, [ctypes.POINTER(_P), _I, _PD, _I, _I, _I, _PI, _PD, _PD, _PD]),
     "a5s_ctx": (_I, [_P, ctypes.POINTER(_P)]),
     "a5s_tree": (_I, [_P, ctypes.POINTER(_P)]),
     "a5s_table": (_I, [_P, _PD, _PD, _PD, _PI]),

@@ -186,3 +186,53 @@ def tune_schedule(sim, n_steps: int = 20, tol_max_E: float = 1e-4, tol_head_z: f
             "n_steps": n_steps, "dt": dt, "bounds": {"max_E_rel": tol_max_E, "head_z_rel": tol_head_z,
                                                       "safety": safety},
             "table": table}
+
+
+def batch_observables(cfgs, schedule=None, use_graph: bool = True, n_threads: int = 8):
+    """Run ``cfgs`` from their initial conditions to their end times as one
+    device-driven batch (FP64, or mixed with ``schedule``). Returns the
+    per-run head observables and the batch counters (blocks, device ms, host
+    ms, cell updates)."""
+    from .streamer import Simulation, run_batch
+    sims = [Simulation(c) for c in cfgs]
+    try:
+        for s in sims:
+            if schedule is not None:
+                s.device.set_precision(True, schedule)
+            s.init()
+        counters = run_batch(sims, [c.end_time for c in cfgs], use_graph=use_graph,
+                             n_threads=n_threads)
+        heads = []
+        for s, c in zip(sims, cfgs):
+            meta, geom, levels = s.tree.export()
+            heads.append(metrics.head_observables(s.device.cc(I_FLD), meta, geom, levels, c))
+        return heads, counters
+    finally:
+        for s in sims:
+            s.close()
+
+
+def tune_batch_schedule(cfgs, candidates: Sequence[Schedule], tol_max_E: float = 1e-4,
+                        tol_head_z: float = 5e-3, n_threads: int = 8) -> Dict:
+    """Schedule of the mixed form for a batch of independent runs. The runs
+    are compared with photoionization off (the photon counts are stochastic,
+    so two runs with it on drift apart by Monte Carlo noise whatever the
+    precision): the FP64 batch once, then each candidate in the given order
+    (cheapest first) until every run's head position and max |E| at its end
+    time are within the bounds. Returns the choice and per-run errors; if no
+    candidate qualifies, the last one."""
+    import dataclasses
+    quiet = [dataclasses.replace(c, photoi_enabled=False) for c in cfgs]
+    ref, _ = batch_observables(quiet, None, n_threads=n_threads)
+    tried = []
+    for sched in candidates:
+        heads, _ = batch_observables(quiet, tuple(sched), n_threads=n_threads)
+        zr = [abs(a[0] - b[0]) / abs(a[0]) for a, b in zip(ref, heads)]
+        er = [abs(a[2] - b[2]) / a[2] for a, b in zip(ref, heads)]
+        ok = max(zr) <= tol_head_z and max(er) <= tol_max_E
+        tried.append({"schedule": list(sched), "head_z_rel_max": max(zr), "max_E_rel_max": max(er),
+                      "max_E_rel_median": float(np.median(er)), "ok": ok})
+        if ok:
+            break
+    return {"schedule": tuple(tried[-1]["schedule"]), "errors": tried[-1], "tried": tried,
+            "bounds": {"max_E_rel": tol_max_E, "head_z_rel": tol_head_z}}

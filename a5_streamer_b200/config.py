@@ -223,6 +223,40 @@ def cylindrical_16mm(photoi: bool = False, **overrides) -> StreamerConfig:
     return dataclasses.replace(cfg, **overrides)
 
 
+def batch_cylindrical_runs(n: int = 64, seed: int = 20261203, photoi: bool = True,
+                           end_time: float = 5e-9, min_dx: float = 4e-6) -> List[StreamerConfig]:
+    """Independent axisymmetric runs of uneven size for the batched form,
+    drawn from ``numpy.random.default_rng(seed)`` in this order per run:
+    background density log-uniform in [1e15, 1e16] m^-3, E_bg uniform in
+    [1.5e6, 2.5e6] V/m, domain length Z uniform in [4, 16] mm, and the four
+    words of the run's photon generator state. The radius is Z/2 (the aspect
+    ratio of the 16 mm case), two base boxes stacked in z, the finest level
+    the first with dx <= min_dx, the seed (1e19 m^-3, sigma 0.1 mm) on the
+    axis 1 mm below the top, transport and photoionization as in the 16 mm
+    case; each run to its own end time."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    out: List[StreamerConfig] = []
+    for _ in range(n):
+        bg = float(10.0 ** rng.uniform(15.0, 16.0))
+        ebg = float(rng.uniform(1.5e6, 2.5e6))
+        z_len = float(rng.uniform(4e-3, 16e-3))
+        st = rng.integers(1, 2147483579, size=3)
+        s4 = int(rng.integers(-2 ** 31, 2 ** 31))
+        r_len = 0.5 * z_len
+        dr_base = r_len / 8
+        lvls_max = 1 + max(0, math.ceil(math.log2(dr_base / min_dx) - 1e-12))
+        sigma = 0.1e-3
+        cfg = cylindrical_16mm(
+            photoi=photoi, domain_len=(r_len, z_len), applied_fld=ebg, bg_dens=bg,
+            lvls_max=lvls_max, end_time=end_time,
+            seeds=[Seed(r0=(0.0, z_len - 1e-3), r1=(0.0, z_len - 1e-3), dens=1e19,
+                        width=math.sqrt(2.0) * sigma, falloff=2)],
+            rng_seed=(int(st[0]), int(st[1]), int(st[2]), s4))
+        out.append(cfg)
+    return out
+
+
 # --- the reference's text configuration format -------------------------------
 _LINE = re.compile(r"^\s*([A-Za-z_][A-Za-z0-9_]*)\s*=\s*(.*?)\s*$")
 

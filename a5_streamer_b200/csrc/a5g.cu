@@ -131,6 +131,11 @@ struct RunDev {
   int mx_pad;
   float *cc32;
   const float *tbl32;
+  // block state of the device-driven loop (a5g_batch): [0] dt of the block,
+  // [1] simulated time, [2] end time, [3] 1 while the run is active
+  double *blk;
+  double dr_min, dt_max;       // finest cell size of the tree; ST_dt_max
+  int use_drt, pad5;
 };
 
 // Scalars of one photoionization call: photons created, the factor fac
@@ -159,7 +164,7 @@ static_assert(sizeof(PhBox) == 48, "PhBox layout");
 enum OpCode {
   OP_COPY = 1, OP_FLUXES, OP_CONSISTENT, OP_UPDATE, OP_RESTRICT, OP_GC, OP_AVERAGE,
   OP_COMPUTE_FLD, OP_FMG, OP_FLD_FROM_POT, OP_DT_RED, OP_REF_FLAGS, OP_PROLONG_NEW,
-  OP_STEP, OP_NOP, OP_PH_SOURCE, OP_PH_DEPOSIT, OP_STEP_MIXED, OP_COMPUTE_FLD_MIXED
+  OP_STEP, OP_NOP, OP_PH_SOURCE, OP_PH_DEPOSIT, OP_STEP_MIXED, OP_COMPUTE_FLD_MIXED, OP_BLOCK_DT
 };
 struct Op {
   int code, i0, i1, i2;
@@ -1589,6 +1594,8 @@ __device__ void average_dens(const RunDev &R) {
 // ---------------------------------------------------------------------------
 // Reductions and refinement flags.
 
+__device__ void dt_reductions(const RunDev &R);
+
 __device__ __forceinline__ double dmax(double a, double b) { return a < b ? b : a; }
 __device__ __forceinline__ double dmin(double a, double b) { return b < a ? b : a; }
 
@@ -1636,6 +1643,36 @@ __device__ void dt_reductions(const RunDev &R) {
 }
 
 // GM_dist_line (src/m_geom.f90:29-46), 2D, with gfortran's NORM2
+// Step size of the next block of the device-driven loop: get_max_dt
+// (src/streamer_2d.f90:271-303, cyl :281-314) from the leaf reductions, with
+// the same operations in the same order as the host's a5g_get_max_dt (table
+// columns at a location, IEEE + - * / only), then the loop's exit tests
+// (src/streamer_2d.f90:72-75): the run stays active unless dt < 1e-14 or
+// time > end time.
+__device__ void block_dt(const RunDev &R) {
+  dt_reductions(R);
+  if (threadIdx.x == 0) {
+    const double max_fld = R.scal[0], min_fld = R.scal[1], max_dns = R.scal[2];
+    const double eps_mach = 2.220446049250313e-16;
+    const double dr_min = R.dr_min;
+    const double mobility = col_at<double>(R, C_MOB, get_loc<double>(R, max_fld));
+    const double max_mobility = col_at<double>(R, C_MOB, get_loc<double>(R, min_fld));
+    const double diff_coeff = col_at<double>(R, C_DIF, get_loc<double>(R, max_fld));
+    const double alpha = col_at<double>(R, C_ALPHA, get_loc<double>(R, max_fld));
+    const double dt_cfl = dr_min / (mobility * max_fld);
+    const double dt_dif = 0.25 * (dr_min * dr_min) / diff_coeff;
+    const double dns = R.coord == 1 ? dmax(eps_mach, max_dns) : max_dns;
+    const double dt_drt = UC_EPS0 / (UC_ELEM_CHARGE * max_mobility * dns);
+    const double dt_alpha = 1 / dmax(mobility * max_fld * alpha, eps_mach);
+    double m = dmin(dmin(1 / (1 / dt_cfl + 1 / dt_dif), dt_alpha), R.dt_max);
+    if (R.use_drt) m = dmin(m, dt_drt);
+    const double dt = 0.5 * m;
+    R.blk[0] = dt;
+    R.blk[3] = (R.blk[3] != 0.0 && !(dt < 1e-14) && !(R.blk[1] > R.blk[2])) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+}
+
 __device__ double dist_line(double x, double y, const double r0[2], const double r1[2]) {
   double line_len2 = 0, temp = 0;
   line_len2 += (r1[0] - r0[0]) * (r1[0] - r0[0]);
@@ -2245,10 +2282,29 @@ __device__ void run_op(const RunDev &R, const Op &op) {
     case OP_DT_RED: dt_reductions(R); break;
     case OP_REF_FLAGS: ref_flags(R, op.d0); break;
     case OP_PROLONG_NEW: prolong_new(R); break;
-    case OP_STEP: step<false>(R, op.d0, op.i0 != 0); break;
-    case OP_STEP_MIXED: step<true>(R, op.d0, op.i0 != 0); break;
+    case OP_STEP:
+    case OP_STEP_MIXED: {
+      // i1 = 1: the block's dt and active flag come from the device block state
+      double dt = op.d0;
+      if (op.i1) {
+        if (R.blk[3] == 0.0) break;
+        dt = R.blk[0];
+      }
+      if (op.code == OP_STEP) step<false>(R, dt, op.i0 != 0);
+      else step<true>(R, dt, op.i0 != 0);
+      if (op.i1 && threadIdx.x == 0) R.blk[1] = R.blk[1] + dt;
+      break;
+    }
+    case OP_BLOCK_DT: block_dt(R); break;
     case OP_COMPUTE_FLD_MIXED: p_compute_fld_mixed(R); break;
-    case OP_PH_SOURCE: ph_source(R, op.d0, op.i0 != 0); break;
+    case OP_PH_SOURCE:
+      if (op.i1 && R.blk[3] == 0.0) {
+        // inactive run of a device-driven batch: no photons this step
+        if (threadIdx.x == 0) R.ph_scal->n_used = 0;
+        break;
+      }
+      ph_source(R, op.i1 ? R.blk[0] : op.d0, op.i0 != 0);
+      break;
     case OP_PH_DEPOSIT: ph_deposit(R); break;
     case OP_NOP: break;
     default: if (threadIdx.x == 0) atomicExch(R.status, A5G_EINVAL);
@@ -2879,6 +2935,13 @@ int a5g_create(const a5g_params *p, a5g_ctx **out) {
     return fail(A5G_ENOMEM, "cudaMalloc failed");
   }
   cudaMemset(c->status, 0, sizeof(int));
+  {
+    // scalars: [0..2] reductions, [8..11] block state (dt, time, end time, active)
+    double z[16] = {0};
+    z[10] = HUGE_VAL;
+    z[11] = 1.0;
+    cudaMemcpy(c->scal, z, sizeof(z), cudaMemcpyHostToDevice);
+  }
   RunDev &h = c->h;
   std::memset(&h, 0, sizeof(RunDev));
   h.coord = p->coord;
@@ -2898,6 +2961,9 @@ int a5g_create(const a5g_params *p, a5g_ctx **out) {
     h.seed_width[s] = p->seed_width[s];
   }
   h.scal = c->scal;
+  h.blk = c->scal + 8;
+  h.dt_max = p->dt_max;
+  h.use_drt = p->use_drt ? 1 : 0;
   h.status = c->status;
   h.mx_fmg = 1;
   h.mx_sw_down = h.mx_sw_up = 4;
@@ -3276,6 +3342,7 @@ int a5g_upload_tree(a5g_ctx *c, int max_id, int min_lvl, int max_lvl, const int 
   h.min_lvl = min_lvl;
   h.max_lvl = max_lvl;
   h.nlev = nlev;
+  h.dr_min = c->p.dr_base * std::pow(0.5, max_lvl - 1);  // as a5g_get_max_dt
   for (int kind = 0; kind < 3; kind++)
     for (int li = 0; li <= nlev; li++) h.lv_off[kind][li] = off[kind][li];
   h.lists = c->lists;
@@ -3646,6 +3713,194 @@ int a5g_step_batch_static(a5g_ctx **ctxs, int n, const double *dts) {
                      cudaMemcpyHostToDevice, c0->stream));
   a5g_run_kernel_slots<<<n, NTHR, dyn, c0->stream>>>(g_static_dev[dev]);
   CK(cudaGetLastError());
+  return A5G_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Device-driven batch of runs (a5g_batch_*): one block of the main loop --
+// get_max_dt and num_steps_amr steps -- for every run in one launch per
+// kernel, with each run's dt, time and active flag kept on the device, so
+// that the block is a fixed sequence of launches that a CUDA graph replays.
+struct a5g_batch {
+  std::vector<a5g_ctx *> ctxs;
+  cudaStream_t stream = nullptr;
+  const RunDev **d_rp = nullptr;
+  Op *d_ops = nullptr;  // [block dt | photon sources | steps], n each
+  bool any_ph = false;
+  int max_team = 0;
+  size_t ph_smem = 0, dyn = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int graph_steps = -1;
+  double *h_state = nullptr;  // pinned, 4 per run
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+static void batch_drop_graph(a5g_batch *b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+  b->graph_steps = -1;
+}
+
+// Operation table of the batch from the members' current precision and
+// photoionization settings.
+static int batch_build_ops(a5g_batch *b) {
+  const int n = (int)b->ctxs.size();
+  std::vector<const RunDev *> rp(n);
+  std::vector<Op> ops(3 * n);
+  b->any_ph = false;
+  b->max_team = 0;
+  size_t ph = 48 << 10;
+  for (int k = 0; k < n; k++) {
+    a5g_ctx *c = b->ctxs[k];
+    rp[k] = c->d_run;
+    const bool phk = c->p.photoi_enabled != 0;
+    if (phk) {
+      b->any_ph = true;
+      b->max_team = std::max(b->max_team, c->p.photoi_team);
+      ph = std::max(ph, ph_smem_bytes(c));
+    }
+    ops[k] = mkop(OP_BLOCK_DT);
+    ops[n + k] = phk ? mkop(OP_PH_SOURCE, 1, 1) : mkop(OP_NOP);
+    ops[2 * n + k] = mkop(c->precision == A5G_MIXED ? OP_STEP_MIXED : OP_STEP, phk ? 1 : 0, 1);
+  }
+  b->ph_smem = std::min(ph, dyn_smem_limit());
+  b->dyn = dyn_smem_limit();
+  CK(cudaMemcpy(b->d_rp, rp.data(), n * sizeof(void *), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(b->d_ops, ops.data(), 3 * n * sizeof(Op), cudaMemcpyHostToDevice));
+  batch_drop_graph(b);
+  return A5G_OK;
+}
+
+// The launches of one block on the batch stream. Every launch takes the
+// largest dynamic shared memory a run may use, so that a captured graph stays
+// valid while the members' trees change between blocks.
+static int batch_enqueue(a5g_batch *b, int num_steps) {
+  const int n = (int)b->ctxs.size();
+  a5g_run_kernel<<<n, NTHR, b->dyn, b->stream>>>(nullptr, Op{}, b->d_rp, b->d_ops);
+  CK(cudaGetLastError());
+  for (int s = 0; s < num_steps; s++) {
+    if (b->any_ph) {
+      a5g_run_kernel<<<n, NTHR, b->dyn, b->stream>>>(nullptr, Op{}, b->d_rp, b->d_ops + n);
+      CK(cudaGetLastError());
+      dim3 grid((unsigned)((b->max_team + PH_THREADS - 1) / PH_THREADS), (unsigned)n);
+      a5g_photon_kernel<<<grid, PH_THREADS, b->ph_smem, b->stream>>>(nullptr, b->d_rp, nullptr,
+                                                                     (int)b->ph_smem);
+      CK(cudaGetLastError());
+    }
+    a5g_run_kernel<<<n, NTHR, b->dyn, b->stream>>>(nullptr, Op{}, b->d_rp, b->d_ops + 2 * n);
+    CK(cudaGetLastError());
+  }
+  return A5G_OK;
+}
+
+int a5g_batch_create(a5g_ctx **ctxs, int n, a5g_batch **out) {
+  if (!ctxs || !out || n < 1) return fail(A5G_EINVAL, "bad batch");
+  *out = nullptr;
+  int dev = -1;
+  CK(cudaGetDevice(&dev));
+  for (int k = 0; k < n; k++) {
+    if (!ctxs[k] || !ctxs[k]->has_tree || !ctxs[k]->has_table)
+      return fail(A5G_ESTATE, "batch member without tree or table");
+    cudaPointerAttributes at{};
+    CK(cudaPointerGetAttributes(&at, ctxs[k]->d_run));
+    if (at.device != dev) return fail(A5G_EINVAL, "batch member on another device than the current one");
+    for (int q = 0; q < k; q++)
+      if (ctxs[q] == ctxs[k]) return fail(A5G_EINVAL, "a context appears twice in the batch");
+  }
+  a5g_batch *b = new a5g_batch();
+  b->ctxs.assign(ctxs, ctxs + n);
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&b->d_rp, n * sizeof(void *)) != cudaSuccess ||
+      cudaMalloc(&b->d_ops, 3 * n * sizeof(Op)) != cudaSuccess ||
+      cudaMallocHost(&b->h_state, 4 * n * sizeof(double)) != cudaSuccess ||
+      cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess) {
+    a5g_batch_destroy(b);
+    return fail(A5G_ENOMEM, "cannot allocate the batch");
+  }
+  int r = batch_build_ops(b);
+  if (r) {
+    a5g_batch_destroy(b);
+    return r;
+  }
+  *out = b;
+  return A5G_OK;
+}
+
+int a5g_batch_destroy(a5g_batch *b) {
+  if (!b) return A5G_OK;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  batch_drop_graph(b);
+  cudaFree(b->d_rp);
+  cudaFree(b->d_ops);
+  if (b->h_state) cudaFreeHost(b->h_state);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return A5G_OK;
+}
+
+int a5g_batch_begin(a5g_batch *b, const double *time, const double *t_end) {
+  if (!b || !time || !t_end) return fail(A5G_EINVAL, "null argument");
+  for (size_t k = 0; k < b->ctxs.size(); k++) {
+    a5g_ctx *c = b->ctxs[k];
+    CK(cudaStreamSynchronize(c->stream));
+    const double st[4] = {0.0, time[k], t_end[k], 1.0};
+    CK(cudaMemcpy(c->scal + 8, st, sizeof(st), cudaMemcpyHostToDevice));
+  }
+  return batch_build_ops(b);
+}
+
+int a5g_batch_block(a5g_batch *b, int num_steps, int use_graph, double *dt, double *time,
+                    int *active, float *gpu_ms) {
+  if (!b || num_steps < 1) return fail(A5G_EINVAL, "bad argument");
+  const int n = (int)b->ctxs.size();
+  for (int k = 0; k < n; k++) {
+    a5g_ctx *c = b->ctxs[k];
+    int r;
+    if (c->p.photoi_enabled && (r = ph_ready(c))) return r;
+    if ((r = mx_ready(c))) return r;
+    // the members' own queued work (uploads, regrids) precedes the block
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  CK(cudaEventRecord(b->ev0, b->stream));
+  if (use_graph) {
+    if (!b->exec || b->graph_steps != num_steps) {
+      batch_drop_graph(b);
+      CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+      int r = batch_enqueue(b, num_steps);
+      cudaGraph_t g = nullptr;
+      cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+      if (r) {
+        if (g) cudaGraphDestroy(g);
+        return r;
+      }
+      if (e != cudaSuccess) return fail(A5G_ECUDA, std::string("stream capture: ") + cudaGetErrorString(e));
+      b->graph = g;
+      CK(cudaGraphInstantiate(&b->exec, b->graph, 0));
+      b->graph_steps = num_steps;
+    }
+    CK(cudaGraphLaunch(b->exec, b->stream));
+  } else {
+    int r = batch_enqueue(b, num_steps);
+    if (r) return r;
+  }
+  CK(cudaEventRecord(b->ev1, b->stream));
+  for (int k = 0; k < n; k++)
+    CK(cudaMemcpyAsync(b->h_state + 4 * k, b->ctxs[k]->scal + 8, 4 * sizeof(double),
+                       cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  for (int k = 0; k < n; k++) {
+    int r = check_status(b->ctxs[k]);
+    if (r) return r;
+    if (dt) dt[k] = b->h_state[4 * k];
+    if (time) time[k] = b->h_state[4 * k + 1];
+    if (active) active[k] = b->h_state[4 * k + 3] != 0.0;
+  }
+  if (gpu_ms) CK(cudaEventElapsedTime(gpu_ms, b->ev0, b->ev1));
   return A5G_OK;
 }
 

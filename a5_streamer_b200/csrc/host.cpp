@@ -6,10 +6,13 @@
 // (initial conditions, table build); the per-step work runs in a5g.cu.
 #include <algorithm>
 #include <array>
+#include <atomic>
+#include <chrono>
 #include <climits>
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/a5t.h"
@@ -674,14 +677,11 @@ int a5s_init(a5s_sim *s, int *n_iter) {
   return a5g_sync(s->ctx);
 }
 
-static int do_block(a5s_sim *s, double dt, int regrid) {
-  int r;
-  for (int n = 0; n < s->cfg.num_steps_amr; n++) {
-    s->time += dt;
-    if ((r = a5g_step(s->ctx, dt))) return r;
-  }
-  if (!regrid) return A5G_OK;
-  int na = 0, nr = 0;
+// The regrid at the end of a main-loop block (src/streamer_2d.f90:130-141):
+// refinement flags, a$D_adjust_refinement, prolongation into new boxes and a
+// field solve when the tree changed.
+static int regrid_block(a5s_sim *s) {
+  int na = 0, nr = 0, r;
   if ((r = s->regrid(&na, &nr))) return r;
   if (na > 0 || nr > 0) {
     int nlev = s->tree->max_lvl - s->tree->min_lvl + 1;
@@ -691,6 +691,16 @@ static int do_block(a5s_sim *s, double dt, int regrid) {
     if ((r = a5g_compute_fld(s->ctx, 0))) return r;
   }
   return A5G_OK;
+}
+
+static int do_block(a5s_sim *s, double dt, int regrid) {
+  int r;
+  for (int n = 0; n < s->cfg.num_steps_amr; n++) {
+    s->time += dt;
+    if ((r = a5g_step(s->ctx, dt))) return r;
+  }
+  if (!regrid) return A5G_OK;
+  return regrid_block(s);
 }
 
 int a5s_advance(a5s_sim *s, int regrid, double *dt_used) {
@@ -715,6 +725,83 @@ int a5s_run(a5s_sim *s, double t_end, int max_blocks, int *n_blocks) {
   }
   if (n_blocks) *n_blocks = nb;
   return a5g_sync(s->ctx);
+}
+
+int a5s_batch_run(a5s_sim **sims, int n, const double *t_end, int use_graph, int n_threads,
+                  int max_blocks, int *n_blocks, double *gpu_ms, double *host_ms,
+                  double *cell_updates) {
+  if (!sims || !t_end || n < 1) return err(A5G_EINVAL, "bad batch");
+  for (int k = 0; k < n; k++) {
+    if (!sims[k]) return err(A5G_EINVAL, "null sim in batch");
+    if (sims[k]->cfg.num_steps_amr != sims[0]->cfg.num_steps_amr)
+      return err(A5G_EINVAL, "batch members need the same num_steps_amr");
+  }
+  std::vector<a5g_ctx *> ctxs(n);
+  std::vector<double> dt(n), tm(n);
+  std::vector<int> act(n);
+  for (int k = 0; k < n; k++) {
+    ctxs[k] = sims[k]->ctx;
+    tm[k] = sims[k]->time;
+  }
+  a5g_batch *b = nullptr;
+  int r = a5g_batch_create(ctxs.data(), n, &b);
+  if (r) return r;
+  if ((r = a5g_batch_begin(b, tm.data(), t_end))) {
+    a5g_batch_destroy(b);
+    return r;
+  }
+  const int steps = sims[0]->cfg.num_steps_amr;
+  int nb = 0;
+  double g_ms = 0, h_ms = 0, cu = 0;
+  std::vector<long long> leaves(n, 0);
+  while (nb < max_blocks) {
+    for (int k = 0; k < n; k++) a5g_n_leaf_cells(ctxs[k], &leaves[k]);
+    float ms = 0;
+    if ((r = a5g_batch_block(b, steps, use_graph, dt.data(), tm.data(), act.data(), &ms))) break;
+    g_ms += ms;
+    std::vector<int> todo;
+    for (int k = 0; k < n; k++) {
+      sims[k]->time = tm[k];
+      if (act[k]) {
+        todo.push_back(k);
+        cu += (double)leaves[k] * steps;
+      }
+    }
+    if (todo.empty()) break;
+    nb++;
+    // regrid the runs that stepped, n_threads at a time (trees and contexts
+    // are independent; each context works on its own stream)
+    const auto t0 = std::chrono::steady_clock::now();
+    std::atomic<size_t> next{0};
+    std::vector<int> rc(todo.size(), A5G_OK);
+    std::vector<std::string> msg(todo.size());
+    auto work = [&]() {
+      size_t i;
+      while ((i = next++) < todo.size()) {
+        rc[i] = regrid_block(sims[todo[i]]);
+        if (rc[i]) msg[i] = a5g_last_error();
+      }
+    };
+    const int nt = std::max(1, std::min(n_threads, (int)todo.size()));
+    std::vector<std::thread> th;
+    for (int t = 1; t < nt; t++) th.emplace_back(work);
+    work();
+    for (auto &t : th) t.join();
+    for (int k = 0; k < n; k++) {
+      int e = a5g_sync(ctxs[k]);
+      if (e && !r) r = e;
+    }
+    h_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    for (size_t i = 0; i < todo.size() && !r; i++)
+      if (rc[i]) r = err(rc[i], "regrid of batch member " + std::to_string(todo[i]) + ": " + msg[i]);
+    if (r) break;
+  }
+  a5g_batch_destroy(b);
+  if (n_blocks) *n_blocks = nb;
+  if (gpu_ms) *gpu_ms = g_ms;
+  if (host_ms) *host_ms = h_ms;
+  if (cell_updates) *cell_updates = cu;
+  return r;
 }
 
 int a5s_time(a5s_sim *s, double *t) {

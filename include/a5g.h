@@ -241,6 +241,28 @@ int a5g_step_batch(a5g_ctx **ctxs, int n, const double *dts);
  *    different streams) race; calls queued on one stream are ordered. */
 #define A5G_STATIC_BATCH_MAX 1024
 int a5g_step_batch_static(a5g_ctx **ctxs, int n, const double *dts);
+/* Device-driven batch: one main-loop block (src/streamer_2d.f90:68-128:
+ * get_max_dt, then num_steps_amr steps) for n runs in one launch per kernel.
+ * Each run's step size, simulated time and active flag live on the device:
+ * the block computes dt from the run's leaf reductions with the host's
+ * arithmetic (a5g_get_max_dt), a run stays active until dt < 1e-14 or its
+ * time exceeds its end time (the loop exits of :72-75), and only active runs
+ * step. Since nothing of a block is decided on the host, the block is a
+ * fixed launch sequence; with use_graph it is captured once in a CUDA graph
+ * and replayed. The reference has no counterpart (it runs one tree per
+ * process); it replaces a5g_get_max_dt + a5g_step per run.
+ *  a5g_batch_begin: each run's current time and end time; also picks up
+ *    changed precision settings;
+ *  a5g_batch_block: one block; returns each run's dt of the block, its time
+ *    after it, whether it stepped, and the block's device time (ms). The
+ *    members' own streams are synchronised first (their regrids and uploads
+ *    come before the block). */
+typedef struct a5g_batch a5g_batch;
+int a5g_batch_create(a5g_ctx **ctxs, int n, a5g_batch **out);
+int a5g_batch_destroy(a5g_batch *b);
+int a5g_batch_begin(a5g_batch *b, const double *time, const double *t_end);
+int a5g_batch_block(a5g_batch *b, int num_steps, int use_graph, double *dt, double *time,
+                    int *active, float *gpu_ms);
 /* Wait for all work queued on the context's stream. */
 int a5g_sync(a5g_ctx *ctx);
 /* The cudaStream_t (as void*) all work of this context is queued on, so a
