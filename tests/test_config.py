@@ -61,3 +61,24 @@ def test_validate_rejects():
         config.cartesian_8mm(box_size=6).validate()
     with pytest.raises(ValueError):
         config.cartesian_8mm(domain_len=(8e-3, 9e-3)).validate()
+
+
+def test_batch_runs_generator():
+    """The uneven-run workload: seeded, deterministic, within its ranges."""
+    a = config.batch_cylindrical_runs(n=64)
+    b = config.batch_cylindrical_runs(n=64)
+    assert len(a) == 64
+    for x, y in zip(a, b):
+        assert x == y
+    for c in a:
+        c.validate()
+        z = c.domain_len[1]
+        assert 4e-3 <= z <= 16e-3 and c.domain_len[0] == 0.5 * z
+        assert 1.5e6 <= c.applied_fld <= 2.5e6
+        assert 1e15 <= c.bg_dens <= 1e16
+        assert c.dr_at(c.lvls_max) <= 4e-6 < c.dr_at(c.lvls_max - 1)
+        assert c.end_time == 5e-9 and c.photoi_enabled and c.is_cyl
+        assert c.seeds[0].r0 == (0.0, z - 1e-3)
+        assert all(0 < v < 2147483579 for v in c.rng_seed[:3])
+    assert len({c.rng_seed for c in a}) == 64
+    assert len({round(c.domain_len[1], 9) for c in a}) == 64
