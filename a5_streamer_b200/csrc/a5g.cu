@@ -103,6 +103,12 @@ struct RunDev {
   double lv_dr[MAXLEV];
   const BoxRec *boxes;
   const BoxRec *sboxes;        // records addressing the shared-memory copy
+  // cell plans and cylindrical weights of the shared-memory solve, built on
+  // the host per topology: level index li uses block cplan_blk[li] (2 NTHR
+  // entries), -1 where the level's colours do not fit one cell per thread
+  const int4 *cplan;
+  const double2 *cwts;
+  int cplan_blk[MAXLEV];
   const int *pbx;
   int smem_doubles;            // per multigrid variable; 0: tree does not fit
   int pad4;
@@ -748,7 +754,7 @@ __device__ __forceinline__ T lap_at(const RunDev &R, double V, const T *phi, con
 }
 
 struct LvlInfo {
-  int nc, ncg, sh, b0, nb;
+  int nc, ncg, sh, b0, nb, li;
   double dr;
 };
 __device__ __forceinline__ LvlInfo lvl_info(const RunDev &R, int lvl) {
@@ -759,6 +765,7 @@ __device__ __forceinline__ LvlInfo lvl_info(const RunDev &R, int lvl) {
   L.sh = 31 - __clz(L.nc);  // log2(nc)
   L.b0 = R.bx_off[li];
   L.nb = R.bx_off[li + 1] - L.b0;
+  L.li = li;
   L.dr = R.lv_dr[li];
   return L;
 }
@@ -1013,7 +1020,7 @@ enum { GK_COPY = 0, GK_RB = 1, GK_NEG = 2, GK_TOP = 3 };
 // of the x / y ghost neighbour, w = i | j << 8 | x kind << 16 | y kind << 18.
 
 // First source and kind of side ghost (side, k) of box B (as phi_ghost).
-__device__ __forceinline__ void ghost_src(const BoxRec &B, int nc, int ncg, int side, int k, int &s0,
+__host__ __device__ __forceinline__ void ghost_src(const BoxRec &B, int nc, int ncg, int side, int k, int &s0,
                                           int &kind) {
   const int dim = side >> 1;
   const bool low = (side & 1) == 0;
@@ -1033,7 +1040,7 @@ __device__ __forceinline__ void ghost_src(const BoxRec &B, int nc, int ncg, int 
   }
 }
 
-__device__ __forceinline__ int4 make_plan(const BoxRec &B, int nc, int ncg, int i, int j) {
+__host__ __device__ __forceinline__ int4 make_plan(const BoxRec &B, int nc, int ncg, int i, int j) {
   int4 c;
   c.x = B.base + i + ncg * j;
   int xk, yk;
@@ -1077,7 +1084,7 @@ __device__ __forceinline__ void plan_nbrs(double V, const T *phi, const int4 &c,
 }
 
 // box_gsrb_clpl weights (i+ioff-1)/(i+ioff-1/2) and (i+ioff)/(i+ioff-1/2)
-__device__ __forceinline__ void cyl_weights(int gi, double &rf1, double &rf2) {
+__host__ __device__ __forceinline__ void cyl_weights(int gi, double &rf1, double &rf2) {
   const double den = gi - 0.5;
   rf1 = (gi - 1) / den;
   rf2 = gi / den;
@@ -1105,12 +1112,26 @@ __device__ __forceinline__ bool plan_fits(const MGV<T> &M, const LvlInfo &L) {
 // Forms the thread's two cell plans (colour p = (i + j) & 1). Each thread
 // reads only its own slots afterwards, so no barrier is needed.
 template <class T>
-__device__ __forceinline__ LevelPlan make_level_plan(const MGV<T> &M, const LvlInfo &L, bool cyl) {
+__device__ __forceinline__ LevelPlan make_level_plan(const RunDev &R, const MGV<T> &M, const LvlInfo &L,
+                                                     bool cyl) {
   LevelPlan P;
   const int half = (L.nc * L.nc) >> 1, hsh = 2 * L.sh - 1, hn = L.nc >> 1;
   const int k = threadIdx.x;
   P.bx = -1;
   P.item = k & (half - 1);
+  if (k < L.nb * half) P.bx = L.b0 + (k >> hsh);
+  const int blk = R.cplan_blk[L.li];
+  if (blk >= 0) {
+    // plans of this level built on the host at the topology upload
+    const size_t o = (size_t)blk * 2 * NTHR + 2 * threadIdx.x;
+    plan_slots()[2 * threadIdx.x] = R.cplan[o];
+    plan_slots()[2 * threadIdx.x + 1] = R.cplan[o + 1];
+    if (cyl) {
+      wts_slots()[2 * threadIdx.x] = R.cwts[o];
+      wts_slots()[2 * threadIdx.x + 1] = R.cwts[o + 1];
+    }
+    return P;
+  }
   int4 c[2];
   c[0].x = c[1].x = -1;
   if (k < L.nb * half) {
@@ -1212,7 +1233,7 @@ __device__ void p_vcycle(const RunDev &R, const MGV<T> &M, int max_lvl, bool sta
   for (int lvl = max_lvl; lvl >= min_lvl + 1; lvl--) {
     const LvlInfo L = lvl_info(R, lvl);
     if (plan_fits(M, L)) {
-      const LevelPlan P = make_level_plan(M, L, R.coord == 1);
+      const LevelPlan P = make_level_plan(R, M, L, R.coord == 1);
       #pragma unroll 1
       for (int it = 1; it <= M.sw_down; it++) plan_sweep(R, M, L, P, it, false);
       plan_fr(R, M, L, P, lvl);
@@ -1225,7 +1246,7 @@ __device__ void p_vcycle(const RunDev &R, const MGV<T> &M, int max_lvl, bool sta
   {
     const LvlInfo L = lvl_info(R, min_lvl);
     if (plan_fits(M, L)) {
-      const LevelPlan P = make_level_plan(M, L, R.coord == 1);
+      const LevelPlan P = make_level_plan(R, M, L, R.coord == 1);
       #pragma unroll 1
       for (int it = 1; it <= M.sw_base; it++) plan_sweep(R, M, L, P, it, stale_base && it == 1);
     } else {
@@ -1236,7 +1257,7 @@ __device__ void p_vcycle(const RunDev &R, const MGV<T> &M, int max_lvl, bool sta
   for (int lvl = min_lvl + 1; lvl <= max_lvl; lvl++) {
     const LvlInfo L = lvl_info(R, lvl);
     if (plan_fits(M, L)) {
-      const LevelPlan P = make_level_plan(M, L, R.coord == 1);
+      const LevelPlan P = make_level_plan(R, M, L, R.coord == 1);
       p_correct(R, M, lvl, false, true);
       #pragma unroll 1
       for (int it = 1; it <= M.sw_up; it++) plan_sweep(R, M, L, P, it, false);
@@ -2555,6 +2576,9 @@ struct a5g_ctx {
   BoxRec *p_boxes = nullptr;
   int *p_pbx = nullptr;
   size_t cap_boxes = 0, cap_pbx = 0;
+  int4 *p_cplan = nullptr;
+  double2 *p_cwts = nullptr;
+  size_t cap_cplan = 0, cap_cwts = 0;
   // photoionization storage
   bool has_ph_table = false;
   double *ph_tbl = nullptr;
@@ -2603,6 +2627,9 @@ static size_t step_smem(const a5g_ctx *c) { return c->precision == A5G_MIXED ? c
 // lvls_max and for max_lvl+1 only).
 struct HostPlans {
   std::vector<BoxRec> boxes, sboxes;
+  std::vector<int4> cplan;      // per fitting level: 2 NTHR cell plans
+  std::vector<double2> cwts;    // and their cylindrical weights
+  int cplan_blk[MAXLEV];
   int smem_doubles = 0;  // doubles per variable of the compact shared-memory copy
   std::vector<int> pbx;
   int bx_off[MAXLEV + 1], pb_off[MAXLEV + 1];
@@ -2680,6 +2707,38 @@ static void build_plans(const std::vector<BoxMeta> &hm, const std::vector<std::v
       b.nb[q] = sb(b.nb[q]);
       b.pnb[q] = sb(b.pnb[q]);
       b.ch[q] = sb(b.ch[q]);
+    }
+  }
+  // Cell plans of every level whose colours have at most one cell per thread
+  // (the per-thread slots make_level_plan fills), on the shared-memory
+  // records: thread k takes cell item k & (half-1) of box k >> log2(half),
+  // its colour-0 and colour-1 cells in plan slots 2k and 2k+1.
+  P.cplan.clear();
+  P.cwts.clear();
+  for (int li = 0; li < MAXLEV; li++) P.cplan_blk[li] = -1;
+  for (int li = 0; li < nlev; li++) {
+    const int nc = P.lv_nc[li], ncg = nc + 2, half = (nc * nc) >> 1, hn = nc >> 1;
+    const int sh = __builtin_ctz(nc), hsh = 2 * sh - 1;
+    const int b0 = P.bx_off[li], nb = P.bx_off[li + 1] - b0;
+    if (nb * half > NTHR) continue;
+    P.cplan_blk[li] = (int)(P.cplan.size() / (2 * NTHR));
+    for (int k = 0; k < NTHR; k++) {
+      int4 c[2];
+      c[0] = c[1] = make_int4(-1, 0, 0, 0);
+      double2 w[2] = {make_double2(0, 0), make_double2(0, 0)};
+      if (k < nb * half) {
+        const BoxRec &B = P.sboxes[b0 + (k >> hsh)];
+        const int item = k & (half - 1);
+        const int j = (item >> (sh - 1)) + 1, m = item & (hn - 1);
+        for (int p = 0; p < 2; p++) {
+          c[p] = make_plan(B, nc, ncg, 2 * m + 2 - ((p + j) & 1), j);
+          cyl_weights(B.gi0 + (c[p].w & 255), w[p].x, w[p].y);
+        }
+      }
+      P.cplan.push_back(c[0]);
+      P.cplan.push_back(c[1]);
+      P.cwts.push_back(w[0]);
+      P.cwts.push_back(w[1]);
     }
   }
 }
@@ -3010,6 +3069,8 @@ int a5g_destroy(a5g_ctx *c) {
   cudaFree(c->p_boxes);
   cudaFree(c->p_sboxes);
   cudaFree(c->p_pbx);
+  cudaFree(c->p_cplan);
+  cudaFree(c->p_cwts);
   cudaFree(c->ph_tbl);
   cudaFree(c->ph_rng);
   cudaFree(c->ph_ncr);
@@ -3312,7 +3373,9 @@ int a5g_upload_tree(a5g_ctx *c, int max_id, int min_lvl, int max_lvl, const int 
   build_plans(hm, lv_ids, lv_leaves, lv_parents, min_lvl, nlev, c->p.dr_base, P);
   if ((r = upload_vec(c, c->p_boxes, c->cap_boxes, P.boxes)) ||
       (r = upload_vec(c, c->p_sboxes, c->cap_sboxes, P.sboxes)) ||
-      (r = upload_vec(c, c->p_pbx, c->cap_pbx, P.pbx)))
+      (r = upload_vec(c, c->p_pbx, c->cap_pbx, P.pbx)) ||
+      (r = upload_vec(c, c->p_cplan, c->cap_cplan, P.cplan)) ||
+      (r = upload_vec(c, c->p_cwts, c->cap_cwts, P.cwts)))
     return r;
   RunDev &h = c->h;
   {
@@ -3339,6 +3402,9 @@ int a5g_upload_tree(a5g_ctx *c, int max_id, int min_lvl, int max_lvl, const int 
   std::memcpy(h.lv_dr, P.lv_dr, sizeof(P.lv_dr));
   h.boxes = c->p_boxes;
   h.pbx = c->p_pbx;
+  h.cplan = c->p_cplan;
+  h.cwts = c->p_cwts;
+  std::memcpy(h.cplan_blk, P.cplan_blk, sizeof(P.cplan_blk));
   h.min_lvl = min_lvl;
   h.max_lvl = max_lvl;
   h.nlev = nlev;

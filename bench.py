@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="budget of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision form")
+    ap.add_argument("--mixed-schedule", default=None,
+                    help="fmg,down,up,base,corr: use this schedule instead of the autotuners' choice")
     ap.add_argument("--runs", type=int, default=64,
                     help="independent uneven runs of the device-driven batch (0: skip)")
     return ap.parse_args()
@@ -201,7 +203,7 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------
-def run_uneven_batch(n_runs, first_schedule):
+def run_uneven_batch(n_runs, first_schedule, fixed=False):
     """The batched form: n independent axisymmetric runs of uneven size
     (config.batch_cylindrical_runs: seeded background density, field, domain
     length; photoionization on) from their initial conditions to their own
@@ -215,15 +217,21 @@ def run_uneven_batch(n_runs, first_schedule):
     threads = os.cpu_count() or 1
     cands = [tuple(first_schedule)] + [c for c in [(0, 2, 2, 4, 1), (0, 2, 2, 4, 2), (1, 1, 1, 4, 1),
                                                     (1, 2, 2, 4, 1)] if c != tuple(first_schedule)]
-    tuned = autotune.tune_batch_schedule(cfgs, cands, n_threads=threads)
+    if fixed:
+        tuned = {"schedule": tuple(first_schedule), "errors": None, "tried": []}
+    else:
+        tuned = autotune.tune_batch_schedule(cfgs, cands, n_threads=threads)
     sched = tuned["schedule"]
     out = {"runs": n_runs, "generator": "numpy default_rng(20261203)", "t_end": cfgs[0].end_time,
            "domain_z_mm": [min(c.domain_len[1] for c in cfgs) * 1e3, max(c.domain_len[1] for c in cfgs) * 1e3],
            "photoionization": True}
     heads = {}
+    import torch
     for form, sc in (("fp64", None), ("mixed", sched)):
         t0 = time.perf_counter()
+        torch.cuda.nvtx.range_push(f"uneven_{form}")
         h, (nb, gpu_ms, host_ms, cu) = autotune.batch_observables(cfgs, sc, n_threads=threads)
+        torch.cuda.nvtx.range_pop()
         heads[form] = h
         out[form] = {"value": cu / (gpu_ms / 1e3), "unit": UNIT, "device_s": gpu_ms / 1e3,
                      "host_regrid_s": host_ms / 1e3, "blocks": nb, "cell_updates": cu,
@@ -343,7 +351,7 @@ def run_b200(args):
                 "unit": UNIT, "ms_per_step": 1e3 * bt / nb,
                 "achieved_gbs": bytes_step * len(reps) * nb / bt / 1e9}
 
-    def time_single(r):
+    def time_single(r, label):
         """K steps of one run, L2 flushed before each, CUDA events on its stream."""
         st = torch.cuda.ExternalStream(r.stream_ptr())
         for _ in range(args.warmup):
@@ -351,12 +359,14 @@ def run_b200(args):
         r.sync()
         a0 = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
         a1 = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+        torch.cuda.nvtx.range_push(label)
         with torch.cuda.stream(st):
             for k in range(K):
                 flush.fill_(k & 0xFF)
                 a0[k].record(st)
                 r.step(dt)
                 a1[k].record(st)
+        torch.cuda.nvtx.range_pop()
         r.sync()
         torch.cuda.synchronize()
         return sum(a.elapsed_time(b) for a, b in zip(a0, a1)) / K
@@ -370,10 +380,14 @@ def run_b200(args):
     if not args.no_mixed:
         from a5_streamer_b200 import autotune
         import dataclasses
-        tuned = autotune.tune_schedule(sim, ref_head=head_fp64)
-        sched = tuned["schedule"]
+        if args.mixed_schedule:
+            sched = tuple(int(v) for v in args.mixed_schedule.split(","))
+            tuned = {"schedule": sched, "table": [], "n_steps": 0}
+        else:
+            tuned = autotune.tune_schedule(sim, ref_head=head_fp64)
+            sched = tuned["schedule"]
         mrun = dv.clone_state(sim, mixed=True, schedule=sched)
-        m_ms = time_single(mrun)
+        m_ms = time_single(mrun, "timed_mixed")
         mrun.close()
         # K steps on the frozen mesh, photoionization off in both copies (the
         # photon counts are stochastic and would diverge between the two)
@@ -413,7 +427,7 @@ def run_b200(args):
         sched_u = mixed["schedule"] if mixed else None
         sched_u = (sched_u["fmg"], sched_u["n_cycle_down"], sched_u["n_cycle_up"], sched_u["n_cycle_base"],
                    sched_u["n_corr"]) if sched_u else (1, 2, 2, cfg.n_cycle_base, 1)
-        uneven = run_uneven_batch(args.runs, sched_u)
+        uneven = run_uneven_batch(args.runs, sched_u, fixed=bool(args.mixed_schedule))
 
     peak, peak_kind = measured_peak()
     achieved = bytes_step / (ms_per_step / 1e3) / 1e9
