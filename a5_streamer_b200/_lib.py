@@ -118,7 +118,9 @@ SIGNATURES = {
     "a5s_advance": (_I, [_P, _I, _PD]),
     "a5s_run": (_I, [_P, _D, _I, _PI]),
     "a5s_time": (_I, [_P, _PD]),
-    "a5s_batch_run": (_I, [ctypes.POINTER(_P), _I, _PD, _I, _I, _I, _PI, _PD, _PD, _PD]),
+    "a5s_batch_run": (_I, [ctypes.POINTER(_P), _I, _PD, _I, _I, _I, _I, _PI, _PD, _PD, _PD]),
+    "a5g_batch_launch": (_I, [_P, _I, _I]),
+    "a5g_batch_finish": (_I, [_P, _PD, _PD, _PI, ctypes.POINTER(ctypes.c_float)]),
     "a5s_ctx": (_I, [_P, ctypes.POINTER(_P)]),
     "a5s_tree": (_I, [_P, ctypes.POINTER(_P)]),
     "a5s_table": (_I, [_P, _PD, _PD, _PD, _PI]),

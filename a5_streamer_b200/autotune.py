@@ -188,11 +188,13 @@ def tune_schedule(sim, n_steps: int = 20, tol_max_E: float = 1e-4, tol_head_z: f
             "table": table}
 
 
-def batch_observables(cfgs, schedule=None, use_graph: bool = True, n_threads: int = 8):
+def batch_observables(cfgs, schedule=None, use_graph: bool = True, n_threads: int = 8,
+                      groups: int = 1):
     """Run ``cfgs`` from their initial conditions to their end times as one
-    device-driven batch (FP64, or mixed with ``schedule``). Returns the
-    per-run head observables and the batch counters (blocks, device ms, host
-    ms, cell updates)."""
+    device-driven batch (FP64, or mixed with ``schedule``; ``groups``
+    pipelined batches). Returns the per-run head observables, the batch
+    counters (blocks, device ms, host ms, cell updates) and the wall time (s)
+    of the batched run."""
     from .streamer import Simulation, run_batch
     sims = [Simulation(c) for c in cfgs]
     try:
@@ -200,13 +202,16 @@ def batch_observables(cfgs, schedule=None, use_graph: bool = True, n_threads: in
             if schedule is not None:
                 s.device.set_precision(True, schedule)
             s.init()
+        import time
+        t0 = time.perf_counter()
         counters = run_batch(sims, [c.end_time for c in cfgs], use_graph=use_graph,
-                             n_threads=n_threads)
+                             n_threads=n_threads, groups=groups)
+        wall = time.perf_counter() - t0
         heads = []
         for s, c in zip(sims, cfgs):
             meta, geom, levels = s.tree.export()
             heads.append(metrics.head_observables(s.device.cc(I_FLD), meta, geom, levels, c))
-        return heads, counters
+        return heads, counters, wall
     finally:
         for s in sims:
             s.close()
@@ -223,10 +228,10 @@ def tune_batch_schedule(cfgs, candidates: Sequence[Schedule], tol_max_E: float =
     candidate qualifies, the last one."""
     import dataclasses
     quiet = [dataclasses.replace(c, photoi_enabled=False) for c in cfgs]
-    ref, _ = batch_observables(quiet, None, n_threads=n_threads)
+    ref, _, _ = batch_observables(quiet, None, n_threads=n_threads)
     tried = []
     for sched in candidates:
-        heads, _ = batch_observables(quiet, tuple(sched), n_threads=n_threads)
+        heads, _, _ = batch_observables(quiet, tuple(sched), n_threads=n_threads)
         zr = [abs(a[0] - b[0]) / abs(a[0]) for a, b in zip(ref, heads)]
         er = [abs(a[2] - b[2]) / a[2] for a, b in zip(ref, heads)]
         ok = max(zr) <= tol_head_z and max(er) <= tol_max_E

@@ -2521,6 +2521,18 @@ __global__ void __launch_bounds__(PH_THREADS) a5g_photon_kernel(const RunDev *si
   }
 }
 
+// Block state of every member of a device-driven batch gathered into one
+// array (5 doubles per run: dt, time, end time, active, device status), so
+// that the host reads a whole batch with a single copy.
+__global__ void a5g_batch_gather_kernel(const RunDev *const *runs, int n, double *out) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const RunDev *r = runs[k];
+#pragma unroll
+    for (int q = 0; q < 4; q++) out[5 * k + q] = r->blk[q];
+    out[5 * k + 4] = (double)*r->status;
+  }
+}
+
 }  // namespace
 
 // Descriptor table of a5g_step_batch_static: a fixed device array, so that
@@ -3798,7 +3810,8 @@ struct a5g_batch {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int graph_steps = -1;
-  double *h_state = nullptr;  // pinned, 4 per run
+  double *h_state = nullptr;  // pinned, 5 per run (a5g_batch_gather_kernel)
+  double *d_state = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
@@ -3881,7 +3894,8 @@ int a5g_batch_create(a5g_ctx **ctxs, int n, a5g_batch **out) {
   if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaMalloc(&b->d_rp, n * sizeof(void *)) != cudaSuccess ||
       cudaMalloc(&b->d_ops, 3 * n * sizeof(Op)) != cudaSuccess ||
-      cudaMallocHost(&b->h_state, 4 * n * sizeof(double)) != cudaSuccess ||
+      cudaMallocHost(&b->h_state, 5 * n * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&b->d_state, 5 * n * sizeof(double)) != cudaSuccess ||
       cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess) {
     a5g_batch_destroy(b);
     return fail(A5G_ENOMEM, "cannot allocate the batch");
@@ -3902,6 +3916,7 @@ int a5g_batch_destroy(a5g_batch *b) {
   cudaFree(b->d_rp);
   cudaFree(b->d_ops);
   if (b->h_state) cudaFreeHost(b->h_state);
+  cudaFree(b->d_state);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
   if (b->stream) cudaStreamDestroy(b->stream);
@@ -3920,8 +3935,7 @@ int a5g_batch_begin(a5g_batch *b, const double *time, const double *t_end) {
   return batch_build_ops(b);
 }
 
-int a5g_batch_block(a5g_batch *b, int num_steps, int use_graph, double *dt, double *time,
-                    int *active, float *gpu_ms) {
+int a5g_batch_launch(a5g_batch *b, int num_steps, int use_graph) {
   if (!b || num_steps < 1) return fail(A5G_EINVAL, "bad argument");
   const int n = (int)b->ctxs.size();
   for (int k = 0; k < n; k++) {
@@ -3955,19 +3969,35 @@ int a5g_batch_block(a5g_batch *b, int num_steps, int use_graph, double *dt, doub
     if (r) return r;
   }
   CK(cudaEventRecord(b->ev1, b->stream));
-  for (int k = 0; k < n; k++)
-    CK(cudaMemcpyAsync(b->h_state + 4 * k, b->ctxs[k]->scal + 8, 4 * sizeof(double),
-                       cudaMemcpyDeviceToHost, b->stream));
+  a5g_batch_gather_kernel<<<(n + 127) / 128, 128, 0, b->stream>>>(b->d_rp, n, b->d_state);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(b->h_state, b->d_state, 5 * n * sizeof(double), cudaMemcpyDeviceToHost,
+                     b->stream));
+  return A5G_OK;
+}
+
+int a5g_batch_finish(a5g_batch *b, double *dt, double *time, int *active, float *gpu_ms) {
+  if (!b) return fail(A5G_EINVAL, "null batch");
+  const int n = (int)b->ctxs.size();
   CK(cudaStreamSynchronize(b->stream));
   for (int k = 0; k < n; k++) {
-    int r = check_status(b->ctxs[k]);
-    if (r) return r;
-    if (dt) dt[k] = b->h_state[4 * k];
-    if (time) time[k] = b->h_state[4 * k + 1];
-    if (active) active[k] = b->h_state[4 * k + 3] != 0.0;
+    if (b->h_state[5 * k + 4] != 0.0) {
+      int r = check_status(b->ctxs[k]);  // reports and clears the status word
+      if (r) return r;
+    }
+    if (dt) dt[k] = b->h_state[5 * k];
+    if (time) time[k] = b->h_state[5 * k + 1];
+    if (active) active[k] = b->h_state[5 * k + 3] != 0.0;
   }
   if (gpu_ms) CK(cudaEventElapsedTime(gpu_ms, b->ev0, b->ev1));
   return A5G_OK;
+}
+
+int a5g_batch_block(a5g_batch *b, int num_steps, int use_graph, double *dt, double *time,
+                    int *active, float *gpu_ms) {
+  int r = a5g_batch_launch(b, num_steps, use_graph);
+  if (r) return r;
+  return a5g_batch_finish(b, dt, time, active, gpu_ms);
 }
 
 // Diagnostics: allow (1) or forbid (0) the shared-memory staging of the

@@ -10,7 +10,10 @@
 #include <chrono>
 #include <climits>
 #include <cmath>
+#include <condition_variable>
 #include <cstring>
+#include <functional>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -727,76 +730,173 @@ int a5s_run(a5s_sim *s, double t_end, int max_blocks, int *n_blocks) {
   return a5g_sync(s->ctx);
 }
 
+// Worker threads that run one job at a time together with the caller: run(f)
+// hands f to every worker, runs it on the calling thread too and returns once
+// every worker has finished it (jobs share their work through a counter).
+class WorkerPool {
+ public:
+  explicit WorkerPool(int n_threads) {
+    for (int t = 1; t < n_threads; t++) th_.emplace_back([this] { loop(); });
+  }
+  ~WorkerPool() {
+    {
+      std::lock_guard<std::mutex> l(mu_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto &t : th_) t.join();
+  }
+  void run(const std::function<void()> &f) {
+    {
+      std::lock_guard<std::mutex> l(mu_);
+      job_ = f;
+      gen_++;
+      pending_ = (int)th_.size();
+    }
+    cv_.notify_all();
+    f();
+    std::unique_lock<std::mutex> l(mu_);
+    done_.wait(l, [&] { return pending_ == 0; });
+  }
+
+ private:
+  void loop() {
+    long seen = 0;
+    for (;;) {
+      std::function<void()> j;
+      {
+        std::unique_lock<std::mutex> l(mu_);
+        cv_.wait(l, [&] { return stop_ || gen_ != seen; });
+        if (stop_) return;
+        seen = gen_;
+        j = job_;
+      }
+      j();
+      std::lock_guard<std::mutex> l(mu_);
+      if (--pending_ == 0) done_.notify_all();
+    }
+  }
+  std::vector<std::thread> th_;
+  std::mutex mu_;
+  std::condition_variable cv_, done_;
+  std::function<void()> job_;
+  long gen_ = 0;
+  int pending_ = 0;
+  bool stop_ = false;
+};
+
+// Regrid the given members on the pool's threads (trees and contexts are
+// independent; each context works on its own stream), and wait for them.
+static int regrid_members(a5s_sim **sims, const std::vector<int> &todo, WorkerPool &pool) {
+  std::atomic<size_t> next{0};
+  std::vector<int> rc(todo.size(), A5G_OK);
+  std::vector<std::string> msg(todo.size());
+  pool.run([&]() {
+    size_t i;
+    while ((i = next++) < todo.size()) {
+      rc[i] = regrid_block(sims[todo[i]]);
+      if (!rc[i]) rc[i] = a5g_sync(sims[todo[i]]->ctx);
+      if (rc[i]) msg[i] = a5g_last_error();
+    }
+  });
+  for (size_t i = 0; i < todo.size(); i++)
+    if (rc[i]) return err(rc[i], "regrid of batch member " + std::to_string(todo[i]) + ": " + msg[i]);
+  return A5G_OK;
+}
+
 int a5s_batch_run(a5s_sim **sims, int n, const double *t_end, int use_graph, int n_threads,
-                  int max_blocks, int *n_blocks, double *gpu_ms, double *host_ms,
+                  int n_groups, int max_blocks, int *n_blocks, double *gpu_ms, double *host_ms,
                   double *cell_updates) {
   if (!sims || !t_end || n < 1) return err(A5G_EINVAL, "bad batch");
+  if (n_groups < 1) return err(A5G_EINVAL, "n_groups must be >= 1");
   for (int k = 0; k < n; k++) {
     if (!sims[k]) return err(A5G_EINVAL, "null sim in batch");
     if (sims[k]->cfg.num_steps_amr != sims[0]->cfg.num_steps_amr)
       return err(A5G_EINVAL, "batch members need the same num_steps_amr");
   }
-  std::vector<a5g_ctx *> ctxs(n);
-  std::vector<double> dt(n), tm(n);
-  std::vector<int> act(n);
-  for (int k = 0; k < n; k++) {
-    ctxs[k] = sims[k]->ctx;
-    tm[k] = sims[k]->time;
-  }
-  a5g_batch *b = nullptr;
-  int r = a5g_batch_create(ctxs.data(), n, &b);
-  if (r) return r;
-  if ((r = a5g_batch_begin(b, tm.data(), t_end))) {
-    a5g_batch_destroy(b);
-    return r;
-  }
+  // members are dealt to groups in turn; each group is a batch of its own
+  // with its own stream, so that one group's block runs on the device while
+  // the host regrids another group's runs
+  const int G = std::min(n_groups, n);
+  struct Group {
+    std::vector<int> mem;
+    a5g_batch *b = nullptr;
+    std::vector<double> dt, tm;
+    std::vector<int> act;
+    std::vector<long long> leaves;
+    int blocks = 0;
+    bool done = false;
+  };
+  std::vector<Group> g(G);
+  for (int k = 0; k < n; k++) g[k % G].mem.push_back(k);
   const int steps = sims[0]->cfg.num_steps_amr;
-  int nb = 0;
-  double g_ms = 0, h_ms = 0, cu = 0;
-  std::vector<long long> leaves(n, 0);
-  while (nb < max_blocks) {
-    for (int k = 0; k < n; k++) a5g_n_leaf_cells(ctxs[k], &leaves[k]);
-    float ms = 0;
-    if ((r = a5g_batch_block(b, steps, use_graph, dt.data(), tm.data(), act.data(), &ms))) break;
-    g_ms += ms;
-    std::vector<int> todo;
-    for (int k = 0; k < n; k++) {
-      sims[k]->time = tm[k];
-      if (act[k]) {
-        todo.push_back(k);
-        cu += (double)leaves[k] * steps;
-      }
+  int r = A5G_OK;
+  for (auto &q : g) {
+    const int m = (int)q.mem.size();
+    std::vector<a5g_ctx *> ctxs(m);
+    std::vector<double> te(m);
+    q.dt.assign(m, 0);
+    q.tm.assign(m, 0);
+    q.act.assign(m, 0);
+    q.leaves.assign(m, 0);
+    for (int i = 0; i < m; i++) {
+      ctxs[i] = sims[q.mem[i]]->ctx;
+      q.tm[i] = sims[q.mem[i]]->time;
+      te[i] = t_end[q.mem[i]];
     }
-    if (todo.empty()) break;
-    nb++;
-    // regrid the runs that stepped, n_threads at a time (trees and contexts
-    // are independent; each context works on its own stream)
-    const auto t0 = std::chrono::steady_clock::now();
-    std::atomic<size_t> next{0};
-    std::vector<int> rc(todo.size(), A5G_OK);
-    std::vector<std::string> msg(todo.size());
-    auto work = [&]() {
-      size_t i;
-      while ((i = next++) < todo.size()) {
-        rc[i] = regrid_block(sims[todo[i]]);
-        if (rc[i]) msg[i] = a5g_last_error();
-      }
-    };
-    const int nt = std::max(1, std::min(n_threads, (int)todo.size()));
-    std::vector<std::thread> th;
-    for (int t = 1; t < nt; t++) th.emplace_back(work);
-    work();
-    for (auto &t : th) t.join();
-    for (int k = 0; k < n; k++) {
-      int e = a5g_sync(ctxs[k]);
-      if (e && !r) r = e;
-    }
-    h_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-    for (size_t i = 0; i < todo.size() && !r; i++)
-      if (rc[i]) r = err(rc[i], "regrid of batch member " + std::to_string(todo[i]) + ": " + msg[i]);
-    if (r) break;
+    if ((r = a5g_batch_create(ctxs.data(), m, &q.b)) || (r = a5g_batch_begin(q.b, q.tm.data(), te.data())))
+      break;
   }
-  a5g_batch_destroy(b);
+  double g_ms = 0, h_ms = 0, cu = 0;
+  WorkerPool pool(std::max(1, std::min(n_threads, n)));
+  auto launch = [&](Group &q) {
+    for (size_t i = 0; i < q.mem.size(); i++) a5g_n_leaf_cells(sims[q.mem[i]]->ctx, &q.leaves[i]);
+    return a5g_batch_launch(q.b, steps, use_graph);
+  };
+  if (!r)
+    for (auto &q : g)
+      if ((r = launch(q))) break;
+  bool any = true;
+  while (!r && any) {
+    any = false;
+    for (auto &q : g) {
+      if (q.done) continue;
+      float ms = 0;
+      if ((r = a5g_batch_finish(q.b, q.dt.data(), q.tm.data(), q.act.data(), &ms))) break;
+      g_ms += ms;
+      std::vector<int> todo;
+      for (size_t i = 0; i < q.mem.size(); i++) {
+        sims[q.mem[i]]->time = q.tm[i];
+        if (q.act[i]) {
+          todo.push_back(q.mem[i]);
+          cu += (double)q.leaves[i] * steps;
+        }
+      }
+      if (todo.empty()) {
+        q.done = true;
+        continue;
+      }
+      q.blocks++;
+      const auto t0 = std::chrono::steady_clock::now();
+      r = regrid_members(sims, todo, pool);
+      h_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+      if (r) break;
+      if (q.blocks >= max_blocks) {
+        q.done = true;
+        continue;
+      }
+      if ((r = launch(q))) break;
+      any = true;
+    }
+  }
+  int nb = 0;
+  for (auto &q : g) {
+    if (q.b) {
+      if (r) a5g_batch_finish(q.b, nullptr, nullptr, nullptr, nullptr);  // drain before destroying
+      a5g_batch_destroy(q.b);
+    }
+    nb = std::max(nb, q.blocks);
+  }
   if (n_blocks) *n_blocks = nb;
   if (gpu_ms) *gpu_ms = g_ms;
   if (host_ms) *host_ms = h_ms;

@@ -218,12 +218,14 @@ class Simulation:
         return rc.reshape(4, n.value).T.copy(), xm.value, inv.value
 
 
-def run_batch(sims, t_end, use_graph: bool = True, n_threads: int = 8,
+def run_batch(sims, t_end, use_graph: bool = True, n_threads: int = 8, groups: int = 1,
               max_blocks: int = 1 << 30):
     """Run several simulations to their end times as one device-driven batch
     (include/a5t.h a5s_batch_run): per main-loop block one launch per kernel
     for all runs, replayed from a CUDA graph when ``use_graph``, regrids on
-    the host in ``n_threads`` threads. Each run ends in the state
+    the host in ``n_threads`` threads; with ``groups`` > 1 the runs are dealt
+    to that many batches whose regrids overlap the others' device work. Each
+    run ends in the state
     ``Simulation.run(t_end[k])`` gives it. Returns (blocks, device ms of the
     blocks, host ms of the regrids, leaf-cell updates over all runs)."""
     n = len(sims)
@@ -233,7 +235,8 @@ def run_batch(sims, t_end, use_graph: bool = True, n_threads: int = 8,
     te = np.ascontiguousarray(t_end, dtype=np.float64)
     nb = ctypes.c_int(0)
     g_ms, h_ms, cu = ctypes.c_double(0), ctypes.c_double(0), ctypes.c_double(0)
-    call("a5s_batch_run", arr, n, _dp(te), 1 if use_graph else 0, int(n_threads), int(max_blocks),
+    call("a5s_batch_run", arr, n, _dp(te), 1 if use_graph else 0, int(n_threads), int(groups),
+         int(max_blocks),
          ctypes.byref(nb), ctypes.byref(g_ms), ctypes.byref(h_ms), ctypes.byref(cu))
     for s in sims:
         s._refresh_view()

@@ -263,6 +263,11 @@ int a5g_batch_destroy(a5g_batch *b);
 int a5g_batch_begin(a5g_batch *b, const double *time, const double *t_end);
 int a5g_batch_block(a5g_batch *b, int num_steps, int use_graph, double *dt, double *time,
                     int *active, float *gpu_ms);
+/* a5g_batch_block in two halves: launch queues the block on the batch's own
+ * stream and returns; finish waits for it and returns its results. Between
+ * the two the host may work on other batches (e.g. regrid their runs). */
+int a5g_batch_launch(a5g_batch *b, int num_steps, int use_graph);
+int a5g_batch_finish(a5g_batch *b, double *dt, double *time, int *active, float *gpu_ms);
 /* Wait for all work queued on the context's stream. */
 int a5g_sync(a5g_ctx *ctx);
 /* The cudaStream_t (as void*) all work of this context is queued on, so a

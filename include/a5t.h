@@ -87,16 +87,19 @@ int a5s_init(a5s_sim *s, int *n_iter);
 int a5s_advance(a5s_sim *s, int regrid, double *dt_used);
 /* Main loop until time > t_end (or max_blocks blocks). */
 int a5s_run(a5s_sim *s, double t_end, int max_blocks, int *n_blocks);
-/* Main loop of n runs as one device-driven batch until each run's
+/* Main loop of n runs as device-driven batches until each run's
  * time > t_end[k]: per block, each run's get_max_dt and its num_steps_amr
- * steps run for all members in one launch per kernel (replayed from a CUDA
- * graph when use_graph), then the runs that stepped are regridded on the
- * host, n_threads at a time. Each run ends in the state a5s_run(t_end[k])
- * gives it. gpu_ms: device time of the blocks; host_ms: wall time of the
- * regrids; cell_updates: leaf cells times steps over all members. Members
- * share num_steps_amr and the current device. */
+ * steps run for all members of a batch in one launch per kernel (replayed
+ * from a CUDA graph when use_graph), then the runs that stepped are
+ * regridded on the host, n_threads at a time. With n_groups > 1 the members
+ * are dealt to that many batches, each on its own stream, and a group's
+ * regrids overlap the other groups' blocks on the device. Each run ends in
+ * the state a5s_run(t_end[k]) gives it. gpu_ms: sum of the blocks' device
+ * times (groups overlap); host_ms: wall time of the regrids; cell_updates:
+ * leaf cells times steps over all members. Members share num_steps_amr and
+ * the current device. */
 int a5s_batch_run(a5s_sim **sims, int n, const double *t_end, int use_graph, int n_threads,
-                  int max_blocks, int *n_blocks, double *gpu_ms, double *host_ms,
+                  int n_groups, int max_blocks, int *n_blocks, double *gpu_ms, double *host_ms,
                   double *cell_updates);
 int a5s_time(a5s_sim *s, double *t);
 int a5s_ctx(a5s_sim *s, a5g_ctx **ctx);

@@ -35,9 +35,9 @@ def _same(a, b, where):
             assert np.array_equal(a.device.fc(d, f), b.device.fc(d, f)), f"{where}: face {d} {f}"
 
 
-@pytest.mark.parametrize("use_graph", [False, True])
+@pytest.mark.parametrize("use_graph,groups", [(False, 1), (True, 1), (True, 2)])
 @pytest.mark.parametrize("mixed", [False, True])
-def test_batch_equals_single_runs(use_graph, mixed):
+def test_batch_equals_single_runs(use_graph, groups, mixed):
     cfgs = _members()
     sched = (0, 1, 1, 4, 1)
     batch = [streamer.Simulation(c) for c in cfgs]
@@ -47,7 +47,7 @@ def test_batch_equals_single_runs(use_graph, mixed):
             s.device.set_precision(True, sched)
         s.init()
     nb, gpu_ms, host_ms, cu = streamer.run_batch(batch, [c.end_time for c in cfgs],
-                                                 use_graph=use_graph, n_threads=4)
+                                                 use_graph=use_graph, n_threads=4, groups=groups)
     assert nb > 0 and gpu_ms > 0 and cu > 0
     for k, (s, c) in enumerate(zip(alone, cfgs)):
         s.run(c.end_time)
