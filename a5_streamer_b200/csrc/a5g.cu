@@ -480,7 +480,7 @@ __device__ void fluxes_koren(const RunDev &R, double dt) {
       const int g = xd ? f : f - nf;
       int i, j;
       if (xd) { i = g % (nc + 1) + 1; j = g / (nc + 1) + 1; }
-      else { i = g % nc + 1; j = g / nc + 1; }
+      else { i = (g & (nc - 1)) + 1; j = (g >> (31 - __clz(nc))) + 1; }
       // stride between the two cells adjacent to the face
       const int s = xd ? 1 : ncg;
       const int c = i + ncg * j;          // cell (i, j): high side of the face
@@ -560,7 +560,7 @@ __device__ void update_solution(const RunDev &R, double dt) {
     const BoxMeta &m = R.meta[id];
     const int nc = m.nc, ncg = nc + 2;
     if (t >= nc * nc) return;
-    const int i = t % nc + 1, j = t / nc + 1, c = i + ncg * j;
+    const int i = (t & (nc - 1)) + 1, j = (t >> (31 - __clz(nc))) + 1, c = i + ncg * j;
     const T inv_dr = T(1 / m.dr);
     double *e = CC(R, I_ELEC, id), *pi = CC(R, I_PION, id);
     const double *fxe = FX(R, F_ELEC, id), *fye = FY(R, F_ELEC, id);
@@ -821,8 +821,8 @@ __device__ __forceinline__ void fill_phi_loop(const RunDev &R, const MGV<T> &M, 
   T *phi = M.phi, *tmp = M.tmp;
   const int per = 4 * L.nc, n = L.nb * per;
   for (int k = threadIdx.x; k < n; k += NTHR) {
-    const BoxRec &B = M.boxes[L.b0 + k / per];
-    const int r = k % per, side = r >> L.sh, kk = (r & (L.nc - 1)) + 1;
+    const BoxRec &B = M.boxes[L.b0 + (k >> (L.sh + 2))];
+    const int r = k & (per - 1), side = r >> L.sh, kk = (r & (L.nc - 1)) + 1;
     const T v = phi_ghost(M.V, phi, B, L.nc, L.ncg, side, kk);
     const int dim = side >> 1, gx = (side & 1) ? L.nc + 1 : 0;
     const int d = B.base + (dim == 0 ? gx + L.ncg * kk : kk + L.ncg * gx);
@@ -854,8 +854,8 @@ __device__ __noinline__ void p_fr(const RunDev &R, const MGV<T> &M, int lvl, boo
   const double fac = UC_ELEM_CHARGE / UC_EPS0;
   const int hn = L.nc >> 1, per = hn * hn, n = L.nb * per;
   for (int k = threadIdx.x; k < n; k += NTHR) {
-    const BoxRec &B = M.boxes[L.b0 + k / per];
-    const int t = k % per, ii = t % hn + 1, jj = t / hn + 1;
+    const BoxRec &B = M.boxes[L.b0 + (k >> (2 * L.sh - 2))];
+    const int t = k & (per - 1), ii = (t & (hn - 1)) + 1, jj = (t >> (L.sh - 1)) + 1;
     const bool leaf = leaf_rhs && (B.flags & CF_LEAF);
     T rs[4], ps[4];
 #pragma unroll
@@ -938,8 +938,8 @@ __device__ void p_correct(const RunDev &R, const MGV<T> &M, int lvl, bool copy, 
   if (copy) {
     const int pg = 4 * L.nc, ng = L.nb * pg;
     for (int k = threadIdx.x; k < ng; k += NTHR) {
-      const BoxRec &B = M.boxes[L.b0 + k / pg];
-      const int r = k % pg, side = r >> L.sh, kk = (r & (L.nc - 1)) + 1;
+      const BoxRec &B = M.boxes[L.b0 + (k >> (L.sh + 2))];
+      const int r = k & (pg - 1), side = r >> L.sh, kk = (r & (L.nc - 1)) + 1;
       const int dim = side >> 1, gx = (side & 1) ? L.nc + 1 : 0;
       const int d = B.base + (dim == 0 ? gx + L.ncg * kk : kk + L.ncg * gx);
       tmp[d] = phi[d];
@@ -959,8 +959,8 @@ __device__ __noinline__ void p_init_level(const RunDev &R, const MGV<T> &M, int 
   const double fac = UC_ELEM_CHARGE / UC_EPS0;
   const int hn = L.nc >> 1, per = hn * hn, n = L.nb * per;
   for (int k = threadIdx.x; k < n; k += NTHR) {
-    const BoxRec &B = M.boxes[L.b0 + k / per];
-    const int t = k % per, ii = t % hn + 1, jj = t / hn + 1;
+    const BoxRec &B = M.boxes[L.b0 + (k >> (2 * L.sh - 2))];
+    const int t = k & (per - 1), ii = (t & (hn - 1)) + 1, jj = (t >> (L.sh - 1)) + 1;
     const bool leaf = leaf_rhs && (B.flags & CF_LEAF);
     T rs[4];
 #pragma unroll
@@ -1373,10 +1373,10 @@ __device__ __noinline__ void p_mx_residual(const RunDev &R, const MGV<float> &M,
   const double fac = UC_ELEM_CHARGE / UC_EPS0;
   const int hn = L.nc >> 1, per = hn * hn, n = L.nb * per;
   for (int k = threadIdx.x; k < n; k += NTHR) {
-    const int b = L.b0 + k / per;
+    const int b = L.b0 + (k >> (2 * L.sh - 2));
     const BoxRec &B = R.boxes[b];  // device-memory slots (phi, rhs, densities)
     const BoxRec &S = M.boxes[b];  // slots of the FP32 arrays
-    const int t = k % per, ii = t % hn + 1, jj = t / hn + 1;
+    const int t = k & (per - 1), ii = (t & (hn - 1)) + 1, jj = (t >> (L.sh - 1)) + 1;
     const bool leaf = (B.flags & CF_LEAF) != 0;
     double rs[4], ps[4], hs[4];
 #pragma unroll
@@ -1409,8 +1409,8 @@ __device__ __noinline__ void p_mx_residual(const RunDev &R, const MGV<float> &M,
   // side ghosts of c and of its tmp start at zero (consistent with c = 0 and V = 0)
   const int pg = 4 * L.nc, ng = L.nb * pg;
   for (int k = threadIdx.x; k < ng; k += NTHR) {
-    const BoxRec &S = M.boxes[L.b0 + k / pg];
-    const int r = k % pg, side = r >> L.sh, kk = (r & (L.nc - 1)) + 1;
+    const BoxRec &S = M.boxes[L.b0 + (k >> (L.sh + 2))];
+    const int r = k & (pg - 1), side = r >> L.sh, kk = (r & (L.nc - 1)) + 1;
     const int dim = side >> 1, gx = (side & 1) ? L.nc + 1 : 0;
     const int d = S.base + (dim == 0 ? gx + L.ncg * kk : kk + L.ncg * gx);
     ce[d] = 0.0f;
@@ -1479,8 +1479,8 @@ __device__ void p_gc_den(const RunDev &R, int iv0, int iv1, bool lim) {
     const LvlInfo L = lvl_info(R, lvl);
     const int per = 4 * L.nc, n = L.nb * per;
     for (int k = threadIdx.x; k < n; k += NTHR) {
-      const BoxRec &B = R.boxes[L.b0 + k / per];
-      const int r = k % per, side = r >> L.sh, kk = (r & (L.nc - 1)) + 1;
+      const BoxRec &B = R.boxes[L.b0 + (k >> (L.sh + 2))];
+      const int r = k & (per - 1), side = r >> L.sh, kk = (r & (L.nc - 1)) + 1;
       const int dim = side >> 1, gx = (side & 1) ? L.nc + 1 : 0;
       const int d = B.base + (dim == 0 ? gx + L.ncg * kk : kk + L.ncg * gx);
       for (int w = 0; w < 2; w++) {
@@ -1632,7 +1632,7 @@ __device__ void dt_reductions(const RunDev &R) {
     const BoxMeta &m = R.meta[id];
     const int nc = m.nc;
     if (t >= nc * nc) return;
-    const int c = (t % nc + 1) + (nc + 2) * (t / nc + 1);
+    const int c = ((t & (nc - 1)) + 1) + (nc + 2) * ((t >> (31 - __clz(nc))) + 1);
     double f = CC(R, I_FLD, id)[c];
     mx = dmax(mx, f);
     mn = dmin(mn, f);
