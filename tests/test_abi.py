@@ -56,3 +56,28 @@ def test_error_raises_with_status_name():
     with pytest.raises(_lib.A5GError) as e:
         _lib.call("a5g_step", None, 1e-12)
     assert "A5G_EINVAL" in str(e.value)
+
+
+def test_new_entry_points_reject_bad_arguments_without_a_device():
+    L = _lib.lib()
+    E = _lib.A5G_EINVAL
+    # precision of a missing context, or an unknown precision
+    assert L.a5g_set_precision(None, 1, None) == E
+    assert L.a5g_get_precision(None, None, None) == E
+    # device-driven batch: null or empty member lists, null batch handles
+    out = ctypes.c_void_p()
+    assert L.a5g_batch_create(None, 1, ctypes.byref(out)) == E
+    assert L.a5g_batch_create(None, 0, ctypes.byref(out)) == E
+    assert L.a5g_batch_begin(None, None, None) == E
+    assert L.a5g_batch_block(None, 2, 1, None, None, None, None) == E
+    assert L.a5g_batch_launch(None, 2, 1) == E
+    assert L.a5g_batch_finish(None, None, None, None, None) == E
+    assert L.a5g_batch_destroy(None) == _lib.A5G_OK
+    # batched driver: no members, bad group count
+    assert L.a5s_batch_run(None, 0, None, 1, 1, 1, 1, None, None, None, None) == E
+    arr = (ctypes.c_void_p * 1)(None)
+    te = (ctypes.c_double * 1)(1e-9)
+    assert L.a5s_batch_run(arr, 1, te, 1, 1, 0, 1, None, None, None, None) == E
+    assert L.a5s_batch_run(arr, 1, te, 1, 1, 1, 1, None, None, None, None) == E  # null member
+    # the allocation-free batch: null member list
+    assert L.a5g_step_batch_static(None, 1, None) == E
