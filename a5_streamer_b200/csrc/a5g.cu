@@ -141,8 +141,14 @@ struct RunDev {
   // [1] simulated time, [2] end time, [3] 1 while the run is active
   double *blk;
   double dr_min, dt_max;       // finest cell size of the tree; ST_dt_max
-  int use_drt, pad5;
+  int use_drt;
+  // dielectric runs (eps not identically 1): the multigrid tags each box
+  // (tags[id]: TAG_NORMAL / TAG_DIEL) and uses the eps operators on
+  // dielectric boxes; such runs take the device-memory multigrid path
+  int diel;
+  int *tags;
 };
+constexpr int TAG_NORMAL = 1, TAG_DIEL = 2;
 
 // Scalars of one photoionization call: photons created, the factor fac
 // of PH_set_src_2d and the master generator state at the start of the call.
@@ -193,6 +199,10 @@ __device__ __forceinline__ double *FX(const RunDev &R, int f, int id) {
 __device__ __forceinline__ double *FY(const RunDev &R, int f, int id) {
   return R.fy + ((size_t)f * R.capacity + id) * FSLOT;
 }
+// max / min with the operand order of Fortran's max / min (NaN handling)
+__device__ __forceinline__ double dmax(double a, double b) { return a < b ? b : a; }
+__device__ __forceinline__ double dmin(double a, double b) { return b < a ? b : a; }
+
 // fx(i, j): i in 1..nc+1, j in 1..nc;  fy(i, j): i in 1..nc, j in 1..nc+1
 __device__ __forceinline__ int fxi(int i, int j, int nc) { return (i - 1) + (nc + 1) * (j - 1); }
 __device__ __forceinline__ int fyi(int i, int j, int nc) { return (i - 1) + nc * (j - 1); }
@@ -737,6 +747,38 @@ __device__ __forceinline__ void phi_nbrs(double V, const T *phi, const BoxRec &B
 }
 
 // box_lpl (m_aX_mg.f90:662-680) / box_clpl (:1027-1049) at one cell
+// A box the multigrid treats with the eps operators (its tag; device-memory
+// multigrid of a dielectric run only).
+__device__ __forceinline__ bool diel_box(const RunDev &R, const BoxRec &B) {
+  return R.diel && R.tags[B.gbase / SLOT] == TAG_DIEL;
+}
+
+// Laplacian of a dielectric box at one cell (mg$D_box_lpld,
+// afivo/src/m_aX_mg.f90:951-1001; cylindrical mg2_box_clpld, :1467-1495):
+// inv_dr^2 * 2 * sum over lx, hx, ly, hy of rfac a0 a / (a0 + a) (u - u0),
+// a0 and a the eps of the cell and of the neighbour.
+__device__ __forceinline__ double lap_diel(const RunDev &R, const BoxRec &B, int ncg, int i, int j,
+                                           double v, const double u[4], double inv_dr_sq) {
+  const double *eps = VAR(R, I_EPS) + B.gbase;
+  const int loc = i + ncg * j;
+  const double a0 = eps[loc];
+  const double a[4] = {eps[loc - 1], eps[loc + 1], eps[loc - ncg], eps[loc + ncg]};
+  double rf[4] = {1, 1, 1, 1};
+  if (R.coord == 1) {
+    const int gi = B.gi0 + i;
+    const double den = gi - 0.5;
+    rf[0] = (gi - 1) / den;
+    rf[1] = gi / den;
+  }
+  double sum = 0;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    if (R.coord == 1) sum = sum + rf[k] * a0 * a[k] / (a0 + a[k]) * (u[k] - v);
+    else sum = sum + a0 * a[k] / (a0 + a[k]) * (u[k] - v);
+  }
+  return inv_dr_sq * 2 * sum;
+}
+
 template <class T>
 __device__ __forceinline__ T lap_at(const RunDev &R, double V, const T *phi, const BoxRec &B, int nc,
                                     int ncg, int i, int j, T inv_dr_sq) {
@@ -744,6 +786,10 @@ __device__ __forceinline__ T lap_at(const RunDev &R, double V, const T *phi, con
   T lx, hx, ly, hy;
   phi_nbrs(V, phi, B, nc, ncg, i, j, g, lx, hx, ly, hy);
   const T v = phi[g];
+  if (diel_box(R, B)) {
+    const double u[4] = {(double)lx, (double)hx, (double)ly, (double)hy};
+    return T(lap_diel(R, B, ncg, i, j, (double)v, u, (double)inv_dr_sq));
+  }
   if (R.coord == 1) {
     const int gi = B.gi0 + i;
     const T den = T(gi) - T(0.5);
@@ -801,7 +847,36 @@ __device__ __noinline__ void p_sweep(const RunDev &R, const MGV<T> &M, int lvl, 
       phi_nbrs(M.V, phi, B, L.nc, L.ncg, i, j, g, lx, hx, ly, hy);
     }
     const T r = rhs[g];
-    if (cyl) {
+    if (diel_box(R, B)) {
+      // mg$D_box_gsrb_lpld (afivo/src/m_aX_mg.f90:895-948; cylindrical
+      // mg2_box_gsrb_clpld, :1499-1531): face weights c = 2 a0 a / (a0 + a),
+      // phi = (sum c rfac u - dx^2 rhs) / sum c rfac
+      const double *eps = VAR(R, I_EPS) + B.gbase;
+      const int loc = i + L.ncg * j;
+      const double a0 = eps[loc];
+      const double a[4] = {eps[loc - 1], eps[loc + 1], eps[loc - L.ncg], eps[loc + L.ncg]};
+      const double u[4] = {(double)lx, (double)hx, (double)ly, (double)hy};
+      double rf[4] = {1, 1, 1, 1};
+      if (cyl) {
+        const int gi = B.gi0 + i;
+        const double den = gi - 0.5;
+        rf[0] = (gi - 1) / den;
+        rf[1] = gi / den;
+      }
+      double su = 0, sc = 0;
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const double c = 2 * a0 * a[k] / (a0 + a[k]);
+        if (cyl) {
+          su = su + c * rf[k] * u[k];
+          sc = sc + c * rf[k];
+        } else {
+          su = su + c * u[k];
+          sc = sc + c;
+        }
+      }
+      phi[g] = T((su - (double)dx2 * (double)r) / sc);
+    } else if (cyl) {
       const int gi = B.gi0 + i;
       const T den = T(gi) - T(0.5);
       const T rf1 = T(gi - 1) / den, rf2 = T(gi) / den;
@@ -932,7 +1007,18 @@ __device__ void p_correct(const RunDev &R, const MGV<T> &M, int lvl, bool copy, 
       const int p2 = B.pbase + i_c2 + pncg * j_c1;
       const int p3 = B.pbase + i_c1 + pncg * j_c2;
       const T c1 = phi[p1] - tmp[p1], c2x = phi[p2] - tmp[p2], c2y = phi[p3] - tmp[p3];
-      phi[g] = v + T(0.5) * c1 + T(0.25) * (c2x + c2y);
+      if (diel_box(R, B)) {
+        // mg$D_box_corr_lpld (afivo/src/m_aX_mg.f90:1003-1071, 2D): eps-weighted
+        // averages of the parent's correction toward each coarse neighbour
+        const double *eps = VAR(R, I_EPS);
+        const double a0 = eps[p1], a1 = eps[p2], a2 = eps[p3];
+        double sum = 0;
+        sum = sum + (a0 * (double)c1 + a1 * (double)c2x) / (a0 + a1);
+        sum = sum + (a0 * (double)c1 + a2 * (double)c2y) / (a0 + a2);
+        phi[g] = T((double)v + 0.5 * sum);
+      } else {
+        phi[g] = v + T(0.5) * c1 + T(0.25) * (c2x + c2y);
+      }
     }
   }
   if (copy) {
@@ -1314,10 +1400,47 @@ __device__ void stage_mg(const RunDev &R, const MGV<T> &M, T *g0, T *g1, T *g2, 
 }
 
 
+// mg$D_set_box_tag (afivo/src/m_aX_mg.f90:673-712) for every box of a
+// dielectric run: the box is treated with the eps operators when its eps
+// (interior, ghost and corner cells) is not identically 1 -- varying, or
+// constant and different from 1. The reference tags a box at its first
+// multigrid use; eps is set when a box is created (set_box_eps) and not
+// changed afterwards, so tagging every box at every solve gives the same
+// tags. One warp per box.
+__device__ void p_set_tags(const RunDev &R) {
+  const double *eps = VAR(R, I_EPS);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int li = 0; li < R.nlev; li++) {
+    const int ncg = R.lv_nc[li] + 2, per = ncg * ncg;
+    const int b0 = R.bx_off[li], nb = R.bx_off[li + 1] - b0;
+    for (int b = warp; b < nb; b += NTHR / 32) {
+      const int base = R.boxes[b0 + b].gbase;
+      double mn = eps[base], mx = mn;
+      for (int c = lane; c < per; c += 32) {
+        const double v = eps[base + c];
+        mn = dmin(mn, v);
+        mx = dmax(mx, v);
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        mn = dmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        mx = dmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+      }
+      if (lane == 0) {
+        const bool deps = mx > mn, ceps = !deps && (mn < 1 || mn > 1);
+        R.tags[base / SLOT] = (deps || ceps) ? TAG_DIEL : TAG_NORMAL;
+      }
+    }
+  }
+  __syncthreads();
+}
+
 // mg$D_fas_fmg in shared memory when the tree fits (the three variables,
-// the box records and the parent-box list), else in device memory
+// the box records and the parent-box list), else in device memory. A
+// dielectric run always takes the device-memory path, whose phases apply the
+// eps operators to the boxes tagged dielectric.
 __device__ void p_fmg(const RunDev &R, bool set_residual, bool first_call, bool leaf_rhs) {
-  if (R.smem_doubles > 0) {
+  if (R.diel) p_set_tags(R);
+  if (R.smem_doubles > 0 && !R.diel) {
     const int S = R.smem_doubles, nbx = R.bx_off[R.nlev], npb = R.pb_off[R.nlev];
     double *base = g_dsmem + PLAN_DOUBLES + (R.coord == 1 ? WTS_DOUBLES : 0);
     BoxRec *sb = reinterpret_cast<BoxRec *>(base + 3 * S);
@@ -1617,8 +1740,6 @@ __device__ void average_dens(const RunDev &R) {
 
 __device__ void dt_reductions(const RunDev &R);
 
-__device__ __forceinline__ double dmax(double a, double b) { return a < b ? b : a; }
-__device__ __forceinline__ double dmin(double a, double b) { return b < a ? b : a; }
 
 // a$D_tree_max_cc / _min_cc over leaves (afivo/src/m_aX_utils.f90:559-619)
 __device__ void dt_reductions(const RunDev &R) {
@@ -2610,6 +2731,10 @@ struct a5g_ctx {
   int cc32_cap = 0;      // box capacity cc32 is sized for
   int mx_smem_fit = 0;   // floats per variable of the shared-memory copy (0: does not fit)
   size_t dyn_smem32 = 0; // dynamic shared memory of a mixed-precision launch
+  // dielectric runs: box tags (device), box sizes of the uploaded tree
+  // (host, 0 for ids not in use) to check uploaded eps values
+  int *tags = nullptr;
+  std::vector<int> h_nc;
   // shared-memory staging of the multigrid (a5g_debug_set_staging can turn it off)
   bool allow_smem = true;
   int fit64 = 0, fit32 = 0;       // per-variable sizes when the tree fits, else 0
@@ -2981,8 +3106,7 @@ int a5g_create(const a5g_params *p, a5g_ctx **out) {
   *out = nullptr;
   if (p->box_size != NC) return fail(A5G_EINVAL, "box_size must be 8");
   if (p->coord != 0 && p->coord != 1) return fail(A5G_EINVAL, "coord must be 0 or 1");
-  if (p->epsilon_diel != 1.0)
-    return fail(A5G_EINVAL, "epsilon_diel != 1 needs the dielectric operators (not built)");
+  if (!(p->epsilon_diel > 0)) return fail(A5G_EINVAL, "epsilon_diel must be > 0");
   if (p->n_seeds < 0 || p->n_seeds > 8) return fail(A5G_EINVAL, "n_seeds must be 0..8");
   if (p->lvls_max < 1 || p->lvls_max > 30) return fail(A5G_EINVAL, "lvls_max must be 1..30");
   if (!(p->dr_base > 0)) return fail(A5G_EINVAL, "dr_base must be > 0");
@@ -3035,6 +3159,7 @@ int a5g_create(const a5g_params *p, a5g_ctx **out) {
   h.blk = c->scal + 8;
   h.dt_max = p->dt_max;
   h.use_drt = p->use_drt ? 1 : 0;
+  h.diel = p->epsilon_diel != 1.0 ? 1 : 0;
   h.status = c->status;
   h.mx_fmg = 1;
   h.mx_sw_down = h.mx_sw_up = 4;
@@ -3095,6 +3220,7 @@ int a5g_destroy(a5g_ctx *c) {
   cudaFree(c->ph_boxes);
   cudaFree(c->tbl32);
   cudaFree(c->cc32);
+  cudaFree(c->tags);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return A5G_OK;
@@ -3138,6 +3264,8 @@ int a5g_set_table(a5g_ctx *c, int n_rows, int n_cols, double x_min, double inv_d
 // FP32 storage of the correction solve when the tree does not fit in shared
 // memory (sized to the box capacity; its contents are scratch).
 static int mx_ready(a5g_ctx *c) {
+  if (c->precision == A5G_MIXED && c->h.diel)
+    return fail(A5G_EINVAL, "the mixed form does not support dielectric runs (eps != 1)");
   if (c->precision != A5G_MIXED || c->mx_smem_fit > 0 || c->cc32_cap >= c->capacity) return A5G_OK;
   cudaFree(c->cc32);
   c->cc32 = nullptr;
@@ -3155,6 +3283,8 @@ int a5g_set_precision(a5g_ctx *c, int precision, const a5g_mg_schedule *sched) {
   a5g_mg_schedule s{1, 2, 2, c->p.n_cycle_base, 1};
   if (sched) s = *sched;
   if (s.fmg != 0 && s.fmg != 1) return fail(A5G_EINVAL, "schedule: fmg must be 0 or 1");
+  if (precision == A5G_MIXED && c->h.diel)
+    return fail(A5G_EINVAL, "the mixed form does not support dielectric runs (eps != 1)");
   if (s.n_cycle_down < 1 || s.n_cycle_down > 8 || s.n_cycle_up < 1 || s.n_cycle_up > 8 ||
       s.n_cycle_base < 1 || s.n_cycle_base > 64 || s.n_corr < 1 || s.n_corr > 8)
     return fail(A5G_EINVAL, "schedule: cycles down/up 1..8, base 1..64, corrections 1..8");
@@ -3284,6 +3414,17 @@ static int grow(a5g_ctx *c, int need) {
   c->capacity = cap;
   c->h.capacity = cap;
   c->h.cc = ncc; c->h.fx = nfx; c->h.fy = nfy; c->h.meta = nmeta; c->h.flags = nflags;
+  {
+    // box tags of the dielectric multigrid: recomputed at every solve
+    int *nt = nullptr;
+    if (cudaMalloc(&nt, (size_t)cap * sizeof(int)) != cudaSuccess)
+      return fail(A5G_ENOMEM, "cannot grow the box tags to " + std::to_string(cap) + " boxes");
+    CK(cudaMemsetAsync(nt, 0, (size_t)cap * sizeof(int), c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    cudaFree(c->tags);
+    c->tags = nt;
+    c->h.tags = nt;
+  }
   if (c->cc32) {  // scratch of the mixed form: reallocated at the next mixed launch
     cudaFree(c->cc32);
     c->cc32 = nullptr;
@@ -3427,6 +3568,9 @@ int a5g_upload_tree(a5g_ctx *c, int max_id, int min_lvl, int max_lvl, const int 
   c->max_id = max_id;
   c->min_lvl = min_lvl;
   c->max_lvl = max_lvl;
+  c->h_nc.assign(max_id + 1, 0);
+  for (int id = 1; id <= max_id; id++)
+    if (meta16[16 * id]) c->h_nc[id] = hm[id].nc;
   long long nl = 0;
   for (int li = 0; li < nlev; li++)
     for (int q = off[1][li]; q < off[1][li + 1]; q++) nl += (long long)hm[lists[q]].nc * hm[lists[q]].nc;
@@ -3461,6 +3605,20 @@ int a5g_upload_cc(a5g_ctx *c, int iv, const double *host) {
                      (size_t)(c->max_id + 1) * SLOT * sizeof(double), cudaMemcpyHostToDevice,
                      c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  if (iv == I_EPS) {
+    // the run is dielectric when eps differs from 1 anywhere in a box in use
+    int diel = c->p.epsilon_diel != 1.0 ? 1 : 0;
+    for (int id = 1; id <= c->max_id && !diel; id++) {
+      const int g = c->h_nc[id] + 2;
+      if (c->h_nc[id] == 0) continue;
+      for (int k = 0; k < g * g && !diel; k++)
+        if (host[(size_t)id * SLOT + k] != 1.0) diel = 1;
+    }
+    if (diel != c->h.diel) {
+      c->h.diel = diel;
+      return push_run(c);
+    }
+  }
   return A5G_OK;
 }
 

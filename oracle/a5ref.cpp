@@ -694,9 +694,80 @@ static void set_box_tag(Box &b, const MG &mg) {
   if (is_deps) b.tag = MG_VEPS_BOX;
 }
 
+// Radius weights of the cylindrical operators at global index g = i + ioff:
+// (g - 1) / (g - 1/2) and g / (g - 1/2) (afivo/src/m_aX_mg.f90:1027-1049).
+static inline void rfac_cyl(int g, double &rf1, double &rf2) {
+  double den = g - 0.5;
+  rf1 = (g - 1) / den;
+  rf2 = g / den;
+}
+
+// Red-black Gauss-Seidel on a box whose eps is not identically 1
+// (mg$D_box_gsrb_lpld, afivo/src/m_aX_mg.f90:895-948; cylindrical
+// mg2_box_gsrb_clpld, :1499-1531): face weights c = 2 a0 a / (a0 + a) from
+// the eps of the cell (a0) and of each neighbour (a), the cylindrical radius
+// factors on the x faces, phi = (sum c rfac u - dx^2 rhs) / sum c rfac; sums
+// in neighbour order lx, hx, ly, hy.
+static void box_gsrb_diel(Box &b, int redblack, const MG &mg) {
+  const double dx2 = b.dr * b.dr;
+  const int nc = b.n_cell, ip = mg.i_phi, ir = mg.i_rhs, ie = mg.i_eps;
+  const bool cyl = b.coord == CYL;
+  const int ioff = (b.ix[0] - 1) * nc;
+  for (int j = 1; j <= nc; j++) {
+    int i0 = 2 - ((redblack ^ j) & 1);
+    for (int i = i0; i <= nc; i += 2) {
+      const double a0 = b.c(i, j, ie);
+      const double u[4] = {b.c(i - 1, j, ip), b.c(i + 1, j, ip), b.c(i, j - 1, ip), b.c(i, j + 1, ip)};
+      const double a[4] = {b.c(i - 1, j, ie), b.c(i + 1, j, ie), b.c(i, j - 1, ie), b.c(i, j + 1, ie)};
+      double rf[4] = {1, 1, 1, 1};
+      if (cyl) rfac_cyl(i + ioff, rf[0], rf[1]);
+      double su = 0, sc = 0;
+      for (int k = 0; k < 4; k++) {
+        const double c = 2 * a0 * a[k] / (a0 + a[k]);
+        if (cyl) {
+          su = su + c * rf[k] * u[k];
+          sc = sc + c * rf[k];
+        } else {
+          su = su + c * u[k];
+          sc = sc + c;
+        }
+      }
+      b.c(i, j, ip) = (su - dx2 * b.c(i, j, ir)) / sc;
+    }
+  }
+}
+
+// Laplacian of a box whose eps is not identically 1 (mg$D_box_lpld,
+// afivo/src/m_aX_mg.f90:951-1001; cylindrical mg2_box_clpld, :1467-1495):
+// inv_dr^2 * 2 * sum rfac a0 a / (a0 + a) (u - u0).
+static void box_op_diel(Box &b, int i_out, const MG &mg) {
+  const int nc = b.n_cell, ip = mg.i_phi, ie = mg.i_eps;
+  const double inv_dr_sq = 1 / (b.dr * b.dr);
+  const bool cyl = b.coord == CYL;
+  const int ioff = (b.ix[0] - 1) * nc;
+  for (int j = 1; j <= nc; j++)
+    for (int i = 1; i <= nc; i++) {
+      const double u0 = b.c(i, j, ip), a0 = b.c(i, j, ie);
+      const double u[4] = {b.c(i - 1, j, ip), b.c(i + 1, j, ip), b.c(i, j - 1, ip), b.c(i, j + 1, ip)};
+      const double a[4] = {b.c(i - 1, j, ie), b.c(i + 1, j, ie), b.c(i, j - 1, ie), b.c(i, j + 1, ie)};
+      double rf[4] = {1, 1, 1, 1};
+      if (cyl) rfac_cyl(i + ioff, rf[0], rf[1]);
+      double sum = 0;
+      for (int k = 0; k < 4; k++) {
+        if (cyl) sum = sum + rf[k] * a0 * a[k] / (a0 + a[k]) * (u[k] - u0);
+        else sum = sum + a0 * a[k] / (a0 + a[k]) * (u[k] - u0);
+      }
+      b.c(i, j, i_out) = inv_dr_sq * 2 * sum;
+    }
+}
+
 // afivo/src/m_aX_mg.f90:636-659 (gsrb_lpl) and 998-1024 (gsrb_clpl)
 static void box_gsrb(Box &b, int redblack, const MG &mg) {
   if (b.tag == INIT_TAG) set_box_tag(b, mg);
+  if (b.tag == MG_CEPS_BOX || b.tag == MG_VEPS_BOX) {
+    box_gsrb_diel(b, redblack, mg);
+    return;
+  }
   double dx2 = b.dr * b.dr;
   int nc = b.n_cell, ip = mg.i_phi, ir = mg.i_rhs;
   if (b.coord == CYL) {
@@ -725,6 +796,10 @@ static void box_gsrb(Box &b, int redblack, const MG &mg) {
 // afivo/src/m_aX_mg.f90:662-680 (box_lpl) and 1027-1049 (box_clpl)
 static void box_op(Box &b, int i_out, const MG &mg) {
   if (b.tag == INIT_TAG) set_box_tag(b, mg);
+  if (b.tag == MG_CEPS_BOX || b.tag == MG_VEPS_BOX) {
+    box_op_diel(b, i_out, mg);
+    return;
+  }
   int nc = b.n_cell, ip = mg.i_phi;
   double inv_dr_sq = 1 / (b.dr * b.dr);
   if (b.coord == CYL) {
@@ -752,6 +827,27 @@ static void box_corr(const Box &p, Box &c, const MG &mg) {
   int nc = c.n_cell, ip = mg.i_phi, ic = mg.i_tmp;
   int off[2];
   child_offset(c, -1, off);
+  if (c.tag == MG_CEPS_BOX || c.tag == MG_VEPS_BOX) {
+    // mg$D_box_corr_lpld, afivo/src/m_aX_mg.f90:1003-1071 (2D): eps-weighted
+    // averages of the parent's correction toward each coarse neighbour
+    const int ie = mg.i_eps;
+    for (int j = 1; j <= nc; j++) {
+      int j_c1 = off[1] + ((j + 1) >> 1);
+      int j_c2 = j_c1 + 1 - 2 * (j & 1);
+      for (int i = 1; i <= nc; i++) {
+        int i_c1 = off[0] + ((i + 1) >> 1);
+        int i_c2 = i_c1 + 1 - 2 * (i & 1);
+        const double u0 = p.c(i_c1, j_c1, ic), a0 = p.c(i_c1, j_c1, ie);
+        const double u1 = p.c(i_c2, j_c1, ic), u2 = p.c(i_c1, j_c2, ic);
+        const double a1 = p.c(i_c2, j_c1, ie), a2 = p.c(i_c1, j_c2, ie);
+        double sum = 0;
+        sum = sum + (a0 * u0 + a1 * u1) / (a0 + a1);
+        sum = sum + (a0 * u0 + a2 * u2) / (a0 + a2);
+        c.c(i, j, ip) = c.c(i, j, ip) + 0.5 * sum;
+      }
+    }
+    return;
+  }
   for (int j = 1; j <= nc; j++) {
     int j_c1 = off[1] + ((j + 1) >> 1);
     int j_c2 = j_c1 + 1 - 2 * (j & 1);
@@ -2436,6 +2532,159 @@ static int kat_mg(bool cyl, int n_fmg, double *res_out, double *err_out, int *ma
   for (int lvl = t.min_lvl; lvl <= t.max_lvl; lvl++)
     for (int id : t.L(lvl).leaves) cells += (long)t.boxes[id].n_cell * t.boxes[id].n_cell;
   return (int)cells;
+}
+
+// afivo/examples/multigrid/test_mg_cyl_diel.f90: cylindrical Poisson
+// problem with eps = 100 in the quadrant r < 0.5, z < 0.5 and 1 elsewhere,
+// manufactured solution of two Gaussians; rhs = eps * lpl(phi) plus the
+// surface charge at the eps jumps, split between the two cells of a face in
+// proportion to their eps; Neumann on the axis, Dirichlet phi_sol elsewhere;
+// refinement where dr^2 max|rhs / eps| > 5e-4. The multigrid uses the eps
+// operators (box tags from the eps of each box).
+static int kat_mg_diel(int n_fmg, double *res_out, double *err_out, int *max_lvl_out) {
+  struct G { double a, x0, y0, s; };
+  const G g[2] = {G{1.0, 0.25, 0.25, 0.04}, G{1.0, 0.75, 0.75, 0.04}};
+  auto gauss = [](const double x[2], const G &q) {
+    double xr0 = (x[0] - q.x0) / q.s, xr1 = (x[1] - q.y0) / q.s;
+    return std::exp(-(xr0 * xr0 + xr1 * xr1));
+  };
+  auto phi_sol = [&](const double x[2]) {
+    double v = 0;
+    for (const G &q : g) v = v + q.a * gauss(x, q);
+    return v;
+  };
+  auto phi_grad = [&](const double x[2], double gr[2]) {
+    gr[0] = gr[1] = 0;
+    for (const G &q : g) {
+      double xr0 = (x[0] - q.x0) / q.s, xr1 = (x[1] - q.y0) / q.s, e = gauss(x, q);
+      gr[0] = gr[0] + q.a * (-2 * xr0 / q.s * e);
+      gr[1] = gr[1] + q.a * (-2 * xr1 / q.s * e);
+    }
+  };
+  auto lpl = [&](const double x[2]) {
+    double v = 0;
+    for (const G &q : g) {
+      double xr0 = (x[0] - q.x0) / q.s, xr1 = (x[1] - q.y0) / q.s;
+      double sum = xr0 * xr0 + xr1 * xr1;
+      v = v + q.a * (4 / (q.s * q.s) * (sum - 1.0 - 0.5 * (x[0] - q.x0) / x[0]) * gauss(x, q));
+    }
+    return v;
+  };
+  const int i_phi = 0, i_tmp = 1, i_rhs = 2, i_err = 3, i_eps = 4;
+  Tree t;
+  double r0[2] = {0, 0};
+  const int box_size = 8;
+  tree_init(t, box_size, 5, 0, 1.0 / box_size, r0, 30, 2, CYL);
+  int ixl[1][2] = {{1, 1}};
+  std::vector<std::array<int, 4>> nbl(1, std::array<int, 4>{-1, -1, -1, -1});
+  set_base(t, 1, ixl, nbl);
+  auto rr = [](const Box &b, double fi, double fj, double xy[2]) {
+    xy[0] = b.r_min[0] + (fi - 0.5) * b.dr;
+    xy[1] = b.r_min[1] + (fj - 0.5) * b.dr;
+  };
+  auto init = [&](Box &b) {
+    const int nc = b.n_cell;
+    const double dr = b.dr;
+    for (int j = 0; j <= nc + 1; j++)
+      for (int i = 0; i <= nc + 1; i++) {
+        double xy[2];
+        r_cc(b, i, j, xy);
+        b.c(i, j, i_phi) = 0;
+        b.c(i, j, i_eps) = (xy[0] < 0.5 && xy[1] < 0.5) ? 100.0 : 1.0;
+        b.c(i, j, i_rhs) = lpl(xy) * b.c(i, j, i_eps);
+      }
+    for (int j = 1; j <= nc; j++)
+      for (int i = 0; i <= nc; i++) {
+        double xy[2], gr[2];
+        rr(b, i + 0.5, (double)j, xy);
+        phi_grad(xy, gr);
+        double qbnd = (b.c(i + 1, j, i_eps) - b.c(i, j, i_eps)) * gr[0] / dr;
+        double w = b.c(i + 1, j, i_eps) / (b.c(i, j, i_eps) + b.c(i + 1, j, i_eps));
+        b.c(i + 1, j, i_rhs) = b.c(i + 1, j, i_rhs) + w * qbnd;
+        b.c(i, j, i_rhs) = b.c(i, j, i_rhs) + (1 - w) * qbnd;
+      }
+    for (int j = 0; j <= nc; j++)
+      for (int i = 1; i <= nc; i++) {
+        double xy[2], gr[2];
+        rr(b, (double)i, j + 0.5, xy);
+        phi_grad(xy, gr);
+        double qbnd = (b.c(i, j + 1, i_eps) - b.c(i, j, i_eps)) * gr[1] / dr;
+        double w = b.c(i, j + 1, i_eps) / (b.c(i, j, i_eps) + b.c(i, j + 1, i_eps));
+        b.c(i, j + 1, i_rhs) = b.c(i, j + 1, i_rhs) + w * qbnd;
+        b.c(i, j, i_rhs) = b.c(i, j, i_rhs) + (1 - w) * qbnd;
+      }
+  };
+  RefFn ref = [&](Tree &tt, int id, std::vector<int> &rf) {
+    Box &b = tt.boxes[id];
+    int nc = b.n_cell;
+    double m = 0;
+    for (int j = 1; j <= nc; j++)
+      for (int i = 1; i <= nc; i++) m = std::max(m, std::fabs(b.c(i, j, i_rhs) / b.c(i, j, i_eps)));
+    if (b.dr * b.dr * m > 5.0e-4) rf[id] = DO_REF;
+  };
+  while (true) {
+    loop_all_boxes(t, init);
+    RefInfo ri;
+    adjust_refinement(t, ref, ri);
+    if (ri.n_add == 0) break;
+  }
+  loop_all_boxes(t, init);
+  MG mg;
+  mg.i_phi = i_phi;
+  mg.i_tmp = i_tmp;
+  mg.i_rhs = i_rhs;
+  mg.i_eps = i_eps;
+  mg.n_cycle_down = 2;
+  mg.n_cycle_up = 2;
+  mg.n_cycle_base = 2;
+  mg.sides_rb = mg_sides_rb;
+  mg.sides_bc = [&](Tree &tt, int id, int nb, int iv) {
+    Box &b = tt.boxes[id];
+    const int nc = b.n_cell;
+    double xy[2];
+    for (int n = 1; n <= nc; n++) {
+      switch (nb) {
+        case NB_LX: b.c(0, n, iv) = b.c(1, n, iv); break;
+        case NB_HX:
+          rr(b, nc + 0.5, (double)n, xy);
+          b.c(nc + 1, n, iv) = 2 * phi_sol(xy) - b.c(nc, n, iv);
+          break;
+        case NB_LY:
+          rr(b, (double)n, 0.5, xy);
+          b.c(n, 0, iv) = 2 * phi_sol(xy) - b.c(n, 1, iv);
+          break;
+        default:
+          rr(b, (double)n, nc + 0.5, xy);
+          b.c(n, nc + 1, iv) = 2 * phi_sol(xy) - b.c(n, nc, iv);
+      }
+    }
+  };
+  for (int it = 1; it <= n_fmg; it++) {
+    fas_fmg(t, mg, true, it == 1);
+    loop_all_boxes(t, [&](Box &b) {
+      int nc = b.n_cell;
+      for (int j = 1; j <= nc; j++)
+        for (int i = 1; i <= nc; i++) {
+          double xy[2];
+          r_cc(b, i, j, xy);
+          b.c(i, j, i_err) = b.c(i, j, i_phi) - phi_sol(xy);
+        }
+    });
+    double mn = tree_min_cc(t, i_tmp), mx = tree_max_cc(t, i_tmp);
+    double emn = tree_min_cc(t, i_err), emx = tree_max_cc(t, i_err);
+    if (res_out) res_out[it - 1] = std::max(std::fabs(mn), std::fabs(mx));
+    if (err_out) err_out[it - 1] = std::max(std::fabs(emn), std::fabs(emx));
+  }
+  if (max_lvl_out) *max_lvl_out = t.max_lvl;
+  int n_diel = 0;
+  for (int lvl = t.min_lvl; lvl <= t.max_lvl; lvl++)
+    for (int id : t.L(lvl).ids)
+      if (t.boxes[id].tag == MG_CEPS_BOX || t.boxes[id].tag == MG_VEPS_BOX) n_diel++;
+  return n_diel;
+}
+
+int a5ref_kat_mg_cyl_diel(int n_fmg, double *res, double *err, int *ml) {
+  return kat_mg_diel(n_fmg, res, err, ml);
 }
 
 int a5ref_kat_mg2_2d(int n_fmg, double *res, double *err, int *ml) {

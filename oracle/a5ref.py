@@ -93,6 +93,7 @@ def lib() -> ctypes.CDLL:
             "a5ref_export_table": (V, [P, pd, pd, pd, pi]),
             "a5ref_applied_voltage": (D, [P]),
             "a5ref_kat_mg2_2d": (I, [I, pd, pd, pi]), "a5ref_kat_mg_cyl": (I, [I, pd, pd, pi]),
+            "a5ref_kat_mg_cyl_diel": (I, [I, pd, pd, pi]),
             "a5ref_kat_lookup": (D, [I, I, D, I]), "a5ref_koren_mlim": (D, [D, D]),
             "a5ref_op_photoionization": (V, [P, D, I]),
             "a5ref_rng_get": (V, [P, pi]), "a5ref_rng_set": (V, [P, pi]),
@@ -343,6 +344,16 @@ def kat_mg(cyl: bool, n_fmg: int):
     fn = lib().a5ref_kat_mg_cyl if cyl else lib().a5ref_kat_mg2_2d
     cells = fn(n_fmg, _dp(res), _dp(err), ctypes.byref(ml))
     return res, err, ml.value, cells
+
+
+def kat_mg_diel(n_fmg: int):
+    """The dielectric multigrid case (test_mg_cyl_diel.f90): per FMG cycle max
+    |residual| and max |error|, the finest level and the number of boxes the
+    multigrid treats as dielectric."""
+    res, err = np.zeros(n_fmg), np.zeros(n_fmg)
+    ml = ctypes.c_int(0)
+    n_diel = lib().a5ref_kat_mg_cyl_diel(n_fmg, _dp(res), _dp(err), ctypes.byref(ml))
+    return res, err, ml.value, n_diel
 
 
 def kat_lookup(n_rows: int, n_pairs: int = 100000, x_max: float = 10.0,

@@ -45,7 +45,7 @@ def test_invalid_parameters_are_rejected_without_a_device():
     assert code == _lib.A5G_EINVAL
     assert b"box_size" in _lib.lib().a5g_last_error()
     p.box_size = 8
-    p.epsilon_diel = 2.0
+    p.epsilon_diel = 0.0  # a permittivity must be positive
     assert _lib.lib().a5g_create(ctypes.byref(p), ctypes.byref(h)) == _lib.A5G_EINVAL
     # null arguments
     assert _lib.lib().a5g_step(None, 1e-12) == _lib.A5G_EINVAL

@@ -36,6 +36,18 @@ def test_mg_cyl_known_answer():
     assert err[-1] < 2e-4
 
 
+def test_mg_cyl_diel_known_answer():
+    """afivo/examples/multigrid/test_mg_cyl_diel.f90: a jump of eps (100 vs 1)
+    with surface charge; the eps operators (gsrb_clpld, clpld, corr_lpld)
+    converge to the manufactured solution at the discretization error."""
+    res, err, max_lvl, n_diel = a5ref.kat_mg_diel(6)
+    assert n_diel > 100 and max_lvl >= 8
+    for k in range(4):
+        assert res[k + 1] < res[k] / 10.0
+    assert err[-1] < 2e-4
+    assert abs(err[-1] - err[-2]) < 1e-8
+
+
 def test_lookup_table_second_order():
     errs = [a5ref.kat_lookup(n) for n in (20, 40, 80, 160, 320)]
     ratios = [errs[k + 1] / errs[k] for k in range(len(errs) - 1)]
