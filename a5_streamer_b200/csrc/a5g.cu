@@ -2557,13 +2557,26 @@ __global__ void __launch_bounds__(PH_THREADS) a5g_photon_kernel(const RunDev *si
     rank_first = sf;
     rank_id = si;
   }
+  // Generator of team thread w: the master's state at draw 4W + 4w. One
+  // thread jumps the master to the block's first team thread (4W + 4 w0),
+  // then every thread jumps from there by 4 threadIdx.x: jumps compose
+  // exactly, and the per-thread jump needs at most 10 doublings instead of
+  // about 19.
+  __shared__ int s_base[4];
+  if (threadIdx.x == 0) {
+    int b[4] = {R.ph_scal->st0[0], R.ph_scal->st0[1], R.ph_scal->st0[2], R.ph_scal->st0[3]};
+    mz_advance(b, 4ull * (unsigned long long)W + 4ull * (unsigned long long)w0, R.ph_jump);
+#pragma unroll
+    for (int q = 0; q < 4; q++) s_base[q] = b[q];
+  }
+  __syncthreads();
   const long long w = w0 + threadIdx.x;
   if (w >= W) return;
   long long lo, len;
   static_chunk(n_used, W, w, lo, len);
   if (len == 0) return;
-  int st[4] = {R.ph_scal->st0[0], R.ph_scal->st0[1], R.ph_scal->st0[2], R.ph_scal->st0[3]};
-  mz_advance(st, 4ull * (unsigned long long)W + 4ull * (unsigned long long)w, R.ph_jump);
+  int st[4] = {s_base[0], s_base[1], s_base[2], s_base[3]};
+  mz_advance(st, 4ull * (unsigned long long)threadIdx.x, R.ph_jump);
   int rs[4];
 #pragma unroll
   for (int q = 0; q < 4; q++) rs[q] = mz_int4(st);

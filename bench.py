@@ -338,20 +338,25 @@ def run_b200(args):
         nb = max(3, K // 10)
         b0 = [torch.cuda.Event(enable_timing=True) for _ in range(nb)]
         b1 = [torch.cuda.Event(enable_timing=True) for _ in range(nb)]
-        with torch.cuda.stream(bstream):
-            for k in range(nb):
-                flush.fill_(k & 0xFF)
-                b0[k].record(bstream)
-                dv.step_batch(reps, dts)
-                b1[k].record(bstream)
-        reps[0].sync()
-        torch.cuda.synchronize()
+        with ClockSampler(local) as bclk:
+            torch.cuda.nvtx.range_push("batched_mixed" if mixed else "batched_fp64")
+            with torch.cuda.stream(bstream):
+                for k in range(nb):
+                    flush.fill_(k & 0xFF)
+                    b0[k].record(bstream)
+                    dv.step_batch(reps, dts)
+                    b1[k].record(bstream)
+            torch.cuda.nvtx.range_pop()
+            reps[0].sync()
+            torch.cuda.synchronize()
         bt = sum(a.elapsed_time(b) for a, b in zip(b0, b1)) / 1e3
         for r in reps:
             r.close()
+        gbs = bytes_step * len(reps) * nb / bt / 1e9
         return {"replicas": len(reps), "steps": nb, "value": n_leaf * len(reps) * nb / bt,
                 "unit": UNIT, "ms_per_step": 1e3 * bt / nb,
-                "achieved_gbs": bytes_step * len(reps) * nb / bt / 1e9}
+                "achieved_gbs": gbs, "frac_of_measured_hbm": gbs / measured_peak()[0],
+                "clocks": bclk.summary()}
 
     def time_single(r, label):
         """K steps of one run, L2 flushed before each, CUDA events on its stream."""
