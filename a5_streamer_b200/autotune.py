@@ -125,12 +125,13 @@ def time_steps(run, dt: float, n: int) -> float:
 
 def tune_schedule(sim, n_steps: int = 20, tol_max_E: float = 1e-4, tol_head_z: float = 5e-3,
                   safety: float = 0.5, candidates: Optional[Sequence[Schedule]] = None,
-                  whole_run: bool = True, ref_head=None) -> Dict:
+                  whole_run: bool = True, ref_head=None, n_time: int = 20) -> Dict:
     """Pick the mixed-precision multigrid schedule for ``sim``'s tree and
-    configuration (see the module docstring). ref_head: the FP64 whole-run
-    observables if the caller has them (else they are computed). Returns the
-    choice, its step time and errors, the FP64 step time and the table of
-    candidates."""
+    configuration (see the module docstring): errors on the frozen mesh after
+    ``n_steps`` steps, step time over ``n_time`` steps. ref_head: the FP64
+    whole-run observables if the caller has them (else they are computed).
+    Returns the choice, its step time and errors, the FP64 step time and the
+    table of candidates."""
     import dataclasses
     cfg = sim.cfg
     cfg_np = dataclasses.replace(cfg, photoi_enabled=False) if cfg.photoi_enabled else cfg
@@ -141,7 +142,7 @@ def tune_schedule(sim, n_steps: int = 20, tol_max_E: float = 1e-4, tol_head_z: f
     ok_b = lambda e: e["max_E_rel"] <= safety * tol_max_E and e["head_z_rel"] <= safety * tol_head_z
     ref = clone_state(sim)
     ref.step(dt)
-    t_fp64 = time_steps(ref, dt, n_steps - 1)
+    t_fp64 = time_steps(ref, dt, max(1, n_time - 1))
     ref.close()
     ref = clone_state(sim, cfg=cfg_np)
     for _ in range(n_steps):
@@ -150,7 +151,7 @@ def tune_schedule(sim, n_steps: int = 20, tol_max_E: float = 1e-4, tol_head_z: f
     for sched in candidates:
         run = clone_state(sim, mixed=True, schedule=sched)
         run.step(dt)
-        ms = time_steps(run, dt, n_steps - 1)
+        ms = time_steps(run, dt, max(1, n_time - 1))
         run.close()
         run = clone_state(sim, mixed=True, schedule=sched, cfg=cfg_np)
         for _ in range(n_steps):

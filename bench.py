@@ -391,7 +391,9 @@ def run_b200(args):
             sched = tuple(int(v) for v in args.mixed_schedule.split(","))
             tuned = {"schedule": sched, "table": [], "n_steps": 0}
         else:
-            tuned = autotune.tune_schedule(sim, ref_head=head_fp64)
+            # the frozen-mesh check over the K steps reported below, and the
+            # whole run to the end time
+            tuned = autotune.tune_schedule(sim, n_steps=K, ref_head=head_fp64)
             sched = tuned["schedule"]
         mrun = dv.clone_state(sim, mixed=True, schedule=sched)
         m_ms = time_single(mrun, "timed_mixed")
@@ -425,7 +427,8 @@ def run_b200(args):
                                  "note": ("photon counts are stochastic: the two runs draw different photons "
                                           "once a cell's rounded count differs") if cfg.photoi_enabled else ""},
             "bounds": {"max_E_rel": 1e-4, "head_z_rel": 5e-3},
-            "tuner": {"candidates": len(tuned["table"]), "n_steps": tuned["n_steps"]},
+            "tuner": {"candidates": len(tuned["table"]), "frozen_mesh_steps": tuned["n_steps"],
+                      "whole_run": True},
             "batched": time_batch(True, sched) if args.batch > 0 else None,
         }
 
