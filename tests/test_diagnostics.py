@@ -1,0 +1,77 @@
+"""Streamer diagnostics (get_streamer_properties / get_cc_axis restated),
+computed from the oracle's state of the axisymmetric case in the device
+layout and checked against direct numpy evaluations of their definitions."""
+import numpy as np
+import pytest
+
+import a5ref
+from a5_streamer_b200 import config, diagnostics
+
+
+@pytest.fixture(scope="module")
+def state():
+    cfg = config.cylindrical_16mm()
+    sim = a5ref.Sim(cfg, n_threads=4)
+    sim.init()
+    for _ in range(3):
+        sim.advance(True)
+    tv = diagnostics.TreeView(sim.meta(), sim.geom(), sim.levels(), cfg.lvls_max)
+    return cfg, sim, tv
+
+
+def _leaf_cells(tv):
+    for bid in tv.leaves():
+        n = tv.nc(bid)
+        for j in range(1, n + 1):
+            for i in range(1, n + 1):
+                yield bid, i, j, n
+
+
+def test_properties(state):
+    cfg, sim, tv = state
+    fx, fy = sim.fc(0, 1), sim.fc(1, 1)
+    cc = {"fld": sim.cc(5), "e": sim.cc(0), "phi": sim.cc(4)}
+    names, props = diagnostics.streamer_properties(
+        tv, cc, {"fx_fld": fx, "fy_fld": fy}, sim.table(), cfg.applied_fld, cfg.applied_voltage,
+        cfg.domain_len_z)
+    p = dict(zip(names, props))
+    assert len(names) == 39 and p["E_bg"] == cfg.applied_fld
+    ez = max(0.5 * abs(fy[b, (i - 1) + n * (j - 1)] + fy[b, (i - 1) + n * j])
+             for b, i, j, n in _leaf_cells(tv))
+    er = [(0.5 * abs(fx[b, (i - 1) + (n + 1) * (j - 1)] + fx[b, i + (n + 1) * (j - 1)]), b, i, j)
+          for b, i, j, n in _leaf_cells(tv)]
+    er_max = max(v for v, *_ in er)
+    assert p["Ez_max"] == ez and p["Er_max"] == er_max
+    b, i, j = next((b, i, j) for v, b, i, j in er if v == er_max)
+    assert p["Er_max(r)"] == tv.r_cc(b, i, j)[0] and p["Er_max(z)"] == tv.r_cc(b, i, j)[1]
+    # r_max(4e6): the largest cell-centre radius among leaf cells with |E| > 4 MV/m
+    fld = sim.cc(5)
+    hot = [tv.r_cc(b, i, j)[0] for b, i, j, n in _leaf_cells(tv) if fld[b, i + (n + 2) * j] > 4e6]
+    assert p["r_max(4e6)"] == (max(hot) if hot else 0.0)
+    assert np.all(np.isfinite(props))
+
+
+def test_get_loc_and_axis(state):
+    cfg, sim, tv = state
+    rng = np.random.default_rng(3)
+    R, Z = cfg.domain_len
+    for r, z in rng.uniform([0, 0], [R, Z], size=(200, 2)):
+        bid, (i, j) = tv.get_loc((r, z))
+        assert bid > 0
+        n, dr = tv.nc(bid), tv.dr(bid)
+        r0, r1 = tv.r_min(bid)
+        assert 1 <= i <= n and 1 <= j <= n
+        assert r0 + (i - 1) * dr <= r <= r0 + i * dr and r1 + (j - 1) * dr <= z <= r1 + j * dr
+        assert tv.children(bid)[0] == 0 or tv.lvl(bid) >= cfg.lvls_max
+    assert tv.get_loc((R + 1.0, 0.0))[0] == -1
+    ax = diagnostics.axis_data(tv, [sim.cc(0), sim.cc(1)], [sim.fc(1, 1), sim.fc(1, 0)])
+    assert ax.shape[0] == 5
+    z = ax[0]
+    assert np.all(np.diff(z) > 0) and z[0] > 0 and z[-1] < Z
+    # each axis cell is the first-column leaf cell containing its centre
+    # (on the axis itself, r = 0, the reference's ceiling gives cell index 0;
+    # get_cc_axis uses only the box there, so locate by a point just off it)
+    for k in range(0, ax.shape[1], 7):
+        bid, (i, j) = tv.get_loc((1e-12, z[k]))
+        n = tv.nc(bid)
+        assert i == 1 and ax[1, k] == sim.cc(0)[bid, 1 + (n + 2) * j]
