@@ -98,6 +98,7 @@ SIGNATURES = {
     "a5g_n_leaf_cells": (_I, [_P, ctypes.POINTER(ctypes.c_longlong)]),
     "a5g_get_stream": (_I, [_P, ctypes.POINTER(_P)]),
     "a5g_debug_set_staging": (_I, [_P, _I]),
+    "a5g_debug_info": (_I, [_P, ctypes.POINTER(ctypes.c_longlong)]),
     "a5g_debug_plans": (_I, [_I, _I, _I, _PI, _PD, _PI, _PI, _D, _PI, _PI, _P, _PI, _PD, _PI]),
     # host tree (include/a5t.h)
     "a5t_create": (_I, [_I, _I, _D, _PD, _I, ctypes.POINTER(_P)]),

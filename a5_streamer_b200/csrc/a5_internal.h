@@ -7,7 +7,8 @@ extern "C" {
 /* Record an error message for a5g_last_error() and return code. */
 int a5g_internal_fail(int code, const char *msg);
 /* Diagnostics: shared-memory doubles per multigrid variable, dynamic shared
- * memory per launch, capacity, levels, device limit, boxes. */
+ * memory per launch, capacity, levels, device limit, boxes, and for the mixed
+ * form the floats per staged FP32 array and the dynamic shared memory. */
 struct a5g_ctx;
 int a5g_debug_info(struct a5g_ctx *ctx, long long *out8);
 #ifdef __cplusplus

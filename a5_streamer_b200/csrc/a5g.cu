@@ -1190,6 +1190,23 @@ struct LevelPlan {
   int item;  // cell index within each colour of the box (row-major, nc/2 per row)
 };
 
+// Asynchronous 16-byte copies global -> shared (cp.async), used to fetch the
+// host-built plans of the next level while the current level's phases run.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  const size_t ga = __cvta_generic_to_global(gmem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(ga) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// The level index whose plans are being fetched into the slots (-1: none).
+// Every thread tracks the same value: the control flow of the multigrid is
+// uniform over the block.
+struct PlanFetch {
+  int li = -1;
+};
+
 template <class T>
 __device__ __forceinline__ bool plan_fits(const MGV<T> &M, const LvlInfo &L) {
   return M.plans && L.nb * ((L.nc * L.nc) >> 1) <= NTHR;
@@ -1199,7 +1216,7 @@ __device__ __forceinline__ bool plan_fits(const MGV<T> &M, const LvlInfo &L) {
 // reads only its own slots afterwards, so no barrier is needed.
 template <class T>
 __device__ __forceinline__ LevelPlan make_level_plan(const RunDev &R, const MGV<T> &M, const LvlInfo &L,
-                                                     bool cyl) {
+                                                     bool cyl, PlanFetch &pf) {
   LevelPlan P;
   const int half = (L.nc * L.nc) >> 1, hsh = 2 * L.sh - 1, hn = L.nc >> 1;
   const int k = threadIdx.x;
@@ -1207,6 +1224,14 @@ __device__ __forceinline__ LevelPlan make_level_plan(const RunDev &R, const MGV<
   P.item = k & (half - 1);
   if (k < L.nb * half) P.bx = L.b0 + (k >> hsh);
   const int blk = R.cplan_blk[L.li];
+  if (pf.li >= 0) {
+    // a fetch is in flight: let it land (it is this level's plans, or slots
+    // about to be overwritten)
+    cp_async_wait_all();
+    const bool mine = pf.li == L.li;
+    pf.li = -1;
+    if (mine) return P;
+  }
   if (blk >= 0) {
     // plans of this level built on the host at the topology upload
     const size_t o = (size_t)blk * 2 * NTHR + 2 * threadIdx.x;
@@ -1239,6 +1264,28 @@ __device__ __forceinline__ LevelPlan make_level_plan(const RunDev &R, const MGV<
     }
   }
   return P;
+}
+
+// Start fetching the host-built plans of level lvl into the slots (each
+// thread its own four 16-byte slots), to be taken by make_level_plan. Only
+// after the last read of the slots by the current level, which a barrier
+// separates from this call.
+template <class T>
+__device__ __forceinline__ void fetch_level_plan(const RunDev &R, const MGV<T> &M, int lvl, bool cyl,
+                                                 PlanFetch &pf) {
+  if (lvl < R.min_lvl || lvl > R.max_lvl || pf.li >= 0) return;
+  const LvlInfo L = lvl_info(R, lvl);
+  const int blk = R.cplan_blk[L.li];
+  if (!plan_fits(M, L) || blk < 0) return;
+  const size_t o = (size_t)blk * 2 * NTHR + 2 * threadIdx.x;
+  cp_async16(&plan_slots()[2 * threadIdx.x], &R.cplan[o]);
+  cp_async16(&plan_slots()[2 * threadIdx.x + 1], &R.cplan[o + 1]);
+  if (cyl) {
+    cp_async16(&wts_slots()[2 * threadIdx.x], &R.cwts[o]);
+    cp_async16(&wts_slots()[2 * threadIdx.x + 1], &R.cwts[o + 1]);
+  }
+  cp_async_commit();
+  pf.li = L.li;
 }
 
 // One red-black half-sweep `it` from the cell plans (p_sweep).
@@ -1314,12 +1361,14 @@ __device__ __forceinline__ void plan_fr(const RunDev &R, const MGV<T> &M, const 
 // coarse ghost fill + rhs; base: 2 n_cycle_base half-sweeps + ghost fill;
 // up: correction, 4 half-sweeps, ghost fill.
 template <class T>
-__device__ void p_vcycle(const RunDev &R, const MGV<T> &M, int max_lvl, bool stale_base) {
+__device__ __forceinline__ void vcycle_body(const RunDev &R, const MGV<T> &M, int max_lvl, bool stale_base,
+                                            PlanFetch &pf, int after) {
   const int min_lvl = R.min_lvl;
+  const bool cyl = R.coord == 1;
   for (int lvl = max_lvl; lvl >= min_lvl + 1; lvl--) {
     const LvlInfo L = lvl_info(R, lvl);
     if (plan_fits(M, L)) {
-      const LevelPlan P = make_level_plan(R, M, L, R.coord == 1);
+      const LevelPlan P = make_level_plan(R, M, L, cyl, pf);
       #pragma unroll 1
       for (int it = 1; it <= M.sw_down; it++) plan_sweep(R, M, L, P, it, false);
       plan_fr(R, M, L, P, lvl);
@@ -1327,23 +1376,25 @@ __device__ void p_vcycle(const RunDev &R, const MGV<T> &M, int max_lvl, bool sta
       for (int it = 1; it <= M.sw_down; it++) p_sweep(R, M, lvl, it, false);
       p_fr(R, M, lvl, true, false, false);
     }
+    fetch_level_plan(R, M, lvl - 1, cyl, pf);
     p_fc(R, M, lvl - 1, true);
   }
   {
     const LvlInfo L = lvl_info(R, min_lvl);
     if (plan_fits(M, L)) {
-      const LevelPlan P = make_level_plan(R, M, L, R.coord == 1);
+      const LevelPlan P = make_level_plan(R, M, L, cyl, pf);
       #pragma unroll 1
       for (int it = 1; it <= M.sw_base; it++) plan_sweep(R, M, L, P, it, stale_base && it == 1);
     } else {
       for (int it = 1; it <= M.sw_base; it++) p_sweep(R, M, min_lvl, it, stale_base && it == 1);
     }
   }
+  fetch_level_plan(R, M, min_lvl < max_lvl ? min_lvl + 1 : after, cyl, pf);
   p_fill(R, M, min_lvl);
   for (int lvl = min_lvl + 1; lvl <= max_lvl; lvl++) {
     const LvlInfo L = lvl_info(R, lvl);
     if (plan_fits(M, L)) {
-      const LevelPlan P = make_level_plan(R, M, L, R.coord == 1);
+      const LevelPlan P = make_level_plan(R, M, L, cyl, pf);
       p_correct(R, M, lvl, false, true);
       #pragma unroll 1
       for (int it = 1; it <= M.sw_up; it++) plan_sweep(R, M, L, P, it, false);
@@ -1351,8 +1402,23 @@ __device__ void p_vcycle(const RunDev &R, const MGV<T> &M, int max_lvl, bool sta
       p_correct(R, M, lvl, false, true);
       for (int it = 1; it <= M.sw_up; it++) p_sweep(R, M, lvl, it, false);
     }
+    fetch_level_plan(R, M, lvl < max_lvl ? lvl + 1 : after, cyl, pf);
     p_fill(R, M, lvl);
   }
+}
+
+// The FP64 V-cycle is inlined into its caller; the FP32 one (mixed form) is
+// kept out of line, which keeps the register allocation of the kernels that
+// contain both forms free of spills in the FP64 phases.
+template <class T>
+__device__ __forceinline__ void p_vcycle(const RunDev &R, const MGV<T> &M, int max_lvl, bool stale_base,
+                                         PlanFetch &pf, int after) {
+  vcycle_body<T>(R, M, max_lvl, stale_base, pf, after);
+}
+template <>
+__device__ __noinline__ void p_vcycle<float>(const RunDev &R, const MGV<float> &M, int max_lvl, bool stale_base,
+                                             PlanFetch &pf, int after) {
+  vcycle_body<float>(R, M, max_lvl, stale_base, pf, after);
 }
 
 // mg$D_fas_fmg, m_aX_mg.f90:163-202. leaf_rhs: compute the space charge of
@@ -1370,11 +1436,13 @@ __device__ void p_fmg_in(const RunDev &R, const MGV<T> &M, bool set_residual, bo
       p_fc(R, M, lvl - 1, false);
     }
   }
+  PlanFetch pf;
   for (int lvl = min_lvl; lvl <= max_lvl; lvl++) {
     p_correct(R, M, lvl, true, lvl > min_lvl);
-    p_vcycle(R, M, lvl, first_call && lvl == min_lvl);
+    p_vcycle(R, M, lvl, first_call && lvl == min_lvl, pf, lvl + 1);
     if (set_residual && lvl == max_lvl) p_residual_all(R, M, lvl);
   }
+  if (pf.li >= 0) cp_async_wait_all();
 }
 
 // Copy the multigrid variables of every box between device memory and the
@@ -1485,6 +1553,10 @@ __device__ void p_fmg(const RunDev &R, bool set_residual, bool first_call, bool 
 // potential, so this is one FAS cycle on phi whose smoothing runs in FP32,
 // while the residual (which cancels) and the accumulation stay in FP64.
 
+// Step 1 on level lvl, one cell per thread; whole warps iterate together so
+// that the restriction can gather a 2x2 quad by warp shuffles (the cells of
+// a box are consecutive threads, i fastest, and a quad's rows lie in one
+// warp). The lane of the quad's lower-left cell writes the parent cell.
 __device__ __noinline__ void p_mx_residual(const RunDev &R, const MGV<float> &M, int lvl) {
   const LvlInfo L = lvl_info(R, lvl);
   const bool down = lvl > R.min_lvl;
@@ -1494,39 +1566,43 @@ __device__ __noinline__ void p_mx_residual(const RunDev &R, const MGV<float> &M,
   float *ce = M.phi, *cr = M.rhs, *ct = M.tmp;
   const double inv_dr_sq = 1 / (L.dr * L.dr);
   const double fac = UC_ELEM_CHARGE / UC_EPS0;
-  const int hn = L.nc >> 1, per = hn * hn, n = L.nb * per;
-  for (int k = threadIdx.x; k < n; k += NTHR) {
-    const int b = L.b0 + (k >> (2 * L.sh - 2));
+  const int per = L.nc * L.nc, n = L.nb * per, nw = (n + 31) & ~31;
+  for (int k = threadIdx.x; k < nw; k += NTHR) {
+    const bool act = k < n;
+    const int b = L.b0 + (act ? k >> (2 * L.sh) : 0);
     const BoxRec &B = R.boxes[b];  // device-memory slots (phi, rhs, densities)
     const BoxRec &S = M.boxes[b];  // slots of the FP32 arrays
-    const int t = k & (per - 1), ii = (t & (hn - 1)) + 1, jj = (t >> (L.sh - 1)) + 1;
-    const bool leaf = (B.flags & CF_LEAF) != 0;
-    double rs[4], ps[4], hs[4];
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-      const int i = 2 * ii - 1 + (q & 1), j = 2 * jj - 1 + (q >> 1);
-      const int loc = i + L.ncg * j, g = B.base + loc, sc = S.base + loc;
-      double rh, res;
-      if (leaf) {
+    const int t = k & (per - 1), i = (t & (L.nc - 1)) + 1, j = (t >> L.sh) + 1;
+    const int g = B.base + i + L.ncg * j, sc = S.base + i + L.ncg * j;
+    double res = 0, ph = 0, rh = 0;
+    if (act) {
+      if (B.flags & CF_LEAF) {
         rh = fac * (e[g] - pi[g]);
-        rhs[g] = rh;
         res = rh - lap_at(R, R.applied_voltage, (const double *)phi, B, L.nc, L.ncg, i, j, inv_dr_sq);
+        rhs[g] = rh;
         cr[sc] = (float)res;
       } else {
         rh = rhs[g];
         res = (double)cr[sc];
       }
+      ph = phi[g];
       ce[sc] = 0.0f;
       ct[sc] = 0.0f;
-      rs[q] = res;
-      ps[q] = phi[g];
-      hs[q] = rh;
     }
     if (down) {
-      const int o = (B.o0 + ii) + pncg * (B.o1 + jj);
-      cr[S.pbase + o] = (float)(0.25 * (rs[0] + rs[1] + rs[2] + rs[3]));
-      phi[B.pbase + o] = 0.25 * (ps[0] + ps[1] + ps[2] + ps[3]);
-      rhs[B.pbase + o] = 0.25 * (hs[0] + hs[1] + hs[2] + hs[3]);
+      const unsigned FULL = 0xffffffffu;
+      const double r1 = __shfl_down_sync(FULL, res, 1), r2 = __shfl_down_sync(FULL, res, L.nc),
+                   r3 = __shfl_down_sync(FULL, res, L.nc + 1);
+      const double p1 = __shfl_down_sync(FULL, ph, 1), p2 = __shfl_down_sync(FULL, ph, L.nc),
+                   p3 = __shfl_down_sync(FULL, ph, L.nc + 1);
+      const double h1 = __shfl_down_sync(FULL, rh, 1), h2 = __shfl_down_sync(FULL, rh, L.nc),
+                   h3 = __shfl_down_sync(FULL, rh, L.nc + 1);
+      if (act && (i & 1) && (j & 1)) {
+        const int o = (B.o0 + (i + 1) / 2) + pncg * (B.o1 + (j + 1) / 2);
+        cr[S.pbase + o] = (float)(0.25 * (res + r1 + r2 + r3));
+        phi[B.pbase + o] = 0.25 * (ph + p1 + p2 + p3);
+        rhs[B.pbase + o] = 0.25 * (rh + h1 + h2 + h3);
+      }
     }
   }
   // side ghosts of c and of its tmp start at zero (consistent with c = 0 and V = 0)
@@ -1561,7 +1637,9 @@ __device__ void p_mx_accumulate(const RunDev &R, const MGV<float> &M) {
 
 // The mixed-precision solve of compute_fld (see above): the FP32 arrays are
 // in shared memory when the tree fits (mx_smem floats per variable), else in
-// the run's FP32 storage cc32.
+// the run's FP32 storage cc32. The FP64 potential and rhs stay in device
+// memory: staging them too (with the FP32 arrays) was measured slower, the
+// copies in and out costing more than the residual and accumulation save.
 __device__ void p_solve_mixed(const RunDev &R) {
   MGV<float> M;
   if (R.mx_smem > 0) {
@@ -1582,18 +1660,23 @@ __device__ void p_solve_mixed(const RunDev &R) {
     M = MGV<float>{R.cc32, R.cc32 + n, R.cc32 + 2 * n, R.boxes, R.pbx, false, 0.0, R.mx_sw_down,
                    R.mx_sw_up, R.mx_sw_base};
   }
+  PlanFetch pf;
   for (int pass = 0; pass < R.mx_n_corr; pass++) {
     for (int lvl = R.max_lvl; lvl >= R.min_lvl; lvl--) p_mx_residual(R, M, lvl);
+    // the plans that follow the last V-cycle of a pass: those of the next
+    // pass's first V-cycle (fetched while the FP64 phases run), or none
+    const int next = pass + 1 < R.mx_n_corr ? (R.mx_fmg ? R.min_lvl : R.max_lvl) : R.max_lvl + 1;
     if (R.mx_fmg) {
       for (int lvl = R.min_lvl; lvl <= R.max_lvl; lvl++) {
         p_correct(R, M, lvl, true, lvl > R.min_lvl);
-        p_vcycle(R, M, lvl, false);
+        p_vcycle(R, M, lvl, false, pf, lvl < R.max_lvl ? lvl + 1 : next);
       }
     } else {
-      p_vcycle(R, M, R.max_lvl, false);
+      p_vcycle(R, M, R.max_lvl, false, pf, next);
     }
     p_mx_accumulate(R, M);
   }
+  if (pf.li >= 0) cp_async_wait_all();
 }
 // a$D_gc_tree(iv, a$D_gc_interp[_lim], a$D_gc_neumann) for one or two
 // variables, levels ascending (m_aX_gc.f90:28-46, 90-330)
@@ -4200,8 +4283,8 @@ int a5g_debug_info(a5g_ctx *c, long long *out8) {
   out8[3] = c->h.nlev;
   out8[4] = (long long)dyn_smem_limit();
   out8[5] = c->h.bx_off[c->h.nlev];
-  out8[6] = 0;
-  out8[7] = 0;
+  out8[6] = c->h.mx_smem;
+  out8[7] = (long long)c->dyn_smem32;
   return A5G_OK;
 }
 

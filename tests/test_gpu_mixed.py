@@ -10,6 +10,8 @@ Bounds, stated against the FP64 oracle on identical inputs:
   - with the reference's own multigrid schedule, the mixed solve tracks the
     FP64 solve to 1e-6 relative in phi and |E|.
 """
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -98,6 +100,12 @@ def test_mixed_batch_equals_single():
     compare(sim, c, where="fp64 member of a mixed batch")
 
 
+def _staging(run):
+    info = (ctypes.c_longlong * 8)()
+    call("a5g_debug_info", run.h, info)
+    return info[6]  # floats per staged FP32 array of the mixed form (0: device memory)
+
+
 @pytest.mark.parametrize("mixed", [False, True])
 def test_device_memory_path(mixed):
     """Multigrid without shared-memory staging (the path of trees larger than
@@ -109,11 +117,12 @@ def test_device_memory_path(mixed):
     if mixed:
         staged = device_from_oracle(sim, cfg)
         for r in (run, staged):
-            r.set_precision(True, (0, 2, 2, 4, 1))
+            r.set_precision(True, (0, 2, 2, 4, 2))
+        assert _staging(staged) > 0 and _staging(run) == 0
         for _ in range(3):
             run.step(DT)
             staged.step(DT)
-        for iv in (dv.I_PHI, dv.I_FLD, dv.I_ELEC):
+        for iv in (dv.I_PHI, dv.I_FLD, dv.I_ELEC, dv.I_RHS):
             assert np.array_equal(run.cc(iv), staged.cc(iv)), iv
     else:
         for _ in range(3):
