@@ -927,32 +927,39 @@ __device__ __noinline__ void p_fr(const RunDev &R, const MGV<T> &M, int lvl, boo
   const double *e = VAR(R, I_ELEC), *pi = VAR(R, I_PION);
   const T inv_dr_sq = T(1 / (L.dr * L.dr));
   const double fac = UC_ELEM_CHARGE / UC_EPS0;
-  const int hn = L.nc >> 1, per = hn * hn, n = L.nb * per;
-  for (int k = threadIdx.x; k < n; k += NTHR) {
-    const BoxRec &B = M.boxes[L.b0 + (k >> (2 * L.sh - 2))];
-    const int t = k & (per - 1), ii = (t & (hn - 1)) + 1, jj = (t >> (L.sh - 1)) + 1;
-    const bool leaf = leaf_rhs && (B.flags & CF_LEAF);
-    T rs[4], ps[4];
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-      const int i = 2 * ii - 1 + (q & 1), j = 2 * jj - 1 + (q >> 1);
-      const int g = B.base + i + L.ncg * j;
+  // one cell per thread, whole warps per iteration: the 2x2 block of a
+  // parent cell is gathered by shuffles (cells of a box are consecutive
+  // threads, i fastest) and added in the order of box_rstr_lpl
+  const int per = L.nc * L.nc, n = L.nb * per, nw = (n + 31) & ~31;
+  for (int k = threadIdx.x; k < nw; k += NTHR) {
+    const bool act = k < n;
+    const BoxRec &B = M.boxes[L.b0 + (act ? k >> (2 * L.sh) : 0)];
+    const int t = k & (per - 1), i = (t & (L.nc - 1)) + 1, j = (t >> L.sh) + 1;
+    const int g = B.base + i + L.ncg * j;
+    T res = 0, ph = 0;
+    if (act) {
       T rh;
-      if (leaf) {
+      if (leaf_rhs && (B.flags & CF_LEAF)) {
         const int gg = B.gbase + i + L.ncg * j;
         rh = T(fac * (e[gg] - pi[gg]));
         rhs[g] = rh;
       } else {
         rh = rhs[g];
       }
-      const T res = rh - lap_at(R, M.V, phi, B, L.nc, L.ncg, i, j, inv_dr_sq);
+      res = rh - lap_at(R, M.V, phi, B, L.nc, L.ncg, i, j, inv_dr_sq);
       if (store_res) tmp[g] = res;
-      rs[q] = res;
-      ps[q] = phi[g];
+      ph = phi[g];
     }
-    const int d = B.pbase + (B.o0 + ii) + pncg * (B.o1 + jj);
-    tmp[d] = T(0.25) * (rs[0] + rs[1] + rs[2] + rs[3]);
-    phi[d] = T(0.25) * (ps[0] + ps[1] + ps[2] + ps[3]);
+    const unsigned FULL = 0xffffffffu;
+    const T r1 = __shfl_down_sync(FULL, res, 1), r2 = __shfl_down_sync(FULL, res, L.nc),
+            r3 = __shfl_down_sync(FULL, res, L.nc + 1);
+    const T p1 = __shfl_down_sync(FULL, ph, 1), p2 = __shfl_down_sync(FULL, ph, L.nc),
+            p3 = __shfl_down_sync(FULL, ph, L.nc + 1);
+    if (act && (i & 1) && (j & 1)) {
+      const int d = B.pbase + (B.o0 + (i + 1) / 2) + pncg * (B.o1 + (j + 1) / 2);
+      tmp[d] = T(0.25) * (res + r1 + r2 + r3);
+      phi[d] = T(0.25) * (ph + p1 + p2 + p3);
+    }
   }
   if (fill) fill_phi_loop(R, M, L, false);
   __syncthreads();
@@ -2050,6 +2057,15 @@ __device__ __forceinline__ int mz_int4(int st[4]) {
 // uni_01 (fosito/m_random.f90:75-80)
 __device__ __forceinline__ double mz_uni01(int st[4]) { return 0.5 + 0x1p-32 * (double)mz_int4(st); }
 
+// x mod m for any 64-bit x (here a row of a jump matrix times a state),
+// from 2^31 = m + 69: two folds x -> (x mod 2^31) + 69 floor(x / 2^31) bring
+// x below 2^31 + 69 * 2^9 < 2m, one conditional subtraction finishes.
+__device__ __forceinline__ unsigned mz_mod(unsigned long long x) {
+  x = (x & 0x7fffffffull) + 69ull * (x >> 31);
+  x = (x & 0x7fffffffull) + 69ull * (x >> 31);
+  return (unsigned)(x >= MZ_M ? x - MZ_M : x);
+}
+
 // Advance the master generator by k draws. While s1, s2, s3 all lie in
 // [0, m) a draw maps (s1, s2, s3) to (s2, s3, s1 - s3 mod m), a linear map
 // mod m, and s4 to 69069 s4 + 1013904243 mod 2^32; J[b] holds both maps for
@@ -2071,8 +2087,8 @@ __device__ void mz_advance(int st[4], unsigned long long k, const MzJump *J) {
     unsigned int n[3];
 #pragma unroll
     for (int r = 0; r < 3; r++)
-      n[r] = (unsigned)(((unsigned long long)j.m[3 * r] * v0 + (unsigned long long)j.m[3 * r + 1] * v1 +
-                         (unsigned long long)j.m[3 * r + 2] * v2) % MZ_M);
+      n[r] = mz_mod((unsigned long long)j.m[3 * r] * v0 + (unsigned long long)j.m[3 * r + 1] * v1 +
+                    (unsigned long long)j.m[3 * r + 2] * v2);
     st[0] = (int)n[0];
     st[1] = (int)n[1];
     st[2] = (int)n[2];
