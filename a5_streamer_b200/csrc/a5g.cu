@@ -816,6 +816,33 @@ __device__ __forceinline__ LvlInfo lvl_info(const RunDev &R, int lvl) {
   return L;
 }
 
+// Cursor over the interior cells of every box of every level, level by
+// level in plan order, for flat loops in which each thread moves forward:
+// cells of different levels can then be in flight together.
+struct CellCursor {
+  int li, lo, hi;  // level index and the flat range [lo, hi) of its cells
+};
+__device__ __forceinline__ int level_cells(const RunDev &R, int li) {
+  return (R.bx_off[li + 1] - R.bx_off[li]) * R.lv_nc[li] * R.lv_nc[li];
+}
+__device__ __forceinline__ CellCursor cell_cursor(const RunDev &R) { return CellCursor{0, 0, level_cells(R, 0)}; }
+// Flat cell k (not below the previous call's k) as level index, box record
+// index and (i, j); false past the last level.
+__device__ __forceinline__ bool cell_at(const RunDev &R, CellCursor &c, int k, int &li, int &b, int &i,
+                                        int &j) {
+  while (k >= c.hi) {
+    if (++c.li >= R.nlev) return false;
+    c.lo = c.hi;
+    c.hi = c.lo + level_cells(R, c.li);
+  }
+  li = c.li;
+  const int nc = R.lv_nc[li], sh = 31 - __clz(nc), t = k - c.lo;
+  b = R.bx_off[li] + (t >> (2 * sh));
+  i = (t & (nc - 1)) + 1;
+  j = ((t >> sh) & (nc - 1)) + 1;
+  return true;
+}
+
 // Red-black Gauss-Seidel half-sweep `it` on level lvl (box_gsrb_lpl,
 // m_aX_mg.f90:636-659; box_gsrb_clpl :998-1024). Ghost neighbours are
 // evaluated from their sources, which equals the ghost fill the reference
@@ -1763,31 +1790,43 @@ __device__ __forceinline__ double face_fld(const double *phi, const double *eps,
 
 // fld_from_pot on every box in one phase (each cell writes its low faces and,
 // on the high box edges, the high faces; |E| from its four faces), then the
-// |E| ghost fill a$D_gc_tree(i_fld, a$D_gc_interp, a$D_gc_neumann).
-__device__ void p_fld_from_pot(const RunDev &R) {
+// |E| ghost fill a$D_gc_tree(i_fld, a$D_gc_interp, a$D_gc_neumann). A thread
+// takes two cells per round, all levels in one flat range, and loads both
+// before it stores either.
+__device__ __noinline__ void p_fld_from_pot(const RunDev &R) {
   const double *phi = VAR(R, I_PHI), *eps = VAR(R, I_EPS);
   double *fld = VAR(R, I_FLD);
-  for (int lvl = R.min_lvl; lvl <= R.max_lvl; lvl++) {
-    const LvlInfo L = lvl_info(R, lvl);
-    const double inv_dr = 1 / L.dr;
-    const int per = L.nc * L.nc, n = L.nb * per;
-    for (int k = threadIdx.x; k < n; k += NTHR) {
-      const BoxRec &B = R.boxes[L.b0 + (k >> (2 * L.sh))];
-      const int t = k & (per - 1), i = (t & (L.nc - 1)) + 1, j = (t >> L.sh) + 1;
-      const int g = B.base + i + L.ncg * j;
-      const int nc = L.nc, ncg = L.ncg;
-      const double fxl = face_fld(phi, eps, g, 1, i, nc, inv_dr);
-      const double fxh = face_fld(phi, eps, g + 1, 1, i + 1, nc, inv_dr);
-      const double fyl = face_fld(phi, eps, g, ncg, j, nc, inv_dr);
-      const double fyh = face_fld(phi, eps, g + ncg, ncg, j + 1, nc, inv_dr);
-      const int id = B.base / SLOT;
+  CellCursor cur = cell_cursor(R);
+  for (int k = threadIdx.x;; k += 2 * NTHR) {
+    int li[2], b[2], ci[2], cj[2];
+    bool ok[2];
+    ok[0] = cell_at(R, cur, k, li[0], b[0], ci[0], cj[0]);
+    ok[1] = ok[0] && cell_at(R, cur, k + NTHR, li[1], b[1], ci[1], cj[1]);
+    if (!ok[0]) break;
+    double f[2][4];
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      if (!ok[u]) continue;
+      const int nc = R.lv_nc[li[u]], ncg = nc + 2, i = ci[u], j = cj[u];
+      const double inv_dr = 1 / R.lv_dr[li[u]];
+      const int g = R.boxes[b[u]].base + i + ncg * j;
+      f[u][0] = face_fld(phi, eps, g, 1, i, nc, inv_dr);
+      f[u][1] = face_fld(phi, eps, g + 1, 1, i + 1, nc, inv_dr);
+      f[u][2] = face_fld(phi, eps, g, ncg, j, nc, inv_dr);
+      f[u][3] = face_fld(phi, eps, g + ncg, ncg, j + 1, nc, inv_dr);
+    }
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      if (!ok[u]) continue;
+      const int nc = R.lv_nc[li[u]], ncg = nc + 2, i = ci[u], j = cj[u];
+      const int base = R.boxes[b[u]].base, id = base / SLOT;
       double *fxf = FX(R, F_FLD, id), *fyf = FY(R, F_FLD, id);
-      fxf[fxi(i, j, nc)] = fxl;
-      if (i == nc) fxf[fxi(nc + 1, j, nc)] = fxh;
-      fyf[fyi(i, j, nc)] = fyl;
-      if (j == nc) fyf[fyi(i, nc + 1, nc)] = fyh;
-      const double sx = fxl + fxh, sy = fyl + fyh;
-      fld[g] = sqrt(0.25 * (sx * sx) + 0.25 * (sy * sy));
+      fxf[fxi(i, j, nc)] = f[u][0];
+      if (i == nc) fxf[fxi(nc + 1, j, nc)] = f[u][1];
+      fyf[fyi(i, j, nc)] = f[u][2];
+      if (j == nc) fyf[fyi(i, nc + 1, nc)] = f[u][3];
+      const double sx = f[u][0] + f[u][1], sy = f[u][2] + f[u][3];
+      fld[base + i + ncg * j] = sqrt(0.25 * (sx * sx) + 0.25 * (sy * sy));
     }
   }
   __syncthreads();
