@@ -165,6 +165,13 @@ struct MzJump {
   unsigned int a, c;
 };
 constexpr int MZ_NJUMP = 40;
+constexpr int PH_THREADS = 256;  // threads per block of the absorption kernel
+// Layout of a run's jump table: MZ_NJUMP jumps of 2^b draws; the jumps of
+// 4t draws, t < PH_THREADS (a thread of an absorption block from its block's
+// generator); the jump of 8W draws (the master's advance per step, W the
+// team); the jumps of 4W + 4 PH_THREADS b draws, b < ceil(W / PH_THREADS)
+// (absorption block b from the master).
+constexpr int MZ_JTHR = MZ_NJUMP, MZ_JSTEP = MZ_JTHR + PH_THREADS, MZ_JBLK = MZ_JSTEP + 1;
 // Per box geometry for the absorption-location descent (a$D_get_loc).
 struct PhBox {
   double r0, r1, dr;
@@ -2110,29 +2117,36 @@ __device__ __forceinline__ unsigned mz_mod(unsigned long long x) {
 // mod m, and s4 to 69069 s4 + 1013904243 mod 2^32; J[b] holds both maps for
 // 2^b draws. Outside that range (a seed set by the caller) the draws are
 // stepped one by one until the state enters it; it then stays there.
+__device__ __forceinline__ bool mz_clean(const int st[4]) {
+  return st[0] >= 0 && st[0] < (int)MZ_M && st[1] >= 0 && st[1] < (int)MZ_M && st[2] >= 0 &&
+         st[2] < (int)MZ_M;
+}
+// One jump (a clean state stays clean).
+__device__ __forceinline__ void mz_apply(int st[4], const MzJump &j) {
+  const unsigned long long v0 = (unsigned)st[0], v1 = (unsigned)st[1], v2 = (unsigned)st[2];
+  unsigned int n[3];
+#pragma unroll
+  for (int r = 0; r < 3; r++)
+    n[r] = mz_mod((unsigned long long)j.m[3 * r] * v0 + (unsigned long long)j.m[3 * r + 1] * v1 +
+                  (unsigned long long)j.m[3 * r + 2] * v2);
+  st[0] = (int)n[0];
+  st[1] = (int)n[1];
+  st[2] = (int)n[2];
+  st[3] = (int)(j.a * (unsigned)st[3] + j.c);
+}
 __device__ void mz_advance(int st[4], unsigned long long k, const MzJump *J) {
-  auto clean = [&]() {
-    return st[0] >= 0 && st[0] < (int)MZ_M && st[1] >= 0 && st[1] < (int)MZ_M && st[2] >= 0 &&
-           st[2] < (int)MZ_M;
-  };
-  while (k > 0 && !clean()) {
+  while (k > 0 && !mz_clean(st)) {
     mz_int4(st);
     k--;
   }
-  for (int b = 0; k != 0 && b < MZ_NJUMP; b++, k >>= 1) {
-    if (!(k & 1)) continue;
-    const MzJump &j = J[b];
-    const unsigned long long v0 = (unsigned)st[0], v1 = (unsigned)st[1], v2 = (unsigned)st[2];
-    unsigned int n[3];
-#pragma unroll
-    for (int r = 0; r < 3; r++)
-      n[r] = mz_mod((unsigned long long)j.m[3 * r] * v0 + (unsigned long long)j.m[3 * r + 1] * v1 +
-                    (unsigned long long)j.m[3 * r + 2] * v2);
-    st[0] = (int)n[0];
-    st[1] = (int)n[1];
-    st[2] = (int)n[2];
-    st[3] = (int)(j.a * (unsigned)st[3] + j.c);
-  }
+  for (int b = 0; k != 0 && b < MZ_NJUMP; b++, k >>= 1)
+    if (k & 1) mz_apply(st, J[b]);
+}
+// Advance by k draws where J[pre] is the jump of exactly k draws: one
+// application from a clean state, mz_advance otherwise (a fresh seed).
+__device__ __forceinline__ void mz_advance_pre(int st[4], unsigned long long k, const MzJump *J, int pre) {
+  if (mz_clean(st)) mz_apply(st, J[pre]);
+  else mz_advance(st, k, J);
 }
 
 // libgomp's static schedule without a chunk size: thread c of W gets the
@@ -2385,7 +2399,7 @@ __device__ void ph_source(const RunDev &R, double dt, bool has_dt) {
     // the master has given 4W draws to the creation team and gives 4W to
     // the absorption team
     int st[4] = {st0[0], st0[1], st0[2], st0[3]};
-    mz_advance(st, 8ull * (unsigned long long)W, R.ph_jump);
+    mz_advance_pre(st, 8ull * (unsigned long long)W, R.ph_jump, MZ_JSTEP);
     for (int q = 0; q < 4; q++) R.ph_rng[q] = st[q];
   }
   __syncthreads();
@@ -2663,7 +2677,6 @@ __global__ void __launch_bounds__(NTHR, 1) a5g_run_kernel_slots(const BatchSlot 
 // number is not above it. blockIdx.y selects the run of a batch. The per-box
 // geometry and the box ranks are staged in shared memory when they fit
 // (ph_smem: bytes available).
-constexpr int PH_THREADS = 256;
 __device__ __forceinline__ int ph_cell_index(int t) { return (t % NC + 1) + (NC + 2) * (t / NC + 1); }
 
 __global__ void __launch_bounds__(PH_THREADS) a5g_photon_kernel(const RunDev *single,
@@ -2698,12 +2711,12 @@ __global__ void __launch_bounds__(PH_THREADS) a5g_photon_kernel(const RunDev *si
   // Generator of team thread w: the master's state at draw 4W + 4w. One
   // thread jumps the master to the block's first team thread (4W + 4 w0),
   // then every thread jumps from there by 4 threadIdx.x: jumps compose
-  // exactly, and the per-thread jump needs at most 10 doublings instead of
-  // about 19.
+  // exactly. Both jumps are single precomputed matrices of the run's table.
   __shared__ int s_base[4];
   if (threadIdx.x == 0) {
     int b[4] = {R.ph_scal->st0[0], R.ph_scal->st0[1], R.ph_scal->st0[2], R.ph_scal->st0[3]};
-    mz_advance(b, 4ull * (unsigned long long)W + 4ull * (unsigned long long)w0, R.ph_jump);
+    mz_advance_pre(b, 4ull * (unsigned long long)W + 4ull * (unsigned long long)w0, R.ph_jump,
+                   MZ_JBLK + (int)blockIdx.x);
 #pragma unroll
     for (int q = 0; q < 4; q++) s_base[q] = b[q];
   }
@@ -2714,7 +2727,7 @@ __global__ void __launch_bounds__(PH_THREADS) a5g_photon_kernel(const RunDev *si
   static_chunk(n_used, W, w, lo, len);
   if (len == 0) return;
   int st[4] = {s_base[0], s_base[1], s_base[2], s_base[3]};
-  mz_advance(st, 4ull * (unsigned long long)threadIdx.x, R.ph_jump);
+  mz_advance_pre(st, 4ull * (unsigned long long)threadIdx.x, R.ph_jump, MZ_JTHR + (int)threadIdx.x);
   int rs[4];
 #pragma unroll
   for (int q = 0; q < 4; q++) rs[q] = mz_int4(st);
@@ -3184,6 +3197,38 @@ static void mz_jump_table(MzJump *J) {
   }
 }
 
+// a followed by b (jumps are powers of one map, so the order does not matter)
+static MzJump mz_compose(const MzJump &a, const MzJump &b) {
+  const unsigned long long m = MZ_M;
+  MzJump r;
+  for (int i = 0; i < 3; i++)
+    for (int q = 0; q < 3; q++)
+      r.m[3 * i + q] = (unsigned int)(((unsigned long long)b.m[3 * i] * a.m[q] % m +
+                                       (unsigned long long)b.m[3 * i + 1] * a.m[3 + q] % m +
+                                       (unsigned long long)b.m[3 * i + 2] * a.m[6 + q] % m) % m);
+  r.a = b.a * a.a;
+  r.c = b.a * a.c + b.c;
+  return r;
+}
+// The jump of k draws from the 2^b jumps.
+static MzJump mz_power(const MzJump *J, unsigned long long k) {
+  MzJump r{{1, 0, 0, 0, 1, 0, 0, 0, 1}, 1u, 0u};
+  for (int b = 0; k != 0 && b < MZ_NJUMP; b++, k >>= 1)
+    if (k & 1) r = mz_compose(r, J[b]);
+  return r;
+}
+// A run's whole jump table (layout at MZ_JTHR), for a team of W threads.
+static std::vector<MzJump> mz_run_table(long long W) {
+  const int nblk = (int)((W + PH_THREADS - 1) / PH_THREADS);
+  std::vector<MzJump> T(MZ_JBLK + nblk);
+  mz_jump_table(T.data());
+  for (int t = 0; t < PH_THREADS; t++) T[MZ_JTHR + t] = mz_power(T.data(), 4ull * t);
+  T[MZ_JSTEP] = mz_power(T.data(), 8ull * (unsigned long long)W);
+  for (int b = 0; b < nblk; b++)
+    T[MZ_JBLK + b] = mz_power(T.data(), 4ull * (unsigned long long)W + 4ull * PH_THREADS * b);
+  return T;
+}
+
 // Photon buffers sized for the current box capacity: per cell a draw, a
 // first photon number and an absorption count; per box and per team thread
 // scratch. At most num_photons + one per leaf cell are created (the expected
@@ -3317,16 +3362,16 @@ int a5g_create(const a5g_params *p, a5g_ctx **out) {
   h.mx_sw_base = 2 * p->n_cycle_base;
   h.mx_n_corr = 1;
   if (p->photoi_enabled) {
-    MzJump J[MZ_NJUMP];
-    mz_jump_table(J);
+    const std::vector<MzJump> J = mz_run_table(p->photoi_team);
+    const size_t jbytes = J.size() * sizeof(MzJump);
     if (cudaMalloc(&c->ph_rng, 4 * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&c->ph_scal, sizeof(PhScal)) != cudaSuccess ||
-        cudaMalloc(&c->ph_jump, sizeof(J)) != cudaSuccess) {
+        cudaMalloc(&c->ph_jump, jbytes) != cudaSuccess) {
       a5g_destroy(c);
       return fail(A5G_ENOMEM, "cudaMalloc failed");
     }
     cudaMemcpy(c->ph_rng, p->rng_seed, 4 * sizeof(int), cudaMemcpyHostToDevice);
-    cudaMemcpy(c->ph_jump, J, sizeof(J), cudaMemcpyHostToDevice);
+    cudaMemcpy(c->ph_jump, J.data(), jbytes, cudaMemcpyHostToDevice);
     cudaMemset(c->ph_scal, 0, sizeof(PhScal));
     h.ph_enabled = 1;
     h.ph_team = p->photoi_team;
