@@ -166,6 +166,12 @@ struct MzJump {
 };
 constexpr int MZ_NJUMP = 40;
 constexpr int PH_THREADS = 256;  // threads per block of the absorption kernel
+// Resident absorption blocks per SM the register allocation is bounded for
+// (8 x 256 threads: 32 registers a thread, a few spilled). The loop is
+// latency-bound (L1/L2 loads, atomics); with twice the warps of the
+// unbounded allocation (58 registers, 4 blocks) the 148-run batched step
+// took 1.44 ms instead of 1.58 ms (6 blocks: 1.47 ms).
+constexpr int PH_BLOCKS_PER_SM = 8;
 // Layout of a run's jump table: MZ_NJUMP jumps of 2^b draws; the jumps of
 // 4t draws, t < PH_THREADS (a thread of an absorption block from its block's
 // generator); the jump of 8W draws (the master's advance per step, W the
@@ -2679,12 +2685,21 @@ __global__ void __launch_bounds__(NTHR, 1) a5g_run_kernel_slots(const BatchSlot 
 // (ph_smem: bytes available).
 __device__ __forceinline__ int ph_cell_index(int t) { return (t % NC + 1) + (NC + 2) * (t / NC + 1); }
 
-__global__ void __launch_bounds__(PH_THREADS) a5g_photon_kernel(const RunDev *single,
+__global__ void __launch_bounds__(PH_THREADS, PH_BLOCKS_PER_SM) a5g_photon_kernel(const RunDev *single,
                                                                const RunDev *const *runs,
                                                                const BatchSlot *slots,
                                                                int ph_smem) {
   const RunDev *rp = runs ? runs[blockIdx.y] : slots ? slots[blockIdx.y].run : single;
-  const RunDev &R = *rp;
+  // the run's descriptor in shared memory: the photon loop reads its fields
+  // after every atomic, which the compiler cannot keep in registers
+  __shared__ RunDev sR;
+  {
+    const int *src = reinterpret_cast<const int *>(rp);
+    int *d = reinterpret_cast<int *>(&sR);
+    for (int k = threadIdx.x; k < (int)(sizeof(RunDev) / sizeof(int)); k += PH_THREADS) d[k] = src[k];
+  }
+  __syncthreads();
+  const RunDev &R = sR;
   if (!R.ph_enabled) return;
   const long long W = R.ph_team;
   const long long w0 = (long long)blockIdx.x * PH_THREADS;
