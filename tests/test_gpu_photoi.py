@@ -76,6 +76,21 @@ def test_step_with_photoionization():
         _check_pho(ref, run, f"step {k}")
 
 
+def test_photoionization_unreduced_seed():
+    """A seed whose lag state lies outside [0, m): the first draws are stepped
+    one by one until the state is reduced, before any precomputed jump."""
+    cfg, ref, run = _setup(512)
+    dirty = (-5, 2147483600, 7, 11)
+    ref.set_rng_state(dirty)
+    run.set_rng_state(dirty)
+    for k in range(2):
+        dt = ref.get_max_dt()
+        ref.step(dt)
+        run.step(dt)
+        compare(ref, run, where=f"step {k}")
+        _check_pho(ref, run, f"step {k}")
+
+
 def test_step_batch_with_photoionization():
     cfgs = [config.cylindrical_16mm(photoi=True, photoi_team=t, rng_seed=s)
             for t, s in ((512, (521288629, 362436069, 16163801, 1131199299)),
