@@ -1494,22 +1494,48 @@ __device__ void p_fmg_in(const RunDev &R, const MGV<T> &M, bool set_residual, bo
 }
 
 // Copy the multigrid variables of every box between device memory and the
-// compact shared-memory arrays (in: to shared memory).
+// compact shared-memory arrays (in: to shared memory). All slots of all
+// levels form one flat range; a thread moves two slots (three variables
+// each) per round, loading all six values before storing any.
 template <class T>
 __device__ void stage_mg(const RunDev &R, const MGV<T> &M, T *g0, T *g1, T *g2, bool in) {
   T *g[3] = {g0, g1, g2};
   T *s[3] = {M.phi, M.rhs, M.tmp};
-  for (int lvl = R.min_lvl; lvl <= R.max_lvl; lvl++) {
-    const int li = lvl - R.min_lvl;
-    const int ncg = R.lv_nc[li] + 2, per = ncg * ncg;
-    const int b0 = R.bx_off[li], n = (R.bx_off[li + 1] - b0) * per;
-    for (int k = threadIdx.x; k < n; k += NTHR) {
-      const BoxRec &B = M.boxes[b0 + k / per];
-      const int c = k % per;
-      for (int v = 0; v < 3; v++) {
-        if (in) s[v][B.base + c] = g[v][B.gbase + c];
-        else g[v][B.gbase + c] = s[v][B.base + c];
-      }
+  auto level_slots = [&](int li) {
+    const int ncg = R.lv_nc[li] + 2;
+    return (R.bx_off[li + 1] - R.bx_off[li]) * ncg * ncg;
+  };
+  int li = 0, lo = 0, hi = level_slots(0);
+  // slot k (not below the previous call's k): source and destination index
+  auto slot_at = [&](int k, int &src, int &dst) {
+    while (k >= hi) {
+      if (++li >= R.nlev) return false;
+      lo = hi;
+      hi = lo + level_slots(li);
+    }
+    const int ncg = R.lv_nc[li] + 2, per = ncg * ncg, t = k - lo;
+    const BoxRec &B = M.boxes[R.bx_off[li] + t / per];
+    const int c = t % per;
+    src = in ? B.gbase + c : B.base + c;
+    dst = in ? B.base + c : B.gbase + c;
+    return true;
+  };
+  T *const *from = in ? g : s;
+  T *const *to = in ? s : g;
+  for (int k = threadIdx.x;; k += 2 * NTHR) {
+    int a0, d0, a1 = 0, d1 = 0;
+    if (!slot_at(k, a0, d0)) break;
+    const bool two = slot_at(k + NTHR, a1, d1);
+    T v0[3], v1[3];
+#pragma unroll
+    for (int v = 0; v < 3; v++) {
+      v0[v] = from[v][a0];
+      if (two) v1[v] = from[v][a1];
+    }
+#pragma unroll
+    for (int v = 0; v < 3; v++) {
+      to[v][d0] = v0[v];
+      if (two) to[v][d1] = v1[v];
     }
   }
   __syncthreads();
