@@ -230,14 +230,21 @@ def run_uneven_batch(n_runs, first_schedule, fixed=False):
     for form, sc in (("fp64", None), ("mixed", sched)):
         # one batch: the blocks' device time; two pipelined groups: the wall
         # time of the whole batched run with the host regrids overlapped
+        # the wall time includes the host regrids, which share the host with
+        # other work: the faster of two whole batched runs is reported
         torch.cuda.nvtx.range_push(f"uneven_{form}")
-        h, (nb, gpu_ms, host_ms, cu), wall1 = autotune.batch_observables(cfgs, sc, n_threads=threads)
+        best = None
+        for _ in range(2):
+            res = autotune.batch_observables(cfgs, sc, n_threads=threads)
+            if best is None or res[2] < best[2]:
+                best = res
+        h, (nb, gpu_ms, host_ms, cu), wall1 = best
         torch.cuda.nvtx.range_pop()
         _, (_, _, host2, cu2), wall2 = autotune.batch_observables(cfgs, sc, n_threads=threads, groups=2)
         heads[form] = h
         out[form] = {"value": cu / (gpu_ms / 1e3), "unit": UNIT, "device_s": gpu_ms / 1e3,
                      "host_regrid_s": host_ms / 1e3, "blocks": nb, "cell_updates": cu,
-                     "value_wall": cu / wall1, "wall_s": wall1,
+                     "value_wall": cu / wall1, "wall_s": wall1, "wall_of": "faster of 2 batched runs",
                      "value_wall_two_groups": cu2 / wall2, "wall_s_two_groups": wall2}
     er = [abs(a[2] - b[2]) / a[2] for a, b in zip(heads["fp64"], heads["mixed"])]
     out["mixed"]["schedule"] = list(sched)
