@@ -218,7 +218,10 @@ int a5g_get_precision(a5g_ctx *ctx, int *precision, a5g_mg_schedule *sched);
  * device launch; with it, three (photon sources, absorption, step). */
 int a5g_step(a5g_ctx *ctx, double dt);
 /* The same step for several independent runs in one launch (one persistent
- * thread block per run). dts[k] is the step of run k. */
+ * thread block per run). dts[k] is the step of run k. The launches go on the
+ * first run's stream after the other runs' streams are synchronized (one
+ * host call per member and step); the device-driven batch (a5g_batch_*)
+ * replays whole blocks of steps from CUDA graphs instead. */
 int a5g_step_batch(a5g_ctx **ctxs, int n, const double *dts);
 /* Batched step that allocates no device memory. Same result as
  * a5g_step_batch; no counterpart in the reference (its Fortran host has no
