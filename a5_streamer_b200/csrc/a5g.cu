@@ -653,7 +653,9 @@ struct MGV {
 // Side ghost (side, k) of the potential: sides_from_nb, mg$D_sides_rb after
 // a$D_gc_prolong0 (m_aX_mg.f90:261-301), or sides_bc_pot
 // (src/streamer_2d.f90:620-638). Reads only interior cells of the box and its
-// neighbours and ghost cells of the parent.
+// neighbours and ghost cells of the parent. This is the readable statement
+// of the recipe; the phases call phi_ghost_sl below, which gives the same
+// values with its loads issued together.
 template <class T>
 __device__ __forceinline__ T phi_ghost(double V, const T *phi, const BoxRec &B, int nc, int ncg,
                                        int side, int k) {
@@ -684,7 +686,9 @@ __device__ __forceinline__ T phi_ghost(double V, const T *phi, const BoxRec &B, 
 
 // Side ghost (side, k) of a density or |E|: sides_from_nb, a$D_gc_interp
 // (lim: a$D_gc_interp_lim) from the parent's neighbour (m_aX_gc.f90:90-295),
-// or a$D_gc_neumann.
+// or a$D_gc_neumann. The readable statement of the recipe; the phases call
+// den_ghost_sl below, which gives the same values with its loads issued
+// together.
 __device__ __forceinline__ double den_ghost(const double *x, const BoxRec &B, int nc, int ncg,
                                             int side, int k, bool lim) {
   const int dim = side >> 1;
@@ -712,6 +716,30 @@ __device__ __forceinline__ double den_ghost(const double *x, const BoxRec &B, in
     return v;
   }
   return x[own];
+}
+
+// den_ghost in straight-line form (the same values and arithmetic): the
+// source addresses of the side's kind are selected first and loaded
+// together, so that a ghost's loads do not wait behind the branches.
+__device__ __forceinline__ double den_ghost_sl(const double *x, const BoxRec &B, int nc, int ncg,
+                                               int side, int k, bool lim) {
+  const int dim = side >> 1;
+  const bool low = (side & 1) == 0;
+  const int nbb = B.nb[side];
+  const int ix = low ? 1 : nc;
+  const int own = B.base + (dim == 0 ? ix + ncg * k : k + ncg * ix);
+  const int cp = nbb + (dim == 0 ? (low ? nc : 1) + ncg * k : k + ncg * (low ? nc : 1));
+  const bool isnb = nbb > 0, isrb = nbb == NBR_RB;
+  const int pn = B.pnb[side], ix_c = low ? nc : 1;
+  const int c1 = (dim == 0 ? B.o1 : B.o0) + ((k + 1) >> 1), c2 = c1 + 1 - 2 * (k & 1);
+  const int r1 = dim == 0 ? pn + ix_c + ncg * c1 : pn + c1 + ncg * ix_c;
+  const int r2 = dim == 0 ? pn + ix_c + ncg * c2 : pn + c2 + ncg * ix_c;
+  const int s0 = isnb ? cp : (isrb ? r1 : own), s1 = isrb ? r2 : s0, s2 = isrb ? own : s0;
+  const double v0 = x[s0], v1 = x[s1], v2 = x[s2];
+  const double sixth = 1 / 6.0, third = 1 / 3.0;
+  double v = 0.5 * v0 + sixth * v1 + third * v2;
+  if (lim && v > 2 * v0) v = 2 * v0;
+  return isrb ? v : v0;
 }
 
 // phi_ghost in straight-line form: the addresses of all candidate sources
@@ -938,7 +966,7 @@ __device__ __forceinline__ void fill_phi_loop(const RunDev &R, const MGV<T> &M, 
   for (int k = threadIdx.x; k < n; k += NTHR) {
     const BoxRec &B = M.boxes[L.b0 + (k >> (L.sh + 2))];
     const int r = k & (per - 1), side = r >> L.sh, kk = (r & (L.nc - 1)) + 1;
-    const T v = phi_ghost(M.V, phi, B, L.nc, L.ncg, side, kk);
+    const T v = phi_ghost_sl(M.V, phi, B, L.nc, L.ncg, side, kk);
     const int dim = side >> 1, gx = (side & 1) ? L.nc + 1 : 0;
     const int d = B.base + (dim == 0 ? gx + L.ncg * kk : kk + L.ncg * gx);
     phi[d] = v;
@@ -1767,7 +1795,7 @@ __device__ void p_gc_den(const RunDev &R, int iv0, int iv1, bool lim) {
         const int iv = w == 0 ? iv0 : iv1;
         if (iv < 0) continue;
         double *x = VAR(R, iv);
-        x[d] = den_ghost(x, B, L.nc, L.ncg, side, kk, lim);
+        x[d] = den_ghost_sl(x, B, L.nc, L.ncg, side, kk, lim);
       }
     }
     __syncthreads();
