@@ -684,43 +684,12 @@ __device__ __forceinline__ T phi_ghost(double V, const T *phi, const BoxRec &B, 
   return phi[own];
 }
 
-// Side ghost (side, k) of a density or |E|: sides_from_nb, a$D_gc_interp
-// (lim: a$D_gc_interp_lim) from the parent's neighbour (m_aX_gc.f90:90-295),
-// or a$D_gc_neumann. The readable statement of the recipe; the phases call
-// den_ghost_sl below, which gives the same values with its loads issued
-// together.
-__device__ __forceinline__ double den_ghost(const double *x, const BoxRec &B, int nc, int ncg,
-                                            int side, int k, bool lim) {
-  const int dim = side >> 1;
-  const bool low = (side & 1) == 0;
-  const int nbb = B.nb[side];
-  if (nbb > 0) return x[nbb + (dim == 0 ? (low ? nc : 1) + ncg * k : k + ncg * (low ? nc : 1))];
-  const int ix = low ? 1 : nc;
-  const int own = B.base + (dim == 0 ? ix + ncg * k : k + ncg * ix);
-  if (nbb == NBR_RB) {
-    const double sixth = 1 / 6.0, third = 1 / 3.0;
-    const int pn = B.pnb[side], ix_c = low ? nc : 1;
-    int s1, s2;
-    if (dim == 0) {
-      const int j_c1 = B.o1 + ((k + 1) >> 1), j_c2 = j_c1 + 1 - 2 * (k & 1);
-      s1 = pn + ix_c + ncg * j_c1;
-      s2 = pn + ix_c + ncg * j_c2;
-    } else {
-      const int i_c1 = B.o0 + ((k + 1) >> 1), i_c2 = i_c1 + 1 - 2 * (k & 1);
-      s1 = pn + i_c1 + ncg * ix_c;
-      s2 = pn + i_c2 + ncg * ix_c;
-    }
-    const double c1 = x[s1], c2 = x[s2];
-    double v = 0.5 * c1 + sixth * c2 + third * x[own];
-    if (lim && v > 2 * c1) v = 2 * c1;
-    return v;
-  }
-  return x[own];
-}
-
-// den_ghost in straight-line form (the same values and arithmetic): the
-// source addresses of the side's kind are selected first and loaded
-// together, so that a ghost's loads do not wait behind the branches.
+// Side ghost (side, k) of a density or |E|: sides_from_nb (a copy of the
+// neighbour's cell), a$D_gc_interp (lim: a$D_gc_interp_lim) from the
+// parent's neighbour, 1/2 c1 + 1/6 c2 + 1/3 own (m_aX_gc.f90:90-295), or
+// a$D_gc_neumann. Straight-line form: the source addresses of the side's
+// kind are selected first and loaded together, so that a ghost's loads do
+// not wait behind branches.
 __device__ __forceinline__ double den_ghost_sl(const double *x, const BoxRec &B, int nc, int ncg,
                                                int side, int k, bool lim) {
   const int dim = side >> 1;
