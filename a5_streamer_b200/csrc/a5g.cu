@@ -1760,11 +1760,17 @@ __device__ void p_gc_den(const RunDev &R, int iv0, int iv1, bool lim) {
       const int r = k & (per - 1), side = r >> L.sh, kk = (r & (L.nc - 1)) + 1;
       const int dim = side >> 1, gx = (side & 1) ? L.nc + 1 : 0;
       const int d = B.base + (dim == 0 ? gx + L.ncg * kk : kk + L.ncg * gx);
+      // both variables' ghost values are formed before either is written
+      double g[2];
+#pragma unroll
       for (int w = 0; w < 2; w++) {
         const int iv = w == 0 ? iv0 : iv1;
-        if (iv < 0) continue;
-        double *x = VAR(R, iv);
-        x[d] = den_ghost_sl(x, B, L.nc, L.ncg, side, kk, lim);
+        if (iv >= 0) g[w] = den_ghost_sl(VAR(R, iv), B, L.nc, L.ncg, side, kk, lim);
+      }
+#pragma unroll
+      for (int w = 0; w < 2; w++) {
+        const int iv = w == 0 ? iv0 : iv1;
+        if (iv >= 0) VAR(R, iv)[d] = g[w];
       }
     }
     __syncthreads();
@@ -1796,18 +1802,31 @@ __device__ void p_restrict(const RunDev &R, int iv0, int iv1) {
       }
       const int src = P.ch[q] + (2 * i - 1) + cg * (2 * j - 1);
       const int d = P.base + ic + L.ncg * jc;
+      // the children's values of both variables are read before either
+      // parent value is written
+      double v[2][4];
+#pragma unroll
       for (int w = 0; w < 2; w++) {
         const int iv = w == 0 ? iv0 : iv1;
         if (iv < 0) continue;
-        double *x = VAR(R, iv);
-        const double a = x[src], b = x[src + 1], c = x[src + cg], dd = x[src + cg + 1];
+        const double *x = VAR(R, iv);
+        v[w][0] = x[src];
+        v[w][1] = x[src + 1];
+        v[w][2] = x[src + cg];
+        v[w][3] = x[src + cg + 1];
+      }
+#pragma unroll
+      for (int w = 0; w < 2; w++) {
+        const int iv = w == 0 ? iv0 : iv1;
+        if (iv < 0) continue;
+        const double a = v[w][0], b = v[w][1], c = v[w][2], dd = v[w][3];
         if (cyl) {
           const double dr16 = 0.0625 * P.dr;
           const double r = P.r0 + (i - 0.5) * P.dr;
           const double rfac = dr16 / r;
-          x[d] = (0.25 - rfac) * (a + c) + (0.25 + rfac) * (b + dd);
+          VAR(R, iv)[d] = (0.25 - rfac) * (a + c) + (0.25 + rfac) * (b + dd);
         } else {
-          x[d] = 0.25 * (a + b + c + dd);
+          VAR(R, iv)[d] = 0.25 * (a + b + c + dd);
         }
       }
     }
