@@ -1902,20 +1902,45 @@ __device__ void p_compute_fld_mixed(const RunDev &R) {
 
 // Whole-array copy / average over every slot (unused slots included; their
 // contents are never read).
+// Four slots per thread and round, all loads before the stores.
 __device__ void copy_var(const RunDev &R, int from, int to) {
   const size_t n = (size_t)R.capacity * SLOT;
   const double *a = R.cc + (size_t)from * n;
   double *b = R.cc + (size_t)to * n;
-  for (size_t k = threadIdx.x; k < n; k += NTHR) b[k] = a[k];
+  for (size_t k = threadIdx.x; k < n; k += 4 * NTHR) {
+    double v[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+      if (k + u * NTHR < n) v[u] = a[k + u * NTHR];
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+      if (k + u * NTHR < n) b[k + u * NTHR] = v[u];
+  }
   __syncthreads();
 }
-// average_dens, src/streamer_2d.f90:492-496
+// average_dens, src/streamer_2d.f90:492-496; both densities, two slots per
+// thread and round, all loads before the stores
 __device__ void average_dens(const RunDev &R) {
   const size_t n = (size_t)R.capacity * SLOT;
-  for (int v = 0; v < 2; v++) {
-    double *x = R.cc + (size_t)v * n;
-    const double *o = R.cc + (size_t)(v + 2) * n;
-    for (size_t k = threadIdx.x; k < n; k += NTHR) x[k] = 0.5 * (x[k] + o[k]);
+  double *x0 = R.cc, *x1 = R.cc + n;
+  const double *o0 = R.cc + 2 * n, *o1 = R.cc + 3 * n;
+  for (size_t k = threadIdx.x; k < n; k += 2 * NTHR) {
+    const size_t k1 = k + NTHR;
+    const bool two = k1 < n;
+    const double a0 = x0[k], b0 = o0[k], a1 = x1[k], b1 = o1[k];
+    double c0 = 0, d0 = 0, c1 = 0, d1 = 0;
+    if (two) {
+      c0 = x0[k1];
+      d0 = o0[k1];
+      c1 = x1[k1];
+      d1 = o1[k1];
+    }
+    x0[k] = 0.5 * (a0 + b0);
+    x1[k] = 0.5 * (a1 + b1);
+    if (two) {
+      x0[k1] = 0.5 * (c0 + d0);
+      x1[k1] = 0.5 * (c1 + d1);
+    }
   }
   __syncthreads();
 }
@@ -2584,9 +2609,17 @@ __device__ void step(const RunDev &R, double dt, bool deposit) {
     const size_t n = (size_t)R.capacity * SLOT;
     const double *e = VAR(R, I_ELEC), *pi = VAR(R, I_PION);
     double *eo = VAR(R, I_ELEC_OLD), *po = VAR(R, I_PION_OLD);
-    for (size_t k = threadIdx.x; k < n; k += NTHR) {
-      eo[k] = e[k];
-      po[k] = pi[k];
+    // two slots per thread and round, all loads before the stores
+    for (size_t k = threadIdx.x; k < n; k += 2 * NTHR) {
+      const size_t k1 = k + NTHR;
+      const bool two = k1 < n;
+      const double a0 = e[k], b0 = pi[k], a1 = two ? e[k1] : 0.0, b1 = two ? pi[k1] : 0.0;
+      eo[k] = a0;
+      po[k] = b0;
+      if (two) {
+        eo[k1] = a1;
+        po[k1] = b1;
+      }
     }
     __syncthreads();
   }
