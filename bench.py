@@ -351,10 +351,10 @@ def run_b200(args):
             torch.cuda.nvtx.range_push("batched_mixed" if mixed else "batched_fp64")
             with torch.cuda.stream(bstream):
                 # a head start for the host: the device spins (a fixed number
-                # of cycles, about 30 ms) while the host queues the timed
+                # of cycles, about 100 ms) while the host queues the timed
                 # steps, so that host work between launches (a stream check
                 # per member) cannot leave the device idle inside the events
-                torch.cuda._sleep(int(30e-3 * 1.965e9))
+                torch.cuda._sleep(int(100e-3 * 1.965e9))
                 for k in range(nb):
                     flush.fill_(k & 0xFF)
                     b0[k].record(bstream)
