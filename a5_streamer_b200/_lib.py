@@ -36,6 +36,7 @@ class Params(ctypes.Structure):
         ("photoi_team", ctypes.c_int), ("photoi_pad", ctypes.c_int),
         ("photoi_coeff", ctypes.c_double), ("photoi_fac_dx", ctypes.c_double),
         ("rng_seed", ctypes.c_int * 4),
+        ("uniform_lvl", ctypes.c_int), ("uniform_pad", ctypes.c_int),
     ]
 
 
@@ -76,6 +77,10 @@ SIGNATURES = {
     "a5g_compute_fld": (_I, [_P, _I]),
     "a5g_fas_fmg": (_I, [_P, _I, _I]),
     "a5g_fld_from_pot": (_I, [_P]),
+    "a5g_mg_fas_vcycle": (_I, [_P, _I, _I]),
+    "a5g_tree_max_cc": (_I, [_P, _I, _PD]),
+    "a5g_tree_min_cc": (_I, [_P, _I, _PD]),
+    "a5g_tree_sum_cc": (_I, [_P, _I, _I, _PD]),
     "a5g_dt_reductions": (_I, [_P, _PD]),
     "a5g_get_max_dt": (_I, [_P, _PD]),
     "a5g_ref_flags": (_I, [_P, _D, _PI]),
@@ -91,6 +96,9 @@ SIGNATURES = {
     "a5g_step_batch": (_I, [ctypes.POINTER(_P), _I, _PD]),
     "a5g_step_batch_static": (_I, [ctypes.POINTER(_P), _I, _PD]),
     "a5g_sync": (_I, [_P]),
+    "a5g_set_ctas": (_I, [_P, _I, ctypes.c_longlong]),
+    "a5g_get_ctas": (_I, [_P, _PI, _PI]),
+    "a5g_set_grid_local": (_I, [_P, _I]),
     "a5g_batch_create": (_I, [ctypes.POINTER(_P), _I, ctypes.POINTER(_P)]),
     "a5g_batch_destroy": (_I, [_P]),
     "a5g_batch_begin": (_I, [_P, _PD, _PD]),
@@ -99,6 +107,7 @@ SIGNATURES = {
     "a5g_get_stream": (_I, [_P, ctypes.POINTER(_P)]),
     "a5g_debug_set_staging": (_I, [_P, _I]),
     "a5g_debug_info": (_I, [_P, ctypes.POINTER(ctypes.c_longlong)]),
+    "a5g_debug_params_layout": (_I, [_PI, _I]),
     "a5g_debug_plans": (_I, [_I, _I, _I, _PI, _PD, _PI, _PI, _D, _PI, _PI, _P, _PI, _PD, _PI]),
     # host tree (include/a5t.h)
     "a5t_create": (_I, [_I, _I, _D, _PD, _I, ctypes.POINTER(_P)]),

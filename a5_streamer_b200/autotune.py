@@ -123,7 +123,7 @@ def time_steps(run, dt: float, n: int) -> float:
     return e0.elapsed_time(e1) / n
 
 
-def tune_schedule(sim, n_steps: int = 20, tol_max_E: float = 1e-4, tol_head_z: float = 5e-3,
+def tune_schedule(sim, n_steps: int = 200, tol_max_E: float = 1e-4, tol_head_z: float = 5e-3,
                   safety: float = 0.5, candidates: Optional[Sequence[Schedule]] = None,
                   whole_run: bool = True, ref_head=None, n_time: int = 20) -> Dict:
     """Pick the mixed-precision multigrid schedule for ``sim``'s tree and

@@ -81,6 +81,10 @@ class StreamerConfig:
     photoi_team: int = 148 * 256
     # master generator state ST_rng (fosito/m_random.f90:12-13 default)
     rng_seed: Tuple[int, int, int, int] = (521288629, 362436069, 16163801, 1131199299)
+    # > 0: every box below this level is refined and the rest kept, instead
+    # of the streamer's refinement criterion: a uniformly refined mesh, as
+    # afivo/examples/multigrid/test_mg_benchmark_2d.f90:40-86 builds
+    uniform_lvl: int = 0
 
     # --- derived quantities -------------------------------------------------
     @property
@@ -150,6 +154,8 @@ class StreamerConfig:
                 raise ValueError(f"transport column {name!r}: bad length")
         if not (1 <= self.lvls_max <= 30):
             raise ValueError("lvls_max must be in 1..30")
+        if self.uniform_lvl < 0 or self.uniform_lvl > self.lvls_max:
+            raise ValueError("uniform_lvl must be in 0..lvls_max")
         if self.photoi_enabled:
             if not self.is_cyl:
                 raise ValueError("photoionization is built for the cylindrical form only "
@@ -200,6 +206,18 @@ def cartesian_8mm(**overrides) -> StreamerConfig:
         dt_max=1e-10, num_steps_amr=2, end_time=2e-9, use_drt=True,
         lkptbl_size=200, lkptbl_max_fld=3e7, td=synthetic_transport())
     return dataclasses.replace(cfg, **overrides)
+
+
+def cartesian_uniform(level: int = 6, **overrides) -> StreamerConfig:
+    """The 8 mm Cartesian case on a uniformly refined mesh of the given level
+    (every box below it refined, as the multigrid benchmark
+    afivo/examples/multigrid/test_mg_benchmark_2d.f90:40-86 builds its mesh):
+    (32 * 2^(level-1))^2 leaf cells, e.g. 1,048,576 at level 6 (dx = 7.8 um)
+    and 4,194,304 at level 7. A large tree for the grid-mode form. The finest
+    allowed level is one above: a$D_adjust_refinement never builds the leaf
+    list of level lvls_max (afivo/src/m_aX_core.f90:495-532), so boxes there
+    would take no transport update."""
+    return cartesian_8mm(lvls_max=level + 1, uniform_lvl=level, **overrides)
 
 
 def cylindrical_16mm(photoi: bool = False, **overrides) -> StreamerConfig:

@@ -25,6 +25,7 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -147,6 +148,16 @@ struct RunDev {
   // dielectric boxes; such runs take the device-memory multigrid path
   int diel;
   int *tags;
+  // partial sums of a5g_tree_sum_cc, one per team thread (capacity doubles)
+  double *sumbuf;
+  int uniform_lvl;             // > 0: uniform refinement to this level
+  int local_cells;             // grid mode: levels of at most this many cells on one block
+  // grid mode (a5g_set_ctas): barrier words of the run's block group
+  // ([0] arrivals, [1] generation, [2] abort), the cycle bound of a barrier
+  // wait, and per-block partial reductions (4 doubles per block)
+  unsigned *gbar;
+  long long gbudget;
+  double *gred;
 };
 constexpr int TAG_NORMAL = 1, TAG_DIEL = 2;
 
@@ -189,7 +200,8 @@ static_assert(sizeof(PhBox) == 48, "PhBox layout");
 enum OpCode {
   OP_COPY = 1, OP_FLUXES, OP_CONSISTENT, OP_UPDATE, OP_RESTRICT, OP_GC, OP_AVERAGE,
   OP_COMPUTE_FLD, OP_FMG, OP_FLD_FROM_POT, OP_DT_RED, OP_REF_FLAGS, OP_PROLONG_NEW,
-  OP_STEP, OP_NOP, OP_PH_SOURCE, OP_PH_DEPOSIT, OP_STEP_MIXED, OP_COMPUTE_FLD_MIXED, OP_BLOCK_DT
+  OP_STEP, OP_NOP, OP_PH_SOURCE, OP_PH_DEPOSIT, OP_STEP_MIXED, OP_COMPUTE_FLD_MIXED, OP_BLOCK_DT,
+  OP_VCYCLE, OP_TREE_RED
 };
 struct Op {
   int code, i0, i1, i2;
@@ -239,10 +251,80 @@ __device__ __forceinline__ void list_range(const RunDev &R, int kind, int lo, in
   n = b - a;
 }
 
+// ---------------------------------------------------------------------------
+// Execution group of a run. A run executes on one thread block, or in grid
+// mode (a5g_set_ctas, for trees too large for one SM) on `size` co-resident
+// blocks of one cooperative launch. Every phase is a flat loop of the group's
+// threads over its items -- thread TID() of NTH() starts at item TID() and
+// strides by NTH() -- and phases are separated by PSYNC(): a block barrier,
+// or in grid mode a grid barrier whose wait is bounded (A5G_TIMEOUT). The
+// state is per block, in shared memory, set at kernel entry (stage_run).
+struct GroupCtl {
+  int size;          // blocks of the run's group
+  int rank;          // this block's rank in the group
+  int tid0;          // rank * NTHR
+  int nth;           // size * NTHR
+  unsigned *bar;     // [0] arrivals, [1] generation, [2] abort
+  long long budget;  // SM clock cycles one barrier wait may take
+  int *status;
+  double *red;       // per-block partial reductions (4 doubles per block)
+};
+__shared__ GroupCtl s_grp;
+
+__device__ __forceinline__ int TID() { return s_grp.tid0 + (int)threadIdx.x; }
+__device__ __forceinline__ int NTH() { return s_grp.nth; }
+// the one thread of the group that writes a run's scalars
+__device__ __forceinline__ bool LEAD() { return s_grp.tid0 == 0 && threadIdx.x == 0; }
+
+// Barrier of the run's block group. One thread per block arrives on the
+// group's counter; the last arrival resets it and advances the generation;
+// the others wait for the generation to change, at most s_grp.budget SM
+// cycles, after which the wait records A5G_TIMEOUT, raises the abort flag
+// (every later barrier of the launch then returns at once) and returns.
+// The fences order each block's writes before its arrival and the waiting
+// block's later reads after the release (gpu-scope acquire also drops stale
+// L1 lines), as a grid-wide barrier requires.
+__device__ __noinline__ void grid_sync() {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned *bar = s_grp.bar;
+    volatile unsigned *vgen = bar + 1, *vabort = bar + 2;
+    if (*vabort == 0u) {
+      const unsigned gen = *vgen;
+      __threadfence();
+      const unsigned prev = atomicAdd(bar, 1u);
+      if (prev == (unsigned)s_grp.size - 1u) {
+        atomicExch(bar, 0u);
+        __threadfence();
+        atomicAdd(bar + 1, 1u);
+      } else {
+        const long long budget = s_grp.budget;
+        const long long t0 = clock64();
+        while (*vgen == gen && *vabort == 0u) {
+          if (clock64() - t0 >= budget) {
+            atomicExch(bar + 2, 1u);
+            atomicExch(s_grp.status, (int)A5G_TIMEOUT);
+            break;
+          }
+          __nanosleep(32);
+        }
+      }
+      __threadfence();
+    }
+  }
+  __syncthreads();
+}
+
+// Barrier between two phases of a run.
+__device__ __forceinline__ void PSYNC() {
+  if (s_grp.size > 1) grid_sync();
+  else __syncthreads();
+}
+
 template <class F>
 __device__ __forceinline__ void box_loop(const int *list, int n, F &&f) {
-  const int g = threadIdx.x / GT, t = threadIdx.x % GT;
-  for (int b = g; b < n; b += NGRP) f(list[b], t);
+  const int g = TID() / GT, t = threadIdx.x % GT, ng = NTH() / GT;
+  for (int b = g; b < n; b += ng) f(list[b], t);
 }
 
 // afivo/src/m_aX_utils.f90:227-239 (a$D_get_child_offset); nb < 0: absent
@@ -871,7 +953,7 @@ __device__ __noinline__ void p_sweep(const RunDev &R, const MGV<T> &M, int lvl, 
   const int p = it & 1;  // parity (i + j) & 1 of the updated cells
   const bool cyl = R.coord == 1;
   const int n = L.nb * half;
-  for (int k = threadIdx.x; k < n; k += NTHR) {
+  for (int k = TID(); k < n; k += NTH()) {
     const BoxRec &B = M.boxes[L.b0 + (k >> hsh)];
     const int t = k & (half - 1);
     const int j = t / hn + 1, m = t % hn;
@@ -922,7 +1004,7 @@ __device__ __noinline__ void p_sweep(const RunDev &R, const MGV<T> &M, int lvl, 
       phi[g] = T(0.25) * (hx + lx + hy + ly - dx2 * r);
     }
   }
-  __syncthreads();
+  PSYNC();
 }
 
 // Ghost fill of the potential on level lvl (fill_gc_phi, :303-316), no
@@ -932,7 +1014,7 @@ template <class T>
 __device__ __forceinline__ void fill_phi_loop(const RunDev &R, const MGV<T> &M, const LvlInfo &L, bool copy_tmp) {
   T *phi = M.phi, *tmp = M.tmp;
   const int per = 4 * L.nc, n = L.nb * per;
-  for (int k = threadIdx.x; k < n; k += NTHR) {
+  for (int k = TID(); k < n; k += NTH()) {
     const BoxRec &B = M.boxes[L.b0 + (k >> (L.sh + 2))];
     const int r = k & (per - 1), side = r >> L.sh, kk = (r & (L.nc - 1)) + 1;
     const T v = phi_ghost_sl(M.V, phi, B, L.nc, L.ncg, side, kk);
@@ -945,7 +1027,7 @@ __device__ __forceinline__ void fill_phi_loop(const RunDev &R, const MGV<T> &M, 
 template <class T>
 __device__ void p_fill(const RunDev &R, const MGV<T> &M, int lvl) {
   fill_phi_loop(R, M, lvl_info(R, lvl), false);
-  __syncthreads();
+  PSYNC();
 }
 
 // For every box of level lvl: the residual rhs - A phi (residual_box,
@@ -968,7 +1050,7 @@ __device__ __noinline__ void p_fr(const RunDev &R, const MGV<T> &M, int lvl, boo
   // parent cell is gathered by shuffles (cells of a box are consecutive
   // threads, i fastest) and added in the order of box_rstr_lpl
   const int per = L.nc * L.nc, n = L.nb * per, nw = (n + 31) & ~31;
-  for (int k = threadIdx.x; k < nw; k += NTHR) {
+  for (int k = TID(); k < nw; k += NTH()) {
     const bool act = k < n;
     const BoxRec &B = M.boxes[L.b0 + (act ? k >> (2 * L.sh) : 0)];
     const int t = k & (per - 1), i = (t & (L.nc - 1)) + 1, j = (t >> L.sh) + 1;
@@ -999,7 +1081,7 @@ __device__ __noinline__ void p_fr(const RunDev &R, const MGV<T> &M, int lvl, boo
     }
   }
   if (fill) fill_phi_loop(R, M, L, false);
-  __syncthreads();
+  PSYNC();
 }
 
 // Ghost fill of level lvl and the coarse right-hand side of its parent
@@ -1014,7 +1096,7 @@ __device__ void p_fc(const RunDev &R, const MGV<T> &M, int lvl, bool copy_tmp) {
   T *phi = M.phi, *tmp = M.tmp, *rhs = M.rhs;
   const T inv_dr_sq = T(1 / (L.dr * L.dr));
   const int per = L.nc * L.nc, n = npb * per;
-  for (int k = threadIdx.x; k < n; k += NTHR) {
+  for (int k = TID(); k < n; k += NTH()) {
     const BoxRec &B = M.boxes[pb[k >> (2 * L.sh)]];
     const int t = k & (per - 1), i = (t & (L.nc - 1)) + 1, j = (t >> L.sh) + 1;
     const int g = B.base + i + L.ncg * j;
@@ -1024,7 +1106,7 @@ __device__ void p_fc(const RunDev &R, const MGV<T> &M, int lvl, bool copy_tmp) {
     if (copy_tmp) tmp[g] = pv;
   }
   fill_phi_loop(R, M, L, copy_tmp);
-  __syncthreads();
+  PSYNC();
 }
 
 // Boxes of level lvl: copy: tmp = phi (a$D_boxes_copy_cc in mg$D_fas_fmg,
@@ -1038,7 +1120,7 @@ __device__ void p_correct(const RunDev &R, const MGV<T> &M, int lvl, bool copy, 
   const int pncg = correct ? R.lv_nc[lvl - 1 - R.min_lvl] + 2 : 0;
   T *phi = M.phi, *tmp = M.tmp;
   const int per = L.nc * L.nc, n = L.nb * per;
-  for (int k = threadIdx.x; k < n; k += NTHR) {
+  for (int k = TID(); k < n; k += NTH()) {
     const BoxRec &B = M.boxes[L.b0 + (k >> (2 * L.sh))];
     const int t = k & (per - 1), i = (t & (L.nc - 1)) + 1, j = (t >> L.sh) + 1;
     const int g = B.base + i + L.ncg * j;
@@ -1067,7 +1149,7 @@ __device__ void p_correct(const RunDev &R, const MGV<T> &M, int lvl, bool copy, 
   }
   if (copy) {
     const int pg = 4 * L.nc, ng = L.nb * pg;
-    for (int k = threadIdx.x; k < ng; k += NTHR) {
+    for (int k = TID(); k < ng; k += NTH()) {
       const BoxRec &B = M.boxes[L.b0 + (k >> (L.sh + 2))];
       const int r = k & (pg - 1), side = r >> L.sh, kk = (r & (L.nc - 1)) + 1;
       const int dim = side >> 1, gx = (side & 1) ? L.nc + 1 : 0;
@@ -1075,7 +1157,7 @@ __device__ void p_correct(const RunDev &R, const MGV<T> &M, int lvl, bool copy, 
       tmp[d] = phi[d];
     }
   }
-  __syncthreads();
+  PSYNC();
 }
 
 // init_phi_rhs for one level (m_aX_mg.f90:450-473): phi = 0 on the boxes of
@@ -1088,7 +1170,7 @@ __device__ __noinline__ void p_init_level(const RunDev &R, const MGV<T> &M, int 
   const double *e = VAR(R, I_ELEC), *pi = VAR(R, I_PION);
   const double fac = UC_ELEM_CHARGE / UC_EPS0;
   const int hn = L.nc >> 1, per = hn * hn, n = L.nb * per;
-  for (int k = threadIdx.x; k < n; k += NTHR) {
+  for (int k = TID(); k < n; k += NTH()) {
     const BoxRec &B = M.boxes[L.b0 + (k >> (2 * L.sh - 2))];
     const int t = k & (per - 1), ii = (t & (hn - 1)) + 1, jj = (t >> (L.sh - 1)) + 1;
     const bool leaf = leaf_rhs && (B.flags & CF_LEAF);
@@ -1107,8 +1189,8 @@ __device__ __noinline__ void p_init_level(const RunDev &R, const MGV<T> &M, int 
     rhs[B.pbase + (B.o0 + ii) + pncg * (B.o1 + jj)] = T(0.25) * (rs[0] + rs[1] + rs[2] + rs[3]);
   }
   const int pc = L.ncg * L.ncg, nz = L.nb * pc;
-  for (int k = threadIdx.x; k < nz; k += NTHR) phi[M.boxes[L.b0 + k / pc].base + k % pc] = T(0);
-  __syncthreads();
+  for (int k = TID(); k < nz; k += NTH()) phi[M.boxes[L.b0 + k / pc].base + k % pc] = T(0);
+  PSYNC();
 }
 
 // Residual rhs - A phi on every cell of levels min..max (set_residual of
@@ -1121,14 +1203,14 @@ __device__ __noinline__ void p_residual_all(const RunDev &R, const MGV<T> &M, in
     const LvlInfo L = lvl_info(R, lvl);
     const T inv_dr_sq = T(1 / (L.dr * L.dr));
     const int per = L.nc * L.nc, n = L.nb * per;
-    for (int k = threadIdx.x; k < n; k += NTHR) {
+    for (int k = TID(); k < n; k += NTH()) {
       const BoxRec &B = M.boxes[L.b0 + (k >> (2 * L.sh))];
       const int t = k & (per - 1), i = (t & (L.nc - 1)) + 1, j = (t >> L.sh) + 1;
       const int g = B.base + i + L.ncg * j;
       tmp[g] = rhs[g] - lap_at(R, M.V, phi, B, L.nc, L.ncg, i, j, inv_dr_sq);
     }
   }
-  __syncthreads();
+  PSYNC();
 }
 
 // ---------------------------------------------------------------------------
@@ -1400,16 +1482,60 @@ __device__ __forceinline__ void plan_fr(const RunDev &R, const MGV<T> &M, const 
   __syncthreads();
 }
 
+// Grid mode: levels with few cells would spend more time in grid barriers
+// than in work, so a run of consecutive phases on such levels goes to block 0
+// of the group alone, behind block barriers, while the other blocks wait at
+// the grid barrier that ends the section. local_top: the highest level L <=
+// max_lvl such that every level min_lvl..L has at most R.local_cells cells
+// (min_lvl - 1: none; always none outside grid mode).
+__device__ __forceinline__ int local_top(const RunDev &R, int max_lvl) {
+  int lc = R.min_lvl - 1;
+  if (s_grp.size == 1) return lc;
+  for (int lvl = R.min_lvl; lvl <= max_lvl; lvl++) {
+    const int li = lvl - R.min_lvl;
+    const int cells = (R.bx_off[li + 1] - R.bx_off[li]) * R.lv_nc[li] * R.lv_nc[li];
+    if (cells > R.local_cells) break;
+    lc = lvl;
+  }
+  return lc;
+}
+// Start of a one-block section: true on block 0, which then runs as a group
+// of one (its writes are published, and the others' reads ordered, by the
+// grid barrier of local_end).
+__device__ __forceinline__ bool local_begin() {
+  if (s_grp.rank != 0) return false;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    s_grp.size = 1;
+    s_grp.nth = NTHR;
+  }
+  __syncthreads();
+  return true;
+}
+// End of the section on every block of a group of `size`.
+__device__ __forceinline__ void local_end(int size) {
+  if (s_grp.rank == 0) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      s_grp.size = size;
+      s_grp.nth = size * NTHR;
+    }
+  }
+  grid_sync();
+}
+
 // mg$D_fas_vcycle (m_aX_mg.f90:208-254), set_residual handled by the caller.
 // Phases per level: down: 4 half-sweeps, residual/restriction (+ ghost fill),
 // coarse ghost fill + rhs; base: 2 n_cycle_base half-sweeps + ghost fill;
-// up: correction, 4 half-sweeps, ghost fill.
+// up: correction, 4 half-sweeps, ghost fill. In grid mode the levels up to
+// local_top run on one block (the down, base and up phases of those levels
+// are consecutive).
 template <class T>
 __device__ __forceinline__ void vcycle_body(const RunDev &R, const MGV<T> &M, int max_lvl, bool stale_base,
                                             PlanFetch &pf, int after) {
   const int min_lvl = R.min_lvl;
   const bool cyl = R.coord == 1;
-  for (int lvl = max_lvl; lvl >= min_lvl + 1; lvl--) {
+  auto down = [&](int lvl) {
     const LvlInfo L = lvl_info(R, lvl);
     if (plan_fits(M, L)) {
       const LevelPlan P = make_level_plan(R, M, L, cyl, pf);
@@ -1422,8 +1548,8 @@ __device__ __forceinline__ void vcycle_body(const RunDev &R, const MGV<T> &M, in
     }
     fetch_level_plan(R, M, lvl - 1, cyl, pf);
     p_fc(R, M, lvl - 1, true);
-  }
-  {
+  };
+  auto base = [&]() {
     const LvlInfo L = lvl_info(R, min_lvl);
     if (plan_fits(M, L)) {
       const LevelPlan P = make_level_plan(R, M, L, cyl, pf);
@@ -1432,10 +1558,10 @@ __device__ __forceinline__ void vcycle_body(const RunDev &R, const MGV<T> &M, in
     } else {
       for (int it = 1; it <= M.sw_base; it++) p_sweep(R, M, min_lvl, it, stale_base && it == 1);
     }
-  }
-  fetch_level_plan(R, M, min_lvl < max_lvl ? min_lvl + 1 : after, cyl, pf);
-  p_fill(R, M, min_lvl);
-  for (int lvl = min_lvl + 1; lvl <= max_lvl; lvl++) {
+    fetch_level_plan(R, M, min_lvl < max_lvl ? min_lvl + 1 : after, cyl, pf);
+    p_fill(R, M, min_lvl);
+  };
+  auto up = [&](int lvl) {
     const LvlInfo L = lvl_info(R, lvl);
     if (plan_fits(M, L)) {
       const LevelPlan P = make_level_plan(R, M, L, cyl, pf);
@@ -1448,7 +1574,21 @@ __device__ __forceinline__ void vcycle_body(const RunDev &R, const MGV<T> &M, in
     }
     fetch_level_plan(R, M, lvl < max_lvl ? lvl + 1 : after, cyl, pf);
     p_fill(R, M, lvl);
+  };
+  const int lc = local_top(R, max_lvl);
+  for (int lvl = max_lvl; lvl >= min_lvl + 1 && lvl > lc; lvl--) down(lvl);
+  if (lc >= min_lvl) {
+    const int size = s_grp.size;
+    if (local_begin()) {
+      for (int lvl = lc; lvl >= min_lvl + 1; lvl--) down(lvl);
+      base();
+      for (int lvl = min_lvl + 1; lvl <= lc; lvl++) up(lvl);
+    }
+    local_end(size);
+  } else {
+    base();
   }
+  for (int lvl = max(min_lvl + 1, lc + 1); lvl <= max_lvl; lvl++) up(lvl);
 }
 
 // The FP64 V-cycle is inlined into its caller; the FP32 one (mixed form) is
@@ -1482,11 +1622,21 @@ __device__ void p_fmg_in(const RunDev &R, const MGV<T> &M, bool set_residual, bo
     }
   }
   PlanFetch pf;
-  for (int lvl = min_lvl; lvl <= max_lvl; lvl++) {
+  auto level = [&](int lvl) {
     p_correct(R, M, lvl, true, lvl > min_lvl);
     p_vcycle(R, M, lvl, first_call && lvl == min_lvl, pf, lvl + 1);
     if (set_residual && lvl == max_lvl) p_residual_all(R, M, lvl);
+  };
+  // grid mode: the FMG's levels up to local_top, whose V-cycles touch only
+  // those levels, on one block
+  const int lc = local_top(R, max_lvl);
+  if (lc >= min_lvl) {
+    const int size = s_grp.size;
+    if (local_begin())
+      for (int lvl = min_lvl; lvl <= lc; lvl++) level(lvl);
+    local_end(size);
   }
+  for (int lvl = max(min_lvl, lc + 1); lvl <= max_lvl; lvl++) level(lvl);
   if (pf.li >= 0) cp_async_wait_all();
 }
 
@@ -1548,11 +1698,11 @@ __device__ void stage_mg(const RunDev &R, const MGV<T> &M, T *g0, T *g1, T *g2, 
 // tags. One warp per box.
 __device__ void p_set_tags(const RunDev &R) {
   const double *eps = VAR(R, I_EPS);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int warp = TID() >> 5, lane = threadIdx.x & 31, nwarp = NTH() >> 5;
   for (int li = 0; li < R.nlev; li++) {
     const int ncg = R.lv_nc[li] + 2, per = ncg * ncg;
     const int b0 = R.bx_off[li], nb = R.bx_off[li + 1] - b0;
-    for (int b = warp; b < nb; b += NTHR / 32) {
+    for (int b = warp; b < nb; b += nwarp) {
       const int base = R.boxes[b0 + b].gbase;
       double mn = eps[base], mx = mn;
       for (int c = lane; c < per; c += 32) {
@@ -1570,14 +1720,36 @@ __device__ void p_set_tags(const RunDev &R) {
       }
     }
   }
-  __syncthreads();
+  PSYNC();
 }
 
 // mg$D_fas_fmg in shared memory when the tree fits (the three variables,
 // the box records and the parent-box list), else in device memory. A
 // dielectric run always takes the device-memory path, whose phases apply the
 // eps operators to the boxes tagged dielectric.
+template <class F>
+__device__ __forceinline__ void mg_staged(const RunDev &R, F &&body);
+
 __device__ void p_fmg(const RunDev &R, bool set_residual, bool first_call, bool leaf_rhs) {
+  mg_staged(R, [&](const MGV<double> &M) { p_fmg_in(R, M, set_residual, first_call, leaf_rhs); });
+}
+
+// mg$D_fas_vcycle(tree, mg, max_lvl, set_residual) on its own
+// (afivo/src/m_aX_mg.f90:208-254): valid potential ghost cells on input and
+// output; with set_residual the residual of levels min..max_lvl in tmp.
+__device__ void p_vcycle_alone(const RunDev &R, int max_lvl, bool set_residual) {
+  mg_staged(R, [&](const MGV<double> &M) {
+    PlanFetch pf;
+    p_vcycle(R, M, max_lvl, false, pf, R.max_lvl + 1);
+    if (set_residual) p_residual_all(R, M, max_lvl);
+    if (pf.li >= 0) cp_async_wait_all();
+  });
+}
+
+// Runs body(M) on the multigrid variables: staged in shared memory when the
+// tree fits, else in device memory (dielectric runs always in device memory).
+template <class F>
+__device__ __forceinline__ void mg_staged(const RunDev &R, F &&body) {
   if (R.diel) p_set_tags(R);
   if (R.smem_doubles > 0 && !R.diel) {
     const int S = R.smem_doubles, nbx = R.bx_off[R.nlev], npb = R.pb_off[R.nlev];
@@ -1595,12 +1767,12 @@ __device__ void p_fmg(const RunDev &R, bool set_residual, bool first_call, bool 
     MGV<double> M{base, base + S, base + 2 * S, sb, spb, true, R.applied_voltage,
                   4, 4, 2 * R.n_cycle_base};
     stage_mg(R, M, VAR(R, MP), VAR(R, MR), VAR(R, MT), true);
-    p_fmg_in(R, M, set_residual, first_call, leaf_rhs);
+    body(M);
     stage_mg(R, M, VAR(R, MP), VAR(R, MR), VAR(R, MT), false);
   } else {
     MGV<double> M{VAR(R, MP), VAR(R, MR), VAR(R, MT), R.boxes, R.pbx, false, R.applied_voltage,
                   4, 4, 2 * R.n_cycle_base};
-    p_fmg_in(R, M, set_residual, first_call, leaf_rhs);
+    body(M);
   }
 }
 
@@ -1638,7 +1810,7 @@ __device__ __noinline__ void p_mx_residual(const RunDev &R, const MGV<float> &M,
   const double inv_dr_sq = 1 / (L.dr * L.dr);
   const double fac = UC_ELEM_CHARGE / UC_EPS0;
   const int per = L.nc * L.nc, n = L.nb * per, nw = (n + 31) & ~31;
-  for (int k = threadIdx.x; k < nw; k += NTHR) {
+  for (int k = TID(); k < nw; k += NTH()) {
     const bool act = k < n;
     const int b = L.b0 + (act ? k >> (2 * L.sh) : 0);
     const BoxRec &B = R.boxes[b];  // device-memory slots (phi, rhs, densities)
@@ -1678,7 +1850,7 @@ __device__ __noinline__ void p_mx_residual(const RunDev &R, const MGV<float> &M,
   }
   // side ghosts of c and of its tmp start at zero (consistent with c = 0 and V = 0)
   const int pg = 4 * L.nc, ng = L.nb * pg;
-  for (int k = threadIdx.x; k < ng; k += NTHR) {
+  for (int k = TID(); k < ng; k += NTH()) {
     const BoxRec &S = M.boxes[L.b0 + (k >> (L.sh + 2))];
     const int r = k & (pg - 1), side = r >> L.sh, kk = (r & (L.nc - 1)) + 1;
     const int dim = side >> 1, gx = (side & 1) ? L.nc + 1 : 0;
@@ -1686,7 +1858,7 @@ __device__ __noinline__ void p_mx_residual(const RunDev &R, const MGV<float> &M,
     ce[d] = 0.0f;
     ct[d] = 0.0f;
   }
-  __syncthreads();
+  PSYNC();
 }
 
 __device__ void p_mx_accumulate(const RunDev &R, const MGV<float> &M) {
@@ -1694,14 +1866,14 @@ __device__ void p_mx_accumulate(const RunDev &R, const MGV<float> &M) {
   for (int lvl = R.min_lvl; lvl <= R.max_lvl; lvl++) {
     const LvlInfo L = lvl_info(R, lvl);
     const int per = L.nc * L.nc, n = L.nb * per;
-    for (int k = threadIdx.x; k < n; k += NTHR) {
+    for (int k = TID(); k < n; k += NTH()) {
       const int b = L.b0 + (k >> (2 * L.sh));
       const int t = k & (per - 1), i = (t & (L.nc - 1)) + 1, j = (t >> L.sh) + 1;
       const int loc = i + L.ncg * j;
       phi[R.boxes[b].base + loc] += (double)M.phi[M.boxes[b].base + loc];
     }
   }
-  __syncthreads();
+  PSYNC();
   const MGV<double> G{phi, VAR(R, MR), VAR(R, MT), R.boxes, R.pbx, false, R.applied_voltage, 0, 0, 0};
   for (int lvl = R.min_lvl; lvl <= R.max_lvl; lvl++) p_fill(R, G, lvl);
 }
@@ -1752,10 +1924,10 @@ __device__ void p_solve_mixed(const RunDev &R) {
 // a$D_gc_tree(iv, a$D_gc_interp[_lim], a$D_gc_neumann) for one or two
 // variables, levels ascending (m_aX_gc.f90:28-46, 90-330)
 __device__ void p_gc_den(const RunDev &R, int iv0, int iv1, bool lim) {
-  for (int lvl = R.min_lvl; lvl <= R.max_lvl; lvl++) {
+  auto level = [&](int lvl) {
     const LvlInfo L = lvl_info(R, lvl);
     const int per = 4 * L.nc, n = L.nb * per;
-    for (int k = threadIdx.x; k < n; k += NTHR) {
+    for (int k = TID(); k < n; k += NTH()) {
       const BoxRec &B = R.boxes[L.b0 + (k >> (L.sh + 2))];
       const int r = k & (per - 1), side = r >> L.sh, kk = (r & (L.nc - 1)) + 1;
       const int dim = side >> 1, gx = (side & 1) ? L.nc + 1 : 0;
@@ -1773,8 +1945,17 @@ __device__ void p_gc_den(const RunDev &R, int iv0, int iv1, bool lim) {
         if (iv >= 0) VAR(R, iv)[d] = g[w];
       }
     }
-    __syncthreads();
+    PSYNC();
+  };
+  // grid mode: the small coarse levels (filled first) on one block
+  const int lc = local_top(R, R.max_lvl);
+  if (lc >= R.min_lvl) {
+    const int size = s_grp.size;
+    if (local_begin())
+      for (int lvl = R.min_lvl; lvl <= lc; lvl++) level(lvl);
+    local_end(size);
   }
+  for (int lvl = max(R.min_lvl, lc + 1); lvl <= R.max_lvl; lvl++) level(lvl);
 }
 
 // a$D_restrict_tree for one or two variables, levels descending
@@ -1782,14 +1963,14 @@ __device__ void p_gc_den(const RunDev &R, int iv0, int iv1, bool lim) {
 // radius evaluated at the child-local index [i, j] as in :104)
 __device__ void p_restrict(const RunDev &R, int iv0, int iv1) {
   const bool cyl = R.coord == 1;
-  for (int lvl = R.max_lvl - 1; lvl >= R.min_lvl; lvl--) {
+  auto level = [&](int lvl) {
     const LvlInfo L = lvl_info(R, lvl);
     const int li = lvl - R.min_lvl;
     const int *pb = R.pbx + R.pb_off[li];
     const int npb = R.pb_off[li + 1] - R.pb_off[li];
     const int cg = R.lv_nc[li + 1] + 2;
     const int per = L.nc * L.nc, n = npb * per;
-    for (int k = threadIdx.x; k < n; k += NTHR) {
+    for (int k = TID(); k < n; k += NTH()) {
       const BoxRec &P = R.boxes[pb[k >> (2 * L.sh)]];
       const int t = k & (per - 1), ic = (t & (L.nc - 1)) + 1, jc = (t >> L.sh) + 1;
       int q = 0, i = ic, j = jc;
@@ -1830,7 +2011,16 @@ __device__ void p_restrict(const RunDev &R, int iv0, int iv1) {
         }
       }
     }
-    __syncthreads();
+    PSYNC();
+  };
+  // grid mode: the small coarse levels (restricted last) on one block
+  const int lc = local_top(R, R.max_lvl);
+  for (int lvl = R.max_lvl - 1; lvl >= R.min_lvl && lvl > lc; lvl--) level(lvl);
+  if (lc >= R.min_lvl) {
+    const int size = s_grp.size;
+    if (local_begin())
+      for (int lvl = min(lc, R.max_lvl - 1); lvl >= R.min_lvl; lvl--) level(lvl);
+    local_end(size);
   }
 }
 
@@ -1853,11 +2043,12 @@ __device__ __noinline__ void p_fld_from_pot(const RunDev &R) {
   const double *phi = VAR(R, I_PHI), *eps = VAR(R, I_EPS);
   double *fld = VAR(R, I_FLD);
   CellCursor cur = cell_cursor(R);
-  for (int k = threadIdx.x;; k += 2 * NTHR) {
+  const int nth = NTH();
+  for (int k = TID();; k += 2 * nth) {
     int li[2], b[2], ci[2], cj[2];
     bool ok[2];
     ok[0] = cell_at(R, cur, k, li[0], b[0], ci[0], cj[0]);
-    ok[1] = ok[0] && cell_at(R, cur, k + NTHR, li[1], b[1], ci[1], cj[1]);
+    ok[1] = ok[0] && cell_at(R, cur, k + nth, li[1], b[1], ci[1], cj[1]);
     if (!ok[0]) break;
     double f[2][4];
 #pragma unroll
@@ -1885,7 +2076,7 @@ __device__ __noinline__ void p_fld_from_pot(const RunDev &R) {
       fld[base + i + ncg * j] = sqrt(0.25 * (sx * sx) + 0.25 * (sy * sy));
     }
   }
-  __syncthreads();
+  PSYNC();
   p_gc_den(R, I_FLD, -1, false);
 }
 
@@ -1907,16 +2098,17 @@ __device__ void copy_var(const RunDev &R, int from, int to) {
   const size_t n = (size_t)R.capacity * SLOT;
   const double *a = R.cc + (size_t)from * n;
   double *b = R.cc + (size_t)to * n;
-  for (size_t k = threadIdx.x; k < n; k += 4 * NTHR) {
+  const size_t nth = NTH();
+  for (size_t k = TID(); k < n; k += 4 * nth) {
     double v[4];
 #pragma unroll
     for (int u = 0; u < 4; u++)
-      if (k + u * NTHR < n) v[u] = a[k + u * NTHR];
+      if (k + u * nth < n) v[u] = a[k + u * nth];
 #pragma unroll
     for (int u = 0; u < 4; u++)
-      if (k + u * NTHR < n) b[k + u * NTHR] = v[u];
+      if (k + u * nth < n) b[k + u * nth] = v[u];
   }
-  __syncthreads();
+  PSYNC();
 }
 // average_dens, src/streamer_2d.f90:492-496; both densities, two slots per
 // thread and round, all loads before the stores
@@ -1924,8 +2116,9 @@ __device__ void average_dens(const RunDev &R) {
   const size_t n = (size_t)R.capacity * SLOT;
   double *x0 = R.cc, *x1 = R.cc + n;
   const double *o0 = R.cc + 2 * n, *o1 = R.cc + 3 * n;
-  for (size_t k = threadIdx.x; k < n; k += 2 * NTHR) {
-    const size_t k1 = k + NTHR;
+  const size_t nth = NTH();
+  for (size_t k = TID(); k < n; k += 2 * nth) {
+    const size_t k1 = k + nth;
     const bool two = k1 < n;
     const double a0 = x0[k], b0 = o0[k], a1 = x1[k], b1 = o1[k];
     double c0 = 0, d0 = 0, c1 = 0, d1 = 0;
@@ -1942,7 +2135,7 @@ __device__ void average_dens(const RunDev &R) {
       x1[k1] = 0.5 * (c1 + d1);
     }
   }
-  __syncthreads();
+  PSYNC();
 }
 
 // ---------------------------------------------------------------------------
@@ -1986,12 +2179,33 @@ __device__ void dt_reductions(const RunDev &R) {
     mx = dmax(red[0][0], mx);
     mn = dmin(red[1][0], mn);
     me = dmax(red[2][0], me);
+    if (s_grp.size > 1) {
+      // grid mode: each block's values, combined by the lead after a barrier
+      // (max and min are exact: any order gives the same result)
+      double *g = s_grp.red + 4 * s_grp.rank;
+      g[0] = mx;
+      g[1] = mn;
+      g[2] = me;
+    }
+  }
+  if (s_grp.size > 1) {
+    grid_sync();
+    if (LEAD()) {
+      for (int r = 1; r < s_grp.size; r++) {
+        const double *g = s_grp.red + 4 * r;
+        mx = dmax(mx, g[0]);
+        mn = dmin(mn, g[1]);
+        me = dmax(me, g[2]);
+      }
+    }
+  }
+  if (LEAD()) {
     R.scal[0] = mx;
     R.scal[1] = mn;
     R.scal[2] = me;
     if (!isfinite(mx) || !isfinite(mn) || !isfinite(me)) atomicExch(R.status, A5G_ENONFINITE);
   }
-  __syncthreads();
+  PSYNC();
 }
 
 // GM_dist_line (src/m_geom.f90:29-46), 2D, with gfortran's NORM2
@@ -2003,7 +2217,7 @@ __device__ void dt_reductions(const RunDev &R) {
 // time > end time.
 __device__ void block_dt(const RunDev &R) {
   dt_reductions(R);
-  if (threadIdx.x == 0) {
+  if (LEAD()) {
     const double max_fld = R.scal[0], min_fld = R.scal[1], max_dns = R.scal[2];
     const double eps_mach = 2.220446049250313e-16;
     const double dr_min = R.dr_min;
@@ -2022,7 +2236,7 @@ __device__ void block_dt(const RunDev &R) {
     R.blk[0] = dt;
     R.blk[3] = (R.blk[3] != 0.0 && !(dt < 1e-14) && !(R.blk[1] > R.blk[2])) ? 1.0 : 0.0;
   }
-  __syncthreads();
+  PSYNC();
 }
 
 __device__ double dist_line(double x, double y, const double r0[2], const double r1[2]) {
@@ -2046,13 +2260,13 @@ __device__ double dist_line(double x, double y, const double r0[2], const double
 // set_ref_flags on every box of levels 1..max_lvl (src/streamer_2d.f90:177-216,
 // cyl :190-227). One warp per box (levels >= 1 have nc = 8: two cells/lane).
 __device__ void ref_flags(const RunDev &R, double time) {
-  for (int id = threadIdx.x; id < R.capacity; id += NTHR) R.flags[id] = INT_MIN + 1;
-  __syncthreads();
+  for (int id = TID(); id < R.capacity; id += NTH()) R.flags[id] = INT_MIN + 1;
+  PSYNC();
   const int *ids;
   int n;
   list_range(R, 0, 1, R.max_lvl, ids, n);
-  const int w = threadIdx.x / 32, l = threadIdx.x % 32;
-  for (int b = w; b < n; b += NTHR / 32) {
+  const int w = TID() / 32, l = threadIdx.x % 32, nw = NTH() / 32;
+  for (int b = w; b < n; b += nw) {
     const int id = ids[b];
     const BoxMeta &m = R.meta[id];
     const int nc = m.nc, ncg = nc + 2;
@@ -2066,7 +2280,10 @@ __device__ void ref_flags(const RunDev &R, double time) {
       mr = dmax(mr, __shfl_xor_sync(0xffffffffu, mr, o));
       mf = dmax(mf, __shfl_xor_sync(0xffffffffu, mf, o));
     }
-    if (l == 0) {
+    if (l == 0 && R.uniform_lvl > 0) {
+      // uniformly refined mesh: refine below the level, keep the rest
+      R.flags[id] = m.lvl < R.uniform_lvl ? 1 : 0;
+    } else if (l == 0) {
       int flag = INT_MIN + 1;
       double dr2 = m.dr * m.dr;
       double crv_phi = dr2 * mr;
@@ -2086,7 +2303,7 @@ __device__ void ref_flags(const RunDev &R, double time) {
       R.flags[id] = flag;
     }
   }
-  __syncthreads();
+  PSYNC();
 }
 
 // prolong_to_new_boxes, src/streamer_2d.f90:592-617, with a$D_prolong1_to
@@ -2129,13 +2346,13 @@ __device__ void prolong_new(const RunDev &R) {
         eps[c] = rel < 0.25 ? R.epsilon_diel : 1.0;
       }
     });
-    __syncthreads();
+    PSYNC();
     box_loop(ids, n, [&](int id, int t) {
       gc_box(R, id, t, I_ELEC, GC_LIM);
       gc_box(R, id, t, I_PION, GC_LIM);
       gc_box(R, id, t, I_PHI, GC_PHI);
     });
-    __syncthreads();
+    PSYNC();
   }
 }
 
@@ -2561,12 +2778,12 @@ __device__ void ph_deposit(const RunDev &R) {
       }
     });
   }
-  __syncthreads();
+  PSYNC();
   for (int lvl = max(R.ph_lvl, R.min_lvl); lvl <= R.max_lvl - 1; lvl++) {
     const int *par = list_p(R, 2, lvl);
     const int np = list_n(R, 2, lvl);
     box_loop(par, np, [&](int id, int t) { gc_box(R, id, t, I_PHO, GC_INTERP); });
-    __syncthreads();
+    PSYNC();
     // a$D_prolong1_from(boxes, id, i_pho, add=.true.), m_aX_prolong.f90:81-191
     box_loop(par, np, [&](int id, int t) {
       const BoxMeta &pm = R.meta[id];
@@ -2592,8 +2809,81 @@ __device__ void ph_deposit(const RunDev &R) {
       b[i_f + ncg * (j_f + 1)] = f0 + flx + fhy + b[i_f + ncg * (j_f + 1)];
       b[(i_f + 1) + ncg * (j_f + 1)] = f0 + fhx + fhy + b[(i_f + 1) + ncg * (j_f + 1)];
     });
-    __syncthreads();
+    PSYNC();
   }
+}
+
+// a$D_tree_max_cc / a$D_tree_min_cc / a$D_tree_sum_cc over the interior
+// cells of the leaves (afivo/src/m_aX_utils.f90:559-680); result in scal[4].
+// kind 0: max, 1: min (exact, so any order gives the reference's value);
+// kind 2: the sum as a team of `team` OpenMP threads forms it: thread c adds
+// lvl_dr^2 * (box sum) over its static chunk of each level's leaves, levels
+// ascending, and the partial sums are added to 0 in thread order. The box sum
+// runs over (j, i) in column-major order; the cylindrical form weights each
+// cell by its radius and multiplies by 2 pi (sum_2pr_box, :661-678).
+__device__ void tree_reduce(const RunDev &R, int iv, int kind, int team) {
+  __shared__ double red[NTHR / 32];
+  const int *ids;
+  int n;
+  list_range(R, 1, R.min_lvl, R.max_lvl, ids, n);
+  if (kind < 2) {
+    const bool mx = kind == 0;
+    double v = mx ? -1.7976931348623157e308 : 1.7976931348623157e308;
+    box_loop(ids, n, [&](int id, int t) {
+      const int nc = R.meta[id].nc;
+      if (t >= nc * nc) return;
+      const int c = ((t & (nc - 1)) + 1) + (nc + 2) * ((t >> (31 - __clz(nc))) + 1);
+      const double x = CC(R, iv, id)[c];
+      v = mx ? dmax(v, x) : dmin(v, x);
+    });
+    for (int o = 16; o > 0; o >>= 1) {
+      const double y = __shfl_xor_sync(0xffffffffu, v, o);
+      v = mx ? dmax(v, y) : dmin(v, y);
+    }
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int k = 0; k < NTHR / 32; k++) v = mx ? dmax(v, red[k]) : dmin(v, red[k]);
+      R.scal[4] = v;
+    }
+    __syncthreads();
+    return;
+  }
+  const bool cyl = R.coord == 1;
+  const long long W = team;
+  int max_l = 0;
+  for (int lvl = R.min_lvl; lvl <= R.max_lvl; lvl++) max_l = max(max_l, list_n(R, 1, lvl));
+  const int n_busy = (int)min((long long)max_l, W);
+  for (int c = threadIdx.x; c < n_busy; c += NTHR) {
+    double my = 0;
+    for (int lvl = R.min_lvl; lvl <= R.max_lvl; lvl++) {
+      long long lo, len;
+      static_chunk(list_n(R, 1, lvl), W, c, lo, len);
+      const int *lv = list_p(R, 1, lvl);
+      const double dr = R.lv_dr[lvl - R.min_lvl], fac = dr * dr;
+      for (long long k = lo; k < lo + len; k++) {
+        const BoxMeta &m = R.meta[lv[k]];
+        const int nc = m.nc, ncg = nc + 2;
+        const double *x = CC(R, iv, lv[k]);
+        double tmp = 0;
+        for (int j = 1; j <= nc; j++)
+          for (int i = 1; i <= nc; i++) {
+            const double v = x[i + ncg * j];
+            tmp = tmp + (cyl ? v * (m.r0 + (i - 0.5) * m.dr) : v);
+          }
+        if (cyl) tmp = tmp * TWOPI_DP;
+        my = my + fac * tmp;
+      }
+    }
+    R.sumbuf[c] = my;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double total = 0;
+    for (int c = 0; c < n_busy; c++) total = total + R.sumbuf[c];
+    R.scal[4] = total;
+  }
+  __syncthreads();
 }
 
 // One full time step, src/streamer_2d.f90:99-127; with deposit, the photon
@@ -2610,8 +2900,9 @@ __device__ void step(const RunDev &R, double dt, bool deposit) {
     const double *e = VAR(R, I_ELEC), *pi = VAR(R, I_PION);
     double *eo = VAR(R, I_ELEC_OLD), *po = VAR(R, I_PION_OLD);
     // two slots per thread and round, all loads before the stores
-    for (size_t k = threadIdx.x; k < n; k += 2 * NTHR) {
-      const size_t k1 = k + NTHR;
+    const size_t nth = NTH();
+    for (size_t k = TID(); k < n; k += 2 * nth) {
+      const size_t k1 = k + nth;
       const bool two = k1 < n;
       const double a0 = e[k], b0 = pi[k], a1 = two ? e[k1] : 0.0, b1 = two ? pi[k1] : 0.0;
       eo[k] = a0;
@@ -2621,16 +2912,16 @@ __device__ void step(const RunDev &R, double dt, bool deposit) {
         po[k1] = b1;
       }
     }
-    __syncthreads();
+    PSYNC();
   }
   using T = typename std::conditional<MIXED, float, double>::type;
   for (int stage = 1; stage <= 2; stage++) {
     fluxes_koren<T>(R, dt);
-    __syncthreads();
+    PSYNC();
     consistent_fluxes(R);
-    __syncthreads();
+    PSYNC();
     update_solution<T>(R, dt);
-    __syncthreads();
+    PSYNC();
     p_restrict(R, I_ELEC, I_PION);
     p_gc_den(R, I_ELEC, I_PION, true);
     if (stage == 1) {
@@ -2646,9 +2937,9 @@ __device__ void step(const RunDev &R, double dt, bool deposit) {
 __device__ void run_op(const RunDev &R, const Op &op) {
   switch (op.code) {
     case OP_COPY: copy_var(R, op.i0, op.i1); break;
-    case OP_FLUXES: fluxes_koren<double>(R, op.d0); __syncthreads(); break;
-    case OP_CONSISTENT: consistent_fluxes(R); __syncthreads(); break;
-    case OP_UPDATE: update_solution<double>(R, op.d0); __syncthreads(); break;
+    case OP_FLUXES: fluxes_koren<double>(R, op.d0); PSYNC(); break;
+    case OP_CONSISTENT: consistent_fluxes(R); PSYNC(); break;
+    case OP_UPDATE: update_solution<double>(R, op.d0); PSYNC(); break;
     case OP_RESTRICT: p_restrict(R, op.i0, -1); break;
     case OP_GC: p_gc_den(R, op.i0, -1, op.i1 == GC_LIM); break;
     case OP_AVERAGE: average_dens(R); break;
@@ -2668,7 +2959,7 @@ __device__ void run_op(const RunDev &R, const Op &op) {
       }
       if (op.code == OP_STEP) step<false>(R, dt, op.i0 != 0);
       else step<true>(R, dt, op.i0 != 0);
-      if (op.i1 && threadIdx.x == 0) R.blk[1] = R.blk[1] + dt;
+      if (op.i1 && LEAD()) R.blk[1] = R.blk[1] + dt;
       break;
     }
     case OP_BLOCK_DT: block_dt(R); break;
@@ -2682,36 +2973,49 @@ __device__ void run_op(const RunDev &R, const Op &op) {
       ph_source(R, op.i1 ? R.blk[0] : op.d0, op.i0 != 0);
       break;
     case OP_PH_DEPOSIT: ph_deposit(R); break;
+    case OP_VCYCLE: p_vcycle_alone(R, op.i0, op.i1 != 0); break;
+    case OP_TREE_RED: tree_reduce(R, op.i0, op.i1, op.i2); break;
     case OP_NOP: break;
-    default: if (threadIdx.x == 0) atomicExch(R.status, A5G_EINVAL);
+    default: if (LEAD()) atomicExch(R.status, A5G_EINVAL);
   }
 }
 
-// One block per run. The run descriptor is staged in shared memory.
+// The run descriptor staged in shared memory, and the block's group: a
+// single-run launch of g blocks is the group of all its blocks (grid mode
+// when g > 1, launched cooperatively so that they are co-resident); in a
+// batch every block is a group of its own.
+__device__ __forceinline__ void stage_run(const RunDev *src, RunDev &sR, int size, int rank) {
+  const int *s = reinterpret_cast<const int *>(src);
+  int *d = reinterpret_cast<int *>(&sR);
+  for (int k = threadIdx.x; k < (int)(sizeof(RunDev) / sizeof(int)); k += NTHR) d[k] = s[k];
+  if (threadIdx.x == 0) {
+    s_grp.size = size;
+    s_grp.rank = rank;
+    s_grp.tid0 = rank * NTHR;
+    s_grp.nth = size * NTHR;
+    s_grp.bar = src->gbar;
+    s_grp.budget = src->gbudget;
+    s_grp.status = src->status;
+    s_grp.red = src->gred;
+  }
+  __syncthreads();
+}
+
+// One block per run of a batch, or one run on all blocks of the launch.
 __global__ void __launch_bounds__(NTHR, 1)
 a5g_run_kernel(const RunDev *single, Op single_op, const RunDev *const *runs, const Op *ops) {
   __shared__ RunDev sR;
-  const RunDev *src = runs ? runs[blockIdx.x] : single;
-  {
-    const int *s = reinterpret_cast<const int *>(src);
-    int *d = reinterpret_cast<int *>(&sR);
-    for (int k = threadIdx.x; k < (int)(sizeof(RunDev) / sizeof(int)); k += NTHR) d[k] = s[k];
-  }
-  __syncthreads();
+  if (runs) stage_run(runs[blockIdx.x], sR, 1, 0);
+  else stage_run(single, sR, (int)gridDim.x, (int)blockIdx.x);
   Op op = runs ? ops[blockIdx.x] : single_op;
   run_op(sR, op);
 }
 
-// One full time step of one run (a5g_step); a kernel of its own so that
-// profilers can select the hot launch by name.
+// One full time step of one run (a5g_step) on the launch's blocks; a kernel
+// of its own so that profilers can select the hot launch by name.
 __global__ void __launch_bounds__(NTHR, 1) a5g_step_kernel(const RunDev *run, double dt, int deposit) {
   __shared__ RunDev sR;
-  {
-    const int *s = reinterpret_cast<const int *>(run);
-    int *d = reinterpret_cast<int *>(&sR);
-    for (int k = threadIdx.x; k < (int)(sizeof(RunDev) / sizeof(int)); k += NTHR) d[k] = s[k];
-  }
-  __syncthreads();
+  stage_run(run, sR, (int)gridDim.x, (int)blockIdx.x);
   step<false>(sR, dt, deposit != 0);
 }
 
@@ -2719,12 +3023,7 @@ __global__ void __launch_bounds__(NTHR, 1) a5g_step_kernel(const RunDev *run, do
 __global__ void __launch_bounds__(NTHR, 1) a5g_step_mixed_kernel(const RunDev *run, double dt,
                                                                  int deposit) {
   __shared__ RunDev sR;
-  {
-    const int *s = reinterpret_cast<const int *>(run);
-    int *d = reinterpret_cast<int *>(&sR);
-    for (int k = threadIdx.x; k < (int)(sizeof(RunDev) / sizeof(int)); k += NTHR) d[k] = s[k];
-  }
-  __syncthreads();
+  stage_run(run, sR, (int)gridDim.x, (int)blockIdx.x);
   step<true>(sR, dt, deposit != 0);
 }
 
@@ -2738,15 +3037,21 @@ struct BatchSlot {
 // a descriptor table (the fixed array below).
 __global__ void __launch_bounds__(NTHR, 1) a5g_run_kernel_slots(const BatchSlot *slots) {
   __shared__ RunDev sR;
-  const RunDev *src = slots[blockIdx.x].run;
-  {
-    const int *s = reinterpret_cast<const int *>(src);
-    int *d = reinterpret_cast<int *>(&sR);
-    for (int k = threadIdx.x; k < (int)(sizeof(RunDev) / sizeof(int)); k += NTHR) d[k] = s[k];
-  }
-  __syncthreads();
+  stage_run(slots[blockIdx.x].run, sR, 1, 0);
   Op op = slots[blockIdx.x].op;
   run_op(sR, op);
+}
+
+// Descriptors of one launch of a5g_step_batch_static passed by value (as
+// kernel parameters, at most SLOT_FILL per launch; 96 x 40 bytes stays under
+// the classic 4 KiB parameter limit) and written to the fixed table, so that
+// no host staging buffer or copy is involved.
+constexpr int SLOT_FILL = 96;
+struct SlotChunk {
+  BatchSlot s[SLOT_FILL];
+};
+__global__ void a5g_fill_slots_kernel(BatchSlot *dst, SlotChunk chunk, int n) {
+  for (int k = threadIdx.x; k < n; k += blockDim.x) dst[k] = chunk.s[k];
 }
 
 // Absorption of the photons of one photoionization call (PH_do_absorp,
@@ -2994,11 +3299,24 @@ struct a5g_ctx {
   bool allow_smem = true;
   int fit64 = 0, fit32 = 0;       // per-variable sizes when the tree fits, else 0
   size_t need64 = 0, need32 = 0;  // dynamic shared memory the staged solves take
+  // partial sums of a5g_tree_sum_cc (one per box of the capacity)
+  double *sumbuf = nullptr;
+  // ordering of the batched steps with this context's own stream: recorded
+  // on this stream before a batch that includes the context (the batch's
+  // stream waits on it), and on the batch's stream after it (this stream
+  // waits on it). Created with the context, so no batch call allocates.
+  cudaEvent_t ev_order = nullptr;
+  // grid mode (a5g_set_ctas): thread blocks per launch of the run's phases,
+  // barrier words and per-block reduction slots
+  int n_cta = 1;
+  unsigned *gbar = nullptr;
+  double *gred = nullptr;
 };
 
-// Shared-memory staging of the multigrid variables as allowed and as fits.
+// Shared-memory staging of the multigrid variables as allowed and as fits
+// (never in grid mode: a block holds only part of the tree's work).
 static void apply_staging(a5g_ctx *c) {
-  const bool on = c->allow_smem;
+  const bool on = c->allow_smem && c->n_cta == 1;
   c->h.smem_doubles = on ? c->fit64 : 0;
   c->dyn_smem = on && c->fit64 ? c->need64 : 0;
   c->mx_smem_fit = on ? c->fit32 : 0;
@@ -3242,7 +3560,10 @@ static int check_status(a5g_ctx *c) {
   if (st != 0) {
     int z = 0;
     CK(cudaMemcpy(c->status, &z, sizeof(int), cudaMemcpyHostToDevice));
-    return fail(st, "device reported status " + std::to_string(st));
+    // a barrier that gave up leaves its words mid-count: start clean
+    if (st == A5G_TIMEOUT) CK(cudaMemset(c->gbar, 0, 4 * sizeof(unsigned)));
+    return fail(st, st == A5G_TIMEOUT ? "a grid barrier wait ran out (A5G_TIMEOUT)"
+                                      : "device reported status " + std::to_string(st));
   }
   return A5G_OK;
 }
@@ -3256,10 +3577,25 @@ static Op mkop(int code, int i0 = 0, int i1 = 0, double d0 = 0) {
   return o;
 }
 
+// Operations whose phases run on the run's whole block group in grid mode;
+// the others (photon sources, tree reductions) always take one block.
+static bool grid_op(int code) { return code != OP_PH_SOURCE && code != OP_TREE_RED; }
+
 static int launch_smem(a5g_ctx *c, const Op &op, size_t smem) {
   if (!c) return fail(A5G_EINVAL, "null context");
   if (!c->has_tree) return fail(A5G_ESTATE, "no tree uploaded");
   if (!c->has_table) return fail(A5G_ESTATE, "no transport table set");
+  if (c->n_cta > 1 && grid_op(op.code)) {
+    // co-resident blocks of one cooperative launch (no staging: smem = 0)
+    const RunDev *run = c->d_run;
+    Op o = op;
+    const RunDev *const *runs = nullptr;
+    const Op *ops = nullptr;
+    void *args[] = {(void *)&run, (void *)&o, (void *)&runs, (void *)&ops};
+    CK(cudaLaunchCooperativeKernel((const void *)a5g_run_kernel, dim3(c->n_cta), dim3(NTHR), args, 0,
+                                   c->stream));
+    return A5G_OK;
+  }
   a5g_run_kernel<<<1, NTHR, smem, c->stream>>>(c->d_run, op, nullptr, nullptr);
   CK(cudaGetLastError());
   return A5G_OK;
@@ -3396,6 +3732,8 @@ int a5g_create(const a5g_params *p, a5g_ctx **out) {
   if (!(p->epsilon_diel > 0)) return fail(A5G_EINVAL, "epsilon_diel must be > 0");
   if (p->n_seeds < 0 || p->n_seeds > 8) return fail(A5G_EINVAL, "n_seeds must be 0..8");
   if (p->lvls_max < 1 || p->lvls_max > 30) return fail(A5G_EINVAL, "lvls_max must be 1..30");
+  if (p->uniform_lvl < 0 || p->uniform_lvl > p->lvls_max)
+    return fail(A5G_EINVAL, "uniform_lvl must be 0..lvls_max");
   if (!(p->dr_base > 0)) return fail(A5G_EINVAL, "dr_base must be > 0");
   if (p->photoi_enabled) {
     if (p->coord != 1)
@@ -3412,11 +3750,15 @@ int a5g_create(const a5g_params *p, a5g_ctx **out) {
   }
   if (cudaMalloc(&c->d_run, sizeof(RunDev)) != cudaSuccess ||
       cudaMalloc(&c->scal, 16 * sizeof(double)) != cudaSuccess ||
-      cudaMalloc(&c->status, sizeof(int)) != cudaSuccess) {
+      cudaMalloc(&c->status, sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&c->gbar, 4 * sizeof(unsigned)) != cudaSuccess ||
+      cudaMalloc(&c->gred, 4 * (size_t)A5G_MAX_CTAS * sizeof(double)) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_order, cudaEventDisableTiming) != cudaSuccess) {
     a5g_destroy(c);
     return fail(A5G_ENOMEM, "cudaMalloc failed");
   }
   cudaMemset(c->status, 0, sizeof(int));
+  cudaMemset(c->gbar, 0, 4 * sizeof(unsigned));
   {
     // scalars: [0..2] reductions, [8..11] block state (dt, time, end time, active)
     double z[16] = {0};
@@ -3446,8 +3788,13 @@ int a5g_create(const a5g_params *p, a5g_ctx **out) {
   h.blk = c->scal + 8;
   h.dt_max = p->dt_max;
   h.use_drt = p->use_drt ? 1 : 0;
+  h.uniform_lvl = p->uniform_lvl;
   h.diel = p->epsilon_diel != 1.0 ? 1 : 0;
   h.status = c->status;
+  h.gbar = c->gbar;
+  h.gred = c->gred;
+  h.gbudget = A5G_DEFAULT_WAIT_CYCLES;
+  h.local_cells = A5G_DEFAULT_LOCAL_CELLS;
   h.mx_fmg = 1;
   h.mx_sw_down = h.mx_sw_up = 4;
   h.mx_sw_base = 2 * p->n_cycle_base;
@@ -3508,6 +3855,10 @@ int a5g_destroy(a5g_ctx *c) {
   cudaFree(c->tbl32);
   cudaFree(c->cc32);
   cudaFree(c->tags);
+  cudaFree(c->sumbuf);
+  cudaFree(c->gbar);
+  cudaFree(c->gred);
+  if (c->ev_order) cudaEventDestroy(c->ev_order);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return A5G_OK;
@@ -3711,6 +4062,14 @@ static int grow(a5g_ctx *c, int need) {
     cudaFree(c->tags);
     c->tags = nt;
     c->h.tags = nt;
+  }
+  {
+    double *ns = nullptr;
+    if (cudaMalloc(&ns, (size_t)cap * sizeof(double)) != cudaSuccess)
+      return fail(A5G_ENOMEM, "cannot grow the reduction buffer to " + std::to_string(cap) + " boxes");
+    cudaFree(c->sumbuf);
+    c->sumbuf = ns;
+    c->h.sumbuf = ns;
   }
   if (c->cc32) {  // scratch of the mixed form: reallocated at the next mixed launch
     cudaFree(c->cc32);
@@ -3977,6 +4336,28 @@ int a5g_fas_fmg(a5g_ctx *c, int set_residual, int first_call) {
   return launch(c, mkop(OP_FMG, set_residual ? 1 : 0, first_call ? 1 : 0));
 }
 int a5g_fld_from_pot(a5g_ctx *c) { return launch(c, mkop(OP_FLD_FROM_POT)); }
+int a5g_mg_fas_vcycle(a5g_ctx *c, int max_lvl, int set_residual) {
+  if (!c) return fail(A5G_EINVAL, "null context");
+  if (c->has_tree && (max_lvl < c->min_lvl || max_lvl > c->max_lvl))
+    return fail(A5G_EINVAL, "max_lvl outside the levels of the tree");
+  return launch(c, mkop(OP_VCYCLE, max_lvl, set_residual ? 1 : 0));
+}
+
+// a$D_tree_max_cc / _min_cc / _sum_cc: one launch, the value read back.
+static int tree_red(a5g_ctx *c, int iv, int kind, int team, double *out) {
+  if (!c || !out) return fail(A5G_EINVAL, "null argument");
+  if (iv < 0 || iv >= A5G_N_VAR_CELL) return fail(A5G_EINVAL, "bad variable index");
+  if (team < 1) return fail(A5G_EINVAL, "team must be >= 1");
+  Op o = mkop(OP_TREE_RED, iv, kind);
+  o.i2 = team;
+  int r = launch(c, o);
+  if (r) return r;
+  CK(cudaMemcpyAsync(out, c->scal + 4, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  return check_status(c);
+}
+int a5g_tree_max_cc(a5g_ctx *c, int iv, double *out) { return tree_red(c, iv, 0, 1, out); }
+int a5g_tree_min_cc(a5g_ctx *c, int iv, double *out) { return tree_red(c, iv, 1, 1, out); }
+int a5g_tree_sum_cc(a5g_ctx *c, int iv, int team, double *out) { return tree_red(c, iv, 2, team, out); }
 
 int a5g_dt_reductions(a5g_ctx *c, double *out3) {
   if (!out3) return fail(A5G_EINVAL, "null argument");
@@ -4094,11 +4475,89 @@ int a5g_step(a5g_ctx *c, double dt) {
   if (c->precision == A5G_MIXED) {
     int r = mx_ready(c);
     if (r) return r;
-    a5g_step_mixed_kernel<<<1, NTHR, c->dyn_smem32, c->stream>>>(c->d_run, dt, deposit);
-  } else {
-    a5g_step_kernel<<<1, NTHR, c->dyn_smem, c->stream>>>(c->d_run, dt, deposit);
   }
+  const void *fn = c->precision == A5G_MIXED ? (const void *)a5g_step_mixed_kernel
+                                             : (const void *)a5g_step_kernel;
+  if (c->n_cta > 1) {
+    const RunDev *run = c->d_run;
+    void *args[] = {(void *)&run, (void *)&dt, (void *)&deposit};
+    CK(cudaLaunchCooperativeKernel(fn, dim3(c->n_cta), dim3(NTHR), args, 0, c->stream));
+    return A5G_OK;
+  }
+  if (c->precision == A5G_MIXED)
+    a5g_step_mixed_kernel<<<1, NTHR, c->dyn_smem32, c->stream>>>(c->d_run, dt, deposit);
+  else
+    a5g_step_kernel<<<1, NTHR, c->dyn_smem, c->stream>>>(c->d_run, dt, deposit);
   CK(cudaGetLastError());
+  return A5G_OK;
+}
+
+// Largest grid of co-resident blocks a cooperative launch of the run kernels
+// may have on the current device (blocks per SM at no dynamic shared memory
+// times the SMs, over the kernels a grid-mode run launches).
+static int max_coresident_ctas() {
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+  int best = INT_MAX;
+  const void *fns[3] = {(const void *)a5g_run_kernel, (const void *)a5g_step_kernel,
+                        (const void *)a5g_step_mixed_kernel};
+  for (const void *fn : fns) {
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, NTHR, 0) != cudaSuccess) return 0;
+    best = std::min(best, nb * sms);
+  }
+  return std::min(best, A5G_MAX_CTAS);
+}
+
+int a5g_set_ctas(a5g_ctx *c, int n_cta, long long wait_cycles) {
+  if (!c) return fail(A5G_EINVAL, "null context");
+  if (n_cta < 1 || n_cta > A5G_MAX_CTAS) return fail(A5G_EINVAL, "n_cta must be 1..A5G_MAX_CTAS");
+  if (n_cta > 1) {
+    const int lim = max_coresident_ctas();
+    if (n_cta > lim)
+      return fail(A5G_EINVAL, "n_cta = " + std::to_string(n_cta) + " exceeds the " + std::to_string(lim) +
+                                  " blocks that can be co-resident on this device");
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaMemset(c->gbar, 0, 4 * sizeof(unsigned)));
+  c->n_cta = n_cta;
+  c->h.gbudget = wait_cycles < 0 ? A5G_DEFAULT_WAIT_CYCLES : wait_cycles;
+  apply_staging(c);
+  int r = push_run(c);
+  if (r) return r;
+  return mx_ready(c);
+}
+
+int a5g_set_grid_local(a5g_ctx *c, int cells) {
+  if (!c) return fail(A5G_EINVAL, "null context");
+  if (cells < 0) return fail(A5G_EINVAL, "cells must be >= 0");
+  c->h.local_cells = cells;
+  return push_run(c);
+}
+
+int a5g_get_ctas(a5g_ctx *c, int *n_cta, int *max_cta) {
+  if (!c) return fail(A5G_EINVAL, "null context");
+  if (n_cta) *n_cta = c->n_cta;
+  if (max_cta) *max_cta = max_coresident_ctas();
+  return A5G_OK;
+}
+
+// Orders a batched launch on stream s after the work already queued on each
+// member's own stream (in), and each member's later work after it (out):
+// events recorded and waited on the device, no host synchronisation.
+static int batch_order_in(a5g_ctx *const *ctxs, int n, cudaStream_t s) {
+  for (int k = 0; k < n; k++) {
+    if (ctxs[k]->stream == s) continue;
+    CK(cudaEventRecord(ctxs[k]->ev_order, ctxs[k]->stream));
+    CK(cudaStreamWaitEvent(s, ctxs[k]->ev_order, 0));
+  }
+  return A5G_OK;
+}
+static int batch_order_out(a5g_ctx *const *ctxs, int n, cudaStream_t s, cudaEvent_t done) {
+  CK(cudaEventRecord(done, s));
+  for (int k = 0; k < n; k++)
+    if (ctxs[k]->stream != s) CK(cudaStreamWaitEvent(ctxs[k]->stream, done, 0));
   return A5G_OK;
 }
 
@@ -4132,8 +4591,9 @@ int a5g_step_batch(a5g_ctx **ctxs, int n, const double *dts) {
     ops[k] = mkop(ctxs[k]->precision == A5G_MIXED ? OP_STEP_MIXED : OP_STEP, ph ? 1 : 0, 0, dts[k]);
     ops[n + k] = ph ? mkop(OP_PH_SOURCE, 1, 0, dts[k]) : mkop(OP_NOP);
   }
-  // other members' queued work must finish before the batch runs on c0's stream
-  for (int k = 1; k < n; k++) CK(cudaStreamSynchronize(ctxs[k]->stream));
+  // the batch runs on c0's stream after the other members' queued work
+  int ro = batch_order_in(ctxs, n, c0->stream);
+  if (ro) return ro;
   const RunDev **d_rp = nullptr;
   Op *d_ops = nullptr;
   CK(cudaMallocAsync((void **)&d_rp, n * sizeof(void *), c0->stream));
@@ -4155,14 +4615,29 @@ int a5g_step_batch(a5g_ctx **ctxs, int n, const double *dts) {
   CK(cudaGetLastError());
   CK(cudaFreeAsync(d_rp, c0->stream));
   CK(cudaFreeAsync(d_ops, c0->stream));
-  return A5G_OK;
+  // the members' own streams continue after the batch
+  return batch_order_out(ctxs, n, c0->stream, c0->ev_order);
 }
 
 // Per-device address of g_batch_scratch, looked up on first use with the
-// device current; host staging of the descriptors in a fixed host array.
+// device current.
 static std::mutex g_static_mu;
 static BatchSlot *g_static_dev[256] = {};
-static BatchSlot g_static_host[A5G_STATIC_BATCH_MAX];
+
+// Writes the n descriptors of one launch into the fixed table on stream s,
+// as kernel parameters of fill launches (ordered with the launch that reads
+// them like any other work of the stream).
+static int static_fill(BatchSlot *table, const BatchSlot *slots, int n, cudaStream_t s) {
+  for (int k0 = 0; k0 < n; k0 += SLOT_FILL) {
+    const int m = std::min(SLOT_FILL, n - k0);
+    SlotChunk chunk;
+    std::memset(&chunk, 0, sizeof(chunk));
+    std::memcpy(chunk.s, slots + k0, (size_t)m * sizeof(BatchSlot));
+    a5g_fill_slots_kernel<<<1, 128, 0, s>>>(table + k0, chunk, m);
+    CK(cudaGetLastError());
+  }
+  return A5G_OK;
+}
 
 int a5g_step_batch_static(a5g_ctx **ctxs, int n, const double *dts) {
   if (!ctxs || !dts || n < 1) return fail(A5G_EINVAL, "bad batch");
@@ -4192,7 +4667,8 @@ int a5g_step_batch_static(a5g_ctx **ctxs, int n, const double *dts) {
     g_static_dev[dev] = static_cast<BatchSlot *>(p);
   }
   a5g_ctx *c0 = ctxs[0];
-  for (int k = 1; k < n; k++) CK(cudaStreamSynchronize(ctxs[k]->stream));
+  int ro = batch_order_in(ctxs, n, c0->stream);
+  if (ro) return ro;
   size_t dyn = 0, ph_smem = 0;
   bool any_ph = false;
   int max_team = 0;
@@ -4210,15 +4686,17 @@ int a5g_step_batch_static(a5g_ctx **ctxs, int n, const double *dts) {
       ph_smem = std::max(ph_smem, ph_smem_bytes(ctxs[k]));
     }
   }
+  // descriptors of this call on the host stack (A5G_STATIC_BATCH_MAX x 40 bytes)
+  BatchSlot slots[A5G_STATIC_BATCH_MAX];
   if (any_ph) {
     // photon sources and absorption first; the table is then rewritten with
-    // the step descriptors (copies and launches are ordered on the stream)
+    // the step descriptors (fills and launches are ordered on the stream)
     for (int k = 0; k < n; k++) {
-      g_static_host[k].run = ctxs[k]->d_run;
-      g_static_host[k].op = ctxs[k]->p.photoi_enabled ? mkop(OP_PH_SOURCE, 1, 0, dts[k]) : mkop(OP_NOP);
+      slots[k].run = ctxs[k]->d_run;
+      slots[k].op = ctxs[k]->p.photoi_enabled ? mkop(OP_PH_SOURCE, 1, 0, dts[k]) : mkop(OP_NOP);
     }
-    CK(cudaMemcpyAsync(g_static_dev[dev], g_static_host, (size_t)n * sizeof(BatchSlot),
-                       cudaMemcpyHostToDevice, c0->stream));
+    int rf = static_fill(g_static_dev[dev], slots, n, c0->stream);
+    if (rf) return rf;
     a5g_run_kernel_slots<<<n, NTHR, dyn, c0->stream>>>(g_static_dev[dev]);
     CK(cudaGetLastError());
     dim3 grid((unsigned)((max_team + PH_THREADS - 1) / PH_THREADS), (unsigned)n);
@@ -4227,16 +4705,16 @@ int a5g_step_batch_static(a5g_ctx **ctxs, int n, const double *dts) {
     CK(cudaGetLastError());
   }
   for (int k = 0; k < n; k++) {
-    g_static_host[k].run = ctxs[k]->d_run;
-    g_static_host[k].op = mkop(ctxs[k]->precision == A5G_MIXED ? OP_STEP_MIXED : OP_STEP,
-                               ctxs[k]->p.photoi_enabled ? 1 : 0, 0, dts[k]);
+    slots[k].run = ctxs[k]->d_run;
+    slots[k].op = mkop(ctxs[k]->precision == A5G_MIXED ? OP_STEP_MIXED : OP_STEP,
+                       ctxs[k]->p.photoi_enabled ? 1 : 0, 0, dts[k]);
   }
-  // pageable source: the copy is staged before the call returns
-  CK(cudaMemcpyAsync(g_static_dev[dev], g_static_host, (size_t)n * sizeof(BatchSlot),
-                     cudaMemcpyHostToDevice, c0->stream));
+  int rf = static_fill(g_static_dev[dev], slots, n, c0->stream);
+  if (rf) return rf;
   a5g_run_kernel_slots<<<n, NTHR, dyn, c0->stream>>>(g_static_dev[dev]);
   CK(cudaGetLastError());
-  return A5G_OK;
+  // the members' own streams continue after the batch
+  return batch_order_out(ctxs, n, c0->stream, c0->ev_order);
 }
 
 // ---------------------------------------------------------------------------
@@ -4388,8 +4866,11 @@ int a5g_batch_launch(a5g_batch *b, int num_steps, int use_graph) {
     int r;
     if (c->p.photoi_enabled && (r = ph_ready(c))) return r;
     if ((r = mx_ready(c))) return r;
-    // the members' own queued work (uploads, regrids) precedes the block
-    CK(cudaStreamSynchronize(c->stream));
+  }
+  // the members' own queued work (uploads, regrids) precedes the block
+  {
+    int r = batch_order_in(b->ctxs.data(), n, b->stream);
+    if (r) return r;
   }
   CK(cudaEventRecord(b->ev0, b->stream));
   if (use_graph) {
@@ -4413,7 +4894,11 @@ int a5g_batch_launch(a5g_batch *b, int num_steps, int use_graph) {
     int r = batch_enqueue(b, num_steps);
     if (r) return r;
   }
-  CK(cudaEventRecord(b->ev1, b->stream));
+  // ev1 ends the timed block; the members' own streams continue after it
+  {
+    int r = batch_order_out(b->ctxs.data(), n, b->stream, b->ev1);
+    if (r) return r;
+  }
   a5g_batch_gather_kernel<<<(n + 127) / 128, 128, 0, b->stream>>>(b->d_rp, n, b->d_state);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(b->h_state, b->d_state, 5 * n * sizeof(double), cudaMemcpyDeviceToHost,
@@ -4477,6 +4962,32 @@ int a5g_debug_info(a5g_ctx *c, long long *out8) {
   out8[6] = c->h.mx_smem;
   out8[7] = (long long)c->dyn_smem32;
   return A5G_OK;
+}
+
+// Internal diagnostics: the layout of a5g_params as this library was
+// compiled, so that tests can hold the documented bindings to it. out[0] is
+// sizeof(a5g_params), out[1..] the offsets of its fields in declaration
+// order; returns the number of values written (at most n).
+int a5g_debug_params_layout(int *out, int n) {
+  if (!out) return 0;
+  const int v[] = {(int)sizeof(a5g_params),
+                   (int)offsetof(a5g_params, box_size), (int)offsetof(a5g_params, coord),
+                   (int)offsetof(a5g_params, lvls_max), (int)offsetof(a5g_params, dr_base),
+                   (int)offsetof(a5g_params, domain_len_z), (int)offsetof(a5g_params, applied_fld),
+                   (int)offsetof(a5g_params, epsilon_diel), (int)offsetof(a5g_params, dt_max),
+                   (int)offsetof(a5g_params, use_drt), (int)offsetof(a5g_params, n_cycle_base),
+                   (int)offsetof(a5g_params, ref_init_time), (int)offsetof(a5g_params, crv_refine),
+                   (int)offsetof(a5g_params, n_seeds), (int)offsetof(a5g_params, seed_r0),
+                   (int)offsetof(a5g_params, seed_r1), (int)offsetof(a5g_params, seed_width),
+                   (int)offsetof(a5g_params, photoi_enabled),
+                   (int)offsetof(a5g_params, photoi_num_photons),
+                   (int)offsetof(a5g_params, photoi_team), (int)offsetof(a5g_params, photoi_pad),
+                   (int)offsetof(a5g_params, photoi_coeff), (int)offsetof(a5g_params, photoi_fac_dx),
+                   (int)offsetof(a5g_params, rng_seed), (int)offsetof(a5g_params, uniform_lvl),
+                   (int)offsetof(a5g_params, uniform_pad)};
+  const int m = std::min(n, (int)(sizeof(v) / sizeof(v[0])));
+  for (int k = 0; k < m; k++) out[k] = v[k];
+  return m;
 }
 
 int a5g_get_stream(a5g_ctx *c, void **stream) {

@@ -59,6 +59,7 @@ def make_params(cfg) -> _lib.Params:
     p.photoi_fac_dx = cfg.photoi_fac_dx
     for i in range(4):
         p.rng_seed[i] = cfg.rng_seed[i]
+    p.uniform_lvl = cfg.uniform_lvl
     return p
 
 
@@ -169,6 +170,28 @@ class DeviceRun:
     def fas_fmg(self, set_residual: bool, first_call: bool):
         call("a5g_fas_fmg", self.h, 1 if set_residual else 0, 1 if first_call else 0)
 
+    def fas_vcycle(self, max_lvl: int, set_residual: bool = False):
+        """mg$D_fas_vcycle (afivo/src/m_aX_mg.f90:208-254)."""
+        call("a5g_mg_fas_vcycle", self.h, int(max_lvl), 1 if set_residual else 0)
+
+    def tree_max_cc(self, iv: int) -> float:
+        """a$D_tree_max_cc: max over the leaves' interior cells."""
+        out = ctypes.c_double()
+        call("a5g_tree_max_cc", self.h, iv, ctypes.byref(out))
+        return out.value
+
+    def tree_min_cc(self, iv: int) -> float:
+        """a$D_tree_min_cc: min over the leaves' interior cells."""
+        out = ctypes.c_double()
+        call("a5g_tree_min_cc", self.h, iv, ctypes.byref(out))
+        return out.value
+
+    def tree_sum_cc(self, iv: int, team: int = 1) -> float:
+        """a$D_tree_sum_cc as an OpenMP team of `team` threads forms it."""
+        out = ctypes.c_double()
+        call("a5g_tree_sum_cc", self.h, iv, int(team), ctypes.byref(out))
+        return out.value
+
     def fld_from_pot(self):
         call("a5g_fld_from_pot", self.h)
 
@@ -240,6 +263,22 @@ class DeviceRun:
     def set_rng_state(self, st) -> None:
         st = np.ascontiguousarray(st, dtype=np.int32)
         call("a5g_set_rng", self.h, _ip(st))
+
+    def set_ctas(self, n_cta: int, wait_cycles: int = -1):
+        """Grid mode: the run's phases on n_cta co-resident thread blocks
+        (a5g_set_ctas); 1 is one block. wait_cycles bounds each barrier wait
+        (< 0: the library's default)."""
+        call("a5g_set_ctas", self.h, int(n_cta), int(wait_cycles))
+
+    def set_grid_local(self, cells: int):
+        """Grid mode: levels of at most `cells` cells run on one block."""
+        call("a5g_set_grid_local", self.h, int(cells))
+
+    def ctas(self) -> Tuple[int, int]:
+        """(blocks per launch of this run, most blocks the device can hold at once)"""
+        n, m = ctypes.c_int(0), ctypes.c_int(0)
+        call("a5g_get_ctas", self.h, ctypes.byref(n), ctypes.byref(m))
+        return n.value, m.value
 
     def sync(self):
         call("a5g_sync", self.h)

@@ -36,6 +36,11 @@ sys.path.insert(0, ROOT)
 
 METRIC = ("cell-updates/s per full step, mixed vs FP64 on 1 B200 at stated error; %HBM roof")
 UNIT = "cell-updates/s"
+# Horizon of the mixed form's frozen-mesh error contract (steps), fixed
+# whatever --steps is: errors grow along a run, so a shorter horizon would be
+# a weaker contract.
+ERR_STEPS = 200
+L2_NOTE = "flushed before every timed step (256 MiB write)"
 
 
 def parse():
@@ -54,6 +59,9 @@ def parse():
                     help="fmg,down,up,base,corr: use this schedule instead of the autotuners' choice")
     ap.add_argument("--runs", type=int, default=64,
                     help="independent uneven runs of the device-driven batch (0: skip)")
+    ap.add_argument("--large-level", type=int, default=6,
+                    help="uniform level of the large-tree grid-mode extra (6: 1M leaf cells; 0: skip)")
+    ap.add_argument("--large-steps", type=int, default=10, help="timed steps of the large-tree extra")
     return ap.parse_args()
 
 
@@ -174,7 +182,9 @@ def run_reference(args):
     cfg, wname = workload_cfg(args.workload)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import a5ref
+    import numpy as np
     threads = os.cpu_count() or 1
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     sim = a5ref.Sim(cfg, n_threads=threads)
     sim.init()
     sim.run(cfg.end_time)
@@ -182,17 +192,27 @@ def run_reference(args):
     dt = sim.get_max_dt()
     for _ in range(args.warmup):
         sim.step(dt)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
+    photons = sim.photons_created() if cfg.photoi_enabled else 0
+    # the device arm's protocol: a 256 MiB write before every timed step
+    # (outside the timed region), here to the host caches
+    flush = np.zeros(256 << 20, dtype=np.uint8)
+    el = 0.0
+    for k in range(args.steps):
+        flush.fill(k & 0xFF)
+        t0 = time.perf_counter()
         sim.step(dt)
-    el = time.perf_counter() - t0
+        el += time.perf_counter() - t0
     value = n_leaf * args.steps / el
+    meta = sim.meta()
     out = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": wname, "leaf_cells": n_leaf, "max_lvl": sim.max_lvl},
+        "config": {"workload": wname, "leaf_cells": n_leaf, "boxes_in_use": int(meta[:, 0].sum()),
+                   "min_lvl": sim.min_lvl, "max_lvl": sim.max_lvl,
+                   "precision": "fp64", "parallelism": f"replicas{world}",
+                   "photons_per_step": photons, "l2": L2_NOTE},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"{args.steps} full steps of the {wname} mesh at t_end, "
                                    f"OpenMP over the boxes of each level"},
@@ -257,6 +277,90 @@ def run_uneven_batch(n_runs, first_schedule, fixed=False):
         "max": max(er), "median": statistics.median(er),
         "note": "photon counts are stochastic: two runs draw different photons once a rounded count differs"}
     return out
+
+
+def run_large_tree(level, steps, warmup, flush, clock_index):
+    """The grid-mode form on a large tree: the 8 mm Cartesian case on a
+    uniformly refined mesh of the given level (config.cartesian_uniform;
+    level 6: 1,048,576 leaf cells), one run on all co-resident blocks of the
+    GPU (a5g_set_ctas), FP64 and mixed; for comparison the same steps on one
+    block. Steps on the initial mesh at the step size get_max_dt gives, L2
+    flushed before each, CUDA events on the run's stream."""
+    import torch
+    from a5_streamer_b200 import config, metrics, streamer
+    cfg = config.cartesian_uniform(level)
+    sim = streamer.Simulation(cfg)
+    run = sim.device
+    n_cta = run.ctas()[1]
+    run.set_ctas(n_cta)
+    sim.init()
+    n_leaf = run.n_leaf_cells()
+    meta, _, levels = sim.tree.export()
+    cen = metrics.census(meta, levels, cfg.box_size)
+    bytes_step = metrics.bytes_per_step(cen)
+    dt = run.get_max_dt()
+    st = torch.cuda.ExternalStream(run.stream_ptr())
+
+    def timed(n):
+        for _ in range(warmup):
+            run.step(dt)
+        run.sync()
+        e0 = [torch.cuda.Event(enable_timing=True) for _ in range(n)]
+        e1 = [torch.cuda.Event(enable_timing=True) for _ in range(n)]
+        with torch.cuda.stream(st):
+            for k in range(n):
+                flush.fill_(k & 0xFF)
+                e0[k].record(st)
+                run.step(dt)
+                e1[k].record(st)
+        run.sync()
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(b) for a, b in zip(e0, e1)) / n
+
+    with ClockSampler(clock_index) as clk:
+        torch.cuda.nvtx.range_push("large_tree_grid")
+        ms = timed(steps)
+        torch.cuda.nvtx.range_pop()
+    peak = measured_peak()[0]
+    gbs = bytes_step / (ms / 1e3) / 1e9
+    out = {"workload": f"cartesian_uniform_lvl{level}", "leaf_cells": n_leaf,
+           "boxes_in_use": int(meta[:, 0].sum()), "min_lvl": sim.tree.min_lvl, "max_lvl": sim.tree.max_lvl,
+           "n_cta": n_cta, "ms_per_step": ms, "value": n_leaf / (ms / 1e3), "unit": UNIT,
+           "algorithmic_bytes_per_step": bytes_step, "achieved_gbs": gbs, "frac_of_measured_hbm": gbs / peak,
+           "clocks": clk.summary()}
+    # the mixed form on the same blocks (the reference's FMG schedule for
+    # the FP32 correction solve, which tracks FP64 to ~1e-9)
+    run.set_precision(True, (1, 2, 2, cfg.n_cycle_base, 1))
+    ms_m = timed(steps)
+    run.set_precision(False)
+    out["mixed"] = {"ms_per_step": ms_m, "value": n_leaf / (ms_m / 1e3),
+                    "speedup_vs_fp64": ms / ms_m, "schedule": [1, 2, 2, cfg.n_cycle_base, 1]}
+    # one block, as the small trees run
+    run.set_ctas(1)
+    ms1 = timed(max(2, steps // 5))
+    out["one_block"] = {"ms_per_step": ms1, "value": n_leaf / (ms1 / 1e3),
+                        "grid_speedup": ms1 / ms}
+    sim.close()
+    return out
+
+
+def moving_streamer_errors(schedule):
+    """Errors of the mixed form where the streamer moves: the 8 mm Cartesian
+    case at E_bg = 7 MV/m (levels up to 6, no photoionization), run from its
+    initial conditions to its end time in FP64 and in the mixed form with
+    `schedule`; head position (argmax of |E| on the symmetry line) and max |E|
+    compared at the end. In the benchmark's own cases the head stays in one
+    cell, so their head error is 0 by construction."""
+    from a5_streamer_b200 import autotune, config
+    cfg = config.cartesian_8mm(applied_fld=7e6, lvls_max=6)
+    h64 = autotune.whole_run_observables(cfg)
+    hmx = autotune.whole_run_observables(cfg, tuple(schedule))
+    return {"case": "cartesian_8mm E_bg=7MV/m lvls_max=6 t=2ns, photoionization off",
+            "schedule": list(schedule),
+            "head_z_m": {"seed": cfg.seeds[0].r0[1], "fp64": h64[0], "mixed": hmx[0]},
+            "head_z_rel": abs(hmx[0] - h64[0]) / abs(h64[0]),
+            "max_E_rel": abs(hmx[2] - h64[2]) / h64[2],
+            "bounds": {"max_E_rel": 1e-4, "head_z_rel": 5e-3}}
 
 
 def run_b200(args):
@@ -405,19 +509,19 @@ def run_b200(args):
             sched = tuple(int(v) for v in args.mixed_schedule.split(","))
             tuned = {"schedule": sched, "table": [], "n_steps": 0}
         else:
-            # the frozen-mesh check over the K steps reported below, and the
-            # whole run to the end time
-            tuned = autotune.tune_schedule(sim, n_steps=K, ref_head=head_fp64)
+            # the frozen-mesh check over the fixed error horizon (ERR_STEPS
+            # steps, whatever K is) and the whole run to the end time
+            tuned = autotune.tune_schedule(sim, n_steps=ERR_STEPS, ref_head=head_fp64)
             sched = tuned["schedule"]
         mrun = dv.clone_state(sim, mixed=True, schedule=sched)
         m_ms = time_single(mrun, "timed_mixed")
         mrun.close()
-        # K steps on the frozen mesh, photoionization off in both copies (the
-        # photon counts are stochastic and would diverge between the two)
+        # ERR_STEPS steps on the frozen mesh, photoionization off in both
+        # copies (the photon counts are stochastic and would diverge)
         cfg_np = dataclasses.replace(cfg, photoi_enabled=False)
         a = dv.clone_state(sim, cfg=cfg_np)
         b = dv.clone_state(sim, mixed=True, schedule=sched, cfg=cfg_np)
-        for _ in range(K):
+        for _ in range(ERR_STEPS):
             a.step(dt)
             b.step(dt)
         a.sync()
@@ -431,7 +535,7 @@ def run_b200(args):
             "speedup_vs_fp64": ms_per_step / m_ms, "dtype": "f32 fluxes/lookups/smoothing, f64 residual/potential/densities/dt",
             "schedule": {"fmg": sched[0], "n_cycle_down": sched[1], "n_cycle_up": sched[2],
                          "n_cycle_base": sched[3], "n_corr": sched[4]},
-            "errors_after_steps": {"steps": K, "photoionization": False,
+            "errors_after_steps": {"steps": ERR_STEPS, "photoionization": False,
                                    **{k: err_k[k] for k in ("max_E_rel", "head_z_rel", "phi_rel", "n_e_rel")}},
             "errors_whole_run": {"t_end": cfg.end_time,
                                  "head_z_rel": abs(head_m[0] - head_fp64[0]) / abs(head_fp64[0]),
@@ -443,8 +547,15 @@ def run_b200(args):
             "bounds": {"max_E_rel": 1e-4, "head_z_rel": 5e-3},
             "tuner": {"candidates": len(tuned["table"]), "frozen_mesh_steps": tuned["n_steps"],
                       "whole_run": True},
+            "errors_moving_streamer": moving_streamer_errors(sched),
             "batched": time_batch(True, sched) if args.batch > 0 else None,
         }
+        if batched and mixed["batched"]:
+            mixed["batched"]["speedup_vs_fp64"] = mixed["batched"]["value"] / batched["value"]
+
+    large = None
+    if args.large_level > 0 and rank == 0:
+        large = run_large_tree(args.large_level, args.large_steps, 3, flush, local)
 
     uneven = None
     if args.runs > 0 and rank == 0:
@@ -479,11 +590,11 @@ def run_b200(args):
                        "min_lvl": sim.tree.min_lvl, "max_lvl": sim.tree.max_lvl,
                        "precision": "fp64", "parallelism": f"replicas{world}",
                        "photons_per_step": photons,
-                       "l2": "flushed before every timed step (256 MiB write)"},
+                       "l2": L2_NOTE},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": K * launches_per_step,
             "clocks": clk.summary(), "batched": batched, "mixed": mixed,
-            "uneven_batch": uneven,
+            "uneven_batch": uneven, "large_tree": large,
         }
         print(json.dumps(out), flush=True)
     sim.close()

@@ -53,7 +53,8 @@ typedef struct a5g_params {
   double dr_base;        /* cell size at level 1 (a$D_lvl_dr) */
   double domain_len_z;   /* domain length along the last axis (m) */
   double applied_fld;    /* background field (V/m); phi(top) = -len_z * fld */
-  double epsilon_diel;   /* must be 1: the dielectric operators are not built */
+  double epsilon_diel;   /* ST_epsilon_diel: permittivity below a quarter of the
+                            domain (set_box_eps); 1 for none, > 0 */
   double dt_max;         /* ST_dt_max */
   int use_drt;           /* 1: dielectric-relaxation limit enters the dt minimum */
   int n_cycle_base;      /* base-level Gauss-Seidel cycles (8 Cartesian, 4 cyl) */
@@ -74,6 +75,12 @@ typedef struct a5g_params {
   double photoi_coeff;    /* photons per ionization (photoi_eta * quench factor) */
   double photoi_fac_dx;   /* table fraction that sets the absorption level (0.25e-3) */
   int rng_seed[4];        /* state of the master generator ST_rng */
+  /* > 0: refine every box below this level and keep the rest instead of the
+   * streamer's criterion (a uniformly refined mesh, as the multigrid
+   * benchmark afivo/examples/multigrid/test_mg_benchmark_2d.f90:40-86
+   * builds); 0: set_ref_flags */
+  int uniform_lvl;
+  int uniform_pad;
 } a5g_params;
 
 /* Box metadata for a5g_upload_tree: per id (0..max_id) 16 ints
@@ -151,8 +158,27 @@ int a5g_average_dens(a5g_ctx *ctx);
 int a5g_compute_fld(a5g_ctx *ctx, int no_guess);
 /* mg$D_fas_fmg(tree, mg, set_residual, first_call) alone */
 int a5g_fas_fmg(a5g_ctx *ctx, int set_residual, int first_call);
+/* mg$D_fas_vcycle(tree, mg, max_lvl, set_residual) alone
+ * (afivo/src/m_aX_mg.f90:208-254): one FAS V-cycle from level max_lvl
+ * (min_lvl..max_lvl of the tree) down to the coarsest level and back, the
+ * potential's ghost cells valid on input and output; set_residual != 0 also
+ * stores rhs - A phi of levels min_lvl..max_lvl in the scratch variable
+ * (i_fld, as the reference's i_tmp). */
+int a5g_mg_fas_vcycle(a5g_ctx *ctx, int max_lvl, int set_residual);
 /* fld_from_pot on all boxes + a$D_gc_tree(i_fld, a$D_gc_interp, neumann) */
 int a5g_fld_from_pot(a5g_ctx *ctx);
+/* a$D_tree_max_cc / a$D_tree_min_cc (afivo/src/m_aX_utils.f90:559-619):
+ * max / min of cell variable iv over the interior cells of the leaves.
+ * Synchronises. */
+int a5g_tree_max_cc(a5g_ctx *ctx, int iv, double *out);
+int a5g_tree_min_cc(a5g_ctx *ctx, int iv, double *out);
+/* a$D_tree_sum_cc (afivo/src/m_aX_utils.f90:621-680): sum over the leaves
+ * of lvl_dr^2 times the box sum (cylindrical: of 2 pi r times the value).
+ * The reference forms it in an OpenMP reduction whose rounding depends on the
+ * team; this call gives the value a team of `team` threads forms (static
+ * chunks of each level's leaves, partial sums added in thread order; team 1
+ * is the plain loop order). Synchronises. */
+int a5g_tree_sum_cc(a5g_ctx *ctx, int iv, int team, double *out);
 /* The reductions of get_max_dt (src/streamer_2d.f90:280-282):
  * out3 = {max |E|, min |E|, max n_e} over leaf interiors. */
 int a5g_dt_reductions(a5g_ctx *ctx, double *out3);
@@ -219,9 +245,11 @@ int a5g_get_precision(a5g_ctx *ctx, int *precision, a5g_mg_schedule *sched);
 int a5g_step(a5g_ctx *ctx, double dt);
 /* The same step for several independent runs in one launch (one persistent
  * thread block per run). dts[k] is the step of run k. The launches go on the
- * first run's stream after the other runs' streams are synchronized (one
- * host call per member and step); the device-driven batch (a5g_batch_*)
- * replays whole blocks of steps from CUDA graphs instead. */
+ * first run's stream, ordered on the device after the work already queued on
+ * every member's stream; work queued afterwards on any member's stream runs
+ * after the batch (event waits, no host synchronisation). The device-driven
+ * batch (a5g_batch_*) replays whole blocks of steps from CUDA graphs
+ * instead. */
 int a5g_step_batch(a5g_ctx **ctxs, int n, const double *dts);
 /* Batched step that allocates no device memory. Same result as
  * a5g_step_batch; no counterpart in the reference (its Fortran host has no
@@ -268,9 +296,37 @@ int a5g_batch_block(a5g_batch *b, int num_steps, int use_graph, double *dt, doub
                     int *active, float *gpu_ms);
 /* a5g_batch_block in two halves: launch queues the block on the batch's own
  * stream and returns; finish waits for it and returns its results. Between
- * the two the host may work on other batches (e.g. regrid their runs). */
+ * the two the host may work on other batches (e.g. regrid their runs). The
+ * block is ordered on the device after the work queued on the members'
+ * streams, and work queued on a member's stream after the launch runs after
+ * the block. */
 int a5g_batch_launch(a5g_batch *b, int num_steps, int use_graph);
 int a5g_batch_finish(a5g_batch *b, double *dt, double *time, int *active, float *gpu_ms);
+/* Grid mode: the run's phases on n_cta thread blocks instead of one. The
+ * reference runs a box loop over the boxes of a level with OpenMP threads
+ * (afivo/src/m_aX_utils.f90:58-185); one block per run keeps a small tree's
+ * phases behind block barriers, which is the fast form for trees of a few
+ * thousand cells, but uses one SM. With n_cta > 1 every operation of the run
+ * (steps, field solves, reductions, flags, prolongation) is one cooperative
+ * launch of n_cta co-resident blocks that share each phase's items, with a
+ * grid barrier between phases; results are identical to one block. Each
+ * barrier wait is bounded by wait_cycles SM clock cycles (< 0: the default,
+ * A5G_DEFAULT_WAIT_CYCLES); a wait that runs out makes the launch return
+ * early and the next synchronising call report A5G_TIMEOUT (0 makes every
+ * wait run out at once: a way to exercise that path). n_cta is limited to the
+ * blocks the device can hold at once (a5g_get_ctas reports it) and to
+ * A5G_MAX_CTAS. The reference has no counterpart (it has no device). */
+#define A5G_MAX_CTAS 256
+#define A5G_DEFAULT_WAIT_CYCLES 4000000000LL
+int a5g_set_ctas(a5g_ctx *ctx, int n_cta, long long wait_cycles);
+int a5g_get_ctas(a5g_ctx *ctx, int *n_cta, int *max_cta);
+/* Grid mode: multigrid levels are visited in order and the coarse ones hold
+ * few cells, so a stretch of phases on levels of at most `cells` cells (from
+ * the coarsest level up) runs on one block of the group while the others
+ * wait at the barrier that ends it, instead of a grid barrier per phase.
+ * 0 spreads every phase over the whole group. Results do not depend on it. */
+#define A5G_DEFAULT_LOCAL_CELLS 8192
+int a5g_set_grid_local(a5g_ctx *ctx, int cells);
 /* Wait for all work queued on the context's stream. */
 int a5g_sync(a5g_ctx *ctx);
 /* The cudaStream_t (as void*) all work of this context is queued on, so a

@@ -1326,6 +1326,7 @@ struct Sim {
   Rng rng;       // ST_rng (src/m_streamer.f90:69)
   PhTbl ph;      // ST_photoi_tbl
   int pho_lvl = 1;
+  long n_photons = 0;  // photons created by the last photoionization call
 };
 
 // src/m_streamer.f90:339-362 (koren_mlim)
@@ -1440,6 +1441,12 @@ static void loop_leaves(Tree &t, const std::function<void(Box &, int)> &f) {
 // src/streamer_2d.f90:177-216 (set_ref_flags); cyl :190-227
 static void set_ref_flags(Sim &s, Tree &t, int id, std::vector<int> &rf) {
   Box &b = t.boxes[id];
+  if (s.p.uniform_lvl > 0) {
+    // uniformly refined mesh (the multigrid benchmark's,
+    // afivo/examples/multigrid/test_mg_benchmark_2d.f90:40-86)
+    rf[id] = b.lvl < s.p.uniform_lvl ? DO_REF : KP_REF;
+    return;
+  }
   int nc = b.n_cell;
   double dr2 = b.dr * b.dr;
   double mrhs = 0, max_fld = -1.7976931348623157e308;
@@ -1880,6 +1887,7 @@ static void set_photoionization(Sim &s, double dt, bool has_dt) {
     }
   }
   const long n_used = (long)src.size();
+  s.n_photons = n_used;
   // absorption, PH_do_absorp (:161-205) in 3D, then the radius, :318-329
   std::vector<Rng> arngs = prng_init(s.rng, (int)W);
   std::vector<double> dst(2 * (size_t)n_used);
@@ -2148,9 +2156,22 @@ void a5ref_op_fmg(a5ref_sim *h, int set_residual, int first_call) {
   h->s.applied_voltage = -h->s.p.domain_len_z * h->s.p.applied_fld;
   fas_fmg(h->s.tree, h->s.mg, set_residual != 0, first_call != 0);
 }
+// mg$D_fas_vcycle(tree, mg, set_residual, highest_lvl), afivo/src/m_aX_mg.f90:208-254
+void a5ref_op_vcycle(a5ref_sim *h, int max_lvl, int set_residual) {
+  h->s.applied_voltage = -h->s.p.domain_len_z * h->s.p.applied_fld;
+  fas_vcycle(h->s.tree, h->s.mg, max_lvl, set_residual != 0);
+}
 void a5ref_op_fld_from_pot(a5ref_sim *h) {
   loop_all_boxes(h->s.tree, [](Box &b) { fld_from_pot(b); });
   gc_tree(h->s.tree, I_FLD, gc_interp, gc_neumann);
+}
+// a$D_tree_max_cc / _min_cc / _sum_cc, afivo/src/m_aX_utils.f90:559-680;
+// the sum as a team of `team` OpenMP threads forms it (team 1: the loop order)
+long long a5ref_photons_created(a5ref_sim *h) { return h->s.n_photons; }
+double a5ref_tree_max_cc(a5ref_sim *h, int iv) { return tree_max_cc(h->s.tree, iv); }
+double a5ref_tree_min_cc(a5ref_sim *h, int iv) { return tree_min_cc(h->s.tree, iv); }
+double a5ref_tree_sum_cc(a5ref_sim *h, int iv, int team) {
+  return tree_sum_team(h->s.tree, iv, team < 1 ? 1 : team);
 }
 void a5ref_op_ref_flags(a5ref_sim *h, int *out) {
   Sim &s = h->s;
@@ -2689,6 +2710,188 @@ int a5ref_kat_mg_cyl_diel(int n_fmg, double *res, double *err, int *ml) {
 
 int a5ref_kat_mg2_2d(int n_fmg, double *res, double *err, int *ml) {
   return kat_mg(false, n_fmg, res, err, ml);
+}
+
+// afivo/examples/transport/test_drift_diff_2d.f90: phi advected with velocity
+// (1, 1) on the periodic square [0, 2 pi]^2 (one base box of 8 x 8 cells, its
+// own neighbour on every side, no coarse levels), exact solution
+// sin^4(x - t) cos^4(y - t) (:187-200). Koren-limited upwind fluxes with the
+// second ghost layer (:283-348, here with the oracle's koren_mlim), flux
+// consistency, the update (:351-361), restriction and limited ghost cells,
+// the trapezoidal step of time_step_method 2 (:84-101), dt = 0.5 / (sum |v| /
+// dr_min + eps) (:68-70; no diffusion), a regrid after every step with the
+// example's criterion (:131-153) and prolong_to_new_children (:369-389).
+// This runs the oracle's own transport machinery -- gc2_box, gc_tree with
+// gc_interp_lim, consistent_fluxes, restrict_tree, prolong1_to and
+// adjust_refinement -- against a known solution.
+//  uniform_lvl > 0: refine uniformly to that level instead (no regrid steps);
+//  regrid = 0: no regrid after the initial mesh (frozen mesh).
+// out: [0] max |error| over the leaves at the end (a$D_tree_max_cc /
+// _min_cc of phi - solution, :103-117), [1] mean |error| (cell-size
+// weighted), [2] sum of phi at the start and [3] at the end
+// (a$D_tree_sum_cc), [4] steps, [5] max level, [6] leaf cells, [7] time.
+static int kat_drift_diff(int uniform_lvl, double end_time, int regrid, double *out) {
+  const int nc = 8, v_phi = 0, v_old = 1, v_err = 2;
+  const double two_pi = 2 * std::acos(-1.0);
+  const double vel[2] = {1.0, 1.0}, diff_coeff = 0.0;
+  Tree t;
+  const double r0[2] = {0, 0};
+  tree_init(t, nc, 3, 1, two_pi / nc, r0, 20, 0, XYZ);
+  const int ixl[1][2] = {{1, 1}};
+  std::vector<std::array<int, 4>> nbl(1, std::array<int, 4>{1, 1, 1, 1});
+  set_base(t, 1, ixl, nbl);
+  auto solution = [&](double x, double y, double tm) {
+    const double a = std::sin(x - vel[0] * tm), b = std::cos(y - vel[1] * tm);
+    const double a2 = a * a, b2 = b * b;
+    return (a2 * a2) * (b2 * b2);
+  };
+  auto set_init = [&](Box &b) {
+    for (int j = 0; j <= nc + 1; j++)
+      for (int i = 0; i <= nc + 1; i++) {
+        const double x = b.r_min[0] + (i - 0.5) * b.dr, y = b.r_min[1] + (j - 0.5) * b.dr;
+        b.c(i, j, v_phi) = solution(x, y, 0.0);
+      }
+  };
+  int n_bc = 0;  // physical-boundary calls: none exist on the periodic square
+  const GcFn no_bc = [&n_bc](Tree &, int, int, int) { n_bc++; };
+  const RefFn ref_fn = [&](Tree &tt, int id, std::vector<int> &rf) {
+    const Box &b = tt.boxes[id];
+    if (uniform_lvl > 0) {
+      rf[id] = b.lvl < uniform_lvl ? DO_REF : KP_REF;
+      return;
+    }
+    double diff = 0;
+    for (int j = 1; j <= nc; j++)
+      for (int i = 1; i <= nc + 1; i++)
+        diff = std::max(diff, std::fabs(b.c(i, j, v_phi) - b.c(i - 1, j, v_phi)));
+    for (int j = 1; j <= nc + 1; j++)
+      for (int i = 1; i <= nc; i++)
+        diff = std::max(diff, std::fabs(b.c(i, j, v_phi) - b.c(i, j - 1, v_phi)));
+    if (b.lvl < 3 || diff > 0.05) rf[id] = DO_REF;
+    else if (diff > 0.2 * 0.05) rf[id] = KP_REF;
+    else if (b.lvl > 4) rf[id] = RM_REF;
+  };
+  RefInfo ri;
+  do {
+    for (int lvl = t.min_lvl; lvl <= t.max_lvl; lvl++)
+      for (int id : t.L(lvl).ids) set_init(t.boxes[id]);
+    gc_tree(t, v_phi, gc_interp_lim, no_bc);
+    adjust_refinement(t, ref_fn, ri);
+  } while (ri.n_add > 0);
+  restrict_tree(t, v_phi);
+  gc_tree(t, v_phi, gc_interp_lim, no_bc);
+
+  auto tree_sum = [&]() { return tree_sum_team(t, v_phi, 1); };
+  // Koren fluxes of the example (:283-348) for velocity vel and diffusion 0
+  auto fluxes = [&](int id) {
+    Box &b = t.boxes[id];
+    const double inv_dr = 1 / b.dr;
+    double gc[4][64];
+    gc2_box(t, id, v_phi, gc);
+    for (int j = 1; j <= nc; j++)
+      for (int i = 1; i <= nc + 1; i++) {
+        const double gradc = b.c(i, j, v_phi) - b.c(i - 1, j, v_phi);
+        double f;
+        if (vel[0] < 0.0) {
+          const double tmp = i == nc + 1 ? gc[NB_HX][j - 1] : b.c(i + 1, j, v_phi);
+          f = vel[0] * (b.c(i, j, v_phi) - koren_mlim(gradc, tmp - b.c(i, j, v_phi)));
+        } else {
+          const double tmp = i == 1 ? gc[NB_LX][j - 1] : b.c(i - 2, j, v_phi);
+          f = vel[0] * (b.c(i - 1, j, v_phi) + koren_mlim(gradc, b.c(i - 1, j, v_phi) - tmp));
+        }
+        b.Fx(i, j, 0) = f - diff_coeff * gradc * inv_dr;
+      }
+    for (int j = 1; j <= nc + 1; j++)
+      for (int i = 1; i <= nc; i++) {
+        const double gradc = b.c(i, j, v_phi) - b.c(i, j - 1, v_phi);
+        double f;
+        if (vel[1] < 0.0) {
+          const double tmp = j == nc + 1 ? gc[NB_HY][i - 1] : b.c(i, j + 1, v_phi);
+          f = vel[1] * (b.c(i, j, v_phi) - koren_mlim(gradc, tmp - b.c(i, j, v_phi)));
+        } else {
+          const double tmp = j == 1 ? gc[NB_LY][i - 1] : b.c(i, j - 2, v_phi);
+          f = vel[1] * (b.c(i, j - 1, v_phi) + koren_mlim(gradc, b.c(i, j - 1, v_phi) - tmp));
+        }
+        b.Fy(i, j, 0) = f - diff_coeff * gradc * inv_dr;
+      }
+  };
+  auto update = [&](Box &b, double dt) {
+    const double inv_dr = 1 / b.dr;
+    for (int j = 1; j <= nc; j++)
+      for (int i = 1; i <= nc; i++)
+        b.c(i, j, v_phi) = b.c(i, j, v_phi) +
+                           dt * ((b.Fx(i, j, 0) - b.Fx(i + 1, j, 0)) * inv_dr +
+                                 (b.Fy(i, j, 0) - b.Fy(i, j + 1, 0)) * inv_dr);
+  };
+  const double sum0 = tree_sum();
+  double time = 0;
+  int steps = 0;
+  while (true) {
+    const double dr_min = t.dr_base * std::pow(0.5, t.max_lvl - 1);
+    const double dt = 0.5 / (2 * diff_coeff * (2 / (dr_min * dr_min)) +
+                             (std::fabs(vel[0]) / dr_min + std::fabs(vel[1]) / dr_min) +
+                             2.220446049250313e-16);
+    if (time > end_time) break;
+    tree_copy_cc(t, v_phi, v_old);
+    for (int stage = 0; stage < 2; stage++) {
+      for (int lvl = t.min_lvl; lvl <= t.max_lvl; lvl++) {
+        const Level &L = t.L(lvl);
+        const int n = (int)L.ids.size();
+#pragma omp parallel for schedule(static)
+        for (int k = 0; k < n; k++) fluxes(L.ids[k]);
+      }
+      consistent_fluxes(t, 0);
+      for (int lvl = t.min_lvl; lvl <= t.max_lvl; lvl++)
+        for (int id : t.L(lvl).ids) update(t.boxes[id], dt);
+      restrict_tree(t, v_phi);
+      gc_tree(t, v_phi, gc_interp_lim, no_bc);
+    }
+    for (int lvl = t.min_lvl; lvl <= t.max_lvl; lvl++)
+      for (int id : t.L(lvl).ids) {
+        Box &b = t.boxes[id];
+        const size_t m = (size_t)b.ncg() * b.ncg();
+        for (size_t k = 0; k < m; k++) b.cc[k + m * v_phi] = 0.5 * (b.cc[k + m * v_phi] + b.cc[k + m * v_old]);
+      }
+    time = time + dt;
+    steps++;
+    if (regrid && uniform_lvl <= 0) {
+      adjust_refinement(t, ref_fn, ri);
+      for (int lvl = 1; lvl <= t.max_lvl && lvl < (int)ri.add.size(); lvl++) {
+        for (int id : ri.add[lvl]) prolong1_to(t, id, v_phi);
+        for (int id : ri.add[lvl]) gc_box(t, id, v_phi, gc_interp_lim, no_bc);
+      }
+      gc_tree(t, v_phi, gc_interp_lim, no_bc);
+    }
+  }
+  double emax = 0, esum = 0, area = 0;
+  for (int lvl = t.min_lvl; lvl <= t.max_lvl; lvl++)
+    for (int id : t.L(lvl).leaves) {
+      Box &b = t.boxes[id];
+      for (int j = 1; j <= nc; j++)
+        for (int i = 1; i <= nc; i++) {
+          const double x = b.r_min[0] + (i - 0.5) * b.dr, y = b.r_min[1] + (j - 0.5) * b.dr;
+          const double e = b.c(i, j, v_phi) - solution(x, y, time);
+          b.c(i, j, v_err) = e;
+          emax = std::max(emax, std::fabs(e));
+          esum += std::fabs(e) * b.dr * b.dr;
+          area += b.dr * b.dr;
+        }
+    }
+  long long n_leaf = 0;
+  for (int lvl = t.min_lvl; lvl <= t.max_lvl; lvl++) n_leaf += (long long)t.L(lvl).leaves.size() * nc * nc;
+  out[0] = emax;
+  out[1] = esum / area;
+  out[2] = sum0;
+  out[3] = tree_sum();
+  out[4] = steps;
+  out[5] = t.max_lvl;
+  out[6] = (double)n_leaf;
+  out[7] = time;
+  return n_bc == 0 ? 0 : -1;
+}
+
+int a5ref_kat_drift_diff(int uniform_lvl, double end_time, int regrid, double *out8) {
+  return kat_drift_diff(uniform_lvl, end_time, regrid, out8);
 }
 int a5ref_kat_mg_cyl(int n_fmg, double *res, double *err, int *ml) {
   return kat_mg(true, n_fmg, res, err, ml);

@@ -73,6 +73,8 @@ typedef struct a5ref_params {
   double photoi_max_dist;  /* table range; the reference uses 2 * domain length */
   double photoi_fac_dx;    /* 0.25e-3 in the cylindrical driver */
   int rng_seed[4];         /* state of the master generator ST_rng */
+  int uniform_lvl;         /* > 0: refine every box below this level, keep the
+                              rest (a uniformly refined mesh) */
 } a5ref_params;
 
 /* The photon loops of PH_set_src_2d run in OpenMP regions whose outcome
@@ -123,6 +125,12 @@ void a5ref_op_compute_fld(a5ref_sim *s, int no_guess);
 void a5ref_op_set_rhs(a5ref_sim *s);
 void a5ref_op_fmg(a5ref_sim *s, int set_residual, int first_call);
 void a5ref_op_fld_from_pot(a5ref_sim *s);
+void a5ref_op_vcycle(a5ref_sim *s, int max_lvl, int set_residual);
+/* Photons created by the last photoionization call. */
+long long a5ref_photons_created(a5ref_sim *s);
+double a5ref_tree_max_cc(a5ref_sim *s, int iv);
+double a5ref_tree_min_cc(a5ref_sim *s, int iv);
+double a5ref_tree_sum_cc(a5ref_sim *s, int iv, int team);
 /* Per-box refinement flags from set_ref_flags (levels 1..max_lvl; boxes not
  * visited hold -huge). out has max_id+1 entries, index = box id. */
 void a5ref_op_ref_flags(a5ref_sim *s, int *out);
@@ -194,6 +202,13 @@ double a5ref_kat_photon_dist(double p_O2, double max_dist, int n_photons, int n_
 void a5ref_kat_rng(const int *state4, int n, int *out);
 /* Koren limiter (src/m_streamer.f90:339-362). */
 double a5ref_koren_mlim(double a, double b);
+/* Known-answer case restating afivo/examples/transport/test_drift_diff_2d.f90:
+ * exact advection of sin^4(x-t) cos^4(y-t) on the periodic square with Koren
+ * fluxes, the trapezoidal step and AMR (uniform_lvl > 0: uniform mesh of that
+ * level; regrid 0: frozen mesh). out8: max and mean |error| at the end, sum
+ * of phi at the start and end, steps, max level, leaf cells, end time.
+ * Returns 0, or -1 if a physical-boundary routine was called. */
+int a5ref_kat_drift_diff(int uniform_lvl, double end_time, int regrid, double *out8);
 
 #ifdef __cplusplus
 }

@@ -51,6 +51,7 @@ class Params(ctypes.Structure):
         ("photoi_len_lo", ctypes.c_double), ("photoi_len_hi", ctypes.c_double),
         ("photoi_max_dist", ctypes.c_double), ("photoi_fac_dx", ctypes.c_double),
         ("rng_seed", ctypes.c_int * 4),
+        ("uniform_lvl", ctypes.c_int),
     ]
 
 
@@ -83,6 +84,10 @@ def lib() -> ctypes.CDLL:
             "a5ref_op_average_dens": (V, [P]), "a5ref_op_compute_fld": (V, [P, I]),
             "a5ref_op_set_rhs": (V, [P]), "a5ref_op_fmg": (V, [P, I, I]),
             "a5ref_op_fld_from_pot": (V, [P]), "a5ref_op_ref_flags": (V, [P, pi]),
+            "a5ref_op_vcycle": (V, [P, I, I]),
+            "a5ref_tree_max_cc": (D, [P, I]), "a5ref_tree_min_cc": (D, [P, I]),
+            "a5ref_tree_sum_cc": (D, [P, I, I]),
+            "a5ref_photons_created": (ctypes.c_longlong, [P]),
             "a5ref_op_regrid": (I, [P, pi, pi]),
             "a5ref_max_id": (I, [P]), "a5ref_max_lvl": (I, [P]), "a5ref_min_lvl": (I, [P]),
             "a5ref_n_leaf_cells": (I, [P]), "a5ref_n_cells_all": (I, [P]),
@@ -101,6 +106,7 @@ def lib() -> ctypes.CDLL:
             "a5ref_kat_photon_table": (I, [I, D, D, D, D, pd, pd]),
             "a5ref_kat_photon_dist": (D, [D, D, I, I]),
             "a5ref_kat_rng": (V, [pi, I, pi]),
+            "a5ref_kat_drift_diff": (I, [I, D, I, pd]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -169,6 +175,7 @@ def make_params(cfg, n_threads: int = 0) -> Params:
     p.photoi_fac_dx = cfg.photoi_fac_dx
     for i in range(4):
         p.rng_seed[i] = cfg.rng_seed[i]
+    p.uniform_lvl = getattr(cfg, "uniform_lvl", 0)
     return p
 
 
@@ -229,6 +236,18 @@ class Sim:
     # ops ------------------------------------------------------------------------
     def op(self, name: str, *args):
         return getattr(lib(), "a5ref_op_" + name)(self.h, *args)
+
+    def tree_max_cc(self, iv: int) -> float:
+        return lib().a5ref_tree_max_cc(self.h, iv)
+
+    def tree_min_cc(self, iv: int) -> float:
+        return lib().a5ref_tree_min_cc(self.h, iv)
+
+    def tree_sum_cc(self, iv: int, team: int = 1) -> float:
+        return lib().a5ref_tree_sum_cc(self.h, iv, team)
+
+    def photons_created(self) -> int:
+        return int(lib().a5ref_photons_created(self.h))
 
     def ref_flags(self) -> np.ndarray:
         out = np.zeros(self.max_id + 1, dtype=np.int32)
@@ -385,3 +404,15 @@ def kat_rng(state4, n: int) -> np.ndarray:
     out = np.zeros(n, dtype=np.int32)
     lib().a5ref_kat_rng(_ip(st), n, _ip(out))
     return out
+
+
+def kat_drift_diff(uniform_lvl: int = 0, end_time: float = 5.0, regrid: bool = True) -> dict:
+    """The drift-diffusion example (afivo/examples/transport/
+    test_drift_diff_2d.f90) on the oracle's transport machinery: errors
+    against the exact advected solution and the conserved sum of phi."""
+    out = np.zeros(8)
+    rc = lib().a5ref_kat_drift_diff(uniform_lvl, end_time, 1 if regrid else 0, _dp(out))
+    if rc != 0:
+        raise RuntimeError("drift-diffusion case touched a physical boundary")
+    keys = ("max_err", "mean_err", "sum0", "sum_end", "steps", "max_lvl", "leaf_cells", "time")
+    return dict(zip(keys, out.tolist()))

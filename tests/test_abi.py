@@ -52,6 +52,48 @@ def test_invalid_parameters_are_rejected_without_a_device():
     assert _lib.lib().a5g_step_batch(None, 0, None) == _lib.A5G_EINVAL
 
 
+def _fortran_params_layout():
+    """Field offsets and size of the Fortran a5g_params_t documented in
+    INTEGRATION.md, by the C layout rules a bind(C) type follows (c_int: 4
+    bytes, c_double: 8 bytes, each aligned to its size; arrays contiguous)."""
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    body = re.search(r"type, bind\(C\) :: a5g_params_t\n(.*?)\n\s*end type a5g_params_t", text, re.S)
+    assert body, "a5g_params_t not found in INTEGRATION.md"
+    sizes = {"integer(c_int)": 4, "real(c_double)": 8}
+    fields, off, align = [], 0, 1
+    for line in body.group(1).splitlines():
+        kind, decl = [x.strip() for x in line.split("::")]
+        size = sizes[kind]
+        for item in re.findall(r"(\w+)(\([^)]*\))?", decl):
+            name, dims = item
+            n = 1
+            for d in re.findall(r"\d+", dims):
+                n *= int(d)
+            off = (off + size - 1) // size * size
+            fields.append((name, off))
+            off += n * size
+            align = max(align, size)
+    return fields, (off + align - 1) // align * align
+
+
+def test_params_layout_documented_python_and_c_agree():
+    """The Fortran binding in INTEGRATION.md, the ctypes mirror and the C
+    struct the library was compiled with have the same fields at the same
+    offsets and the same size: a caller following any of them passes the
+    object a5g_create reads."""
+    fields, size = _fortran_params_layout()
+    names = [f for f, _ in _lib.Params._fields_]
+    assert [f for f, _ in fields] == names
+    for name, off in fields:
+        assert getattr(_lib.Params, name).offset == off, name
+    assert ctypes.sizeof(_lib.Params) == size
+    out = (ctypes.c_int * 64)()
+    n = _lib.lib().a5g_debug_params_layout(out, 64)
+    assert n == 1 + len(names)
+    assert out[0] == size
+    assert list(out[1:n]) == [off for _, off in fields]
+
+
 def test_error_raises_with_status_name():
     with pytest.raises(_lib.A5GError) as e:
         _lib.call("a5g_step", None, 1e-12)

@@ -52,12 +52,26 @@ def test_driver_matches_oracle(name):
         _compare_full(sim, ref, f"block {k}")
 
 
-def test_run_to_end_time():
-    cfg = config.cartesian_8mm()
+@pytest.mark.parametrize("name", ["cartesian_8mm", "cylindrical_16mm", "cylindrical_16mm_photoi"])
+def test_run_to_end_time(name):
+    """Whole runs from the initial conditions to the end time, regrids
+    included. cylindrical_16mm_photoi is the benchmark's workload (the mesh
+    bench.py times: levels -1..7 at t = 10 ns) with Monte Carlo
+    photoionization, reproduced for the oracle's stated team size."""
+    cfg = {"cartesian_8mm": config.cartesian_8mm(),
+           "cylindrical_16mm": config.cylindrical_16mm(),
+           "cylindrical_16mm_photoi": config.cylindrical_16mm(photoi=True)}[name]
     sim = streamer.Simulation(cfg)
     ref = a5ref.Sim(cfg, n_threads=4)
     sim.init(); ref.init()
     nb1 = sim.run(cfg.end_time)
     nb2 = ref.run(cfg.end_time)
     assert nb1 == nb2
+    assert sim.time == ref.time and sim.time > cfg.end_time
     _compare_full(sim, ref, "end")
+    if cfg.photoi_enabled:
+        meta = ref.meta()
+        m = side_mask(meta, cfg.box_size)
+        assert np.array_equal(sim.device.cc(7)[m], ref.cc(7)[m]), "photoionization source differs"
+        assert np.array_equal(sim.device.rng_state(), ref.rng_state())
+    assert sim.device.n_leaf_cells() == ref.n_leaf_cells()

@@ -105,6 +105,38 @@ def test_fmg_set_residual(case):
     assert np.array_equal(sim.cc(5)[m], run.cc(5)[m])
 
 
+@pytest.mark.parametrize("below_top", [0, 2])
+@pytest.mark.parametrize("set_residual", [False, True])
+def test_vcycle_parity(case, below_top, set_residual):
+    """mg$D_fas_vcycle alone (a5g_mg_fas_vcycle): from the state after a
+    field solve (valid potential ghost cells, as the routine requires), one
+    V-cycle from the finest level or from two levels below it."""
+    cfg, sim, run = _fresh(case)
+    sim.op("compute_fld", 0)
+    run.compute_fld(False)
+    max_lvl = sim.max_lvl - below_top
+    for k in range(2):
+        sim.op("vcycle", max_lvl, int(set_residual))
+        run.fas_vcycle(max_lvl, set_residual)
+        compare(sim, run, cc_vars=[0, 1, 4, 6], where=f"vcycle {k}")
+    if set_residual:
+        # the residual of levels min..max_lvl is left in tmp (|E| elsewhere)
+        from parity import interior_mask
+        m = interior_mask(sim.meta(), cfg.box_size)
+        assert np.array_equal(sim.cc(5)[m], run.cc(5)[m])
+
+
+@pytest.mark.parametrize("iv", [0, 1, 4, 5])
+def test_tree_reductions(case, iv):
+    """a$D_tree_max_cc / _min_cc / _sum_cc over the leaves; the sum as teams
+    of several sizes form it."""
+    cfg, sim, run = _fresh(case)
+    assert run.tree_max_cc(iv) == sim.tree_max_cc(iv)
+    assert run.tree_min_cc(iv) == sim.tree_min_cc(iv)
+    for team in (1, 3, 64, 1000):
+        assert run.tree_sum_cc(iv, team) == sim.tree_sum_cc(iv, team), team
+
+
 def test_dt_and_flags(case):
     cfg, sim, run = _fresh(case)
     assert np.array_equal(sim.dt_reductions(), run.dt_reductions())

@@ -7,6 +7,11 @@ examples print residuals and errors that must behave in a known way:
     at the discretization error;
   * fosito/test/test_m_lookup_table.f90: second-order convergence of the
     table interpolation;
+  * afivo/examples/transport/test_drift_diff_2d.f90: the exact advected
+    solution on an adaptive periodic mesh (bounded error, conserved sum on a
+    frozen mesh, second-order convergence on uniform meshes), which pins the
+    transport half (fluxes, flux consistency, restriction, ghost cells,
+    prolongation, refinement);
   * src/m_streamer.f90:339-362: the four branches of koren_mlim;
 plus a manufactured solution solved with the streamer's own boundary
 conditions (grounded bottom, applied voltage on top, Neumann sides) on the
@@ -101,3 +106,67 @@ def test_manufactured_poisson_streamer_bcs():
     # converged to the discretization error, far below the potential scale
     assert errs[-1] < 1e-3 * abs(V)
     assert abs(errs[-1] - errs[-2]) < 1e-6 * abs(V)
+
+
+def test_drift_diff_known_answer():
+    """afivo/examples/transport/test_drift_diff_2d.f90 (its own parameters:
+    velocity (1, 1), no diffusion, trapezoidal steps, a regrid after every
+    step, t = 5): the transport half of the oracle -- Koren fluxes with the
+    second ghost layer, flux consistency at refinement boundaries,
+    restriction, limited ghost cells, prolongation of new boxes -- follows the
+    exact advected solution sin^4(x - t) cos^4(y - t)."""
+    r = a5ref.kat_drift_diff(0, 5.0, True)
+    assert r["time"] > 5.0 and r["steps"] > 800
+    assert r["max_lvl"] == 6                 # dr = 2 pi / 256 where the solution varies fastest
+    assert r["max_err"] < 0.02               # measured 0.0128
+    assert r["mean_err"] < 2.0e-3            # measured 1.4e-3
+    # the regrids prolong linearly (not conservatively): the sum drifts slowly
+    assert abs(r["sum_end"] - r["sum0"]) / r["sum0"] < 0.01
+
+
+def test_drift_diff_conserves_on_a_frozen_mesh():
+    """Without regrids the finite-volume update with consistent fluxes on the
+    periodic square conserves the sum of phi to rounding."""
+    r = a5ref.kat_drift_diff(0, 1.0, False)
+    assert r["max_lvl"] == 6 and r["steps"] > 150
+    assert abs(r["sum_end"] - r["sum0"]) / r["sum0"] < 1e-13
+
+
+def test_drift_diff_second_order_on_uniform_meshes():
+    """Uniform meshes of levels 3, 4, 5 to t = 1: the mean error falls by
+    about 4 per level (Koren's scheme is second order away from extrema), and
+    the initial sum approaches the integral (3 pi / 4)^2."""
+    errs = [a5ref.kat_drift_diff(lvl, 1.0, True) for lvl in (3, 4, 5)]
+    for a, b in zip(errs, errs[1:]):
+        assert a["mean_err"] / b["mean_err"] > 3.5, (a["mean_err"], b["mean_err"])
+        assert a["max_err"] / b["max_err"] > 2.2
+    assert abs(errs[-1]["sum0"] - (0.75 * math.pi) ** 2) < 1e-3
+    for r in errs:
+        assert abs(r["sum_end"] - r["sum0"]) / r["sum0"] < 1e-13
+
+
+def test_tree_sum_cc_formula():
+    """a$D_tree_sum_cc (afivo/src/m_aX_utils.f90:621-680) with one thread:
+    the oracle's value equals the plain loop over levels, leaves and cells of
+    lvl_dr^2 times the box sum (cylindrical: 2 pi r times the value)."""
+    for cfg in (config.cartesian_8mm(), config.cylindrical_16mm()):
+        sim = a5ref.Sim(cfg, n_threads=2)
+        sim.init()
+        meta, geom, levels = sim.meta(), sim.geom(), sim.levels()
+        x = sim.cc(a5ref.I_ELEC)
+        total = 0.0
+        for lvl in sorted(levels):
+            leaves = levels[lvl][1]
+            dr = cfg.dr_base * 0.5 ** (lvl - 1)
+            for id_ in leaves:
+                n = int(meta[id_, 14])
+                g = n + 2
+                tmp = 0.0
+                for j in range(1, n + 1):
+                    for i in range(1, n + 1):
+                        v = float(x[id_, i + g * j])
+                        tmp = tmp + (v * (geom[id_, 0] + (i - 0.5) * geom[id_, 3]) if cfg.coord == "cyl" else v)
+                if cfg.coord == "cyl":
+                    tmp = tmp * (2 * math.acos(-1.0))
+                total = total + dr * dr * tmp
+        assert sim.tree_sum_cc(a5ref.I_ELEC, 1) == total

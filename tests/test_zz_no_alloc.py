@@ -4,8 +4,14 @@ the time loop, or a stepping path that must not block on the allocator).
 
 Through the C ABI, two calls in a row of the allocation-free entry point must
 give exactly (bit for bit, the tolerance of the other parity tests) what two
-calls of a5g_step_batch give on identical inputs. Runs standalone in a fresh
-process as well as after the other tests."""
+calls of a5g_step_batch give on identical inputs, for FP64 members, for
+members with Monte Carlo photoionization (whose photon pass rewrites the
+shared descriptor table before the step pass) and for mixed-precision
+members; the FP64 members also match the oracle directly. Every member is
+read through its own stream right after the calls, without a wait on the
+first member: the batch is ordered before the members' later work on the
+device. Runs standalone in a fresh process as well as after the other
+tests."""
 import ctypes
 
 import numpy as np
@@ -13,14 +19,20 @@ import pytest
 
 import a5ref
 from a5_streamer_b200 import _lib, config
-from a5_streamer_b200 import device as dv
-from parity import device_from_oracle
+from parity import compare, device_from_oracle
 
 pytestmark = pytest.mark.gpu
 
 
-def _runs(cfg, sim, n):
-    return [device_from_oracle(sim, cfg) for _ in range(n)]
+def _member(cfg, sim, mixed=False):
+    run = device_from_oracle(sim, cfg)
+    if cfg.photoi_enabled:
+        dist, frac, _ = sim.photon_table()
+        run.set_photon_table(dist, frac)
+        run.set_rng_state(sim.rng_state())
+    if mixed:
+        run.set_precision(True, (0, 2, 2, 4, 2))
+    return run
 
 
 def _state(run):
@@ -35,26 +47,48 @@ def _call(name, runs, dts):
     _lib.call(name, arr, len(runs), d.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
 
 
-@pytest.mark.parametrize("make_cfg", [config.cartesian_8mm, config.cylindrical_16mm])
-def test_static_batch_matches_batch(make_cfg):
-    cfg = make_cfg()
-    sim = a5ref.Sim(cfg, n_threads=2)
-    sim.init()
-    sim.advance(True)
-    dt = sim.get_max_dt()
-    a = _runs(cfg, sim, 3)
-    b = _runs(cfg, sim, 3)
-    dts = [dt, 0.5 * dt, 0.25 * dt]
-    for _ in range(2):
+def _oracles(cfgs):
+    sims = []
+    for cfg in cfgs:
+        sim = a5ref.Sim(cfg, n_threads=2)
+        sim.init()
+        sim.advance(True)
+        sims.append(sim)
+    return sims
+
+
+@pytest.mark.parametrize("kind", ["fp64", "photoionization", "mixed"])
+def test_static_batch_matches_batch(kind):
+    if kind == "photoionization":
+        cfgs = [config.cylindrical_16mm(photoi=True, photoi_team=512),
+                config.cylindrical_16mm(photoi=True, photoi_team=2000, rng_seed=(1, 2, 3, 4)),
+                config.cylindrical_16mm()]
+    else:
+        cfgs = [config.cartesian_8mm(), config.cylindrical_16mm(), config.cartesian_8mm()]
+    sims = _oracles(cfgs)
+    mixed = kind == "mixed"
+    a = [_member(c, s, mixed and k != 1) for k, (c, s) in enumerate(zip(cfgs, sims))]
+    b = [_member(c, s, mixed and k != 1) for k, (c, s) in enumerate(zip(cfgs, sims))]
+    base = [s.get_max_dt() for s in sims]
+    for step in range(2):
+        dts = [dt * (1.0 - 0.25 * step) for dt in base]
         _call("a5g_step_batch", a, dts)
         _call("a5g_step_batch_static", b, dts)
-    a[0].sync()
-    b[0].sync()
-    for ra, rb in zip(a, b):
+        if not mixed:
+            for s, dt in zip(sims, dts):
+                s.step(dt)
+    # no sync of member 0 first: each read below is queued on the member's
+    # own stream, which the batch call ordered after the batch
+    for ra, rb in zip(a[::-1], b[::-1]):
         for xa, xb in zip(_state(ra), _state(rb)):
             assert np.array_equal(xa, xb)
+    if not mixed:
+        for s, rb in zip(sims, b):
+            compare(s, rb, where=f"static batch ({kind})")
+            if s.cfg.photoi_enabled:
+                assert np.array_equal(s.rng_state(), rb.rng_state())
     # the result is a real step: it moved the densities
-    assert not np.array_equal(_state(a[0])[0], sim.cc(0))
+    assert not np.array_equal(_state(b[0])[0], sims[0].cc(0) if mixed else _oracles(cfgs[:1])[0].cc(0))
 
 
 def test_static_batch_rejects_oversize():
