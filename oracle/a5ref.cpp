@@ -2056,6 +2056,40 @@ static void apply_threads(const a5ref_params &p) {
 #endif
 }
 
+// a$D_reduction_loc with reduce_max (afivo/src/m_aX_utils.f90:499-555):
+// leaves level by level in list order; a box result replaces the running one
+// when max(tmp, running) differs from the running value. The reference's
+// location is undefined when nothing replaces the initial value; here it is
+// id -1 then.
+template <class F>
+static double reduction_max_loc(Tree &t, F box_subr, double init, int &id_out, int ix_out[2]) {
+  double my_val = init;
+  int my_id = -1, my_ix[2] = {-1, -1};
+  for (int lvl = t.min_lvl; lvl <= t.max_lvl; lvl++)
+    for (int id : t.L(lvl).leaves) {
+      double tmp;
+      int tix[2] = {-1, -1};
+      box_subr(t.boxes[id], tmp, tix);
+      const double nv = std::max(tmp, my_val);
+      if (std::fabs(nv - my_val) > 0) {
+        my_id = id;
+        my_ix[0] = tix[0];
+        my_ix[1] = tix[1];
+        my_val = tmp;
+      }
+    }
+  id_out = -1;
+  ix_out[0] = ix_out[1] = -1;
+  const double nv = std::max(my_val, init);
+  if (std::fabs(nv - init) > 0) {
+    id_out = my_id;
+    ix_out[0] = my_ix[0];
+    ix_out[1] = my_ix[1];
+    return my_val;
+  }
+  return init;
+}
+
 extern "C" {
 
 a5ref_sim *a5ref_create(const a5ref_params *p) {
@@ -2168,6 +2202,192 @@ void a5ref_op_fld_from_pot(a5ref_sim *h) {
 // a$D_tree_max_cc / _min_cc / _sum_cc, afivo/src/m_aX_utils.f90:559-680;
 // the sum as a team of `team` OpenMP threads forms it (team 1: the loop order)
 long long a5ref_photons_created(a5ref_sim *h) { return h->s.n_photons; }
+
+// ---------------------------------------------------------------------------
+// Streamer diagnostics of the axisymmetric program, one thread.
+
+// get_streamer_properties (src/streamer_cyl.f90:682-828): the 39 values in
+// the reference's order, with box_maxfld_z / box_maxfld_r (maxloc: first
+// maximum in column-major order), box_fld_maxr / box_fld_maxz (:835-903) and
+// the alpha column read for both alpha and mu (:708-709, :718-719). The
+// boundary stop (:721-723) is not taken.
+void a5ref_streamer_properties(a5ref_sim *h, double *props) {
+  Sim &s = h->s;
+  Tree &t = s.tree;
+  const double L = s.p.domain_len_z, V = s.applied_voltage;
+  auto maxfld = [](bool radial) {
+    return [radial](Box &b, double &val, int ix[2]) {
+      const int nc = b.n_cell;
+      double best = 0;
+      bool first = true;
+      for (int j = 1; j <= nc; j++)
+        for (int i = 1; i <= nc; i++) {
+          const double a = radial ? std::fabs(b.Fx(i, j, F_FLD) + b.Fx(i + 1, j, F_FLD))
+                                  : std::fabs(b.Fy(i, j, F_FLD) + b.Fy(i, j + 1, F_FLD));
+          if (first || a > best) {
+            best = a;
+            ix[0] = i;
+            ix[1] = j;
+            first = false;
+          }
+        }
+      val = radial ? 0.5 * std::fabs(b.Fx(ix[0], ix[1], F_FLD) + b.Fx(ix[0] + 1, ix[1], F_FLD))
+                   : 0.5 * std::fabs(b.Fy(ix[0], ix[1], F_FLD) + b.Fy(ix[0], ix[1] + 1, F_FLD));
+    };
+  };
+  auto fld_max_pos = [](double thr, int axis) {
+    return [thr, axis](Box &b, double &val, int ix[2]) {
+      val = 0;
+      const int nc = b.n_cell;
+      for (int j = 1; j <= nc; j++)
+        for (int i = 1; i <= nc; i++)
+          if (b.c(i, j, I_FLD) > thr) {
+            const double rz[2] = {b.r_min[0] + (i - 0.5) * b.dr, b.r_min[1] + (j - 0.5) * b.dr};
+            if (rz[axis] > val) {
+              val = rz[axis];
+              ix[0] = i;
+              ix[1] = j;
+            }
+          }
+    };
+  };
+  int ip = 0;
+  props[ip++] = s.p.applied_fld;  // ST_get_fld(ST_time), no field modulation
+  int ez_id, ez_ix[2], er_id, er_ix[2];
+  const double ez_max = reduction_max_loc(t, maxfld(false), -1.0e99, ez_id, ez_ix);
+  props[ip++] = ez_max;
+  props[ip++] = reduction_max_loc(t, maxfld(true), -1.0e99, er_id, er_ix);
+  double rz[2];
+  {
+    const Box &b = t.boxes[er_id];
+    rz[0] = b.r_min[0] + (er_ix[0] - 0.5) * b.dr;
+    rz[1] = b.r_min[1] + (er_ix[1] - 0.5) * b.dr;
+  }
+  props[ip++] = rz[0];
+  props[ip++] = rz[1];
+  const double z_head = rz[1];
+  const double er_norm = t.boxes[er_id].c(er_ix[0], er_ix[1], I_FLD);
+  props[ip++] = er_norm;
+  for (double e : {ez_max, er_norm}) {
+    const double alpha = lt_get_col(s.td, I_ALPHA, e);
+    const double mu = lt_get_col(s.td, I_ALPHA, e);
+    props[ip++] = alpha;
+    props[ip++] = alpha * mu * e;
+  }
+  int id, ix[2];
+  {
+    const double rr[2] = {0.0, rz[1]};
+    get_loc(t, rr, t.lvls_max, id, ix);
+  }
+  props[ip++] = t.boxes[id].c(ix[0], ix[1], I_ELEC);
+  const double phi_head = t.boxes[id].c(ix[0], ix[1], I_PHI);
+  props[ip++] = phi_head - (rz[1] / L) * V;
+  {
+    const Box &b = t.boxes[ez_id];
+    rz[0] = b.r_min[0] + (ez_ix[0] - 0.5) * b.dr;
+    rz[1] = b.r_min[1] + (ez_ix[1] - 0.5) * b.dr;
+  }
+  props[ip++] = rz[1];
+  for (double dz : {2.0e-3, 4.0e-3}) {
+    const double rr[2] = {0.0, rz[1] + dz};
+    int lid, lix[2];
+    get_loc(t, rr, t.lvls_max, lid, lix);
+    props[ip++] = lid > 0 ? phi_head - t.boxes[lid].c(lix[0], lix[1], I_PHI) : 0.0;
+  }
+  for (int i = 4; i <= 14; i += 2) {
+    const double thr = i * 1e6;
+    int lid, lix[2];
+    props[ip++] = reduction_max_loc(t, fld_max_pos(thr, 0), 0.0, lid, lix);
+    props[ip++] = lid > 0 ? phi_head - t.boxes[lid].c(lix[0], lix[1], I_PHI) : 0.0;
+    props[ip++] = reduction_max_loc(t, fld_max_pos(thr, 1), 0.0, lid, lix) - z_head;
+    props[ip++] = lid > 0 ? phi_head - t.boxes[lid].c(lix[0], lix[1], I_PHI) : 0.0;
+  }
+}
+
+// The arrays a$D_write_vtk (afivo/src/m_aX_io.f90:20-207, 2D) builds for a
+// file of the leaves of levels 1..max_lvl: node coordinates (2 per node,
+// written by m_vtk.f90 as Float32 x 3), connectivity, offsets, cell types and
+// the values of n_iv cell variables ivs plus, for n_if face variables ifs, the
+// cell means of fx and fy. Any output may be NULL; returns the cell count.
+int a5ref_vtk_arrays(a5ref_sim *h, int n_iv, const int *ivs, int n_if, const int *ifs,
+                     double *coords, int *connects, int *offsets, int *types, double *vals) {
+  Tree &t = h->s.tree;
+  const int bc = t.n_cell, bn = t.n_cell + 1;
+  const int nodes_per_box = bn * bn, cells_per_box = bc * bc;
+  int n_grids = 0;
+  for (int lvl = 1; lvl <= t.max_lvl; lvl++) n_grids += (int)t.L(lvl).leaves.size();
+  const int n_cells = cells_per_box * n_grids;
+  int ig = 0;
+  for (int lvl = 1; lvl <= t.max_lvl; lvl++)
+    for (int id : t.L(lvl).leaves) {
+      Box &b = t.boxes[id];
+      ig++;
+      const int cell_ix = (ig - 1) * cells_per_box, node_ix = (ig - 1) * nodes_per_box;
+      for (int j = 1; j <= bn; j++)
+        for (int i = 1; i <= bn; i++) {
+          const int n_ix = 2 * (node_ix + (j - 1) * bn + i);  // 1-based pair end
+          if (coords) {
+            coords[n_ix - 2] = b.r_min[0] + (i - 1) * b.dr;
+            coords[n_ix - 1] = b.r_min[1] + (j - 1) * b.dr;
+          }
+        }
+      for (int j = 1; j <= bc; j++)
+        for (int i = 1; i <= bc; i++) {
+          const int n_ix = node_ix + (j - 1) * bn + i - 1;
+          const int c_ix = cell_ix + (j - 1) * bc + i;  // 1-based
+          if (vals) {
+            for (int v = 0; v < n_iv; v++) vals[(size_t)v * n_cells + (c_ix - 1)] = b.c(i, j, ivs[v]);
+            for (int f = 0; f < n_if; f++) {
+              vals[(size_t)(n_iv + 2 * f) * n_cells + (c_ix - 1)] =
+                  0.5 * (b.Fx(i, j, ifs[f]) + b.Fx(i + 1, j, ifs[f]));
+              vals[(size_t)(n_iv + 2 * f + 1) * n_cells + (c_ix - 1)] =
+                  0.5 * (b.Fy(i, j, ifs[f]) + b.Fy(i, j + 1, ifs[f]));
+            }
+          }
+          if (offsets) offsets[c_ix - 1] = 4 * c_ix;
+          if (types) types[c_ix - 1] = 8;  // VTK pixel
+          if (connects) {
+            const int q[4] = {n_ix, n_ix + 1, n_ix + bn, n_ix + bn + 1};
+            for (int k = 0; k < 4; k++) connects[4 * (c_ix - 1) + k] = q[k];
+          }
+        }
+    }
+  return n_cells;
+}
+
+// get_cc_axis(tree, [i_elec, i_pion], [f_fld, f_elec]) (src/streamer_cyl.f90:
+// 905-956): per axis cell z, n_e, n_i and the face averages of the field and
+// the electron flux, box by box from z = 0 up. out: 5 x n (row-major by
+// quantity), capacity cap cells; returns n (call with out NULL to size).
+int a5ref_cc_axis(a5ref_sim *h, double *out, int cap) {
+  Tree &t = h->s.tree;
+  const int nc = t.n_cell;
+  std::vector<double> z_l, e_l, i_l, f_l, x_l;
+  double z = 0;
+  while (true) {
+    const double rr[2] = {0.0, z};
+    int id, ix[2];
+    get_loc(t, rr, t.lvls_max, id, ix);
+    if (id == -1) break;
+    Box &b = t.boxes[id];
+    const double box_z = b.r_min[1], box_dz = b.dr;
+    for (int j = 1; j <= nc; j++) {
+      z_l.push_back(box_z + (j - 0.5) * box_dz);
+      e_l.push_back(b.c(1, j, I_ELEC));
+      i_l.push_back(b.c(1, j, I_PION));
+      f_l.push_back(0.5 * (b.Fy(1, j, F_FLD) + b.Fy(1, j + 1, F_FLD)));
+      x_l.push_back(0.5 * (b.Fy(1, j, F_ELEC) + b.Fy(1, j + 1, F_ELEC)));
+    }
+    z = box_z + (nc + 1) * box_dz;
+  }
+  const int n = (int)z_l.size();
+  if (out && n <= cap) {
+    const std::vector<double> *rows[5] = {&z_l, &e_l, &i_l, &f_l, &x_l};
+    for (int r = 0; r < 5; r++)
+      for (int k = 0; k < n; k++) out[(size_t)r * n + k] = (*rows[r])[k];
+  }
+  return n;
+}
 double a5ref_tree_max_cc(a5ref_sim *h, int iv) { return tree_max_cc(h->s.tree, iv); }
 double a5ref_tree_min_cc(a5ref_sim *h, int iv) { return tree_min_cc(h->s.tree, iv); }
 double a5ref_tree_sum_cc(a5ref_sim *h, int iv, int team) {

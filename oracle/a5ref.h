@@ -128,6 +128,18 @@ void a5ref_op_fld_from_pot(a5ref_sim *s);
 void a5ref_op_vcycle(a5ref_sim *s, int max_lvl, int set_residual);
 /* Photons created by the last photoionization call. */
 long long a5ref_photons_created(a5ref_sim *s);
+/* get_streamer_properties (src/streamer_cyl.f90:682-828): 39 values. */
+void a5ref_streamer_properties(a5ref_sim *s, double *props39);
+/* get_cc_axis (src/streamer_cyl.f90:905-956): 5 x n values (z, n_e, n_i,
+ * axial field, axial electron flux); returns n. */
+int a5ref_cc_axis(a5ref_sim *s, double *out, int cap);
+/* The arrays of a$D_write_vtk (afivo/src/m_aX_io.f90:20-207) for the leaves
+ * of levels 1..max_lvl: node coordinates (x, y per node), connectivity,
+ * offsets, cell types, and per cell the n_iv variables ivs and the fx / fy
+ * cell means of the n_if face variables ifs (variable-major). Outputs may be
+ * NULL; returns the number of cells. */
+int a5ref_vtk_arrays(a5ref_sim *s, int n_iv, const int *ivs, int n_if, const int *ifs,
+                     double *coords, int *connects, int *offsets, int *types, double *vals);
 double a5ref_tree_max_cc(a5ref_sim *s, int iv);
 double a5ref_tree_min_cc(a5ref_sim *s, int iv);
 double a5ref_tree_sum_cc(a5ref_sim *s, int iv, int team);

@@ -88,6 +88,9 @@ def lib() -> ctypes.CDLL:
             "a5ref_tree_max_cc": (D, [P, I]), "a5ref_tree_min_cc": (D, [P, I]),
             "a5ref_tree_sum_cc": (D, [P, I, I]),
             "a5ref_photons_created": (ctypes.c_longlong, [P]),
+            "a5ref_streamer_properties": (V, [P, pd]),
+            "a5ref_cc_axis": (I, [P, pd, I]),
+            "a5ref_vtk_arrays": (I, [P, I, pi, I, pi, pd, pi, pi, pi, pd]),
             "a5ref_op_regrid": (I, [P, pi, pi]),
             "a5ref_max_id": (I, [P]), "a5ref_max_lvl": (I, [P]), "a5ref_min_lvl": (I, [P]),
             "a5ref_n_leaf_cells": (I, [P]), "a5ref_n_cells_all": (I, [P]),
@@ -248,6 +251,39 @@ class Sim:
 
     def photons_created(self) -> int:
         return int(lib().a5ref_photons_created(self.h))
+
+    def streamer_properties(self) -> np.ndarray:
+        """get_streamer_properties restated in the oracle (39 values)."""
+        out = np.zeros(39)
+        lib().a5ref_streamer_properties(self.h, _dp(out))
+        return out
+
+    def vtk_arrays(self, ivs, ifs=()):
+        """a$D_write_vtk's arrays restated in the oracle: dict of coords
+        (n_nodes x 2), connectivity, offsets, types and the values (one row
+        per cell variable, then fx and fy means per face variable)."""
+        iv = np.ascontiguousarray(ivs, dtype=np.int32)
+        fv = np.ascontiguousarray(ifs if len(ifs) else [0], dtype=np.int32)
+        n = lib().a5ref_vtk_arrays(self.h, len(ivs), _ip(iv), len(ifs), _ip(fv), None, None, None,
+                                   None, None)
+        nodes = (n // (self.nc * self.nc)) * (self.nc + 1) ** 2
+        coords = np.zeros(2 * nodes)
+        con = np.zeros(4 * n, dtype=np.int32)
+        off = np.zeros(n, dtype=np.int32)
+        ty = np.zeros(n, dtype=np.int32)
+        vals = np.zeros((len(ivs) + 2 * len(ifs), n))
+        lib().a5ref_vtk_arrays(self.h, len(ivs), _ip(iv), len(ifs), _ip(fv), _dp(coords), _ip(con),
+                               _ip(off), _ip(ty), _dp(vals))
+        return {"coords": coords.reshape(-1, 2), "connectivity": con, "offsets": off, "types": ty,
+                "values": vals}
+
+    def cc_axis(self) -> np.ndarray:
+        """get_cc_axis restated in the oracle: rows z, n_e, n_i, axial field,
+        axial electron flux."""
+        n = lib().a5ref_cc_axis(self.h, None, 0)
+        out = np.zeros(5 * max(n, 1))
+        lib().a5ref_cc_axis(self.h, _dp(out), n)
+        return out[:5 * n].reshape(5, n)
 
     def ref_flags(self) -> np.ndarray:
         out = np.zeros(self.max_id + 1, dtype=np.int32)

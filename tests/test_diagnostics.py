@@ -75,3 +75,31 @@ def test_get_loc_and_axis(state):
         bid, (i, j) = tv.get_loc((1e-12, z[k]))
         n = tv.nc(bid)
         assert i == 1 and ax[1, k] == sim.cc(0)[bid, 1 + (n + 2) * j]
+
+
+@pytest.mark.parametrize("fld", [2.0e6, 5.0e6])
+def test_properties_and_axis_match_the_oracle_restatement(fld):
+    """diagnostics.streamer_properties / axis_data against the oracle's own
+    restatement of get_streamer_properties and get_cc_axis
+    (src/streamer_cyl.f90:682-956, written from the Fortran statement by
+    statement: a$D_reduction_loc's replacement rule, maxloc's first maximum,
+    the alpha column read for mu), to the bit. At 5 MV/m the field exceeds
+    the 4..8 MV/m thresholds, so the radial and axial extents and their
+    potential drops are exercised too."""
+    cfg = config.cylindrical_16mm(applied_fld=fld, lvls_max=8)
+    sim = a5ref.Sim(cfg, n_threads=4)
+    sim.init()
+    for _ in range(6):
+        sim.advance(True)
+    tv = diagnostics.TreeView(sim.meta(), sim.geom(), sim.levels(), cfg.lvls_max)
+    names, props = diagnostics.streamer_properties(
+        tv, {"fld": sim.cc(5), "e": sim.cc(0), "phi": sim.cc(4)},
+        {"fx_fld": sim.fc(0, 1), "fy_fld": sim.fc(1, 1)}, sim.table(), cfg.applied_fld,
+        cfg.applied_voltage, cfg.domain_len_z)
+    ref = sim.streamer_properties()
+    bad = [(n, a, b) for n, a, b in zip(names, props, ref) if not a == b]
+    assert not bad, bad
+    if fld > 4e6:
+        assert props[names.index("r_max(4e6)")] > 0 and props[names.index("dphi_r(4e6)")] != 0
+    ax = diagnostics.axis_data(tv, [sim.cc(0), sim.cc(1)], [sim.fc(1, 1), sim.fc(1, 0)])
+    assert np.array_equal(ax, sim.cc_axis())

@@ -57,3 +57,30 @@ def test_face_means_and_axis_profile():
     assert my[k] == 0.5 * (fy[b, (i - 1) + nc * (j - 1)] + fy[b, (i - 1) + nc * j])
     z, f, n = output.axis_profile(sim.cc(5), sim.cc(0), meta, geom, levels, cfg)
     assert np.all(np.diff(z) >= 0) and len(z) == len(f) == len(n) > 0
+
+
+def test_vtk_matches_the_reference_layout(tmp_path):
+    """The file output.write_vtk writes against the oracle's restatement of
+    the arrays a$D_write_vtk builds (afivo/src/m_aX_io.f90:20-207): the same
+    node coordinates (stored as Float32, as m_vtk.f90 writes them), the same
+    pixel connectivity, offsets and types, and the same cell values and face
+    means in the same order, to the bit."""
+    cfg = config.cylindrical_16mm()
+    sim = a5ref.Sim(cfg, n_threads=2)
+    sim.init()
+    for _ in range(2):
+        sim.advance(True)
+    meta, geom, levels = sim.meta(), sim.geom(), sim.levels()
+    mesh = output.leaf_mesh(meta, geom, levels)
+    mx, my = output.face_means(mesh, sim.fc(0, 1), sim.fc(1, 1))
+    path = output.write_vtk(str(tmp_path / "ref"), meta, geom, levels,
+                            {"n_e": sim.cc(0), "phi": sim.cc(4), "fld_x": mx, "fld_y": my})
+    d = output.read_vtk(path)
+    ref = sim.vtk_arrays([a5ref.I_ELEC, a5ref.I_PHI], [a5ref.F_FLD])
+    assert np.array_equal(d["Points"][:, :2], ref["coords"].astype(np.float32))
+    assert np.all(d["Points"][:, 2] == 0)
+    assert np.array_equal(d["connectivity"], ref["connectivity"])
+    assert np.array_equal(d["offsets"], ref["offsets"])
+    assert np.array_equal(d["types"], ref["types"])
+    for k, name in enumerate(("n_e", "phi", "fld_x", "fld_y")):
+        assert np.array_equal(d[name], ref["values"][k]), name
