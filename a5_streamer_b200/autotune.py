@@ -189,11 +189,42 @@ def tune_schedule(sim, n_steps: int = 200, tol_max_E: float = 1e-4, tol_head_z: 
             "table": table}
 
 
+def cta_mapping(cells: Sequence[int], total: int, power: float) -> List[int]:
+    """Blocks per run of a batch (the box-to-block mapping): one each, and
+    the remaining total - n blocks dealt in proportion to cells**power by
+    largest remainders (power 0: evenly; 1: in proportion to the tree
+    size). Never more than total blocks in all."""
+    n = len(cells)
+    out = [1] * n
+    spare = total - n
+    if spare <= 0 or power is None:
+        return out
+    w = np.asarray([float(c) ** power for c in cells])
+    share = spare * w / w.sum()
+    base = np.floor(share).astype(int)
+    rest = spare - int(base.sum())
+    order = np.argsort(-(share - base), kind="stable")
+    base[order[:rest]] += 1
+    return [1 + int(b) for b in base]
+
+
+def apply_mapping(sims, total: int, power) -> List[int]:
+    """Set each simulation's blocks per launch from its current leaf cells."""
+    if power is None:
+        return [1] * len(sims)
+    m = cta_mapping([s.device.n_leaf_cells() for s in sims], total, power)
+    for s, k in zip(sims, m):
+        s.device.set_ctas(k)
+    return m
+
+
 def batch_observables(cfgs, schedule=None, use_graph: bool = True, n_threads: int = 8,
-                      groups: int = 1):
-    """Run ``cfgs`` from their initial conditions to their end times as one
-    device-driven batch (FP64, or mixed with ``schedule``; ``groups``
-    pipelined batches). Returns the per-run head observables, the batch
+                      groups: int = 1, mapping=None, max_blocks: int = 1 << 30):
+    """Run ``cfgs`` from their initial conditions to their end times (or
+    ``max_blocks`` blocks) as one device-driven batch (FP64, or mixed with
+    ``schedule``; ``groups`` pipelined batches). ``mapping``: None for one
+    block per run, else (total blocks, power) of ``cta_mapping`` applied to
+    the initial trees. Returns the per-run head observables, the batch
     counters (blocks, device ms, host ms, cell updates) and the wall time (s)
     of the batched run."""
     from .streamer import Simulation, run_batch
@@ -203,10 +234,12 @@ def batch_observables(cfgs, schedule=None, use_graph: bool = True, n_threads: in
             if schedule is not None:
                 s.device.set_precision(True, schedule)
             s.init()
+        if mapping is not None:
+            apply_mapping(sims, mapping[0], mapping[1])
         import time
         t0 = time.perf_counter()
         counters = run_batch(sims, [c.end_time for c in cfgs], use_graph=use_graph,
-                             n_threads=n_threads, groups=groups)
+                             n_threads=n_threads, groups=groups, max_blocks=max_blocks)
         wall = time.perf_counter() - t0
         heads = []
         for s, c in zip(sims, cfgs):
@@ -242,3 +275,23 @@ def tune_batch_schedule(cfgs, candidates: Sequence[Schedule], tol_max_E: float =
             break
     return {"schedule": tuple(tried[-1]["schedule"]), "errors": tried[-1], "tried": tried,
             "bounds": {"max_E_rel": tol_max_E, "head_z_rel": tol_head_z}}
+
+
+def tune_batch_mapping(cfgs, schedule=None, total: int = 148,
+                       powers: Sequence[Optional[float]] = (None, 0.0, 0.5, 1.0),
+                       n_blocks: int = 4, n_threads: int = 8) -> Dict:
+    """The box-to-block mapping of a batch, chosen by measurement: for each
+    candidate (None: one block per run; else cta_mapping's power) the first
+    ``n_blocks`` blocks of the batched run from the initial conditions are
+    timed on the device, and the candidate with the highest leaf-cell
+    updates per device second wins. The mapping changes only which threads
+    do which work, so every candidate gives the same results."""
+    table = []
+    for pw in powers:
+        _, (nb, gpu_ms, _, cu), _ = batch_observables(
+            cfgs, schedule, n_threads=n_threads, mapping=None if pw is None else (total, pw),
+            max_blocks=n_blocks)
+        table.append({"power": pw, "blocks": nb, "device_ms": gpu_ms,
+                      "value": cu / (gpu_ms / 1e3) if gpu_ms > 0 else 0.0})
+    best = max(table, key=lambda r: r["value"])
+    return {"power": best["power"], "total": total, "table": table}

@@ -3042,6 +3042,18 @@ __global__ void __launch_bounds__(NTHR, 1) a5g_run_kernel_slots(const BatchSlot 
   run_op(sR, op);
 }
 
+// A device-driven batch whose members take several blocks each (the
+// members' a5g_set_ctas): block b runs operation ops[k] of run k as rank r of
+// its run's group of m blocks, gmap[3 b ..] = {k, r, m}; one cooperative
+// launch holds every member's group, each synchronising on its own barrier.
+__global__ void __launch_bounds__(NTHR, 1) a5g_batch_map_kernel(const RunDev *const *runs, const Op *ops,
+                                                                const int *gmap) {
+  __shared__ RunDev sR;
+  const int k = gmap[3 * blockIdx.x], r = gmap[3 * blockIdx.x + 1], m = gmap[3 * blockIdx.x + 2];
+  stage_run(runs[k], sR, m, r);
+  run_op(sR, ops[k]);
+}
+
 // Descriptors of one launch of a5g_step_batch_static passed by value (as
 // kernel parameters, at most SLOT_FILL per launch; 96 x 40 bytes stays under
 // the classic 4 KiB parameter limit) and written to the fixed table, so that
@@ -3529,11 +3541,11 @@ static size_t dyn_smem_limit() {
     int optin = 0;
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     size_t stat = 0;
-    constexpr int NF = 5;
+    constexpr int NF = 6;
     cudaFuncAttributes fa[NF];
     const void *fns[NF] = {(const void *)a5g_run_kernel, (const void *)a5g_step_kernel,
                            (const void *)a5g_run_kernel_slots, (const void *)a5g_photon_kernel,
-                           (const void *)a5g_step_mixed_kernel};
+                           (const void *)a5g_step_mixed_kernel, (const void *)a5g_batch_map_kernel};
     for (int k = 0; k < NF; k++)
       if (cudaFuncGetAttributes(&fa[k], fns[k]) == cudaSuccess)
         stat = std::max(stat, fa[k].sharedSizeBytes);
@@ -4500,8 +4512,8 @@ static int max_coresident_ctas() {
   if (cudaGetDevice(&dev) != cudaSuccess) return 0;
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
   int best = INT_MAX;
-  const void *fns[3] = {(const void *)a5g_run_kernel, (const void *)a5g_step_kernel,
-                        (const void *)a5g_step_mixed_kernel};
+  const void *fns[4] = {(const void *)a5g_run_kernel, (const void *)a5g_step_kernel,
+                        (const void *)a5g_step_mixed_kernel, (const void *)a5g_batch_map_kernel};
   for (const void *fn : fns) {
     int nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, NTHR, 0) != cudaSuccess) return 0;
@@ -4736,6 +4748,12 @@ struct a5g_batch {
   double *h_state = nullptr;  // pinned, 5 per run (a5g_batch_gather_kernel)
   double *d_state = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // block-to-run map when some member takes several blocks (3 ints per
+  // block, A5G_MAX_CTAS blocks at most): the block-dt and step launches are
+  // then one cooperative launch of n_blocks blocks
+  int *d_gmap = nullptr;
+  int n_blocks = 0;
+  bool mapped = false;
 };
 
 static void batch_drop_graph(a5g_batch *b) {
@@ -4772,7 +4790,46 @@ static int batch_build_ops(a5g_batch *b) {
   b->dyn = dyn_smem_limit();
   CK(cudaMemcpy(b->d_rp, rp.data(), n * sizeof(void *), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(b->d_ops, ops.data(), 3 * n * sizeof(Op), cudaMemcpyHostToDevice));
+  // box-to-block mapping: each member's group of c->n_cta blocks
+  b->mapped = false;
+  int total = 0;
+  for (int k = 0; k < n; k++) {
+    total += b->ctxs[k]->n_cta;
+    if (b->ctxs[k]->n_cta > 1) b->mapped = true;
+  }
+  if (b->mapped) {
+    const int lim = max_coresident_ctas();
+    if (total > lim)
+      return fail(A5G_EINVAL, "batch members take " + std::to_string(total) + " blocks; at most " +
+                                  std::to_string(lim) + " can be co-resident");
+    std::vector<int> gmap(3 * (size_t)total);
+    int blk = 0;
+    for (int k = 0; k < n; k++)
+      for (int r = 0; r < b->ctxs[k]->n_cta; r++, blk++) {
+        gmap[3 * blk] = k;
+        gmap[3 * blk + 1] = r;
+        gmap[3 * blk + 2] = b->ctxs[k]->n_cta;
+      }
+    CK(cudaMemcpy(b->d_gmap, gmap.data(), gmap.size() * sizeof(int), cudaMemcpyHostToDevice));
+    b->n_blocks = total;
+  }
   batch_drop_graph(b);
+  return A5G_OK;
+}
+
+// One launch of the batch's block-dt or step operations (ops: n entries).
+static int batch_launch_ops(a5g_batch *b, const Op *ops) {
+  const int n = (int)b->ctxs.size();
+  if (b->mapped) {
+    const RunDev *const *runs = b->d_rp;
+    const int *gmap = b->d_gmap;
+    void *args[] = {(void *)&runs, (void *)&ops, (void *)&gmap};
+    CK(cudaLaunchCooperativeKernel((const void *)a5g_batch_map_kernel, dim3(b->n_blocks), dim3(NTHR), args,
+                                   b->dyn, b->stream));
+    return A5G_OK;
+  }
+  a5g_run_kernel<<<n, NTHR, b->dyn, b->stream>>>(nullptr, Op{}, b->d_rp, ops);
+  CK(cudaGetLastError());
   return A5G_OK;
 }
 
@@ -4781,8 +4838,8 @@ static int batch_build_ops(a5g_batch *b) {
 // valid while the members' trees change between blocks.
 static int batch_enqueue(a5g_batch *b, int num_steps) {
   const int n = (int)b->ctxs.size();
-  a5g_run_kernel<<<n, NTHR, b->dyn, b->stream>>>(nullptr, Op{}, b->d_rp, b->d_ops);
-  CK(cudaGetLastError());
+  int r = batch_launch_ops(b, b->d_ops);
+  if (r) return r;
   for (int s = 0; s < num_steps; s++) {
     if (b->any_ph) {
       a5g_run_kernel<<<n, NTHR, b->dyn, b->stream>>>(nullptr, Op{}, b->d_rp, b->d_ops + n);
@@ -4792,8 +4849,7 @@ static int batch_enqueue(a5g_batch *b, int num_steps) {
                                                                      (int)b->ph_smem);
       CK(cudaGetLastError());
     }
-    a5g_run_kernel<<<n, NTHR, b->dyn, b->stream>>>(nullptr, Op{}, b->d_rp, b->d_ops + 2 * n);
-    CK(cudaGetLastError());
+    if ((r = batch_launch_ops(b, b->d_ops + 2 * n))) return r;
   }
   return A5G_OK;
 }
@@ -4819,6 +4875,7 @@ int a5g_batch_create(a5g_ctx **ctxs, int n, a5g_batch **out) {
       cudaMalloc(&b->d_ops, 3 * n * sizeof(Op)) != cudaSuccess ||
       cudaMallocHost(&b->h_state, 5 * n * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&b->d_state, 5 * n * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&b->d_gmap, 3 * (size_t)A5G_MAX_CTAS * sizeof(int)) != cudaSuccess ||
       cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess) {
     a5g_batch_destroy(b);
     return fail(A5G_ENOMEM, "cannot allocate the batch");
@@ -4840,6 +4897,7 @@ int a5g_batch_destroy(a5g_batch *b) {
   cudaFree(b->d_ops);
   if (b->h_state) cudaFreeHost(b->h_state);
   cudaFree(b->d_state);
+  cudaFree(b->d_gmap);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
   if (b->stream) cudaStreamDestroy(b->stream);

@@ -283,11 +283,16 @@ int a5g_step_batch_static(a5g_ctx **ctxs, int n, const double *dts);
  * and replayed. The reference has no counterpart (it runs one tree per
  * process); it replaces a5g_get_max_dt + a5g_step per run.
  *  a5g_batch_begin: each run's current time and end time; also picks up
- *    changed precision settings;
+ *    changed precision and block settings;
  *  a5g_batch_block: one block; returns each run's dt of the block, its time
  *    after it, whether it stepped, and the block's device time (ms). The
  *    members' own streams are synchronised first (their regrids and uploads
  *    come before the block). */
+/* Box-to-block mapping: a member set to n_cta > 1 blocks (a5g_set_ctas)
+ * takes that many blocks of the batch's launches, as its own group with its
+ * own grid barrier; when any member does, the block-dt and step launches are
+ * single cooperative launches of all members' blocks (at most the blocks the
+ * device holds at once). Results do not depend on the mapping. */
 typedef struct a5g_batch a5g_batch;
 int a5g_batch_create(a5g_ctx **ctxs, int n, a5g_batch **out);
 int a5g_batch_destroy(a5g_batch *b);

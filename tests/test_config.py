@@ -82,3 +82,14 @@ def test_batch_runs_generator():
         assert all(0 < v < 2147483579 for v in c.rng_seed[:3])
     assert len({c.rng_seed for c in a}) == 64
     assert len({round(c.domain_len[1], 9) for c in a}) == 64
+
+
+def test_cta_mapping_deals_every_block_once():
+    from a5_streamer_b200.autotune import cta_mapping
+    for cells, total, power in (([100, 200, 50, 5000], 148, 1.0), ([100] * 64, 148, 0.0),
+                                ([3000, 10, 10], 148, 0.5), ([5] * 200, 148, 1.0)):
+        m = cta_mapping(cells, total, power)
+        assert len(m) == len(cells) and min(m) >= 1
+        assert sum(m) == max(total, len(cells))
+    m = cta_mapping([100, 200, 50, 5000], 148, 1.0)
+    assert m[3] == max(m) and m[2] == min(m)

@@ -75,3 +75,25 @@ def test_batch_finished_runs_stay_put():
     ref.run(cfgs[0].end_time)
     _same(sims[0], ref, "short member")
     assert sims[1].time > cfgs[1].end_time
+
+
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_batch_with_blocks_per_run_equals_single_runs(use_graph):
+    """Box-to-block mapping: members take 1, 3, 2, 4 and 1 blocks of one
+    cooperative launch (a5g_set_ctas on each member), each group with its own
+    barrier; every member still ends bit-identical to the run driven alone on
+    one block."""
+    cfgs = _members()
+    ctas = [1, 3, 2, 4, 1]
+    batch = [streamer.Simulation(c) for c in cfgs]
+    alone = [streamer.Simulation(c) for c in cfgs]
+    for s, m in zip(batch, ctas):
+        s.device.set_ctas(m)
+    for s in batch + alone:
+        s.init()
+    nb, gpu_ms, _, cu = streamer.run_batch(batch, [c.end_time for c in cfgs], use_graph=use_graph,
+                                           n_threads=4)
+    assert nb > 0 and cu > 0
+    for k, (s, c) in enumerate(zip(alone, cfgs)):
+        s.run(c.end_time)
+        _same(batch[k], s, f"member {k} ({ctas[k]} blocks)")
