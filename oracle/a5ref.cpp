@@ -2928,6 +2928,96 @@ int a5ref_kat_mg_cyl_diel(int n_fmg, double *res, double *err, int *ml) {
   return kat_mg_diel(n_fmg, res, err, ml);
 }
 
+// afivo/examples/multigrid/test_mg3_2d.f90: a jump in eps (1 below y = 0.5,
+// 4 above) on the unit square, 2x2-cell boxes, refined to level 4 everywhere
+// and to level 7 within 5 dr of the centre (:90-101), phi = 0 at the bottom
+// and 1 at the top, Neumann sides (:120-141), no charge, FMG cycles with
+// set_residual (:64-69). The known answer is the layered solution: continuity
+// of eps dphi/dy gives phi = 1.6 y below the interface and 0.8 + 0.4 (y - 0.5)
+// above it. Per cycle: max |residual| and max |phi - exact| over the leaves.
+static int kat_mg3_2d(int n_fmg, double *res_out, double *err_out, int *max_lvl_out) {
+  const int i_phi = 0, i_tmp = 1, i_rhs = 2, i_eps = 3, i_err = 4;
+  Tree t;
+  const double r0[2] = {0, 0};
+  const int box_size = 2;
+  tree_init(t, box_size, 5, 0, 1.0 / box_size, r0, 30, 0, XYZ);
+  const int ixl[1][2] = {{1, 1}};
+  std::vector<std::array<int, 4>> nbl(1, std::array<int, 4>{-1, -1, -1, -1});
+  set_base(t, 1, ixl, nbl);
+  auto exact = [](double y) { return y < 0.5 ? 1.6 * y : 0.8 + 0.4 * (y - 0.5); };
+  const RefFn ref = [&](Tree &tt, int id, std::vector<int> &rf) {
+    const Box &b = tt.boxes[id];
+    const double d = 5 * b.dr;
+    bool inside = true;
+    for (int k = 0; k < 2; k++) {
+      const double r_max = b.r_min[k] + b.dr * b.n_cell;
+      if (!(0.5 + d >= b.r_min[k] && 0.5 - d <= r_max)) inside = false;
+    }
+    rf[id] = (b.lvl < 4 || (b.lvl < 7 && inside)) ? DO_REF : KP_REF;
+  };
+  for (int it = 0; it < 20; it++) {
+    RefInfo ri;
+    adjust_refinement(t, ref, ri);
+    if (ri.n_add == 0) break;
+  }
+  loop_all_boxes(t, [&](Box &b) {
+    const int nc = b.n_cell;
+    for (int j = 0; j <= nc + 1; j++)
+      for (int i = 0; i <= nc + 1; i++) {
+        double xy[2];
+        r_cc(b, i, j, xy);
+        b.c(i, j, i_phi) = 0;
+        b.c(i, j, i_rhs) = 0;
+        b.c(i, j, i_eps) = xy[1] < 0.5 ? 1.0 : 4.0;
+      }
+  });
+  MG mg;
+  mg.i_phi = i_phi;
+  mg.i_tmp = i_tmp;
+  mg.i_rhs = i_rhs;
+  mg.i_eps = i_eps;
+  mg.n_cycle_down = 2;
+  mg.n_cycle_up = 2;
+  mg.n_cycle_base = 2;
+  mg.sides_rb = mg_sides_rb;
+  mg.sides_bc = [](Tree &tt, int id, int nb, int iv) {
+    Box &b = tt.boxes[id];
+    const int nc = b.n_cell;
+    for (int n = 1; n <= nc; n++) {
+      switch (nb) {
+        case NB_LX: b.c(0, n, iv) = b.c(1, n, iv); break;
+        case NB_HX: b.c(nc + 1, n, iv) = b.c(nc, n, iv); break;
+        case NB_LY: b.c(n, 0, iv) = -b.c(n, 1, iv); break;
+        default: b.c(n, nc + 1, iv) = 2 - b.c(n, nc, iv);
+      }
+    }
+  };
+  for (int it = 1; it <= n_fmg; it++) {
+    fas_fmg(t, mg, true, it == 1);
+    loop_all_boxes(t, [&](Box &b) {
+      const int nc = b.n_cell;
+      for (int j = 1; j <= nc; j++)
+        for (int i = 1; i <= nc; i++) {
+          double xy[2];
+          r_cc(b, i, j, xy);
+          b.c(i, j, i_err) = b.c(i, j, i_phi) - exact(xy[1]);
+        }
+    });
+    const double mn = tree_min_cc(t, i_tmp), mx = tree_max_cc(t, i_tmp);
+    const double emn = tree_min_cc(t, i_err), emx = tree_max_cc(t, i_err);
+    if (res_out) res_out[it - 1] = std::max(std::fabs(mn), std::fabs(mx));
+    if (err_out) err_out[it - 1] = std::max(std::fabs(emn), std::fabs(emx));
+  }
+  if (max_lvl_out) *max_lvl_out = t.max_lvl;
+  int n_leaf = 0;
+  for (int lvl = t.min_lvl; lvl <= t.max_lvl; lvl++) n_leaf += (int)t.L(lvl).leaves.size();
+  return n_leaf;
+}
+
+int a5ref_kat_mg3_2d(int n_fmg, double *res, double *err, int *ml) {
+  return kat_mg3_2d(n_fmg, res, err, ml);
+}
+
 int a5ref_kat_mg2_2d(int n_fmg, double *res, double *err, int *ml) {
   return kat_mg(false, n_fmg, res, err, ml);
 }

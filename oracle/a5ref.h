@@ -188,6 +188,9 @@ int a5ref_kat_mg_cyl(int n_fmg, double *res_out, double *err_out,
  * number of boxes the multigrid treats as dielectric. */
 int a5ref_kat_mg_cyl_diel(int n_fmg, double *res_out, double *err_out,
                           int *max_lvl_out);
+/* Layered dielectric restating afivo/examples/multigrid/test_mg3_2d.f90
+ * (eps 1 / 4, exact piecewise-linear potential); returns the leaf boxes. */
+int a5ref_kat_mg3_2d(int n_fmg, double *res_out, double *err_out, int *max_lvl_out);
 /* Lookup-table convergence test restating fosito/test/test_m_lookup_table.f90:
  * max error of LT_get_col on sin(x) for a table of n_rows over [0, x_max]. */
 double a5ref_kat_lookup(int n_rows, int n_pairs, double x_max, int n_samples);

@@ -102,6 +102,7 @@ def lib() -> ctypes.CDLL:
             "a5ref_applied_voltage": (D, [P]),
             "a5ref_kat_mg2_2d": (I, [I, pd, pd, pi]), "a5ref_kat_mg_cyl": (I, [I, pd, pd, pi]),
             "a5ref_kat_mg_cyl_diel": (I, [I, pd, pd, pi]),
+            "a5ref_kat_mg3_2d": (I, [I, pd, pd, pi]),
             "a5ref_kat_lookup": (D, [I, I, D, I]), "a5ref_koren_mlim": (D, [D, D]),
             "a5ref_op_photoionization": (V, [P, D, I]),
             "a5ref_rng_get": (V, [P, pi]), "a5ref_rng_set": (V, [P, pi]),
@@ -409,6 +410,16 @@ def kat_mg_diel(n_fmg: int):
     ml = ctypes.c_int(0)
     n_diel = lib().a5ref_kat_mg_cyl_diel(n_fmg, _dp(res), _dp(err), ctypes.byref(ml))
     return res, err, ml.value, n_diel
+
+
+def kat_mg3_2d(n_fmg: int):
+    """The layered dielectric case (test_mg3_2d.f90): per FMG cycle max
+    |residual| and max |error| against the piecewise-linear solution, the
+    finest level and the number of leaf boxes."""
+    res, err = np.zeros(n_fmg), np.zeros(n_fmg)
+    ml = ctypes.c_int(0)
+    n = lib().a5ref_kat_mg3_2d(n_fmg, _dp(res), _dp(err), ctypes.byref(ml))
+    return res, err, ml.value, n
 
 
 def kat_lookup(n_rows: int, n_pairs: int = 100000, x_max: float = 10.0,

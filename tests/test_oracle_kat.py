@@ -170,3 +170,18 @@ def test_tree_sum_cc_formula():
                     tmp = tmp * (2 * math.acos(-1.0))
                 total = total + dr * dr * tmp
         assert sim.tree_sum_cc(a5ref.I_ELEC, 1) == total
+
+
+def test_mg3_2d_layered_dielectric_known_answer():
+    """afivo/examples/multigrid/test_mg3_2d.f90: eps jumps from 1 to 4 at
+    y = 0.5 (a cell face on every level). With the harmonic face weights of
+    the eps operators the layered solution (1.6 y below, 0.8 + 0.4 (y - 0.5)
+    above) satisfies the discrete equations exactly, so the multigrid must
+    converge to it to rounding -- across the refinement boundaries of the
+    level-7 patch around the centre as well."""
+    res, err, max_lvl, n_leaf = a5ref.kat_mg3_2d(8)
+    assert max_lvl == 7 and n_leaf > 300
+    for k in range(3):
+        assert res[k + 1] < res[k] / 10.0
+    assert err[0] < 1e-7
+    assert max(err[4:]) < 1e-13
