@@ -99,6 +99,7 @@ SIGNATURES = {
     "a5g_set_ctas": (_I, [_P, _I, ctypes.c_longlong]),
     "a5g_get_ctas": (_I, [_P, _PI, _PI]),
     "a5g_set_grid_local": (_I, [_P, _I]),
+    "a5g_set_level_set": (_I, [_P, _PD, _PD]),
     "a5g_batch_create": (_I, [ctypes.POINTER(_P), _I, ctypes.POINTER(_P)]),
     "a5g_batch_destroy": (_I, [_P]),
     "a5g_batch_begin": (_I, [_P, _PD, _PD]),

@@ -150,6 +150,10 @@ struct RunDev {
   int *tags;
   // partial sums of a5g_tree_sum_cc, one per team thread (capacity doubles)
   double *sumbuf;
+  // level-set boundaries of the multigrid (a5g_set_level_set): level-set
+  // function and boundary value per cell, slot layout; has_lsf: set
+  const double *lsf, *bval;
+  int has_lsf, pad6;
   int uniform_lvl;             // > 0: uniform refinement to this level
   int local_cells;             // grid mode: levels of at most this many cells on one block
   // grid mode (a5g_set_ctas): barrier words of the run's block group
@@ -159,7 +163,7 @@ struct RunDev {
   long long gbudget;
   double *gred;
 };
-constexpr int TAG_NORMAL = 1, TAG_DIEL = 2;
+constexpr int TAG_NORMAL = 1, TAG_DIEL = 2, TAG_LSF = 3;
 
 // Scalars of one photoionization call: photons created, the factor fac
 // of PH_set_src_2d and the master generator state at the start of the call.
@@ -844,6 +848,49 @@ __device__ __forceinline__ void phi_nbrs(double V, const T *phi, const BoxRec &B
 __device__ __forceinline__ bool diel_box(const RunDev &R, const BoxRec &B) {
   return R.diel && R.tags[B.gbase / SLOT] == TAG_DIEL;
 }
+// A box the multigrid treats with the level-set operators (its tag).
+__device__ __forceinline__ bool lsf_box(const RunDev &R, const BoxRec &B) {
+  return R.has_lsf && R.tags[B.gbase / SLOT] == TAG_LSF;
+}
+
+// lsf_dist_val (afivo/src/m_aX_mg.f90:1077-1104): from cell a (level set la,
+// boundary value ba) to neighbour b (level set lb, value vb, boundary value
+// bb): where the level set changes sign between them, the interface at
+// distance la / (la - lb) with the interpolated boundary value; else b.
+__device__ __forceinline__ void lsf_dist_val(double la, double ba, double lb, double vb, double bb,
+                                             double &dist, double &val) {
+  if (la * lb < 0) {
+    dist = la / (la - lb);
+    val = ba * (1 - dist) + bb * dist;
+  } else {
+    dist = 1;
+    val = vb;
+  }
+}
+
+// Distances and values of the four neighbours (lx, hx, ly, hy; values u,
+// ghost neighbours from their recipes) of cell (i, j) of a level-set box.
+__device__ __forceinline__ void lsf_nbrs(const RunDev &R, const BoxRec &B, int ncg, int i, int j,
+                                         const double u[4], double dd[4], double val[4]) {
+  const double *L = R.lsf + B.gbase, *Bv = R.bval + B.gbase;
+  const int loc = i + ncg * j;
+  const int nb[4] = {loc - 1, loc + 1, loc - ncg, loc + ncg};
+  const double la = L[loc], ba = Bv[loc];
+#pragma unroll
+  for (int k = 0; k < 4; k++) lsf_dist_val(la, ba, L[nb[k]], u[k], Bv[nb[k]], dd[k], val[k]);
+}
+
+// mg$D_box_lpllsf at one cell (afivo/src/m_aX_mg.f90:1270-1340, 2D):
+// 2 inv_dr^2 (sum over x and y of (d2 v1 + d1 v2 - (d1 + d2) u0) /
+// ((d1 + d2) d1 d2)), in the reference's operation order.
+__device__ __forceinline__ double lap_lsf(const RunDev &R, const BoxRec &B, int ncg, int i, int j,
+                                          double f0, const double u[4], double inv_dr_sq) {
+  double dd[4], val[4];
+  lsf_nbrs(R, B, ncg, i, j, u, dd, val);
+  return 2 * inv_dr_sq *
+         ((dd[1] * val[0] + dd[0] * val[1] - (dd[0] + dd[1]) * f0) / ((dd[0] + dd[1]) * dd[0] * dd[1]) +
+          (dd[3] * val[2] + dd[2] * val[3] - (dd[2] + dd[3]) * f0) / ((dd[2] + dd[3]) * dd[2] * dd[3]));
+}
 
 // Laplacian of a dielectric box at one cell (mg$D_box_lpld,
 // afivo/src/m_aX_mg.f90:951-1001; cylindrical mg2_box_clpld, :1467-1495):
@@ -878,6 +925,10 @@ __device__ __forceinline__ T lap_at(const RunDev &R, double V, const T *phi, con
   T lx, hx, ly, hy;
   phi_nbrs(V, phi, B, nc, ncg, i, j, g, lx, hx, ly, hy);
   const T v = phi[g];
+  if (lsf_box(R, B)) {
+    const double u[4] = {(double)lx, (double)hx, (double)ly, (double)hy};
+    return T(lap_lsf(R, B, ncg, i, j, (double)v, u, (double)inv_dr_sq));
+  }
   if (diel_box(R, B)) {
     const double u[4] = {(double)lx, (double)hx, (double)ly, (double)hy};
     return T(lap_diel(R, B, ncg, i, j, (double)v, u, (double)inv_dr_sq));
@@ -966,7 +1017,17 @@ __device__ __noinline__ void p_sweep(const RunDev &R, const MGV<T> &M, int lvl, 
       phi_nbrs(M.V, phi, B, L.nc, L.ncg, i, j, g, lx, hx, ly, hy);
     }
     const T r = rhs[g];
-    if (diel_box(R, B)) {
+    if (lsf_box(R, B)) {
+      // mg$D_box_gsrb_lpllsf (afivo/src/m_aX_mg.f90:1190-1267, 2D)
+      const double u[4] = {(double)lx, (double)hx, (double)ly, (double)hy};
+      double dd[4], val[4];
+      lsf_nbrs(R, B, L.ncg, i, j, u, dd, val);
+      const double prod = dd[0] * dd[1] * dd[2] * dd[3];
+      phi[g] = T(1 / (dd[0] * dd[1] + dd[2] * dd[3]) *
+                 ((dd[1] * val[0] + dd[0] * val[1]) * dd[2] * dd[3] / (dd[0] + dd[1]) +
+                  (dd[3] * val[2] + dd[2] * val[3]) * dd[0] * dd[1] / (dd[2] + dd[3]) -
+                  0.5 * prod * (double)dx2 * (double)r));
+    } else if (diel_box(R, B)) {
       // mg$D_box_gsrb_lpld (afivo/src/m_aX_mg.f90:895-948; cylindrical
       // mg2_box_gsrb_clpld, :1499-1531): face weights c = 2 a0 a / (a0 + a),
       // phi = (sum c rfac u - dx^2 rhs) / sum c rfac
@@ -1133,7 +1194,21 @@ __device__ void p_correct(const RunDev &R, const MGV<T> &M, int lvl, bool copy, 
       const int p2 = B.pbase + i_c2 + pncg * j_c1;
       const int p3 = B.pbase + i_c1 + pncg * j_c2;
       const T c1 = phi[p1] - tmp[p1], c2x = phi[p2] - tmp[p2], c2y = phi[p3] - tmp[p3];
-      if (diel_box(R, B)) {
+      if (lsf_box(R, B)) {
+        // mg$D_box_corr_lpllsf (afivo/src/m_aX_mg.f90:1106-1187, 2D): the
+        // correction along the lines to the three coarse cells, each cut at
+        // the interface, where a correction is 0
+        const double *lsf = R.lsf;
+        const double la = lsf[B.gbase + i + L.ncg * j];
+        const int pp[3] = {p1, p2, p3};
+        const double cv[3] = {(double)c1, (double)c2x, (double)c2y};
+        double dist[3], val[3];
+#pragma unroll
+        for (int q = 0; q < 3; q++) lsf_dist_val(la, 0.0, lsf[pp[q]], cv[q], 0.0, dist[q], val[q]);
+        const double cw[3] = {2 * dist[1] * dist[2], dist[0] * dist[2], dist[0] * dist[1]};
+        phi[g] = T((double)v + (cw[0] * val[0] + cw[1] * val[1] + cw[2] * val[2]) /
+                                   (cw[0] + cw[1] + cw[2]));
+      } else if (diel_box(R, B)) {
         // mg$D_box_corr_lpld (afivo/src/m_aX_mg.f90:1003-1071, 2D): eps-weighted
         // averages of the parent's correction toward each coarse neighbour
         const double *eps = VAR(R, I_EPS);
@@ -1705,18 +1780,28 @@ __device__ void p_set_tags(const RunDev &R) {
     for (int b = warp; b < nb; b += nwarp) {
       const int base = R.boxes[b0 + b].gbase;
       double mn = eps[base], mx = mn;
+      double ln = R.has_lsf ? R.lsf[base] : 0.0, lx = ln;
       for (int c = lane; c < per; c += 32) {
         const double v = eps[base + c];
         mn = dmin(mn, v);
         mx = dmax(mx, v);
+        if (R.has_lsf) {
+          const double w = R.lsf[base + c];
+          ln = dmin(ln, w);
+          lx = dmax(lx, w);
+        }
       }
       for (int o = 16; o > 0; o >>= 1) {
         mn = dmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
         mx = dmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        ln = dmin(ln, __shfl_xor_sync(0xffffffffu, ln, o));
+        lx = dmax(lx, __shfl_xor_sync(0xffffffffu, lx, o));
       }
       if (lane == 0) {
+        // mg$D_set_box_tag: level set first, eps tags override it
         const bool deps = mx > mn, ceps = !deps && (mn < 1 || mn > 1);
-        R.tags[base / SLOT] = (deps || ceps) ? TAG_DIEL : TAG_NORMAL;
+        const bool is_lsf = R.has_lsf && ln * lx < 0;
+        R.tags[base / SLOT] = (deps || ceps) ? TAG_DIEL : (is_lsf ? TAG_LSF : TAG_NORMAL);
       }
     }
   }
@@ -1750,8 +1835,8 @@ __device__ void p_vcycle_alone(const RunDev &R, int max_lvl, bool set_residual) 
 // tree fits, else in device memory (dielectric runs always in device memory).
 template <class F>
 __device__ __forceinline__ void mg_staged(const RunDev &R, F &&body) {
-  if (R.diel) p_set_tags(R);
-  if (R.smem_doubles > 0 && !R.diel) {
+  if (R.diel || R.has_lsf) p_set_tags(R);
+  if (R.smem_doubles > 0 && !R.diel && !R.has_lsf) {
     const int S = R.smem_doubles, nbx = R.bx_off[R.nlev], npb = R.pb_off[R.nlev];
     double *base = g_dsmem + PLAN_DOUBLES + (R.coord == 1 ? WTS_DOUBLES : 0);
     BoxRec *sb = reinterpret_cast<BoxRec *>(base + 3 * S);
@@ -3323,12 +3408,15 @@ struct a5g_ctx {
   int n_cta = 1;
   unsigned *gbar = nullptr;
   double *gred = nullptr;
+  // level-set boundaries (a5g_set_level_set): two cell arrays of the box
+  // capacity, grown with the box storage
+  double *lsf = nullptr, *bval = nullptr;
 };
 
 // Shared-memory staging of the multigrid variables as allowed and as fits
 // (never in grid mode: a block holds only part of the tree's work).
 static void apply_staging(a5g_ctx *c) {
-  const bool on = c->allow_smem && c->n_cta == 1;
+  const bool on = c->allow_smem && c->n_cta == 1 && !c->h.has_lsf;
   c->h.smem_doubles = on ? c->fit64 : 0;
   c->dyn_smem = on && c->fit64 ? c->need64 : 0;
   c->mx_smem_fit = on ? c->fit32 : 0;
@@ -3870,6 +3958,8 @@ int a5g_destroy(a5g_ctx *c) {
   cudaFree(c->sumbuf);
   cudaFree(c->gbar);
   cudaFree(c->gred);
+  cudaFree(c->lsf);
+  cudaFree(c->bval);
   if (c->ev_order) cudaEventDestroy(c->ev_order);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -3916,6 +4006,8 @@ int a5g_set_table(a5g_ctx *c, int n_rows, int n_cols, double x_min, double inv_d
 static int mx_ready(a5g_ctx *c) {
   if (c->precision == A5G_MIXED && c->h.diel)
     return fail(A5G_EINVAL, "the mixed form does not support dielectric runs (eps != 1)");
+  if (c->precision == A5G_MIXED && c->h.has_lsf)
+    return fail(A5G_EINVAL, "the mixed form does not support level-set boundaries");
   if (c->precision != A5G_MIXED || c->mx_smem_fit > 0 || c->cc32_cap >= c->capacity) return A5G_OK;
   cudaFree(c->cc32);
   c->cc32 = nullptr;
@@ -4026,6 +4118,7 @@ int a5g_set_rng(a5g_ctx *c, const int *st) {
 
 static int grow(a5g_ctx *c, int need) {
   if (need <= c->capacity) return A5G_OK;
+  const int old_cap = c->capacity;
   int cap = std::max(need, c->capacity + c->capacity / 2);
   cap = std::max(cap, 64);
   double *ncc = nullptr, *nfx = nullptr, *nfy = nullptr;
@@ -4082,6 +4175,27 @@ static int grow(a5g_ctx *c, int need) {
     cudaFree(c->sumbuf);
     c->sumbuf = ns;
     c->h.sumbuf = ns;
+  }
+  if (c->lsf) {
+    // level-set arrays follow the box storage (new boxes hold 0 until set)
+    double *nl = nullptr, *nb = nullptr;
+    const size_t old = (size_t)old_cap * SLOT, sz = (size_t)cap * SLOT;
+    if (cudaMalloc(&nl, sz * sizeof(double)) != cudaSuccess || cudaMalloc(&nb, sz * sizeof(double)) != cudaSuccess) {
+      cudaFree(nl);
+      cudaFree(nb);
+      return fail(A5G_ENOMEM, "cannot grow the level-set arrays");
+    }
+    CK(cudaMemsetAsync(nl, 0, sz * sizeof(double), c->stream));
+    CK(cudaMemsetAsync(nb, 0, sz * sizeof(double), c->stream));
+    CK(cudaMemcpyAsync(nl, c->lsf, old * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(nb, c->bval, old * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    cudaFree(c->lsf);
+    cudaFree(c->bval);
+    c->lsf = nl;
+    c->bval = nb;
+    c->h.lsf = nl;
+    c->h.bval = nb;
   }
   if (c->cc32) {  // scratch of the mixed form: reallocated at the next mixed launch
     cudaFree(c->cc32);
@@ -4539,6 +4653,39 @@ int a5g_set_ctas(a5g_ctx *c, int n_cta, long long wait_cycles) {
   int r = push_run(c);
   if (r) return r;
   return mx_ready(c);
+}
+
+int a5g_set_level_set(a5g_ctx *c, const double *lsf, const double *bval) {
+  if (!c) return fail(A5G_EINVAL, "null context");
+  if ((lsf == nullptr) != (bval == nullptr)) return fail(A5G_EINVAL, "set both lsf and bval, or neither");
+  if (!lsf) {
+    CK(cudaStreamSynchronize(c->stream));
+    c->h.has_lsf = 0;
+    return push_run(c);
+  }
+  if (!c->has_tree) return fail(A5G_ESTATE, "no tree uploaded");
+  if (c->precision == A5G_MIXED)
+    return fail(A5G_EINVAL, "the mixed form does not support level-set boundaries");
+  const size_t sz = (size_t)c->capacity * SLOT, n = (size_t)(c->max_id + 1) * SLOT;
+  if (!c->lsf) {
+    if (cudaMalloc(&c->lsf, sz * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&c->bval, sz * sizeof(double)) != cudaSuccess) {
+      cudaFree(c->lsf);
+      cudaFree(c->bval);
+      c->lsf = c->bval = nullptr;
+      return fail(A5G_ENOMEM, "cannot allocate the level-set arrays");
+    }
+    CK(cudaMemsetAsync(c->lsf, 0, sz * sizeof(double), c->stream));
+    CK(cudaMemsetAsync(c->bval, 0, sz * sizeof(double), c->stream));
+  }
+  CK(cudaMemcpyAsync(c->lsf, lsf, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->bval, bval, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->h.lsf = c->lsf;
+  c->h.bval = c->bval;
+  c->h.has_lsf = 1;
+  apply_staging(c);
+  return push_run(c);
 }
 
 int a5g_set_grid_local(a5g_ctx *c, int cells) {

@@ -270,6 +270,17 @@ class DeviceRun:
         (< 0: the library's default)."""
         call("a5g_set_ctas", self.h, int(n_cta), int(wait_cycles))
 
+    def set_level_set(self, lsf, bval):
+        """Level-set boundaries of the field solve (a5g_set_level_set): per
+        cell the level-set function and the boundary potential, downloaded
+        layout; None, None removes them."""
+        if lsf is None:
+            call("a5g_set_level_set", self.h, None, None)
+            return
+        lsf = np.ascontiguousarray(lsf, dtype=np.float64)
+        bval = np.ascontiguousarray(bval, dtype=np.float64)
+        call("a5g_set_level_set", self.h, _dp(lsf), _dp(bval))
+
     def set_grid_local(self, cells: int):
         """Grid mode: levels of at most `cells` cells run on one block."""
         call("a5g_set_grid_local", self.h, int(cells))

@@ -307,6 +307,18 @@ int a5g_batch_block(a5g_batch *b, int num_steps, int use_graph, double *dt, doub
  * the block. */
 int a5g_batch_launch(a5g_batch *b, int num_steps, int use_graph);
 int a5g_batch_finish(a5g_batch *b, double *dt, double *time, int *active, float *gpu_ms);
+/* Internal boundaries of the field solve from a level set, the multigrid
+ * operators mg$D_box_gsrb_lpllsf / mg$D_box_lpllsf / mg$D_box_corr_lpllsf
+ * (afivo/src/m_aX_mg.f90:1073-1340) that Afivo's mg$D_auto_* apply to the
+ * boxes where the level-set function changes sign (mg$D_set_box_tag,
+ * :673-712): lsf and bval give per cell (ids 0..max_id, slot layout as
+ * a5g_upload_cc, ghost cells included) the level-set function and the
+ * potential on its zero contour. The solve then takes neighbours across the
+ * contour at their distance with the boundary value. Restriction stays
+ * mg$D_box_rstr_lpl (the reference's default). NULL, NULL removes the level
+ * set. New boxes of a later topology hold 0 until set again; the mixed form
+ * rejects level sets. */
+int a5g_set_level_set(a5g_ctx *ctx, const double *lsf, const double *bval);
 /* Grid mode: the run's phases on n_cta thread blocks instead of one. The
  * reference runs a box loop over the boxes of a level with OpenMP threads
  * (afivo/src/m_aX_utils.f90:58-185); one block per run keeps a small tree's

@@ -46,8 +46,10 @@ static const int INIT_TAG = -INT_MAX;
 static const int XYZ = 0, CYL = 1;
 
 // Streamer variable indices, src/m_streamer.f90:17-43 (0-based).
+// I_LSF, I_BVAL: level-set function and boundary value of the level-set
+// multigrid operators (unused unless a level set is set)
 enum { I_ELEC = 0, I_PION, I_ELEC_OLD, I_PION_OLD, I_PHI, I_FLD, I_RHS,
-       I_PHO, I_EPS, N_VAR_CELL };
+       I_PHO, I_EPS, I_LSF, I_BVAL, N_VAR_CELL };
 enum { F_ELEC = 0, F_FLD, N_VAR_FACE };
 enum { I_MOBILITY = 0, I_DIFFUSION, I_ALPHA, I_ETA };
 
@@ -667,17 +669,29 @@ static void restrict_tree(Tree &t, int iv) {
 
 // ---------------------------------------------------------------------------
 // Multigrid, afivo/src/m_aX_mg.f90
-enum { MG_NORMAL_BOX = 1, MG_CEPS_BOX = 3, MG_VEPS_BOX = 4 };
+enum { MG_NORMAL_BOX = 1, MG_LSF_BOX = 2, MG_CEPS_BOX = 3, MG_VEPS_BOX = 4 };
 
 struct MG {
-  int i_phi = -1, i_rhs = -1, i_tmp = -1, i_eps = -1;
+  int i_phi = -1, i_rhs = -1, i_tmp = -1, i_eps = -1, i_lsf = -1, i_bval = -1;
   int n_cycle_down = 2, n_cycle_up = 2, n_cycle_base = 2;
   GcFn sides_bc, sides_rb;
 };
 
-// afivo/src/m_aX_mg.f90:574-603 (mg$D_set_box_tag); lsf is not used here.
+// afivo/src/m_aX_mg.f90:673-712 (mg$D_set_box_tag): a level-set box where
+// the level-set function changes sign in the box (ghost and corner cells
+// included), an eps box where eps varies or is a constant other than 1.
 static void set_box_tag(Box &b, const MG &mg) {
-  bool is_eps = false, is_deps = false;
+  bool is_lsf = false, is_eps = false, is_deps = false;
+  if (mg.i_lsf != -1) {
+    const int ncg = b.ncg();
+    double a = b.c(0, 0, mg.i_lsf), bb = a;
+    for (int j = 0; j < ncg; j++)
+      for (int i = 0; i < ncg; i++) {
+        a = std::min(a, b.c(i, j, mg.i_lsf));
+        bb = std::max(bb, b.c(i, j, mg.i_lsf));
+      }
+    is_lsf = a * bb < 0;
+  }
   if (mg.i_eps != -1) {
     int ncg = b.ncg();
     double a = b.c(0, 0, mg.i_eps), bb = a;
@@ -690,8 +704,73 @@ static void set_box_tag(Box &b, const MG &mg) {
     if (!is_deps) is_eps = (a < 1 || a > 1);
   }
   b.tag = MG_NORMAL_BOX;
+  if (is_lsf) b.tag = MG_LSF_BOX;
   if (is_eps) b.tag = MG_CEPS_BOX;
   if (is_deps) b.tag = MG_VEPS_BOX;
+}
+
+// lsf_dist_val (afivo/src/m_aX_mg.f90:1077-1104): distance (0..1] from a
+// to neighbour b and the value there: where the level set changes sign
+// between them, the interface at lsf_a / (lsf_a - lsf_b), with the boundary
+// values interpolated; else b itself and its value.
+static inline void lsf_dist_val(const double va[3], const double vb[3], double &dist, double &val) {
+  if (va[0] * vb[0] < 0) {
+    dist = va[0] / (va[0] - vb[0]);
+    val = va[2] * (1 - dist) + vb[2] * dist;
+  } else {
+    dist = 1;
+    val = vb[1];
+  }
+}
+
+// The four neighbours (lx, hx, ly, hy) of cell (i, j) as distances and
+// values for the level-set operators.
+static inline void lsf_nbrs(const Box &b, int i, int j, const MG &mg, int iv, double dd[4],
+                            double val[4]) {
+  const double va[3] = {b.c(i, j, mg.i_lsf), b.c(i, j, iv), b.c(i, j, mg.i_bval)};
+  const int di[4] = {-1, 1, 0, 0}, dj[4] = {0, 0, -1, 1};
+  for (int k = 0; k < 4; k++) {
+    const double vb[3] = {b.c(i + di[k], j + dj[k], mg.i_lsf), b.c(i + di[k], j + dj[k], iv),
+                          b.c(i + di[k], j + dj[k], mg.i_bval)};
+    lsf_dist_val(va, vb, dd[k], val[k]);
+  }
+}
+
+// mg$D_box_gsrb_lpllsf (afivo/src/m_aX_mg.f90:1190-1267, 2D): Gauss-Seidel
+// for the Laplacian with neighbours at distances dd dx (Fortran operation
+// order kept: 1 / (dd1 dd2 + dd3 dd4) * (...)).
+static void box_gsrb_lsf(Box &b, int redblack, const MG &mg) {
+  const double dx2 = b.dr * b.dr;
+  const int nc = b.n_cell;
+  for (int j = 1; j <= nc; j++) {
+    const int i0 = 2 - ((redblack ^ j) & 1);
+    for (int i = i0; i <= nc; i += 2) {
+      double dd[4], val[4];
+      lsf_nbrs(b, i, j, mg, mg.i_phi, dd, val);
+      const double prod = dd[0] * dd[1] * dd[2] * dd[3];
+      b.c(i, j, mg.i_phi) = 1 / (dd[0] * dd[1] + dd[2] * dd[3]) *
+                            ((dd[1] * val[0] + dd[0] * val[1]) * dd[2] * dd[3] / (dd[0] + dd[1]) +
+                             (dd[3] * val[2] + dd[2] * val[3]) * dd[0] * dd[1] / (dd[2] + dd[3]) -
+                             0.5 * prod * dx2 * b.c(i, j, mg.i_rhs));
+    }
+  }
+}
+
+// mg$D_box_lpllsf (afivo/src/m_aX_mg.f90:1270-1340, 2D)
+static void box_op_lsf(Box &b, int i_out, const MG &mg) {
+  const double inv_dr_sq = 1 / (b.dr * b.dr);
+  const int nc = b.n_cell;
+  for (int j = 1; j <= nc; j++)
+    for (int i = 1; i <= nc; i++) {
+      double dd[4], val[4];
+      lsf_nbrs(b, i, j, mg, mg.i_phi, dd, val);
+      const double f0 = b.c(i, j, mg.i_phi);
+      b.c(i, j, i_out) = 2 * inv_dr_sq *
+                         ((dd[1] * val[0] + dd[0] * val[1] - (dd[0] + dd[1]) * f0) /
+                              ((dd[0] + dd[1]) * dd[0] * dd[1]) +
+                          (dd[3] * val[2] + dd[2] * val[3] - (dd[2] + dd[3]) * f0) /
+                              ((dd[2] + dd[3]) * dd[2] * dd[3]));
+    }
 }
 
 // Radius weights of the cylindrical operators at global index g = i + ioff:
@@ -764,6 +843,10 @@ static void box_op_diel(Box &b, int i_out, const MG &mg) {
 // afivo/src/m_aX_mg.f90:636-659 (gsrb_lpl) and 998-1024 (gsrb_clpl)
 static void box_gsrb(Box &b, int redblack, const MG &mg) {
   if (b.tag == INIT_TAG) set_box_tag(b, mg);
+  if (b.tag == MG_LSF_BOX) {
+    box_gsrb_lsf(b, redblack, mg);
+    return;
+  }
   if (b.tag == MG_CEPS_BOX || b.tag == MG_VEPS_BOX) {
     box_gsrb_diel(b, redblack, mg);
     return;
@@ -796,6 +879,10 @@ static void box_gsrb(Box &b, int redblack, const MG &mg) {
 // afivo/src/m_aX_mg.f90:662-680 (box_lpl) and 1027-1049 (box_clpl)
 static void box_op(Box &b, int i_out, const MG &mg) {
   if (b.tag == INIT_TAG) set_box_tag(b, mg);
+  if (b.tag == MG_LSF_BOX) {
+    box_op_lsf(b, i_out, mg);
+    return;
+  }
   if (b.tag == MG_CEPS_BOX || b.tag == MG_VEPS_BOX) {
     box_op_diel(b, i_out, mg);
     return;
@@ -827,6 +914,30 @@ static void box_corr(const Box &p, Box &c, const MG &mg) {
   int nc = c.n_cell, ip = mg.i_phi, ic = mg.i_tmp;
   int off[2];
   child_offset(c, -1, off);
+  if (c.tag == MG_LSF_BOX) {
+    // mg$D_box_corr_lpllsf (afivo/src/m_aX_mg.f90:1106-1187, 2D): the
+    // correction interpolated along the lines to the three nearest coarse
+    // cells, each cut at the interface (boundary value 0 for a correction)
+    for (int j = 1; j <= nc; j++) {
+      int j_c1 = off[1] + ((j + 1) >> 1);
+      int j_c2 = j_c1 + 1 - 2 * (j & 1);
+      for (int i = 1; i <= nc; i++) {
+        int i_c1 = off[0] + ((i + 1) >> 1);
+        int i_c2 = i_c1 + 1 - 2 * (i & 1);
+        const double va[3] = {c.c(i, j, mg.i_lsf), c.c(i, j, ic), 0.0};
+        const int pi[3] = {i_c1, i_c2, i_c1}, pj[3] = {j_c1, j_c1, j_c2};
+        double dist[3], val[3];
+        for (int k = 0; k < 3; k++) {
+          const double vb[3] = {p.c(pi[k], pj[k], mg.i_lsf), p.c(pi[k], pj[k], ic), 0.0};
+          lsf_dist_val(va, vb, dist[k], val[k]);
+        }
+        const double cw[3] = {2 * dist[1] * dist[2], dist[0] * dist[2], dist[0] * dist[1]};
+        c.c(i, j, ip) = c.c(i, j, ip) + (cw[0] * val[0] + cw[1] * val[1] + cw[2] * val[2]) /
+                                            (cw[0] + cw[1] + cw[2]);
+      }
+    }
+    return;
+  }
   if (c.tag == MG_CEPS_BOX || c.tag == MG_VEPS_BOX) {
     // mg$D_box_corr_lpld, afivo/src/m_aX_mg.f90:1003-1071 (2D): eps-weighted
     // averages of the parent's correction toward each coarse neighbour
@@ -2203,6 +2314,22 @@ void a5ref_op_fld_from_pot(a5ref_sim *h) {
 // the sum as a team of `team` OpenMP threads forms it (team 1: the loop order)
 long long a5ref_photons_created(a5ref_sim *h) { return h->s.n_photons; }
 
+// Level-set boundaries of the run's field solves: lsf and bval per cell in
+// the export layout (ids 0..max_id); NULL removes them. Every box's
+// multigrid tag is set again at its next use (mg$D_set_box_tag).
+void a5ref_set_level_set(a5ref_sim *h, const double *lsf, const double *bval) {
+  Sim &s = h->s;
+  if (!lsf) {
+    s.mg.i_lsf = s.mg.i_bval = -1;
+  } else {
+    a5ref_import_cc(h, I_LSF, lsf);
+    a5ref_import_cc(h, I_BVAL, bval);
+    s.mg.i_lsf = I_LSF;
+    s.mg.i_bval = I_BVAL;
+  }
+  for (int id = 1; id <= s.tree.max_id; id++) s.tree.boxes[id].tag = INIT_TAG;
+}
+
 // ---------------------------------------------------------------------------
 // Streamer diagnostics of the axisymmetric program, one thread.
 
@@ -3016,6 +3143,94 @@ static int kat_mg3_2d(int n_fmg, double *res_out, double *err_out, int *max_lvl_
 
 int a5ref_kat_mg3_2d(int n_fmg, double *res, double *err, int *ml) {
   return kat_mg3_2d(n_fmg, res, err, ml);
+}
+
+// afivo/examples/multigrid/test_mgb_2d.f90: internal boundaries from a level
+// set on the 4 x 4 square (8x8-cell boxes, refined uniformly to level 6,
+// :32-44, 83-89), phi = phi0 = 1e3 on the zero contour, phi = 0 at the
+// bottom and top, Neumann sides (:115-131), no charge, FMG cycles with the
+// level-set operators on the boxes the contour crosses (mg2_auto_*, default
+// restriction). shape 0: the example's ellipse sqrt(100 x^2 + y^2) - 1.8
+// around the centre (:100-104); shape 1: the plane y = 1.3, whose exact
+// solution phi0 y / 1.3 below and phi0 (4 - y) / 2.7 above satisfies the
+// operators' one-sided differences exactly. Per cycle: max |residual| and
+// (shape 1) max |phi - exact| over the leaves; returns the boxes tagged.
+static int kat_mgb_2d(int shape, int n_fmg, double *res_out, double *err_out) {
+  const int i_phi = 0, i_tmp = 1, i_rhs = 2, i_lsf = 3, i_bval = 4, i_err = 5;
+  const double phi0 = 1e3, y0 = 1.3;
+  Tree t;
+  const double r0[2] = {0, 0};
+  const int box_size = 8;
+  tree_init(t, box_size, 6, 0, 4.0 / box_size, r0, 30, 8, XYZ);
+  const int ixl[1][2] = {{1, 1}};
+  std::vector<std::array<int, 4>> nbl(1, std::array<int, 4>{-1, -1, -1, -1});
+  set_base(t, 1, ixl, nbl);
+  const RefFn ref = [](Tree &tt, int id, std::vector<int> &rf) {
+    if (tt.boxes[id].lvl < 6) rf[id] = DO_REF;
+  };
+  for (int it = 0; it < 20; it++) {
+    RefInfo ri;
+    adjust_refinement(t, ref, ri);
+    if (ri.n_add == 0) break;
+  }
+  auto exact = [&](double y) { return y < y0 ? phi0 * y / y0 : phi0 * (4 - y) / (4 - y0); };
+  loop_all_boxes(t, [&](Box &b) {
+    const int nc = b.n_cell;
+    for (int j = 0; j <= nc + 1; j++)
+      for (int i = 0; i <= nc + 1; i++) {
+        double xy[2];
+        r_cc(b, i, j, xy);
+        const double x = xy[0] - 2, y = xy[1] - 2;
+        b.c(i, j, i_phi) = 0;
+        b.c(i, j, i_rhs) = 0;
+        b.c(i, j, i_lsf) = shape == 0 ? std::sqrt(100 * (x * x) + y * y) - 1.8 : xy[1] - y0;
+        b.c(i, j, i_bval) = phi0;
+      }
+  });
+  MG mg;
+  mg.i_phi = i_phi;
+  mg.i_tmp = i_tmp;
+  mg.i_rhs = i_rhs;
+  mg.i_lsf = i_lsf;
+  mg.i_bval = i_bval;
+  mg.sides_rb = mg_sides_rb;
+  mg.sides_bc = [](Tree &tt, int id, int nb, int iv) {
+    Box &b = tt.boxes[id];
+    const int nc = b.n_cell;
+    for (int n = 1; n <= nc; n++) {
+      switch (nb) {
+        case NB_LX: b.c(0, n, iv) = b.c(1, n, iv); break;
+        case NB_HX: b.c(nc + 1, n, iv) = b.c(nc, n, iv); break;
+        case NB_LY: b.c(n, 0, iv) = -b.c(n, 1, iv); break;
+        default: b.c(n, nc + 1, iv) = -b.c(n, nc, iv);
+      }
+    }
+  };
+  for (int it = 1; it <= n_fmg; it++) {
+    fas_fmg(t, mg, true, it == 1);
+    loop_all_boxes(t, [&](Box &b) {
+      const int nc = b.n_cell;
+      for (int j = 1; j <= nc; j++)
+        for (int i = 1; i <= nc; i++) {
+          double xy[2];
+          r_cc(b, i, j, xy);
+          b.c(i, j, i_err) = b.c(i, j, i_phi) - exact(xy[1]);
+        }
+    });
+    const double mn = tree_min_cc(t, i_tmp), mx = tree_max_cc(t, i_tmp);
+    if (res_out) res_out[it - 1] = std::max(std::fabs(mn), std::fabs(mx));
+    if (err_out)
+      err_out[it - 1] = std::max(std::fabs(tree_min_cc(t, i_err)), std::fabs(tree_max_cc(t, i_err)));
+  }
+  int n_lsf = 0;
+  for (int lvl = t.min_lvl; lvl <= t.max_lvl; lvl++)
+    for (int id : t.L(lvl).ids)
+      if (t.boxes[id].tag == MG_LSF_BOX) n_lsf++;
+  return n_lsf;
+}
+
+int a5ref_kat_mgb_2d(int shape, int n_fmg, double *res, double *err) {
+  return kat_mgb_2d(shape, n_fmg, res, err);
 }
 
 int a5ref_kat_mg2_2d(int n_fmg, double *res, double *err, int *ml) {

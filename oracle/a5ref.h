@@ -126,6 +126,9 @@ void a5ref_op_set_rhs(a5ref_sim *s);
 void a5ref_op_fmg(a5ref_sim *s, int set_residual, int first_call);
 void a5ref_op_fld_from_pot(a5ref_sim *s);
 void a5ref_op_vcycle(a5ref_sim *s, int max_lvl, int set_residual);
+/* Level-set boundaries of the field solves (lsf, bval per cell, export
+ * layout; NULL removes them); box tags are reset. */
+void a5ref_set_level_set(a5ref_sim *s, const double *lsf, const double *bval);
 /* Photons created by the last photoionization call. */
 long long a5ref_photons_created(a5ref_sim *s);
 /* get_streamer_properties (src/streamer_cyl.f90:682-828): 39 values. */
@@ -191,6 +194,11 @@ int a5ref_kat_mg_cyl_diel(int n_fmg, double *res_out, double *err_out,
 /* Layered dielectric restating afivo/examples/multigrid/test_mg3_2d.f90
  * (eps 1 / 4, exact piecewise-linear potential); returns the leaf boxes. */
 int a5ref_kat_mg3_2d(int n_fmg, double *res_out, double *err_out, int *max_lvl_out);
+/* Level-set boundary restating afivo/examples/multigrid/test_mgb_2d.f90
+ * (shape 0: its ellipse; 1: a plane with an exact piecewise-linear
+ * solution); returns the boxes the multigrid treats with the level-set
+ * operators. */
+int a5ref_kat_mgb_2d(int shape, int n_fmg, double *res_out, double *err_out);
 /* Lookup-table convergence test restating fosito/test/test_m_lookup_table.f90:
  * max error of LT_get_col on sin(x) for a table of n_rows over [0, x_max]. */
 double a5ref_kat_lookup(int n_rows, int n_pairs, double x_max, int n_samples);

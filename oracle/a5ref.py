@@ -88,6 +88,7 @@ def lib() -> ctypes.CDLL:
             "a5ref_tree_max_cc": (D, [P, I]), "a5ref_tree_min_cc": (D, [P, I]),
             "a5ref_tree_sum_cc": (D, [P, I, I]),
             "a5ref_photons_created": (ctypes.c_longlong, [P]),
+            "a5ref_set_level_set": (V, [P, pd, pd]),
             "a5ref_streamer_properties": (V, [P, pd]),
             "a5ref_cc_axis": (I, [P, pd, I]),
             "a5ref_vtk_arrays": (I, [P, I, pi, I, pi, pd, pi, pi, pi, pd]),
@@ -103,6 +104,7 @@ def lib() -> ctypes.CDLL:
             "a5ref_kat_mg2_2d": (I, [I, pd, pd, pi]), "a5ref_kat_mg_cyl": (I, [I, pd, pd, pi]),
             "a5ref_kat_mg_cyl_diel": (I, [I, pd, pd, pi]),
             "a5ref_kat_mg3_2d": (I, [I, pd, pd, pi]),
+            "a5ref_kat_mgb_2d": (I, [I, I, pd, pd]),
             "a5ref_kat_lookup": (D, [I, I, D, I]), "a5ref_koren_mlim": (D, [D, D]),
             "a5ref_op_photoionization": (V, [P, D, I]),
             "a5ref_rng_get": (V, [P, pi]), "a5ref_rng_set": (V, [P, pi]),
@@ -249,6 +251,14 @@ class Sim:
 
     def tree_sum_cc(self, iv: int, team: int = 1) -> float:
         return lib().a5ref_tree_sum_cc(self.h, iv, team)
+
+    def set_level_set(self, lsf, bval):
+        if lsf is None:
+            lib().a5ref_set_level_set(self.h, None, None)
+            return
+        lsf = np.ascontiguousarray(lsf, dtype=np.float64)
+        bval = np.ascontiguousarray(bval, dtype=np.float64)
+        lib().a5ref_set_level_set(self.h, _dp(lsf), _dp(bval))
 
     def photons_created(self) -> int:
         return int(lib().a5ref_photons_created(self.h))
@@ -420,6 +430,15 @@ def kat_mg3_2d(n_fmg: int):
     ml = ctypes.c_int(0)
     n = lib().a5ref_kat_mg3_2d(n_fmg, _dp(res), _dp(err), ctypes.byref(ml))
     return res, err, ml.value, n
+
+
+def kat_mgb_2d(shape: str, n_fmg: int):
+    """The level-set boundary case (test_mgb_2d.f90; 'ellipse' or 'plane'):
+    per FMG cycle max |residual| and max |error| (plane), and the number of
+    boxes tagged for the level-set operators."""
+    res, err = np.zeros(n_fmg), np.zeros(n_fmg)
+    n = lib().a5ref_kat_mgb_2d(0 if shape == "ellipse" else 1, n_fmg, _dp(res), _dp(err))
+    return res, err, n
 
 
 def kat_lookup(n_rows: int, n_pairs: int = 100000, x_max: float = 10.0,

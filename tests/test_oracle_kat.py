@@ -185,3 +185,21 @@ def test_mg3_2d_layered_dielectric_known_answer():
         assert res[k + 1] < res[k] / 10.0
     assert err[0] < 1e-7
     assert max(err[4:]) < 1e-13
+
+
+def test_mgb_2d_level_set_known_answer():
+    """afivo/examples/multigrid/test_mgb_2d.f90: internal boundaries from a
+    level set (value 1e3 on the zero contour). For the plane y = 1.3 the
+    one-sided differences of the level-set operators are exact for the
+    piecewise-linear solution, so the multigrid converges to it to rounding;
+    for the example's own ellipse the residual falls by a large factor per
+    cycle."""
+    res, err, n_lsf = a5ref.kat_mgb_2d("plane", 12)
+    assert n_lsf > 30
+    for k in range(6):
+        assert res[k + 1] < res[k] / 10.0
+    assert err[-1] < 1e-12 * 1e3
+    res, _, n_lsf = a5ref.kat_mgb_2d("ellipse", 10)
+    assert n_lsf > 60
+    for k in range(7):
+        assert res[k + 1] < res[k] / 10.0
