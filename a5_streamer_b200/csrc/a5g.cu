@@ -1004,7 +1004,7 @@ __device__ __noinline__ void p_sweep(const RunDev &R, const MGV<T> &M, int lvl, 
   const int p = it & 1;  // parity (i + j) & 1 of the updated cells
   const bool cyl = R.coord == 1;
   const int n = L.nb * half;
-  for (int k = TID(); k < n; k += NTH()) {
+  for (int k = TID(), nt_ = NTH(); k < n; k += nt_) {
     const BoxRec &B = M.boxes[L.b0 + (k >> hsh)];
     const int t = k & (half - 1);
     const int j = t / hn + 1, m = t % hn;
@@ -1075,7 +1075,7 @@ template <class T>
 __device__ __forceinline__ void fill_phi_loop(const RunDev &R, const MGV<T> &M, const LvlInfo &L, bool copy_tmp) {
   T *phi = M.phi, *tmp = M.tmp;
   const int per = 4 * L.nc, n = L.nb * per;
-  for (int k = TID(); k < n; k += NTH()) {
+  for (int k = TID(), nt_ = NTH(); k < n; k += nt_) {
     const BoxRec &B = M.boxes[L.b0 + (k >> (L.sh + 2))];
     const int r = k & (per - 1), side = r >> L.sh, kk = (r & (L.nc - 1)) + 1;
     const T v = phi_ghost_sl(M.V, phi, B, L.nc, L.ncg, side, kk);
@@ -1111,7 +1111,7 @@ __device__ __noinline__ void p_fr(const RunDev &R, const MGV<T> &M, int lvl, boo
   // parent cell is gathered by shuffles (cells of a box are consecutive
   // threads, i fastest) and added in the order of box_rstr_lpl
   const int per = L.nc * L.nc, n = L.nb * per, nw = (n + 31) & ~31;
-  for (int k = TID(); k < nw; k += NTH()) {
+  for (int k = TID(), nt_ = NTH(); k < nw; k += nt_) {
     const bool act = k < n;
     const BoxRec &B = M.boxes[L.b0 + (act ? k >> (2 * L.sh) : 0)];
     const int t = k & (per - 1), i = (t & (L.nc - 1)) + 1, j = (t >> L.sh) + 1;
@@ -1157,7 +1157,7 @@ __device__ void p_fc(const RunDev &R, const MGV<T> &M, int lvl, bool copy_tmp) {
   T *phi = M.phi, *tmp = M.tmp, *rhs = M.rhs;
   const T inv_dr_sq = T(1 / (L.dr * L.dr));
   const int per = L.nc * L.nc, n = npb * per;
-  for (int k = TID(); k < n; k += NTH()) {
+  for (int k = TID(), nt_ = NTH(); k < n; k += nt_) {
     const BoxRec &B = M.boxes[pb[k >> (2 * L.sh)]];
     const int t = k & (per - 1), i = (t & (L.nc - 1)) + 1, j = (t >> L.sh) + 1;
     const int g = B.base + i + L.ncg * j;
@@ -1181,7 +1181,7 @@ __device__ void p_correct(const RunDev &R, const MGV<T> &M, int lvl, bool copy, 
   const int pncg = correct ? R.lv_nc[lvl - 1 - R.min_lvl] + 2 : 0;
   T *phi = M.phi, *tmp = M.tmp;
   const int per = L.nc * L.nc, n = L.nb * per;
-  for (int k = TID(); k < n; k += NTH()) {
+  for (int k = TID(), nt_ = NTH(); k < n; k += nt_) {
     const BoxRec &B = M.boxes[L.b0 + (k >> (2 * L.sh))];
     const int t = k & (per - 1), i = (t & (L.nc - 1)) + 1, j = (t >> L.sh) + 1;
     const int g = B.base + i + L.ncg * j;
@@ -1224,7 +1224,7 @@ __device__ void p_correct(const RunDev &R, const MGV<T> &M, int lvl, bool copy, 
   }
   if (copy) {
     const int pg = 4 * L.nc, ng = L.nb * pg;
-    for (int k = TID(); k < ng; k += NTH()) {
+    for (int k = TID(), nt_ = NTH(); k < ng; k += nt_) {
       const BoxRec &B = M.boxes[L.b0 + (k >> (L.sh + 2))];
       const int r = k & (pg - 1), side = r >> L.sh, kk = (r & (L.nc - 1)) + 1;
       const int dim = side >> 1, gx = (side & 1) ? L.nc + 1 : 0;
@@ -1245,7 +1245,7 @@ __device__ __noinline__ void p_init_level(const RunDev &R, const MGV<T> &M, int 
   const double *e = VAR(R, I_ELEC), *pi = VAR(R, I_PION);
   const double fac = UC_ELEM_CHARGE / UC_EPS0;
   const int hn = L.nc >> 1, per = hn * hn, n = L.nb * per;
-  for (int k = TID(); k < n; k += NTH()) {
+  for (int k = TID(), nt_ = NTH(); k < n; k += nt_) {
     const BoxRec &B = M.boxes[L.b0 + (k >> (2 * L.sh - 2))];
     const int t = k & (per - 1), ii = (t & (hn - 1)) + 1, jj = (t >> (L.sh - 1)) + 1;
     const bool leaf = leaf_rhs && (B.flags & CF_LEAF);
@@ -1264,7 +1264,7 @@ __device__ __noinline__ void p_init_level(const RunDev &R, const MGV<T> &M, int 
     rhs[B.pbase + (B.o0 + ii) + pncg * (B.o1 + jj)] = T(0.25) * (rs[0] + rs[1] + rs[2] + rs[3]);
   }
   const int pc = L.ncg * L.ncg, nz = L.nb * pc;
-  for (int k = TID(); k < nz; k += NTH()) phi[M.boxes[L.b0 + k / pc].base + k % pc] = T(0);
+  for (int k = TID(), nt_ = NTH(); k < nz; k += nt_) phi[M.boxes[L.b0 + k / pc].base + k % pc] = T(0);
   PSYNC();
 }
 
@@ -1278,7 +1278,7 @@ __device__ __noinline__ void p_residual_all(const RunDev &R, const MGV<T> &M, in
     const LvlInfo L = lvl_info(R, lvl);
     const T inv_dr_sq = T(1 / (L.dr * L.dr));
     const int per = L.nc * L.nc, n = L.nb * per;
-    for (int k = TID(); k < n; k += NTH()) {
+    for (int k = TID(), nt_ = NTH(); k < n; k += nt_) {
       const BoxRec &B = M.boxes[L.b0 + (k >> (2 * L.sh))];
       const int t = k & (per - 1), i = (t & (L.nc - 1)) + 1, j = (t >> L.sh) + 1;
       const int g = B.base + i + L.ncg * j;
@@ -1610,7 +1610,14 @@ __device__ __forceinline__ void vcycle_body(const RunDev &R, const MGV<T> &M, in
                                             PlanFetch &pf, int after) {
   const int min_lvl = R.min_lvl;
   const bool cyl = R.coord == 1;
-  auto down = [&](int lvl) {
+  // grid mode: the levels min_lvl..lc run on block 0 alone (the others wait
+  // at the barrier of local_end); each level's code appears once
+  const int lc = local_top(R, max_lvl);
+  const int size = s_grp.size;
+  bool work = true;
+  for (int lvl = max_lvl; lvl >= min_lvl + 1; lvl--) {
+    if (lvl == lc) work = local_begin();
+    if (!work) continue;
     const LvlInfo L = lvl_info(R, lvl);
     if (plan_fits(M, L)) {
       const LevelPlan P = make_level_plan(R, M, L, cyl, pf);
@@ -1623,8 +1630,9 @@ __device__ __forceinline__ void vcycle_body(const RunDev &R, const MGV<T> &M, in
     }
     fetch_level_plan(R, M, lvl - 1, cyl, pf);
     p_fc(R, M, lvl - 1, true);
-  };
-  auto base = [&]() {
+  }
+  if (lc == min_lvl) work = local_begin();
+  if (work) {
     const LvlInfo L = lvl_info(R, min_lvl);
     if (plan_fits(M, L)) {
       const LevelPlan P = make_level_plan(R, M, L, cyl, pf);
@@ -1635,8 +1643,13 @@ __device__ __forceinline__ void vcycle_body(const RunDev &R, const MGV<T> &M, in
     }
     fetch_level_plan(R, M, min_lvl < max_lvl ? min_lvl + 1 : after, cyl, pf);
     p_fill(R, M, min_lvl);
-  };
-  auto up = [&](int lvl) {
+  }
+  for (int lvl = min_lvl + 1; lvl <= max_lvl; lvl++) {
+    if (lvl == lc + 1 && lc >= min_lvl) {
+      local_end(size);
+      work = true;
+    }
+    if (!work) continue;
     const LvlInfo L = lvl_info(R, lvl);
     if (plan_fits(M, L)) {
       const LevelPlan P = make_level_plan(R, M, L, cyl, pf);
@@ -1649,21 +1662,8 @@ __device__ __forceinline__ void vcycle_body(const RunDev &R, const MGV<T> &M, in
     }
     fetch_level_plan(R, M, lvl < max_lvl ? lvl + 1 : after, cyl, pf);
     p_fill(R, M, lvl);
-  };
-  const int lc = local_top(R, max_lvl);
-  for (int lvl = max_lvl; lvl >= min_lvl + 1 && lvl > lc; lvl--) down(lvl);
-  if (lc >= min_lvl) {
-    const int size = s_grp.size;
-    if (local_begin()) {
-      for (int lvl = lc; lvl >= min_lvl + 1; lvl--) down(lvl);
-      base();
-      for (int lvl = min_lvl + 1; lvl <= lc; lvl++) up(lvl);
-    }
-    local_end(size);
-  } else {
-    base();
   }
-  for (int lvl = max(min_lvl + 1, lc + 1); lvl <= max_lvl; lvl++) up(lvl);
+  if (lc == max_lvl && lc >= min_lvl) local_end(size);
 }
 
 // The FP64 V-cycle is inlined into its caller; the FP32 one (mixed form) is
@@ -1697,21 +1697,23 @@ __device__ void p_fmg_in(const RunDev &R, const MGV<T> &M, bool set_residual, bo
     }
   }
   PlanFetch pf;
-  auto level = [&](int lvl) {
+  // grid mode: the FMG's levels up to local_top, whose V-cycles touch only
+  // those levels, on block 0 alone
+  const int lc = local_top(R, max_lvl);
+  const int size = s_grp.size;
+  bool work = true;
+  if (lc >= min_lvl) work = local_begin();
+  for (int lvl = min_lvl; lvl <= max_lvl; lvl++) {
+    if (lvl == lc + 1 && lc >= min_lvl) {
+      local_end(size);
+      work = true;
+    }
+    if (!work) continue;
     p_correct(R, M, lvl, true, lvl > min_lvl);
     p_vcycle(R, M, lvl, first_call && lvl == min_lvl, pf, lvl + 1);
     if (set_residual && lvl == max_lvl) p_residual_all(R, M, lvl);
-  };
-  // grid mode: the FMG's levels up to local_top, whose V-cycles touch only
-  // those levels, on one block
-  const int lc = local_top(R, max_lvl);
-  if (lc >= min_lvl) {
-    const int size = s_grp.size;
-    if (local_begin())
-      for (int lvl = min_lvl; lvl <= lc; lvl++) level(lvl);
-    local_end(size);
   }
-  for (int lvl = max(min_lvl, lc + 1); lvl <= max_lvl; lvl++) level(lvl);
+  if (lc == max_lvl && lc >= min_lvl) local_end(size);
   if (pf.li >= 0) cp_async_wait_all();
 }
 
@@ -1895,7 +1897,7 @@ __device__ __noinline__ void p_mx_residual(const RunDev &R, const MGV<float> &M,
   const double inv_dr_sq = 1 / (L.dr * L.dr);
   const double fac = UC_ELEM_CHARGE / UC_EPS0;
   const int per = L.nc * L.nc, n = L.nb * per, nw = (n + 31) & ~31;
-  for (int k = TID(); k < nw; k += NTH()) {
+  for (int k = TID(), nt_ = NTH(); k < nw; k += nt_) {
     const bool act = k < n;
     const int b = L.b0 + (act ? k >> (2 * L.sh) : 0);
     const BoxRec &B = R.boxes[b];  // device-memory slots (phi, rhs, densities)
@@ -1935,7 +1937,7 @@ __device__ __noinline__ void p_mx_residual(const RunDev &R, const MGV<float> &M,
   }
   // side ghosts of c and of its tmp start at zero (consistent with c = 0 and V = 0)
   const int pg = 4 * L.nc, ng = L.nb * pg;
-  for (int k = TID(); k < ng; k += NTH()) {
+  for (int k = TID(), nt_ = NTH(); k < ng; k += nt_) {
     const BoxRec &S = M.boxes[L.b0 + (k >> (L.sh + 2))];
     const int r = k & (pg - 1), side = r >> L.sh, kk = (r & (L.nc - 1)) + 1;
     const int dim = side >> 1, gx = (side & 1) ? L.nc + 1 : 0;
@@ -1951,7 +1953,7 @@ __device__ void p_mx_accumulate(const RunDev &R, const MGV<float> &M) {
   for (int lvl = R.min_lvl; lvl <= R.max_lvl; lvl++) {
     const LvlInfo L = lvl_info(R, lvl);
     const int per = L.nc * L.nc, n = L.nb * per;
-    for (int k = TID(); k < n; k += NTH()) {
+    for (int k = TID(), nt_ = NTH(); k < n; k += nt_) {
       const int b = L.b0 + (k >> (2 * L.sh));
       const int t = k & (per - 1), i = (t & (L.nc - 1)) + 1, j = (t >> L.sh) + 1;
       const int loc = i + L.ncg * j;
@@ -2009,10 +2011,20 @@ __device__ void p_solve_mixed(const RunDev &R) {
 // a$D_gc_tree(iv, a$D_gc_interp[_lim], a$D_gc_neumann) for one or two
 // variables, levels ascending (m_aX_gc.f90:28-46, 90-330)
 __device__ void p_gc_den(const RunDev &R, int iv0, int iv1, bool lim) {
-  auto level = [&](int lvl) {
+  // grid mode: the small coarse levels (filled first) on block 0 alone
+  const int lc = local_top(R, R.max_lvl);
+  const int size = s_grp.size;
+  bool work = true;
+  if (lc >= R.min_lvl) work = local_begin();
+  for (int lvl = R.min_lvl; lvl <= R.max_lvl; lvl++) {
+    if (lvl == lc + 1 && lc >= R.min_lvl) {
+      local_end(size);
+      work = true;
+    }
+    if (!work) continue;
     const LvlInfo L = lvl_info(R, lvl);
     const int per = 4 * L.nc, n = L.nb * per;
-    for (int k = TID(); k < n; k += NTH()) {
+    for (int k = TID(), nt_ = NTH(); k < n; k += nt_) {
       const BoxRec &B = R.boxes[L.b0 + (k >> (L.sh + 2))];
       const int r = k & (per - 1), side = r >> L.sh, kk = (r & (L.nc - 1)) + 1;
       const int dim = side >> 1, gx = (side & 1) ? L.nc + 1 : 0;
@@ -2031,16 +2043,8 @@ __device__ void p_gc_den(const RunDev &R, int iv0, int iv1, bool lim) {
       }
     }
     PSYNC();
-  };
-  // grid mode: the small coarse levels (filled first) on one block
-  const int lc = local_top(R, R.max_lvl);
-  if (lc >= R.min_lvl) {
-    const int size = s_grp.size;
-    if (local_begin())
-      for (int lvl = R.min_lvl; lvl <= lc; lvl++) level(lvl);
-    local_end(size);
   }
-  for (int lvl = max(R.min_lvl, lc + 1); lvl <= R.max_lvl; lvl++) level(lvl);
+  if (lc == R.max_lvl && lc >= R.min_lvl) local_end(size);
 }
 
 // a$D_restrict_tree for one or two variables, levels descending
@@ -2048,14 +2052,22 @@ __device__ void p_gc_den(const RunDev &R, int iv0, int iv1, bool lim) {
 // radius evaluated at the child-local index [i, j] as in :104)
 __device__ void p_restrict(const RunDev &R, int iv0, int iv1) {
   const bool cyl = R.coord == 1;
-  auto level = [&](int lvl) {
+  // grid mode: the small coarse levels (restricted last) on block 0 alone
+  const int lc = local_top(R, R.max_lvl);
+  const int top = min(lc, R.max_lvl - 1);
+  const bool loc = lc >= R.min_lvl && top >= R.min_lvl;
+  const int size = s_grp.size;
+  bool work = true;
+  for (int lvl = R.max_lvl - 1; lvl >= R.min_lvl; lvl--) {
+    if (loc && lvl == top) work = local_begin();
+    if (!work) continue;
     const LvlInfo L = lvl_info(R, lvl);
     const int li = lvl - R.min_lvl;
     const int *pb = R.pbx + R.pb_off[li];
     const int npb = R.pb_off[li + 1] - R.pb_off[li];
     const int cg = R.lv_nc[li + 1] + 2;
     const int per = L.nc * L.nc, n = npb * per;
-    for (int k = TID(); k < n; k += NTH()) {
+    for (int k = TID(), nt_ = NTH(); k < n; k += nt_) {
       const BoxRec &P = R.boxes[pb[k >> (2 * L.sh)]];
       const int t = k & (per - 1), ic = (t & (L.nc - 1)) + 1, jc = (t >> L.sh) + 1;
       int q = 0, i = ic, j = jc;
@@ -2097,16 +2109,8 @@ __device__ void p_restrict(const RunDev &R, int iv0, int iv1) {
       }
     }
     PSYNC();
-  };
-  // grid mode: the small coarse levels (restricted last) on one block
-  const int lc = local_top(R, R.max_lvl);
-  for (int lvl = R.max_lvl - 1; lvl >= R.min_lvl && lvl > lc; lvl--) level(lvl);
-  if (lc >= R.min_lvl) {
-    const int size = s_grp.size;
-    if (local_begin())
-      for (int lvl = min(lc, R.max_lvl - 1); lvl >= R.min_lvl; lvl--) level(lvl);
-    local_end(size);
   }
+  if (loc) local_end(size);
 }
 
 // Field of one face from the potential (fld_from_pot, src/streamer_2d.f90:
@@ -2345,7 +2349,7 @@ __device__ double dist_line(double x, double y, const double r0[2], const double
 // set_ref_flags on every box of levels 1..max_lvl (src/streamer_2d.f90:177-216,
 // cyl :190-227). One warp per box (levels >= 1 have nc = 8: two cells/lane).
 __device__ void ref_flags(const RunDev &R, double time) {
-  for (int id = TID(); id < R.capacity; id += NTH()) R.flags[id] = INT_MIN + 1;
+  for (int id = TID(), nt_ = NTH(); id < R.capacity; id += nt_) R.flags[id] = INT_MIN + 1;
   PSYNC();
   const int *ids;
   int n;
