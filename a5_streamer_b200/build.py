@@ -36,7 +36,8 @@ def sources():
 
 def headers():
     inc = os.path.join(ROOT, "include")
-    return [os.path.join(inc, f) for f in os.listdir(inc) if f.endswith(".h")]
+    return ([os.path.join(inc, f) for f in os.listdir(inc) if f.endswith(".h")]
+            + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))])
 
 
 def needs_build() -> bool:
