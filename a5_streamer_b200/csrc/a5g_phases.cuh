@@ -1374,9 +1374,10 @@ __device__ __noinline__ void p_vcycle<float>(const RunDev &R, const MGV<float> &
 }
 
 // mg$D_fas_fmg, m_aX_mg.f90:163-202. leaf_rhs: compute the space charge of
-// the leaves where it is first needed (compute_fld).
+// the leaves where it is first needed (compute_fld). Inlined into each
+// caller, so that the multigrid variables' descriptor M stays in registers.
 template <class T>
-__device__ void p_fmg_in(const RunDev &R, const MGV<T> &M, bool set_residual, bool first_call,
+__device__ __forceinline__ void p_fmg_in(const RunDev &R, const MGV<T> &M, bool set_residual, bool first_call,
                          bool leaf_rhs) {
   const int min_lvl = R.min_lvl, max_lvl = R.max_lvl;
   if (first_call) {
@@ -1507,28 +1508,43 @@ __device__ void p_set_tags(const RunDev &R) {
 // dielectric run always takes the device-memory path, whose phases apply the
 // eps operators to the boxes tagged dielectric.
 template <class F>
-__device__ __forceinline__ void mg_staged(const RunDev &R, F &&body);
+__device__ __forceinline__ void mg_staged(const RunDev &R, const F &body);
 
-__device__ void p_fmg(const RunDev &R, bool set_residual, bool first_call, bool leaf_rhs) {
-  mg_staged(R, [&](const MGV<double> &M) { p_fmg_in(R, M, set_residual, first_call, leaf_rhs); });
-}
-
+// The solves run by mg_staged, as function objects whose bodies are inlined
+// into both branches (shared-memory and device-memory variables), so that
+// each copy sees its descriptor M as constants.
+struct FmgBody {
+  bool set_residual, first_call, leaf_rhs;
+  __device__ __forceinline__ void operator()(const RunDev &R, const MGV<double> &M) const {
+    p_fmg_in(R, M, set_residual, first_call, leaf_rhs);
+  }
+};
 // mg$D_fas_vcycle(tree, mg, max_lvl, set_residual) on its own
 // (afivo/src/m_aX_mg.f90:208-254): valid potential ghost cells on input and
 // output; with set_residual the residual of levels min..max_lvl in tmp.
-__device__ void p_vcycle_alone(const RunDev &R, int max_lvl, bool set_residual) {
-  mg_staged(R, [&](const MGV<double> &M) {
+struct VcycleBody {
+  int max_lvl;
+  bool set_residual;
+  __device__ __forceinline__ void operator()(const RunDev &R, const MGV<double> &M) const {
     PlanFetch pf;
     p_vcycle(R, M, max_lvl, false, pf, R.max_lvl + 1);
     if (set_residual) p_residual_all(R, M, max_lvl);
     if (pf.li >= 0) cp_async_wait_all();
-  });
+  }
+};
+
+__device__ void p_fmg(const RunDev &R, bool set_residual, bool first_call, bool leaf_rhs) {
+  mg_staged(R, FmgBody{set_residual, first_call, leaf_rhs});
+}
+
+__device__ void p_vcycle_alone(const RunDev &R, int max_lvl, bool set_residual) {
+  mg_staged(R, VcycleBody{max_lvl, set_residual});
 }
 
 // Runs body(M) on the multigrid variables: staged in shared memory when the
 // tree fits, else in device memory (dielectric runs always in device memory).
 template <class F>
-__device__ __forceinline__ void mg_staged(const RunDev &R, F &&body) {
+__device__ __forceinline__ void mg_staged(const RunDev &R, const F &body) {
   if (R.diel || R.has_lsf) p_set_tags(R);
   if (R.smem_doubles > 0 && !R.diel && !R.has_lsf) {
     const int S = R.smem_doubles, nbx = R.bx_off[R.nlev], npb = R.pb_off[R.nlev];
@@ -1546,12 +1562,12 @@ __device__ __forceinline__ void mg_staged(const RunDev &R, F &&body) {
     MGV<double> M{base, base + S, base + 2 * S, sb, spb, true, R.applied_voltage,
                   4, 4, 2 * R.n_cycle_base};
     stage_mg(R, M, VAR(R, MP), VAR(R, MR), VAR(R, MT), true);
-    body(M);
+    body(R, M);
     stage_mg(R, M, VAR(R, MP), VAR(R, MR), VAR(R, MT), false);
   } else {
     MGV<double> M{VAR(R, MP), VAR(R, MR), VAR(R, MT), R.boxes, R.pbx, false, R.applied_voltage,
                   4, 4, 2 * R.n_cycle_base};
-    body(M);
+    body(R, M);
   }
 }
 
