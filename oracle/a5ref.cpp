@@ -19,6 +19,7 @@
 #include <cstdint>
 #include <cstring>
 #include <functional>
+#include <stdexcept>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
@@ -3440,3 +3441,6 @@ double a5ref_kat_lookup(int n_rows, int n_pairs, double x_max, int n_samples) {
 }
 
 }  // extern "C"
+
+// The 3D octree form (uniformly refined octrees), same translation unit.
+#include "a5ref3.inc"

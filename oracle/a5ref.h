@@ -233,6 +233,65 @@ double a5ref_koren_mlim(double a, double b);
  * Returns 0, or -1 if a physical-boundary routine was called. */
 int a5ref_kat_drift_diff(int uniform_lvl, double end_time, int regrid, double *out8);
 
+/* ---------------------------------------------------------------------------
+ * The 3D octree form (src/streamer_3d.f90, afivo's m_a3_* routines) on
+ * uniformly refined octrees: params with dim 3, uniform_lvl >= 1 (every box
+ * below that level refined; the tree is coarsened to 2^3-cell boxes below
+ * level 1), n_base[3] base boxes, epsilon_diel 1 and no photoionization;
+ * a5ref3_create returns NULL for anything else. Refinement-boundary rules
+ * never apply on such a tree. Layouts: cell variables in slots of
+ * (box_size+2)^3 doubles per id (i fastest), faces in slots of
+ * (box_size+1) box_size^2 per id and direction, meta 24 ints per id (in_use,
+ * lvl, ix[3], parent, children[8], neighbors[6], n_cell), geometry 4 doubles
+ * per id (r_min[3], dr). */
+typedef struct a5ref3_sim a5ref3_sim;
+a5ref3_sim *a5ref3_create(const a5ref_params *p);
+void a5ref3_destroy(a5ref3_sim *s);
+/* set_init_cond / compute_fld / refine until uniform_lvl is reached
+ * (src/streamer_3d.f90:55-61); returns #iterations, -1 on failure. */
+int a5ref3_init(a5ref3_sim *s);
+void a5ref3_set_init_cond(a5ref3_sim *s);
+void a5ref3_dt_reductions(a5ref3_sim *s, double out3[3]);
+double a5ref3_get_max_dt(a5ref3_sim *s);
+void a5ref3_step(a5ref3_sim *s, double dt);
+double a5ref3_advance(a5ref3_sim *s);
+double a5ref3_time(a5ref3_sim *s);
+void a5ref3_set_time(a5ref3_sim *s, double t);
+void a5ref3_op_copy_cc(a5ref3_sim *s, int iv_from, int iv_to);
+void a5ref3_op_fluxes_koren(a5ref3_sim *s, double dt);
+void a5ref3_op_update_solution(a5ref3_sim *s, double dt);
+void a5ref3_op_restrict_tree(a5ref3_sim *s, int iv);
+void a5ref3_op_gc_tree(a5ref3_sim *s, int iv);
+void a5ref3_op_average_dens(a5ref3_sim *s);
+void a5ref3_op_set_rhs(a5ref3_sim *s);
+void a5ref3_op_compute_fld(a5ref3_sim *s, int no_guess);
+void a5ref3_op_fmg(a5ref3_sim *s, int set_residual, int first_call);
+void a5ref3_op_vcycle(a5ref3_sim *s, int max_lvl, int set_residual);
+void a5ref3_op_fld_from_pot(a5ref3_sim *s);
+double a5ref3_tree_max_cc(a5ref3_sim *s, int iv);
+double a5ref3_tree_min_cc(a5ref3_sim *s, int iv);
+double a5ref3_applied_voltage(a5ref3_sim *s);
+int a5ref3_max_id(a5ref3_sim *s);
+int a5ref3_max_lvl(a5ref3_sim *s);
+int a5ref3_min_lvl(a5ref3_sim *s);
+long long a5ref3_n_leaf_cells(a5ref3_sim *s);
+void a5ref3_export_meta(a5ref3_sim *s, int *meta24);
+void a5ref3_export_geom(a5ref3_sim *s, double *geom4);
+int a5ref3_export_levels(a5ref3_sim *s, int *counts, int *ids, int cap);
+void a5ref3_export_cc(a5ref3_sim *s, int iv, double *out);
+void a5ref3_import_cc(a5ref3_sim *s, int iv, const double *in);
+void a5ref3_export_fc(a5ref3_sim *s, int dimf, int f, double *out);
+void a5ref3_import_fc(a5ref3_sim *s, int dimf, int f, const double *in);
+void a5ref3_export_table(a5ref3_sim *s, double *rows_cols, double *x_min, double *inv_dx,
+                         int *n_rows);
+/* afivo/examples/multigrid/test_mg2_3d.f90 on a uniform octree of `level`:
+ * max |residual| and max |error| after each of n_fmg FMG cycles. Returns the
+ * finest level, < 0 on failure. */
+int a5ref3_kat_mg(int level, int n_fmg, double *res, double *err);
+/* afivo/examples/transport/test_drift_diff_3d.f90 on a uniform octree of
+ * `level`: out8 as a5ref_kat_drift_diff. */
+int a5ref3_kat_drift_diff(int level, double end_time, double *out8);
+
 #ifdef __cplusplus
 }
 #endif
