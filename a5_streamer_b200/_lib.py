@@ -138,6 +138,42 @@ SIGNATURES = {
 }
 
 
+class Params3(ctypes.Structure):
+    """a5g3_params (include/a5g3.h)."""
+    _fields_ = [
+        ("box_size", ctypes.c_int), ("n_base", ctypes.c_int * 3), ("uniform_lvl", ctypes.c_int),
+        ("n_cycle_base", ctypes.c_int), ("use_drt", ctypes.c_int), ("pad", ctypes.c_int),
+        ("dr_base", ctypes.c_double), ("domain_len_z", ctypes.c_double),
+        ("applied_fld", ctypes.c_double), ("dt_max", ctypes.c_double),
+    ]
+
+
+_PP = ctypes.POINTER(ctypes.c_void_p)
+_LL = ctypes.c_longlong
+SIGNATURES.update({
+    "a5g3_last_error": (ctypes.c_char_p, []),
+    "a5g3_create": (_I, [ctypes.POINTER(Params3), _PP]),
+    "a5g3_destroy": (_I, [_P]),
+    "a5g3_info": (_I, [_P, _PI, _PI, _PI, ctypes.POINTER(_LL)]),
+    "a5g3_export_meta": (_I, [_P, _PI]),
+    "a5g3_export_levels": (_I, [_P, _PI, _PI, _I, _PI]),
+    "a5g3_set_table": (_I, [_P, _I, _I, _D, _D, _PD]),
+    "a5g3_set_init_cond": (_I, [_P, _D, _I, _PD, _PD, _PD, _PD, _PI]),
+    "a5g3_upload_cc": (_I, [_P, _I, _PD]), "a5g3_download_cc": (_I, [_P, _I, _PD]),
+    "a5g3_upload_fc": (_I, [_P, _I, _I, _PD]), "a5g3_download_fc": (_I, [_P, _I, _I, _PD]),
+    "a5g3_tree_copy_cc": (_I, [_P, _I, _I]),
+    "a5g3_fluxes_koren": (_I, [_P, _D]), "a5g3_update_solution": (_I, [_P, _D]),
+    "a5g3_restrict_tree": (_I, [_P, _I]), "a5g3_gc_tree": (_I, [_P, _I]),
+    "a5g3_average_dens": (_I, [_P]), "a5g3_compute_fld": (_I, [_P, _I]),
+    "a5g3_fmg": (_I, [_P, _I, _I]), "a5g3_vcycle": (_I, [_P, _I, _I]),
+    "a5g3_set_rhs": (_I, [_P]), "a5g3_fld_from_pot": (_I, [_P]),
+    "a5g3_tree_max_cc": (_I, [_P, _I, _PD]), "a5g3_tree_min_cc": (_I, [_P, _I, _PD]),
+    "a5g3_dt_reductions": (_I, [_P, _PD]), "a5g3_get_max_dt": (_I, [_P, _PD]),
+    "a5g3_step": (_I, [_P, _D]), "a5g3_sync": (_I, [_P]),
+    "a5g3_stream": (_I, [_P, _PP]),
+})
+
+
 class SimConfig(ctypes.Structure):
     _fields_ = [
         ("dev", Params), ("n_base", ctypes.c_int * 2), ("bg_dens", ctypes.c_double),
@@ -175,3 +211,13 @@ def check(code: int) -> None:
 
 def call(name: str, *args) -> None:
     check(getattr(lib(), name)(*args))
+
+
+def check3(code: int) -> None:
+    if code != A5G_OK:
+        msg = lib().a5g3_last_error()
+        raise A5GError(code, msg.decode() if msg else "")
+
+
+def call3(name: str, *args) -> None:
+    check3(getattr(lib(), name)(*args))

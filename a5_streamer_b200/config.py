@@ -132,8 +132,15 @@ class StreamerConfig:
         return self.dr_base * 0.5 ** (lvl - 1)
 
     def validate(self) -> None:
-        if self.dim != 2:
-            raise ValueError("only dim=2 is implemented")
+        if self.dim not in (2, 3):
+            raise ValueError("dim must be 2 or 3")
+        if self.dim == 3:
+            # the 3D octree form runs on uniformly refined octrees
+            # (include/a5g3.h): Cartesian, eps = 1, no photoionization
+            if self.coord != "xyz" or self.uniform_lvl < 1:
+                raise ValueError("the 3D form needs coord 'xyz' and a uniform mesh (uniform_lvl >= 1)")
+            if self.photoi_enabled or self.epsilon_diel != 1.0:
+                raise ValueError("the 3D form has no photoionization and no dielectric")
         if self.coord not in ("xyz", "cyl"):
             raise ValueError(f"coord must be 'xyz' or 'cyl', got {self.coord!r}")
         nc = self.box_size
@@ -141,9 +148,10 @@ class StreamerConfig:
             raise ValueError("box_size must be a power of two >= 4")
         if len(self.n_base) != self.dim or len(self.domain_len) != self.dim:
             raise ValueError("n_base and domain_len need one entry per dimension")
-        dy = self.domain_len[1] / (self.n_base[1] * nc)
-        if abs(dy - self.dr_base) > 1e-12 * self.dr_base:
-            raise ValueError("base cells must be square: domain_len / n_base must agree")
+        for d in range(1, self.dim):
+            dy = self.domain_len[d] / (self.n_base[d] * nc)
+            if abs(dy - self.dr_base) > 1e-12 * self.dr_base:
+                raise ValueError("base cells must be square: domain_len / n_base must agree")
         if len(self.seeds) > 8:
             raise ValueError("at most 8 seeds")
         for name in TD_COLUMNS:
@@ -218,6 +226,27 @@ def cartesian_uniform(level: int = 6, **overrides) -> StreamerConfig:
     list of level lvls_max (afivo/src/m_aX_core.f90:495-532), so boxes there
     would take no transport update."""
     return cartesian_8mm(lvls_max=level + 1, uniform_lvl=level, **overrides)
+
+
+def cube_16mm_uniform(level: int = 5, **overrides) -> StreamerConfig:
+    """The 3D case on a uniformly refined octree: a 16 mm cube of one base
+    box (8^3 cells, base dx 2 mm) refined to the given level (dx = 2 mm /
+    2^(level-1): 125 um and 2,097,152 leaf cells at level 5, 62.5 um and
+    16,777,216 at level 6), E_bg = 2e6 V/m along z, background 1e15 m^-3, two
+    Gaussian seeds of 1e19 m^-3 and sigma 0.3 mm at (8, 6.5, 14) mm and
+    (8, 9.5, 14) mm, synthetic transport with attachment, no
+    photoionization, t_end = 8 ns. The streamer's own refinement criterion
+    would refine further near the seeds; on this mesh every level is
+    complete."""
+    sigma = 0.3e-3
+    seeds = [Seed(r0=(8e-3, y, 14e-3), r1=(8e-3, y, 14e-3), dens=1e19, width=math.sqrt(2.0) * sigma,
+                  falloff=2) for y in (6.5e-3, 9.5e-3)]
+    cfg = StreamerConfig(
+        dim=3, coord="xyz", box_size=8, n_base=(1, 1, 1), domain_len=(16e-3, 16e-3, 16e-3),
+        lvls_max=level + 1, uniform_lvl=level, applied_fld=2.0e6, epsilon_diel=1.0, bg_dens=1e15,
+        seeds=seeds, dt_max=1e-10, num_steps_amr=2, end_time=8e-9, use_drt=True,
+        lkptbl_size=200, lkptbl_max_fld=3e7, td=synthetic_transport(eta_a=1.0e3, eta_b=4e6))
+    return dataclasses.replace(cfg, **overrides)
 
 
 def cylindrical_16mm(photoi: bool = False, **overrides) -> StreamerConfig:

@@ -1,0 +1,1398 @@
+// a5g3 -- the 3D octree form of the device path on sm_100a (see
+// include/a5g3.h): uniformly refined octrees of 8^3-cell boxes resident in
+// HBM, one kernel per phase over a level's (or the leaves') box list, one
+// thread block per box, the whole time step replayed from a CUDA graph.
+//
+// Arithmetic follows the reference expression by expression (compiled with
+// --fmad=false, so every multiply and add is rounded on its own) and gives
+// the same doubles as the CPU restatement of src/streamer_3d.f90 and afivo's
+// m_a3_* routines.
+//
+// Memory layout in HBM: cell variable iv of box id is the slot
+// cc[iv][id][(nc+2)^3] of SLOT3 = (box_size+2)^3 doubles (i fastest, then j,
+// k); face variable f of direction d is fc[d][f][id][FSLOT3]. Box ids index
+// slots directly. A box is one thread block: its slot is 8 KB of contiguous
+// doubles per variable, read with coalesced loads.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "a5g3.h"
+
+namespace {
+
+constexpr int NC3 = 8;                                  // box_size on levels >= 1
+constexpr int G3 = NC3 + 2;
+constexpr int SLOT3 = G3 * G3 * G3;                     // 1000 doubles
+constexpr int FSLOT3 = (NC3 + 1) * NC3 * NC3;           // 576 doubles
+constexpr int NV3 = A5G_N_VAR_CELL, NF3 = A5G_N_VAR_FACE;
+enum { I_ELEC = 0, I_PION, I_ELEC_OLD, I_PION_OLD, I_PHI, I_FLD, I_RHS, I_PHO, I_EPS };
+enum { F_ELEC = 0, F_FLD };
+enum { C_MOB = 0, C_DIF, C_ALPHA, C_ETA };
+constexpr int NTH3 = 256;                               // threads per box block
+constexpr double UC_EPS0 = 8.8541878176e-12;            // fosito/m_units_constants.f90:201
+constexpr double UC_ELEM_CHARGE = 1.6022e-19;           // :202
+
+// Device view of one run, passed by value to every kernel.
+struct Run3 {
+  double *cc;          // NV3 variables x cap slots
+  double *fc;          // 3 directions x NF3 variables x cap face slots
+  const int *nc;       // [cap] cells per box edge
+  const int *nbr;      // [cap][6] neighbours (lx hx ly hy lz hz), < 0 physical
+  const int *chl;      // [cap][8] children
+  const int *par;      // [cap] parent
+  const int *off;      // [cap][3] offset of the box's cells in its parent (child offset)
+  const double *geo;   // [cap][4] r_min[3], dr
+  const double *lt;    // transport table, rows x 4, column-major
+  double *scal;        // device scalars (S_*)
+  double *part;        // per-block partial reductions
+  long long cap;       // slots (max_id + 1)
+  int lt_rows;
+  double lt_xmin, lt_inv_dx;
+  double voltage;      // applied potential at the high-z wall
+};
+enum { S_DT = 0, S_RED = 1 };  // scal[0] dt; scal[1..3] reductions; scal[4] tree max/min
+
+__device__ __forceinline__ double *VAR(const Run3 &R, int iv) { return R.cc + (size_t)iv * R.cap * SLOT3; }
+__device__ __forceinline__ double *CC(const Run3 &R, int iv, int id) {
+  return R.cc + ((size_t)iv * R.cap + id) * SLOT3;
+}
+__device__ __forceinline__ double *FC(const Run3 &R, int d, int f, int id) {
+  return R.fc + (((size_t)d * NF3 + f) * R.cap + id) * FSLOT3;
+}
+__device__ __forceinline__ int ix3(int g, int i, int j, int k) { return i + g * (j + g * k); }
+
+// fosito/m_lookup_table.f90:107-125 (get_loc, ceiling of the fractional
+// index; beyond the int range clamped to the table end) and :154-161
+struct Loc3 {
+  int ix;
+  double fr;
+};
+__device__ __forceinline__ Loc3 lt_loc(const Run3 &R, double x) {
+  const double frac = (x - R.lt_xmin) * R.lt_inv_dx;
+  Loc3 l;
+  if (frac < 2.0e9 && frac > -2.0e9) {
+    l.ix = (int)ceil(frac);
+    l.fr = l.ix - frac;
+  } else {
+    l.ix = frac > 0 ? R.lt_rows : 0;
+    l.fr = 0;
+  }
+  if (l.ix < 1) {
+    l.ix = 1;
+    l.fr = 1;
+  } else if (l.ix >= R.lt_rows) {
+    l.ix = R.lt_rows - 1;
+    l.fr = 0;
+  }
+  return l;
+}
+__device__ __forceinline__ double lt_col(const Run3 &R, int col, const Loc3 &l) {
+  const double *c = R.lt + (size_t)R.lt_rows * col;
+  return l.fr * c[l.ix - 1] + (1 - l.fr) * c[l.ix];
+}
+
+// src/m_streamer.f90:339-362 (koren_mlim)
+__device__ __forceinline__ double koren_mlim(double a, double b) {
+  const double sixth = 1 / 6.0;
+  const double aa = a * a, ab = a * b;
+  if (ab <= 0) return 0;
+  if (aa <= 0.25 * ab) return a;
+  if (aa <= 2.5 * ab) return sixth * (b + 2 * a);
+  return b;
+}
+
+// gfortran's NORM2 of a 3-vector: scaled sum of squares, the scale raised
+// whenever a larger |x| appears
+__device__ __forceinline__ double norm2_3(const double x[3]) {
+  double scale = 0.0, ssq = 1.0;
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    if (x[k] != 0.0) {
+      const double ax = fabs(x[k]);
+      if (scale < ax) {
+        const double v = scale / ax;
+        ssq = 1.0 + ssq * v * v;
+        scale = ax;
+      } else {
+        const double v = ax / scale;
+        ssq += v * v;
+      }
+    }
+  }
+  return scale * sqrt(ssq);
+}
+
+// ---------------------------------------------------------------------------
+// a3_tree_copy_cc for two variable pairs at once (elec -> elec_old, pion ->
+// pion_old at the start of a step); whole slots, two doubles per thread.
+__global__ void k3_copy2(Run3 R, int a0, int b0, int a1, int b1) {
+  const size_t n2 = (size_t)R.cap * SLOT3 / 2;
+  const double2 *s0 = reinterpret_cast<const double2 *>(VAR(R, a0));
+  const double2 *s1 = reinterpret_cast<const double2 *>(VAR(R, a1));
+  double2 *d0 = reinterpret_cast<double2 *>(VAR(R, b0));
+  double2 *d1 = reinterpret_cast<double2 *>(VAR(R, b1));
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n2; k += (size_t)gridDim.x * blockDim.x) {
+    const double2 x = s0[k];
+    d0[k] = x;
+    if (a1 >= 0) d1[k] = s1[k];
+  }
+}
+
+// average_dens (src/streamer_3d.f90:557-563): x = 0.5 (x + x_old) for n_e
+// and n_i, whole slots.
+__global__ void k3_average(Run3 R) {
+  const size_t n = (size_t)R.cap * SLOT3;
+  double *e = VAR(R, I_ELEC), *p = VAR(R, I_PION);
+  const double *eo = VAR(R, I_ELEC_OLD), *po = VAR(R, I_PION_OLD);
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    e[k] = 0.5 * (e[k] + eo[k]);
+    p[k] = 0.5 * (p[k] + po[k]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// fluxes_koren (src/streamer_3d.f90:396-554) on one leaf box per block: the
+// box's n_e and |E| slots staged in shared memory (coalesced), the second
+// ghost layer (a3_gc2_box with sides2_from_nb / a3_gc2_neumann,
+// afivo/src/m_aX_gc.f90:407-483, 588-622) read from the neighbour's slot or
+// the box's own, then every x, y and z face of the box (3 (nc+1) nc^2).
+__global__ void __launch_bounds__(NTH3) k3_fluxes(Run3 R, const int *ids) {
+  __shared__ double se[SLOT3], sf[SLOT3];
+  const int id = ids[blockIdx.x];
+  const int nc = R.nc[id], g = nc + 2, gs = g * g * g;
+  {
+    const double *e = CC(R, I_ELEC, id), *f = CC(R, I_FLD, id);
+    for (int k = threadIdx.x; k < gs; k += NTH3) {
+      se[k] = e[k];
+      sf[k] = f[k];
+    }
+  }
+  __syncthreads();
+  const double dt = R.scal[S_DT];
+  const double inv_dr = 1 / R.geo[4 * id + 3];
+  const double fac = -0.8 * UC_EPS0 / (UC_ELEM_CHARGE * dt);
+  const int *nb = R.nbr + 6 * id;
+  const int F = (nc + 1) * nc * nc;
+  for (int q = threadIdx.x; q < 3 * F; q += NTH3) {
+    const int d = q / F, r = q - d * F;
+    int i, j, k;
+    if (d == 0) {
+      i = r % (nc + 1) + 1;
+      j = (r / (nc + 1)) % nc + 1;
+      k = r / ((nc + 1) * nc) + 1;
+    } else if (d == 1) {
+      i = r % nc + 1;
+      j = (r / nc) % (nc + 1) + 1;
+      k = r / (nc * (nc + 1)) + 1;
+    } else {
+      i = r % nc + 1;
+      j = (r / nc) % nc + 1;
+      k = r / (nc * nc) + 1;
+    }
+    // position along the face normal and the cell strides
+    const int a = d == 0 ? i : d == 1 ? j : k;
+    const int st = d == 0 ? 1 : d == 1 ? g : g * g;
+    const int c0 = ix3(g, i, j, k), cm1 = c0 - st;
+    const double e0 = se[c0], em1 = se[cm1];
+    double em2, ep1;
+    // second ghost layer where the stencil leaves the box (a == 1 / nc + 1)
+    if (a == 1) {
+      const int n = nb[2 * d];
+      // c0 is cell 1: the neighbour's cell nc - 1, or own cell 2
+      em2 = n > 0 ? CC(R, I_ELEC, n)[c0 + (nc - 2) * st] : se[c0 + st];
+    } else {
+      em2 = se[c0 - 2 * st];
+    }
+    if (a == nc + 1) {
+      const int n = nb[2 * d + 1];
+      // c0 is the ghost cell nc + 1: the neighbour's cell 2, or own cell nc - 1
+      ep1 = n > 0 ? CC(R, I_ELEC, n)[c0 - (nc - 1) * st] : se[c0 - 2 * st];
+    } else {
+      ep1 = se[c0 + st];
+    }
+    const double fld_avg = 0.5 * (sf[c0] + sf[cm1]);
+    const Loc3 loc = lt_loc(R, fld_avg);
+    const double mobility = lt_col(R, C_MOB, loc);
+    const double diff_coeff = lt_col(R, C_DIF, loc);
+    double *fe = FC(R, d, F_ELEC, id);
+    const double fld = FC(R, d, F_FLD, id)[r];
+    const double v_drift = -mobility * fld;
+    const double gradc = e0 - em1;
+    double out;
+    if (v_drift < 0.0) {
+      const double gradn = ep1 - e0;
+      out = v_drift * (e0 - koren_mlim(gradc, gradn));
+      if (out < fac * fld) out = fac * fld;
+    } else {
+      const double gradp = em1 - em2;
+      out = v_drift * (em1 + koren_mlim(gradc, gradp));
+      if (out > fac * fld) out = fac * fld;
+    }
+    fe[r] = out - diff_coeff * gradc * inv_dr;
+  }
+}
+
+// update_solution (src/streamer_3d.f90:566-615) on one leaf box per block,
+// one interior cell per thread and round; then the dielectric conversion
+// (eps > 1: n_e moves into n_i).
+__global__ void __launch_bounds__(NTH3) k3_update(Run3 R, const int *ids) {
+  const int id = ids[blockIdx.x];
+  const int nc = R.nc[id], g = nc + 2, n = nc * nc * nc;
+  const double dt = R.scal[S_DT];
+  const double inv_dr = 1 / R.geo[4 * id + 3];
+  const double *fx = FC(R, 0, F_ELEC, id), *fy = FC(R, 1, F_ELEC, id), *fz = FC(R, 2, F_ELEC, id);
+  double *e = CC(R, I_ELEC, id), *p = CC(R, I_PION, id);
+  const double *fld = CC(R, I_FLD, id), *eps = CC(R, I_EPS, id);
+  for (int t = threadIdx.x; t < n; t += NTH3) {
+    const int i = t % nc + 1, j = (t / nc) % nc + 1, k = t / (nc * nc) + 1;
+    const int c = ix3(g, i, j, k);
+    const Loc3 loc = lt_loc(R, fld[c]);
+    const double alpha = lt_col(R, C_ALPHA, loc), eta = lt_col(R, C_ETA, loc);
+    const int xl = (i - 1) + (nc + 1) * ((j - 1) + nc * (k - 1));
+    const int yl = (i - 1) + nc * ((j - 1) + (nc + 1) * (k - 1));
+    const int zl = (i - 1) + nc * ((j - 1) + nc * (k - 1));
+    const double x0 = fx[xl], x1 = fx[xl + 1], y0 = fy[yl], y1 = fy[yl + nc], z0 = fz[zl], z1 = fz[zl + nc * nc];
+    double dflux[3];
+    dflux[0] = x0 + x1;
+    dflux[1] = y0 + y1;
+    dflux[2] = z0 + z1;
+    const double src = 0.5 * norm2_3(dflux) * (alpha - eta);
+    double sflux = x0 - x1;
+    sflux = sflux + y0;
+    sflux = sflux - y1;
+    sflux = sflux + z0;
+    sflux = sflux - z1;
+    sflux = sflux * inv_dr;
+    double ev = e[c] + (src + sflux) * dt;
+    double pv = p[c] + src * dt;
+    if (eps[c] > 1.0) {
+      pv = pv - ev;
+      ev = 0;
+    }
+    e[c] = ev;
+    p[c] = pv;
+  }
+}
+
+// a3_restrict_box (afivo/src/m_aX_restrict.f90:67-142, 3D) from every box of
+// a level to its parent, for up to two variables: each parent cell is 0.125
+// times the sum of its eight child cells in column-major order. One block per
+// child box; the child's cells land in its octant of the parent (child
+// offset), so the blocks write disjoint parent cells.
+__global__ void __launch_bounds__(NTH3) k3_restrict(Run3 R, const int *ids, int iv0, int iv1) {
+  const int id = ids[blockIdx.x];
+  const int nc = R.nc[id], g = nc + 2, hnc = nc >> 1, nh = hnc * hnc * hnc;
+  const int p = R.par[id];
+  const int pg = R.nc[p] + 2;
+  const int *o = R.off + 3 * id;
+  for (int t = threadIdx.x; t < 2 * nh; t += NTH3) {
+    const int iv = t < nh ? iv0 : iv1;
+    if (iv < 0) continue;
+    const int u = t < nh ? t : t - nh;
+    const int i = u % hnc + 1, j = (u / hnc) % hnc + 1, k = u / (hnc * hnc) + 1;
+    const double *c = CC(R, iv, id);
+    const int f = ix3(g, 2 * i - 1, 2 * j - 1, 2 * k - 1);
+    double s = c[f];
+    s = s + c[f + 1];
+    s = s + c[f + g];
+    s = s + c[f + g + 1];
+    s = s + c[f + g * g];
+    s = s + c[f + g * g + 1];
+    s = s + c[f + g * g + g];
+    s = s + c[f + g * g + g + 1];
+    CC(R, iv, p)[ix3(pg, o[0] + i, o[1] + j, o[2] + k)] = 0.125 * s;
+  }
+}
+
+// Ghost cells of the boxes in ids for up to two variables (a3_gc_box,
+// afivo/src/m_aX_gc.f90:50-68): the facing layer of a same-level neighbour
+// (sides_from_nb, :368-402), or on a physical side the box's own first
+// layer: Neumann (a3_gc_neumann, :298-330), or for the potential with
+// bc = 1 sides_bc_pot (src/streamer_3d.f90:693-715): Neumann on x and y,
+// -phi at low z, 2 V - phi at high z.
+__global__ void __launch_bounds__(NTH3) k3_gc(Run3 R, const int *ids, int iv0, int iv1, int bc) {
+  const int id = ids[blockIdx.x];
+  const int nc = R.nc[id], g = nc + 2, per = nc * nc;
+  const int *nb = R.nbr + 6 * id;
+  for (int t = threadIdx.x; t < 12 * per; t += NTH3) {
+    const int iv = t < 6 * per ? iv0 : iv1;
+    if (iv < 0) continue;
+    const int u = t < 6 * per ? t : t - 6 * per;
+    const int side = u / per, w = u - side * per;
+    const int a = w % nc + 1, b = w / nc + 1;
+    const int d = side >> 1;
+    const bool low = (side & 1) == 0;
+    const int st = d == 0 ? 1 : d == 1 ? g : g * g;
+    // the ghost cell and the box's own first cell on that side
+    int gcell;
+    if (d == 0) gcell = ix3(g, low ? 0 : nc + 1, a, b);
+    else if (d == 1) gcell = ix3(g, a, low ? 0 : nc + 1, b);
+    else gcell = ix3(g, a, b, low ? 0 : nc + 1);
+    const int own = low ? gcell + st : gcell - st;
+    double *x = CC(R, iv, id);
+    const int n = nb[side];
+    double v;
+    if (n > 0) {
+      // the neighbour's cell nc (low side) or 1 (high side)
+      v = CC(R, iv, n)[low ? gcell + nc * st : gcell - nc * st];
+    } else if (bc == 1 && side == 4) {
+      v = -x[own];
+    } else if (bc == 1 && side == 5) {
+      v = 2 * R.voltage - x[own];
+    } else {
+      v = x[own];
+    }
+    x[gcell] = v;
+  }
+}
+
+// set_init_cond and set_box_eps (src/streamer_3d.f90:217-270) on every cell
+// of every box (ghost cells included): background plus seeds
+// (GM_dens_line, src/m_geom.f90:29-111), n_i = n_e, phi = 0, eps = 1.
+struct Seeds3 {
+  int n;
+  double bg;
+  double r0[8][3], r1[8][3], dens[8], width[8];
+  int falloff[8];
+};
+__device__ double dist_line3(const double r[3], const double *r0, const double *r1) {
+  double line_len2 = 0, temp = 0;
+  for (int d = 0; d < 3; d++) line_len2 += (r1[d] - r0[d]) * (r1[d] - r0[d]);
+  for (int d = 0; d < 3; d++) temp += (r[d] - r0[d]) * (r1[d] - r0[d]);
+  double v[3];
+  if (temp <= 0.0) {
+    for (int d = 0; d < 3; d++) v[d] = r[d] - r0[d];
+  } else if (temp >= line_len2) {
+    for (int d = 0; d < 3; d++) v[d] = r[d] - r1[d];
+  } else {
+    for (int d = 0; d < 3; d++) v[d] = r[d] - (r0[d] + temp / line_len2 * (r1[d] - r0[d]));
+  }
+  return norm2_3(v);
+}
+__device__ double dens_line3(const double r[3], const double *r0, const double *r1, double width, int falloff) {
+  const double dist = dist_line3(r, r0, r1);
+  switch (falloff) {
+    case 1: {
+      const double tmp = dist / width;
+      if (tmp > log(0.5 * 1.7976931348623157e308)) return 0;
+      return 2 / (1 + exp(tmp));
+    }
+    case 2: {
+      const double x = dist / width;
+      return exp(-(x * x));
+    }
+    case 3: {
+      if (dist < width) return 1;
+      if (dist < 2 * width) {
+        const double temp = dist / width - 1;
+        return (1 - (3 * (temp * temp) - 2 * (temp * temp * temp)));
+      }
+      return 0.0;
+    }
+    case 4: return dist < width ? 1.0 : 0.0;
+    default: return 0;
+  }
+}
+__global__ void __launch_bounds__(NTH3) k3_init(Run3 R, const int *ids, Seeds3 S) {
+  const int id = ids[blockIdx.x];
+  const int nc = R.nc[id], g = nc + 2, gs = g * g * g;
+  const double *geo = R.geo + 4 * id;
+  double *e = CC(R, I_ELEC, id), *p = CC(R, I_PION, id), *phi = CC(R, I_PHI, id), *eps = CC(R, I_EPS, id);
+  for (int t = threadIdx.x; t < gs; t += NTH3) {
+    const int i = t % g, j = (t / g) % g, k = t / (g * g);
+    const double xyz[3] = {geo[0] + (i - 0.5) * geo[3], geo[1] + (j - 0.5) * geo[3], geo[2] + (k - 0.5) * geo[3]};
+    double v = S.bg;
+    for (int s = 0; s < S.n; s++) v = v + S.dens[s] * dens_line3(xyz, S.r0[s], S.r1[s], S.width[s], S.falloff[s]);
+    e[t] = v;
+    p[t] = v;
+    phi[t] = 0;
+    eps[t] = 1.0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Multigrid (afivo/src/m_aX_mg.f90, 3D Laplacian operators lpl).
+
+// One red-black Gauss-Seidel half-sweep `it` of mg3_box_gsrb_lpl (:769-811)
+// on every box of a level: the cells with (i + j + k + it) even, phi =
+// sixth (sum of the six neighbours - dx^2 rhs). A neighbour outside the box
+// is evaluated from its source, which equals the ghost fill gsrb_boxes
+// performs after every half-sweep (:403-426): the facing cell of the
+// same-level neighbour (of the colour not updated here) or, on a physical
+// side, sides_bc_pot of the cell itself (read before it is written). mem:
+// read the ghost cells in memory instead (the first half-sweep on the base
+// level of a first FMG call, whose ghosts the reference leaves as they were).
+__global__ void __launch_bounds__(NTH3) k3_sweep(Run3 R, const int *ids, int it, int mem) {
+  const int id = ids[blockIdx.x];
+  const int nc = R.nc[id], g = nc + 2, hn = nc >> 1, half = nc * nc * hn;
+  const double dr = R.geo[4 * id + 3], dx2 = dr * dr;
+  const double sixth = 1 / 6.0;
+  double *phi = CC(R, I_PHI, id);
+  const double *rhs = CC(R, I_RHS, id);
+  const int *nb = R.nbr + 6 * id;
+  for (int t = threadIdx.x; t < half; t += NTH3) {
+    const int k = t / (nc * hn) + 1, rem = t - (k - 1) * nc * hn;
+    const int j = rem / hn + 1, m = rem - (j - 1) * hn;
+    const int i = 2 - ((it + j + k) & 1) + 2 * m;
+    const int c = ix3(g, i, j, k);
+    const int pos[3] = {i, j, k}, st[3] = {1, g, g * g};
+    double v[6];
+#pragma unroll
+    for (int s = 0; s < 6; s++) {
+      const int d = s >> 1;
+      const bool hi = s & 1;
+      const int a = pos[d] + (hi ? 1 : -1);
+      const int cn = hi ? c + st[d] : c - st[d];
+      if (mem || (a >= 1 && a <= nc)) {
+        v[s] = phi[cn];
+      } else {
+        const int n = nb[s];
+        if (n > 0) v[s] = CC(R, I_PHI, n)[hi ? cn - nc * st[d] : cn + nc * st[d]];
+        else if (s == 4) v[s] = -phi[c];
+        else if (s == 5) v[s] = 2 * R.voltage - phi[c];
+        else v[s] = phi[c];
+      }
+    }
+    double sum = v[1] + v[0];
+    sum = sum + v[3];
+    sum = sum + v[2];
+    sum = sum + v[5];
+    sum = sum + v[4];
+    phi[c] = sixth * (sum - dx2 * rhs[c]);
+  }
+}
+
+// mg3_box_lpl (:814-848) at interior cell c of a box's phi slot
+__device__ __forceinline__ double lpl3(const double *phi, int c, int g, double inv_dr_sq) {
+  double s = phi[c - 1] + phi[c + 1];
+  s = s + phi[c - g];
+  s = s + phi[c + g];
+  s = s + phi[c - g * g];
+  s = s + phi[c + g * g];
+  return inv_dr_sq * (s - 6 * phi[c]);
+}
+
+// update_coarse / set_coarse_phi_rhs, fine part (:430-523): the residual
+// rhs - lpl(phi) of each box of a level (residual_box, :551-565), restricted
+// with phi to the parent (mg3_box_rstr_lpl, :851-893): parent tmp = mean of
+// the eight residuals, parent phi = mean of the eight phi (column-major
+// sums). The box's own tmp is left as it was (update_coarse restores it;
+// set_coarse_phi_rhs's copy there is overwritten before any read). Four
+// boxes per block, one parent cell per thread.
+__global__ void __launch_bounds__(NTH3) k3_resid_restrict(Run3 R, const int *ids, int n) {
+  const int b = blockIdx.x * 4 + (threadIdx.x >> 6);
+  if (b >= n) return;
+  const int id = ids[b];
+  const int nc = R.nc[id], g = nc + 2, hnc = nc >> 1, nh = hnc * hnc * hnc;
+  const int u = threadIdx.x & 63;
+  if (u >= nh) return;
+  const int i = u % hnc + 1, j = (u / hnc) % hnc + 1, k = u / (hnc * hnc) + 1;
+  const double dr = R.geo[4 * id + 3], inv_dr_sq = 1 / (dr * dr);
+  const double *phi = CC(R, I_PHI, id), *rhs = CC(R, I_RHS, id);
+  const int f = ix3(g, 2 * i - 1, 2 * j - 1, 2 * k - 1);
+  const int o8[8] = {0, 1, g, g + 1, g * g, g * g + 1, g * g + g, g * g + g + 1};
+  double sr = 0, sp = 0;
+#pragma unroll
+  for (int q = 0; q < 8; q++) {
+    const int c = f + o8[q];
+    const double r = rhs[c] - lpl3(phi, c, g, inv_dr_sq);
+    sr = q == 0 ? r : sr + r;
+    sp = q == 0 ? phi[c] : sp + phi[c];
+  }
+  const int p = R.par[id], pg = R.nc[p] + 2;
+  const int *o = R.off + 3 * id;
+  const int pc = ix3(pg, o[0] + i, o[1] + j, o[2] + k);
+  CC(R, I_FLD, p)[pc] = 0.125 * sr;
+  CC(R, I_PHI, p)[pc] = 0.125 * sp;
+}
+
+// Coarse part of update_coarse / set_coarse_phi_rhs (:471-485, :514-521) on
+// the parent boxes of a level: rhs = lpl(phi) on interior cells, then rhs =
+// rhs + tmp on the whole slot (a3_box_add_cc), then with copy tmp = phi
+// (a3_box_copy_cc). One slot element per thread.
+__global__ void __launch_bounds__(NTH3) k3_coarse_rhs(Run3 R, const int *ids, int copy) {
+  const int id = ids[blockIdx.x];
+  const int nc = R.nc[id], g = nc + 2, gs = g * g * g;
+  const double dr = R.geo[4 * id + 3], inv_dr_sq = 1 / (dr * dr);
+  const double *phi = CC(R, I_PHI, id);
+  double *rhs = CC(R, I_RHS, id), *tmp = CC(R, I_FLD, id);
+  for (int c = threadIdx.x; c < gs; c += NTH3) {
+    const int i = c % g, j = (c / g) % g, k = c / (g * g);
+    const bool in = i >= 1 && i <= nc && j >= 1 && j <= nc && k >= 1 && k <= nc;
+    const double a = in ? lpl3(phi, c, g, inv_dr_sq) : rhs[c];
+    rhs[c] = a + tmp[c];
+    if (copy) tmp[c] = phi[c];
+  }
+}
+
+// correct_children (:374-401): on each parent box tmp = phi - tmp (whole
+// slot) ...
+__global__ void __launch_bounds__(NTH3) k3_corr_diff(Run3 R, const int *ids) {
+  const int id = ids[blockIdx.x];
+  const int g = R.nc[id] + 2, gs = g * g * g;
+  const double *phi = CC(R, I_PHI, id);
+  double *tmp = CC(R, I_FLD, id);
+  for (int c = threadIdx.x; c < gs; c += NTH3) tmp[c] = phi[c] - tmp[c];
+}
+
+// ... then mg3_box_corr_lpl (:714-766) on each child: phi += 0.25 (c1 + c2x
+// + c2y + c2z) of the parent's correction, c1 the closest coarse cell.
+__global__ void __launch_bounds__(NTH3) k3_correct(Run3 R, const int *ids) {
+  const int id = ids[blockIdx.x];
+  const int nc = R.nc[id], g = nc + 2, n = nc * nc * nc;
+  const int p = R.par[id], pg = R.nc[p] + 2;
+  const int *o = R.off + 3 * id;
+  const double *corr = CC(R, I_FLD, p);
+  double *phi = CC(R, I_PHI, id);
+  for (int t = threadIdx.x; t < n; t += NTH3) {
+    const int i = t % nc + 1, j = (t / nc) % nc + 1, k = t / (nc * nc) + 1;
+    const int i1 = o[0] + ((i + 1) >> 1), i2 = i1 + 1 - 2 * (i & 1);
+    const int j1 = o[1] + ((j + 1) >> 1), j2 = j1 + 1 - 2 * (j & 1);
+    const int k1 = o[2] + ((k + 1) >> 1), k2 = k1 + 1 - 2 * (k & 1);
+    double s = corr[ix3(pg, i1, j1, k1)] + corr[ix3(pg, i2, j1, k1)];
+    s = s + corr[ix3(pg, i1, j2, k1)];
+    s = s + corr[ix3(pg, i1, j1, k2)];
+    const int c = ix3(g, i, j, k);
+    phi[c] = phi[c] + 0.25 * s;
+  }
+}
+
+// a3_boxes_copy_cc (whole slots) for the boxes of a list
+__global__ void __launch_bounds__(NTH3) k3_copy_boxes(Run3 R, const int *ids, int from, int to) {
+  const int id = ids[blockIdx.x];
+  const int g = R.nc[id] + 2, gs = g * g * g;
+  const double *a = CC(R, from, id);
+  double *b = CC(R, to, id);
+  for (int c = threadIdx.x; c < gs; c += NTH3) b[c] = a[c];
+}
+
+// init_phi_rhs (:526-549) for one level: phi = 0 on each box's slot and its
+// rhs restricted to the parent.
+__global__ void __launch_bounds__(NTH3) k3_init_phi_rhs(Run3 R, const int *ids) {
+  const int id = ids[blockIdx.x];
+  const int nc = R.nc[id], g = nc + 2, gs = g * g * g, hnc = nc >> 1, nh = hnc * hnc * hnc;
+  double *phi = CC(R, I_PHI, id);
+  for (int c = threadIdx.x; c < gs; c += NTH3) phi[c] = 0.0;
+  const double *rhs = CC(R, I_RHS, id);
+  const int p = R.par[id], pg = R.nc[p] + 2;
+  const int *o = R.off + 3 * id;
+  for (int u = threadIdx.x; u < nh; u += NTH3) {
+    const int i = u % hnc + 1, j = (u / hnc) % hnc + 1, k = u / (hnc * hnc) + 1;
+    const int f = ix3(g, 2 * i - 1, 2 * j - 1, 2 * k - 1);
+    double s = rhs[f];
+    s = s + rhs[f + 1];
+    s = s + rhs[f + g];
+    s = s + rhs[f + g + 1];
+    s = s + rhs[f + g * g];
+    s = s + rhs[f + g * g + 1];
+    s = s + rhs[f + g * g + g];
+    s = s + rhs[f + g * g + g + 1];
+    CC(R, I_RHS, p)[ix3(pg, o[0] + i, o[1] + j, o[2] + k)] = 0.125 * s;
+  }
+}
+
+// residual_box (:551-565) on the boxes of a level: tmp = rhs - lpl(phi)
+__global__ void __launch_bounds__(NTH3) k3_residual(Run3 R, const int *ids) {
+  const int id = ids[blockIdx.x];
+  const int nc = R.nc[id], g = nc + 2, n = nc * nc * nc;
+  const double dr = R.geo[4 * id + 3], inv_dr_sq = 1 / (dr * dr);
+  const double *phi = CC(R, I_PHI, id), *rhs = CC(R, I_RHS, id);
+  double *tmp = CC(R, I_FLD, id);
+  for (int t = threadIdx.x; t < n; t += NTH3) {
+    const int c = ix3(g, t % nc + 1, (t / nc) % nc + 1, t / (nc * nc) + 1);
+    tmp[c] = rhs[c] - lpl3(phi, c, g, inv_dr_sq);
+  }
+}
+
+// compute_fld's space charge (src/streamer_3d.f90:317-329): rhs = e/eps0
+// (n_e - n_i) on whole slots of the leaves of levels >= 1
+__global__ void __launch_bounds__(NTH3) k3_set_rhs(Run3 R, const int *ids) {
+  const int id = ids[blockIdx.x];
+  const int g = R.nc[id] + 2, gs = g * g * g;
+  const double fac = UC_ELEM_CHARGE / UC_EPS0;
+  const double *e = CC(R, I_ELEC, id), *p = CC(R, I_PION, id);
+  double *rhs = CC(R, I_RHS, id);
+  for (int c = threadIdx.x; c < gs; c += NTH3) rhs[c] = fac * (e[c] - p[c]);
+}
+
+// fld_from_pot (src/streamer_3d.f90:348-393) on every box: the face fields
+// (eps-weighted on the box-edge faces) into the F_FLD slots and shared
+// memory, then |E| = 0.5 sqrt(sx^2 + sy^2 + sz^2) per interior cell.
+__global__ void __launch_bounds__(NTH3) k3_fld(Run3 R, const int *ids) {
+  __shared__ double sfc[3 * FSLOT3];
+  const int id = ids[blockIdx.x];
+  const int nc = R.nc[id], g = nc + 2, F = (nc + 1) * nc * nc;
+  const double inv_dr = 1 / R.geo[4 * id + 3];
+  const double *phi = CC(R, I_PHI, id), *eps = CC(R, I_EPS, id);
+  for (int q = threadIdx.x; q < 3 * F; q += NTH3) {
+    const int d = q / F, r = q - d * F;
+    int i, j, k, a;
+    if (d == 0) {
+      i = r % (nc + 1) + 1;
+      j = (r / (nc + 1)) % nc + 1;
+      k = r / ((nc + 1) * nc) + 1;
+      a = i;
+    } else if (d == 1) {
+      i = r % nc + 1;
+      j = (r / nc) % (nc + 1) + 1;
+      k = r / (nc * (nc + 1)) + 1;
+      a = j;
+    } else {
+      i = r % nc + 1;
+      j = (r / nc) % nc + 1;
+      k = r / (nc * nc) + 1;
+      a = k;
+    }
+    const int st = d == 0 ? 1 : d == 1 ? g : g * g;
+    const int c0 = ix3(g, i, j, k), cm = c0 - st;
+    double v;
+    if (a == 1) {
+      v = 2 * inv_dr * (phi[cm] - phi[c0]) * eps[cm] / (eps[c0] + eps[cm]);
+    } else if (a == nc + 1) {
+      v = 2 * inv_dr * (phi[cm] - phi[c0]) * eps[c0] / (eps[c0] + eps[cm]);
+    } else {
+      v = inv_dr * (phi[cm] - phi[c0]);
+    }
+    sfc[d * FSLOT3 + r] = v;
+    FC(R, d, F_FLD, id)[r] = v;
+  }
+  __syncthreads();
+  double *fld = CC(R, I_FLD, id);
+  const int n = nc * nc * nc;
+  for (int t = threadIdx.x; t < n; t += NTH3) {
+    const int i = t % nc + 1, j = (t / nc) % nc + 1, k = t / (nc * nc) + 1;
+    const int xl = (i - 1) + (nc + 1) * ((j - 1) + nc * (k - 1));
+    const int yl = (i - 1) + nc * ((j - 1) + (nc + 1) * (k - 1));
+    const int zl = (i - 1) + nc * ((j - 1) + nc * (k - 1));
+    const double sx = sfc[xl] + sfc[xl + 1];
+    const double sy = sfc[FSLOT3 + yl] + sfc[FSLOT3 + yl + nc];
+    const double sz = sfc[2 * FSLOT3 + zl] + sfc[2 * FSLOT3 + zl + nc * nc];
+    fld[ix3(g, i, j, k)] = 0.5 * sqrt(sx * sx + sy * sy + sz * sz);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Reductions over the interior cells of the leaves (a3_tree_max_cc /
+// a3_tree_min_cc, afivo/src/m_aX_utils.f90:559-619; exact, so in any order).
+// kind 0: the three of get_max_dt (max |E|, min |E|, max n_e) per block into
+// part[3 b ..]; kind 1 / 2: max / min of variable iv into part[b].
+__device__ __forceinline__ double red_op(double a, double b, bool mx) { return mx ? fmax(a, b) : fmin(a, b); }
+__global__ void __launch_bounds__(NTH3) k3_reduce_boxes(Run3 R, const int *ids, int kind, int iv) {
+  __shared__ double red[3][NTH3 / 32];
+  const int id = ids[blockIdx.x];
+  const int nc = R.nc[id], g = nc + 2, n = nc * nc * nc;
+  const double HUGE_D = 1.7976931348623157e308;
+  const double *a = CC(R, kind == 0 ? I_FLD : iv, id), *e = CC(R, I_ELEC, id);
+  double v0 = kind == 2 ? HUGE_D : -HUGE_D, v1 = HUGE_D, v2 = -HUGE_D;
+  for (int t = threadIdx.x; t < n; t += NTH3) {
+    const int c = ix3(g, t % nc + 1, (t / nc) % nc + 1, t / (nc * nc) + 1);
+    v0 = red_op(v0, a[c], kind != 2);
+    if (kind == 0) {
+      v1 = fmin(v1, a[c]);
+      v2 = fmax(v2, e[c]);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    v0 = red_op(v0, __shfl_xor_sync(0xffffffffu, v0, o), kind != 2);
+    v1 = fmin(v1, __shfl_xor_sync(0xffffffffu, v1, o));
+    v2 = fmax(v2, __shfl_xor_sync(0xffffffffu, v2, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = v0;
+    red[1][threadIdx.x >> 5] = v1;
+    red[2][threadIdx.x >> 5] = v2;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < NTH3 / 32; w++) {
+      v0 = red_op(v0, red[0][w], kind != 2);
+      v1 = fmin(v1, red[1][w]);
+      v2 = fmax(v2, red[2][w]);
+    }
+    if (kind == 0) {
+      R.part[3 * blockIdx.x] = v0;
+      R.part[3 * blockIdx.x + 1] = v1;
+      R.part[3 * blockIdx.x + 2] = v2;
+    } else {
+      R.part[blockIdx.x] = v0;
+    }
+  }
+}
+// The blocks' partial results into scal[S_RED ..] (one block).
+__global__ void __launch_bounds__(NTH3) k3_reduce_final(Run3 R, int nb, int kind) {
+  __shared__ double red[3][NTH3 / 32];
+  const double HUGE_D = 1.7976931348623157e308;
+  const int w = kind == 0 ? 3 : 1;
+  double v0 = kind == 2 ? HUGE_D : -HUGE_D, v1 = HUGE_D, v2 = -HUGE_D;
+  for (int b = threadIdx.x; b < nb; b += NTH3) {
+    v0 = red_op(v0, R.part[w * b], kind != 2);
+    if (kind == 0) {
+      v1 = fmin(v1, R.part[3 * b + 1]);
+      v2 = fmax(v2, R.part[3 * b + 2]);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    v0 = red_op(v0, __shfl_xor_sync(0xffffffffu, v0, o), kind != 2);
+    v1 = fmin(v1, __shfl_xor_sync(0xffffffffu, v1, o));
+    v2 = fmax(v2, __shfl_xor_sync(0xffffffffu, v2, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = v0;
+    red[1][threadIdx.x >> 5] = v1;
+    red[2][threadIdx.x >> 5] = v2;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int q = 1; q < NTH3 / 32; q++) {
+      v0 = red_op(v0, red[0][q], kind != 2);
+      v1 = fmin(v1, red[1][q]);
+      v2 = fmax(v2, red[2][q]);
+    }
+    R.scal[S_RED] = v0;
+    R.scal[S_RED + 1] = v1;
+    R.scal[S_RED + 2] = v2;
+  }
+}
+
+// The step size of the next launches (device scalar, so that one captured
+// graph serves every step).
+__global__ void k3_set_dt(double *scal, double dt) { scal[S_DT] = dt; }
+
+}  // namespace
+
+// ===========================================================================
+// Host side.
+
+static thread_local std::string g_err3;
+static int fail3(int code, const std::string &msg) {
+  g_err3 = msg;
+  return code;
+}
+#define CK3(x)                                                                   \
+  do {                                                                           \
+    cudaError_t e_ = (x);                                                        \
+    if (e_ != cudaSuccess) return fail3(A5G_ECUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+struct a5g3_ctx {
+  a5g3_params p{};
+  int max_id = 0, min_lvl = 1, max_lvl = 1;
+  long long cap = 0;
+  // host copy of the tree (per id)
+  std::vector<int> lvl, ix, nc, nbr, chl, par, off;
+  std::vector<double> geo;
+  std::vector<int> lv_off, lv_n;  // per level index: offset into lv_ids, count
+  std::vector<int> lv_ids;        // ids level by level, min_lvl..max_lvl
+  // device
+  double *d_cc = nullptr, *d_fc = nullptr, *d_lt = nullptr, *d_scal = nullptr, *d_part = nullptr;
+  int *d_nc = nullptr, *d_nbr = nullptr, *d_chl = nullptr, *d_par = nullptr, *d_off = nullptr;
+  int *d_ids = nullptr;
+  double *d_geo = nullptr;
+  int lt_rows = 0;
+  double lt_xmin = 0, lt_inv_dx = 0;
+  std::vector<double> h_lt;
+  double voltage = 0;
+  cudaStream_t stream = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  double *h_red = nullptr;  // pinned, 4 doubles
+
+  int li(int l) const { return l - min_lvl; }
+  const int *ids(int l) const { return d_ids + lv_off[li(l)]; }
+  int count(int l) const { return lv_n[li(l)]; }
+  const int *all_ids() const { return d_ids; }
+  int n_all() const { return (int)lv_ids.size(); }
+  Run3 run() const {
+    Run3 R;
+    R.cc = d_cc;
+    R.fc = d_fc;
+    R.nc = d_nc;
+    R.nbr = d_nbr;
+    R.chl = d_chl;
+    R.par = d_par;
+    R.off = d_off;
+    R.geo = d_geo;
+    R.lt = d_lt;
+    R.scal = d_scal;
+    R.part = d_part;
+    R.cap = cap;
+    R.lt_rows = lt_rows;
+    R.lt_xmin = lt_xmin;
+    R.lt_inv_dx = lt_inv_dx;
+    R.voltage = voltage;
+    return R;
+  }
+};
+
+// The uniform octree with the reference's ids: a3_set_base
+// (afivo/src/m_aX_core.f90:134-217: the base boxes on level 1 in ix order
+// (x fastest), one box per base box on each coarse level min_lvl..0, ids
+// level by level from min_lvl), then a3_adjust_refinement with every box of
+// the finest level flagged (:456-520, add_children :753-788): each parent's
+// eight children take consecutive ids in child order (x fastest), parents in
+// level order. Neighbours are the same-level boxes across each face, or -1
+// at the domain walls (the physical boundary of nb_list).
+static void build_tree(a5g3_ctx *c) {
+  const a5g3_params &p = c->p;
+  const int nc8 = p.box_size;
+  const int nx = p.n_base[0], ny = p.n_base[1], nz = p.n_base[2], nbase = nx * ny * nz;
+  c->min_lvl = 1 - (int)std::lround(std::log((double)nc8 / 2) / std::log(2.0));
+  c->max_lvl = p.uniform_lvl;
+  const int nlev = c->max_lvl - c->min_lvl + 1;
+  long long total = 1;  // id 0 unused
+  std::vector<long long> per(nlev);
+  for (int l = c->min_lvl; l <= c->max_lvl; l++) {
+    per[l - c->min_lvl] = l <= 1 ? nbase : per[l - 1 - c->min_lvl] * 8;
+    total += per[l - c->min_lvl];
+  }
+  c->cap = total;
+  c->max_id = (int)(total - 1);
+  const size_t n = (size_t)total;
+  c->lvl.assign(n, 0);
+  c->ix.assign(3 * n, 0);
+  c->nc.assign(n, 0);
+  c->nbr.assign(6 * n, 0);
+  c->chl.assign(8 * n, 0);
+  c->par.assign(n, 0);
+  c->off.assign(3 * n, 0);
+  c->geo.assign(4 * n, 0.0);
+  c->lv_off.assign(nlev, 0);
+  c->lv_n.assign(nlev, 0);
+  c->lv_ids.clear();
+  int next = 1;
+  // base and coarse levels
+  for (int l = c->min_lvl; l <= 1; l++) {
+    c->lv_off[l - c->min_lvl] = (int)c->lv_ids.size();
+    c->lv_n[l - c->min_lvl] = nbase;
+    const int first = next;
+    for (int kk = 0; kk < nz; kk++)
+      for (int j = 0; j < ny; j++)
+        for (int i = 0; i < nx; i++) {
+          const int id = next++;
+          const int q = i + nx * (j + ny * kk);
+          c->lv_ids.push_back(id);
+          c->lvl[id] = l;
+          const int bix[3] = {i + 1, j + 1, kk + 1};
+          for (int d = 0; d < 3; d++) {
+            c->ix[3 * id + d] = bix[d];
+            c->geo[4 * id + d] = 0.0 + (bix[d] - 1) * p.dr_base * nc8;
+          }
+          c->geo[4 * id + 3] = p.dr_base * std::pow(0.5, l - 1);
+          c->nc[id] = nc8 / (1 << (1 - l));
+          const int nbq[6] = {i > 0 ? q - 1 : -1, i < nx - 1 ? q + 1 : -1, j > 0 ? q - nx : -1,
+                              j < ny - 1 ? q + nx : -1, kk > 0 ? q - nx * ny : -1, kk < nz - 1 ? q + nx * ny : -1};
+          for (int s = 0; s < 6; s++) c->nbr[6 * id + s] = nbq[s] >= 0 ? first + nbq[s] : -1;
+          if (l > c->min_lvl) {
+            const int pid = id - nbase;
+            c->par[id] = pid;
+            c->chl[8 * pid] = id;
+          }
+        }
+  }
+  // finer levels: children of each parent in order
+  for (int l = 2; l <= c->max_lvl; l++) {
+    const int L0 = c->lv_off[l - 1 - c->min_lvl], Ln = c->lv_n[l - 1 - c->min_lvl];
+    c->lv_off[l - c->min_lvl] = (int)c->lv_ids.size();
+    c->lv_n[l - c->min_lvl] = 8 * Ln;
+    for (int q = 0; q < Ln; q++) {
+      const int pid = c->lv_ids[L0 + q];
+      for (int ch = 0; ch < 8; ch++) {
+        const int id = next++;
+        c->lv_ids.push_back(id);
+        c->chl[8 * pid + ch] = id;
+        c->par[id] = pid;
+        c->lvl[id] = l;
+        c->nc[id] = nc8;
+        const int dix[3] = {ch & 1, (ch >> 1) & 1, (ch >> 2) & 1};
+        for (int d = 0; d < 3; d++) {
+          c->ix[3 * id + d] = 2 * c->ix[3 * pid + d] - 1 + dix[d];
+          c->geo[4 * id + d] = c->geo[4 * pid + d] + 0.5 * c->geo[4 * pid + 3] * dix[d] * nc8;
+          c->off[3 * id + d] = l > 1 ? ((c->ix[3 * id + d] - 1) & 1) * (nc8 >> 1) : 0;
+        }
+        c->geo[4 * id + 3] = 0.5 * c->geo[4 * pid + 3];
+      }
+    }
+    // same-level neighbours through a (ix) -> id map of the level
+    const long long ext[3] = {(long long)nx << (l - 1), (long long)ny << (l - 1), (long long)nz << (l - 1)};
+    std::vector<int> at((size_t)(ext[0] * ext[1] * ext[2]), 0);
+    const int F0 = c->lv_off[l - c->min_lvl], Fn = c->lv_n[l - c->min_lvl];
+    auto key = [&](long long a, long long b, long long d) { return (size_t)(a - 1 + ext[0] * ((b - 1) + ext[1] * (d - 1))); };
+    for (int q = 0; q < Fn; q++) {
+      const int id = c->lv_ids[F0 + q];
+      at[key(c->ix[3 * id], c->ix[3 * id + 1], c->ix[3 * id + 2])] = id;
+    }
+    for (int q = 0; q < Fn; q++) {
+      const int id = c->lv_ids[F0 + q];
+      for (int s = 0; s < 6; s++) {
+        long long v[3] = {c->ix[3 * id], c->ix[3 * id + 1], c->ix[3 * id + 2]};
+        const int d = s >> 1;
+        v[d] += (s & 1) ? 1 : -1;
+        c->nbr[6 * id + s] = (v[d] < 1 || v[d] > ext[d]) ? -1 : at[key(v[0], v[1], v[2])];
+      }
+    }
+  }
+}
+
+static int grid_for(long long n) { return (int)std::min<long long>((n + NTH3 - 1) / NTH3, 148LL * 16); }
+
+template <class T>
+static int upload(T *&dst, const std::vector<T> &src, cudaStream_t s) {
+  CK3(cudaMallocAsync((void **)&dst, std::max<size_t>(1, src.size()) * sizeof(T), s));
+  if (!src.empty()) CK3(cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+  return A5G_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Launch sequences (all on the context's stream).
+
+// a3_gc_tree for up to two variables on every box (bc 0: Neumann sides;
+// bc 1: sides_bc_pot)
+static void enq_gc_all(a5g3_ctx *c, int iv0, int iv1, int bc) {
+  k3_gc<<<c->n_all(), NTH3, 0, c->stream>>>(c->run(), c->all_ids(), iv0, iv1, bc);
+}
+static void enq_fill(a5g3_ctx *c, int l) { k3_gc<<<c->count(l), NTH3, 0, c->stream>>>(c->run(), c->ids(l), I_PHI, -1, 1); }
+
+// gsrb_boxes (afivo/src/m_aX_mg.f90:403-426): 2 n_cycle half-sweeps with the
+// ghost sources evaluated inside the sweeps, then the ghost fill the last
+// half-sweep is followed by. stale: the first half-sweep reads the ghost
+// cells in memory.
+static void enq_gsrb(a5g3_ctx *c, int l, int n_cycle, bool stale) {
+  for (int it = 1; it <= 2 * n_cycle; it++)
+    k3_sweep<<<c->count(l), NTH3, 0, c->stream>>>(c->run(), c->ids(l), it, stale && it == 1 ? 1 : 0);
+  enq_fill(c, l);
+}
+
+// update_coarse (:430-486) / set_coarse_phi_rhs (:490-523) for level l
+static void enq_coarse(a5g3_ctx *c, int l, bool copy) {
+  const int n = c->count(l);
+  k3_resid_restrict<<<(n + 3) / 4, NTH3, 0, c->stream>>>(c->run(), c->ids(l), n);
+  enq_fill(c, l - 1);
+  k3_coarse_rhs<<<c->count(l - 1), NTH3, 0, c->stream>>>(c->run(), c->ids(l - 1), copy ? 1 : 0);
+}
+
+// correct_children (:374-401) of level l - 1's parents and fill_gc_phi of l
+static void enq_correct(a5g3_ctx *c, int l) {
+  k3_corr_diff<<<c->count(l - 1), NTH3, 0, c->stream>>>(c->run(), c->ids(l - 1));
+  k3_correct<<<c->count(l), NTH3, 0, c->stream>>>(c->run(), c->ids(l));
+  enq_fill(c, l);
+}
+
+// mg3_fas_vcycle (afivo/src/m_aX_mg.f90:208-255)
+static void enq_vcycle(a5g3_ctx *c, int max_lvl, bool set_residual, bool stale_base) {
+  const int lo = c->min_lvl;
+  for (int l = max_lvl; l >= lo + 1; l--) {
+    enq_gsrb(c, l, 2, false);
+    enq_coarse(c, l, true);
+  }
+  enq_gsrb(c, lo, c->p.n_cycle_base, stale_base);
+  for (int l = lo + 1; l <= max_lvl; l++) {
+    enq_correct(c, l);
+    enq_gsrb(c, l, 2, false);
+  }
+  if (set_residual)
+    for (int l = lo; l <= max_lvl; l++) k3_residual<<<c->count(l), NTH3, 0, c->stream>>>(c->run(), c->ids(l));
+}
+
+// mg3_fas_fmg (afivo/src/m_aX_mg.f90:164-203)
+static void enq_fmg(a5g3_ctx *c, bool set_residual, bool first_call) {
+  const int lo = c->min_lvl, hi = c->max_lvl;
+  if (first_call) {
+    for (int l = hi; l >= lo + 1; l--) k3_init_phi_rhs<<<c->count(l), NTH3, 0, c->stream>>>(c->run(), c->ids(l));
+  } else {
+    for (int l = hi; l >= lo + 1; l--) {
+      if (l == hi) enq_fill(c, l);
+      enq_coarse(c, l, false);
+    }
+  }
+  for (int l = lo; l <= hi; l++) {
+    k3_copy_boxes<<<c->count(l), NTH3, 0, c->stream>>>(c->run(), c->ids(l), I_PHI, I_FLD);
+    if (l > lo) enq_correct(c, l);
+    enq_vcycle(c, l, set_residual && l == hi, first_call && l == lo);
+  }
+}
+
+// compute_fld (src/streamer_3d.f90:309-345) with one FMG cycle
+static void enq_compute_fld(a5g3_ctx *c, bool no_guess) {
+  k3_set_rhs<<<c->count(c->max_lvl), NTH3, 0, c->stream>>>(c->run(), c->ids(c->max_lvl));
+  enq_fmg(c, false, no_guess);
+  k3_fld<<<c->n_all(), NTH3, 0, c->stream>>>(c->run(), c->all_ids());
+  enq_gc_all(c, I_FLD, -1, 0);
+}
+
+// a3_restrict_tree (afivo/src/m_aX_restrict.f90:23-64) for up to two variables
+static void enq_restrict(a5g3_ctx *c, int iv0, int iv1) {
+  for (int l = c->max_lvl; l >= c->min_lvl + 1; l--)
+    k3_restrict<<<c->count(l), NTH3, 0, c->stream>>>(c->run(), c->ids(l), iv0, iv1);
+}
+
+// One time step (src/streamer_3d.f90:96-128): the leaves are the boxes of the
+// finest level; consistent fluxes change nothing on a uniform octree.
+static void enq_step(a5g3_ctx *c) {
+  const long long ncell = c->cap * SLOT3;
+  k3_copy2<<<grid_for(ncell / 2), NTH3, 0, c->stream>>>(c->run(), I_ELEC, I_ELEC_OLD, I_PION, I_PION_OLD);
+  const int hi = c->max_lvl;
+  for (int stage = 1; stage <= 2; stage++) {
+    k3_fluxes<<<c->count(hi), NTH3, 0, c->stream>>>(c->run(), c->ids(hi));
+    k3_update<<<c->count(hi), NTH3, 0, c->stream>>>(c->run(), c->ids(hi));
+    enq_restrict(c, I_ELEC, I_PION);
+    enq_gc_all(c, I_ELEC, I_PION, 0);
+    if (stage == 1) enq_compute_fld(c, false);
+  }
+  k3_average<<<grid_for(ncell), NTH3, 0, c->stream>>>(c->run());
+  enq_compute_fld(c, false);
+}
+
+static int launched(a5g3_ctx *c) {
+  CK3(cudaGetLastError());
+  (void)c;
+  return A5G_OK;
+}
+static int ready(a5g3_ctx *c) {
+  if (!c) return fail3(A5G_EINVAL, "null context");
+  if (!c->d_lt) return fail3(A5G_ESTATE, "no transport table set");
+  return A5G_OK;
+}
+
+extern "C" {
+
+const char *a5g3_last_error(void) { return g_err3.c_str(); }
+
+int a5g3_create(const a5g3_params *p, a5g3_ctx **out) {
+  if (!p || !out) return fail3(A5G_EINVAL, "null argument");
+  *out = nullptr;
+  if (p->box_size != NC3) return fail3(A5G_EINVAL, "box_size must be 8");
+  if (p->uniform_lvl < 1 || p->uniform_lvl > 12) return fail3(A5G_EINVAL, "uniform_lvl must be 1..12");
+  for (int d = 0; d < 3; d++)
+    if (p->n_base[d] < 1 || p->n_base[d] > 64) return fail3(A5G_EINVAL, "n_base must be 1..64");
+  if (!(p->dr_base > 0) || p->n_cycle_base < 1) return fail3(A5G_EINVAL, "dr_base > 0 and n_cycle_base >= 1 required");
+  a5g3_ctx *c = new a5g3_ctx();
+  c->p = *p;
+  build_tree(c);
+  const size_t ncc = (size_t)NV3 * c->cap * SLOT3, nfc = (size_t)3 * NF3 * c->cap * FSLOT3;
+  auto bail = [&](int code) {
+    a5g3_destroy(c);
+    return code;
+  };
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return bail(fail3(A5G_ECUDA, "stream creation failed"));
+  if (cudaMalloc((void **)&c->d_cc, ncc * sizeof(double)) != cudaSuccess ||
+      cudaMalloc((void **)&c->d_fc, nfc * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    return bail(fail3(A5G_ENOMEM, "device allocation of the cell/face storage failed"));
+  }
+  if (cudaMemsetAsync(c->d_cc, 0, ncc * sizeof(double), c->stream) != cudaSuccess ||
+      cudaMemsetAsync(c->d_fc, 0, nfc * sizeof(double), c->stream) != cudaSuccess)
+    return bail(fail3(A5G_ECUDA, "memset failed"));
+  int r;
+  if ((r = upload(c->d_nc, c->nc, c->stream)) || (r = upload(c->d_nbr, c->nbr, c->stream)) ||
+      (r = upload(c->d_chl, c->chl, c->stream)) || (r = upload(c->d_par, c->par, c->stream)) ||
+      (r = upload(c->d_off, c->off, c->stream)) || (r = upload(c->d_geo, c->geo, c->stream)) ||
+      (r = upload(c->d_ids, c->lv_ids, c->stream)))
+    return bail(r);
+  if (cudaMalloc((void **)&c->d_scal, 16 * sizeof(double)) != cudaSuccess ||
+      cudaMalloc((void **)&c->d_part, (size_t)3 * c->cap * sizeof(double)) != cudaSuccess ||
+      cudaMallocHost((void **)&c->h_red, 4 * sizeof(double)) != cudaSuccess)
+    return bail(fail3(A5G_ENOMEM, "device allocation failed"));
+  c->voltage = -p->domain_len_z * p->applied_fld;
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return bail(fail3(A5G_ECUDA, "setup failed"));
+  *out = c;
+  return A5G_OK;
+}
+
+int a5g3_destroy(a5g3_ctx *c) {
+  if (!c) return A5G_OK;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->exec) cudaGraphExecDestroy(c->exec);
+  if (c->graph) cudaGraphDestroy(c->graph);
+  for (void *ptr : {(void *)c->d_cc, (void *)c->d_fc, (void *)c->d_lt, (void *)c->d_scal, (void *)c->d_part,
+                    (void *)c->d_nc, (void *)c->d_nbr, (void *)c->d_chl, (void *)c->d_par, (void *)c->d_off,
+                    (void *)c->d_ids, (void *)c->d_geo})
+    if (ptr) cudaFree(ptr);
+  if (c->h_red) cudaFreeHost(c->h_red);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return A5G_OK;
+}
+
+int a5g3_info(a5g3_ctx *c, int *max_id, int *min_lvl, int *max_lvl, long long *n_leaf_cells) {
+  if (!c) return fail3(A5G_EINVAL, "null context");
+  if (max_id) *max_id = c->max_id;
+  if (min_lvl) *min_lvl = c->min_lvl;
+  if (max_lvl) *max_lvl = c->max_lvl;
+  if (n_leaf_cells) *n_leaf_cells = (long long)c->count(c->max_lvl) * NC3 * NC3 * NC3;
+  return A5G_OK;
+}
+
+int a5g3_export_meta(a5g3_ctx *c, int *m24) {
+  if (!c || !m24) return fail3(A5G_EINVAL, "null argument");
+  for (int id = 0; id <= c->max_id; id++) {
+    int *m = m24 + 24 * id;
+    std::memset(m, 0, 24 * sizeof(int));
+    if (id == 0) continue;
+    m[0] = 1;
+    m[1] = c->lvl[id];
+    for (int d = 0; d < 3; d++) m[2 + d] = c->ix[3 * id + d];
+    m[5] = c->par[id];
+    for (int k = 0; k < 8; k++) m[6 + k] = c->chl[8 * id + k];
+    for (int k = 0; k < 6; k++) m[14 + k] = c->nbr[6 * id + k];
+    m[20] = c->nc[id];
+  }
+  return A5G_OK;
+}
+
+int a5g3_export_levels(a5g3_ctx *c, int *counts, int *ids, int cap, int *n_out) {
+  if (!c) return fail3(A5G_EINVAL, "null context");
+  int k = 0;
+  for (int l = c->min_lvl; l <= c->max_lvl; l++) {
+    const int q = c->li(l), n = c->lv_n[q];
+    const bool leaf = l == c->max_lvl;
+    if (counts) {
+      counts[3 * q] = n;
+      counts[3 * q + 1] = leaf ? n : 0;
+      counts[3 * q + 2] = leaf ? 0 : n;
+    }
+    for (int pass = 0; pass < 2; pass++)  // ids, then leaves or parents
+      for (int t = 0; t < n; t++) {
+        if (ids && k < cap) ids[k] = c->lv_ids[c->lv_off[q] + t];
+        k++;
+      }
+  }
+  if (n_out) *n_out = k;
+  return A5G_OK;
+}
+
+int a5g3_set_table(a5g3_ctx *c, int n_rows, int n_cols, double x_min, double inv_dx, const double *rc) {
+  if (!c || !rc || n_rows < 2 || n_cols != 4) return fail3(A5G_EINVAL, "bad table (n_rows >= 2, 4 columns)");
+  if (c->d_lt) cudaFree(c->d_lt);
+  c->d_lt = nullptr;
+  c->h_lt.assign(rc, rc + (size_t)n_rows * n_cols);
+  CK3(cudaMalloc((void **)&c->d_lt, c->h_lt.size() * sizeof(double)));
+  CK3(cudaMemcpy(c->d_lt, rc, c->h_lt.size() * sizeof(double), cudaMemcpyHostToDevice));
+  c->lt_rows = n_rows;
+  c->lt_xmin = x_min;
+  c->lt_inv_dx = inv_dx;
+  if (c->exec) {
+    cudaGraphExecDestroy(c->exec);
+    cudaGraphDestroy(c->graph);
+    c->exec = nullptr;
+    c->graph = nullptr;
+  }
+  return A5G_OK;
+}
+
+int a5g3_set_init_cond(a5g3_ctx *c, double bg, int n_seeds, const double *r0, const double *r1, const double *dens,
+                       const double *width, const int *falloff) {
+  if (!c) return fail3(A5G_EINVAL, "null context");
+  if (n_seeds < 0 || n_seeds > 8 || (n_seeds > 0 && (!r0 || !r1 || !dens || !width || !falloff)))
+    return fail3(A5G_EINVAL, "0..8 seeds with all arrays");
+  Seeds3 S{};
+  S.n = n_seeds;
+  S.bg = bg;
+  for (int s = 0; s < n_seeds; s++) {
+    for (int d = 0; d < 3; d++) {
+      S.r0[s][d] = r0[3 * s + d];
+      S.r1[s][d] = r1[3 * s + d];
+    }
+    S.dens[s] = dens[s];
+    S.width[s] = width[s];
+    S.falloff[s] = falloff[s];
+  }
+  k3_init<<<c->n_all(), NTH3, 0, c->stream>>>(c->run(), c->all_ids(), S);
+  return launched(c);
+}
+
+int a5g3_upload_cc(a5g3_ctx *c, int iv, const double *h) {
+  if (!c || !h || iv < 0 || iv >= NV3) return fail3(A5G_EINVAL, "bad argument");
+  CK3(cudaMemcpyAsync(c->d_cc + (size_t)iv * c->cap * SLOT3, h, (size_t)c->cap * SLOT3 * sizeof(double),
+                      cudaMemcpyHostToDevice, c->stream));
+  CK3(cudaStreamSynchronize(c->stream));
+  return A5G_OK;
+}
+int a5g3_download_cc(a5g3_ctx *c, int iv, double *h) {
+  if (!c || !h || iv < 0 || iv >= NV3) return fail3(A5G_EINVAL, "bad argument");
+  CK3(cudaMemcpyAsync(h, c->d_cc + (size_t)iv * c->cap * SLOT3, (size_t)c->cap * SLOT3 * sizeof(double),
+                      cudaMemcpyDeviceToHost, c->stream));
+  CK3(cudaStreamSynchronize(c->stream));
+  return A5G_OK;
+}
+int a5g3_upload_fc(a5g3_ctx *c, int d, int f, const double *h) {
+  if (!c || !h || d < 0 || d > 2 || f < 0 || f >= NF3) return fail3(A5G_EINVAL, "bad argument");
+  CK3(cudaMemcpyAsync(c->d_fc + ((size_t)d * NF3 + f) * c->cap * FSLOT3, h, (size_t)c->cap * FSLOT3 * sizeof(double),
+                      cudaMemcpyHostToDevice, c->stream));
+  CK3(cudaStreamSynchronize(c->stream));
+  return A5G_OK;
+}
+int a5g3_download_fc(a5g3_ctx *c, int d, int f, double *h) {
+  if (!c || !h || d < 0 || d > 2 || f < 0 || f >= NF3) return fail3(A5G_EINVAL, "bad argument");
+  CK3(cudaMemcpyAsync(h, c->d_fc + ((size_t)d * NF3 + f) * c->cap * FSLOT3, (size_t)c->cap * FSLOT3 * sizeof(double),
+                      cudaMemcpyDeviceToHost, c->stream));
+  CK3(cudaStreamSynchronize(c->stream));
+  return A5G_OK;
+}
+
+int a5g3_tree_copy_cc(a5g3_ctx *c, int a, int b) {
+  if (!c || a < 0 || a >= NV3 || b < 0 || b >= NV3) return fail3(A5G_EINVAL, "bad argument");
+  k3_copy2<<<grid_for(c->cap * SLOT3 / 2), NTH3, 0, c->stream>>>(c->run(), a, b, -1, -1);
+  return launched(c);
+}
+static int with_dt(a5g3_ctx *c, double dt) {
+  if (!(dt > 0)) return fail3(A5G_EINVAL, "dt must be > 0");
+  k3_set_dt<<<1, 1, 0, c->stream>>>(c->d_scal, dt);
+  return launched(c);
+}
+int a5g3_fluxes_koren(a5g3_ctx *c, double dt) {
+  int r = ready(c);
+  if (r || (r = with_dt(c, dt))) return r;
+  k3_fluxes<<<c->count(c->max_lvl), NTH3, 0, c->stream>>>(c->run(), c->ids(c->max_lvl));
+  return launched(c);
+}
+int a5g3_update_solution(a5g3_ctx *c, double dt) {
+  int r = ready(c);
+  if (r || (r = with_dt(c, dt))) return r;
+  k3_update<<<c->count(c->max_lvl), NTH3, 0, c->stream>>>(c->run(), c->ids(c->max_lvl));
+  return launched(c);
+}
+int a5g3_restrict_tree(a5g3_ctx *c, int iv) {
+  if (!c || iv < 0 || iv >= NV3) return fail3(A5G_EINVAL, "bad argument");
+  enq_restrict(c, iv, -1);
+  return launched(c);
+}
+int a5g3_gc_tree(a5g3_ctx *c, int iv) {
+  if (!c || iv < 0 || iv >= NV3) return fail3(A5G_EINVAL, "bad argument");
+  enq_gc_all(c, iv, -1, 0);
+  return launched(c);
+}
+int a5g3_average_dens(a5g3_ctx *c) {
+  if (!c) return fail3(A5G_EINVAL, "null context");
+  k3_average<<<grid_for(c->cap * SLOT3), NTH3, 0, c->stream>>>(c->run());
+  return launched(c);
+}
+int a5g3_compute_fld(a5g3_ctx *c, int no_guess) {
+  if (!c) return fail3(A5G_EINVAL, "null context");
+  enq_compute_fld(c, no_guess != 0);
+  return launched(c);
+}
+int a5g3_fmg(a5g3_ctx *c, int set_residual, int first_call) {
+  if (!c) return fail3(A5G_EINVAL, "null context");
+  enq_fmg(c, set_residual != 0, first_call != 0);
+  return launched(c);
+}
+int a5g3_vcycle(a5g3_ctx *c, int max_lvl, int set_residual) {
+  if (!c || max_lvl < c->min_lvl || max_lvl > c->max_lvl) return fail3(A5G_EINVAL, "bad argument");
+  enq_vcycle(c, max_lvl, set_residual != 0, false);
+  return launched(c);
+}
+int a5g3_set_rhs(a5g3_ctx *c) {
+  if (!c) return fail3(A5G_EINVAL, "null context");
+  k3_set_rhs<<<c->count(c->max_lvl), NTH3, 0, c->stream>>>(c->run(), c->ids(c->max_lvl));
+  return launched(c);
+}
+int a5g3_fld_from_pot(a5g3_ctx *c) {
+  if (!c) return fail3(A5G_EINVAL, "null context");
+  k3_fld<<<c->n_all(), NTH3, 0, c->stream>>>(c->run(), c->all_ids());
+  enq_gc_all(c, I_FLD, -1, 0);
+  return launched(c);
+}
+
+static int reduce(a5g3_ctx *c, int kind, int iv, double *out, int n_out) {
+  const int hi = c->max_lvl, nb = c->count(hi);
+  k3_reduce_boxes<<<nb, NTH3, 0, c->stream>>>(c->run(), c->ids(hi), kind, iv);
+  k3_reduce_final<<<1, NTH3, 0, c->stream>>>(c->run(), nb, kind);
+  CK3(cudaGetLastError());
+  CK3(cudaMemcpyAsync(c->h_red, c->d_scal + S_RED, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK3(cudaStreamSynchronize(c->stream));
+  for (int q = 0; q < n_out; q++) out[q] = c->h_red[q];
+  return A5G_OK;
+}
+int a5g3_tree_max_cc(a5g3_ctx *c, int iv, double *out) {
+  if (!c || !out || iv < 0 || iv >= NV3) return fail3(A5G_EINVAL, "bad argument");
+  return reduce(c, 1, iv, out, 1);
+}
+int a5g3_tree_min_cc(a5g3_ctx *c, int iv, double *out) {
+  if (!c || !out || iv < 0 || iv >= NV3) return fail3(A5G_EINVAL, "bad argument");
+  return reduce(c, 2, iv, out, 1);
+}
+int a5g3_dt_reductions(a5g3_ctx *c, double *out3) {
+  if (!c || !out3) return fail3(A5G_EINVAL, "bad argument");
+  return reduce(c, 0, 0, out3, 3);
+}
+
+// LT_get_col (fosito/m_lookup_table.f90:107-125, 154-161) on the host copy
+static double host_col(const a5g3_ctx *c, int col, double x) {
+  const double frac = (x - c->lt_xmin) * c->lt_inv_dx;
+  int ix;
+  double fr;
+  if (frac < 2.0e9 && frac > -2.0e9) {
+    ix = (int)std::ceil(frac);
+    fr = ix - frac;
+  } else {
+    ix = frac > 0 ? c->lt_rows : 0;
+    fr = 0;
+  }
+  if (ix < 1) {
+    ix = 1;
+    fr = 1;
+  } else if (ix >= c->lt_rows) {
+    ix = c->lt_rows - 1;
+    fr = 0;
+  }
+  const double *v = c->h_lt.data() + (size_t)c->lt_rows * col;
+  return fr * v[ix - 1] + (1 - fr) * v[ix];
+}
+
+// get_max_dt (src/streamer_3d.f90:274-305)
+int a5g3_get_max_dt(a5g3_ctx *c, double *dt) {
+  int r = ready(c);
+  if (r) return r;
+  if (!dt) return fail3(A5G_EINVAL, "null argument");
+  double red[3];
+  if ((r = a5g3_dt_reductions(c, red))) return r;
+  const double max_fld = red[0], min_fld = red[1], max_dns = red[2];
+  const double dr_min = std::ldexp(c->p.dr_base, -(c->max_lvl - 1));
+  const double mobility = host_col(c, C_MOB, max_fld), max_mobility = host_col(c, C_MOB, min_fld);
+  const double diff_coeff = host_col(c, C_DIF, max_fld), alpha = host_col(c, C_ALPHA, max_fld);
+  const double dt_cfl = dr_min / (mobility * max_fld);
+  const double dt_dif = 0.25 * (dr_min * dr_min) / diff_coeff;
+  const double dt_drt = UC_EPS0 / (UC_ELEM_CHARGE * max_mobility * max_dns);
+  const double dt_alpha = 1 / std::max(mobility * max_fld * alpha, 2.220446049250313e-16);
+  double m = std::min(std::min(1 / (1 / dt_cfl + 1 / dt_dif), dt_alpha), c->p.dt_max);
+  if (c->p.use_drt) m = std::min(m, dt_drt);
+  *dt = 0.5 * m;
+  return A5G_OK;
+}
+
+int a5g3_step(a5g3_ctx *c, double dt) {
+  int r = ready(c);
+  if (r || (r = with_dt(c, dt))) return r;
+  if (!c->exec) {
+    CK3(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    enq_step(c);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (e != cudaSuccess) return fail3(A5G_ECUDA, std::string("step capture: ") + cudaGetErrorString(e));
+    c->graph = g;
+    CK3(cudaGraphInstantiate(&c->exec, c->graph, 0));
+  }
+  CK3(cudaGraphLaunch(c->exec, c->stream));
+  return A5G_OK;
+}
+
+int a5g3_sync(a5g3_ctx *c) {
+  if (!c) return fail3(A5G_EINVAL, "null context");
+  CK3(cudaStreamSynchronize(c->stream));
+  return A5G_OK;
+}
+
+int a5g3_stream(a5g3_ctx *c, void **s) {
+  if (!c || !s) return fail3(A5G_EINVAL, "null argument");
+  *s = (void *)c->stream;
+  return A5G_OK;
+}
+
+}  // extern "C"

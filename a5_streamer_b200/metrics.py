@@ -68,6 +68,21 @@ def census(meta: np.ndarray, levels: Dict[int, Tuple[np.ndarray, np.ndarray, np.
     return Census(dim, nc, min(levels), max(levels), cells, leaf, par)
 
 
+def census3(meta24: np.ndarray, levels, nc: int) -> Census:
+    """Census of a 3D octree from its 24-int meta rows (n_cell in column 20)."""
+    cells, leaf, par = {}, {}, {}
+    for lvl, (ids, lv, pa) in levels.items():
+        cnt = lambda xs: int(sum(int(meta24[i, 20]) ** 3 for i in xs))
+        cells[lvl], leaf[lvl], par[lvl] = cnt(ids), cnt(lv), cnt(pa)
+    return Census(3, nc, min(levels), max(levels), cells, leaf, par)
+
+
+def bytes_per_step_3d(run) -> float:
+    """The model above with D = 3 (g = 1.5 words per variable per ghost fill at
+    nc = 8) on a 3D run's tree (device3.Run3)."""
+    return bytes_per_step(census3(run.meta(), run.levels(), run.nc))
+
+
 def bytes_per_step(c: Census, n_down: int = 2, n_up: int = 2, word: int = 8,
                    photons: float = 0.0) -> float:
     """Algorithmic bytes of one full step; photons > 0 adds the photon

@@ -56,8 +56,9 @@ class Params(ctypes.Structure):
 
 
 def build(force: bool = False) -> str:
-    src = os.path.join(HERE, "a5ref.cpp")
-    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
+    srcs = [os.path.join(HERE, f) for f in ("a5ref.cpp", "a5ref3.inc", "a5ref.h")]
+    if (force or not os.path.exists(LIB_PATH)
+            or any(os.path.getmtime(LIB_PATH) < os.path.getmtime(f) for f in srcs)):
         subprocess.check_call(["make", "-s", "-C", HERE])
     return LIB_PATH
 
@@ -113,6 +114,29 @@ def lib() -> ctypes.CDLL:
             "a5ref_kat_photon_dist": (D, [D, D, I, I]),
             "a5ref_kat_rng": (V, [pi, I, pi]),
             "a5ref_kat_drift_diff": (I, [I, D, I, pd]),
+            # the 3D octree form (uniform octrees)
+            "a5ref3_create": (P, [ctypes.POINTER(Params)]), "a5ref3_destroy": (V, [P]),
+            "a5ref3_init": (I, [P]), "a5ref3_set_init_cond": (V, [P]),
+            "a5ref3_dt_reductions": (V, [P, pd]), "a5ref3_get_max_dt": (D, [P]),
+            "a5ref3_step": (V, [P, D]), "a5ref3_advance": (D, [P]),
+            "a5ref3_time": (D, [P]), "a5ref3_set_time": (V, [P, D]),
+            "a5ref3_op_copy_cc": (V, [P, I, I]), "a5ref3_op_fluxes_koren": (V, [P, D]),
+            "a5ref3_op_update_solution": (V, [P, D]), "a5ref3_op_restrict_tree": (V, [P, I]),
+            "a5ref3_op_gc_tree": (V, [P, I]), "a5ref3_op_average_dens": (V, [P]),
+            "a5ref3_op_set_rhs": (V, [P]), "a5ref3_op_compute_fld": (V, [P, I]),
+            "a5ref3_op_fmg": (V, [P, I, I]), "a5ref3_op_vcycle": (V, [P, I, I]),
+            "a5ref3_op_fld_from_pot": (V, [P]),
+            "a5ref3_tree_max_cc": (D, [P, I]), "a5ref3_tree_min_cc": (D, [P, I]),
+            "a5ref3_applied_voltage": (D, [P]),
+            "a5ref3_max_id": (I, [P]), "a5ref3_max_lvl": (I, [P]), "a5ref3_min_lvl": (I, [P]),
+            "a5ref3_n_leaf_cells": (ctypes.c_longlong, [P]),
+            "a5ref3_export_meta": (V, [P, pi]), "a5ref3_export_geom": (V, [P, pd]),
+            "a5ref3_export_levels": (I, [P, pi, pi, I]),
+            "a5ref3_export_cc": (V, [P, I, pd]), "a5ref3_import_cc": (V, [P, I, pd]),
+            "a5ref3_export_fc": (V, [P, I, I, pd]), "a5ref3_import_fc": (V, [P, I, I, pd]),
+            "a5ref3_export_table": (V, [P, pd, pd, pd, pi]),
+            "a5ref3_kat_mg": (I, [I, I, pd, pd]),
+            "a5ref3_kat_drift_diff": (I, [I, D, pd]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -480,5 +504,161 @@ def kat_drift_diff(uniform_lvl: int = 0, end_time: float = 5.0, regrid: bool = T
     rc = lib().a5ref_kat_drift_diff(uniform_lvl, end_time, 1 if regrid else 0, _dp(out))
     if rc != 0:
         raise RuntimeError("drift-diffusion case touched a physical boundary")
+    keys = ("max_err", "mean_err", "sum0", "sum_end", "steps", "max_lvl", "leaf_cells", "time")
+    return dict(zip(keys, out.tolist()))
+
+
+class Sim3:
+    """One oracle simulation of the 3D octree form (a uniformly refined
+    octree; src/streamer_3d.f90 with afivo's m_a3_* routines)."""
+
+    def __init__(self, cfg, n_threads: int = 0):
+        self.cfg = cfg
+        self._p = make_params(cfg, n_threads)
+        self.h = lib().a5ref3_create(ctypes.byref(self._p))
+        if not self.h:
+            raise ValueError("oracle rejected the 3D parameters")
+        self.nc = cfg.box_size
+
+    def close(self):
+        if self.h:
+            lib().a5ref3_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def init(self) -> int:
+        it = lib().a5ref3_init(self.h)
+        if it < 0:
+            raise RuntimeError("3D oracle: tree construction failed")
+        return it
+
+    def set_init_cond(self):
+        lib().a5ref3_set_init_cond(self.h)
+
+    def get_max_dt(self) -> float:
+        return lib().a5ref3_get_max_dt(self.h)
+
+    def dt_reductions(self) -> np.ndarray:
+        out = np.zeros(3)
+        lib().a5ref3_dt_reductions(self.h, _dp(out))
+        return out
+
+    def step(self, dt: float):
+        lib().a5ref3_step(self.h, dt)
+
+    def advance(self) -> float:
+        return lib().a5ref3_advance(self.h)
+
+    @property
+    def time(self) -> float:
+        return lib().a5ref3_time(self.h)
+
+    @time.setter
+    def time(self, t: float):
+        lib().a5ref3_set_time(self.h, t)
+
+    def op(self, name: str, *args):
+        return getattr(lib(), "a5ref3_op_" + name)(self.h, *args)
+
+    def tree_max_cc(self, iv: int) -> float:
+        return lib().a5ref3_tree_max_cc(self.h, iv)
+
+    def tree_min_cc(self, iv: int) -> float:
+        return lib().a5ref3_tree_min_cc(self.h, iv)
+
+    @property
+    def max_id(self) -> int:
+        return lib().a5ref3_max_id(self.h)
+
+    @property
+    def max_lvl(self) -> int:
+        return lib().a5ref3_max_lvl(self.h)
+
+    @property
+    def min_lvl(self) -> int:
+        return lib().a5ref3_min_lvl(self.h)
+
+    def n_leaf_cells(self) -> int:
+        return lib().a5ref3_n_leaf_cells(self.h)
+
+    def meta(self) -> np.ndarray:
+        m = np.zeros((self.max_id + 1, 24), dtype=np.int32)
+        lib().a5ref3_export_meta(self.h, _ip(m))
+        return m
+
+    def geom(self) -> np.ndarray:
+        g = np.zeros((self.max_id + 1, 4))
+        lib().a5ref3_export_geom(self.h, _dp(g))
+        return g
+
+    def levels(self):
+        nlev = self.max_lvl - self.min_lvl + 1
+        counts = np.zeros((nlev, 3), dtype=np.int32)
+        cap = 3 * (self.max_id + 1)
+        ids = np.zeros(cap, dtype=np.int32)
+        lib().a5ref3_export_levels(self.h, _ip(counts), _ip(ids), cap)
+        out, k = {}, 0
+        for li in range(nlev):
+            n_ids, n_lv, n_pa = counts[li]
+            a = ids[k:k + n_ids].copy(); k += n_ids
+            b = ids[k:k + n_lv].copy(); k += n_lv
+            c = ids[k:k + n_pa].copy(); k += n_pa
+            out[self.min_lvl + li] = (a, b, c)
+        return out
+
+    def cc(self, iv: int) -> np.ndarray:
+        out = np.zeros((self.max_id + 1, (self.nc + 2) ** 3))
+        lib().a5ref3_export_cc(self.h, iv, _dp(out))
+        return out
+
+    def set_cc(self, iv: int, data: np.ndarray):
+        data = np.ascontiguousarray(data, dtype=np.float64)
+        lib().a5ref3_import_cc(self.h, iv, _dp(data))
+
+    def fc(self, dimf: int, f: int) -> np.ndarray:
+        out = np.zeros((self.max_id + 1, (self.nc + 1) * self.nc * self.nc))
+        lib().a5ref3_export_fc(self.h, dimf, f, _dp(out))
+        return out
+
+    def set_fc(self, dimf: int, f: int, data: np.ndarray):
+        data = np.ascontiguousarray(data, dtype=np.float64)
+        lib().a5ref3_import_fc(self.h, dimf, f, _dp(data))
+
+    def table(self):
+        n_rows = ctypes.c_int()
+        x_min, inv_dx = ctypes.c_double(), ctypes.c_double()
+        lib().a5ref3_export_table(self.h, None, ctypes.byref(x_min), ctypes.byref(inv_dx),
+                                  ctypes.byref(n_rows))
+        rc = np.zeros(n_rows.value * 4)
+        lib().a5ref3_export_table(self.h, _dp(rc), None, None, None)
+        return rc, x_min.value, inv_dx.value, n_rows.value
+
+    @property
+    def applied_voltage(self) -> float:
+        return lib().a5ref3_applied_voltage(self.h)
+
+
+def kat_mg3(level: int, n_fmg: int):
+    """test_mg2_3d on a uniform octree: max |residual| and max |error| after
+    each FMG cycle."""
+    res, err = np.zeros(n_fmg), np.zeros(n_fmg)
+    lvl = lib().a5ref3_kat_mg(level, n_fmg, _dp(res), _dp(err))
+    if lvl < 0:
+        raise RuntimeError("3D multigrid case failed")
+    return res, err
+
+
+def kat_drift_diff3(level: int, end_time: float = 1.0) -> dict:
+    """test_drift_diff_3d on a uniform octree: errors against the exact
+    advected solution and the conserved sum of phi."""
+    out = np.zeros(8)
+    rc = lib().a5ref3_kat_drift_diff(level, end_time, _dp(out))
+    if rc != 0:
+        raise RuntimeError("3D drift-diffusion case failed")
     keys = ("max_err", "mean_err", "sum0", "sum_end", "steps", "max_lvl", "leaf_cells", "time")
     return dict(zip(keys, out.tolist()))

@@ -14,9 +14,9 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def declared():
     names = []
-    for h in ("a5g.h", "a5t.h"):
+    for h in ("a5g.h", "a5t.h", "a5g3.h"):
         src = open(os.path.join(ROOT, "include", h)).read()
-        names += re.findall(r"^\s*(?:const\s+)?\w+\s*\*?\s*(a5[gts]_\w+)\s*\(", src, re.M)
+        names += re.findall(r"^\s*(?:const\s+)?\w+\s*\*?\s*(a5(?:[gts]|g3)_\w+)\s*\(", src, re.M)
     return sorted(set(names))
 
 
