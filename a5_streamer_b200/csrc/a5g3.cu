@@ -55,6 +55,11 @@ struct Run3 {
   int lt_rows;
   double lt_xmin, lt_inv_dx;
   double voltage;      // applied potential at the high-z wall
+  // the levels: ids of level lo + q at ids[lv_off[q] .. + lv_n[q]], lv_nc[q]
+  // cells per box edge
+  const int *ids;
+  int lo, nlev, n_cycle_base;
+  int lv_off[16], lv_n[16], lv_nc[16];
 };
 enum { S_DT = 0, S_RED = 1 };  // scal[0] dt; scal[1..3] reductions; scal[4] tree max/min
 
@@ -316,40 +321,42 @@ __global__ void __launch_bounds__(NTH3) k3_restrict(Run3 R, const int *ids, int 
 // layer: Neumann (a3_gc_neumann, :298-330), or for the potential with
 // bc = 1 sides_bc_pot (src/streamer_3d.f90:693-715): Neumann on x and y,
 // -phi at low z, 2 V - phi at high z.
+// Item t of box id: variable (t < 6 nc^2 ? iv0 : iv1), side, cell.
+__device__ __forceinline__ void it_gc(const Run3 &R, int id, int t, int iv0, int iv1, int bc) {
+  const int nc = R.nc[id], g = nc + 2, per = nc * nc;
+  const int iv = t < 6 * per ? iv0 : iv1;
+  if (iv < 0) return;
+  const int u = t < 6 * per ? t : t - 6 * per;
+  const int side = u / per, w = u - side * per;
+  const int a = w % nc + 1, b = w / nc + 1;
+  const int d = side >> 1;
+  const bool low = (side & 1) == 0;
+  const int st = d == 0 ? 1 : d == 1 ? g : g * g;
+  // the ghost cell and the box's own first cell on that side
+  int gcell;
+  if (d == 0) gcell = ix3(g, low ? 0 : nc + 1, a, b);
+  else if (d == 1) gcell = ix3(g, a, low ? 0 : nc + 1, b);
+  else gcell = ix3(g, a, b, low ? 0 : nc + 1);
+  const int own = low ? gcell + st : gcell - st;
+  double *x = CC(R, iv, id);
+  const int n = R.nbr[6 * id + side];
+  double v;
+  if (n > 0) {
+    // the neighbour's cell nc (low side) or 1 (high side)
+    v = CC(R, iv, n)[low ? gcell + nc * st : gcell - nc * st];
+  } else if (bc == 1 && side == 4) {
+    v = -x[own];
+  } else if (bc == 1 && side == 5) {
+    v = 2 * R.voltage - x[own];
+  } else {
+    v = x[own];
+  }
+  x[gcell] = v;
+}
 __global__ void __launch_bounds__(NTH3) k3_gc(Run3 R, const int *ids, int iv0, int iv1, int bc) {
   const int id = ids[blockIdx.x];
-  const int nc = R.nc[id], g = nc + 2, per = nc * nc;
-  const int *nb = R.nbr + 6 * id;
-  for (int t = threadIdx.x; t < 12 * per; t += NTH3) {
-    const int iv = t < 6 * per ? iv0 : iv1;
-    if (iv < 0) continue;
-    const int u = t < 6 * per ? t : t - 6 * per;
-    const int side = u / per, w = u - side * per;
-    const int a = w % nc + 1, b = w / nc + 1;
-    const int d = side >> 1;
-    const bool low = (side & 1) == 0;
-    const int st = d == 0 ? 1 : d == 1 ? g : g * g;
-    // the ghost cell and the box's own first cell on that side
-    int gcell;
-    if (d == 0) gcell = ix3(g, low ? 0 : nc + 1, a, b);
-    else if (d == 1) gcell = ix3(g, a, low ? 0 : nc + 1, b);
-    else gcell = ix3(g, a, b, low ? 0 : nc + 1);
-    const int own = low ? gcell + st : gcell - st;
-    double *x = CC(R, iv, id);
-    const int n = nb[side];
-    double v;
-    if (n > 0) {
-      // the neighbour's cell nc (low side) or 1 (high side)
-      v = CC(R, iv, n)[low ? gcell + nc * st : gcell - nc * st];
-    } else if (bc == 1 && side == 4) {
-      v = -x[own];
-    } else if (bc == 1 && side == 5) {
-      v = 2 * R.voltage - x[own];
-    } else {
-      v = x[own];
-    }
-    x[gcell] = v;
-  }
+  const int per = R.nc[id] * R.nc[id];
+  for (int t = threadIdx.x; t < 12 * per; t += NTH3) it_gc(R, id, t, iv0, iv1, bc);
 }
 
 // set_init_cond and set_box_eps (src/streamer_3d.f90:217-270) on every cell
@@ -417,55 +424,31 @@ __global__ void __launch_bounds__(NTH3) k3_init(Run3 R, const int *ids, Seeds3 S
 }
 
 // ---------------------------------------------------------------------------
-// Multigrid (afivo/src/m_aX_mg.f90, 3D Laplacian operators lpl).
+// Multigrid (afivo/src/m_aX_mg.f90, 3D Laplacian operators lpl). Each phase
+// is a flat loop over the items of one level (cells or slot elements of all
+// its boxes, box-major); phase() runs a share of them, so that the same
+// code serves a grid of many blocks on the fine levels (k3_phase) and one
+// block running a whole sequence of small coarse-level phases behind block
+// barriers (k3_coarse).
+enum {
+  PH_SWEEP = 0,         // a0 = half-sweep number, a1 = read ghosts from memory
+  PH_FILL,              // fill_gc_phi: ghost cells of phi (sides_bc_pot)
+  PH_RESID_RESTRICT,    // residual and phi restricted to the parents
+  PH_COARSE_RHS,        // a0 = copy tmp = phi
+  PH_CORR_DIFF,         // tmp = phi - tmp
+  PH_CORRECT,           // phi += prolonged correction of the parent
+  PH_COPY,              // a0 -> a1, whole slots
+  PH_INIT_PHI_RHS,      // phi = 0, rhs restricted to the parents
+  PH_RESIDUAL           // tmp = rhs - lpl(phi)
+};
 
-// One red-black Gauss-Seidel half-sweep `it` of mg3_box_gsrb_lpl (:769-811)
-// on every box of a level: the cells with (i + j + k + it) even, phi =
-// sixth (sum of the six neighbours - dx^2 rhs). A neighbour outside the box
-// is evaluated from its source, which equals the ghost fill gsrb_boxes
-// performs after every half-sweep (:403-426): the facing cell of the
-// same-level neighbour (of the colour not updated here) or, on a physical
-// side, sides_bc_pot of the cell itself (read before it is written). mem:
-// read the ghost cells in memory instead (the first half-sweep on the base
-// level of a first FMG call, whose ghosts the reference leaves as they were).
-__global__ void __launch_bounds__(NTH3) k3_sweep(Run3 R, const int *ids, int it, int mem) {
-  const int id = ids[blockIdx.x];
-  const int nc = R.nc[id], g = nc + 2, hn = nc >> 1, half = nc * nc * hn;
-  const double dr = R.geo[4 * id + 3], dx2 = dr * dr;
-  const double sixth = 1 / 6.0;
-  double *phi = CC(R, I_PHI, id);
-  const double *rhs = CC(R, I_RHS, id);
-  const int *nb = R.nbr + 6 * id;
-  for (int t = threadIdx.x; t < half; t += NTH3) {
-    const int k = t / (nc * hn) + 1, rem = t - (k - 1) * nc * hn;
-    const int j = rem / hn + 1, m = rem - (j - 1) * hn;
-    const int i = 2 - ((it + j + k) & 1) + 2 * m;
-    const int c = ix3(g, i, j, k);
-    const int pos[3] = {i, j, k}, st[3] = {1, g, g * g};
-    double v[6];
-#pragma unroll
-    for (int s = 0; s < 6; s++) {
-      const int d = s >> 1;
-      const bool hi = s & 1;
-      const int a = pos[d] + (hi ? 1 : -1);
-      const int cn = hi ? c + st[d] : c - st[d];
-      if (mem || (a >= 1 && a <= nc)) {
-        v[s] = phi[cn];
-      } else {
-        const int n = nb[s];
-        if (n > 0) v[s] = CC(R, I_PHI, n)[hi ? cn - nc * st[d] : cn + nc * st[d]];
-        else if (s == 4) v[s] = -phi[c];
-        else if (s == 5) v[s] = 2 * R.voltage - phi[c];
-        else v[s] = phi[c];
-      }
-    }
-    double sum = v[1] + v[0];
-    sum = sum + v[3];
-    sum = sum + v[2];
-    sum = sum + v[5];
-    sum = sum + v[4];
-    phi[c] = sixth * (sum - dx2 * rhs[c]);
-  }
+struct Lv {
+  const int *ids;
+  int n, nc;
+};
+__device__ __forceinline__ Lv lv_of(const Run3 &R, int l) {
+  const int q = l - R.lo;
+  return Lv{R.ids + R.lv_off[q], R.lv_n[q], R.lv_nc[q]};
 }
 
 // mg3_box_lpl (:814-848) at interior cell c of a box's phi slot
@@ -478,20 +461,81 @@ __device__ __forceinline__ double lpl3(const double *phi, int c, int g, double i
   return inv_dr_sq * (s - 6 * phi[c]);
 }
 
-// update_coarse / set_coarse_phi_rhs, fine part (:430-523): the residual
-// rhs - lpl(phi) of each box of a level (residual_box, :551-565), restricted
-// with phi to the parent (mg3_box_rstr_lpl, :851-893): parent tmp = mean of
-// the eight residuals, parent phi = mean of the eight phi (column-major
-// sums). The box's own tmp is left as it was (update_coarse restores it;
-// set_coarse_phi_rhs's copy there is overwritten before any read). Four
-// boxes per block, one parent cell per thread.
-__global__ void __launch_bounds__(NTH3) k3_resid_restrict(Run3 R, const int *ids, int n) {
-  const int b = blockIdx.x * 4 + (threadIdx.x >> 6);
-  if (b >= n) return;
-  const int id = ids[b];
-  const int nc = R.nc[id], g = nc + 2, hnc = nc >> 1, nh = hnc * hnc * hnc;
-  const int u = threadIdx.x & 63;
-  if (u >= nh) return;
+// The value phi has, after a ghost fill (fill_gc_phi, :358-371), at the
+// neighbour of cell c (position a along direction s >> 1, cell stride st)
+// across side s: the cell itself inside the box, else the facing cell of
+// the same-level neighbour or sides_bc_pot of cell c (src/streamer_3d.f90:
+// 693-715). Equal to the ghost cell in memory whenever that was filled after
+// the sources last changed.
+__device__ __forceinline__ double phi_side(const Run3 &R, int id, int nc, const double *phi, int c, int s, int a,
+                                           int st) {
+  const bool hi = s & 1;
+  const int cn = hi ? c + st : c - st;
+  const int an = hi ? a + 1 : a - 1;
+  if (an >= 1 && an <= nc) return phi[cn];
+  const int n = R.nbr[6 * id + s];
+  if (n > 0) return CC(R, I_PHI, n)[hi ? cn - nc * st : cn + nc * st];
+  if (s == 4) return -phi[c];
+  if (s == 5) return 2 * R.voltage - phi[c];
+  return phi[c];
+}
+
+// mg3_box_lpl (:814-848) at interior cell (i, j, k) = c of box id, the ghost
+// neighbours from their sources (phi_side)
+__device__ __forceinline__ double lpl3_src(const Run3 &R, int id, int nc, const double *phi, int c, int i, int j,
+                                           int k, double inv_dr_sq) {
+  const int g = nc + 2;
+  double s = phi_side(R, id, nc, phi, c, 0, i, 1) + phi_side(R, id, nc, phi, c, 1, i, 1);
+  s = s + phi_side(R, id, nc, phi, c, 2, j, g);
+  s = s + phi_side(R, id, nc, phi, c, 3, j, g);
+  s = s + phi_side(R, id, nc, phi, c, 4, k, g * g);
+  s = s + phi_side(R, id, nc, phi, c, 5, k, g * g);
+  return inv_dr_sq * (s - 6 * phi[c]);
+}
+
+// One cell of a red-black Gauss-Seidel half-sweep `it` of mg3_box_gsrb_lpl
+// (:769-811): the cells with (i + j + k + it) even, phi = sixth (sum of the
+// six neighbours - dx^2 rhs). A neighbour outside the box is evaluated from
+// its source, which equals the ghost fill gsrb_boxes performs after every
+// half-sweep (:403-426): the facing cell of the same-level neighbour (of
+// the colour not updated here) or, on a physical side, sides_bc_pot of the
+// cell itself (read before it is written). mem: read the ghost cells in
+// memory instead (the first half-sweep on the base level of a first FMG
+// call, whose ghosts the reference leaves as they were).
+__device__ __forceinline__ void it_sweep(const Run3 &R, int id, int nc, int t, int it, int mem) {
+  const int g = nc + 2, hn = nc >> 1;
+  const int k = t / (nc * hn) + 1, rem = t - (k - 1) * nc * hn;
+  const int j = rem / hn + 1, m = rem - (j - 1) * hn;
+  const int i = 2 - ((it + j + k) & 1) + 2 * m;
+  const int c = ix3(g, i, j, k);
+  const double dr = R.geo[4 * id + 3], dx2 = dr * dr;
+  const double sixth = 1 / 6.0;
+  double *phi = CC(R, I_PHI, id);
+  const int pos[3] = {i, j, k}, st[3] = {1, g, g * g};
+  double v[6];
+#pragma unroll
+  for (int s = 0; s < 6; s++) {
+    const int d = s >> 1;
+    v[s] = mem ? phi[(s & 1) ? c + st[d] : c - st[d]] : phi_side(R, id, nc, phi, c, s, pos[d], st[d]);
+  }
+  double sum = v[1] + v[0];
+  sum = sum + v[3];
+  sum = sum + v[2];
+  sum = sum + v[5];
+  sum = sum + v[4];
+  phi[c] = sixth * (sum - dx2 * CC(R, I_RHS, id)[c]);
+}
+
+// update_coarse / set_coarse_phi_rhs, fine part (:430-523), for one parent
+// cell u of box id: the residual rhs - lpl(phi) of its eight child cells
+// (residual_box, :551-565) and their phi, each summed in column-major order,
+// times 0.125 into the parent's tmp and phi (mg3_box_rstr_lpl, :851-893).
+// The box's own tmp is left as it was (update_coarse restores it;
+// set_coarse_phi_rhs's copy there is overwritten before any read). Ghost
+// neighbours come from their sources, so no fill of this level is needed
+// before it.
+__device__ __forceinline__ void it_resid_restrict(const Run3 &R, int id, int nc, int u) {
+  const int g = nc + 2, hnc = nc >> 1;
   const int i = u % hnc + 1, j = (u / hnc) % hnc + 1, k = u / (hnc * hnc) + 1;
   const double dr = R.geo[4 * id + 3], inv_dr_sq = 1 / (dr * dr);
   const double *phi = CC(R, I_PHI, id), *rhs = CC(R, I_RHS, id);
@@ -501,7 +545,8 @@ __global__ void __launch_bounds__(NTH3) k3_resid_restrict(Run3 R, const int *ids
 #pragma unroll
   for (int q = 0; q < 8; q++) {
     const int c = f + o8[q];
-    const double r = rhs[c] - lpl3(phi, c, g, inv_dr_sq);
+    const double r =
+        rhs[c] - lpl3_src(R, id, nc, phi, c, 2 * i - 1 + (q & 1), 2 * j - 1 + ((q >> 1) & 1), 2 * k - 1 + (q >> 2), inv_dr_sq);
     sr = q == 0 ? r : sr + r;
     sp = q == 0 ? phi[c] : sp + phi[c];
   }
@@ -512,101 +557,196 @@ __global__ void __launch_bounds__(NTH3) k3_resid_restrict(Run3 R, const int *ids
   CC(R, I_PHI, p)[pc] = 0.125 * sp;
 }
 
-// Coarse part of update_coarse / set_coarse_phi_rhs (:471-485, :514-521) on
-// the parent boxes of a level: rhs = lpl(phi) on interior cells, then rhs =
-// rhs + tmp on the whole slot (a3_box_add_cc), then with copy tmp = phi
-// (a3_box_copy_cc). One slot element per thread.
-__global__ void __launch_bounds__(NTH3) k3_coarse_rhs(Run3 R, const int *ids, int copy) {
-  const int id = ids[blockIdx.x];
-  const int nc = R.nc[id], g = nc + 2, gs = g * g * g;
+// Coarse part of update_coarse / set_coarse_phi_rhs (:471-485, :514-521) at
+// slot element c of parent box id: rhs = lpl(phi) on interior cells, then
+// rhs = rhs + tmp on the whole slot (a3_box_add_cc), then with copy tmp =
+// phi (a3_box_copy_cc).
+__device__ __forceinline__ void it_coarse_rhs(const Run3 &R, int id, int nc, int c, int copy) {
+  const int g = nc + 2;
+  const int i = c % g, j = (c / g) % g, k = c / (g * g);
+  const bool in = i >= 1 && i <= nc && j >= 1 && j <= nc && k >= 1 && k <= nc;
   const double dr = R.geo[4 * id + 3], inv_dr_sq = 1 / (dr * dr);
   const double *phi = CC(R, I_PHI, id);
   double *rhs = CC(R, I_RHS, id), *tmp = CC(R, I_FLD, id);
-  for (int c = threadIdx.x; c < gs; c += NTH3) {
-    const int i = c % g, j = (c / g) % g, k = c / (g * g);
-    const bool in = i >= 1 && i <= nc && j >= 1 && j <= nc && k >= 1 && k <= nc;
-    const double a = in ? lpl3(phi, c, g, inv_dr_sq) : rhs[c];
-    rhs[c] = a + tmp[c];
-    if (copy) tmp[c] = phi[c];
-  }
+  const double a = in ? lpl3(phi, c, g, inv_dr_sq) : rhs[c];
+  rhs[c] = a + tmp[c];
+  if (copy) tmp[c] = phi[c];
 }
 
-// correct_children (:374-401): on each parent box tmp = phi - tmp (whole
-// slot) ...
-__global__ void __launch_bounds__(NTH3) k3_corr_diff(Run3 R, const int *ids) {
-  const int id = ids[blockIdx.x];
-  const int g = R.nc[id] + 2, gs = g * g * g;
-  const double *phi = CC(R, I_PHI, id);
-  double *tmp = CC(R, I_FLD, id);
-  for (int c = threadIdx.x; c < gs; c += NTH3) tmp[c] = phi[c] - tmp[c];
-}
-
-// ... then mg3_box_corr_lpl (:714-766) on each child: phi += 0.25 (c1 + c2x
+// correct_children (:374-401): on the parent, tmp = phi - tmp (whole slot),
+// then mg3_box_corr_lpl (:714-766) on each child cell: phi += 0.25 (c1 + c2x
 // + c2y + c2z) of the parent's correction, c1 the closest coarse cell.
-__global__ void __launch_bounds__(NTH3) k3_correct(Run3 R, const int *ids) {
-  const int id = ids[blockIdx.x];
-  const int nc = R.nc[id], g = nc + 2, n = nc * nc * nc;
+__device__ __forceinline__ void it_correct(const Run3 &R, int id, int nc, int t) {
+  const int g = nc + 2;
   const int p = R.par[id], pg = R.nc[p] + 2;
   const int *o = R.off + 3 * id;
   const double *corr = CC(R, I_FLD, p);
   double *phi = CC(R, I_PHI, id);
-  for (int t = threadIdx.x; t < n; t += NTH3) {
-    const int i = t % nc + 1, j = (t / nc) % nc + 1, k = t / (nc * nc) + 1;
-    const int i1 = o[0] + ((i + 1) >> 1), i2 = i1 + 1 - 2 * (i & 1);
-    const int j1 = o[1] + ((j + 1) >> 1), j2 = j1 + 1 - 2 * (j & 1);
-    const int k1 = o[2] + ((k + 1) >> 1), k2 = k1 + 1 - 2 * (k & 1);
-    double s = corr[ix3(pg, i1, j1, k1)] + corr[ix3(pg, i2, j1, k1)];
-    s = s + corr[ix3(pg, i1, j2, k1)];
-    s = s + corr[ix3(pg, i1, j1, k2)];
-    const int c = ix3(g, i, j, k);
-    phi[c] = phi[c] + 0.25 * s;
-  }
+  const int i = t % nc + 1, j = (t / nc) % nc + 1, k = t / (nc * nc) + 1;
+  const int i1 = o[0] + ((i + 1) >> 1), i2 = i1 + 1 - 2 * (i & 1);
+  const int j1 = o[1] + ((j + 1) >> 1), j2 = j1 + 1 - 2 * (j & 1);
+  const int k1 = o[2] + ((k + 1) >> 1), k2 = k1 + 1 - 2 * (k & 1);
+  double s = corr[ix3(pg, i1, j1, k1)] + corr[ix3(pg, i2, j1, k1)];
+  s = s + corr[ix3(pg, i1, j2, k1)];
+  s = s + corr[ix3(pg, i1, j1, k2)];
+  const int c = ix3(g, i, j, k);
+  phi[c] = phi[c] + 0.25 * s;
 }
 
-// a3_boxes_copy_cc (whole slots) for the boxes of a list
-__global__ void __launch_bounds__(NTH3) k3_copy_boxes(Run3 R, const int *ids, int from, int to) {
-  const int id = ids[blockIdx.x];
-  const int g = R.nc[id] + 2, gs = g * g * g;
-  const double *a = CC(R, from, id);
-  double *b = CC(R, to, id);
-  for (int c = threadIdx.x; c < gs; c += NTH3) b[c] = a[c];
-}
-
-// init_phi_rhs (:526-549) for one level: phi = 0 on each box's slot and its
-// rhs restricted to the parent.
-__global__ void __launch_bounds__(NTH3) k3_init_phi_rhs(Run3 R, const int *ids) {
-  const int id = ids[blockIdx.x];
-  const int nc = R.nc[id], g = nc + 2, gs = g * g * g, hnc = nc >> 1, nh = hnc * hnc * hnc;
-  double *phi = CC(R, I_PHI, id);
-  for (int c = threadIdx.x; c < gs; c += NTH3) phi[c] = 0.0;
+// init_phi_rhs (:526-549), the restriction of one parent cell's rhs
+__device__ __forceinline__ void it_restrict_rhs(const Run3 &R, int id, int nc, int u) {
+  const int g = nc + 2, hnc = nc >> 1;
+  const int i = u % hnc + 1, j = (u / hnc) % hnc + 1, k = u / (hnc * hnc) + 1;
   const double *rhs = CC(R, I_RHS, id);
+  const int f = ix3(g, 2 * i - 1, 2 * j - 1, 2 * k - 1);
+  double s = rhs[f];
+  s = s + rhs[f + 1];
+  s = s + rhs[f + g];
+  s = s + rhs[f + g + 1];
+  s = s + rhs[f + g * g];
+  s = s + rhs[f + g * g + 1];
+  s = s + rhs[f + g * g + g];
+  s = s + rhs[f + g * g + g + 1];
   const int p = R.par[id], pg = R.nc[p] + 2;
   const int *o = R.off + 3 * id;
-  for (int u = threadIdx.x; u < nh; u += NTH3) {
-    const int i = u % hnc + 1, j = (u / hnc) % hnc + 1, k = u / (hnc * hnc) + 1;
-    const int f = ix3(g, 2 * i - 1, 2 * j - 1, 2 * k - 1);
-    double s = rhs[f];
-    s = s + rhs[f + 1];
-    s = s + rhs[f + g];
-    s = s + rhs[f + g + 1];
-    s = s + rhs[f + g * g];
-    s = s + rhs[f + g * g + 1];
-    s = s + rhs[f + g * g + g];
-    s = s + rhs[f + g * g + g + 1];
-    CC(R, I_RHS, p)[ix3(pg, o[0] + i, o[1] + j, o[2] + k)] = 0.125 * s;
+  CC(R, I_RHS, p)[ix3(pg, o[0] + i, o[1] + j, o[2] + k)] = 0.125 * s;
+}
+
+// Items k0, k0 + stride, ... of phase op on level l (fewer than 2^31 items
+// per level; a5g3_create checks the tree).
+// NCT: the level's box size at compile time (8 on levels >= 1), 0: read it.
+template <int NCT>
+__device__ __forceinline__ void phase(const Run3 &R, int op, int l, int a0, int a1, int k0, int stride) {
+  const Lv L = lv_of(R, l);
+  const int nc = NCT ? NCT : L.nc, g = nc + 2, gs = g * g * g, n3 = nc * nc * nc, hnc = nc >> 1, nh = hnc * hnc * hnc;
+  switch (op) {
+    case PH_SWEEP: {
+      const int per = n3 / 2;
+      for (int k = k0; k < L.n * per; k += stride)
+        it_sweep(R, L.ids[k / per], nc, k % per, a0, a1);
+      break;
+    }
+    case PH_FILL: {
+      const int per = 6 * nc * nc;
+      for (int k = k0; k < L.n * per; k += stride)
+        it_gc(R, L.ids[k / per], k % per, I_PHI, -1, 1);
+      break;
+    }
+    case PH_RESID_RESTRICT:
+      for (int k = k0; k < L.n * nh; k += stride) it_resid_restrict(R, L.ids[k / nh], nc, k % nh);
+      break;
+    case PH_COARSE_RHS:
+      for (int k = k0; k < L.n * gs; k += stride) it_coarse_rhs(R, L.ids[k / gs], nc, k % gs, a0);
+      break;
+    case PH_CORR_DIFF:
+      for (int k = k0; k < L.n * gs; k += stride) {
+        const int id = L.ids[k / gs], c = k % gs;
+        double *tmp = CC(R, I_FLD, id);
+        tmp[c] = CC(R, I_PHI, id)[c] - tmp[c];
+      }
+      break;
+    case PH_CORRECT:
+      for (int k = k0; k < L.n * n3; k += stride) it_correct(R, L.ids[k / n3], nc, k % n3);
+      break;
+    case PH_COPY:
+      for (int k = k0; k < L.n * gs; k += stride) {
+        const int id = L.ids[k / gs], c = k % gs;
+        CC(R, a1, id)[c] = CC(R, a0, id)[c];
+      }
+      break;
+    case PH_INIT_PHI_RHS:
+      for (int k = k0; k < L.n * (gs + nh); k += stride) {
+        const int q = k / (gs + nh);
+        const int r = k % (gs + nh), id = L.ids[q];
+        if (r < gs) CC(R, I_PHI, id)[r] = 0.0;
+        else it_restrict_rhs(R, id, nc, r - gs);
+      }
+      break;
+    case PH_RESIDUAL: {
+      for (int k = k0; k < L.n * n3; k += stride) {
+        const int id = L.ids[k / n3], t = k % n3;
+        const double h = R.geo[4 * id + 3], inv_dr_sq = 1 / (h * h);
+        const int c = ix3(g, t % nc + 1, (t / nc) % nc + 1, t / (nc * nc) + 1);
+        CC(R, I_FLD, id)[c] = CC(R, I_RHS, id)[c] - lpl3(CC(R, I_PHI, id), c, g, inv_dr_sq);
+      }
+      break;
+    }
   }
 }
 
-// residual_box (:551-565) on the boxes of a level: tmp = rhs - lpl(phi)
-__global__ void __launch_bounds__(NTH3) k3_residual(Run3 R, const int *ids) {
-  const int id = ids[blockIdx.x];
-  const int nc = R.nc[id], g = nc + 2, n = nc * nc * nc;
-  const double dr = R.geo[4 * id + 3], inv_dr_sq = 1 / (dr * dr);
-  const double *phi = CC(R, I_PHI, id), *rhs = CC(R, I_RHS, id);
-  double *tmp = CC(R, I_FLD, id);
-  for (int t = threadIdx.x; t < n; t += NTH3) {
-    const int c = ix3(g, t % nc + 1, (t / nc) % nc + 1, t / (nc * nc) + 1);
-    tmp[c] = rhs[c] - lpl3(phi, c, g, inv_dr_sq);
+__host__ __device__ __forceinline__ long long phase_items(int op, int n, int nc) {
+  const long long g = nc + 2, gs = g * g * g, n3 = (long long)nc * nc * nc, nh = n3 / 8;
+  switch (op) {
+    case PH_SWEEP: return n * (n3 / 2);
+    case PH_FILL: return n * 6LL * nc * nc;
+    case PH_RESID_RESTRICT: return n * nh;
+    case PH_CORRECT:
+    case PH_RESIDUAL: return n * n3;
+    case PH_INIT_PHI_RHS: return n * (gs + nh);
+    default: return n * gs;
+  }
+}
+
+// One phase on the grid (grid-stride over its items).
+template <int NCT>
+__global__ void __launch_bounds__(NTH3) k3_phase(Run3 R, int op, int l, int a0, int a1) {
+  phase<NCT>(R, op, l, a0, a1, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+
+// ---------------------------------------------------------------------------
+// The coarse levels lo..top in one block: the sequences of the multigrid
+// cycle that stay on those levels run as one launch, each phase spread over
+// the block's threads and ended by a block barrier.
+constexpr int NTHC = 1024;
+__device__ __forceinline__ void c_phase(const Run3 &R, int op, int l, int a0 = 0, int a1 = 0) {
+  phase<0>(R, op, l, a0, a1, threadIdx.x, NTHC);
+  __syncthreads();
+}
+__device__ void c_gsrb(const Run3 &R, int l, int n_cycle, bool stale) {
+  for (int it = 1; it <= 2 * n_cycle; it++) c_phase(R, PH_SWEEP, l, it, stale && it == 1 ? 1 : 0);
+  c_phase(R, PH_FILL, l);
+}
+__device__ void c_coarse(const Run3 &R, int l, int copy) {
+  c_phase(R, PH_RESID_RESTRICT, l);
+  c_phase(R, PH_FILL, l - 1);
+  c_phase(R, PH_COARSE_RHS, l - 1, copy);
+}
+__device__ void c_correct(const Run3 &R, int l) {
+  c_phase(R, PH_CORR_DIFF, l - 1);
+  c_phase(R, PH_CORRECT, l);
+  c_phase(R, PH_FILL, l);
+}
+// mg3_fas_vcycle (:208-255) on levels lo..top
+__device__ void c_vcycle(const Run3 &R, int top, bool stale) {
+  for (int l = top; l >= R.lo + 1; l--) {
+    c_gsrb(R, l, 2, false);
+    c_coarse(R, l, 1);
+  }
+  c_gsrb(R, R.lo, R.n_cycle_base, stale);
+  for (int l = R.lo + 1; l <= top; l++) {
+    c_correct(R, l);
+    c_gsrb(R, l, 2, false);
+  }
+}
+enum { CM_VCYCLE = 0, CM_FMG, CM_SETC, CM_INIT };
+__global__ void __launch_bounds__(NTHC) k3_coarse(Run3 R, int mode, int top, int flag) {
+  switch (mode) {
+    case CM_VCYCLE:  // the middle of a V-cycle: down from top, base, up to top
+      c_vcycle(R, top, flag != 0);
+      break;
+    case CM_FMG:  // the FMG's levels lo..top (mg3_fas_fmg, :186-202); flag: first call
+      for (int l = R.lo; l <= top; l++) {
+        c_phase(R, PH_COPY, l, I_PHI, I_FLD);
+        if (l > R.lo) c_correct(R, l);
+        c_vcycle(R, l, flag != 0 && l == R.lo);
+      }
+      break;
+    case CM_SETC:  // set_coarse_phi_rhs for levels top..lo+1 (:176-180)
+      for (int l = top; l >= R.lo + 1; l--) c_coarse(R, l, 0);
+      break;
+    case CM_INIT:  // init_phi_rhs on levels top..lo+1 (:526-549)
+      for (int l = top; l >= R.lo + 1; l--) c_phase(R, PH_INIT_PHI_RHS, l);
+      break;
   }
 }
 
@@ -803,7 +943,9 @@ struct a5g3_ctx {
   cudaGraphExec_t exec = nullptr;
   double *h_red = nullptr;  // pinned, 4 doubles
 
+  int coarse_top = 0;  // levels min_lvl..coarse_top run in one block (k3_coarse)
   int li(int l) const { return l - min_lvl; }
+  int nc_of(int l) const { return l >= 1 ? p.box_size : p.box_size >> (1 - l); }
   const int *ids(int l) const { return d_ids + lv_off[li(l)]; }
   int count(int l) const { return lv_n[li(l)]; }
   const int *all_ids() const { return d_ids; }
@@ -826,6 +968,16 @@ struct a5g3_ctx {
     R.lt_xmin = lt_xmin;
     R.lt_inv_dx = lt_inv_dx;
     R.voltage = voltage;
+    R.ids = d_ids;
+    R.lo = min_lvl;
+    R.nlev = max_lvl - min_lvl + 1;
+    R.n_cycle_base = p.n_cycle_base;
+    for (int q = 0; q < 16; q++) {
+      const bool in = q < R.nlev;
+      R.lv_off[q] = in ? lv_off[q] : 0;
+      R.lv_n[q] = in ? lv_n[q] : 0;
+      R.lv_nc[q] = in ? nc_of(min_lvl + q) : 0;
+    }
     return R;
   }
 };
@@ -939,6 +1091,7 @@ static void build_tree(a5g3_ctx *c) {
   }
 }
 
+constexpr int COARSE_BOXES = 8;
 static int grid_for(long long n) { return (int)std::min<long long>((n + NTH3 - 1) / NTH3, 148LL * 16); }
 
 template <class T>
@@ -956,62 +1109,83 @@ static int upload(T *&dst, const std::vector<T> &src, cudaStream_t s) {
 static void enq_gc_all(a5g3_ctx *c, int iv0, int iv1, int bc) {
   k3_gc<<<c->n_all(), NTH3, 0, c->stream>>>(c->run(), c->all_ids(), iv0, iv1, bc);
 }
-static void enq_fill(a5g3_ctx *c, int l) { k3_gc<<<c->count(l), NTH3, 0, c->stream>>>(c->run(), c->ids(l), I_PHI, -1, 1); }
+// One multigrid phase of level l on the grid, about one item per thread.
+static void enq_phase(a5g3_ctx *c, int op, int l, int a0 = 0, int a1 = 0) {
+  const long long n = phase_items(op, c->count(l), c->nc_of(l));
+  const int grid = (int)std::min<long long>((n + NTH3 - 1) / NTH3, 1LL << 20);
+  if (c->nc_of(l) == NC3) k3_phase<NC3><<<grid, NTH3, 0, c->stream>>>(c->run(), op, l, a0, a1);
+  else k3_phase<0><<<grid, NTH3, 0, c->stream>>>(c->run(), op, l, a0, a1);
+}
+static void enq_fill(a5g3_ctx *c, int l) { enq_phase(c, PH_FILL, l); }
 
 // gsrb_boxes (afivo/src/m_aX_mg.f90:403-426): 2 n_cycle half-sweeps with the
-// ghost sources evaluated inside the sweeps, then the ghost fill the last
-// half-sweep is followed by. stale: the first half-sweep reads the ghost
-// cells in memory.
-static void enq_gsrb(a5g3_ctx *c, int l, int n_cycle, bool stale) {
-  for (int it = 1; it <= 2 * n_cycle; it++)
-    k3_sweep<<<c->count(l), NTH3, 0, c->stream>>>(c->run(), c->ids(l), it, stale && it == 1 ? 1 : 0);
-  enq_fill(c, l);
+// ghost sources evaluated inside the sweeps, then (fill) the ghost fill the
+// last half-sweep is followed by. stale: the first half-sweep reads the
+// ghost cells in memory. Ghost fills whose values no later phase reads from
+// memory are left out (fill = false): the phases that follow evaluate those
+// ghost cells from their sources, and every level's ghost cells are filled
+// after its last change in a cycle.
+static void enq_gsrb(a5g3_ctx *c, int l, int n_cycle, bool stale, bool fill = true) {
+  for (int it = 1; it <= 2 * n_cycle; it++) enq_phase(c, PH_SWEEP, l, it, stale && it == 1 ? 1 : 0);
+  if (fill) enq_fill(c, l);
 }
 
 // update_coarse (:430-486) / set_coarse_phi_rhs (:490-523) for level l
 static void enq_coarse(a5g3_ctx *c, int l, bool copy) {
-  const int n = c->count(l);
-  k3_resid_restrict<<<(n + 3) / 4, NTH3, 0, c->stream>>>(c->run(), c->ids(l), n);
+  enq_phase(c, PH_RESID_RESTRICT, l);
   enq_fill(c, l - 1);
-  k3_coarse_rhs<<<c->count(l - 1), NTH3, 0, c->stream>>>(c->run(), c->ids(l - 1), copy ? 1 : 0);
+  enq_phase(c, PH_COARSE_RHS, l - 1, copy ? 1 : 0);
 }
 
-// correct_children (:374-401) of level l - 1's parents and fill_gc_phi of l
+// correct_children (:374-401) of level l - 1's parents; its fill_gc_phi of
+// l is left out, as every caller smooths level l next (sweeps evaluate their
+// ghost neighbours from the sources) and fills it after that.
 static void enq_correct(a5g3_ctx *c, int l) {
-  k3_corr_diff<<<c->count(l - 1), NTH3, 0, c->stream>>>(c->run(), c->ids(l - 1));
-  k3_correct<<<c->count(l), NTH3, 0, c->stream>>>(c->run(), c->ids(l));
-  enq_fill(c, l);
+  enq_phase(c, PH_CORR_DIFF, l - 1);
+  enq_phase(c, PH_CORRECT, l);
 }
 
-// mg3_fas_vcycle (afivo/src/m_aX_mg.f90:208-255)
+static void enq_coarse_kernel(a5g3_ctx *c, int mode, int top, int flag) {
+  k3_coarse<<<1, NTHC, 0, c->stream>>>(c->run(), mode, top, flag);
+}
+
+// mg3_fas_vcycle (afivo/src/m_aX_mg.f90:208-255). The levels lo..top (top =
+// the coarse section, at most max_lvl) run in one k3_coarse launch.
 static void enq_vcycle(a5g3_ctx *c, int max_lvl, bool set_residual, bool stale_base) {
-  const int lo = c->min_lvl;
-  for (int l = max_lvl; l >= lo + 1; l--) {
-    enq_gsrb(c, l, 2, false);
+  const int lo = c->min_lvl, top = std::min(max_lvl, c->coarse_top);
+  for (int l = max_lvl; l >= std::max(lo, top) + 1; l--) {
+    enq_gsrb(c, l, 2, false, false);  // the residual evaluates the ghosts itself
     enq_coarse(c, l, true);
   }
-  enq_gsrb(c, lo, c->p.n_cycle_base, stale_base);
-  for (int l = lo + 1; l <= max_lvl; l++) {
+  if (top >= lo) {
+    enq_coarse_kernel(c, CM_VCYCLE, top, stale_base ? 1 : 0);
+  } else {
+    enq_gsrb(c, lo, c->p.n_cycle_base, stale_base);
+  }
+  for (int l = std::max(lo, top) + 1; l <= max_lvl; l++) {
     enq_correct(c, l);
     enq_gsrb(c, l, 2, false);
   }
   if (set_residual)
-    for (int l = lo; l <= max_lvl; l++) k3_residual<<<c->count(l), NTH3, 0, c->stream>>>(c->run(), c->ids(l));
+    for (int l = lo; l <= max_lvl; l++) enq_phase(c, PH_RESIDUAL, l);
 }
 
-// mg3_fas_fmg (afivo/src/m_aX_mg.f90:164-203)
+// mg3_fas_fmg (afivo/src/m_aX_mg.f90:164-203); the coarse section's part of
+// each stage in one k3_coarse launch.
 static void enq_fmg(a5g3_ctx *c, bool set_residual, bool first_call) {
-  const int lo = c->min_lvl, hi = c->max_lvl;
+  const int lo = c->min_lvl, hi = c->max_lvl, top = c->coarse_top;
   if (first_call) {
-    for (int l = hi; l >= lo + 1; l--) k3_init_phi_rhs<<<c->count(l), NTH3, 0, c->stream>>>(c->run(), c->ids(l));
+    for (int l = hi; l >= std::max(lo, top) + 1; l--) enq_phase(c, PH_INIT_PHI_RHS, l);
+    if (top >= lo + 1) enq_coarse_kernel(c, CM_INIT, top, 0);
   } else {
-    for (int l = hi; l >= lo + 1; l--) {
-      if (l == hi) enq_fill(c, l);
-      enq_coarse(c, l, false);
-    }
+    // (the residual evaluates the finest level's ghost cells itself, so its
+    // fill_gc_phi, :497-498, is left out)
+    for (int l = hi; l >= std::max(lo, top) + 1; l--) enq_coarse(c, l, false);
+    if (top >= lo + 1) enq_coarse_kernel(c, CM_SETC, top, 0);
   }
-  for (int l = lo; l <= hi; l++) {
-    k3_copy_boxes<<<c->count(l), NTH3, 0, c->stream>>>(c->run(), c->ids(l), I_PHI, I_FLD);
+  if (top >= lo) enq_coarse_kernel(c, CM_FMG, top, first_call ? 1 : 0);
+  for (int l = std::max(lo, top + 1); l <= hi; l++) {
+    enq_phase(c, PH_COPY, l, I_PHI, I_FLD);
     if (l > lo) enq_correct(c, l);
     enq_vcycle(c, l, set_residual && l == hi, first_call && l == lo);
   }
@@ -1068,6 +1242,11 @@ int a5g3_create(const a5g3_params *p, a5g3_ctx **out) {
   *out = nullptr;
   if (p->box_size != NC3) return fail3(A5G_EINVAL, "box_size must be 8");
   if (p->uniform_lvl < 1 || p->uniform_lvl > 12) return fail3(A5G_EINVAL, "uniform_lvl must be 1..12");
+  {
+    // every phase of the finest level must have fewer than 2^31 items
+    const double boxes = (double)p->n_base[0] * p->n_base[1] * p->n_base[2] * std::pow(8.0, p->uniform_lvl - 1);
+    if (boxes * (SLOT3 + 64) >= 2147483647.0) return fail3(A5G_EINVAL, "tree too large (uniform_lvl)");
+  }
   for (int d = 0; d < 3; d++)
     if (p->n_base[d] < 1 || p->n_base[d] > 64) return fail3(A5G_EINVAL, "n_base must be 1..64");
   if (!(p->dr_base > 0) || p->n_cycle_base < 1) return fail3(A5G_EINVAL, "dr_base > 0 and n_cycle_base >= 1 required");
@@ -1100,6 +1279,10 @@ int a5g3_create(const a5g3_params *p, a5g3_ctx **out) {
       cudaMallocHost((void **)&c->h_red, 4 * sizeof(double)) != cudaSuccess)
     return bail(fail3(A5G_ENOMEM, "device allocation failed"));
   c->voltage = -p->domain_len_z * p->applied_fld;
+  // the coarse section: the levels from min_lvl up with at most
+  // COARSE_BOXES boxes each (4,096 cells), never the finest level
+  c->coarse_top = c->min_lvl - 1;
+  for (int l = c->min_lvl; l < c->max_lvl && c->count(l) <= COARSE_BOXES; l++) c->coarse_top = l;
   if (cudaStreamSynchronize(c->stream) != cudaSuccess) return bail(fail3(A5G_ECUDA, "setup failed"));
   *out = c;
   return A5G_OK;
