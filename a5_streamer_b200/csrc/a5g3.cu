@@ -60,6 +60,7 @@ struct Run3 {
   const int *ids;
   int lo, nlev, n_cycle_base;
   int lv_off[16], lv_n[16], lv_nc[16];
+  int lv_first[16];    // a level's ids are lv_first .. lv_first + lv_n - 1
 };
 enum { S_DT = 0, S_RED = 1 };  // scal[0] dt; scal[1..3] reductions; scal[4] tree max/min
 
@@ -443,12 +444,11 @@ enum {
 };
 
 struct Lv {
-  const int *ids;
-  int n, nc;
+  int first, n, nc;
 };
 __device__ __forceinline__ Lv lv_of(const Run3 &R, int l) {
   const int q = l - R.lo;
-  return Lv{R.ids + R.lv_off[q], R.lv_n[q], R.lv_nc[q]};
+  return Lv{R.lv_first[q], R.lv_n[q], R.lv_nc[q]};
 }
 
 // mg3_box_lpl (:814-848) at interior cell c of a box's phi slot
@@ -623,48 +623,54 @@ __device__ __forceinline__ void phase(const Run3 &R, int op, int l, int a0, int 
     case PH_SWEEP: {
       const int per = n3 / 2;
       for (int k = k0; k < L.n * per; k += stride)
-        it_sweep(R, L.ids[k / per], nc, k % per, a0, a1);
+        it_sweep(R, L.first + k / per, nc, k % per, a0, a1);
       break;
     }
     case PH_FILL: {
       const int per = 6 * nc * nc;
       for (int k = k0; k < L.n * per; k += stride)
-        it_gc(R, L.ids[k / per], k % per, I_PHI, -1, 1);
+        it_gc(R, L.first + k / per, k % per, I_PHI, -1, 1);
       break;
     }
     case PH_RESID_RESTRICT:
-      for (int k = k0; k < L.n * nh; k += stride) it_resid_restrict(R, L.ids[k / nh], nc, k % nh);
+      for (int k = k0; k < L.n * nh; k += stride) it_resid_restrict(R, L.first + k / nh, nc, k % nh);
       break;
     case PH_COARSE_RHS:
-      for (int k = k0; k < L.n * gs; k += stride) it_coarse_rhs(R, L.ids[k / gs], nc, k % gs, a0);
+      for (int k = k0; k < L.n * gs; k += stride) it_coarse_rhs(R, L.first + k / gs, nc, k % gs, a0);
       break;
-    case PH_CORR_DIFF:
-      for (int k = k0; k < L.n * gs; k += stride) {
-        const int id = L.ids[k / gs], c = k % gs;
-        double *tmp = CC(R, I_FLD, id);
-        tmp[c] = CC(R, I_PHI, id)[c] - tmp[c];
+    case PH_CORR_DIFF: {
+      // whole slots, two doubles per item (slots start on 16-byte boundaries)
+      const int h = gs / 2;
+      for (int k = k0; k < L.n * h; k += stride) {
+        const int id = L.first + k / h, c = k % h;
+        double2 *tmp = reinterpret_cast<double2 *>(CC(R, I_FLD, id)) + c;
+        const double2 ph = reinterpret_cast<const double2 *>(CC(R, I_PHI, id))[c], t = *tmp;
+        *tmp = make_double2(ph.x - t.x, ph.y - t.y);
       }
       break;
+    }
     case PH_CORRECT:
-      for (int k = k0; k < L.n * n3; k += stride) it_correct(R, L.ids[k / n3], nc, k % n3);
+      for (int k = k0; k < L.n * n3; k += stride) it_correct(R, L.first + k / n3, nc, k % n3);
       break;
-    case PH_COPY:
-      for (int k = k0; k < L.n * gs; k += stride) {
-        const int id = L.ids[k / gs], c = k % gs;
-        CC(R, a1, id)[c] = CC(R, a0, id)[c];
+    case PH_COPY: {
+      const int h = gs / 2;
+      for (int k = k0; k < L.n * h; k += stride) {
+        const int id = L.first + k / h, c = k % h;
+        reinterpret_cast<double2 *>(CC(R, a1, id))[c] = reinterpret_cast<const double2 *>(CC(R, a0, id))[c];
       }
       break;
+    }
     case PH_INIT_PHI_RHS:
       for (int k = k0; k < L.n * (gs + nh); k += stride) {
         const int q = k / (gs + nh);
-        const int r = k % (gs + nh), id = L.ids[q];
+        const int r = k % (gs + nh), id = L.first + q;
         if (r < gs) CC(R, I_PHI, id)[r] = 0.0;
         else it_restrict_rhs(R, id, nc, r - gs);
       }
       break;
     case PH_RESIDUAL: {
       for (int k = k0; k < L.n * n3; k += stride) {
-        const int id = L.ids[k / n3], t = k % n3;
+        const int id = L.first + k / n3, t = k % n3;
         const double h = R.geo[4 * id + 3], inv_dr_sq = 1 / (h * h);
         const int c = ix3(g, t % nc + 1, (t / nc) % nc + 1, t / (nc * nc) + 1);
         CC(R, I_FLD, id)[c] = CC(R, I_RHS, id)[c] - lpl3(CC(R, I_PHI, id), c, g, inv_dr_sq);
@@ -683,14 +689,17 @@ __host__ __device__ __forceinline__ long long phase_items(int op, int n, int nc)
     case PH_CORRECT:
     case PH_RESIDUAL: return n * n3;
     case PH_INIT_PHI_RHS: return n * (gs + nh);
+    case PH_COPY:
+    case PH_CORR_DIFF: return n * (gs / 2);
     default: return n * gs;
   }
 }
 
 // One phase on the grid (grid-stride over its items).
-template <int NCT>
-__global__ void __launch_bounds__(NTH3) k3_phase(Run3 R, int op, int l, int a0, int a1) {
-  phase<NCT>(R, op, l, a0, a1, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+// One kernel per phase and box size, so that each has its own registers.
+template <int NCT, int OP>
+__global__ void __launch_bounds__(NTH3) k3_phase(Run3 R, int l, int a0, int a1) {
+  phase<NCT>(R, OP, l, a0, a1, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -974,6 +983,7 @@ struct a5g3_ctx {
     R.n_cycle_base = p.n_cycle_base;
     for (int q = 0; q < 16; q++) {
       const bool in = q < R.nlev;
+      R.lv_first[q] = in ? lv_ids[lv_off[q]] : 0;
       R.lv_off[q] = in ? lv_off[q] : 0;
       R.lv_n[q] = in ? lv_n[q] : 0;
       R.lv_nc[q] = in ? nc_of(min_lvl + q) : 0;
@@ -1109,12 +1119,29 @@ static int upload(T *&dst, const std::vector<T> &src, cudaStream_t s) {
 static void enq_gc_all(a5g3_ctx *c, int iv0, int iv1, int bc) {
   k3_gc<<<c->n_all(), NTH3, 0, c->stream>>>(c->run(), c->all_ids(), iv0, iv1, bc);
 }
+template <int NCT>
+static void launch_phase(a5g3_ctx *c, int op, int grid, int l, int a0, int a1) {
+  const Run3 R = c->run();
+  cudaStream_t s = c->stream;
+  switch (op) {
+    case PH_SWEEP: k3_phase<NCT, PH_SWEEP><<<grid, NTH3, 0, s>>>(R, l, a0, a1); break;
+    case PH_FILL: k3_phase<NCT, PH_FILL><<<grid, NTH3, 0, s>>>(R, l, a0, a1); break;
+    case PH_RESID_RESTRICT: k3_phase<NCT, PH_RESID_RESTRICT><<<grid, NTH3, 0, s>>>(R, l, a0, a1); break;
+    case PH_COARSE_RHS: k3_phase<NCT, PH_COARSE_RHS><<<grid, NTH3, 0, s>>>(R, l, a0, a1); break;
+    case PH_CORR_DIFF: k3_phase<NCT, PH_CORR_DIFF><<<grid, NTH3, 0, s>>>(R, l, a0, a1); break;
+    case PH_CORRECT: k3_phase<NCT, PH_CORRECT><<<grid, NTH3, 0, s>>>(R, l, a0, a1); break;
+    case PH_COPY: k3_phase<NCT, PH_COPY><<<grid, NTH3, 0, s>>>(R, l, a0, a1); break;
+    case PH_INIT_PHI_RHS: k3_phase<NCT, PH_INIT_PHI_RHS><<<grid, NTH3, 0, s>>>(R, l, a0, a1); break;
+    case PH_RESIDUAL: k3_phase<NCT, PH_RESIDUAL><<<grid, NTH3, 0, s>>>(R, l, a0, a1); break;
+  }
+}
+
 // One multigrid phase of level l on the grid, about one item per thread.
 static void enq_phase(a5g3_ctx *c, int op, int l, int a0 = 0, int a1 = 0) {
   const long long n = phase_items(op, c->count(l), c->nc_of(l));
   const int grid = (int)std::min<long long>((n + NTH3 - 1) / NTH3, 1LL << 20);
-  if (c->nc_of(l) == NC3) k3_phase<NC3><<<grid, NTH3, 0, c->stream>>>(c->run(), op, l, a0, a1);
-  else k3_phase<0><<<grid, NTH3, 0, c->stream>>>(c->run(), op, l, a0, a1);
+  if (c->nc_of(l) == NC3) launch_phase<NC3>(c, op, grid, l, a0, a1);
+  else launch_phase<0>(c, op, grid, l, a0, a1);
 }
 static void enq_fill(a5g3_ctx *c, int l) { enq_phase(c, PH_FILL, l); }
 
