@@ -62,6 +62,9 @@ def parse():
     ap.add_argument("--large-level", type=int, default=6,
                     help="uniform level of the large-tree grid-mode extra (6: 1M leaf cells; 0: skip)")
     ap.add_argument("--large-steps", type=int, default=10, help="timed steps of the large-tree extra")
+    ap.add_argument("--cube-level", type=int, default=6,
+                    help="uniform level of the 3D octree extra (6: 16.8M leaf cells; 0: skip)")
+    ap.add_argument("--cube-steps", type=int, default=10, help="timed steps of the 3D extra")
     return ap.parse_args()
 
 
@@ -355,6 +358,73 @@ def run_large_tree(level, steps, warmup, flush, clock_index):
     return out
 
 
+def run_cube_3d(level, steps, warmup, flush, clock_index, cpu_seconds=3.0):
+    """The 3D octree form (include/a5g3.h): the 16 mm cube of the 3D case on a
+    uniformly refined octree of the given level (6: 16,777,216 leaf cells,
+    dx = 62.5 um), FP64, initial conditions and first field solve on the
+    device, then steps at the step size get_max_dt gives, each a replay of the
+    captured step graph, L2 flushed before each, CUDA events on the run's
+    stream. Beside it, the oracle's 3D step on a level-4 cube (262,144 leaf
+    cells) timed on the host cores for about cpu_seconds."""
+    import torch
+    from a5_streamer_b200 import config, device3
+    cfg = config.cube_16mm_uniform(level)
+    run = device3.Run3(cfg)
+    run.init()
+    run.sync()
+    dt = run.get_max_dt()
+    st = torch.cuda.ExternalStream(run.stream_ptr())
+    for _ in range(warmup):
+        run.step(dt)
+    run.sync()
+    e0 = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    e1 = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    with ClockSampler(clock_index) as clk:
+        torch.cuda.nvtx.range_push("octree_3d")
+        with torch.cuda.stream(st):
+            for k in range(steps):
+                flush.fill_(k & 0xFF)
+                e0[k].record(st)
+                run.step(dt)
+                e1[k].record(st)
+        run.sync()
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
+    ms = sum(a.elapsed_time(b) for a, b in zip(e0, e1)) / steps
+    bytes_step = run.bytes_per_step()
+    peak = measured_peak()[0]
+    gbs = bytes_step / (ms / 1e3) / 1e9
+    n_leaf = run.n_leaf_cells
+    out = {"workload": f"cube_16mm_uniform_lvl{level}", "leaf_cells": n_leaf, "boxes": run.max_id,
+           "min_lvl": run.min_lvl, "max_lvl": run.max_lvl, "precision": "fp64",
+           "ms_per_step": ms, "value": n_leaf / (ms / 1e3), "unit": UNIT,
+           "algorithmic_bytes_per_step": bytes_step, "achieved_gbs": gbs, "frac_of_measured_hbm": gbs / peak,
+           "clocks": clk.summary(), "l2": L2_NOTE}
+    run.close()
+    # the oracle's 3D step on the host cores (a bounded sample on a smaller cube)
+    try:
+        if cpu_seconds <= 0:
+            raise RuntimeError("skipped (--no-cpu-baseline)")
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import a5ref
+        cfg4 = config.cube_16mm_uniform(4)
+        sim = a5ref.Sim3(cfg4, n_threads=os.cpu_count() or 1)
+        sim.init()
+        dt4 = sim.get_max_dt()
+        t0, n = time.perf_counter(), 0
+        while time.perf_counter() - t0 < cpu_seconds:
+            sim.step(dt4)
+            n += 1
+        el = time.perf_counter() - t0
+        out["cpu_port"] = {"value": sim.n_leaf_cells() * n / el, "unit": UNIT, "cores": os.cpu_count() or 1,
+                           "sample": f"{n} steps ({el:.1f} s) of the level-4 cube (262,144 leaf cells), "
+                                     "oracle port, OpenMP over the boxes of each level"}
+        sim.close()
+    except Exception as exc:  # the oracle is test infrastructure; report, do not fail
+        out["cpu_port"] = {"unavailable": str(exc)}
+    return out
+
+
 def moving_streamer_errors(schedule):
     """Errors of the mixed form where the streamer moves: the 8 mm Cartesian
     case at E_bg = 7 MV/m (levels up to 6, no photoionization), whose head
@@ -583,6 +653,10 @@ def run_b200(args):
     large = None
     if args.large_level > 0 and rank == 0:
         large = run_large_tree(args.large_level, args.large_steps, 3, flush, local)
+    cube = None
+    if args.cube_level > 0 and rank == 0:
+        cube = run_cube_3d(args.cube_level, args.cube_steps, 3, flush, local,
+                           cpu_seconds=0.0 if args.no_cpu_baseline else 3.0)
 
     uneven = None
     if args.runs > 0 and rank == 0:
@@ -621,7 +695,7 @@ def run_b200(args):
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": K * launches_per_step,
             "clocks": clk.summary(), "batched": batched, "mixed": mixed,
-            "uneven_batch": uneven, "large_tree": large,
+            "uneven_batch": uneven, "large_tree": large, "octree_3d": cube,
         }
         print(json.dumps(out), flush=True)
     sim.close()
