@@ -3444,3 +3444,4 @@ double a5ref_kat_lookup(int n_rows, int n_pairs, double x_max, int n_samples) {
 
 // The 3D octree form (uniformly refined octrees), same translation unit.
 #include "a5ref3.inc"
+#include "a5ref_tl.inc"

@@ -292,6 +292,23 @@ int a5ref3_kat_mg(int level, int n_fmg, double *res, double *err);
  * `level`: out8 as a5ref_kat_drift_diff. */
 int a5ref3_kat_drift_diff(int level, double end_time, double *out8);
 
+/* Differentiation check (a5ref_tl.inc). P(p): set_init_cond on every box,
+ * compute_fld with no guess, n_steps time steps at the step sizes dts on the
+ * current (fixed) mesh, then J = the softmax-weighted height of the leaf
+ * cells next to the line x = x0 (weights dy exp((|E| - max |E|) / T)).
+ * a5ref_program returns J; a5ref_tl_program also runs n_dir tangent-linear
+ * directions in lockstep (per direction: the derivative of the table rows,
+ * n_rows x 4 column-major, in dtbl, and of the applied voltage in dV) and
+ * writes dJ[n_dir]. */
+double a5ref_program(a5ref_sim *s, int n_steps, const double *dts, double x0, double T);
+double a5ref_tl_program(a5ref_sim *s, int n_steps, const double *dts, double x0, double T,
+                        int n_dir, const double *dtbl, const double *dV, double *dJ);
+/* (y, dy, |E|) of each leaf cell next to x = x0; returns the count. */
+int a5ref_head_profile(a5ref_sim *s, double x0, double *out3);
+/* Replace the table rows (n_rows x 4, column-major) / the applied field. */
+void a5ref_set_table_rows(a5ref_sim *s, const double *rows_cols);
+void a5ref_set_applied_fld(a5ref_sim *s, double fld);
+
 #ifdef __cplusplus
 }
 #endif

@@ -114,6 +114,11 @@ def lib() -> ctypes.CDLL:
             "a5ref_kat_photon_dist": (D, [D, D, I, I]),
             "a5ref_kat_rng": (V, [pi, I, pi]),
             "a5ref_kat_drift_diff": (I, [I, D, I, pd]),
+            # differentiation check (a5ref_tl.inc)
+            "a5ref_program": (D, [P, I, pd, D, D]),
+            "a5ref_tl_program": (D, [P, I, pd, D, D, I, pd, pd, pd]),
+            "a5ref_head_profile": (I, [P, D, pd]),
+            "a5ref_set_table_rows": (V, [P, pd]), "a5ref_set_applied_fld": (V, [P, D]),
             # the 3D octree form (uniform octrees)
             "a5ref3_create": (P, [ctypes.POINTER(Params)]), "a5ref3_destroy": (V, [P]),
             "a5ref3_init": (I, [P]), "a5ref3_set_init_cond": (V, [P]),
@@ -409,6 +414,40 @@ class Sim:
 
     def photoionization(self, dt: float | None):
         lib().a5ref_op_photoionization(self.h, 0.0 if dt is None else dt, 0 if dt is None else 1)
+
+    # differentiation check (a5ref_tl.inc) ---------------------------------------
+    def program(self, dts, x0: float, T: float) -> float:
+        """J of the fixed-mesh program: initial conditions, first field solve,
+        len(dts) steps, head height at the line x = x0 with softmax temperature T."""
+        d = np.ascontiguousarray(dts, dtype=np.float64)
+        return lib().a5ref_program(self.h, len(d), _dp(d), x0, T)
+
+    def tl_program(self, dts, x0: float, T: float, dtbl, dV):
+        """(J, dJ): tangent-linear run along the directions dtbl[k] (derivative
+        of the table rows, n_rows x 4) and dV[k] (of the applied voltage)."""
+        d = np.ascontiguousarray(dts, dtype=np.float64)
+        dtbl = np.asarray(dtbl, dtype=np.float64)
+        n_dir = dtbl.shape[0]
+        dt_cm = np.ascontiguousarray(np.transpose(dtbl, (0, 2, 1)))  # column-major rows
+        dv = np.ascontiguousarray(dV, dtype=np.float64)
+        dJ = np.zeros(n_dir)
+        J = lib().a5ref_tl_program(self.h, len(d), _dp(d), x0, T, n_dir, _dp(dt_cm), _dp(dv),
+                                   _dp(dJ))
+        return J, dJ
+
+    def head_profile(self, x0: float) -> np.ndarray:
+        n = lib().a5ref_head_profile(self.h, x0, None)
+        out = np.zeros((max(n, 1), 3))
+        lib().a5ref_head_profile(self.h, x0, _dp(out))
+        return out[:n]
+
+    def set_table_rows(self, rows: np.ndarray):
+        """rows: n_rows x 4 (mobility, diffusion, alpha, eta)."""
+        rc = np.ascontiguousarray(np.asarray(rows, dtype=np.float64).T)
+        lib().a5ref_set_table_rows(self.h, _dp(rc))
+
+    def set_applied_fld(self, fld: float):
+        lib().a5ref_set_applied_fld(self.h, fld)
 
     def rng_state(self) -> np.ndarray:
         st = np.zeros(4, dtype=np.int32)
