@@ -174,6 +174,26 @@ SIGNATURES.update({
 })
 
 
+class AdjParams(ctypes.Structure):
+    """a5a_params (include/a5a.h)."""
+    _fields_ = [("n_steps", ctypes.c_int), ("checkpoint_every", ctypes.c_int),
+                ("x0", ctypes.c_double), ("temperature", ctypes.c_double)]
+
+
+_PU = ctypes.POINTER(ctypes.c_uint)
+SIGNATURES.update({
+    # adjoint (include/a5a.h)
+    "a5a_create": (_I, [_P, ctypes.POINTER(AdjParams), _PD, _PP]),
+    "a5a_destroy": (_I, [_P]),
+    "a5a_forward": (_I, [_P, _PD]),
+    "a5a_gradient": (_I, [_P, _PD, _PD, _PD]),
+    "a5a_debug_tape": (_I, [_I, _I, _I, _PI, _PD, _PI, _PI, _I, _I, _I,
+                            ctypes.POINTER(ctypes.c_longlong), _PI, _PU, _PD, _PI, _PU, _PD]),
+    "a5g_set_applied_field": (_I, [_P, _D]),
+    "a5s_set_init_cond": (_I, [_P]),
+})
+
+
 class SimConfig(ctypes.Structure):
     _fields_ = [
         ("dev", Params), ("n_base", ctypes.c_int * 2), ("bg_dens", ctypes.c_double),

@@ -108,3 +108,161 @@ def head_temperature(profile: np.ndarray, tau: float) -> float:
     if not kappa > 0:
         raise ValueError("no curvature at the |E| maximum")
     return 0.5 * kappa * tau * tau
+
+
+def head_profile(meta: np.ndarray, geom: np.ndarray, levels, E: np.ndarray, x0: float,
+                 nc: int = 8) -> np.ndarray:
+    """(y, dy, |E|) of the leaf cells next to the line x = x0 (either side),
+    levels in order, leaves in list order, cells by height: the profile the
+    observable is taken over. E is the |E| variable in slot layout."""
+    out = []
+    for lvl in sorted(levels):
+        for id_ in levels[lvl][1]:
+            r0, r1, dr = geom[id_, 0], geom[id_, 1], geom[id_, 3]
+            n = meta[id_, 14]
+            tol = 1e-9 * dr
+            if abs(r0 + n * dr - x0) <= tol:
+                i = n
+            elif abs(r0 - x0) <= tol:
+                i = 1
+            else:
+                continue
+            for j in range(1, n + 1):
+                out.append((r1 + (j - 0.5) * dr, dr, E[id_, i + (n + 2) * j]))
+    return np.array(out).reshape(-1, 3)
+
+
+AdjParams = _lib.AdjParams
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _ip(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+def debug_tape(meta, geom, levels, capacity: int, n_cycle_base: int, seg: int):
+    """The transposed phases of one operation (a5a_debug_tape), as arrays
+    (phase_row, row_d, row_self, row_term, term_s, term_c, vector length)."""
+    meta = np.ascontiguousarray(meta, dtype=np.int32)
+    geom = np.ascontiguousarray(geom, dtype=np.float64)
+    lo, hi = min(levels), max(levels)
+    counts, ids = [], []
+    for lvl in range(lo, hi + 1):
+        a, b, c = levels[lvl]
+        counts += [len(a), len(b), len(c)]
+        ids += list(a) + list(b) + list(c)
+    counts = np.asarray(counts, dtype=np.int32)
+    ids = np.asarray(ids if ids else [0], dtype=np.int32)
+    sizes = (ctypes.c_longlong * 4)()
+    args = (meta.shape[0] - 1, lo, hi, _ip(meta), _dp(geom), _ip(counts), _ip(ids), capacity,
+            n_cycle_base, seg, sizes)
+    call("a5a_debug_tape", *args, None, None, None, None, None, None)
+    n_p, n_r, n_t, n_x = (int(v) for v in sizes)
+    pr = np.zeros(n_p + 1, dtype=np.int32)
+    rd = np.zeros(max(n_r, 1), dtype=np.uint32)
+    rs = np.zeros(max(n_r, 1))
+    rt = np.zeros(n_r + 1, dtype=np.int32)
+    ts = np.zeros(max(n_t, 1), dtype=np.uint32)
+    tc = np.zeros(max(n_t, 1))
+    u = ctypes.POINTER(ctypes.c_uint)
+    call("a5a_debug_tape", *args, _ip(pr), rd.ctypes.data_as(u), _dp(rs), _ip(rt),
+         ts.ctypes.data_as(u), _dp(tc))
+    return pr, rd[:n_r], rs[:n_r], rt, ts[:n_t], tc[:n_t], n_x
+
+
+class HeadAdjoint:
+    """Device adjoint (include/a5a.h) of the head observable on the fixed mesh
+    of an initialised :class:`streamer.Simulation`.
+
+    ``schedule`` runs the nominal program once to record the step sizes (one
+    get_max_dt per block of num_steps_amr steps, as the main loop takes
+    them) and the softmax temperature; ``value`` and ``gradient`` evaluate P
+    at parameters p, setting the run's table and applied field first."""
+
+    def __init__(self, sim, problem: HeadProblem | None = None):
+        self.sim = sim
+        self.prob = problem or HeadProblem()
+        self.cfg = sim.cfg
+        self.ctx = sim.device._borrowed
+        self.h = None
+        self.dts = None
+        self.temperature = None
+        tab, self.x_min, self.inv_dx = sim.table()
+        self.n_rows = tab.shape[0]
+
+    def set_params(self, p) -> None:
+        rows = table_rows(p, self.n_rows, self.cfg.lkptbl_max_fld)
+        flat = np.ascontiguousarray(rows.T.reshape(-1))
+        call("a5g_set_table", self.ctx, self.n_rows, 4, self.x_min, self.inv_dx, _dp(flat))
+        call("a5g_set_applied_field", self.ctx, float(p[4]))
+
+    def schedule(self, p=None):
+        """Record dts and T on the nominal trajectory; returns (dts, T)."""
+        p = self.prob.nominal() if p is None else p
+        self.set_params(p)
+        call("a5s_set_init_cond", self.sim.h)
+        dev = self.sim.device
+        dev.compute_fld(True)
+        dts = []
+        while len(dts) < self.prob.n_steps:
+            dt = ctypes.c_double(0)
+            call("a5g_get_max_dt", self.ctx, ctypes.byref(dt))
+            for _ in range(self.cfg.num_steps_amr):
+                call("a5g_step", self.ctx, dt.value)
+                dts.append(dt.value)
+        self.dts = np.array(dts[:self.prob.n_steps])
+        meta, geom, levels = self.sim.tree.export()
+        prof = head_profile(meta, geom, levels, dev.cc(5), self.prob.x0, self.cfg.box_size)
+        self.temperature = head_temperature(prof, self.prob.tau)
+        return self.dts, self.temperature
+
+    def bind(self, dts=None, temperature=None):
+        """Create the device adjoint; the run is put in the initial state."""
+        if dts is not None:
+            self.dts = np.ascontiguousarray(dts, dtype=np.float64)
+        if temperature is not None:
+            self.temperature = float(temperature)
+        if self.dts is None or self.temperature is None:
+            raise ValueError("call schedule() or pass dts and temperature")
+        self.close()
+        call("a5s_set_init_cond", self.sim.h)
+        ap = AdjParams(len(self.dts), self.prob.checkpoint_every, self.prob.x0, self.temperature)
+        h = ctypes.c_void_p()
+        d = np.ascontiguousarray(self.dts, dtype=np.float64)
+        call("a5a_create", self.ctx, ctypes.byref(ap), _dp(d), ctypes.byref(h))
+        self.h = h
+        return self
+
+    def close(self):
+        if self.h is not None and self.h.value:
+            _lib.lib().a5a_destroy(self.h)
+        self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def value(self, p) -> float:
+        self.set_params(p)
+        J = ctypes.c_double(0)
+        call("a5a_forward", self.h, ctypes.byref(J))
+        return J.value
+
+    def gradient_raw(self, p):
+        """(J, dJ/d(table rows) n_rows x 4, dJ/dV) at parameters p."""
+        self.set_params(p)
+        J = ctypes.c_double(0)
+        dV = ctypes.c_double(0)
+        g = np.zeros(4 * self.n_rows)
+        call("a5a_gradient", self.h, ctypes.byref(J), _dp(g), ctypes.byref(dV))
+        return J.value, g.reshape(4, self.n_rows).T.copy(), dV.value
+
+    def gradient(self, p):
+        """(J, dJ/dp) at parameters p = (mu, D, A, B, E_bg)."""
+        J, gt, gv = self.gradient_raw(p)
+        return J, chain_to_params(gt, gv, p, self.cfg.domain_len_z)

@@ -19,6 +19,7 @@
 // in the reference's Fortran (compiled for x86-64 without FMA) and as in the
 // CPU oracle; each device routine cites the reference routine it follows.
 #include "../../include/a5g.h"
+#include "a5_internal.h"
 
 #include <cuda_runtime.h>
 
@@ -495,6 +496,8 @@ struct a5g_ctx {
   // level-set boundaries (a5g_set_level_set): two cell arrays of the box
   // capacity, grown with the box storage
   double *lsf = nullptr, *bval = nullptr;
+  // host copy of the last uploaded topology (a5g_internal_view)
+  A5Topo topo;
 };
 
 // Shared-memory staging of the multigrid variables as allowed and as fits
@@ -1461,6 +1464,14 @@ int a5g_upload_tree(a5g_ctx *c, int max_id, int min_lvl, int max_lvl, const int 
     if ((r = upload_vec(c, c->ph_boxes, c->ph_boxes_cap, pb))) return r;
     h.ph_boxes = c->ph_boxes;
   }
+  c->topo.max_id = max_id;
+  c->topo.min_lvl = min_lvl;
+  c->topo.max_lvl = max_lvl;
+  c->topo.meta16.assign(meta16, meta16 + 16 * (size_t)(max_id + 1));
+  c->topo.geom4.assign(geom4, geom4 + 4 * (size_t)(max_id + 1));
+  c->topo.ids = lv_ids;
+  c->topo.leaves = lv_leaves;
+  c->topo.parents = lv_parents;
   c->has_tree = true;
   CK(cudaStreamSynchronize(c->stream));
   return push_run(c);
@@ -2256,6 +2267,40 @@ extern "C" int a5g_debug_set_staging(a5g_ctx *c, int allow_smem) {
   int r = push_run(c);
   if (r) return r;
   return mx_ready(c);
+}
+
+int a5g_set_applied_field(a5g_ctx *c, double applied_fld) {
+  if (!c) return fail(A5G_EINVAL, "null argument");
+  if (!std::isfinite(applied_fld)) return fail(A5G_EINVAL, "applied field must be finite");
+  c->p.applied_fld = applied_fld;
+  c->h.applied_voltage = -c->p.domain_len_z * applied_fld;
+  return push_run(c);
+}
+
+int a5g_internal_view(a5g_ctx *c, A5View *v) {
+  if (!c || !v) return fail(A5G_EINVAL, "null argument");
+  v->stream = (void *)c->stream;
+  v->cc = c->cc;
+  v->fx = c->fx;
+  v->fy = c->fy;
+  v->capacity = c->capacity;
+  v->coord = c->p.coord;
+  v->n_cycle_base = c->p.n_cycle_base;
+  v->precision = c->precision;
+  v->photoi_enabled = c->p.photoi_enabled;
+  v->n_cta = c->n_cta;
+  v->has_lsf = c->h.has_lsf;
+  v->has_table = c->has_table;
+  v->applied_fld = c->p.applied_fld;
+  v->domain_len_z = c->p.domain_len_z;
+  v->epsilon_diel = c->p.epsilon_diel;
+  v->tbl_rows = c->tbl_rows;
+  v->tbl_cols = c->tbl_cols;
+  v->tbl_xmin = c->tbl_xmin;
+  v->tbl_inv_dx = c->tbl_inv_dx;
+  v->tbl_host = c->h_tbl.data();
+  v->topo = c->has_tree ? &c->topo : nullptr;
+  return A5G_OK;
 }
 
 int a5g_sync(a5g_ctx *c) {

@@ -680,6 +680,13 @@ int a5s_init(a5s_sim *s, int *n_iter) {
   return a5g_sync(s->ctx);
 }
 
+int a5s_set_init_cond(a5s_sim *s) {
+  if (!s) return err(A5G_EINVAL, "null sim");
+  int r = s->init_cond_all();
+  if (r) return r;
+  return a5g_sync(s->ctx);
+}
+
 // The regrid at the end of a main-loop block (src/streamer_2d.f90:130-141):
 // refinement flags, a$D_adjust_refinement, prolongation into new boxes and a
 // field solve when the tree changed.

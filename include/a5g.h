@@ -346,6 +346,12 @@ int a5g_get_ctas(a5g_ctx *ctx, int *n_cta, int *max_cta);
 int a5g_set_grid_local(a5g_ctx *ctx, int cells);
 /* Wait for all work queued on the context's stream. */
 int a5g_sync(a5g_ctx *ctx);
+/* Change the background field of a run (ST_applied_fld; the potential at
+ * the top is -domain_len_z * applied_fld, src/m_streamer.f90:411) without
+ * rebuilding it, for runs that vary it on a fixed mesh (finite-difference
+ * checks of the adjoint, include/a5a.h). Takes effect at the next field
+ * solve. */
+int a5g_set_applied_field(a5g_ctx *ctx, double applied_fld);
 /* The cudaStream_t (as void*) all work of this context is queued on, so a
  * caller can order its own work or timing events with it. */
 int a5g_get_stream(a5g_ctx *ctx, void **stream);

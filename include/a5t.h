@@ -83,6 +83,9 @@ int a5s_create(const a5s_config *cfg, a5s_sim **out);
 int a5s_destroy(a5s_sim *s);
 /* Initial refinement loop (src/streamer_2d.f90:58-63). */
 int a5s_init(a5s_sim *s, int *n_iter);
+/* set_init_cond on every box of the current tree (src/streamer_2d.f90:218-248:
+ * the seed densities, phi = 0, eps), without refinement. */
+int a5s_set_init_cond(a5s_sim *s);
 /* One main-loop block: get_max_dt, num_steps_amr steps, regrid. */
 int a5s_advance(a5s_sim *s, int regrid, double *dt_used);
 /* Main loop until time > t_end (or max_blocks blocks). */
