@@ -75,6 +75,7 @@ SIGNATURES = {
     "a5g_gc_tree": (_I, [_P, _I, _I]),
     "a5g_average_dens": (_I, [_P]),
     "a5g_compute_fld": (_I, [_P, _I]),
+    "a5g_compute_fld_fp64": (_I, [_P, _I]),
     "a5g_fas_fmg": (_I, [_P, _I, _I]),
     "a5g_fld_from_pot": (_I, [_P]),
     "a5g_mg_fas_vcycle": (_I, [_P, _I, _I]),

@@ -1113,6 +1113,9 @@ static int mx_ready(a5g_ctx *c) {
   c->cc32 = nullptr;
   c->cc32_cap = 0;
   CK(cudaMalloc(&c->cc32, (size_t)3 * c->capacity * SLOT * sizeof(float)));
+  // defined contents: no phase reads an entry it has not written, and zeros
+  // keep it so if one did
+  CK(cudaMemsetAsync(c->cc32, 0, (size_t)3 * c->capacity * SLOT * sizeof(float), c->stream));
   c->cc32_cap = c->capacity;
   c->h.cc32 = c->cc32;
   return push_run(c);
@@ -1566,6 +1569,9 @@ int a5g_compute_fld(a5g_ctx *c, int no_guess) {
   }
   return launch(c, mkop(OP_COMPUTE_FLD, no_guess ? 1 : 0));
 }
+int a5g_compute_fld_fp64(a5g_ctx *c, int no_guess) {
+  return launch(c, mkop(OP_COMPUTE_FLD, no_guess ? 1 : 0));
+}
 int a5g_fas_fmg(a5g_ctx *c, int set_residual, int first_call) {
   return launch(c, mkop(OP_FMG, set_residual ? 1 : 0, first_call ? 1 : 0));
 }
@@ -1943,8 +1949,15 @@ int a5g_step_batch_static(a5g_ctx **ctxs, int n, const double *dts) {
   for (int k = 0; k < n; k++) {
     dyn = std::max(dyn, std::max(ctxs[k]->dyn_smem, step_smem(ctxs[k])));
     if (ctxs[k]->precision == A5G_MIXED) {
-      int r = mx_ready(ctxs[k]);
-      if (r) return r;
+      // the checks of mx_ready without its allocation: a mixed member whose
+      // FP32 storage is not sized to its tree is refused here
+      const a5g_ctx *m = ctxs[k];
+      if (m->h.diel || m->h.has_lsf)
+        return fail(A5G_EINVAL, "the mixed form does not support dielectric or level-set runs");
+      if (m->mx_smem_fit == 0 && m->cc32_cap < m->capacity)
+        return fail(A5G_ESTATE, "a5g_step_batch_static: a mixed-precision member's FP32 storage "
+                                "is not sized to its tree (call a5g_step_batch or a5g_step once "
+                                "after each tree upload)");
     }
     if (ctxs[k]->p.photoi_enabled) {
       int r = ph_ready(ctxs[k]);

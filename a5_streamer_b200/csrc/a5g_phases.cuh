@@ -1614,14 +1614,22 @@ __device__ __noinline__ void p_mx_residual(const RunDev &R, const MGV<float> &M,
     const int g = B.base + i + L.ncg * j, sc = S.base + i + L.ncg * j;
     double res = 0, ph = 0, rh = 0;
     if (act) {
-      if (B.flags & CF_LEAF) {
-        rh = fac * (e[g] - pi[g]);
-        res = rh - lap_at(R, R.applied_voltage, (const double *)phi, B, L.nc, L.ncg, i, j, inv_dr_sq);
-        rhs[g] = rh;
-        cr[sc] = (float)res;
-      } else {
+      if (B.flags & CF_PARENT) {
+        // the children's residual, restricted into cr on the finer level
         rh = rhs[g];
         res = (double)cr[sc];
+      } else {
+        // leaves get the space charge; a box in neither list (on level
+        // lvls_max, whose lists are never rebuilt) keeps its stored rhs, as
+        // residual_box of the FP64 solve reads it
+        if (B.flags & CF_LEAF) {
+          rh = fac * (e[g] - pi[g]);
+          rhs[g] = rh;
+        } else {
+          rh = rhs[g];
+        }
+        res = rh - lap_at(R, R.applied_voltage, (const double *)phi, B, L.nc, L.ncg, i, j, inv_dr_sq);
+        cr[sc] = (float)res;
       }
       ph = phi[g];
       ce[sc] = 0.0f;

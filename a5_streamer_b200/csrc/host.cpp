@@ -698,7 +698,10 @@ static int regrid_block(a5s_sim *s) {
     std::vector<int> counts(nlev), ids(std::max(na, 1));
     a5t_new_boxes(s->tree, counts.data(), ids.data());
     if ((r = a5g_prolong_new(s->ctx, counts.data(), ids.data()))) return r;
-    if ((r = a5g_compute_fld(s->ctx, 0))) return r;
+    // in FP64 whatever the run's precision: after a prolongation the
+    // potential's correction is large and smooth, and the mixed form's FP32
+    // correction pass would lose the digits it needs
+    if ((r = a5g_compute_fld_fp64(s->ctx, 0))) return r;
   }
   return A5G_OK;
 }

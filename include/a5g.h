@@ -156,6 +156,13 @@ int a5g_average_dens(a5g_ctx *ctx);
 /* compute_fld, src/streamer_2d.f90:307-343: space charge, one FAS FMG cycle
  * (afivo/src/m_aX_mg.f90:163-565), fld_from_pot and the |E| ghost fill. */
 int a5g_compute_fld(a5g_ctx *ctx, int no_guess);
+/* compute_fld in FP64 whatever the run's precision (a5g_set_precision). For
+ * the solve that follows prolong_to_new_boxes (src/streamer_2d.f90:134-138)
+ * in the mixed form: on new boxes the potential's correction is large and
+ * smooth, and one FP32 correction pass evaluates its Laplacian with too few
+ * digits (max |E| 1.7e-3 off on the 7 MV/m 8 mm case) where the FP64 FAS
+ * solve is not. The a5s driver uses it after every regrid. */
+int a5g_compute_fld_fp64(a5g_ctx *ctx, int no_guess);
 /* mg$D_fas_fmg(tree, mg, set_residual, first_call) alone */
 int a5g_fas_fmg(a5g_ctx *ctx, int set_residual, int first_call);
 /* mg$D_fas_vcycle(tree, mg, max_lvl, set_residual) alone
@@ -269,7 +276,11 @@ int a5g_step_batch(a5g_ctx **ctxs, int n, const double *dts);
  *    (cudaGetSymbolAddress) with that device current; make that first call
  *    before any stream capture;
  *  - every call shares the one array: calls that overlap on the GPU (on
- *    different streams) race; calls queued on one stream are ordered. */
+ *    different streams) race; calls queued on one stream are ordered;
+ *  - a mixed-precision member whose tree does not fit in shared memory keeps
+ *    its FP32 multigrid arrays in device memory, which this call does not
+ *    allocate: after each tree upload, step it once through a5g_step or
+ *    a5g_step_batch, else this call returns A5G_ESTATE. */
 #define A5G_STATIC_BATCH_MAX 1024
 int a5g_step_batch_static(a5g_ctx **ctxs, int n, const double *dts);
 /* Device-driven batch: one main-loop block (src/streamer_2d.f90:68-128:

@@ -184,3 +184,26 @@ def test_precision_argument_checks():
         run.set_precision(True, (0, 0, 2, 8, 1))
     run.set_precision(False)
     assert run.precision()[0] is False
+
+
+def test_mixed_on_a_tree_reaching_lvls_max():
+    """The moving streamer at 7 MV/m refines to its finest allowed level,
+    whose boxes are in neither the leaf nor the parent list. The mixed form
+    stays finite and deterministic there, and close to FP64."""
+    from a5_streamer_b200 import config, streamer
+    cfg = config.cartesian_8mm(applied_fld=7e6, lvls_max=6)
+    out = []
+    for mixed in (False, True, True):
+        s = streamer.Simulation(cfg)
+        if mixed:
+            s.device.set_precision(True, (1, 2, 2, 8, 1))
+        s.init()
+        for _ in range(8):
+            s.advance(True)
+        meta = s.tree.export()[0]
+        out.append((s.device.tree_max_cc(5), s.device.cc(5), meta))
+        s.close()
+    assert (out[0][2][:, 0].astype(bool) & (out[0][2][:, 1] == cfg.lvls_max)).any()
+    assert np.isfinite(out[1][0])
+    assert np.array_equal(out[1][1], out[2][1])
+    assert abs(out[1][0] - out[0][0]) <= 1e-4 * out[0][0]

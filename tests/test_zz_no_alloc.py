@@ -102,3 +102,36 @@ def test_static_batch_rejects_oversize():
     code = _lib.lib().a5g_step_batch_static(arr, n, d.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
     assert code == _lib.A5G_EINVAL
     assert b"A5G_STATIC_BATCH_MAX" in _lib.lib().a5g_last_error()
+
+
+def test_static_batch_refuses_unsized_fp32_storage():
+    """A mixed member whose tree is not staged in shared memory keeps FP32
+    arrays in device memory, sized to its box storage. When a tree upload
+    grows that storage, the allocation-free call does not allocate new
+    arrays: it refuses the member until one ordinary step has sized them,
+    and then gives what a5g_step_batch gives."""
+    cfg = config.cartesian_8mm()
+    small = a5ref.Sim(cfg, n_threads=2)
+    small.init()
+    big_cfg = config.cartesian_uniform(4)
+    big = a5ref.Sim(big_cfg, n_threads=2)
+    big.init()
+    runs = []
+    for _ in range(2):
+        r = _member(cfg, small, mixed=True)
+        _lib.call("a5g_debug_set_staging", r.h, 0)   # FP32 arrays in device memory
+        device_from_oracle(big, big_cfg, r)          # grows the box storage
+        runs.append(r)
+    a, b = runs
+    dt = [big.get_max_dt()]
+    arr = (ctypes.c_void_p * 1)(b.h.value)
+    d = np.ascontiguousarray(dt, dtype=np.float64)
+    code = _lib.lib().a5g_step_batch_static(arr, 1, d.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    assert code == _lib.A5G_ESTATE
+    assert b"FP32 storage" in _lib.lib().a5g_last_error()
+    _call("a5g_step_batch", [a], dt)
+    _call("a5g_step_batch", [b], dt)     # sizes b's FP32 arrays
+    _call("a5g_step_batch", [a], dt)
+    _call("a5g_step_batch_static", [b], dt)
+    for xa, xb in zip(_state(a), _state(b)):
+        assert np.array_equal(xa, xb)
