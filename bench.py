@@ -65,6 +65,7 @@ def parse():
     ap.add_argument("--cube-level", type=int, default=6,
                     help="uniform level of the 3D octree extra (6: 16.8M leaf cells; 0: skip)")
     ap.add_argument("--cube-steps", type=int, default=10, help="timed steps of the 3D extra")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiation extra")
     return ap.parse_args()
 
 
@@ -425,6 +426,57 @@ def run_cube_3d(level, steps, warmup, flush, clock_index, cpu_seconds=3.0):
     return out
 
 
+def run_adjoint(reps=3):
+    """The differentiation addition (include/a5a.h): the 8 mm Cartesian case
+    without photoionization, 200 steps at the nominal step-size schedule on
+    the mesh of the initial refinement, checkpoints every 20 steps; the head
+    observable's gradient with respect to (mu, D, A, B, E_bg). Timed (wall
+    clock, each call synchronised): the program alone (a5a_forward) and the
+    gradient (a5a_gradient: forward pass with stored states, recomputation of
+    each interval, reverse pass); errors of the gradient against central
+    differences (h = 1e-6 relative) of the device program."""
+    import numpy as np
+    from a5_streamer_b200 import adjoint, streamer
+    prob = adjoint.HeadProblem()
+    cfg = prob.config()
+    sim = streamer.Simulation(cfg)
+    sim.init()
+    adj = adjoint.HeadAdjoint(sim, prob)
+    dts, T = adj.schedule()
+    adj.bind()
+    p0 = prob.nominal()
+    adj.value(p0)
+    adj.gradient(p0)
+    tf, tg = [], []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        J = adj.value(p0)
+        tf.append(time.perf_counter() - t0)
+        t0 = time.perf_counter()
+        J2, g = adj.gradient(p0)
+        tg.append(time.perf_counter() - t0)
+    fd = np.zeros(5)
+    for k in range(5):
+        v = []
+        for sg in (1.0, -1.0):
+            p = p0.copy()
+            p[k] *= 1 + sg * 1e-6
+            v.append(adj.value(p))
+        fd[k] = (v[0] - v[1]) / (2e-6 * p0[k])
+    adj.close()
+    n_leaf = sim.device.n_leaf_cells()
+    sim.close()
+    rel = np.abs(g - fd) / np.abs(fd)
+    return {"workload": "cartesian_8mm fixed mesh, 200 steps, checkpoints every 20, photoionization off",
+            "leaf_cells": n_leaf, "steps": prob.n_steps, "observable": "head height at x = 4 mm",
+            "temperature_V_per_m": T, "tau_m": prob.tau, "J_m": J,
+            "params": list(adjoint.PARAM_NAMES), "p0": p0.tolist(),
+            "dJ_dp": g.tolist(), "dJ_dlnp": (g * p0).tolist(), "fd": fd.tolist(),
+            "rel_err_vs_fd": rel.tolist(), "max_rel_err_vs_fd": float(rel.max()),
+            "forward_s": min(tf), "gradient_s": min(tg), "gradient_over_forward": min(tg) / min(tf),
+            "timing": f"wall clock, best of {reps}, each call synchronised"}
+
+
 def moving_streamer_errors(schedule):
     """Errors of the mixed form where the streamer moves: the 8 mm Cartesian
     case at E_bg = 7 MV/m (levels up to 6, no photoionization), whose head
@@ -658,6 +710,10 @@ def run_b200(args):
         cube = run_cube_3d(args.cube_level, args.cube_steps, 3, flush, local,
                            cpu_seconds=0.0 if args.no_cpu_baseline else 3.0)
 
+    adj = None
+    if not args.no_adjoint and rank == 0:
+        adj = run_adjoint()
+
     uneven = None
     if args.runs > 0 and rank == 0:
         sched_u = mixed["schedule"] if mixed else None
@@ -696,6 +752,7 @@ def run_b200(args):
             "gpu_launches": K * launches_per_step,
             "clocks": clk.summary(), "batched": batched, "mixed": mixed,
             "uneven_batch": uneven, "large_tree": large, "octree_3d": cube,
+            "adjoint": adj,
         }
         print(json.dumps(out), flush=True)
     sim.close()
