@@ -171,6 +171,8 @@ SIGNATURES.update({
     "a5g3_tree_max_cc": (_I, [_P, _I, _PD]), "a5g3_tree_min_cc": (_I, [_P, _I, _PD]),
     "a5g3_dt_reductions": (_I, [_P, _PD]), "a5g3_get_max_dt": (_I, [_P, _PD]),
     "a5g3_step": (_I, [_P, _D]), "a5g3_sync": (_I, [_P]),
+    "a5g3_set_precision": (_I, [_P, _I, ctypes.POINTER(MGSchedule)]),
+    "a5g3_get_precision": (_I, [_P, _PI, ctypes.POINTER(MGSchedule)]),
     "a5g3_stream": (_I, [_P, _PP]),
 })
 

@@ -49,6 +49,7 @@ struct Run3 {
   const int *off;      // [cap][3] offset of the box's cells in its parent (child offset)
   const double *geo;   // [cap][4] r_min[3], dr
   const double *lt;    // transport table, rows x 4, column-major
+  const float *lt32;   // its FP32 copy (the mixed form's lookups)
   double *scal;        // device scalars (S_*)
   double *part;        // per-block partial reductions
   long long cap;       // slots (max_id + 1)
@@ -73,46 +74,6 @@ __device__ __forceinline__ double *FC(const Run3 &R, int d, int f, int id) {
 }
 __device__ __forceinline__ int ix3(int g, int i, int j, int k) { return i + g * (j + g * k); }
 
-// fosito/m_lookup_table.f90:107-125 (get_loc, ceiling of the fractional
-// index; beyond the int range clamped to the table end) and :154-161
-struct Loc3 {
-  int ix;
-  double fr;
-};
-__device__ __forceinline__ Loc3 lt_loc(const Run3 &R, double x) {
-  const double frac = (x - R.lt_xmin) * R.lt_inv_dx;
-  Loc3 l;
-  if (frac < 2.0e9 && frac > -2.0e9) {
-    l.ix = (int)ceil(frac);
-    l.fr = l.ix - frac;
-  } else {
-    l.ix = frac > 0 ? R.lt_rows : 0;
-    l.fr = 0;
-  }
-  if (l.ix < 1) {
-    l.ix = 1;
-    l.fr = 1;
-  } else if (l.ix >= R.lt_rows) {
-    l.ix = R.lt_rows - 1;
-    l.fr = 0;
-  }
-  return l;
-}
-__device__ __forceinline__ double lt_col(const Run3 &R, int col, const Loc3 &l) {
-  const double *c = R.lt + (size_t)R.lt_rows * col;
-  return l.fr * c[l.ix - 1] + (1 - l.fr) * c[l.ix];
-}
-
-// src/m_streamer.f90:339-362 (koren_mlim)
-__device__ __forceinline__ double koren_mlim(double a, double b) {
-  const double sixth = 1 / 6.0;
-  const double aa = a * a, ab = a * b;
-  if (ab <= 0) return 0;
-  if (aa <= 0.25 * ab) return a;
-  if (aa <= 2.5 * ab) return sixth * (b + 2 * a);
-  return b;
-}
-
 // gfortran's NORM2 of a 3-vector: scaled sum of squares, the scale raised
 // whenever a larger |x| appears
 __device__ __forceinline__ double norm2_3(const double x[3]) {
@@ -133,6 +94,80 @@ __device__ __forceinline__ double norm2_3(const double x[3]) {
   }
   return scale * sqrt(ssq);
 }
+
+// The same lookup, limiter and norm in the arithmetic type T of the transport
+// (double: the expressions above; float: the mixed form, on the FP32 table).
+template <class T>
+struct LocT {
+  int ix;
+  T fr;
+};
+template <class T>
+__device__ __forceinline__ const T *lt_tab(const Run3 &R);
+template <>
+__device__ __forceinline__ const double *lt_tab<double>(const Run3 &R) { return R.lt; }
+template <>
+__device__ __forceinline__ const float *lt_tab<float>(const Run3 &R) { return R.lt32; }
+template <class T>
+__device__ __forceinline__ LocT<T> lt_locT(const Run3 &R, T x) {
+  const T frac = (x - T(R.lt_xmin)) * T(R.lt_inv_dx);
+  LocT<T> l;
+  if (frac < T(2.0e9) && frac > T(-2.0e9)) {
+    l.ix = (int)ceil(frac);
+    l.fr = T(l.ix) - frac;
+  } else {
+    l.ix = frac > T(0) ? R.lt_rows : 0;
+    l.fr = 0;
+  }
+  if (l.ix < 1) {
+    l.ix = 1;
+    l.fr = 1;
+  } else if (l.ix >= R.lt_rows) {
+    l.ix = R.lt_rows - 1;
+    l.fr = 0;
+  }
+  return l;
+}
+template <class T>
+__device__ __forceinline__ T lt_colT(const Run3 &R, int col, const LocT<T> &l) {
+  const T *c = lt_tab<T>(R) + (size_t)R.lt_rows * col;
+  return l.fr * c[l.ix - 1] + (T(1) - l.fr) * c[l.ix];
+}
+template <class T>
+__device__ __forceinline__ T koren_mlimT(T a, T b) {
+  const T sixth = T(1 / 6.0);
+  const T aa = a * a, ab = a * b;
+  if (ab <= T(0)) return 0;
+  if (aa <= T(0.25) * ab) return a;
+  if (aa <= T(2.5) * ab) return sixth * (b + 2 * a);
+  return b;
+}
+template <class T>
+__device__ __forceinline__ T norm2_3T(const T x[3]) {
+  T scale = 0, ssq = 1;
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    if (x[k] != T(0)) {
+      const T ax = fabs(x[k]);
+      if (scale < ax) {
+        const T v = scale / ax;
+        ssq = T(1) + ssq * v * v;
+        scale = ax;
+      } else {
+        const T v = ax / scale;
+        ssq += v * v;
+      }
+    }
+  }
+  return scale * sqrt(ssq);
+}
+// Densities enter the FP32 fluxes scaled by 2^-40, an exact power of two:
+// Koren's limiter and the flux are homogeneous of degree one in the density,
+// and the squares of density differences stay inside the float range.
+template <class T>
+__device__ __forceinline__ T dscale() { return T(1); }
+template <>
+__device__ __forceinline__ float dscale<float>() { return 0x1p-40f; }
 
 // ---------------------------------------------------------------------------
 // a3_tree_copy_cc for two variable pairs at once (elec -> elec_old, pion ->
@@ -168,21 +203,23 @@ __global__ void k3_average(Run3 R) {
 // ghost layer (a3_gc2_box with sides2_from_nb / a3_gc2_neumann,
 // afivo/src/m_aX_gc.f90:407-483, 588-622) read from the neighbour's slot or
 // the box's own, then every x, y and z face of the box (3 (nc+1) nc^2).
+template <class T>
 __global__ void __launch_bounds__(NTH3) k3_fluxes(Run3 R, const int *ids) {
-  __shared__ double se[SLOT3], sf[SLOT3];
+  __shared__ T se[SLOT3], sf[SLOT3];
   const int id = ids[blockIdx.x];
   const int nc = R.nc[id], g = nc + 2, gs = g * g * g;
+  const T ds = dscale<T>();
   {
     const double *e = CC(R, I_ELEC, id), *f = CC(R, I_FLD, id);
     for (int k = threadIdx.x; k < gs; k += NTH3) {
-      se[k] = e[k];
-      sf[k] = f[k];
+      se[k] = T(e[k]) * ds;
+      sf[k] = T(f[k]);
     }
   }
   __syncthreads();
   const double dt = R.scal[S_DT];
-  const double inv_dr = 1 / R.geo[4 * id + 3];
-  const double fac = -0.8 * UC_EPS0 / (UC_ELEM_CHARGE * dt);
+  const T inv_dr = T(1 / R.geo[4 * id + 3]);
+  const T fac = T(-0.8 * UC_EPS0 / (UC_ELEM_CHARGE * dt)) * ds;
   const int *nb = R.nbr + 6 * id;
   const int F = (nc + 1) * nc * nc;
   for (int q = threadIdx.x; q < 3 * F; q += NTH3) {
@@ -205,78 +242,81 @@ __global__ void __launch_bounds__(NTH3) k3_fluxes(Run3 R, const int *ids) {
     const int a = d == 0 ? i : d == 1 ? j : k;
     const int st = d == 0 ? 1 : d == 1 ? g : g * g;
     const int c0 = ix3(g, i, j, k), cm1 = c0 - st;
-    const double e0 = se[c0], em1 = se[cm1];
-    double em2, ep1;
+    const T e0 = se[c0], em1 = se[cm1];
+    T em2, ep1;
     // second ghost layer where the stencil leaves the box (a == 1 / nc + 1)
     if (a == 1) {
       const int n = nb[2 * d];
       // c0 is cell 1: the neighbour's cell nc - 1, or own cell 2
-      em2 = n > 0 ? CC(R, I_ELEC, n)[c0 + (nc - 2) * st] : se[c0 + st];
+      em2 = n > 0 ? T(CC(R, I_ELEC, n)[c0 + (nc - 2) * st]) * ds : se[c0 + st];
     } else {
       em2 = se[c0 - 2 * st];
     }
     if (a == nc + 1) {
       const int n = nb[2 * d + 1];
       // c0 is the ghost cell nc + 1: the neighbour's cell 2, or own cell nc - 1
-      ep1 = n > 0 ? CC(R, I_ELEC, n)[c0 - (nc - 1) * st] : se[c0 - 2 * st];
+      ep1 = n > 0 ? T(CC(R, I_ELEC, n)[c0 - (nc - 1) * st]) * ds : se[c0 - 2 * st];
     } else {
       ep1 = se[c0 + st];
     }
-    const double fld_avg = 0.5 * (sf[c0] + sf[cm1]);
-    const Loc3 loc = lt_loc(R, fld_avg);
-    const double mobility = lt_col(R, C_MOB, loc);
-    const double diff_coeff = lt_col(R, C_DIF, loc);
+    const T fld_avg = T(0.5) * (sf[c0] + sf[cm1]);
+    const LocT<T> loc = lt_locT<T>(R, fld_avg);
+    const T mobility = lt_colT<T>(R, C_MOB, loc);
+    const T diff_coeff = lt_colT<T>(R, C_DIF, loc);
     double *fe = FC(R, d, F_ELEC, id);
-    const double fld = FC(R, d, F_FLD, id)[r];
-    const double v_drift = -mobility * fld;
-    const double gradc = e0 - em1;
-    double out;
-    if (v_drift < 0.0) {
-      const double gradn = ep1 - e0;
-      out = v_drift * (e0 - koren_mlim(gradc, gradn));
+    const T fld = T(FC(R, d, F_FLD, id)[r]);
+    const T v_drift = -mobility * fld;
+    const T gradc = e0 - em1;
+    T out;
+    if (v_drift < T(0)) {
+      const T gradn = ep1 - e0;
+      out = v_drift * (e0 - koren_mlimT<T>(gradc, gradn));
       if (out < fac * fld) out = fac * fld;
     } else {
-      const double gradp = em1 - em2;
-      out = v_drift * (em1 + koren_mlim(gradc, gradp));
+      const T gradp = em1 - em2;
+      out = v_drift * (em1 + koren_mlimT<T>(gradc, gradp));
       if (out > fac * fld) out = fac * fld;
     }
-    fe[r] = out - diff_coeff * gradc * inv_dr;
+    fe[r] = (double)(out - diff_coeff * gradc * inv_dr) / (double)ds;
   }
 }
 
 // update_solution (src/streamer_3d.f90:566-615) on one leaf box per block,
 // one interior cell per thread and round; then the dielectric conversion
 // (eps > 1: n_e moves into n_i).
+template <class T>
 __global__ void __launch_bounds__(NTH3) k3_update(Run3 R, const int *ids) {
   const int id = ids[blockIdx.x];
   const int nc = R.nc[id], g = nc + 2, n = nc * nc * nc;
   const double dt = R.scal[S_DT];
-  const double inv_dr = 1 / R.geo[4 * id + 3];
+  const T tdt = T(dt);
+  const T inv_dr = T(1 / R.geo[4 * id + 3]);
   const double *fx = FC(R, 0, F_ELEC, id), *fy = FC(R, 1, F_ELEC, id), *fz = FC(R, 2, F_ELEC, id);
   double *e = CC(R, I_ELEC, id), *p = CC(R, I_PION, id);
   const double *fld = CC(R, I_FLD, id), *eps = CC(R, I_EPS, id);
   for (int t = threadIdx.x; t < n; t += NTH3) {
     const int i = t % nc + 1, j = (t / nc) % nc + 1, k = t / (nc * nc) + 1;
     const int c = ix3(g, i, j, k);
-    const Loc3 loc = lt_loc(R, fld[c]);
-    const double alpha = lt_col(R, C_ALPHA, loc), eta = lt_col(R, C_ETA, loc);
+    const LocT<T> loc = lt_locT<T>(R, T(fld[c]));
+    const T alpha = lt_colT<T>(R, C_ALPHA, loc), eta = lt_colT<T>(R, C_ETA, loc);
     const int xl = (i - 1) + (nc + 1) * ((j - 1) + nc * (k - 1));
     const int yl = (i - 1) + nc * ((j - 1) + (nc + 1) * (k - 1));
     const int zl = (i - 1) + nc * ((j - 1) + nc * (k - 1));
-    const double x0 = fx[xl], x1 = fx[xl + 1], y0 = fy[yl], y1 = fy[yl + nc], z0 = fz[zl], z1 = fz[zl + nc * nc];
-    double dflux[3];
+    const T x0 = T(fx[xl]), x1 = T(fx[xl + 1]), y0 = T(fy[yl]), y1 = T(fy[yl + nc]), z0 = T(fz[zl]),
+            z1 = T(fz[zl + nc * nc]);
+    T dflux[3];
     dflux[0] = x0 + x1;
     dflux[1] = y0 + y1;
     dflux[2] = z0 + z1;
-    const double src = 0.5 * norm2_3(dflux) * (alpha - eta);
-    double sflux = x0 - x1;
+    const T src = T(0.5) * norm2_3T<T>(dflux) * (alpha - eta);
+    T sflux = x0 - x1;
     sflux = sflux + y0;
     sflux = sflux - y1;
     sflux = sflux + z0;
     sflux = sflux - z1;
     sflux = sflux * inv_dr;
-    double ev = e[c] + (src + sflux) * dt;
-    double pv = p[c] + src * dt;
+    double ev = e[c] + (double)((src + sflux) * tdt);
+    double pv = p[c] + (double)(src * tdt);
     if (eps[c] > 1.0) {
       pv = pv - ev;
       ev = 0;
@@ -451,9 +491,26 @@ __device__ __forceinline__ Lv lv_of(const Run3 &R, int l) {
   return Lv{R.lv_first[q], R.lv_n[q], R.lv_nc[q]};
 }
 
+// The arrays a multigrid solve works on: the potential, its right-hand side
+// and the scratch variable tmp (per-box slots of SLOT3 entries), and the
+// potential of the high-z wall. The FP64 solve works on the run's own
+// variables with the applied voltage; the mixed form's correction solve on
+// FP32 arrays with wall value 0 (its correction equation is homogeneous).
+template <class T>
+struct MG3 {
+  T *phi, *rhs, *tmp;
+  double voltage;
+};
+template <class T>
+__device__ __forceinline__ T *SL(T *a, int id) { return a + (size_t)id * SLOT3; }
+template <class T> struct Pair;
+template <> struct Pair<double> { using type = double2; };
+template <> struct Pair<float> { using type = float2; };
+
 // mg3_box_lpl (:814-848) at interior cell c of a box's phi slot
-__device__ __forceinline__ double lpl3(const double *phi, int c, int g, double inv_dr_sq) {
-  double s = phi[c - 1] + phi[c + 1];
+template <class T>
+__device__ __forceinline__ T lpl3(const T *phi, int c, int g, T inv_dr_sq) {
+  T s = phi[c - 1] + phi[c + 1];
   s = s + phi[c - g];
   s = s + phi[c + g];
   s = s + phi[c - g * g];
@@ -467,29 +524,31 @@ __device__ __forceinline__ double lpl3(const double *phi, int c, int g, double i
 // the same-level neighbour or sides_bc_pot of cell c (src/streamer_3d.f90:
 // 693-715). Equal to the ghost cell in memory whenever that was filled after
 // the sources last changed.
-__device__ __forceinline__ double phi_side(const Run3 &R, int id, int nc, const double *phi, int c, int s, int a,
-                                           int st) {
+template <class T>
+__device__ __forceinline__ T phi_side(const Run3 &R, const MG3<T> &M, int id, int nc, const T *phi, int c, int s,
+                                      int a, int st) {
   const bool hi = s & 1;
   const int cn = hi ? c + st : c - st;
   const int an = hi ? a + 1 : a - 1;
   if (an >= 1 && an <= nc) return phi[cn];
   const int n = R.nbr[6 * id + s];
-  if (n > 0) return CC(R, I_PHI, n)[hi ? cn - nc * st : cn + nc * st];
+  if (n > 0) return SL(M.phi, n)[hi ? cn - nc * st : cn + nc * st];
   if (s == 4) return -phi[c];
-  if (s == 5) return 2 * R.voltage - phi[c];
+  if (s == 5) return T(2 * M.voltage) - phi[c];
   return phi[c];
 }
 
 // mg3_box_lpl (:814-848) at interior cell (i, j, k) = c of box id, the ghost
 // neighbours from their sources (phi_side)
-__device__ __forceinline__ double lpl3_src(const Run3 &R, int id, int nc, const double *phi, int c, int i, int j,
-                                           int k, double inv_dr_sq) {
+template <class T>
+__device__ __forceinline__ T lpl3_src(const Run3 &R, const MG3<T> &M, int id, int nc, const T *phi, int c, int i,
+                                      int j, int k, T inv_dr_sq) {
   const int g = nc + 2;
-  double s = phi_side(R, id, nc, phi, c, 0, i, 1) + phi_side(R, id, nc, phi, c, 1, i, 1);
-  s = s + phi_side(R, id, nc, phi, c, 2, j, g);
-  s = s + phi_side(R, id, nc, phi, c, 3, j, g);
-  s = s + phi_side(R, id, nc, phi, c, 4, k, g * g);
-  s = s + phi_side(R, id, nc, phi, c, 5, k, g * g);
+  T s = phi_side(R, M, id, nc, phi, c, 0, i, 1) + phi_side(R, M, id, nc, phi, c, 1, i, 1);
+  s = s + phi_side(R, M, id, nc, phi, c, 2, j, g);
+  s = s + phi_side(R, M, id, nc, phi, c, 3, j, g);
+  s = s + phi_side(R, M, id, nc, phi, c, 4, k, g * g);
+  s = s + phi_side(R, M, id, nc, phi, c, 5, k, g * g);
   return inv_dr_sq * (s - 6 * phi[c]);
 }
 
@@ -502,28 +561,30 @@ __device__ __forceinline__ double lpl3_src(const Run3 &R, int id, int nc, const 
 // cell itself (read before it is written). mem: read the ghost cells in
 // memory instead (the first half-sweep on the base level of a first FMG
 // call, whose ghosts the reference leaves as they were).
-__device__ __forceinline__ void it_sweep(const Run3 &R, int id, int nc, int t, int it, int mem) {
+template <class T>
+__device__ __forceinline__ void it_sweep(const Run3 &R, const MG3<T> &M, int id, int nc, int t, int it, int mem) {
   const int g = nc + 2, hn = nc >> 1;
   const int k = t / (nc * hn) + 1, rem = t - (k - 1) * nc * hn;
   const int j = rem / hn + 1, m = rem - (j - 1) * hn;
   const int i = 2 - ((it + j + k) & 1) + 2 * m;
   const int c = ix3(g, i, j, k);
-  const double dr = R.geo[4 * id + 3], dx2 = dr * dr;
-  const double sixth = 1 / 6.0;
-  double *phi = CC(R, I_PHI, id);
+  const double dr = R.geo[4 * id + 3];
+  const T dx2 = T(dr * dr);
+  const T sixth = T(1 / 6.0);
+  T *phi = SL(M.phi, id);
   const int pos[3] = {i, j, k}, st[3] = {1, g, g * g};
-  double v[6];
+  T v[6];
 #pragma unroll
   for (int s = 0; s < 6; s++) {
     const int d = s >> 1;
-    v[s] = mem ? phi[(s & 1) ? c + st[d] : c - st[d]] : phi_side(R, id, nc, phi, c, s, pos[d], st[d]);
+    v[s] = mem ? phi[(s & 1) ? c + st[d] : c - st[d]] : phi_side(R, M, id, nc, phi, c, s, pos[d], st[d]);
   }
-  double sum = v[1] + v[0];
+  T sum = v[1] + v[0];
   sum = sum + v[3];
   sum = sum + v[2];
   sum = sum + v[5];
   sum = sum + v[4];
-  phi[c] = sixth * (sum - dx2 * CC(R, I_RHS, id)[c]);
+  phi[c] = sixth * (sum - dx2 * SL(M.rhs, id)[c]);
 }
 
 // update_coarse / set_coarse_phi_rhs, fine part (:430-523), for one parent
@@ -534,41 +595,45 @@ __device__ __forceinline__ void it_sweep(const Run3 &R, int id, int nc, int t, i
 // set_coarse_phi_rhs's copy there is overwritten before any read). Ghost
 // neighbours come from their sources, so no fill of this level is needed
 // before it.
-__device__ __forceinline__ void it_resid_restrict(const Run3 &R, int id, int nc, int u) {
+template <class T>
+__device__ __forceinline__ void it_resid_restrict(const Run3 &R, const MG3<T> &M, int id, int nc, int u) {
   const int g = nc + 2, hnc = nc >> 1;
   const int i = u % hnc + 1, j = (u / hnc) % hnc + 1, k = u / (hnc * hnc) + 1;
-  const double dr = R.geo[4 * id + 3], inv_dr_sq = 1 / (dr * dr);
-  const double *phi = CC(R, I_PHI, id), *rhs = CC(R, I_RHS, id);
+  const double dr = R.geo[4 * id + 3];
+  const T inv_dr_sq = T(1 / (dr * dr));
+  const T *phi = SL(M.phi, id), *rhs = SL(M.rhs, id);
   const int f = ix3(g, 2 * i - 1, 2 * j - 1, 2 * k - 1);
   const int o8[8] = {0, 1, g, g + 1, g * g, g * g + 1, g * g + g, g * g + g + 1};
-  double sr = 0, sp = 0;
+  T sr = 0, sp = 0;
 #pragma unroll
   for (int q = 0; q < 8; q++) {
     const int c = f + o8[q];
-    const double r =
-        rhs[c] - lpl3_src(R, id, nc, phi, c, 2 * i - 1 + (q & 1), 2 * j - 1 + ((q >> 1) & 1), 2 * k - 1 + (q >> 2), inv_dr_sq);
+    const T r = rhs[c] - lpl3_src(R, M, id, nc, phi, c, 2 * i - 1 + (q & 1), 2 * j - 1 + ((q >> 1) & 1),
+                                  2 * k - 1 + (q >> 2), inv_dr_sq);
     sr = q == 0 ? r : sr + r;
     sp = q == 0 ? phi[c] : sp + phi[c];
   }
   const int p = R.par[id], pg = R.nc[p] + 2;
   const int *o = R.off + 3 * id;
   const int pc = ix3(pg, o[0] + i, o[1] + j, o[2] + k);
-  CC(R, I_FLD, p)[pc] = 0.125 * sr;
-  CC(R, I_PHI, p)[pc] = 0.125 * sp;
+  SL(M.tmp, p)[pc] = T(0.125) * sr;
+  SL(M.phi, p)[pc] = T(0.125) * sp;
 }
 
 // Coarse part of update_coarse / set_coarse_phi_rhs (:471-485, :514-521) at
 // slot element c of parent box id: rhs = lpl(phi) on interior cells, then
 // rhs = rhs + tmp on the whole slot (a3_box_add_cc), then with copy tmp =
 // phi (a3_box_copy_cc).
-__device__ __forceinline__ void it_coarse_rhs(const Run3 &R, int id, int nc, int c, int copy) {
+template <class T>
+__device__ __forceinline__ void it_coarse_rhs(const Run3 &R, const MG3<T> &M, int id, int nc, int c, int copy) {
   const int g = nc + 2;
   const int i = c % g, j = (c / g) % g, k = c / (g * g);
   const bool in = i >= 1 && i <= nc && j >= 1 && j <= nc && k >= 1 && k <= nc;
-  const double dr = R.geo[4 * id + 3], inv_dr_sq = 1 / (dr * dr);
-  const double *phi = CC(R, I_PHI, id);
-  double *rhs = CC(R, I_RHS, id), *tmp = CC(R, I_FLD, id);
-  const double a = in ? lpl3(phi, c, g, inv_dr_sq) : rhs[c];
+  const double dr = R.geo[4 * id + 3];
+  const T inv_dr_sq = T(1 / (dr * dr));
+  const T *phi = SL(M.phi, id);
+  T *rhs = SL(M.rhs, id), *tmp = SL(M.tmp, id);
+  const T a = in ? lpl3(phi, c, g, inv_dr_sq) : rhs[c];
   rhs[c] = a + tmp[c];
   if (copy) tmp[c] = phi[c];
 }
@@ -576,30 +641,32 @@ __device__ __forceinline__ void it_coarse_rhs(const Run3 &R, int id, int nc, int
 // correct_children (:374-401): on the parent, tmp = phi - tmp (whole slot),
 // then mg3_box_corr_lpl (:714-766) on each child cell: phi += 0.25 (c1 + c2x
 // + c2y + c2z) of the parent's correction, c1 the closest coarse cell.
-__device__ __forceinline__ void it_correct(const Run3 &R, int id, int nc, int t) {
+template <class T>
+__device__ __forceinline__ void it_correct(const Run3 &R, const MG3<T> &M, int id, int nc, int t) {
   const int g = nc + 2;
   const int p = R.par[id], pg = R.nc[p] + 2;
   const int *o = R.off + 3 * id;
-  const double *corr = CC(R, I_FLD, p);
-  double *phi = CC(R, I_PHI, id);
+  const T *corr = SL(M.tmp, p);
+  T *phi = SL(M.phi, id);
   const int i = t % nc + 1, j = (t / nc) % nc + 1, k = t / (nc * nc) + 1;
   const int i1 = o[0] + ((i + 1) >> 1), i2 = i1 + 1 - 2 * (i & 1);
   const int j1 = o[1] + ((j + 1) >> 1), j2 = j1 + 1 - 2 * (j & 1);
   const int k1 = o[2] + ((k + 1) >> 1), k2 = k1 + 1 - 2 * (k & 1);
-  double s = corr[ix3(pg, i1, j1, k1)] + corr[ix3(pg, i2, j1, k1)];
+  T s = corr[ix3(pg, i1, j1, k1)] + corr[ix3(pg, i2, j1, k1)];
   s = s + corr[ix3(pg, i1, j2, k1)];
   s = s + corr[ix3(pg, i1, j1, k2)];
   const int c = ix3(g, i, j, k);
-  phi[c] = phi[c] + 0.25 * s;
+  phi[c] = phi[c] + T(0.25) * s;
 }
 
 // init_phi_rhs (:526-549), the restriction of one parent cell's rhs
-__device__ __forceinline__ void it_restrict_rhs(const Run3 &R, int id, int nc, int u) {
+template <class T>
+__device__ __forceinline__ void it_restrict_rhs(const Run3 &R, const MG3<T> &M, int id, int nc, int u) {
   const int g = nc + 2, hnc = nc >> 1;
   const int i = u % hnc + 1, j = (u / hnc) % hnc + 1, k = u / (hnc * hnc) + 1;
-  const double *rhs = CC(R, I_RHS, id);
+  const T *rhs = SL(M.rhs, id);
   const int f = ix3(g, 2 * i - 1, 2 * j - 1, 2 * k - 1);
-  double s = rhs[f];
+  T s = rhs[f];
   s = s + rhs[f + 1];
   s = s + rhs[f + g];
   s = s + rhs[f + g + 1];
@@ -609,54 +676,86 @@ __device__ __forceinline__ void it_restrict_rhs(const Run3 &R, int id, int nc, i
   s = s + rhs[f + g * g + g + 1];
   const int p = R.par[id], pg = R.nc[p] + 2;
   const int *o = R.off + 3 * id;
-  CC(R, I_RHS, p)[ix3(pg, o[0] + i, o[1] + j, o[2] + k)] = 0.125 * s;
+  SL(M.rhs, p)[ix3(pg, o[0] + i, o[1] + j, o[2] + k)] = T(0.125) * s;
+}
+
+// fill_gc_phi (:358-371) for item t of box id: a ghost cell of phi from the
+// facing cell of the same-level neighbour or sides_bc_pot
+// (src/streamer_3d.f90:693-715: Neumann on x and y, -phi at low z, 2 V - phi
+// at high z).
+template <class T>
+__device__ __forceinline__ void it_fill(const Run3 &R, const MG3<T> &M, int id, int t) {
+  const int nc = R.nc[id], g = nc + 2, per = nc * nc;
+  const int side = t / per, w = t - side * per;
+  const int a = w % nc + 1, b = w / nc + 1;
+  const int d = side >> 1;
+  const bool low = (side & 1) == 0;
+  const int st = d == 0 ? 1 : d == 1 ? g : g * g;
+  int gcell;
+  if (d == 0) gcell = ix3(g, low ? 0 : nc + 1, a, b);
+  else if (d == 1) gcell = ix3(g, a, low ? 0 : nc + 1, b);
+  else gcell = ix3(g, a, b, low ? 0 : nc + 1);
+  const int own = low ? gcell + st : gcell - st;
+  T *x = SL(M.phi, id);
+  const int n = R.nbr[6 * id + side];
+  T v;
+  if (n > 0) v = SL(M.phi, n)[low ? gcell + nc * st : gcell - nc * st];
+  else if (side == 4) v = -x[own];
+  else if (side == 5) v = T(2 * M.voltage) - x[own];
+  else v = x[own];
+  x[gcell] = v;
 }
 
 // Items k0, k0 + stride, ... of phase op on level l (fewer than 2^31 items
 // per level; a5g3_create checks the tree).
 // NCT: the level's box size at compile time (8 on levels >= 1), 0: read it.
-template <int NCT>
-__device__ __forceinline__ void phase(const Run3 &R, int op, int l, int a0, int a1, int k0, int stride) {
+template <int NCT, class T>
+__device__ __forceinline__ void phase(const Run3 &R, const MG3<T> &M, int op, int l, int a0, int a1, int k0,
+                                      int stride) {
   const Lv L = lv_of(R, l);
   const int nc = NCT ? NCT : L.nc, g = nc + 2, gs = g * g * g, n3 = nc * nc * nc, hnc = nc >> 1, nh = hnc * hnc * hnc;
+  using P2 = typename Pair<T>::type;
   switch (op) {
     case PH_SWEEP: {
       const int per = n3 / 2;
       for (int k = k0; k < L.n * per; k += stride)
-        it_sweep(R, L.first + k / per, nc, k % per, a0, a1);
+        it_sweep(R, M, L.first + k / per, nc, k % per, a0, a1);
       break;
     }
     case PH_FILL: {
       const int per = 6 * nc * nc;
-      for (int k = k0; k < L.n * per; k += stride)
-        it_gc(R, L.first + k / per, k % per, I_PHI, -1, 1);
+      for (int k = k0; k < L.n * per; k += stride) it_fill(R, M, L.first + k / per, k % per);
       break;
     }
     case PH_RESID_RESTRICT:
-      for (int k = k0; k < L.n * nh; k += stride) it_resid_restrict(R, L.first + k / nh, nc, k % nh);
+      for (int k = k0; k < L.n * nh; k += stride) it_resid_restrict(R, M, L.first + k / nh, nc, k % nh);
       break;
     case PH_COARSE_RHS:
-      for (int k = k0; k < L.n * gs; k += stride) it_coarse_rhs(R, L.first + k / gs, nc, k % gs, a0);
+      for (int k = k0; k < L.n * gs; k += stride) it_coarse_rhs(R, M, L.first + k / gs, nc, k % gs, a0);
       break;
     case PH_CORR_DIFF: {
-      // whole slots, two doubles per item (slots start on 16-byte boundaries)
+      // whole slots, two values per item (slots start on 8 SLOT3-byte boundaries)
       const int h = gs / 2;
       for (int k = k0; k < L.n * h; k += stride) {
         const int id = L.first + k / h, c = k % h;
-        double2 *tmp = reinterpret_cast<double2 *>(CC(R, I_FLD, id)) + c;
-        const double2 ph = reinterpret_cast<const double2 *>(CC(R, I_PHI, id))[c], t = *tmp;
-        *tmp = make_double2(ph.x - t.x, ph.y - t.y);
+        P2 *tmp = reinterpret_cast<P2 *>(SL(M.tmp, id)) + c;
+        const P2 ph = reinterpret_cast<const P2 *>(SL(M.phi, id))[c], t = *tmp;
+        P2 o;
+        o.x = ph.x - t.x;
+        o.y = ph.y - t.y;
+        *tmp = o;
       }
       break;
     }
     case PH_CORRECT:
-      for (int k = k0; k < L.n * n3; k += stride) it_correct(R, L.first + k / n3, nc, k % n3);
+      for (int k = k0; k < L.n * n3; k += stride) it_correct(R, M, L.first + k / n3, nc, k % n3);
       break;
     case PH_COPY: {
+      // tmp = phi, whole slots
       const int h = gs / 2;
       for (int k = k0; k < L.n * h; k += stride) {
         const int id = L.first + k / h, c = k % h;
-        reinterpret_cast<double2 *>(CC(R, a1, id))[c] = reinterpret_cast<const double2 *>(CC(R, a0, id))[c];
+        reinterpret_cast<P2 *>(SL(M.tmp, id))[c] = reinterpret_cast<const P2 *>(SL(M.phi, id))[c];
       }
       break;
     }
@@ -664,20 +763,22 @@ __device__ __forceinline__ void phase(const Run3 &R, int op, int l, int a0, int 
       for (int k = k0; k < L.n * (gs + nh); k += stride) {
         const int q = k / (gs + nh);
         const int r = k % (gs + nh), id = L.first + q;
-        if (r < gs) CC(R, I_PHI, id)[r] = 0.0;
-        else it_restrict_rhs(R, id, nc, r - gs);
+        if (r < gs) SL(M.phi, id)[r] = T(0);
+        else it_restrict_rhs(R, M, id, nc, r - gs);
       }
       break;
     case PH_RESIDUAL: {
       for (int k = k0; k < L.n * n3; k += stride) {
         const int id = L.first + k / n3, t = k % n3;
-        const double h = R.geo[4 * id + 3], inv_dr_sq = 1 / (h * h);
+        const double h = R.geo[4 * id + 3];
+        const T inv_dr_sq = T(1 / (h * h));
         const int c = ix3(g, t % nc + 1, (t / nc) % nc + 1, t / (nc * nc) + 1);
-        CC(R, I_FLD, id)[c] = CC(R, I_RHS, id)[c] - lpl3(CC(R, I_PHI, id), c, g, inv_dr_sq);
+        SL(M.tmp, id)[c] = SL(M.rhs, id)[c] - lpl3(SL(M.phi, id), c, g, inv_dr_sq);
       }
       break;
     }
   }
+  (void)a1;
 }
 
 __host__ __device__ __forceinline__ long long phase_items(int op, int n, int nc) {
@@ -696,66 +797,111 @@ __host__ __device__ __forceinline__ long long phase_items(int op, int n, int nc)
 }
 
 // One phase on the grid (grid-stride over its items).
-// One kernel per phase and box size, so that each has its own registers.
-template <int NCT, int OP>
-__global__ void __launch_bounds__(NTH3) k3_phase(Run3 R, int l, int a0, int a1) {
-  phase<NCT>(R, OP, l, a0, a1, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+// One kernel per phase, box size and storage type, so that each has its own
+// registers.
+template <int NCT, int OP, class T>
+__global__ void __launch_bounds__(NTH3) k3_phase(Run3 R, MG3<T> M, int l, int a0, int a1) {
+  phase<NCT>(R, M, OP, l, a0, a1, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
+
+// Multigrid work per level visit: Gauss-Seidel cycles on the way down, on the
+// way up and on the base level (the reference: 2, 2, n_cycle_base).
+struct Sweeps3 {
+  int down, up, base;
+};
 
 // ---------------------------------------------------------------------------
 // The coarse levels lo..top in one block: the sequences of the multigrid
 // cycle that stay on those levels run as one launch, each phase spread over
 // the block's threads and ended by a block barrier.
 constexpr int NTHC = 1024;
-__device__ __forceinline__ void c_phase(const Run3 &R, int op, int l, int a0 = 0, int a1 = 0) {
-  phase<0>(R, op, l, a0, a1, threadIdx.x, NTHC);
+template <class T>
+__device__ __forceinline__ void c_phase(const Run3 &R, const MG3<T> &M, int op, int l, int a0 = 0, int a1 = 0) {
+  phase<0>(R, M, op, l, a0, a1, threadIdx.x, NTHC);
   __syncthreads();
 }
-__device__ void c_gsrb(const Run3 &R, int l, int n_cycle, bool stale) {
-  for (int it = 1; it <= 2 * n_cycle; it++) c_phase(R, PH_SWEEP, l, it, stale && it == 1 ? 1 : 0);
-  c_phase(R, PH_FILL, l);
+template <class T>
+__device__ void c_gsrb(const Run3 &R, const MG3<T> &M, int l, int n_cycle, bool stale) {
+  for (int it = 1; it <= 2 * n_cycle; it++) c_phase(R, M, PH_SWEEP, l, it, stale && it == 1 ? 1 : 0);
+  c_phase(R, M, PH_FILL, l);
 }
-__device__ void c_coarse(const Run3 &R, int l, int copy) {
-  c_phase(R, PH_RESID_RESTRICT, l);
-  c_phase(R, PH_FILL, l - 1);
-  c_phase(R, PH_COARSE_RHS, l - 1, copy);
+template <class T>
+__device__ void c_coarse(const Run3 &R, const MG3<T> &M, int l, int copy) {
+  c_phase(R, M, PH_RESID_RESTRICT, l);
+  c_phase(R, M, PH_FILL, l - 1);
+  c_phase(R, M, PH_COARSE_RHS, l - 1, copy);
 }
-__device__ void c_correct(const Run3 &R, int l) {
-  c_phase(R, PH_CORR_DIFF, l - 1);
-  c_phase(R, PH_CORRECT, l);
-  c_phase(R, PH_FILL, l);
+template <class T>
+__device__ void c_correct(const Run3 &R, const MG3<T> &M, int l) {
+  c_phase(R, M, PH_CORR_DIFF, l - 1);
+  c_phase(R, M, PH_CORRECT, l);
+  c_phase(R, M, PH_FILL, l);
 }
 // mg3_fas_vcycle (:208-255) on levels lo..top
-__device__ void c_vcycle(const Run3 &R, int top, bool stale) {
+template <class T>
+__device__ void c_vcycle(const Run3 &R, const MG3<T> &M, const Sweeps3 &S, int top, bool stale) {
   for (int l = top; l >= R.lo + 1; l--) {
-    c_gsrb(R, l, 2, false);
-    c_coarse(R, l, 1);
+    c_gsrb(R, M, l, S.down, false);
+    c_coarse(R, M, l, 1);
   }
-  c_gsrb(R, R.lo, R.n_cycle_base, stale);
+  c_gsrb(R, M, R.lo, S.base, stale);
   for (int l = R.lo + 1; l <= top; l++) {
-    c_correct(R, l);
-    c_gsrb(R, l, 2, false);
+    c_correct(R, M, l);
+    c_gsrb(R, M, l, S.up, false);
   }
 }
 enum { CM_VCYCLE = 0, CM_FMG, CM_SETC, CM_INIT };
-__global__ void __launch_bounds__(NTHC) k3_coarse(Run3 R, int mode, int top, int flag) {
+template <class T>
+__global__ void __launch_bounds__(NTHC) k3_coarse(Run3 R, MG3<T> M, Sweeps3 S, int mode, int top, int flag) {
   switch (mode) {
     case CM_VCYCLE:  // the middle of a V-cycle: down from top, base, up to top
-      c_vcycle(R, top, flag != 0);
+      c_vcycle(R, M, S, top, flag != 0);
       break;
     case CM_FMG:  // the FMG's levels lo..top (mg3_fas_fmg, :186-202); flag: first call
       for (int l = R.lo; l <= top; l++) {
-        c_phase(R, PH_COPY, l, I_PHI, I_FLD);
-        if (l > R.lo) c_correct(R, l);
-        c_vcycle(R, l, flag != 0 && l == R.lo);
+        c_phase(R, M, PH_COPY, l);
+        if (l > R.lo) c_correct(R, M, l);
+        c_vcycle(R, M, S, l, flag != 0 && l == R.lo);
       }
       break;
     case CM_SETC:  // set_coarse_phi_rhs for levels top..lo+1 (:176-180)
-      for (int l = top; l >= R.lo + 1; l--) c_coarse(R, l, 0);
+      for (int l = top; l >= R.lo + 1; l--) c_coarse(R, M, l, 0);
       break;
     case CM_INIT:  // init_phi_rhs on levels top..lo+1 (:526-549)
-      for (int l = top; l >= R.lo + 1; l--) c_phase(R, PH_INIT_PHI_RHS, l);
+      for (int l = top; l >= R.lo + 1; l--) c_phase(R, M, PH_INIT_PHI_RHS, l);
       break;
+  }
+}
+
+// The mixed form's field solve (defect correction): the FP64 residual of the
+// finest level (the leaves of a uniform octree) rhs - lpl(phi), ghost
+// neighbours from their sources with the applied voltage, into the FP32
+// correction solve's rhs (0 on ghost cells), and the correction 0 on the
+// whole slot.
+__global__ void __launch_bounds__(NTH3) k3_mx_resid(Run3 R, MG3<float> C, const int *ids) {
+  const int id = ids[blockIdx.x];
+  const int nc = R.nc[id], g = nc + 2, gs = g * g * g;
+  const MG3<double> F{VAR(R, I_PHI), VAR(R, I_RHS), VAR(R, I_FLD), R.voltage};
+  const double dr = R.geo[4 * id + 3], inv_dr_sq = 1 / (dr * dr);
+  const double *phi = SL(F.phi, id), *rhs = SL(F.rhs, id);
+  float *cr = SL(C.rhs, id), *cp = SL(C.phi, id);
+  for (int c = threadIdx.x; c < gs; c += NTH3) {
+    const int i = c % g, j = (c / g) % g, k = c / (g * g);
+    const bool in = i >= 1 && i <= nc && j >= 1 && j <= nc && k >= 1 && k <= nc;
+    cr[c] = in ? (float)(rhs[c] - lpl3_src(R, F, id, nc, phi, c, i, j, k, inv_dr_sq)) : 0.0f;
+    cp[c] = 0.0f;
+  }
+}
+// phi += c on the interior cells of every box (FP64 accumulation of the FP32
+// correction); the ghost cells are filled after it in FP64.
+__global__ void __launch_bounds__(NTH3) k3_mx_acc(Run3 R, MG3<float> C, const int *ids) {
+  const int id = ids[blockIdx.x];
+  const int nc = R.nc[id], g = nc + 2, n = nc * nc * nc;
+  double *phi = CC(R, I_PHI, id);
+  const float *cp = SL(C.phi, id);
+  for (int t = threadIdx.x; t < n; t += NTH3) {
+    const int c = ix3(g, t % nc + 1, (t / nc) % nc + 1, t / (nc * nc) + 1);
+    phi[c] = phi[c] + (double)cp[c];
   }
 }
 
@@ -929,6 +1075,9 @@ static int fail3(int code, const std::string &msg) {
     if (e_ != cudaSuccess) return fail3(A5G_ECUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
   } while (0)
 
+template <class T>
+static T *SL_host(T *a, int id) { return a + (size_t)id * SLOT3; }
+
 struct a5g3_ctx {
   a5g3_params p{};
   int max_id = 0, min_lvl = 1, max_lvl = 1;
@@ -952,7 +1101,23 @@ struct a5g3_ctx {
   cudaGraphExec_t exec = nullptr;
   double *h_red = nullptr;  // pinned, 4 doubles
 
+  // mixed precision (a5g3_set_precision): schedule of the FP32 correction
+  // solve, its three FP32 arrays (phi, rhs, tmp; cap slots each) and the
+  // FP32 copy of the table
+  int precision = A5G_FP64;
+  a5g_mg_schedule sched{1, 2, 2, 4, 1};
+  float *d_c32 = nullptr, *d_lt32 = nullptr;
+
   int coarse_top = 0;  // levels min_lvl..coarse_top run in one block (k3_coarse)
+  MG3<double> mg64() const {
+    const size_t n = (size_t)cap * SLOT3;
+    return MG3<double>{d_cc + I_PHI * n, d_cc + I_RHS * n, d_cc + I_FLD * n, voltage};
+  }
+  MG3<float> mg32() const {
+    const size_t n = (size_t)cap * SLOT3;
+    return MG3<float>{d_c32, d_c32 + n, d_c32 + 2 * n, 0.0};
+  }
+  Sweeps3 sweeps64() const { return Sweeps3{2, 2, p.n_cycle_base}; }
   int li(int l) const { return l - min_lvl; }
   int nc_of(int l) const { return l >= 1 ? p.box_size : p.box_size >> (1 - l); }
   const int *ids(int l) const { return d_ids + lv_off[li(l)]; }
@@ -970,6 +1135,7 @@ struct a5g3_ctx {
     R.off = d_off;
     R.geo = d_geo;
     R.lt = d_lt;
+    R.lt32 = d_lt32;
     R.scal = d_scal;
     R.part = d_part;
     R.cap = cap;
@@ -1119,31 +1285,33 @@ static int upload(T *&dst, const std::vector<T> &src, cudaStream_t s) {
 static void enq_gc_all(a5g3_ctx *c, int iv0, int iv1, int bc) {
   k3_gc<<<c->n_all(), NTH3, 0, c->stream>>>(c->run(), c->all_ids(), iv0, iv1, bc);
 }
-template <int NCT>
-static void launch_phase(a5g3_ctx *c, int op, int grid, int l, int a0, int a1) {
+template <int NCT, class T>
+static void launch_phase(a5g3_ctx *c, const MG3<T> &M, int op, int grid, int l, int a0, int a1) {
   const Run3 R = c->run();
   cudaStream_t s = c->stream;
   switch (op) {
-    case PH_SWEEP: k3_phase<NCT, PH_SWEEP><<<grid, NTH3, 0, s>>>(R, l, a0, a1); break;
-    case PH_FILL: k3_phase<NCT, PH_FILL><<<grid, NTH3, 0, s>>>(R, l, a0, a1); break;
-    case PH_RESID_RESTRICT: k3_phase<NCT, PH_RESID_RESTRICT><<<grid, NTH3, 0, s>>>(R, l, a0, a1); break;
-    case PH_COARSE_RHS: k3_phase<NCT, PH_COARSE_RHS><<<grid, NTH3, 0, s>>>(R, l, a0, a1); break;
-    case PH_CORR_DIFF: k3_phase<NCT, PH_CORR_DIFF><<<grid, NTH3, 0, s>>>(R, l, a0, a1); break;
-    case PH_CORRECT: k3_phase<NCT, PH_CORRECT><<<grid, NTH3, 0, s>>>(R, l, a0, a1); break;
-    case PH_COPY: k3_phase<NCT, PH_COPY><<<grid, NTH3, 0, s>>>(R, l, a0, a1); break;
-    case PH_INIT_PHI_RHS: k3_phase<NCT, PH_INIT_PHI_RHS><<<grid, NTH3, 0, s>>>(R, l, a0, a1); break;
-    case PH_RESIDUAL: k3_phase<NCT, PH_RESIDUAL><<<grid, NTH3, 0, s>>>(R, l, a0, a1); break;
+    case PH_SWEEP: k3_phase<NCT, PH_SWEEP, T><<<grid, NTH3, 0, s>>>(R, M, l, a0, a1); break;
+    case PH_FILL: k3_phase<NCT, PH_FILL, T><<<grid, NTH3, 0, s>>>(R, M, l, a0, a1); break;
+    case PH_RESID_RESTRICT: k3_phase<NCT, PH_RESID_RESTRICT, T><<<grid, NTH3, 0, s>>>(R, M, l, a0, a1); break;
+    case PH_COARSE_RHS: k3_phase<NCT, PH_COARSE_RHS, T><<<grid, NTH3, 0, s>>>(R, M, l, a0, a1); break;
+    case PH_CORR_DIFF: k3_phase<NCT, PH_CORR_DIFF, T><<<grid, NTH3, 0, s>>>(R, M, l, a0, a1); break;
+    case PH_CORRECT: k3_phase<NCT, PH_CORRECT, T><<<grid, NTH3, 0, s>>>(R, M, l, a0, a1); break;
+    case PH_COPY: k3_phase<NCT, PH_COPY, T><<<grid, NTH3, 0, s>>>(R, M, l, a0, a1); break;
+    case PH_INIT_PHI_RHS: k3_phase<NCT, PH_INIT_PHI_RHS, T><<<grid, NTH3, 0, s>>>(R, M, l, a0, a1); break;
+    case PH_RESIDUAL: k3_phase<NCT, PH_RESIDUAL, T><<<grid, NTH3, 0, s>>>(R, M, l, a0, a1); break;
   }
 }
 
 // One multigrid phase of level l on the grid, about one item per thread.
-static void enq_phase(a5g3_ctx *c, int op, int l, int a0 = 0, int a1 = 0) {
+template <class T>
+static void enq_phase(a5g3_ctx *c, const MG3<T> &M, int op, int l, int a0 = 0, int a1 = 0) {
   const long long n = phase_items(op, c->count(l), c->nc_of(l));
   const int grid = (int)std::min<long long>((n + NTH3 - 1) / NTH3, 1LL << 20);
-  if (c->nc_of(l) == NC3) launch_phase<NC3>(c, op, grid, l, a0, a1);
-  else launch_phase<0>(c, op, grid, l, a0, a1);
+  if (c->nc_of(l) == NC3) launch_phase<NC3>(c, M, op, grid, l, a0, a1);
+  else launch_phase<0>(c, M, op, grid, l, a0, a1);
 }
-static void enq_fill(a5g3_ctx *c, int l) { enq_phase(c, PH_FILL, l); }
+template <class T>
+static void enq_fill(a5g3_ctx *c, const MG3<T> &M, int l) { enq_phase(c, M, PH_FILL, l); }
 
 // gsrb_boxes (afivo/src/m_aX_mg.f90:403-426): 2 n_cycle half-sweeps with the
 // ghost sources evaluated inside the sweeps, then (fill) the ghost fill the
@@ -1152,76 +1320,118 @@ static void enq_fill(a5g3_ctx *c, int l) { enq_phase(c, PH_FILL, l); }
 // memory are left out (fill = false): the phases that follow evaluate those
 // ghost cells from their sources, and every level's ghost cells are filled
 // after its last change in a cycle.
-static void enq_gsrb(a5g3_ctx *c, int l, int n_cycle, bool stale, bool fill = true) {
-  for (int it = 1; it <= 2 * n_cycle; it++) enq_phase(c, PH_SWEEP, l, it, stale && it == 1 ? 1 : 0);
-  if (fill) enq_fill(c, l);
+template <class T>
+static void enq_gsrb(a5g3_ctx *c, const MG3<T> &M, int l, int n_cycle, bool stale, bool fill = true) {
+  for (int it = 1; it <= 2 * n_cycle; it++) enq_phase(c, M, PH_SWEEP, l, it, stale && it == 1 ? 1 : 0);
+  if (fill) enq_fill(c, M, l);
 }
 
 // update_coarse (:430-486) / set_coarse_phi_rhs (:490-523) for level l
-static void enq_coarse(a5g3_ctx *c, int l, bool copy) {
-  enq_phase(c, PH_RESID_RESTRICT, l);
-  enq_fill(c, l - 1);
-  enq_phase(c, PH_COARSE_RHS, l - 1, copy ? 1 : 0);
+template <class T>
+static void enq_coarse(a5g3_ctx *c, const MG3<T> &M, int l, bool copy) {
+  enq_phase(c, M, PH_RESID_RESTRICT, l);
+  enq_fill(c, M, l - 1);
+  enq_phase(c, M, PH_COARSE_RHS, l - 1, copy ? 1 : 0);
 }
 
 // correct_children (:374-401) of level l - 1's parents; its fill_gc_phi of
 // l is left out, as every caller smooths level l next (sweeps evaluate their
 // ghost neighbours from the sources) and fills it after that.
-static void enq_correct(a5g3_ctx *c, int l) {
-  enq_phase(c, PH_CORR_DIFF, l - 1);
-  enq_phase(c, PH_CORRECT, l);
+template <class T>
+static void enq_correct(a5g3_ctx *c, const MG3<T> &M, int l) {
+  enq_phase(c, M, PH_CORR_DIFF, l - 1);
+  enq_phase(c, M, PH_CORRECT, l);
 }
 
-static void enq_coarse_kernel(a5g3_ctx *c, int mode, int top, int flag) {
-  k3_coarse<<<1, NTHC, 0, c->stream>>>(c->run(), mode, top, flag);
+template <class T>
+static void enq_coarse_kernel(a5g3_ctx *c, const MG3<T> &M, const Sweeps3 &S, int mode, int top, int flag) {
+  k3_coarse<T><<<1, NTHC, 0, c->stream>>>(c->run(), M, S, mode, top, flag);
 }
 
 // mg3_fas_vcycle (afivo/src/m_aX_mg.f90:208-255). The levels lo..top (top =
 // the coarse section, at most max_lvl) run in one k3_coarse launch.
-static void enq_vcycle(a5g3_ctx *c, int max_lvl, bool set_residual, bool stale_base) {
+template <class T>
+static void enq_vcycle(a5g3_ctx *c, const MG3<T> &M, const Sweeps3 &S, int max_lvl, bool set_residual,
+                       bool stale_base) {
   const int lo = c->min_lvl, top = std::min(max_lvl, c->coarse_top);
   for (int l = max_lvl; l >= std::max(lo, top) + 1; l--) {
-    enq_gsrb(c, l, 2, false, false);  // the residual evaluates the ghosts itself
-    enq_coarse(c, l, true);
+    enq_gsrb(c, M, l, S.down, false, false);  // the residual evaluates the ghosts itself
+    enq_coarse(c, M, l, true);
   }
   if (top >= lo) {
-    enq_coarse_kernel(c, CM_VCYCLE, top, stale_base ? 1 : 0);
+    enq_coarse_kernel(c, M, S, CM_VCYCLE, top, stale_base ? 1 : 0);
   } else {
-    enq_gsrb(c, lo, c->p.n_cycle_base, stale_base);
+    enq_gsrb(c, M, lo, S.base, stale_base);
   }
   for (int l = std::max(lo, top) + 1; l <= max_lvl; l++) {
-    enq_correct(c, l);
-    enq_gsrb(c, l, 2, false);
+    enq_correct(c, M, l);
+    enq_gsrb(c, M, l, S.up, false);
   }
   if (set_residual)
-    for (int l = lo; l <= max_lvl; l++) enq_phase(c, PH_RESIDUAL, l);
+    for (int l = lo; l <= max_lvl; l++) enq_phase(c, M, PH_RESIDUAL, l);
 }
 
-// mg3_fas_fmg (afivo/src/m_aX_mg.f90:164-203); the coarse section's part of
-// each stage in one k3_coarse launch.
+// The FMG's stages (mg3_fas_fmg, :186-202) after its coarse set-up: on each
+// level from the coarsest, tmp = phi, the correction from the coarser level,
+// a V-cycle; the coarse section's part in one k3_coarse launch.
+template <class T>
+static void enq_fmg_stages(a5g3_ctx *c, const MG3<T> &M, const Sweeps3 &S, bool set_residual, bool first_call) {
+  const int lo = c->min_lvl, hi = c->max_lvl, top = c->coarse_top;
+  if (top >= lo) enq_coarse_kernel(c, M, S, CM_FMG, top, first_call ? 1 : 0);
+  for (int l = std::max(lo, top + 1); l <= hi; l++) {
+    enq_phase(c, M, PH_COPY, l);
+    if (l > lo) enq_correct(c, M, l);
+    enq_vcycle(c, M, S, l, set_residual && l == hi, first_call && l == lo);
+  }
+}
+
+// mg3_fas_fmg (afivo/src/m_aX_mg.f90:164-203) in FP64 on the run's variables
 static void enq_fmg(a5g3_ctx *c, bool set_residual, bool first_call) {
+  const MG3<double> M = c->mg64();
+  const Sweeps3 S = c->sweeps64();
   const int lo = c->min_lvl, hi = c->max_lvl, top = c->coarse_top;
   if (first_call) {
-    for (int l = hi; l >= std::max(lo, top) + 1; l--) enq_phase(c, PH_INIT_PHI_RHS, l);
-    if (top >= lo + 1) enq_coarse_kernel(c, CM_INIT, top, 0);
+    for (int l = hi; l >= std::max(lo, top) + 1; l--) enq_phase(c, M, PH_INIT_PHI_RHS, l);
+    if (top >= lo + 1) enq_coarse_kernel(c, M, S, CM_INIT, top, 0);
   } else {
     // (the residual evaluates the finest level's ghost cells itself, so its
     // fill_gc_phi, :497-498, is left out)
-    for (int l = hi; l >= std::max(lo, top) + 1; l--) enq_coarse(c, l, false);
-    if (top >= lo + 1) enq_coarse_kernel(c, CM_SETC, top, 0);
+    for (int l = hi; l >= std::max(lo, top) + 1; l--) enq_coarse(c, M, l, false);
+    if (top >= lo + 1) enq_coarse_kernel(c, M, S, CM_SETC, top, 0);
   }
-  if (top >= lo) enq_coarse_kernel(c, CM_FMG, top, first_call ? 1 : 0);
-  for (int l = std::max(lo, top + 1); l <= hi; l++) {
-    enq_phase(c, PH_COPY, l, I_PHI, I_FLD);
-    if (l > lo) enq_correct(c, l);
-    enq_vcycle(c, l, set_residual && l == hi, first_call && l == lo);
+  enq_fmg_stages(c, M, S, set_residual, first_call);
+}
+
+// The mixed form's field solve: per correction pass, the FP64 residual of
+// the leaves into the FP32 correction equation (homogeneous wall values),
+// restricted to the coarser levels with the correction 0 everywhere
+// (init_phi_rhs's phases on the FP32 arrays), the FP32 solve with the run's
+// schedule (FMG stages or one V-cycle), then phi += c in FP64 and the FP64
+// ghost fill of phi.
+static void enq_solve_mixed(a5g3_ctx *c) {
+  const MG3<float> C = c->mg32();
+  const Sweeps3 S{c->sched.n_cycle_down, c->sched.n_cycle_up, c->sched.n_cycle_base};
+  const int lo = c->min_lvl, hi = c->max_lvl, top = c->coarse_top;
+  for (int pass = 0; pass < c->sched.n_corr; pass++) {
+    k3_mx_resid<<<c->count(hi), NTH3, 0, c->stream>>>(c->run(), C, c->ids(hi));
+    for (int l = hi; l >= std::max(lo, top) + 1; l--) enq_phase(c, C, PH_INIT_PHI_RHS, l);
+    if (top >= lo + 1) enq_coarse_kernel(c, C, S, CM_INIT, top, 0);
+    // the coarsest level's correction: 0 (its ids are the first of the tree)
+    cudaMemsetAsync(SL_host(C.phi, c->lv_ids[c->lv_off[0]]), 0, (size_t)c->count(lo) * SLOT3 * sizeof(float),
+                    c->stream);
+    if (c->sched.fmg) enq_fmg_stages(c, C, S, false, false);
+    else enq_vcycle(c, C, S, hi, false, false);
+    k3_mx_acc<<<c->n_all(), NTH3, 0, c->stream>>>(c->run(), C, c->all_ids());
+    enq_gc_all(c, I_PHI, -1, 1);
   }
 }
 
-// compute_fld (src/streamer_3d.f90:309-345) with one FMG cycle
+// compute_fld (src/streamer_3d.f90:309-345) with one FMG cycle; in the mixed
+// form (not on a first call) the defect-correction solve
 static void enq_compute_fld(a5g3_ctx *c, bool no_guess) {
   k3_set_rhs<<<c->count(c->max_lvl), NTH3, 0, c->stream>>>(c->run(), c->ids(c->max_lvl));
-  enq_fmg(c, false, no_guess);
+  if (c->precision == A5G_MIXED && !no_guess) enq_solve_mixed(c);
+  else enq_fmg(c, false, no_guess);
   k3_fld<<<c->n_all(), NTH3, 0, c->stream>>>(c->run(), c->all_ids());
   enq_gc_all(c, I_FLD, -1, 0);
 }
@@ -1233,20 +1443,39 @@ static void enq_restrict(a5g3_ctx *c, int iv0, int iv1) {
 }
 
 // One time step (src/streamer_3d.f90:96-128): the leaves are the boxes of the
-// finest level; consistent fluxes change nothing on a uniform octree.
+// finest level; consistent fluxes change nothing on a uniform octree. The
+// mixed form runs the fluxes and the update in FP32 and the field solves by
+// defect correction.
 static void enq_step(a5g3_ctx *c) {
   const long long ncell = c->cap * SLOT3;
   k3_copy2<<<grid_for(ncell / 2), NTH3, 0, c->stream>>>(c->run(), I_ELEC, I_ELEC_OLD, I_PION, I_PION_OLD);
   const int hi = c->max_lvl;
+  const bool mx = c->precision == A5G_MIXED;
   for (int stage = 1; stage <= 2; stage++) {
-    k3_fluxes<<<c->count(hi), NTH3, 0, c->stream>>>(c->run(), c->ids(hi));
-    k3_update<<<c->count(hi), NTH3, 0, c->stream>>>(c->run(), c->ids(hi));
+    if (mx) {
+      k3_fluxes<float><<<c->count(hi), NTH3, 0, c->stream>>>(c->run(), c->ids(hi));
+      k3_update<float><<<c->count(hi), NTH3, 0, c->stream>>>(c->run(), c->ids(hi));
+    } else {
+      k3_fluxes<double><<<c->count(hi), NTH3, 0, c->stream>>>(c->run(), c->ids(hi));
+      k3_update<double><<<c->count(hi), NTH3, 0, c->stream>>>(c->run(), c->ids(hi));
+    }
     enq_restrict(c, I_ELEC, I_PION);
     enq_gc_all(c, I_ELEC, I_PION, 0);
     if (stage == 1) enq_compute_fld(c, false);
   }
   k3_average<<<grid_for(ncell), NTH3, 0, c->stream>>>(c->run());
   enq_compute_fld(c, false);
+}
+
+// The captured step holds the launch arguments (table pointers, precision):
+// settings that change them drop it, and the next step captures anew.
+static void drop_graph(a5g3_ctx *c) {
+  if (c->exec) {
+    cudaGraphExecDestroy(c->exec);
+    cudaGraphDestroy(c->graph);
+    c->exec = nullptr;
+    c->graph = nullptr;
+  }
 }
 
 static int launched(a5g3_ctx *c) {
@@ -1320,7 +1549,8 @@ int a5g3_destroy(a5g3_ctx *c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->exec) cudaGraphExecDestroy(c->exec);
   if (c->graph) cudaGraphDestroy(c->graph);
-  for (void *ptr : {(void *)c->d_cc, (void *)c->d_fc, (void *)c->d_lt, (void *)c->d_scal, (void *)c->d_part,
+  for (void *ptr : {(void *)c->d_cc, (void *)c->d_fc, (void *)c->d_lt, (void *)c->d_lt32, (void *)c->d_c32,
+                    (void *)c->d_scal, (void *)c->d_part,
                     (void *)c->d_nc, (void *)c->d_nbr, (void *)c->d_chl, (void *)c->d_par, (void *)c->d_off,
                     (void *)c->d_ids, (void *)c->d_geo})
     if (ptr) cudaFree(ptr);
@@ -1384,15 +1614,49 @@ int a5g3_set_table(a5g3_ctx *c, int n_rows, int n_cols, double x_min, double inv
   c->h_lt.assign(rc, rc + (size_t)n_rows * n_cols);
   CK3(cudaMalloc((void **)&c->d_lt, c->h_lt.size() * sizeof(double)));
   CK3(cudaMemcpy(c->d_lt, rc, c->h_lt.size() * sizeof(double), cudaMemcpyHostToDevice));
+  {
+    // FP32 copy for the lookups of the mixed form
+    std::vector<float> t32(c->h_lt.size());
+    for (size_t k = 0; k < t32.size(); k++) t32[k] = (float)c->h_lt[k];
+    if (c->d_lt32) cudaFree(c->d_lt32);
+    c->d_lt32 = nullptr;
+    CK3(cudaMalloc((void **)&c->d_lt32, t32.size() * sizeof(float)));
+    CK3(cudaMemcpy(c->d_lt32, t32.data(), t32.size() * sizeof(float), cudaMemcpyHostToDevice));
+  }
   c->lt_rows = n_rows;
   c->lt_xmin = x_min;
   c->lt_inv_dx = inv_dx;
-  if (c->exec) {
-    cudaGraphExecDestroy(c->exec);
-    cudaGraphDestroy(c->graph);
-    c->exec = nullptr;
-    c->graph = nullptr;
+  drop_graph(c);
+  return A5G_OK;
+}
+
+int a5g3_set_precision(a5g3_ctx *c, int precision, const a5g_mg_schedule *sched) {
+  if (!c) return fail3(A5G_EINVAL, "null context");
+  if (precision != A5G_FP64 && precision != A5G_MIXED) return fail3(A5G_EINVAL, "precision must be A5G_FP64 or A5G_MIXED");
+  a5g_mg_schedule s{1, 2, 2, c->p.n_cycle_base, 1};
+  if (sched) s = *sched;
+  if (s.fmg < 0 || s.fmg > 1 || s.n_cycle_down < 1 || s.n_cycle_up < 1 || s.n_cycle_base < 1 || s.n_corr < 1 ||
+      s.n_cycle_down > 8 || s.n_cycle_up > 8 || s.n_cycle_base > 64 || s.n_corr > 8)
+    return fail3(A5G_EINVAL, "bad schedule (fmg 0/1, cycles 1..8, base 1..64, corrections 1..8)");
+  if (precision == A5G_MIXED && !c->d_c32) {
+    const size_t n = (size_t)3 * c->cap * SLOT3;
+    if (cudaMalloc((void **)&c->d_c32, n * sizeof(float)) != cudaSuccess) {
+      cudaGetLastError();
+      return fail3(A5G_ENOMEM, "device allocation of the FP32 multigrid storage failed");
+    }
+    // defined contents everywhere (ghost cells of coarse rhs are carried along)
+    CK3(cudaMemsetAsync(c->d_c32, 0, n * sizeof(float), c->stream));
   }
+  c->precision = precision;
+  c->sched = s;
+  drop_graph(c);
+  return A5G_OK;
+}
+
+int a5g3_get_precision(a5g3_ctx *c, int *precision, a5g_mg_schedule *sched) {
+  if (!c) return fail3(A5G_EINVAL, "null context");
+  if (precision) *precision = c->precision;
+  if (sched) *sched = c->sched;
   return A5G_OK;
 }
 
@@ -1459,13 +1723,13 @@ static int with_dt(a5g3_ctx *c, double dt) {
 int a5g3_fluxes_koren(a5g3_ctx *c, double dt) {
   int r = ready(c);
   if (r || (r = with_dt(c, dt))) return r;
-  k3_fluxes<<<c->count(c->max_lvl), NTH3, 0, c->stream>>>(c->run(), c->ids(c->max_lvl));
+  k3_fluxes<double><<<c->count(c->max_lvl), NTH3, 0, c->stream>>>(c->run(), c->ids(c->max_lvl));
   return launched(c);
 }
 int a5g3_update_solution(a5g3_ctx *c, double dt) {
   int r = ready(c);
   if (r || (r = with_dt(c, dt))) return r;
-  k3_update<<<c->count(c->max_lvl), NTH3, 0, c->stream>>>(c->run(), c->ids(c->max_lvl));
+  k3_update<double><<<c->count(c->max_lvl), NTH3, 0, c->stream>>>(c->run(), c->ids(c->max_lvl));
   return launched(c);
 }
 int a5g3_restrict_tree(a5g3_ctx *c, int iv) {
@@ -1495,7 +1759,7 @@ int a5g3_fmg(a5g3_ctx *c, int set_residual, int first_call) {
 }
 int a5g3_vcycle(a5g3_ctx *c, int max_lvl, int set_residual) {
   if (!c || max_lvl < c->min_lvl || max_lvl > c->max_lvl) return fail3(A5G_EINVAL, "bad argument");
-  enq_vcycle(c, max_lvl, set_residual != 0, false);
+  enq_vcycle(c, c->mg64(), c->sweeps64(), max_lvl, set_residual != 0, false);
   return launched(c);
 }
 int a5g3_set_rhs(a5g3_ctx *c) {

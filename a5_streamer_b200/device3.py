@@ -198,6 +198,16 @@ class Run3:
     def step(self, dt: float):
         _lib.call3("a5g3_step", self.h, dt)
 
+    def set_precision(self, mixed: bool, schedule=None):
+        """FP64 (the reference's arithmetic) or the mixed form (include/a5g3.h
+        a5g3_set_precision); schedule: (fmg, n_cycle_down, n_cycle_up,
+        n_cycle_base, n_corr) of the FP32 correction solve, None for the
+        reference's."""
+        sp = None
+        if schedule is not None:
+            sp = ctypes.byref(_lib.MGSchedule(*[int(v) for v in schedule]))
+        _lib.call3("a5g3_set_precision", self.h, _lib.A5G_MIXED if mixed else _lib.A5G_FP64, sp)
+
     def sync(self):
         _lib.call3("a5g3_sync", self.h)
 

@@ -401,6 +401,40 @@ def run_cube_3d(level, steps, warmup, flush, clock_index, cpu_seconds=3.0):
            "ms_per_step": ms, "value": n_leaf / (ms / 1e3), "unit": UNIT,
            "algorithmic_bytes_per_step": bytes_step, "achieved_gbs": gbs, "frac_of_measured_hbm": gbs / peak,
            "clocks": clk.summary(), "l2": L2_NOTE}
+    # the mixed form from the same initial state, the same steps; errors of
+    # its end state against the FP64 run's
+    E64, z64 = head_3d(run)
+    out["mixed"] = {}
+    for name, sched in (("reference_schedule", None), ("vcycle_2corr", (0, 1, 1, 4, 2))):
+        mx = device3.Run3(cfg)
+        mx.init()
+        mx.set_precision(True, sched)
+        mx.sync()
+        for _ in range(warmup):
+            mx.step(dt)
+        mx.sync()
+        stm = torch.cuda.ExternalStream(mx.stream_ptr())
+        f0 = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        f1 = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        with ClockSampler(clock_index) as clk2:
+            with torch.cuda.stream(stm):
+                for k in range(steps):
+                    flush.fill_(k & 0xFF)
+                    f0[k].record(stm)
+                    mx.step(dt)
+                    f1[k].record(stm)
+            mx.sync()
+            torch.cuda.synchronize()
+        ms_m = sum(a.elapsed_time(b) for a, b in zip(f0, f1)) / steps
+        Em, zm = head_3d(mx)
+        out["mixed"][name] = {
+            "schedule": list(sched) if sched else [1, 2, 2, cfg.n_cycle_base, 1],
+            "ms_per_step": ms_m, "value": n_leaf / (ms_m / 1e3), "speedup_vs_fp64": ms / ms_m,
+            "errors_vs_fp64": {"steps": warmup + steps, "max_E_rel": abs(Em - E64) / E64,
+                               "head_z_rel": abs(zm - z64) / z64},
+            "clocks": clk2.summary()}
+        mx.close()
+    out["mixed"]["bounds"] = {"max_E_rel": 1e-4, "head_z_rel": 5e-3}
     run.close()
     # the oracle's 3D step on the host cores (a bounded sample on a smaller cube)
     try:
@@ -475,6 +509,20 @@ def run_adjoint(reps=3):
             "rel_err_vs_fd": rel.tolist(), "max_rel_err_vs_fd": float(rel.max()),
             "forward_s": min(tf), "gradient_s": min(tg), "gradient_over_forward": min(tg) / min(tf),
             "timing": f"wall clock, best of {reps}, each call synchronised"}
+
+
+def head_3d(run):
+    """(max |E| over the leaves, height of the cell holding it) of a 3D run."""
+    import numpy as np
+    E = run.cc(5)
+    meta = run.meta()
+    lvl, g = run.max_lvl, run.nc + 2
+    ids = run.levels()[lvl][0]
+    sub = E[ids].reshape(len(ids), g, g, g)[:, 1:-1, 1:-1, 1:-1]
+    q = np.unravel_index(np.argmax(sub), sub.shape)
+    dr = run.cfg.dr_at(lvl)
+    z = (meta[ids[q[0]], 4] - 1) * run.nc * dr + (q[1] + 0.5) * dr
+    return float(sub[q]), float(z)
 
 
 def moving_streamer_errors(schedule):

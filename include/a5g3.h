@@ -113,6 +113,18 @@ int a5g3_get_max_dt(a5g3_ctx *ctx, double *dt);
  * graph captured at the first call; dt is read from device memory, so one
  * graph serves every step. Asynchronous on the context's stream. */
 int a5g3_step(a5g3_ctx *ctx, double dt);
+/* Precision of the run's steps, as a5g_set_precision does in 2D: with
+ * A5G_MIXED the fluxes, the update and their lookups run in FP32 (densities
+ * scaled by 2^-40 inside the fluxes, accumulated in FP64), and every field
+ * solve with a guess is a defect correction -- per pass the FP64 residual of
+ * the leaves, an FP32 multigrid on the correction equation with homogeneous
+ * wall values and the schedule sched (NULL: the reference's FMG, 2, 2,
+ * n_cycle_base, one pass), and the FP64 accumulation of the potential. The
+ * densities, potential, field and step-size reductions stay FP64. The first
+ * call allocates 3 FP32 variables of the box capacity. A first solve (no
+ * guess) stays FP64. */
+int a5g3_set_precision(a5g3_ctx *ctx, int precision, const a5g_mg_schedule *sched);
+int a5g3_get_precision(a5g3_ctx *ctx, int *precision, a5g_mg_schedule *sched);
 int a5g3_sync(a5g3_ctx *ctx);
 /* The context's CUDA stream (a cudaStream_t), for event timing. */
 int a5g3_stream(a5g3_ctx *ctx, void **stream);
