@@ -417,6 +417,7 @@ def run_cube_3d(level, steps, warmup, flush, clock_index, cpu_seconds=3.0):
         f0 = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
         f1 = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
         with ClockSampler(clock_index) as clk2:
+            torch.cuda.nvtx.range_push("octree_3d_mixed_" + name)
             with torch.cuda.stream(stm):
                 for k in range(steps):
                     flush.fill_(k & 0xFF)
@@ -425,6 +426,7 @@ def run_cube_3d(level, steps, warmup, flush, clock_index, cpu_seconds=3.0):
                     f1[k].record(stm)
             mx.sync()
             torch.cuda.synchronize()
+            torch.cuda.nvtx.range_pop()
         ms_m = sum(a.elapsed_time(b) for a, b in zip(f0, f1)) / steps
         Em, zm = head_3d(mx)
         out["mixed"][name] = {
