@@ -207,7 +207,7 @@ template <class T>
 __global__ void __launch_bounds__(NTH3) k3_fluxes(Run3 R, const int *ids) {
   __shared__ T se[SLOT3], sf[SLOT3];
   const int id = ids[blockIdx.x];
-  const int nc = R.nc[id], g = nc + 2, gs = g * g * g;
+  constexpr int nc = NC3, g = nc + 2, gs = g * g * g;  // the leaves are boxes of levels >= 1
   const T ds = dscale<T>();
   {
     const double *e = CC(R, I_ELEC, id), *f = CC(R, I_FLD, id);
@@ -287,7 +287,7 @@ __global__ void __launch_bounds__(NTH3) k3_fluxes(Run3 R, const int *ids) {
 template <class T>
 __global__ void __launch_bounds__(NTH3) k3_update(Run3 R, const int *ids) {
   const int id = ids[blockIdx.x];
-  const int nc = R.nc[id], g = nc + 2, n = nc * nc * nc;
+  constexpr int nc = NC3, g = nc + 2, n = nc * nc * nc;  // the leaves are boxes of levels >= 1
   const double dt = R.scal[S_DT];
   const T tdt = T(dt);
   const T inv_dr = T(1 / R.geo[4 * id + 3]);
@@ -363,8 +363,9 @@ __global__ void __launch_bounds__(NTH3) k3_restrict(Run3 R, const int *ids, int 
 // bc = 1 sides_bc_pot (src/streamer_3d.f90:693-715): Neumann on x and y,
 // -phi at low z, 2 V - phi at high z.
 // Item t of box id: variable (t < 6 nc^2 ? iv0 : iv1), side, cell.
+template <int NCT>
 __device__ __forceinline__ void it_gc(const Run3 &R, int id, int t, int iv0, int iv1, int bc) {
-  const int nc = R.nc[id], g = nc + 2, per = nc * nc;
+  const int nc = NCT ? NCT : R.nc[id], g = nc + 2, per = nc * nc;
   const int iv = t < 6 * per ? iv0 : iv1;
   if (iv < 0) return;
   const int u = t < 6 * per ? t : t - 6 * per;
@@ -396,8 +397,12 @@ __device__ __forceinline__ void it_gc(const Run3 &R, int id, int t, int iv0, int
 }
 __global__ void __launch_bounds__(NTH3) k3_gc(Run3 R, const int *ids, int iv0, int iv1, int bc) {
   const int id = ids[blockIdx.x];
-  const int per = R.nc[id] * R.nc[id];
-  for (int t = threadIdx.x; t < 12 * per; t += NTH3) it_gc(R, id, t, iv0, iv1, bc);
+  const int nc = R.nc[id], per = nc * nc;
+  // boxes of levels >= 1 with the box size at compile time
+  if (nc == NC3)
+    for (int t = threadIdx.x; t < 12 * NC3 * NC3; t += NTH3) it_gc<NC3>(R, id, t, iv0, iv1, bc);
+  else
+    for (int t = threadIdx.x; t < 12 * per; t += NTH3) it_gc<0>(R, id, t, iv0, iv1, bc);
 }
 
 // set_init_cond and set_box_eps (src/streamer_3d.f90:217-270) on every cell
@@ -684,8 +689,8 @@ __device__ __forceinline__ void it_restrict_rhs(const Run3 &R, const MG3<T> &M, 
 // (src/streamer_3d.f90:693-715: Neumann on x and y, -phi at low z, 2 V - phi
 // at high z).
 template <class T>
-__device__ __forceinline__ void it_fill(const Run3 &R, const MG3<T> &M, int id, int t) {
-  const int nc = R.nc[id], g = nc + 2, per = nc * nc;
+__device__ __forceinline__ void it_fill(const Run3 &R, const MG3<T> &M, int id, int nc, int t) {
+  const int g = nc + 2, per = nc * nc;
   const int side = t / per, w = t - side * per;
   const int a = w % nc + 1, b = w / nc + 1;
   const int d = side >> 1;
@@ -724,7 +729,7 @@ __device__ __forceinline__ void phase(const Run3 &R, const MG3<T> &M, int op, in
     }
     case PH_FILL: {
       const int per = 6 * nc * nc;
-      for (int k = k0; k < L.n * per; k += stride) it_fill(R, M, L.first + k / per, k % per);
+      for (int k = k0; k < L.n * per; k += stride) it_fill(R, M, L.first + k / per, nc, k % per);
       break;
     }
     case PH_RESID_RESTRICT:
@@ -817,7 +822,10 @@ struct Sweeps3 {
 constexpr int NTHC = 1024;
 template <class T>
 __device__ __forceinline__ void c_phase(const Run3 &R, const MG3<T> &M, int op, int l, int a0 = 0, int a1 = 0) {
-  phase<0>(R, M, op, l, a0, a1, threadIdx.x, NTHC);
+  // levels >= 1 with the box size at compile time (the levels below hold a
+  // single box each)
+  if (lv_of(R, l).nc == NC3) phase<NC3>(R, M, op, l, a0, a1, threadIdx.x, NTHC);
+  else phase<0>(R, M, op, l, a0, a1, threadIdx.x, NTHC);
   __syncthreads();
 }
 template <class T>
@@ -919,10 +927,9 @@ __global__ void __launch_bounds__(NTH3) k3_set_rhs(Run3 R, const int *ids) {
 // fld_from_pot (src/streamer_3d.f90:348-393) on every box: the face fields
 // (eps-weighted on the box-edge faces) into the F_FLD slots and shared
 // memory, then |E| = 0.5 sqrt(sx^2 + sy^2 + sz^2) per interior cell.
-__global__ void __launch_bounds__(NTH3) k3_fld(Run3 R, const int *ids) {
-  __shared__ double sfc[3 * FSLOT3];
-  const int id = ids[blockIdx.x];
-  const int nc = R.nc[id], g = nc + 2, F = (nc + 1) * nc * nc;
+template <int NCT>
+__device__ __forceinline__ void fld_box(const Run3 &R, int id, double *sfc) {
+  const int nc = NCT ? NCT : R.nc[id], g = nc + 2, F = (nc + 1) * nc * nc;
   const double inv_dr = 1 / R.geo[4 * id + 3];
   const double *phi = CC(R, I_PHI, id), *eps = CC(R, I_EPS, id);
   for (int q = threadIdx.x; q < 3 * F; q += NTH3) {
@@ -970,6 +977,13 @@ __global__ void __launch_bounds__(NTH3) k3_fld(Run3 R, const int *ids) {
     const double sz = sfc[2 * FSLOT3 + zl] + sfc[2 * FSLOT3 + zl + nc * nc];
     fld[ix3(g, i, j, k)] = 0.5 * sqrt(sx * sx + sy * sy + sz * sz);
   }
+}
+__global__ void __launch_bounds__(NTH3) k3_fld(Run3 R, const int *ids) {
+  __shared__ double sfc[3 * FSLOT3];
+  const int id = ids[blockIdx.x];
+  // boxes of levels >= 1 with the box size at compile time
+  if (R.nc[id] == NC3) fld_box<NC3>(R, id, sfc);
+  else fld_box<0>(R, id, sfc);
 }
 
 // ---------------------------------------------------------------------------
