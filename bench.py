@@ -59,8 +59,9 @@ def parse():
                     help="fmg,down,up,base,corr: use this schedule instead of the autotuners' choice")
     ap.add_argument("--runs", type=int, default=64,
                     help="independent uneven runs of the device-driven batch (0: skip)")
-    ap.add_argument("--large-level", type=int, default=6,
-                    help="uniform level of the large-tree grid-mode extra (6: 1M leaf cells; 0: skip)")
+    ap.add_argument("--large-level", type=int, default=7,
+                    help="uniform level of the large-tree grid-mode extra (7: 4.2M leaf cells, the peak "
+                         "size the axisymmetric case's description states; 6: 1M; 0: skip)")
     ap.add_argument("--large-steps", type=int, default=10, help="timed steps of the large-tree extra")
     ap.add_argument("--cube-level", type=int, default=6,
                     help="uniform level of the 3D octree extra (6: 16.8M leaf cells; 0: skip)")
