@@ -295,6 +295,46 @@ def run_uneven_batch(n_runs, first_schedule, fixed=False):
     return out
 
 
+def run_uneven_sharded(n_runs, schedule, rank, world, device="cuda"):
+    """The uneven batch over `world` ranks: the runs dealt by estimated cost
+    (domain area, proportional to the leaf cells of the initial mesh) with
+    replicas.partition_runs, each rank stepping its share by the
+    device-driven batch with no data-path collective; the schedule of the
+    mixed form is the single-run tuner's, not re-tuned. Whole-job value:
+    cell updates summed over ranks / the slowest rank's device time. Every
+    rank makes the same reductions in the same order after its local work,
+    also when that work failed."""
+    from a5_streamer_b200 import autotune, config, replicas
+    cfgs = config.batch_cylindrical_runs(n_runs)
+    mine = replicas.partition_runs([c.domain_len[0] * c.domain_len[1] for c in cfgs], world)[rank]
+    threads = max(1, (os.cpu_count() or 1) // world)
+    out = {"runs": n_runs, "ranks": world, "runs_per_rank": len(mine), "generator": "numpy default_rng(20261203)",
+           "t_end": cfgs[0].end_time, "partition": "replicas.partition_runs by domain area (LPT)",
+           "schedule_mixed": list(schedule)}
+    for form, sc in (("fp64", None), ("mixed", tuple(schedule))):
+        ok, dev_s, cu, wall = 1.0, 0.0, 0.0, 0.0
+        err = ""
+        try:
+            if mine:
+                _, (_, gpu_ms, _, cu), wall = autotune.batch_observables([cfgs[i] for i in mine], sc,
+                                                                          n_threads=threads)
+                dev_s = gpu_ms / 1e3
+        except Exception as exc:  # reported after the reductions, which every rank makes
+            ok, err = 0.0, str(exc)
+        ok_all = -replicas.max_over_ranks(-ok, device=device)
+        dev_max = replicas.max_over_ranks(dev_s, device=device)
+        cu_sum = replicas.sum_over_ranks(cu, device=device)
+        wall_max = replicas.max_over_ranks(wall, device=device)
+        if ok_all < 1.0:
+            out[form] = {"unavailable": err or "failed on another rank"}
+        else:
+            out[form] = {"value": cu_sum / dev_max, "unit": UNIT, "device_s_max_over_ranks": dev_max,
+                         "cell_updates": cu_sum, "value_wall": cu_sum / wall_max, "wall_s_max_over_ranks": wall_max}
+    if "value" in out["fp64"] and "value" in out["mixed"]:
+        out["mixed"]["speedup_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    return out
+
+
 def run_large_tree(level, steps, warmup, flush, clock_index):
     """The grid-mode form on a large tree: the 8 mm Cartesian case on a
     uniformly refined mesh of the given level (config.cartesian_uniform;
@@ -766,11 +806,14 @@ def run_b200(args):
         adj = run_adjoint()
 
     uneven = None
-    if args.runs > 0 and rank == 0:
+    if args.runs > 0:
         sched_u = mixed["schedule"] if mixed else None
         sched_u = (sched_u["fmg"], sched_u["n_cycle_down"], sched_u["n_cycle_up"], sched_u["n_cycle_base"],
                    sched_u["n_corr"]) if sched_u else (1, 2, 2, cfg.n_cycle_base, 1)
-        uneven = run_uneven_batch(args.runs, sched_u, fixed=bool(args.mixed_schedule))
+        if world == 1:
+            uneven = run_uneven_batch(args.runs, sched_u, fixed=bool(args.mixed_schedule))
+        else:
+            uneven = run_uneven_sharded(args.runs, sched_u, rank, world)
 
     peak, peak_kind = measured_peak()
     achieved = bytes_step / (ms_per_step / 1e3) / 1e9
