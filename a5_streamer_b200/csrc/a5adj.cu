@@ -148,6 +148,11 @@ class Builder {
     tp.row_self.push_back(self);
   }
   void term(uint32_t s, double c) {
+    // the row's own entry goes into its self coefficient
+    if (s == tp.row_d.back()) {
+      tp.row_self.back() += c;
+      return;
+    }
     // merge a repeated source of the row
     for (size_t t = (size_t)tp.row_term.back(); t < tp.term_s.size(); t++)
       if (tp.term_s[t] == s) {
@@ -163,8 +168,66 @@ class Builder {
   uint32_t c(int iv, int id, int i, int j) const { return X.cc(iv, id, i, j, T.b[id].nc); }
 
   // ---- multigrid pieces (Cartesian, plain operator), afivo/src/m_aX_mg.f90
-  // box_gsrb_lpl half-sweep (:714-760) over a level's boxes
-  void gsrb_half(const std::vector<int> &ids, int redblack) {
+  // The recipe of ghost cell k of side nb of box id (a$D_gc_box with
+  // mg$D_sides_rb, :261-301, after a$D_gc_prolong0, and sides_bc_pot,
+  // src/streamer_2d.f90:620-638), times scale, into the current row.
+  void ghost_terms(int id, int nb, int k, double scale) {
+    const HBox &b = T.b[id];
+    const int nc = b.nc, nb_id = b.nb[nb], dim = nb >> 1;
+    int gi, gj;  // ghost cell
+    if (dim == 0) { gi = (nb & 1) ? nc + 1 : 0; gj = k; }
+    else { gi = k; gj = (nb & 1) ? nc + 1 : 0; }
+    if (nb_id > 0) {
+      const int ncn = T.b[nb_id].nc;
+      int si = gi, sj = gj;
+      if (dim == 0) si = (nb & 1) ? 1 : ncn;
+      else sj = (nb & 1) ? 1 : ncn;
+      term(X.cc(I_PHI, nb_id, si, sj, ncn), scale);
+    } else if (nb_id == 0) {
+      // prolong0 from the parent, then 0.5 g + f - 0.25 (f_in + f_side)
+      int off[2];
+      child_offset(b, -1, off);
+      const int p = b.parent;
+      const int ic1 = off[0] + ((gi + 1) >> 1), jc1 = off[1] + ((gj + 1) >> 1);
+      term(c(I_PHI, p, ic1, jc1), 0.5 * scale);
+      if (dim == 0) {
+        const int i = (nb & 1) ? nc : 1, di = (nb & 1) ? -1 : 1;
+        const int dj = -1 + 2 * (k & 1);
+        term(c(I_PHI, id, i, k), scale);
+        term(c(I_PHI, id, i + di, k), -0.25 * scale);
+        term(c(I_PHI, id, i, k + dj), -0.25 * scale);
+      } else {
+        const int j = (nb & 1) ? nc : 1, dj = (nb & 1) ? -1 : 1;
+        const int di = -1 + 2 * (k & 1);
+        term(c(I_PHI, id, k, j), scale);
+        term(c(I_PHI, id, k + di, j), -0.25 * scale);
+        term(c(I_PHI, id, k, j + dj), -0.25 * scale);
+      }
+    } else {
+      switch (nb) {
+        case 0: term(c(I_PHI, id, 1, k), scale); break;
+        case 1: term(c(I_PHI, id, nc, k), scale); break;
+        case 2: term(c(I_PHI, id, k, 1), -scale); break;
+        default:
+          term((uint32_t)X.v, 2.0 * scale);
+          term(c(I_PHI, id, k, nc), -scale);
+          break;
+      }
+    }
+  }
+  // phi at neighbour (ii, jj) of an interior cell, times scale: the cell
+  // itself, or with inl a side ghost through its recipe
+  void nbr_terms(int id, int ii, int jj, double scale, bool inl) {
+    const int nc = T.b[id].nc;
+    if (inl && (ii == 0 || ii == nc + 1)) ghost_terms(id, ii == 0 ? 0 : 1, jj, scale);
+    else if (inl && (jj == 0 || jj == nc + 1)) ghost_terms(id, jj == 0 ? 2 : 3, ii, scale);
+    else term(c(I_PHI, id, ii, jj), scale);
+  }
+  // box_gsrb_lpl half-sweep (:714-760) over a level's boxes. inl: the side
+  // ghosts it reads are their recipes, which equals reading them after the
+  // fill gsrb_boxes makes after every half-sweep (:343-366); without inl the
+  // ghost cells in memory are read.
+  void gsrb_half(const std::vector<int> &ids, int redblack, bool inl) {
     for (int id : ids) {
       const HBox &b = T.b[id];
       const double dx2 = b.dr * b.dr;
@@ -172,10 +235,10 @@ class Builder {
         int i0 = 2 - ((redblack ^ j) & 1);
         for (int i = i0; i <= b.nc; i += 2) {
           row(c(I_PHI, id, i, j), 0.0);
-          term(c(I_PHI, id, i + 1, j), 0.25);
-          term(c(I_PHI, id, i - 1, j), 0.25);
-          term(c(I_PHI, id, i, j + 1), 0.25);
-          term(c(I_PHI, id, i, j - 1), 0.25);
+          nbr_terms(id, i + 1, j, 0.25, inl);
+          nbr_terms(id, i - 1, j, 0.25, inl);
+          nbr_terms(id, i, j + 1, 0.25, inl);
+          nbr_terms(id, i, j - 1, 0.25, inl);
           term(c(I_RHS, id, i, j), -0.25 * dx2);
           end_row();
         }
@@ -193,68 +256,30 @@ class Builder {
     term(c(I_PHI, id, i, j + 1), scale * inv);
     term(c(I_PHI, id, i, j), -4 * scale * inv);
   }
-  // ghost cells of phi of a level's boxes: a$D_gc_box with mg$D_sides_rb
-  // (:261-301, after a$D_gc_prolong0) and sides_bc_pot
-  // (src/streamer_2d.f90:620-638)
+  // ghost cells of phi of a level's boxes (fill_gc_phi, :303-316)
   void fill_gc_phi(const std::vector<int> &ids) {
     for (int id : ids) {
-      const HBox &b = T.b[id];
-      const int nc = b.nc;
-      for (int nb = 0; nb < 4; nb++) {
-        const int nb_id = b.nb[nb], dim = nb >> 1;
+      const int nc = T.b[id].nc;
+      for (int nb = 0; nb < 4; nb++)
         for (int k = 1; k <= nc; k++) {
-          int gi, gj;  // ghost cell
-          if (dim == 0) { gi = (nb & 1) ? nc + 1 : 0; gj = k; }
+          int gi, gj;
+          if ((nb >> 1) == 0) { gi = (nb & 1) ? nc + 1 : 0; gj = k; }
           else { gi = k; gj = (nb & 1) ? nc + 1 : 0; }
           row(c(I_PHI, id, gi, gj), 0.0);
-          if (nb_id > 0) {
-            const int ncn = T.b[nb_id].nc;
-            int si = gi, sj = gj;
-            if (dim == 0) si = (nb & 1) ? 1 : ncn;
-            else sj = (nb & 1) ? 1 : ncn;
-            term(X.cc(I_PHI, nb_id, si, sj, ncn), 1.0);
-          } else if (nb_id == 0) {
-            // prolong0 from the parent, then 0.5 g + f - 0.25 (f_in + f_side)
-            int off[2];
-            child_offset(b, -1, off);
-            const int p = b.parent;
-            const int ic1 = off[0] + ((gi + 1) >> 1), jc1 = off[1] + ((gj + 1) >> 1);
-            term(c(I_PHI, p, ic1, jc1), 0.5);
-            if (dim == 0) {
-              const int i = (nb & 1) ? nc : 1, di = (nb & 1) ? -1 : 1;
-              const int dj = -1 + 2 * (k & 1);
-              term(c(I_PHI, id, i, k), 1.0);
-              term(c(I_PHI, id, i + di, k), -0.25);
-              term(c(I_PHI, id, i, k + dj), -0.25);
-            } else {
-              const int j = (nb & 1) ? nc : 1, dj = (nb & 1) ? -1 : 1;
-              const int di = -1 + 2 * (k & 1);
-              term(c(I_PHI, id, k, j), 1.0);
-              term(c(I_PHI, id, k + di, j), -0.25);
-              term(c(I_PHI, id, k, j + dj), -0.25);
-            }
-          } else {
-            switch (nb) {
-              case 0: term(c(I_PHI, id, 1, k), 1.0); break;
-              case 1: term(c(I_PHI, id, nc, k), 1.0); break;
-              case 2: term(c(I_PHI, id, k, 1), -1.0); break;
-              default:
-                term((uint32_t)X.v, 2.0);
-                term(c(I_PHI, id, k, nc), -1.0);
-                break;
-            }
-          }
+          ghost_terms(id, nb, k, 1.0);
           end_row();
         }
-      }
     }
     end_phase();
   }
-  void gsrb_boxes(const std::vector<int> &ids, int n_cycle) {
-    for (int it = 1; it <= 2 * n_cycle; it++) {
-      gsrb_half(ids, it);
-      fill_gc_phi(ids);
-    }
+  // gsrb_boxes (:343-366): the half-sweeps read their side ghosts through the
+  // recipes, and the fill after the last one is kept (later phases read the
+  // ghost cells from memory). stale: the first half-sweep reads the ghost
+  // cells as they are (the base level of a first FMG call, whose ghosts
+  // init_phi_rhs does not fill).
+  void gsrb_boxes(const std::vector<int> &ids, int n_cycle, bool stale = false) {
+    for (int it = 1; it <= 2 * n_cycle; it++) gsrb_half(ids, it, !(stale && it == 1));
+    fill_gc_phi(ids);
   }
   // rows of a parent quadrant from one child: dst(parent cell) = 0.25 sum
   // of the 2x2 child cells of var iv (box_rstr_lpl, :683-705)
@@ -399,13 +424,14 @@ class Builder {
       }
     end_phase();
   }
-  // mg$D_fas_vcycle (:208-254), set_residual false
-  void vcycle(int max_lvl) {
+  // mg$D_fas_vcycle (:208-254), set_residual false; stale_base: the base
+  // level's first half-sweep reads the ghost cells as they are
+  void vcycle(int max_lvl, bool stale_base = false) {
     for (int lvl = max_lvl; lvl >= T.min_lvl + 1; lvl--) {
       gsrb_boxes(T.L_ids(lvl), n_down);
       update_coarse(lvl);
     }
-    gsrb_boxes(T.L_ids(T.min_lvl), n_base);
+    gsrb_boxes(T.L_ids(T.min_lvl), n_base, stale_base);
     for (int lvl = T.min_lvl + 1; lvl <= max_lvl; lvl++) {
       correct_children(T.L_parents(lvl - 1));
       fill_gc_phi(T.L_ids(lvl));
@@ -424,7 +450,9 @@ class Builder {
         correct_children(T.L_parents(lvl - 1));
         fill_gc_phi(T.L_ids(lvl));
       }
-      vcycle(lvl);
+      // the first call's first base-level sweep reads the ghost cells as the
+      // previous fills left them (init_phi_rhs fills none)
+      vcycle(lvl, first_call && lvl == T.min_lvl);
     }
   }
 
