@@ -14,9 +14,9 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def declared():
     names = []
-    for h in ("a5g.h", "a5t.h", "a5g3.h"):
+    for h in ("a5g.h", "a5t.h", "a5g3.h", "a5a.h"):
         src = open(os.path.join(ROOT, "include", h)).read()
-        names += re.findall(r"^\s*(?:const\s+)?\w+\s*\*?\s*(a5(?:[gts]|g3)_\w+)\s*\(", src, re.M)
+        names += re.findall(r"^\s*(?:const\s+)?\w+\s*\*?\s*(a5(?:[gtsa]|g3)_\w+)\s*\(", src, re.M)
     return sorted(set(names))
 
 
@@ -50,6 +50,26 @@ def test_invalid_parameters_are_rejected_without_a_device():
     # null arguments
     assert _lib.lib().a5g_step(None, 1e-12) == _lib.A5G_EINVAL
     assert _lib.lib().a5g_step_batch(None, 0, None) == _lib.A5G_EINVAL
+
+
+def test_adjoint_rejects_bad_arguments_without_a_device():
+    L = _lib.lib()
+    ap = _lib.AdjParams(200, 20, 4e-3, 1.0)
+    h = ctypes.c_void_p()
+    dts = (ctypes.c_double * 200)(*([1e-12] * 200))
+    assert L.a5a_create(None, ctypes.byref(ap), dts, ctypes.byref(h)) == _lib.A5G_EINVAL
+    assert L.a5a_forward(None, None) == _lib.A5G_EINVAL
+    assert L.a5a_gradient(None, None, None, None) == _lib.A5G_EINVAL
+    assert L.a5a_destroy(None) == _lib.A5G_OK
+    sizes = (ctypes.c_longlong * 4)()
+    one = (ctypes.c_int * 16)()
+    geo = (ctypes.c_double * 4)()
+    cnt = (ctypes.c_int * 3)()
+    ids = (ctypes.c_int * 1)()
+    # a segment outside 0..8
+    assert L.a5a_debug_tape(0, 1, 1, one, geo, cnt, ids, 1, 8, 9, sizes,
+                            None, None, None, None, None, None) == _lib.A5G_EINVAL
+    assert b"segment" in L.a5g_last_error()
 
 
 def _fortran_params_layout():
