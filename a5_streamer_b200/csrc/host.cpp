@@ -11,6 +11,7 @@
 #include <climits>
 #include <cmath>
 #include <condition_variable>
+#include <cstdint>
 #include <cstring>
 #include <functional>
 #include <mutex>
@@ -936,6 +937,254 @@ int a5s_table(a5s_sim *s, double *rows_cols, double *x_min, double *inv_dx, int 
   if (inv_dx) *inv_dx = s->tbl_inv_dx;
   if (n_rows) *n_rows = s->tbl_rows;
   return A5G_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Checkpoint / resume. The reference persists nothing but output snapshots;
+// a checkpoint here is the whole state a run's next block depends on: time,
+// generator state, the tree (per-id arrays and the level lists exactly as
+// a$D_adjust_refinement left them, including the lists of level lvls_max
+// that it never rebuilds), and every cell and face variable of ids
+// 0..max_id with ghost cells. Layout (native byte order, no padding):
+//   u32 magic 'A5CK', u32 version, u64 configuration fingerprint,
+//   i32 box_size, coord, lvls_max, min_lvl, max_lvl, max_id, n_lists,
+//       cell slot, face slot, photoionization, f64 time, i32 rng[4],
+//   per id: i32 in_use, lvl, ix0, ix1, parent, n_cell, ch[4], nb[4];
+//           f64 dr, r_min0, r_min1,
+//   per list level: i32 n_ids, n_leaves, n_parents, then the three lists,
+//   f64 cc[var][id][cell slot], f64 fc[dim][var][id][face slot].
+namespace {
+
+constexpr uint32_t kCkMagic = 0x4B433541u;  // "A5CK"
+constexpr uint32_t kCkVersion = 1;
+
+struct CkWriter {
+  unsigned char *p;
+  size_t cap, n = 0;
+  void put(const void *src, size_t bytes) {
+    if (p && n + bytes <= cap) std::memcpy(p + n, src, bytes);
+    n += bytes;
+  }
+  template <class T> void v(T x) { put(&x, sizeof(T)); }
+};
+
+struct CkReader {
+  const unsigned char *p;
+  size_t len, n = 0;
+  bool ok = true;
+  void get(void *dst, size_t bytes) {
+    if (!ok || n + bytes > len) {
+      ok = false;
+      return;
+    }
+    std::memcpy(dst, p + n, bytes);
+    n += bytes;
+  }
+  template <class T> T v() {
+    T x{};
+    get(&x, sizeof(T));
+    return x;
+  }
+};
+
+// FNV-1a over the settings that change a run's arithmetic: a checkpoint is
+// only resumed by a run of the same configuration.
+uint64_t ck_fingerprint(const a5s_sim *s) {
+  uint64_t h = 1469598103934665603ull;
+  auto mix = [&](const void *q, size_t bytes) {
+    const unsigned char *b = static_cast<const unsigned char *>(q);
+    for (size_t i = 0; i < bytes; i++) h = (h ^ b[i]) * 1099511628211ull;
+  };
+  const a5g_params &d = s->cfg.dev;
+  const int ints[] = {d.box_size, d.coord, d.lvls_max, d.use_drt, d.n_cycle_base, d.n_seeds,
+                      d.photoi_enabled, d.photoi_num_photons, d.photoi_team, d.uniform_lvl,
+                      s->cfg.n_base[0], s->cfg.n_base[1], s->cfg.num_steps_amr};
+  const double dbl[] = {d.dr_base, d.domain_len_z, d.applied_fld, d.epsilon_diel, d.dt_max,
+                        d.ref_init_time, d.crv_refine, d.photoi_coeff, d.photoi_fac_dx};
+  mix(ints, sizeof(ints));
+  mix(dbl, sizeof(dbl));
+  mix(d.seed_r0, sizeof(d.seed_r0));
+  mix(d.seed_r1, sizeof(d.seed_r1));
+  mix(d.seed_width, sizeof(d.seed_width));
+  mix(s->table.data(), s->table.size() * sizeof(double));
+  return h;
+}
+
+int ck_write(a5s_sim *s, CkWriter &w) {
+  const a5t_tree *t = s->tree;
+  const int nc = t->nc, cslot = (nc + 2) * (nc + 2), fslot = (nc + 1) * nc;
+  const int nlists = (int)t->ids.size(), M = t->max_id + 1;
+  int rng[4] = {0, 0, 0, 0};
+  int r;
+  if (w.p && s->cfg.dev.photoi_enabled && (r = a5g_get_rng(s->ctx, rng))) return r;
+  w.v(kCkMagic);
+  w.v(kCkVersion);
+  w.v(ck_fingerprint(s));
+  for (int x : {nc, t->coord, t->lvls_max, t->min_lvl, t->max_lvl, t->max_id, nlists, cslot, fslot,
+                s->cfg.dev.photoi_enabled})
+    w.v(x);
+  w.v(s->time);
+  w.put(rng, sizeof(rng));
+  for (int id = 0; id < M; id++) {
+    for (int x : {(int)t->in_use[id], t->lvl[id], t->ix0[id], t->ix1[id], t->parent[id], t->ncell[id]})
+      w.v(x);
+    w.put(t->ch[id].data(), 4 * sizeof(int));
+    w.put(t->nb[id].data(), 4 * sizeof(int));
+    w.v(t->dr[id]);
+    w.v(t->rmin0[id]);
+    w.v(t->rmin1[id]);
+  }
+  for (int k = 0; k < nlists; k++) {
+    w.v((int)t->ids[k].size());
+    w.v((int)t->leaves[k].size());
+    w.v((int)t->parents[k].size());
+    w.put(t->ids[k].data(), t->ids[k].size() * sizeof(int));
+    w.put(t->leaves[k].data(), t->leaves[k].size() * sizeof(int));
+    w.put(t->parents[k].data(), t->parents[k].size() * sizeof(int));
+  }
+  std::vector<double> buf;
+  for (int iv = 0; iv < A5G_N_VAR_CELL; iv++) {
+    if (w.p) {
+      buf.resize((size_t)M * cslot);
+      if ((r = a5g_download_cc(s->ctx, iv, buf.data()))) return r;
+    }
+    w.put(buf.data(), (size_t)M * cslot * sizeof(double));
+  }
+  for (int dim = 0; dim < 2; dim++)
+    for (int f = 0; f < A5G_N_VAR_FACE; f++) {
+      if (w.p) {
+        buf.resize((size_t)M * fslot);
+        if ((r = a5g_download_fc(s->ctx, dim, f, buf.data()))) return r;
+      }
+      w.put(buf.data(), (size_t)M * fslot * sizeof(double));
+    }
+  return A5G_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int a5s_checkpoint_size(a5s_sim *s, size_t *bytes) {
+  if (!s || !bytes) return err(A5G_EINVAL, "null argument");
+  CkWriter w{nullptr, 0};
+  int r = ck_write(s, w);
+  if (r) return r;
+  *bytes = w.n;
+  return A5G_OK;
+}
+
+int a5s_checkpoint_save(a5s_sim *s, void *buf, size_t cap, size_t *written) {
+  if (!s || !buf) return err(A5G_EINVAL, "null argument");
+  size_t need = 0;
+  int r = a5s_checkpoint_size(s, &need);
+  if (r) return r;
+  if (cap < need) return err(A5G_EINVAL, "checkpoint buffer too small (a5s_checkpoint_size gives the size)");
+  CkWriter w{static_cast<unsigned char *>(buf), cap};
+  if ((r = ck_write(s, w))) return r;
+  if (written) *written = w.n;
+  return A5G_OK;
+}
+
+int a5s_checkpoint_load(a5s_sim *s, const void *buf, size_t len) {
+  if (!s || !buf) return err(A5G_EINVAL, "null argument");
+  CkReader rd{static_cast<const unsigned char *>(buf), len};
+  if (rd.v<uint32_t>() != kCkMagic || !rd.ok) return err(A5G_EINVAL, "not a checkpoint");
+  if (rd.v<uint32_t>() != kCkVersion) return err(A5G_EINVAL, "checkpoint version not supported");
+  if (rd.v<uint64_t>() != ck_fingerprint(s))
+    return err(A5G_EINVAL, "checkpoint was written by a run of another configuration");
+  int hdr[10];
+  for (int &x : hdr) x = rd.v<int>();
+  a5t_tree *cur = s->tree;
+  const int nc = hdr[0], min_lvl = hdr[3], max_lvl = hdr[4], max_id = hdr[5], nlists = hdr[6];
+  if (!rd.ok || nc != cur->nc || hdr[1] != cur->coord || hdr[2] != cur->lvls_max ||
+      min_lvl != cur->min_lvl || nlists != (int)cur->ids.size() || hdr[7] != (nc + 2) * (nc + 2) ||
+      hdr[8] != (nc + 1) * nc || hdr[9] != s->cfg.dev.photoi_enabled)
+    return err(A5G_EINVAL, "checkpoint header does not match this run");
+  if (max_id < 1 || max_lvl < 1 || max_lvl > cur->lvls_max)
+    return err(A5G_EINVAL, "checkpoint header out of range");
+  const int M = max_id + 1, cslot = hdr[7], fslot = hdr[8];
+  const size_t body = (size_t)M * (14 * sizeof(int) + 3 * sizeof(double)) +
+                      (size_t)M * (A5G_N_VAR_CELL * cslot + 2 * A5G_N_VAR_FACE * fslot) * sizeof(double);
+  if (body > len) return err(A5G_EINVAL, "checkpoint truncated");
+  const double time = rd.v<double>();
+  int rng[4];
+  rd.get(rng, sizeof(rng));
+  // the tree is built aside and swapped in only once it has been read whole
+  a5t_tree nt;
+  nt.nc = cur->nc;
+  nt.lvls_max = cur->lvls_max;
+  nt.dr_base = cur->dr_base;
+  nt.r_base[0] = cur->r_base[0];
+  nt.r_base[1] = cur->r_base[1];
+  nt.coord = cur->coord;
+  nt.min_lvl = min_lvl;
+  nt.max_lvl = max_lvl;
+  nt.grow_ids(max_id);
+  for (int id = 0; id < M; id++) {
+    nt.in_use[id] = (char)rd.v<int>();
+    nt.lvl[id] = rd.v<int>();
+    nt.ix0[id] = rd.v<int>();
+    nt.ix1[id] = rd.v<int>();
+    nt.parent[id] = rd.v<int>();
+    nt.ncell[id] = rd.v<int>();
+    rd.get(nt.ch[id].data(), 4 * sizeof(int));
+    rd.get(nt.nb[id].data(), 4 * sizeof(int));
+    nt.dr[id] = rd.v<double>();
+    nt.rmin0[id] = rd.v<double>();
+    nt.rmin1[id] = rd.v<double>();
+  }
+  nt.ids.assign(nlists, {});
+  nt.leaves.assign(nlists, {});
+  nt.parents.assign(nlists, {});
+  nt.added.assign(nlists, {});
+  auto in_range = [&](const std::vector<int> &v) {
+    for (int id : v)
+      if (id < 1 || id > max_id) return false;
+    return true;
+  };
+  for (int k = 0; k < nlists && rd.ok; k++) {
+    const int a = rd.v<int>(), b = rd.v<int>(), c = rd.v<int>();
+    if (!rd.ok || a < 0 || b < 0 || c < 0 || a > M || b > M || c > M)
+      return err(A5G_EINVAL, "checkpoint level list out of range");
+    nt.ids[k].resize(a);
+    nt.leaves[k].resize(b);
+    nt.parents[k].resize(c);
+    rd.get(nt.ids[k].data(), a * sizeof(int));
+    rd.get(nt.leaves[k].data(), b * sizeof(int));
+    rd.get(nt.parents[k].data(), c * sizeof(int));
+    if (!in_range(nt.ids[k]) || !in_range(nt.leaves[k]) || !in_range(nt.parents[k]))
+      return err(A5G_EINVAL, "checkpoint level list names an id out of range");
+  }
+  for (int id = 1; id < M && rd.ok; id++) {
+    for (int q = 0; q < 4; q++)
+      if (nt.ch[id][q] < 0 || nt.ch[id][q] > max_id || nt.nb[id][q] > max_id)
+        return err(A5G_EINVAL, "checkpoint box links out of range");
+    if (nt.parent[id] < 0 || nt.parent[id] > max_id) return err(A5G_EINVAL, "checkpoint box record out of range");
+    if (!nt.in_use[id]) continue;
+    const int l = nt.lvl[id];
+    if (l < min_lvl || l > nt.lvls_max || nt.ncell[id] != (l >= 1 ? nc : nc >> (1 - l)))
+      return err(A5G_EINVAL, "checkpoint box record out of range");
+  }
+  std::vector<double> cc((size_t)A5G_N_VAR_CELL * M * cslot), fc((size_t)2 * A5G_N_VAR_FACE * M * fslot);
+  rd.get(cc.data(), cc.size() * sizeof(double));
+  rd.get(fc.data(), fc.size() * sizeof(double));
+  if (!rd.ok) return err(A5G_EINVAL, "checkpoint truncated");
+  if (rd.n != len) return err(A5G_EINVAL, "checkpoint has trailing bytes");
+  *cur = std::move(nt);
+  int r;
+  if ((r = s->upload_tree())) return r;
+  for (int iv = 0; iv < A5G_N_VAR_CELL; iv++)
+    if ((r = a5g_upload_cc(s->ctx, iv, cc.data() + (size_t)iv * M * cslot))) return r;
+  for (int dim = 0; dim < 2; dim++)
+    for (int f = 0; f < A5G_N_VAR_FACE; f++)
+      if ((r = a5g_upload_fc(s->ctx, dim, f, fc.data() + ((size_t)dim * A5G_N_VAR_FACE + f) * M * fslot)))
+        return r;
+  if (s->cfg.dev.photoi_enabled && (r = a5g_set_rng(s->ctx, rng))) return r;
+  s->time = time;
+  return a5g_sync(s->ctx);
 }
 
 }  // extern "C"

@@ -217,6 +217,30 @@ class Simulation:
         call("a5s_table", self.h, _dp(rc), None, None, None)
         return rc.reshape(4, n.value).T.copy(), xm.value, inv.value
 
+    # -- checkpoint / resume (include/a5t.h a5s_checkpoint_*) ---------------
+    def checkpoint(self) -> bytes:
+        """The run's whole state (time, generator, tree, every cell and face
+        variable) as bytes; ``restore`` on a run of the same configuration
+        continues from it exactly."""
+        n = ctypes.c_size_t(0)
+        call("a5s_checkpoint_size", self.h, ctypes.byref(n))
+        buf = ctypes.create_string_buffer(n.value)
+        w = ctypes.c_size_t(0)
+        call("a5s_checkpoint_save", self.h, buf, n.value, ctypes.byref(w))
+        return buf.raw[:w.value]
+
+    def restore(self, data: bytes) -> None:
+        call("a5s_checkpoint_load", self.h, data, len(data))
+        self._refresh_view()
+
+    def save(self, path: str) -> None:
+        with open(path, "wb") as fh:
+            fh.write(self.checkpoint())
+
+    def load(self, path: str) -> None:
+        with open(path, "rb") as fh:
+            self.restore(fh.read())
+
 
 def run_batch(sims, t_end, use_graph: bool = True, n_threads: int = 8, groups: int = 1,
               max_blocks: int = 1 << 30):

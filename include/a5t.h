@@ -110,6 +110,28 @@ int a5s_tree(a5s_sim *s, a5t_tree **tree);
 /* The built transport table (rows_cols n_rows x 4, column-major). */
 int a5s_table(a5s_sim *s, double *rows_cols, double *x_min, double *inv_dx, int *n_rows);
 
+/* Checkpoint / resume of a run. The reference has no counterpart: it
+ * persists only output snapshots (afivo/src/m_aX_io.f90:20-600), and a run
+ * restarts from its initial conditions.
+ * A checkpoint holds everything the run's next main-loop block depends on:
+ * the simulated time, the photon generator's state, the tree (per-id
+ * records and the level lists as a$D_adjust_refinement left them) and every
+ * cell and face variable of ids 0..max_id, ghost cells included. A run
+ * resumed from it continues exactly as the run that wrote it would have.
+ * Run settings (precision and schedule, thread blocks per run, level-set
+ * boundaries) are not part of it: set them on the resumed run again.
+ *  a5s_checkpoint_size: bytes the next a5s_checkpoint_save writes;
+ *  a5s_checkpoint_save: writes it into buf (cap bytes; A5G_EINVAL if too
+ *    small); waits for the run's queued device work;
+ *  a5s_checkpoint_load: replaces the run's state with the checkpoint's.
+ *    The run must have been created from the same configuration (a
+ *    fingerprint of the settings and the transport table is compared):
+ *    A5G_EINVAL otherwise, or for a truncated or malformed buffer, and the
+ *    run is left unchanged. */
+int a5s_checkpoint_size(a5s_sim *s, size_t *bytes);
+int a5s_checkpoint_save(a5s_sim *s, void *buf, size_t cap, size_t *written);
+int a5s_checkpoint_load(a5s_sim *s, const void *buf, size_t len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -143,3 +143,8 @@ def test_new_entry_points_reject_bad_arguments_without_a_device():
     assert L.a5s_batch_run(arr, 1, te, 1, 1, 1, 1, None, None, None, None) == E  # null member
     # the allocation-free batch: null member list
     assert L.a5g_step_batch_static(None, 1, None) == E
+    # checkpoint / resume: null run or buffer
+    n = ctypes.c_size_t(0)
+    assert L.a5s_checkpoint_size(None, ctypes.byref(n)) == E
+    assert L.a5s_checkpoint_save(None, None, 0, None) == E
+    assert L.a5s_checkpoint_load(None, b"A5CK", 4) == E
