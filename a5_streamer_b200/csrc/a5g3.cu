@@ -281,10 +281,44 @@ __global__ void __launch_bounds__(NTH3) k3_fluxes(Run3 R, const int *ids) {
   }
 }
 
+// Side ghosts pushed by the box that owns their value: a cell on face side
+// (2d low, 2d+1 high) of box id is the value of the facing side ghost of the
+// same-level neighbour there (sides_from_nb, afivo/src/m_aX_gc.f90:368-402),
+// or, on a physical side, of the box's own ghost (a3_gc_neumann, :298-330).
+// On a uniform octree every side ghost of a level has exactly one such
+// writer, so a kernel that computes every box of a level can fill that
+// level's side ghosts in the same pass, with the values a3_gc_box reads
+// afterwards. (i, j, k) is the cell, v its new value; bc 1: the physical
+// sides of the potential (sides_bc_pot, src/streamer_3d.f90:693-715: -phi at
+// low z, 2 V - phi at high z, Neumann on x and y), as k3_gc.
+__device__ __forceinline__ void push_side_ghosts(const Run3 &R, int iv, int id, int nc, int i, int j, int k,
+                                                 double v, int bc = 0) {
+  const int g = nc + 2;
+  const int c[3] = {i, j, k};
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    if (c[d] != 1 && c[d] != nc) continue;
+#pragma unroll
+    for (int hi = 0; hi < 2; hi++) {
+      if (c[d] != (hi ? nc : 1)) continue;
+      const int n = R.nbr[6 * id + 2 * d + hi];
+      int q[3] = {i, j, k};
+      // the neighbour's ghost on its facing side, or the own ghost
+      q[d] = n > 0 ? (hi ? 0 : nc + 1) : (hi ? nc + 1 : 0);
+      double w = v;
+      if (n <= 0 && bc == 1 && d == 2) w = hi ? 2 * R.voltage - v : -v;
+      CC(R, iv, n > 0 ? n : id)[ix3(g, q[0], q[1], q[2])] = w;
+    }
+  }
+}
+
 // update_solution (src/streamer_3d.f90:566-615) on one leaf box per block,
 // one interior cell per thread and round; then the dielectric conversion
-// (eps > 1: n_e moves into n_i).
-template <class T>
+// (eps > 1: n_e moves into n_i). PUSH: also the side ghosts of n_e and n_i
+// on the leaves' level (push_side_ghosts; the update reads no ghost cell),
+// so that the ghost fill after the restriction covers the coarser levels
+// only.
+template <class T, bool PUSH>
 __global__ void __launch_bounds__(NTH3) k3_update(Run3 R, const int *ids) {
   const int id = ids[blockIdx.x];
   constexpr int nc = NC3, g = nc + 2, n = nc * nc * nc;  // the leaves are boxes of levels >= 1
@@ -323,6 +357,10 @@ __global__ void __launch_bounds__(NTH3) k3_update(Run3 R, const int *ids) {
     }
     e[c] = ev;
     p[c] = pv;
+    if (PUSH) {
+      push_side_ghosts(R, I_ELEC, id, nc, i, j, k, ev);
+      push_side_ghosts(R, I_PION, id, nc, i, j, k, pv);
+    }
   }
 }
 
@@ -901,15 +939,19 @@ __global__ void __launch_bounds__(NTH3) k3_mx_resid(Run3 R, MG3<float> C, const 
   }
 }
 // phi += c on the interior cells of every box (FP64 accumulation of the FP32
-// correction); the ghost cells are filled after it in FP64.
+// correction), with the FP64 ghost fill of phi (sides_bc_pot on physical
+// sides) pushed in the same pass.
 __global__ void __launch_bounds__(NTH3) k3_mx_acc(Run3 R, MG3<float> C, const int *ids) {
   const int id = ids[blockIdx.x];
   const int nc = R.nc[id], g = nc + 2, n = nc * nc * nc;
   double *phi = CC(R, I_PHI, id);
   const float *cp = SL(C.phi, id);
   for (int t = threadIdx.x; t < n; t += NTH3) {
-    const int c = ix3(g, t % nc + 1, (t / nc) % nc + 1, t / (nc * nc) + 1);
-    phi[c] = phi[c] + (double)cp[c];
+    const int i = t % nc + 1, j = (t / nc) % nc + 1, k = t / (nc * nc) + 1;
+    const int c = ix3(g, i, j, k);
+    const double v = phi[c] + (double)cp[c];
+    phi[c] = v;
+    push_side_ghosts(R, I_PHI, id, nc, i, j, k, v, 1);
   }
 }
 
@@ -975,7 +1017,9 @@ __device__ __forceinline__ void fld_box(const Run3 &R, int id, double *sfc) {
     const double sx = sfc[xl] + sfc[xl + 1];
     const double sy = sfc[FSLOT3 + yl] + sfc[FSLOT3 + yl + nc];
     const double sz = sfc[2 * FSLOT3 + zl] + sfc[2 * FSLOT3 + zl + nc * nc];
-    fld[ix3(g, i, j, k)] = 0.5 * sqrt(sx * sx + sy * sy + sz * sz);
+    const double v = 0.5 * sqrt(sx * sx + sy * sy + sz * sz);
+    fld[ix3(g, i, j, k)] = v;
+    push_side_ghosts(R, I_FLD, id, nc, i, j, k, v);
   }
 }
 __global__ void __launch_bounds__(NTH3) k3_fld(Run3 R, const int *ids) {
@@ -1436,7 +1480,6 @@ static void enq_solve_mixed(a5g3_ctx *c) {
     if (c->sched.fmg) enq_fmg_stages(c, C, S, false, false);
     else enq_vcycle(c, C, S, hi, false, false);
     k3_mx_acc<<<c->n_all(), NTH3, 0, c->stream>>>(c->run(), C, c->all_ids());
-    enq_gc_all(c, I_PHI, -1, 1);
   }
 }
 
@@ -1446,8 +1489,8 @@ static void enq_compute_fld(a5g3_ctx *c, bool no_guess) {
   k3_set_rhs<<<c->count(c->max_lvl), NTH3, 0, c->stream>>>(c->run(), c->ids(c->max_lvl));
   if (c->precision == A5G_MIXED && !no_guess) enq_solve_mixed(c);
   else enq_fmg(c, false, no_guess);
+  // the |E| side ghosts of every level are filled by k3_fld itself
   k3_fld<<<c->n_all(), NTH3, 0, c->stream>>>(c->run(), c->all_ids());
-  enq_gc_all(c, I_FLD, -1, 0);
 }
 
 // a3_restrict_tree (afivo/src/m_aX_restrict.f90:23-64) for up to two variables
@@ -1468,13 +1511,16 @@ static void enq_step(a5g3_ctx *c) {
   for (int stage = 1; stage <= 2; stage++) {
     if (mx) {
       k3_fluxes<float><<<c->count(hi), NTH3, 0, c->stream>>>(c->run(), c->ids(hi));
-      k3_update<float><<<c->count(hi), NTH3, 0, c->stream>>>(c->run(), c->ids(hi));
+      k3_update<float, true><<<c->count(hi), NTH3, 0, c->stream>>>(c->run(), c->ids(hi));
     } else {
       k3_fluxes<double><<<c->count(hi), NTH3, 0, c->stream>>>(c->run(), c->ids(hi));
-      k3_update<double><<<c->count(hi), NTH3, 0, c->stream>>>(c->run(), c->ids(hi));
+      k3_update<double, true><<<c->count(hi), NTH3, 0, c->stream>>>(c->run(), c->ids(hi));
     }
     enq_restrict(c, I_ELEC, I_PION);
-    enq_gc_all(c, I_ELEC, I_PION, 0);
+    // the leaves' side ghosts were pushed by the update: the coarser levels
+    // (the first ids of the level-ordered list)
+    if (c->n_all() > c->count(hi))
+      k3_gc<<<c->n_all() - c->count(hi), NTH3, 0, c->stream>>>(c->run(), c->all_ids(), I_ELEC, I_PION, 0);
     if (stage == 1) enq_compute_fld(c, false);
   }
   k3_average<<<grid_for(ncell), NTH3, 0, c->stream>>>(c->run());
@@ -1743,7 +1789,7 @@ int a5g3_fluxes_koren(a5g3_ctx *c, double dt) {
 int a5g3_update_solution(a5g3_ctx *c, double dt) {
   int r = ready(c);
   if (r || (r = with_dt(c, dt))) return r;
-  k3_update<double><<<c->count(c->max_lvl), NTH3, 0, c->stream>>>(c->run(), c->ids(c->max_lvl));
+  k3_update<double, false><<<c->count(c->max_lvl), NTH3, 0, c->stream>>>(c->run(), c->ids(c->max_lvl));
   return launched(c);
 }
 int a5g3_restrict_tree(a5g3_ctx *c, int iv) {
@@ -1784,7 +1830,6 @@ int a5g3_set_rhs(a5g3_ctx *c) {
 int a5g3_fld_from_pot(a5g3_ctx *c) {
   if (!c) return fail3(A5G_EINVAL, "null context");
   k3_fld<<<c->n_all(), NTH3, 0, c->stream>>>(c->run(), c->all_ids());
-  enq_gc_all(c, I_FLD, -1, 0);
   return launched(c);
 }
 
