@@ -194,6 +194,7 @@ SIGNATURES.update({
                             ctypes.POINTER(ctypes.c_longlong), _PI, _PU, _PD, _PI, _PU, _PD]),
     "a5g_set_applied_field": (_I, [_P, _D]),
     "a5s_set_init_cond": (_I, [_P]),
+    "a5t_check": (_I, [_P]),
     # checkpoint / resume (include/a5t.h)
     "a5s_checkpoint_size": (_I, [_P, ctypes.POINTER(ctypes.c_size_t)]),
     "a5s_checkpoint_save": (_I, [_P, ctypes.c_void_p, ctypes.c_size_t,

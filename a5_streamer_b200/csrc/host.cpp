@@ -1012,6 +1012,39 @@ uint64_t ck_fingerprint(const a5s_sim *s) {
   return h;
 }
 
+// The invariants a device upload relies on: every box in use is listed
+// exactly once, on its own level, among the level lists of min_lvl..max_lvl
+// (lists above max_lvl are kept as a$D_adjust_refinement leaves them);
+// leaves and parents are boxes of their level; parents, children and
+// neighbours of a box in use are in use on the adjacent / same level.
+bool tree_consistent(const a5t_tree &t) {
+  const int M = t.max_id + 1;
+  if (t.max_lvl < t.min_lvl || t.max_lvl - t.min_lvl >= (int)t.ids.size()) return false;
+  std::vector<int> seen(M, 0);
+  auto ok_id = [&](int id, int lvl) { return id >= 1 && id < M && t.in_use[id] && t.lvl[id] == lvl; };
+  for (int k = 0; k <= t.max_lvl - t.min_lvl; k++) {
+    const int lvl = t.min_lvl + k;
+    for (int id : t.ids[k])
+      if (!ok_id(id, lvl) || seen[id]++) return false;
+    for (int id : t.leaves[k])
+      if (!ok_id(id, lvl)) return false;
+    for (int id : t.parents[k])
+      if (!ok_id(id, lvl)) return false;
+  }
+  for (int id = 1; id < M; id++) {
+    if (!t.in_use[id]) continue;
+    const int l = t.lvl[id], p = t.parent[id];
+    if (seen[id] != 1 || l > t.max_lvl) return false;
+    if (l == t.min_lvl ? p != 0 : !ok_id(p, l - 1)) return false;
+    for (int q = 0; q < 4; q++) {
+      const int c = t.ch[id][q], n = t.nb[id][q];
+      if (c > 0 && (!ok_id(c, l + 1) || t.parent[c] != id)) return false;
+      if (n > 0 && !ok_id(n, l)) return false;
+    }
+  }
+  return true;
+}
+
 int ck_write(a5s_sim *s, CkWriter &w) {
   const a5t_tree *t = s->tree;
   const int nc = t->nc, cslot = (nc + 2) * (nc + 2), fslot = (nc + 1) * nc;
@@ -1066,6 +1099,12 @@ int ck_write(a5s_sim *s, CkWriter &w) {
 }  // namespace
 
 extern "C" {
+
+int a5t_check(a5t_tree *t) {
+  if (!t) return err(A5G_EINVAL, "null tree");
+  if (t->max_id == 0) return A5G_OK;
+  return tree_consistent(*t) ? A5G_OK : err(A5G_EINVAL, "tree inconsistent");
+}
 
 int a5s_checkpoint_size(a5s_sim *s, size_t *bytes) {
   if (!s || !bytes) return err(A5G_EINVAL, "null argument");
@@ -1168,6 +1207,7 @@ int a5s_checkpoint_load(a5s_sim *s, const void *buf, size_t len) {
     if (l < min_lvl || l > nt.lvls_max || nt.ncell[id] != (l >= 1 ? nc : nc >> (1 - l)))
       return err(A5G_EINVAL, "checkpoint box record out of range");
   }
+  if (!tree_consistent(nt)) return err(A5G_EINVAL, "checkpoint tree inconsistent");
   std::vector<double> cc((size_t)A5G_N_VAR_CELL * M * cslot), fc((size_t)2 * A5G_N_VAR_FACE * M * fslot);
   rd.get(cc.data(), cc.size() * sizeof(double));
   rd.get(fc.data(), fc.size() * sizeof(double));

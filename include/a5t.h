@@ -43,6 +43,12 @@ int a5t_max_lvl(a5t_tree *t);
  * written (call once with NULL lvl_ids to size it). */
 int a5t_export(a5t_tree *t, int *meta16, double *geom4, int *lvl_counts, int *lvl_ids);
 int a5t_n_level_ids(a5t_tree *t);
+/* Checks the invariants a topology upload relies on (A5G_EINVAL if one
+ * fails): every box in use listed exactly once in its level's list, leaves
+ * and parents boxes of their level, parents, children and neighbours in use
+ * on the adjacent / same level. Host only; a5s_checkpoint_load applies it to
+ * a checkpoint's tree before anything reaches the device. */
+int a5t_check(a5t_tree *t);
 /* Boxes added by the last adjust_refinement, per level min_lvl..max_lvl
  * (ref_info%lvls(lvl)%add). Returns the total. */
 int a5t_new_boxes(a5t_tree *t, int *counts, int *ids);

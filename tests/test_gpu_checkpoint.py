@@ -113,7 +113,13 @@ def test_bad_checkpoints_are_rejected_and_change_nothing():
     ck = a.checkpoint()
     before = _state(a)
     t0 = a.time
-    for bad in (b"", ck[:10], ck[:len(ck) // 2], ck + b"\0", b"XXXX" + ck[4:]):
+    # a box record whose level disagrees with its level list (header 80
+    # bytes, then 80-byte records per id; the level is the record's second int)
+    import struct
+    off = 80 + 80 * 1 + 4
+    (lvl,) = struct.unpack_from("<i", ck, off)
+    relevelled = ck[:off] + struct.pack("<i", lvl + 1) + ck[off + 4:]
+    for bad in (b"", ck[:10], ck[:len(ck) // 2], ck + b"\0", b"XXXX" + ck[4:], relevelled):
         with pytest.raises(_lib.A5GError) as e:
             a.restore(bad)
         assert e.value.code == _lib.A5G_EINVAL
@@ -129,3 +135,58 @@ def test_bad_checkpoints_are_rejected_and_change_nothing():
     c = streamer.Simulation(cfg)
     c.restore(ck)
     assert a.advance(True) == c.advance(True)
+
+
+def test_layout_is_the_documented_one():
+    """The buffer parses with the layout written out beside a5s_checkpoint_*
+    (native byte order, no padding), and its parts are the run's own tree,
+    time and cell data."""
+    import struct
+    cfg = config.cylindrical_16mm(photoi=True)
+    sim = streamer.Simulation(cfg)
+    sim.init()
+    sim.advance(True)
+    ck = sim.checkpoint()
+    magic, version, _fp = struct.unpack_from("<IIQ", ck, 0)
+    assert magic == 0x4B433541 and version == 1
+    off = 16
+    (nc, coord, lvls_max, min_lvl, max_lvl, max_id, n_lists, cslot, fslot, photoi) = \
+        struct.unpack_from("<10i", ck, off)
+    off += 40
+    (t,) = struct.unpack_from("<d", ck, off)
+    off += 8
+    rng = np.frombuffer(ck, dtype="<i4", count=4, offset=off)
+    off += 16
+    assert (nc, coord, photoi) == (8, 1, 1) and cslot == 100 and fslot == 72
+    assert t == sim.time and np.array_equal(rng, sim.device.rng_state())
+    assert (min_lvl, max_lvl, max_id) == (sim.tree.min_lvl, sim.tree.max_lvl, sim.tree.max_id)
+    rec = np.dtype([("i", "<i4", 14), ("d", "<f8", 3)])
+    recs = np.frombuffer(ck, dtype=rec, count=max_id + 1, offset=off)
+    off += rec.itemsize * (max_id + 1)
+    meta, geom, levels = sim.tree.export()
+    used = meta[:, 0] == 1
+    assert np.array_equal(recs["i"][1:, 0], meta[1:, 0])            # in_use
+    ri, rd = recs["i"][used], recs["d"][used]
+    assert np.array_equal(ri[:, 1], meta[used, 1])                  # level
+    assert np.array_equal(ri[:, 4], meta[used, 5])                  # parent
+    assert np.array_equal(ri[:, 5], meta[used, 14])                 # cells per edge
+    assert np.array_equal(ri[:, 6:10], meta[used, 6:10])            # children
+    assert np.array_equal(ri[:, 10:14], meta[used, 10:14])          # neighbours
+    assert np.array_equal(rd[:, 0], geom[used, 3])                  # dr
+    for k in range(n_lists):
+        a, b, c = struct.unpack_from("<3i", ck, off)
+        off += 12
+        lst = np.frombuffer(ck, dtype="<i4", count=a + b + c, offset=off)
+        off += 4 * (a + b + c)
+        lvl = min_lvl + k
+        if lvl in levels:
+            ids, leaves, parents = levels[lvl]
+            assert np.array_equal(lst[:a], ids) and np.array_equal(lst[a:a + b], leaves)
+            assert np.array_equal(lst[a + b:], parents)
+    cc = np.frombuffer(ck, dtype="<f8", count=9 * (max_id + 1) * cslot, offset=off)
+    off += 8 * cc.size
+    for iv in range(9):
+        x = cc[iv * (max_id + 1) * cslot:(iv + 1) * (max_id + 1) * cslot].reshape(max_id + 1, cslot)
+        assert np.array_equal(x[used], sim.device.cc(iv)[used]), iv
+    off += 8 * 2 * 2 * (max_id + 1) * fslot
+    assert off == len(ck)

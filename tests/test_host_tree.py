@@ -6,6 +6,7 @@ import pytest
 
 import a5ref
 from a5_streamer_b200 import config, streamer
+from a5_streamer_b200._lib import lib
 
 CASES = {
     "cart": config.cartesian_8mm(),
@@ -23,6 +24,9 @@ def _product_tree(cfg):
 
 
 def _same(t, sim, where):
+    # the invariants the checkpoint loader requires hold for every tree the
+    # refinement produces
+    assert lib().a5t_check(t.h) == 0, where
     meta, geom, levels = t.export()
     assert np.array_equal(meta, sim.meta()), where
     assert np.array_equal(geom, sim.geom()), where
