@@ -568,6 +568,35 @@ __device__ __forceinline__ T phi_ghost_sl(double V, const T *phi, const BoxRec &
   return isnb ? v0 : (isrb ? vrb : vbc);
 }
 
+// phi_ghost_sl with the refinement-boundary source read where the parent's
+// ghost cell takes it from: at a refinement boundary the parent has a
+// same-level neighbour on that side (2:1 balance), so the parent's ghost
+// cell under the fine ghost is a copy of that neighbour's cell (pnb). Right
+// after the parent's ghost fill both hold the same value; reading the
+// neighbour's cell lets the fills of all levels run in one phase.
+template <class T>
+__device__ __forceinline__ T phi_ghost_flat(double V, const T *phi, const BoxRec &B, int nc, int ncg,
+                                            int side, int k) {
+  const int dim = side >> 1;
+  const bool low = (side & 1) == 0;
+  const int nbb = B.nb[side];
+  const int ix = low ? 1 : nc;
+  const int own = B.base + (dim == 0 ? ix + ncg * k : k + ncg * ix);
+  const int di = low ? 1 : -1, dk = -1 + 2 * (k & 1);
+  const int h2 = (k + 1) >> 1, xc = low ? nc : 1;
+  const int pc = B.pnb[side] + (dim == 0 ? xc + ncg * (B.o1 + h2) : (B.o0 + h2) + ncg * xc);
+  const int a = own + (dim == 0 ? di : dk);
+  const int b = own + ncg * (dim == 0 ? dk : di);
+  const int cp = nbb + (dim == 0 ? (low ? nc : 1) + ncg * k : k + ncg * (low ? nc : 1));
+  const bool isnb = nbb > 0, isrb = nbb == NBR_RB;
+  const int s0 = isnb ? cp : (isrb ? pc : own);
+  const int s1 = isrb ? own : s0, s2 = isrb ? a : s0, s3 = isrb ? b : s0;
+  const T v0 = phi[s0], v1 = phi[s1], v2 = phi[s2], v3 = phi[s3];
+  const T vrb = T(0.5) * v0 + v1 - T(0.25) * (v2 + v3);
+  const T vbc = side == 2 ? -v0 : (side == 3 ? T(2 * V) - v0 : v0);
+  return isnb ? v0 : (isrb ? vrb : vbc);
+}
+
 // Neighbours (lx, hx, ly, hy) of interior cell (i, j). A cell has at most
 // one ghost neighbour in x and one in y; both are evaluated unconditionally
 // (straight-line) and selected where needed.
@@ -1677,8 +1706,20 @@ __device__ void p_mx_accumulate(const RunDev &R, const MGV<float> &M) {
     }
   }
   PSYNC();
-  const MGV<double> G{phi, VAR(R, MR), VAR(R, MT), R.boxes, R.pbx, false, R.applied_voltage, 0, 0, 0};
-  for (int lvl = R.min_lvl; lvl <= R.max_lvl; lvl++) p_fill(R, G, lvl);
+  // the FP64 ghost fill of phi on every level in one phase (phi_ghost_flat:
+  // no level waits for the coarser level's fill)
+  for (int lvl = R.min_lvl; lvl <= R.max_lvl; lvl++) {
+    const LvlInfo L = lvl_info(R, lvl);
+    const int per = 4 * L.nc, n = L.nb * per;
+    for (int k = TID(), nt_ = NTH(); k < n; k += nt_) {
+      const BoxRec &B = R.boxes[L.b0 + (k >> (L.sh + 2))];
+      const int r = k & (per - 1), side = r >> L.sh, kk = (r & (L.nc - 1)) + 1;
+      const double v = phi_ghost_flat(R.applied_voltage, (const double *)phi, B, L.nc, L.ncg, side, kk);
+      const int dim = side >> 1, gx = (side & 1) ? L.nc + 1 : 0;
+      phi[B.base + (dim == 0 ? gx + L.ncg * kk : kk + L.ncg * gx)] = v;
+    }
+  }
+  PSYNC();
 }
 
 // The mixed-precision solve of compute_fld (see above): the FP32 arrays are

@@ -111,6 +111,27 @@ class Emulator:
         out[ph & (side == 3)] = 2 * self.V - v[ph & (side == 3)]
         return out
 
+    def phi_ghost_flat(self, phi, B, nc, ncg, side, k):
+        """The device's phi_ghost_flat: phi_ghost with the refinement-boundary
+        source read from the parent's same-level neighbour (pnb) instead of
+        the parent's ghost cell."""
+        out = self.phi_ghost(phi, B, nc, ncg, side, k)
+        dim, low = side >> 1, (side & 1) == 0
+        rb = B["nb"][np.arange(len(B)), side] == NBR_RB
+        if rb.any():
+            ix = np.where(low, 1, nc)
+            own = B["base"] + np.where(dim == 0, ix + ncg * k, k + ncg * ix)
+            di = np.where(low, 1, -1)
+            dk = -1 + 2 * (k & 1)
+            xc = np.where(low, nc, 1)
+            h2 = (k + 1) >> 1
+            pn = B["pnb"][np.arange(len(B)), side]
+            pc = pn + np.where(dim == 0, xc + ncg * (B["o1"] + h2), (B["o0"] + h2) + ncg * xc)
+            a = np.where(dim == 0, own + di, own + dk)
+            b = np.where(dim == 0, own + ncg * dk, own + ncg * di)
+            out[rb] = (0.5 * phi[pc[rb]] + phi[own[rb]]) - 0.25 * (phi[a[rb]] + phi[b[rb]])
+        return out
+
     def nbrs(self, phi, B, nc, ncg, i, j, g):
         vals = []
         for side, inner, k, off in ((0, i > 1, j, -1), (1, i < nc, j, 1), (2, j > 1, i, -ncg),

@@ -62,3 +62,28 @@ def test_plan_sizes():
     # leaves (a reference quirk kept for parity)
     top = P.boxes[P.bx_off[P.nlev - 1]:P.bx_off[P.nlev]]
     assert sim.max_lvl == cfg.lvls_max and not (top["flags"] & 1).any()
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_flat_fill_equals_level_by_level_fill(name):
+    """After the oracle's FMG every level's ghost cells hold the level-by-level
+    fill of the final potential. The one-phase fill of the mixed form's
+    accumulation (phi_ghost_flat: the refinement-boundary source read from
+    the parent's same-level neighbour) must give exactly those values, from
+    the interior cells alone."""
+    cfg, sim, meta, em = _setup(name)
+    sim.op("set_rhs")
+    sim.op("fmg", 0, 0)
+    phi = np.array(sim.cc(4), dtype=np.float64).reshape(-1)
+    n_rb = 0
+    for lvl in range(em.P.min_lvl, em.P.max_lvl + 1):
+        li, nc, ncg, boxes, dr = em.lvl(lvl)
+        if len(boxes) == 0:
+            continue
+        B, side, k = em.ghosts(boxes, nc)
+        d = em.ghost_dst(B, nc, ncg, side, k)
+        v = em.phi_ghost_flat(phi, B, nc, ncg, side, k)
+        assert np.array_equal(v, phi[d]), lvl
+        n_rb += int((B["nb"][np.arange(len(B)), side] == -1).sum())
+    # the trees have refinement boundaries, so the flat source is exercised
+    assert n_rb > 0
