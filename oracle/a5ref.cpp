@@ -2681,6 +2681,54 @@ void a5ref_import_fc(a5ref_sim *h, int dimf, int f, const double *in) {
   }
 }
 
+// The tree of a run checkpoint (the layout of a5s_checkpoint_save in the
+// product library): per id 0..max_id, 14 ints (in_use, lvl, ix0, ix1,
+// parent, n_cell, children[4], neighbors[4]) and 3 doubles (dr, r_min0,
+// r_min1); the level lists of levels min_lvl .. min_lvl + n_lists - 1 as
+// counts[3 k + {0,1,2}] and the ids concatenated. Boxes in use get zeroed
+// storage (init_box) and the initial multigrid tag; cell and face data
+// follow through a5ref_import_cc / a5ref_import_fc. Returns 0, or -1 if the
+// tree does not fit this run. Lets the oracle resume from a checkpoint the
+// device path wrote.
+int a5ref_import_tree(a5ref_sim *h, int max_id, int min_lvl, int max_lvl, const int *rec_i,
+                      const double *rec_d, int n_lists, const int *counts, const int *ids) {
+  Tree &t = h->s.tree;
+  if (!rec_i || !rec_d || !counts || max_id < 1 || min_lvl != t.min_lvl ||
+      n_lists != (int)t.lv.size() || max_lvl < min_lvl || max_lvl > t.lvls_max)
+    return -1;
+  t.boxes.assign(max_id + 1, Box());
+  for (int id = 1; id <= max_id; id++) {
+    Box &b = t.boxes[id];
+    const int *r = rec_i + 14 * id;
+    const double *d = rec_d + 3 * id;
+    b.lvl = r[1];
+    b.ix[0] = r[2];
+    b.ix[1] = r[3];
+    b.parent = r[4];
+    b.n_cell = r[5];
+    for (int k = 0; k < 4; k++) b.children[k] = r[6 + k];
+    for (int k = 0; k < 4; k++) b.neighbors[k] = r[10 + k];
+    b.dr = d[0];
+    b.r_min[0] = d[1];
+    b.r_min[1] = d[2];
+    b.coord = t.coord;
+    if (r[0]) init_box(b, b.n_cell, t.n_var_cell, t.n_var_face);
+  }
+  t.max_id = max_id;
+  t.max_lvl = max_lvl;
+  int k = 0;
+  for (int q = 0; q < n_lists; q++) {
+    Level &L = t.lv[q];
+    L.ids.assign(ids + k, ids + k + counts[3 * q]);
+    k += counts[3 * q];
+    L.leaves.assign(ids + k, ids + k + counts[3 * q + 1]);
+    k += counts[3 * q + 1];
+    L.parents.assign(ids + k, ids + k + counts[3 * q + 2]);
+    k += counts[3 * q + 2];
+  }
+  return 0;
+}
+
 void a5ref_export_table(a5ref_sim *h, double *rows_cols, double *x_min, double *inv_dx,
                         int *n_rows) {
   const LT &td = h->s.td;

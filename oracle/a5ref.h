@@ -173,6 +173,10 @@ void a5ref_import_cc(a5ref_sim *s, int iv, const double *in);
 /* Face data fx/fy of face variable f: per id a slot of (nc+1)*nc doubles. */
 void a5ref_export_fc(a5ref_sim *s, int dimf, int f, double *out);
 void a5ref_import_fc(a5ref_sim *s, int dimf, int f, const double *in);
+/* The tree of a run checkpoint (per-id records and level lists in the
+ * layout of a5s_checkpoint_save); data follow with a5ref_import_cc/_fc. */
+int a5ref_import_tree(a5ref_sim *s, int max_id, int min_lvl, int max_lvl, const int *rec_i,
+                      const double *rec_d, int n_lists, const int *counts, const int *ids);
 /* The built lookup table rows_cols (n_rows x 4, column-major) and x grid. */
 void a5ref_export_table(a5ref_sim *s, double *rows_cols, double *x_min,
                         double *inv_dx, int *n_rows);

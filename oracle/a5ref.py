@@ -100,6 +100,7 @@ def lib() -> ctypes.CDLL:
             "a5ref_export_levels": (I, [P, pi, pi, I]),
             "a5ref_export_cc": (V, [P, I, pd]), "a5ref_import_cc": (V, [P, I, pd]),
             "a5ref_export_fc": (V, [P, I, I, pd]), "a5ref_import_fc": (V, [P, I, I, pd]),
+            "a5ref_import_tree": (I, [P, I, I, I, pi, pd, I, pi, pi]),
             "a5ref_export_table": (V, [P, pd, pd, pd, pi]),
             "a5ref_applied_voltage": (D, [P]),
             "a5ref_kat_mg2_2d": (I, [I, pd, pd, pi]), "a5ref_kat_mg_cyl": (I, [I, pd, pd, pi]),
@@ -457,6 +458,90 @@ class Sim:
     def set_rng_state(self, st) -> None:
         st = np.ascontiguousarray(st, dtype=np.int32)
         lib().a5ref_rng_set(self.h, _ip(st))
+
+    # run checkpoints in the product's layout (a5s_checkpoint_save) -------
+    _CK_MAGIC, _CK_VERSION = 0x4B433541, 1
+
+    def checkpoint(self) -> bytes:
+        """This run's state in the layout of a5s_checkpoint_save (native
+        little-endian, fingerprint 0); the level lists above max_lvl, which no
+        operation reads before rebuilding them, are written empty."""
+        import struct
+        nc, M = self.nc, self.max_id + 1
+        n_lists = self.cfg.lvls_max + 2 - self.min_lvl
+        photoi = 1 if self.cfg.photoi_enabled else 0
+        rng = self.rng_state() if photoi else np.zeros(4, dtype=np.int32)
+        out = [struct.pack("<IIQ", self._CK_MAGIC, self._CK_VERSION, 0),
+               struct.pack("<10i", nc, 1 if self.cfg.coord == "cyl" else 0, self.cfg.lvls_max,
+                           self.min_lvl, self.max_lvl, self.max_id, n_lists, (nc + 2) ** 2,
+                           (nc + 1) * nc, photoi),
+               struct.pack("<d", self.time), rng.astype("<i4").tobytes()]
+        meta, geom = self.meta(), self.geom()
+        rec = np.zeros(M, dtype=[("i", "<i4", 14), ("d", "<f8", 3)])
+        rec["i"][:, 0:4] = meta[:, 0:4]
+        rec["i"][:, 4] = meta[:, 5]
+        rec["i"][:, 5] = meta[:, 14]
+        rec["i"][:, 6:14] = meta[:, 6:14]
+        rec["d"][:, 0] = geom[:, 3]
+        rec["d"][:, 1:3] = geom[:, 0:2]
+        out.append(rec.tobytes())
+        levels = self.levels()
+        for k in range(n_lists):
+            a, b, c = levels.get(self.min_lvl + k, ([], [], []))
+            out.append(struct.pack("<3i", len(a), len(b), len(c)))
+            out.append(np.concatenate([np.asarray(x, dtype="<i4") for x in (a, b, c)]).tobytes())
+        for iv in range(9):
+            out.append(self.cc(iv).astype("<f8").tobytes())
+        for d in range(2):
+            for f in range(2):
+                out.append(self.fc(d, f).astype("<f8").tobytes())
+        return b"".join(out)
+
+    def load_checkpoint(self, buf: bytes) -> None:
+        """Resume from a checkpoint in the layout of a5s_checkpoint_save, for
+        instance one the device path wrote (the fingerprint is not checked)."""
+        import struct
+        magic, version, _ = struct.unpack_from("<IIQ", buf, 0)
+        if (magic, version) != (self._CK_MAGIC, self._CK_VERSION):
+            raise ValueError("not a checkpoint of this layout")
+        nc, _coord, _lm, min_lvl, max_lvl, max_id, n_lists, cslot, fslot, photoi = \
+            struct.unpack_from("<10i", buf, 16)
+        if nc != self.nc or cslot != (nc + 2) ** 2 or fslot != (nc + 1) * nc:
+            raise ValueError("checkpoint of another box size")
+        (t,) = struct.unpack_from("<d", buf, 56)
+        rng = np.frombuffer(buf, dtype="<i4", count=4, offset=64)
+        off = 80
+        M = max_id + 1
+        rec = np.frombuffer(buf, dtype=[("i", "<i4", 14), ("d", "<f8", 3)], count=M, offset=off)
+        off += rec.itemsize * M
+        counts, ids = [], []
+        for _ in range(n_lists):
+            a, b, c = struct.unpack_from("<3i", buf, off)
+            off += 12
+            counts += [a, b, c]
+            ids.append(np.frombuffer(buf, dtype="<i4", count=a + b + c, offset=off))
+            off += 4 * (a + b + c)
+        ri = np.ascontiguousarray(rec["i"], dtype=np.int32)
+        rd = np.ascontiguousarray(rec["d"], dtype=np.float64)
+        cnt = np.asarray(counts, dtype=np.int32)
+        idv = np.ascontiguousarray(np.concatenate(ids + [np.zeros(1, dtype="<i4")]), dtype=np.int32)
+        if lib().a5ref_import_tree(self.h, max_id, min_lvl, max_lvl, _ip(ri), _dp(rd), n_lists,
+                                   _ip(cnt), _ip(idv)) != 0:
+            raise ValueError("checkpoint tree does not fit this run")
+        for iv in range(9):
+            x = np.frombuffer(buf, dtype="<f8", count=M * cslot, offset=off)
+            off += 8 * M * cslot
+            self.set_cc(iv, x.reshape(M, cslot))
+        for d in range(2):
+            for f in range(2):
+                x = np.frombuffer(buf, dtype="<f8", count=M * fslot, offset=off)
+                off += 8 * M * fslot
+                self.set_fc(d, f, x.reshape(M, fslot))
+        if off != len(buf):
+            raise ValueError("checkpoint length does not match its header")
+        self.time = t
+        if photoi:
+            self.set_rng_state(rng)
 
     def photon_table(self):
         """(distances at the table's cumulative fractions, frac_in_tbl, absorption level)"""
