@@ -22,6 +22,10 @@ from typing import Dict, Optional, Sequence
 import numpy as np
 
 VTK_PIXEL = 8
+# output names of the cell variables (src/m_streamer.f90:17-43 order) and the
+# set the streamer programs write by default
+CC_NAMES = ["e", "i", "e_old", "i_old", "phi", "fld", "rhs", "pho", "eps"]
+DEFAULT_NAMES = ["e", "i", "phi", "fld", "rhs", "pho", "eps"]
 
 
 def leaf_mesh(meta: np.ndarray, geom: np.ndarray, levels) -> Dict[str, np.ndarray]:
@@ -155,19 +159,22 @@ def write_run(filename: str, sim, names: Optional[Sequence[str]] = None, n_cycle
     (electron and ion density, potential, |E|, space charge, photoionization,
     eps) and the cell-averaged electron flux and field, as the streamer
     programs do with their output variable names."""
-    from .device import N_VAR_CELL
-    all_names = ["e", "i", "e_old", "i_old", "phi", "fld", "rhs", "pho", "eps"]
-    names = list(names) if names is not None else ["e", "i", "phi", "fld", "rhs", "pho", "eps"]
     meta, geom, levels = sim.tree.export()
+    return write_state(filename, meta, geom, levels, sim.device.cc, sim.device.fc, sim.time,
+                       names, n_cycle)
+
+
+def write_state(filename: str, meta, geom, levels, cc, fc, time: float,
+                names: Optional[Sequence[str]] = None, n_cycle: int = 0) -> str:
+    """``write_run`` from any source of a run's state: cc(iv) and fc(dim, f)
+    give variables in the download layout (a device run, or a checkpoint read
+    on the host)."""
+    names = list(names) if names is not None else list(DEFAULT_NAMES)
     mesh = leaf_mesh(meta, geom, levels)
-    data = {}
-    for n in names:
-        iv = all_names.index(n)
-        assert iv < N_VAR_CELL
-        data[n] = cell_values(mesh, sim.device.cc(iv))
-    fx, fy = face_means(mesh, sim.device.fc(0, 0), sim.device.fc(1, 0))
+    data = {n: cell_values(mesh, cc(CC_NAMES.index(n))) for n in names}
+    fx, fy = face_means(mesh, fc(0, 0), fc(1, 0))
     data["flux_x"], data["flux_y"] = fx, fy
-    return write_vtk(filename, meta, geom, levels, data, time=sim.time, n_cycle=n_cycle)
+    return write_vtk(filename, meta, geom, levels, data, time=time, n_cycle=n_cycle)
 
 
 def axis_profile(fld: np.ndarray, dens: np.ndarray, meta, geom, levels, cfg):

@@ -59,3 +59,57 @@ def test_malformed_checkpoints_are_rejected():
         b.load_checkpoint(b"XXXX" + ck[4:])
     with pytest.raises(ValueError):
         b.load_checkpoint(ck + b"\0" * 8)
+
+
+def test_host_reader_gives_the_run_state(tmp_path):
+    """a5_streamer_b200.checkpoint reads a checkpoint on the host into the
+    package's formats: the tree as Tree.export gives it, the cell and face
+    variables in the download layout, time and generator state."""
+    from a5_streamer_b200 import checkpoint
+    cfg = config.cylindrical_16mm(photoi=True)
+    sim = a5ref.Sim(cfg, n_threads=2)
+    sim.init()
+    sim.advance(True)
+    path = tmp_path / "run.a5ck"
+    path.write_bytes(sim.checkpoint())
+    ck = checkpoint.load(str(path))
+    assert ck.time == sim.time and np.array_equal(ck.rng, sim.rng_state())
+    assert (ck.min_lvl, ck.max_lvl, ck.max_id) == (sim.min_lvl, sim.max_lvl, sim.max_id)
+    assert ck.coord == 1 and ck.photoionization and ck.box_size == cfg.box_size
+    assert np.array_equal(ck.meta, sim.meta()) and np.array_equal(ck.geom, sim.geom())
+    rl = sim.levels()
+    assert sorted(ck.levels) == sorted(rl)
+    for lvl in rl:
+        for x, y in zip(ck.levels[lvl], rl[lvl]):
+            assert np.array_equal(x, y)
+    for iv in range(9):
+        assert np.array_equal(ck.cc[iv], sim.cc(iv)), iv
+    for d in range(2):
+        for f in range(2):
+            assert np.array_equal(ck.fc[2 * d + f], sim.fc(d, f))
+    assert ck.n_leaf_cells() == sim.n_leaf_cells()
+
+
+def test_vtk_from_a_checkpoint_equals_the_live_output(tmp_path):
+    from a5_streamer_b200 import checkpoint, output
+    cfg = config.cartesian_8mm()
+    sim = a5ref.Sim(cfg, n_threads=2)
+    sim.init()
+    sim.advance(True)
+    path = tmp_path / "run.a5ck"
+    path.write_bytes(sim.checkpoint())
+    a = checkpoint.write_vtk(str(path), str(tmp_path / "from_ck"))
+    b = output.write_state(str(tmp_path / "live"), sim.meta(), sim.geom(), sim.levels(),
+                           sim.cc, sim.fc, sim.time)
+    assert open(a, "rb").read() == open(b, "rb").read()
+
+
+def test_host_reader_rejects_malformed_buffers():
+    from a5_streamer_b200 import checkpoint
+    cfg = config.cartesian_8mm()
+    sim = a5ref.Sim(cfg, n_threads=2)
+    sim.init()
+    ck = sim.checkpoint()
+    for bad in (b"", ck[:40], b"XXXX" + ck[4:], ck[:-8], ck + b"\0" * 8):
+        with pytest.raises(ValueError):
+            checkpoint.read(bad)
