@@ -113,3 +113,16 @@ def test_host_reader_rejects_malformed_buffers():
     for bad in (b"", ck[:40], b"XXXX" + ck[4:], ck[:-8], ck + b"\0" * 8):
         with pytest.raises(ValueError):
             checkpoint.read(bad)
+
+
+def test_host_reader_and_library_agree_on_the_header():
+    """The magic and version the host reader expects are the library's."""
+    import os
+    import re
+    from a5_streamer_b200 import checkpoint
+    src = open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                            "a5_streamer_b200", "csrc", "host.cpp")).read()
+    magic = int(re.search(r"kCkMagic = (0x[0-9A-Fa-f]+)u", src).group(1), 16)
+    version = int(re.search(r"kCkVersion = (\d+)", src).group(1))
+    assert (magic, version) == (checkpoint.MAGIC, checkpoint.VERSION)
+    assert (magic, version) == (a5ref.Sim._CK_MAGIC, a5ref.Sim._CK_VERSION)
